@@ -1,0 +1,248 @@
+/*
+ * fcm_b200.h -- C-ABI of the B200-native fluctuating force-coupling-method (FCM)
+ * mobility solve for Brownian suspensions of rigid multi-blob bodies.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, and returns an
+ * int status (FCM_OK == 0).  Array arguments may be HOST or DEVICE pointers: the
+ * library inspects each pointer (cudaPointerGetAttributes) and copies as needed.
+ * Host arrays are borrowed for the duration of the call only.  Device buffers are
+ * owned by the context.  A context is not thread-safe; separate contexts may run on
+ * separate streams.  All work is issued on the context's stream (fcm_set_stream);
+ * calls that return data to a host pointer synchronise that stream.
+ *
+ * The functions replace the public methods of the reference's five C++ classes
+ * (fft_solver, fcm_fluid_solver, collection_of_rigid_bodies, linked_list,
+ * gmres_solver).  Each declaration cites the reference method it replaces as
+ * file:line within the reference project.  The reference's MPI domain
+ * decomposition is collapsed to one rank on one GPU: every MPI_Allreduce in the
+ * replaced methods becomes a local sum.
+ *
+ * Array layouts (all FP64 at the boundary):
+ *   blob_ref_pos : 3*nb, blob-major (x,y,z of blob m at 3m..3m+2); the columns of
+ *                  the reference's `blob_ref_pos` (3 x nb) matrix.
+ *   Y            : Nb*3, blob-major xyz (row np of the reference's `all_blob_pos`).
+ *   F, V, lambda : 3*Nb, index 3*np+c (the reference's `vec` layout).
+ *   body x, q    : 3*M and 4*M (q = scalar part then vector part).
+ *   U (bodies)   : 6*M, (Ux,Uy,Uz,Wx,Wy,Wz) per body.
+ *   system vec   : 3*Nb + 6*M = [lambda ; U] (gmres_solver.cpp:60).
+ *   grid arrays  : the reference's FFTW layout: real [x][y][pad] with
+ *                  pad = 2*(nz/2+1); after a forward transform the complex
+ *                  result is in FFTW_TRANSPOSED_ORDER [y][x][kz] (re,im).
+ */
+#ifndef FCM_B200_H
+#define FCM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+enum fcm_status {
+  FCM_OK = 0,
+  FCM_ERR_INVALID = 1,       /* bad argument or parameter                        */
+  FCM_ERR_CUDA = 2,          /* CUDA runtime error (message in fcm_last_error)    */
+  FCM_ERR_CUFFT = 3,         /* cuFFT error                                       */
+  FCM_ERR_STATE = 4,         /* call out of order (e.g. interpolation before
+                                fcm_set_up_gaussians)                             */
+  FCM_ERR_NOT_CONVERGED = 5, /* GMRES reached max_iter above tol; the iterate is
+                                still returned, as gmres_solver.cpp:294-300 does  */
+  FCM_ERR_NONFINITE = 6,     /* a NaN/Inf appeared (residual, forces, velocities) */
+  FCM_ERR_OVERLAP = 7,       /* prohibited overlap after a step; bodies restored  */
+  FCM_ERR_NOMEM = 8,         /* device allocation failed                          */
+  FCM_ERR_CAPACITY = 9       /* caller-provided output buffer too small           */
+};
+
+/* ------------------------------------------------------------------ parameters
+ * Runtime replacements for the compile-time macros of config.hpp.  Defaults
+ * (fcm_default_params) follow config.hpp with SLIP_CHANNEL false and
+ * SIMULATION_ALGORITHM 2 (Euler-Maruyama). */
+typedef struct fcm_params {
+  int32_t nx, ny, nz;        /* NUM_FFT_GRID_POINTS_{X,Y,Z} (config.hpp:65-67)     */
+  int32_t ngauss;            /* NUM_FCM_GAUSSIAN_POINTS, stencil width W (:69)     */
+  double dx;                 /* DX, grid spacing; box side L_d = dx*n_d (:88-91)   */
+  double blob_radius;        /* BLOB_RADIUS a (:48)                                */
+  double viscosity;          /* FLUID_VISCOSITY eta (:49)                          */
+  double kT;                 /* ENERGY_SCALE (:50)                                 */
+  double dt;                 /* DT (:84)                                           */
+  int32_t num_bodies;        /* NUM_BODIES M (:47)                                 */
+  int32_t blobs_per_body;    /* nb (collection_of_rigid_bodies.cpp:21-32)          */
+  int32_t ncells;            /* NUM_LINKED_LIST_CELLS_PER_DIM (:71), must be >= 3  */
+  int32_t potential;         /* INTERACTION_POTENTIAL_TYPE (:20): 0 soft sphere,
+                                1 hydrophobic, 2 hydrophilic (linked_list.cpp:362-497);
+                                3 = polynomial repulsion F_s((rc^2-r^2)/(rc^2-4a^2))^4
+                                for r < rc (no counterpart in the reference)       */
+  double steric_fs;          /* potential 3: force scale F_s                       */
+  double steric_rc;          /* potential 3: cutoff r_c                            */
+  int32_t gmres_max_iter;    /* GMRES_MAX_ITER (:63)                               */
+  double gmres_tol;          /* GMRES_TOL (:62), relative residual                 */
+  double fd_delta;           /* FINITE_DIFFERENCE_DELTA_FACTOR (:73)               */
+  int32_t algorithm;         /* SIMULATION_ALGORITHM (:26): 1 = GDC, 2 = EM        */
+  int32_t precision;         /* 0 = FP64 throughout; 1 = FP32 grid work (spread,
+                                FFT, projection, interpolation) inside FP64
+                                iterative refinement                               */
+  int32_t noise;             /* 1 = fluctuating stress on (main.cpp:231),
+                                0 = noise off (deterministic runs)                  */
+  int32_t skip_on_overlap;   /* SKIP_ON_OVERLAP (:35)                              */
+} fcm_params;
+
+/* Per-step diagnostics returned by fcm_step. */
+typedef struct fcm_step_info {
+  int32_t gmres_iters;       /* Krylov iterations (sum over refinement sweeps)     */
+  int32_t refinement_sweeps; /* outer FP64 sweeps (1 for precision 0)              */
+  double gmres_rel_residual; /* final relative residual of the saddle-point system */
+  double divU;               /* GDC drift divergence (0 for EM)                    */
+  int32_t overlap;           /* 1 if the step was rejected and bodies restored     */
+  int32_t status;            /* status of the GMRES solve                          */
+} fcm_step_info;
+
+typedef struct fcm_ctx fcm_ctx;   /* opaque solver context: one suspension */
+typedef struct fcm_fft fcm_fft;   /* opaque standalone 3-D real FFT        */
+
+/* Fill *p with config.hpp's defaults (single body type, 256^3 grid ...). */
+void fcm_default_params(fcm_params* p);
+
+/* Text of the last error recorded on this thread (never NULL). */
+const char* fcm_last_error(void);
+
+/* Library version string. */
+const char* fcm_version(void);
+
+/* ================================================================ fft_solver
+ * fft_solver.hpp:10-31.  In-place 3-D real transforms on an array of
+ * total_local_size = nx*ny*pad doubles, unnormalised, forward sign e^{-iqx},
+ * k-space result in FFTW_TRANSPOSED_ORDER [y][x][kz].  The inverse treats its
+ * input as FFTW 2.x's rfftwnd does: complex inverse transforms along x and y,
+ * then a half-complex-to-real transform along z that ignores the imaginary parts
+ * of the kz = 0 and kz = nz/2 terms. */
+int fcm_fft_create(int32_t nx, int32_t ny, int32_t nz, fcm_fft** out);   /* fft_solver.cpp:17-28 initialise */
+int fcm_fft_destroy(fcm_fft* f);                                           /* fft_solver.cpp:8-15 ~fft_solver */
+int fcm_fft_local_sizes(const fcm_fft* f, int32_t* local_nx, int32_t* local_x_start,
+                        int32_t* local_ny_after_transpose,
+                        int32_t* local_y_start_after_transpose,
+                        int64_t* total_local_size, int32_t* pad);          /* fft_solver.cpp:24-26 */
+int fcm_fft_transform(fcm_fft* f, double* in);                             /* fft_solver.cpp:32-36 */
+int fcm_fft_inverse_transform(fcm_fft* f, double* in);                     /* fft_solver.cpp:38-42 */
+
+/* ================================================================ context */
+/* Create a context for one suspension.  blob_ref_pos: 3*nb reference blob
+ * positions of the (single) body shape.  Replaces
+ * collection_of_rigid_bodies::initialise (collection_of_rigid_bodies.cpp:15-153),
+ * fcm_fluid_solver::initialise (fcm_fluid_solver.cpp:29-129),
+ * gmres_solver::initialise (gmres_solver.cpp:14-34) and
+ * linked_list::initialise (linked_list.cpp:23-72). */
+int fcm_create(const fcm_params* p, const double* blob_ref_pos, fcm_ctx** out);
+int fcm_destroy(fcm_ctx* ctx);
+/* Issue all further work of this context on `stream` (a cudaStream_t). */
+int fcm_set_stream(fcm_ctx* ctx, void* stream);
+int fcm_get_params(const fcm_ctx* ctx, fcm_params* p);
+
+/* ================================================================ collection_of_rigid_bodies */
+/* Body state (particle x and quaternion q, particle.hpp:21-22). */
+int fcm_set_bodies(fcm_ctx* ctx, const double* x, const double* q);
+int fcm_get_bodies(fcm_ctx* ctx, double* x, double* q);
+int fcm_get_midstep_bodies(fcm_ctx* ctx, double* x, double* q);
+/* External force and torque per body (6*M), added to -K^T F in the RHS.  The
+ * reference has none (only steric and wall forces); NULL clears it. */
+int fcm_set_external_forces(fcm_ctx* ctx, const double* fe);
+/* collection_of_rigid_bodies.cpp:155-174 (midstep=0) and :176-193 (midstep=1). */
+int fcm_fill_all_blob_pos(fcm_ctx* ctx, int32_t at_midstep);
+/* Overwrite / read all_blob_pos directly (Nb*3). */
+int fcm_set_all_blob_pos(fcm_ctx* ctx, const double* Y);
+int fcm_get_all_blob_pos(fcm_ctx* ctx, double* Y);
+/* collection_of_rigid_bodies.cpp:707-731: out(3Nb) = K*in(6M) at the midstep. */
+int fcm_multiply_by_K_at_midstep(fcm_ctx* ctx, const double* in, double* out);
+/* collection_of_rigid_bodies.cpp:733-757: out(6M) = K^T*in(3Nb) at the midstep. */
+int fcm_multiply_by_KT_at_midstep(fcm_ctx* ctx, const double* in, double* out);
+/* collection_of_rigid_bodies.cpp:623-664: populate the cell list from
+ * all_blob_pos and set blob_forces = steric forces (EM also sets the midstep
+ * bodies to the current bodies, :625-629). */
+int fcm_calculate_forces(fcm_ctx* ctx);
+int fcm_get_blob_forces(fcm_ctx* ctx, double* F);
+int fcm_set_blob_forces(fcm_ctx* ctx, const double* F);
+/* collection_of_rigid_bodies.cpp:566-621: rigid projection of V (3Nb; NULL =
+ * the context's last interpolated velocities) with ref_KTKinv, half step to the
+ * midstep.  *overlap as the reference's return value. */
+int fcm_advance_to_midstep(fcm_ctx* ctx, const double* V, int32_t* overlap);
+/* collection_of_rigid_bodies.cpp:869-953: finite-difference div(U) of the random
+ * velocity field over six body perturbations. */
+int fcm_calculate_divU(fcm_ctx* ctx, double* divU);
+/* collection_of_rigid_bodies.cpp:759-790: bodies += nu*dt*U (6M). */
+int fcm_end_of_step_update(fcm_ctx* ctx, const double* U, double nu, int32_t* overlap);
+/* collection_of_rigid_bodies.cpp:792-796. */
+int fcm_reset_to_start_of_step(fcm_ctx* ctx);
+/* collection_of_rigid_bodies.cpp:195-205 on the current all_blob_pos. */
+int fcm_check_for_overlap(fcm_ctx* ctx, int32_t* overlap);
+
+/* ================================================================ linked_list */
+/* linked_list.cpp:74-102: cell of every blob from all_blob_pos. */
+int fcm_list_populate(fcm_ctx* ctx);
+/* Cell id of every blob (Nb ints), linked_list.cpp:74-78. */
+int fcm_list_get_cells(fcm_ctx* ctx, int32_t* cell_of_blob);
+/* Inter-body pair set visited by linked_list.cpp:192-281 as (i<j) int pairs,
+ * sorted lexicographically.  *npairs receives the total; FCM_ERR_CAPACITY if it
+ * exceeds cap (then nothing is written). */
+int fcm_list_get_pairs(fcm_ctx* ctx, int32_t* pairs, int64_t cap, int64_t* npairs);
+/* linked_list.cpp:192-281: blob_forces(3Nb) += steric forces. */
+int fcm_apply_barrier_forces(fcm_ctx* ctx, double* blob_forces);
+
+/* ================================================================ fcm_fluid_solver */
+/* fcm_fluid_solver.cpp:131-165 on Y (Nb*3; NULL = all_blob_pos). */
+int fcm_set_up_gaussians(fcm_ctx* ctx, const double* Y);
+/* fcm_fluid_solver.cpp:167-361 with the stress drawn from a counter-based
+ * Philox4x32-10 stream keyed by (seed, counter). */
+int fcm_produce_random_velocity_field(fcm_ctx* ctx, uint64_t seed, uint64_t counter);
+/* fcm_fluid_solver.cpp:167-361 with the six stress arrays supplied by the caller
+ * (the reference's sxx..syz after the fill at :174-234, each nx*ny*pad doubles). */
+int fcm_inject_random_stress(fcm_ctx* ctx, const double* sxx, const double* syy,
+                             const double* szz, const double* sxy,
+                             const double* sxz, const double* syz);
+/* fcm_fluid_solver.cpp:426-487: V(3Nb) = J u_rand (NULL keeps it in the context). */
+int fcm_calculate_random_blob_velocities(fcm_ctx* ctx, double* V);
+/* fcm_fluid_solver.cpp:552-634: spread F (3Nb) onto the force grids. */
+int fcm_set_up_force_distribution(fcm_ctx* ctx, const double* F);
+/* fcm_fluid_solver.cpp:636-701: Stokes solve of the force grids. */
+int fcm_produce_deterministic_velocity_field(fcm_ctx* ctx);
+/* fcm_fluid_solver.cpp:363-424: V(3Nb) = J u (NULL keeps it in the context). */
+int fcm_calculate_deterministic_blob_velocities(fcm_ctx* ctx, double* V);
+/* The context's last interpolated velocities (fcm.V) to V (3Nb). */
+int fcm_get_V(fcm_ctx* ctx, double* V);
+/* Velocity grids u{x,y,z} (deterministic: which=0, random: which=1) in the
+ * reference's padded [x][y][pad] layout, 3 arrays of nx*ny*pad doubles. */
+int fcm_get_velocity_field(fcm_ctx* ctx, int32_t which, double* ux, double* uy, double* uz);
+/* M*F in one call: spread, Stokes solve, interpolation (V = 3Nb). */
+int fcm_apply_mobility(fcm_ctx* ctx, const double* F, double* V);
+/* fcm_fluid_solver.cpp:842-881: single-body mobility at the box centre,
+ * ref_Minv = inv_sympd(M_body) ((3nb)^2), ref_N = inv(K^T ref_Minv K) (6x6). */
+int fcm_produce_reference_matrices(fcm_ctx* ctx);
+/* Column-major ref_Minv ((3nb)^2), ref_N (36), ref_KTKinv (36); any may be NULL. */
+int fcm_get_reference_matrices(fcm_ctx* ctx, double* ref_Minv, double* ref_N, double* ref_KTKinv);
+int fcm_set_reference_matrices(fcm_ctx* ctx, const double* ref_Minv, const double* ref_N);
+
+/* ================================================================ gmres_solver */
+/* gmres_solver.cpp:58-70: RHS = [-V ; -K^T blob_forces - external]. */
+int fcm_assemble_RHS(fcm_ctx* ctx);
+int fcm_get_RHS(fcm_ctx* ctx, double* rhs);
+int fcm_set_RHS(fcm_ctx* ctx, const double* rhs);
+/* gmres_solver.cpp:85-146 (system vectors, 3Nb+6M). */
+int fcm_multiply_by_Pinv(fcm_ctx* ctx, const double* in, double* out);
+/* gmres_solver.cpp:72-83. */
+int fcm_multiply_by_saddle_point_matrix(fcm_ctx* ctx, const double* in, double* out);
+/* gmres_solver.cpp:148-306: right-preconditioned GMRES(max_iter) on the stored
+ * RHS; soln (3Nb+6M, may be NULL) receives P^{-1} sum y_i q_i.  Returns FCM_OK,
+ * FCM_ERR_NOT_CONVERGED (solution still written) or an error. */
+int fcm_invert_saddle_point_system(fcm_ctx* ctx, double* soln, int32_t* iters,
+                                   double* rel_residual);
+
+/* ================================================================ time step */
+/* One accepted-or-rejected time step of main.cpp:222-451 for the configured
+ * algorithm (EM or GDC), noise from Philox (seed, counter=step index) when
+ * params.noise is 1.  Returns FCM_OK or FCM_ERR_OVERLAP (state restored). */
+int fcm_step(fcm_ctx* ctx, uint64_t seed, uint64_t step_index, fcm_step_info* info);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FCM_B200_H */

@@ -1,0 +1,106 @@
+"""ctypes binding of the C-ABI in include/fcm_b200.h (libfcm_b200.so).
+
+The library is loaded from the package directory; if it is missing the import
+fails loudly (build it with ``python -m timstochrigidbodiessim_b200.build``).
+There is no CPU fallback.
+"""
+import ctypes
+import os
+
+from .params import FcmParams, FcmStepInfo
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libfcm_b200.so")
+
+D = ctypes.POINTER(ctypes.c_double)
+I32 = ctypes.POINTER(ctypes.c_int32)
+I64 = ctypes.POINTER(ctypes.c_int64)
+VP = ctypes.c_void_p
+
+# name -> (restype, argtypes); every function of include/fcm_b200.h
+SIGNATURES = {
+    "fcm_default_params": (None, [ctypes.POINTER(FcmParams)]),
+    "fcm_last_error": (ctypes.c_char_p, []),
+    "fcm_version": (ctypes.c_char_p, []),
+    "fcm_fft_create": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(VP)]),
+    "fcm_fft_destroy": (ctypes.c_int, [VP]),
+    "fcm_fft_local_sizes": (ctypes.c_int, [VP, I32, I32, I32, I32, I64, I32]),
+    "fcm_fft_transform": (ctypes.c_int, [VP, VP]),
+    "fcm_fft_inverse_transform": (ctypes.c_int, [VP, VP]),
+    "fcm_create": (ctypes.c_int, [ctypes.POINTER(FcmParams), VP, ctypes.POINTER(VP)]),
+    "fcm_destroy": (ctypes.c_int, [VP]),
+    "fcm_set_stream": (ctypes.c_int, [VP, VP]),
+    "fcm_get_params": (ctypes.c_int, [VP, ctypes.POINTER(FcmParams)]),
+    "fcm_set_bodies": (ctypes.c_int, [VP, VP, VP]),
+    "fcm_get_bodies": (ctypes.c_int, [VP, VP, VP]),
+    "fcm_get_midstep_bodies": (ctypes.c_int, [VP, VP, VP]),
+    "fcm_set_external_forces": (ctypes.c_int, [VP, VP]),
+    "fcm_fill_all_blob_pos": (ctypes.c_int, [VP, ctypes.c_int32]),
+    "fcm_set_all_blob_pos": (ctypes.c_int, [VP, VP]),
+    "fcm_get_all_blob_pos": (ctypes.c_int, [VP, VP]),
+    "fcm_multiply_by_K_at_midstep": (ctypes.c_int, [VP, VP, VP]),
+    "fcm_multiply_by_KT_at_midstep": (ctypes.c_int, [VP, VP, VP]),
+    "fcm_calculate_forces": (ctypes.c_int, [VP]),
+    "fcm_get_blob_forces": (ctypes.c_int, [VP, VP]),
+    "fcm_set_blob_forces": (ctypes.c_int, [VP, VP]),
+    "fcm_advance_to_midstep": (ctypes.c_int, [VP, VP, I32]),
+    "fcm_calculate_divU": (ctypes.c_int, [VP, D]),
+    "fcm_end_of_step_update": (ctypes.c_int, [VP, VP, ctypes.c_double, I32]),
+    "fcm_reset_to_start_of_step": (ctypes.c_int, [VP]),
+    "fcm_check_for_overlap": (ctypes.c_int, [VP, I32]),
+    "fcm_list_populate": (ctypes.c_int, [VP]),
+    "fcm_list_get_cells": (ctypes.c_int, [VP, VP]),
+    "fcm_list_get_pairs": (ctypes.c_int, [VP, VP, ctypes.c_int64, I64]),
+    "fcm_apply_barrier_forces": (ctypes.c_int, [VP, VP]),
+    "fcm_set_up_gaussians": (ctypes.c_int, [VP, VP]),
+    "fcm_produce_random_velocity_field": (ctypes.c_int, [VP, ctypes.c_uint64, ctypes.c_uint64]),
+    "fcm_inject_random_stress": (ctypes.c_int, [VP, VP, VP, VP, VP, VP, VP]),
+    "fcm_calculate_random_blob_velocities": (ctypes.c_int, [VP, VP]),
+    "fcm_set_up_force_distribution": (ctypes.c_int, [VP, VP]),
+    "fcm_produce_deterministic_velocity_field": (ctypes.c_int, [VP]),
+    "fcm_calculate_deterministic_blob_velocities": (ctypes.c_int, [VP, VP]),
+    "fcm_get_V": (ctypes.c_int, [VP, VP]),
+    "fcm_get_velocity_field": (ctypes.c_int, [VP, ctypes.c_int32, VP, VP, VP]),
+    "fcm_apply_mobility": (ctypes.c_int, [VP, VP, VP]),
+    "fcm_produce_reference_matrices": (ctypes.c_int, [VP]),
+    "fcm_get_reference_matrices": (ctypes.c_int, [VP, VP, VP, VP]),
+    "fcm_set_reference_matrices": (ctypes.c_int, [VP, VP, VP]),
+    "fcm_assemble_RHS": (ctypes.c_int, [VP]),
+    "fcm_get_RHS": (ctypes.c_int, [VP, VP]),
+    "fcm_set_RHS": (ctypes.c_int, [VP, VP]),
+    "fcm_multiply_by_Pinv": (ctypes.c_int, [VP, VP, VP]),
+    "fcm_multiply_by_saddle_point_matrix": (ctypes.c_int, [VP, VP, VP]),
+    "fcm_invert_saddle_point_system": (ctypes.c_int, [VP, VP, I32, D]),
+    "fcm_step": (ctypes.c_int, [VP, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(FcmStepInfo)]),
+}
+
+_lib = None
+
+
+class FcmError(RuntimeError):
+    def __init__(self, status, where, message):
+        from .params import STATUS_NAMES
+        self.status = status
+        super().__init__("%s failed: %s (%s)" % (where, STATUS_NAMES.get(status, status), message))
+
+
+def load(path=LIB_PATH):
+    """Load libfcm_b200.so; raises if it is missing (no fallback exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError("libfcm_b200.so not built (%s); run python -m timstochrigidbodiessim_b200.build" % path)
+    L = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def check(status, where, ok=(0,)):
+    if status not in ok:
+        msg = load().fcm_last_error()
+        raise FcmError(status, where, msg.decode() if msg else "")
+    return status

@@ -1,0 +1,1384 @@
+// fcm_api.cu -- host orchestration and the extern "C" entry points of
+// include/fcm_b200.h.  Every entry point catches C++ exceptions, records the
+// error text (fcm_last_error) and returns a status code.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "fcm_internal.cuh"
+
+namespace fcm {
+
+static thread_local std::string g_err;
+void set_error(const std::string& m) { g_err = m; }
+
+namespace {
+bool dense_inv(const std::vector<double>& A, int n, std::vector<double>& out);
+}
+
+// Cyclic Jacobi eigen-decomposition of a symmetric n x n matrix (column-major).
+static void jacobi_eigen(std::vector<double> A, int n, std::vector<double>& evals, std::vector<double>& V) {
+  V.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) V[(size_t)i * n + i] = 1.0;
+  auto a = [&](int i, int j) -> double& { return A[(size_t)j * n + i]; };
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0;
+    for (int i = 0; i < n; ++i)
+      for (int j = i + 1; j < n; ++j) off += a(i, j) * a(i, j);
+    if (off < 1e-300) break;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        if (a(p, q) == 0.0) continue;
+        const double theta = (a(q, q) - a(p, p)) / (2.0 * a(p, q));
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double cs = 1.0 / std::sqrt(t * t + 1.0), sn = t * cs;
+        for (int k = 0; k < n; ++k) {
+          const double akp = a(k, p), akq = a(k, q);
+          a(k, p) = cs * akp - sn * akq;
+          a(k, q) = sn * akp + cs * akq;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double apk = a(p, k), aqk = a(q, k);
+          a(p, k) = cs * apk - sn * aqk;
+          a(q, k) = sn * apk + cs * aqk;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double vkp = V[(size_t)p * n + k], vkq = V[(size_t)q * n + k];
+          V[(size_t)p * n + k] = cs * vkp - sn * vkq;
+          V[(size_t)q * n + k] = sn * vkp + cs * vkq;
+        }
+      }
+  }
+  evals.resize(n);
+  for (int i = 0; i < n; ++i) evals[i] = a(i, i);
+}
+
+// inv() of the reference (Gauss-Jordan) when A is well conditioned; for a
+// singular symmetric A -- K^T K and K^T M^{-1} K of a body whose blobs are
+// collinear, where spin about the axis moves no blob -- the Moore-Penrose
+// pseudo-inverse (eigenvalues below 1e-10 of the largest are dropped).  The
+// reference's bodies (twisted rods, tetrahedra, hedgehogs) never reach the
+// second branch.
+bool sym_inv_or_pinv(const std::vector<double>& A, int n, std::vector<double>& out, bool* used_pinv) {
+  std::vector<double> ev, V;
+  jacobi_eigen(A, n, ev, V);
+  double mx = 0.0;
+  for (double e : ev) mx = std::max(mx, std::fabs(e));
+  bool singular = !(mx > 0.0);
+  for (double e : ev)
+    if (std::fabs(e) <= 1e-10 * mx) singular = true;
+  if (used_pinv) *used_pinv = singular;
+  if (!singular) return dense_inv(A, n, out);
+  out.assign((size_t)n * n, 0.0);
+  for (int k = 0; k < n; ++k) {
+    if (!(std::fabs(ev[k]) > 1e-10 * mx)) continue;
+    const double inv = 1.0 / ev[k];
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) out[(size_t)j * n + i] += V[(size_t)k * n + i] * inv * V[(size_t)k * n + j];
+  }
+  return true;
+}
+
+namespace {
+
+const double PI = 3.14159265358979323846264338327950288;
+
+// ------------------------------------------------------------------ helpers
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+int copy_in(Ctx* c, void* dst, const void* src, size_t bytes) {
+  if (bytes == 0) return FCM_OK;
+  if (!src) {
+    set_error("null input pointer");
+    return FCM_ERR_INVALID;
+  }
+  FCM_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, c->stream));
+  return FCM_OK;
+}
+
+int copy_out(Ctx* c, void* dst, const void* src, size_t bytes) {
+  if (!dst || bytes == 0) return FCM_OK;
+  FCM_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, c->stream));
+  if (!is_device_ptr(dst)) FCM_CUDA(cudaStreamSynchronize(c->stream));
+  return FCM_OK;
+}
+
+template <typename T>
+int dev_alloc(T** p, size_t n) {
+  if (cudaMalloc((void**)p, sizeof(T) * (n > 0 ? n : 1)) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("cudaMalloc of " + std::to_string(sizeof(T) * n) + " bytes failed");
+    return FCM_ERR_NOMEM;
+  }
+  return FCM_OK;
+}
+
+// Dense helpers (column-major) for the reference matrices: inv() by
+// Gauss-Jordan with partial pivoting, inv_sympd() by Cholesky.
+bool dense_inv(const std::vector<double>& A, int n, std::vector<double>& out) {
+  std::vector<double> a = A;
+  out.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) out[(size_t)i * n + i] = 1.0;
+  auto at = [n](std::vector<double>& M, int i, int j) -> double& { return M[(size_t)j * n + i]; };
+  for (int col = 0; col < n; ++col) {
+    int piv = col;
+    for (int r = col + 1; r < n; ++r)
+      if (std::fabs(at(a, r, col)) > std::fabs(at(a, piv, col))) piv = r;
+    if (at(a, piv, col) == 0.0) return false;
+    if (piv != col)
+      for (int j = 0; j < n; ++j) {
+        std::swap(at(a, col, j), at(a, piv, j));
+        std::swap(at(out, col, j), at(out, piv, j));
+      }
+    const double d = at(a, col, col);
+    for (int j = 0; j < n; ++j) {
+      at(a, col, j) /= d;
+      at(out, col, j) /= d;
+    }
+    for (int r = 0; r < n; ++r) {
+      if (r == col) continue;
+      const double f = at(a, r, col);
+      if (f == 0.0) continue;
+      for (int j = 0; j < n; ++j) {
+        at(a, r, j) -= f * at(a, col, j);
+        at(out, r, j) -= f * at(out, col, j);
+      }
+    }
+  }
+  return true;
+}
+
+bool dense_inv_sympd(const std::vector<double>& A, int n, std::vector<double>& out) {
+  std::vector<double> L((size_t)n * n, 0.0), Li((size_t)n * n, 0.0);
+  auto a = [&](int i, int j) { return A[(size_t)j * n + i]; };
+  auto l = [&](int i, int j) -> double& { return L[(size_t)j * n + i]; };
+  auto li = [&](int i, int j) -> double& { return Li[(size_t)j * n + i]; };
+  for (int j = 0; j < n; ++j) {
+    double d = a(j, j);
+    for (int k = 0; k < j; ++k) d -= l(j, k) * l(j, k);
+    if (!(d > 0.0)) return false;
+    const double ljj = std::sqrt(d);
+    l(j, j) = ljj;
+    for (int i = j + 1; i < n; ++i) {
+      double s = a(i, j);
+      for (int k = 0; k < j; ++k) s -= l(i, k) * l(j, k);
+      l(i, j) = s / ljj;
+    }
+  }
+  for (int j = 0; j < n; ++j) {
+    li(j, j) = 1.0 / l(j, j);
+    for (int i = j + 1; i < n; ++i) {
+      double s = 0.0;
+      for (int k = j; k < i; ++k) s -= l(i, k) * li(k, j);
+      li(i, j) = s / l(i, i);
+    }
+  }
+  out.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j <= i; ++j) {
+      double s = 0.0;
+      for (int k = i; k < n; ++k) s += li(k, i) * li(k, j);
+      out[(size_t)j * n + i] = s;
+      out[(size_t)i * n + j] = s;
+    }
+  return true;
+}
+
+// K of the reference shape, (3nb) x 6 column-major: rows 3m..3m+2 = [I, rcross(r_m)]
+// (rcross.cpp:5-9: rcross(x) = {{0,x2,-x1},{-x2,0,x0},{x1,-x0,0}}).
+std::vector<double> reference_K(const std::vector<double>& ref, int nb) {
+  const int n3 = 3 * nb;
+  std::vector<double> K((size_t)n3 * 6, 0.0);
+  for (int m = 0; m < nb; ++m) {
+    const double* x = &ref[3 * m];
+    const double C[3][3] = {{0, x[2], -x[1]}, {-x[2], 0, x[0]}, {x[1], -x[0], 0}};
+    for (int d = 0; d < 3; ++d) K[(size_t)d * n3 + 3 * m + d] = 1.0;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) K[(size_t)(3 + j) * n3 + 3 * m + i] = C[i][j];
+  }
+  return K;
+}
+
+// ------------------------------------------------------------------ cuFFT exec
+inline cufftResult exec_r2c(cufftHandle p, double* in, cufftDoubleComplex* out) { return cufftExecD2Z(p, in, out); }
+inline cufftResult exec_r2c(cufftHandle p, float* in, cufftComplex* out) { return cufftExecR2C(p, in, out); }
+inline cufftResult exec_c2r(cufftHandle p, cufftDoubleComplex* in, double* out) { return cufftExecZ2D(p, in, out); }
+inline cufftResult exec_c2r(cufftHandle p, cufftComplex* in, float* out) { return cufftExecC2R(p, in, out); }
+template <typename T>
+cufftType r2c_type();
+template <>
+cufftType r2c_type<double>() { return CUFFT_D2Z; }
+template <>
+cufftType r2c_type<float>() { return CUFFT_R2C; }
+template <typename T>
+cufftType c2r_type();
+template <>
+cufftType c2r_type<double>() { return CUFFT_Z2D; }
+template <>
+cufftType c2r_type<float>() { return CUFFT_C2R; }
+
+template <typename T>
+GridBufs<T>& grid_of(Ctx* c);
+template <>
+GridBufs<double>& grid_of<double>(Ctx* c) { return c->g64; }
+template <>
+GridBufs<float>& grid_of<float>(Ctx* c) { return c->g32; }
+
+template <typename T>
+int ensure_grid(Ctx* c) {
+  GridBufs<T>& gb = grid_of<T>(c);
+  if (gb.ready) return FCM_OK;
+  FCM_TRY(dev_alloc(&gb.r, 3 * (size_t)c->g.G));
+  FCM_TRY(dev_alloc(&gb.c, 3 * (size_t)c->g.Gc));
+  FCM_TRY(dev_alloc(&gb.urand, 3 * (size_t)c->g.G));
+  FCM_CUDA(cudaMemsetAsync(gb.urand, 0, sizeof(T) * 3 * (size_t)c->g.G, c->stream));
+  int n[3] = {c->g.nx, c->g.ny, c->g.nz};
+  FCM_CUFFT(cufftPlanMany(&gb.r2c, 3, n, nullptr, 1, (int)c->g.G, nullptr, 1, (int)c->g.Gc, r2c_type<T>(), 3));
+  FCM_CUFFT(cufftPlanMany(&gb.c2r, 3, n, nullptr, 1, (int)c->g.Gc, nullptr, 1, (int)c->g.G, c2r_type<T>(), 3));
+  FCM_CUFFT(cufftSetStream(gb.r2c, c->stream));
+  FCM_CUFFT(cufftSetStream(gb.c2r, c->stream));
+  FCM_TRY(blob_table_alloc(gb.blobs, c->Nb, c->p.ngauss, c->g));
+  FCM_TRY(blob_table_alloc(gb.ref_blobs, c->nb, c->p.ngauss, c->g));
+  gb.ready = true;
+  return FCM_OK;
+}
+
+template <typename T>
+void free_grid(GridBufs<T>& gb) {
+  cudaFree(gb.r);
+  cudaFree(gb.c);
+  cudaFree(gb.urand);
+  if (gb.r2c) cufftDestroy(gb.r2c);
+  if (gb.c2r) cufftDestroy(gb.c2r);
+  blob_table_free(gb.blobs);
+  blob_table_free(gb.ref_blobs);
+  gb = GridBufs<T>();
+}
+
+int set_stream_all(Ctx* c) {
+  if (c->g64.ready) {
+    FCM_CUFFT(cufftSetStream(c->g64.r2c, c->stream));
+    FCM_CUFFT(cufftSetStream(c->g64.c2r, c->stream));
+  }
+  if (c->g32.ready) {
+    FCM_CUFFT(cufftSetStream(c->g32.r2c, c->stream));
+    FCM_CUFFT(cufftSetStream(c->g32.c2r, c->stream));
+  }
+  if (c->plan_r2c6) FCM_CUFFT(cufftSetStream(c->plan_r2c6, c->stream));
+  return FCM_OK;
+}
+
+// ------------------------------------------------------------------ FCM pieces
+// Gaussian tables of all blobs from Y (device), FP64 always, FP32 for precision 1.
+int set_up_gaussians_dev(Ctx* c, const double* dY) {
+  FCM_TRY(launch_set_up_gaussians<double>(*c, c->g64.blobs, dY, c->stream));
+  if (c->p.precision == 1) FCM_TRY(launch_set_up_gaussians<float>(*c, c->g32.blobs, dY, c->stream));
+  c->gauss_ready = true;
+  return FCM_OK;
+}
+
+template <typename T>
+int spread_t(Ctx* c, const BlobTable<T>& t, const double* dF) {
+  return launch_spread<T>(*c, t, dF, grid_of<T>(c).r, c->stream);
+}
+
+template <typename T>
+int stokes_t(Ctx* c) {
+  GridBufs<T>& gb = grid_of<T>(c);
+  FCM_CUFFT(exec_r2c(gb.r2c, gb.r, gb.c));
+  FCM_TRY(launch_project<T>(*c, gb.c, c->stream));
+  FCM_CUFFT(exec_c2r(gb.c2r, gb.c, gb.r));
+  return FCM_OK;
+}
+
+template <typename T>
+int interp_t(Ctx* c, const BlobTable<T>& t, const T* grid, double* dV) {
+  return launch_interp<T>(*c, t, grid, dV, c->stream);
+}
+
+// V (3Nb, device) = M F with the grid precision `prec`.
+int mobility_dev(Ctx* c, int prec, const double* dF, double* dV) {
+  if (prec == 0) {
+    FCM_TRY(spread_t<double>(c, c->g64.blobs, dF));
+    FCM_TRY(stokes_t<double>(c));
+    FCM_TRY(interp_t<double>(c, c->g64.blobs, c->g64.r, dV));
+  } else {
+    FCM_TRY(spread_t<float>(c, c->g32.blobs, dF));
+    FCM_TRY(stokes_t<float>(c));
+    FCM_TRY(interp_t<float>(c, c->g32.blobs, c->g32.r, dV));
+  }
+  return FCM_OK;
+}
+
+int random_velocities_dev(Ctx* c, double* dV) {
+  if (!c->urand_ready) {
+    FCM_CUDA(cudaMemsetAsync(dV, 0, sizeof(double) * 3 * (size_t)c->Nb, c->stream));
+    return FCM_OK;
+  }
+  if (c->urand_prec == 0) return interp_t<double>(c, c->g64.blobs, c->g64.urand, dV);
+  return interp_t<float>(c, c->g32.blobs, c->g32.urand, dV);
+}
+
+int noise_dev(Ctx* c, uint64_t seed, uint64_t counter) {
+  if (c->p.precision == 1) {
+    FCM_TRY(launch_noise_kspace<float>(*c, c->g32.c, seed, counter, c->stream));
+    FCM_CUFFT(exec_c2r(c->g32.c2r, c->g32.c, c->g32.urand));
+    c->urand_prec = 1;
+  } else {
+    FCM_TRY(launch_noise_kspace<double>(*c, c->g64.c, seed, counter, c->stream));
+    FCM_CUFFT(exec_c2r(c->g64.c2r, c->g64.c, c->g64.urand));
+    c->urand_prec = 0;
+  }
+  c->urand_ready = true;
+  return FCM_OK;
+}
+
+// gmres_solver.cpp:72-83 on device vectors (system size).
+int saddle_matvec(Ctx* c, int prec, const double* in, double* out) {
+  FCM_TRY(mobility_dev(c, prec, in, out));
+  FCM_TRY(launch_multiply_K(*c, c->d_qm, in + 3 * (size_t)c->Nb, out, 1.0, c->stream));
+  FCM_TRY(launch_multiply_KT(*c, c->d_qm, in, out + 3 * (size_t)c->Nb, -1.0, nullptr, 0.0, c->stream));
+  return FCM_OK;
+}
+
+// gmres_solver.cpp:148-306 (right preconditioning, MGS, Givens, no restarts)
+// on the device vector d_b; the solution is written to d_x.
+int gmres_dev(Ctx* c, int prec, const double* d_b, double* d_x, double tol, int maxit_req, int* iters_out,
+              double* rel_out) {
+  const long long n = c->nsys;
+  const int max_iter = std::min<long long>(n, std::min(maxit_req, c->maxit_alloc)) > 0
+                           ? (int)std::min<long long>(n, std::min(maxit_req, c->maxit_alloc))
+                           : 1;
+  double* Q = c->d_Qm;
+  auto Qc = [&](int i) { return Q + (size_t)i * n; };
+  double* hbuf = c->h_pinned;
+  FCM_TRY(blas_norm_sq_partial(*c, d_b, n, c->d_H, c->stream));
+  FCM_CUDA(cudaMemcpyAsync(hbuf, c->d_H, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  FCM_CUDA(cudaStreamSynchronize(c->stream));
+  const double norm_of_RHS = hbuf[0];
+  if (!(norm_of_RHS > 0.0)) {
+    FCM_CUDA(cudaMemsetAsync(d_x, 0, sizeof(double) * n, c->stream));
+    if (iters_out) *iters_out = 0;
+    if (rel_out) *rel_out = 0.0;
+    if (norm_of_RHS == 0.0) return FCM_OK;
+    set_error("non-finite right-hand side");
+    return FCM_ERR_NONFINITE;
+  }
+  FCM_TRY(blas_copy_scaled(Qc(0), d_b, c->d_H, 1, n, c->stream));
+  const int hn = max_iter + 1;
+  std::vector<double> H((size_t)hn * hn, 0.0), beta(hn, 0.0), CS(max_iter, 0.0), SN(max_iter, 0.0);
+  auto Hm = [&](int i, int j) -> double& { return H[(size_t)j * hn + i]; };
+  beta[0] = norm_of_RHS;
+  double* z = c->d_sys_a;
+  for (int iter = 1; iter <= max_iter; ++iter) {
+    FCM_TRY(launch_pinv(*c, c->d_qm, Qc(iter - 1), z, c->stream));
+    FCM_TRY(saddle_matvec(c, prec, z, Qc(iter)));
+    for (int i = 0; i < iter; ++i)
+      FCM_TRY(blas_mgs_step(*c, Qc(iter), i > 0 ? Qc(i - 1) : nullptr, i > 0 ? c->d_H + (i - 1) : nullptr, Qc(i),
+                            n, c->d_H + i, c->stream));
+    FCM_TRY(blas_mgs_step(*c, Qc(iter), Qc(iter - 1), c->d_H + (iter - 1), nullptr, n, c->d_H + iter, c->stream));
+    FCM_TRY(blas_scale(Qc(iter), c->d_H + iter, 1, n, c->stream));
+    FCM_CUDA(cudaMemcpyAsync(hbuf, c->d_H, sizeof(double) * (iter + 1), cudaMemcpyDeviceToHost, c->stream));
+    FCM_CUDA(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i <= iter; ++i) Hm(i, iter - 1) = hbuf[i];
+    for (int i = 1; i < iter; i++) {
+      const double temp = CS[i - 1] * Hm(i - 1, iter - 1) + SN[i - 1] * Hm(i, iter - 1);
+      Hm(i, iter - 1) = CS[i - 1] * Hm(i, iter - 1) - SN[i - 1] * Hm(i - 1, iter - 1);
+      Hm(i - 1, iter - 1) = temp;
+    }
+    if (Hm(iter, iter - 1) == 0.0) {
+      CS[iter - 1] = 1.0;
+      SN[iter - 1] = 0.0;
+    } else if (std::fabs(Hm(iter, iter - 1)) > std::fabs(Hm(iter - 1, iter - 1))) {
+      const double temp = Hm(iter - 1, iter - 1) / Hm(iter, iter - 1);
+      SN[iter - 1] = (2.0 * double(Hm(iter, iter - 1) > 0) - 1.0) / std::sqrt(1.0 + temp * temp);
+      CS[iter - 1] = temp * SN[iter - 1];
+    } else {
+      const double temp = Hm(iter, iter - 1) / Hm(iter - 1, iter - 1);
+      CS[iter - 1] = (2.0 * double(Hm(iter - 1, iter - 1) > 0) - 1.0) / std::sqrt(1.0 + temp * temp);
+      SN[iter - 1] = temp * CS[iter - 1];
+    }
+    Hm(iter - 1, iter - 1) = CS[iter - 1] * Hm(iter - 1, iter - 1) + SN[iter - 1] * Hm(iter, iter - 1);
+    Hm(iter, iter - 1) = 0.0;
+    beta[iter] = -SN[iter - 1] * beta[iter - 1];
+    beta[iter - 1] = CS[iter - 1] * beta[iter - 1];
+    const double relative_error = std::fabs(beta[iter]) / norm_of_RHS;
+    if (!std::isfinite(relative_error)) {
+      set_error("GMRES residual became non-finite");
+      if (iters_out) *iters_out = iter;
+      if (rel_out) *rel_out = relative_error;
+      return FCM_ERR_NONFINITE;
+    }
+    if (relative_error < tol || iter == max_iter) {
+      std::vector<double> y(iter, 0.0);
+      y[iter - 1] = beta[iter - 1] / Hm(iter - 1, iter - 1);
+      for (int i = iter - 2; i >= 0; i--) {
+        y[i] = beta[i];
+        for (int j = iter - 1; j > i; j--) y[i] -= Hm(i, j) * y[j];
+        y[i] /= Hm(i, i);
+      }
+      for (int i = 0; i < iter; ++i) hbuf[i] = y[i];
+      FCM_CUDA(cudaMemcpyAsync(c->d_y, hbuf, sizeof(double) * iter, cudaMemcpyHostToDevice, c->stream));
+      FCM_TRY(blas_combine(c->d_sys_b, Q, c->d_y, iter, n, c->stream));
+      FCM_TRY(launch_pinv(*c, c->d_qm, c->d_sys_b, d_x, c->stream));
+      FCM_CUDA(cudaStreamSynchronize(c->stream));  // hbuf is reused by the caller
+      if (iters_out) *iters_out = iter;
+      if (rel_out) *rel_out = relative_error;
+      return relative_error < tol ? FCM_OK : FCM_ERR_NOT_CONVERGED;
+    }
+  }
+  return FCM_ERR_STATE;
+}
+
+// Saddle-point solve of d_rhs into d_soln.  precision 0: one GMRES; precision 1:
+// FP64 iterative refinement around FP32-grid GMRES sweeps.
+int solve_dev(Ctx* c, const double* d_rhs, double* d_soln, int* iters, double* rel, int* sweeps) {
+  const long long n = c->nsys;
+  if (c->p.precision == 0) {
+    if (sweeps) *sweeps = 1;
+    return gmres_dev(c, 0, d_rhs, d_soln, c->p.gmres_tol, c->p.gmres_max_iter, iters, rel);
+  }
+  // r = b; x = 0; repeat: dx = GMRES32(r); x += dx; r = b - A64 x.
+  double* x = d_soln;
+  double* res = c->d_res;
+  double* dx = c->d_dx;
+  FCM_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, c->stream));
+  FCM_CUDA(cudaMemcpyAsync(res, d_rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+  FCM_TRY(blas_norm_sq_partial(*c, d_rhs, n, c->d_H, c->stream));
+  FCM_CUDA(cudaMemcpyAsync(c->h_pinned, c->d_H, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  FCM_CUDA(cudaStreamSynchronize(c->stream));
+  const double nb = c->h_pinned[0];
+  int total = 0, sw = 0, st = FCM_OK;
+  double relr = 0.0;
+  const double inner_tol = std::max(c->p.gmres_tol, 1e-5);
+  for (sw = 1; sw <= 8; ++sw) {
+    int it = 0;
+    double rr = 0;
+    int s = gmres_dev(c, 1, res, dx, inner_tol, c->p.gmres_max_iter, &it, &rr);
+    total += it;
+    if (s != FCM_OK && s != FCM_ERR_NOT_CONVERGED) return s;
+    FCM_TRY(blas_axpby(x, dx, 1.0, 1.0, n, c->stream));
+    FCM_TRY(saddle_matvec(c, 0, x, res));
+    FCM_TRY(blas_axpby(res, d_rhs, 1.0, -1.0, n, c->stream));
+    FCM_TRY(blas_norm_sq_partial(*c, res, n, c->d_H, c->stream));
+    FCM_CUDA(cudaMemcpyAsync(c->h_pinned, c->d_H, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    FCM_CUDA(cudaStreamSynchronize(c->stream));
+    relr = nb > 0 ? c->h_pinned[0] / nb : 0.0;
+    if (!std::isfinite(relr)) {
+      st = FCM_ERR_NONFINITE;
+      break;
+    }
+    if (relr < c->p.gmres_tol) {
+      st = FCM_OK;
+      break;
+    }
+    st = FCM_ERR_NOT_CONVERGED;
+  }
+  if (iters) *iters = total;
+  if (rel) *rel = relr;
+  if (sweeps) *sweeps = std::min(sw, 8);
+  return st;
+}
+
+int calculate_forces_dev(Ctx* c) {
+  if (c->p.algorithm == 2) {  // collection_of_rigid_bodies.cpp:625-629
+    FCM_CUDA(cudaMemcpyAsync(c->d_xm, c->d_x, sizeof(double) * 3 * c->M, cudaMemcpyDeviceToDevice, c->stream));
+    FCM_CUDA(cudaMemcpyAsync(c->d_qm, c->d_q, sizeof(double) * 4 * c->M, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  FCM_TRY(cells_build(*c, c->stream));
+  FCM_TRY(cells_steric_forces(*c, c->d_F, false, c->stream));
+  return FCM_OK;
+}
+
+int assemble_rhs_dev(Ctx* c) {
+  const size_t n3 = 3 * (size_t)c->Nb;
+  FCM_CUDA(cudaMemcpyAsync(c->d_rhs, c->d_V, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->stream));
+  FCM_TRY(blas_axpby(c->d_rhs, c->d_rhs, 0.0, -1.0, (long long)n3, c->stream));
+  FCM_TRY(launch_multiply_KT(*c, c->d_qm, c->d_F, c->d_rhs + n3, -1.0, c->d_fe, -1.0, c->stream));
+  return FCM_OK;
+}
+
+int overlap_dev(Ctx* c, int* ov) {
+  FCM_TRY(cells_overlap(*c, c->d_flag, c->stream));
+  int h = 0;
+  FCM_CUDA(cudaMemcpyAsync(&h, c->d_flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  FCM_CUDA(cudaStreamSynchronize(c->stream));
+  *ov = h;
+  return FCM_OK;
+}
+
+int end_of_step_update_dev(Ctx* c, const double* dU, double nu, int* overlap) {
+  FCM_CUDA(cudaMemcpyAsync(c->d_xs, c->d_x, sizeof(double) * 3 * c->M, cudaMemcpyDeviceToDevice, c->stream));
+  FCM_CUDA(cudaMemcpyAsync(c->d_qs, c->d_q, sizeof(double) * 4 * c->M, cudaMemcpyDeviceToDevice, c->stream));
+  const double scale = nu * c->p.dt;
+  FCM_TRY(launch_body_update(*c, c->d_x, c->d_q, dU, scale, c->stream));
+  FCM_TRY(launch_fill_blob_pos(*c, c->d_x, c->d_q, c->d_Y, c->stream));
+  FCM_TRY(cells_build(*c, c->stream));
+  int ov = 0;
+  if (c->p.skip_on_overlap) FCM_TRY(overlap_dev(c, &ov));
+  if (overlap) *overlap = ov;
+  return FCM_OK;
+}
+
+int advance_to_midstep_dev(Ctx* c, const double* dV, int* overlap) {
+  FCM_CUDA(cudaMemcpyAsync(c->d_xm, c->d_x, sizeof(double) * 3 * c->M, cudaMemcpyDeviceToDevice, c->stream));
+  FCM_CUDA(cudaMemcpyAsync(c->d_qm, c->d_q, sizeof(double) * 4 * c->M, cudaMemcpyDeviceToDevice, c->stream));
+  FCM_TRY(launch_rigid_projection(*c, c->d_q, dV, c->d_U0, c->stream));
+  FCM_TRY(launch_body_update(*c, c->d_xm, c->d_qm, c->d_U0, 0.5 * c->p.dt, c->stream));
+  FCM_TRY(launch_fill_blob_pos(*c, c->d_xm, c->d_qm, c->d_Y, c->stream));
+  FCM_TRY(cells_build(*c, c->stream));
+  int ov = 0;
+  if (c->p.skip_on_overlap) FCM_TRY(overlap_dev(c, &ov));
+  if (overlap) *overlap = ov;
+  return FCM_OK;
+}
+
+int divU_dev(Ctx* c, double* out) {
+  FCM_CUDA(cudaMemcpyAsync(c->d_xs, c->d_x, sizeof(double) * 3 * c->M, cudaMemcpyDeviceToDevice, c->stream));
+  FCM_CUDA(cudaMemcpyAsync(c->d_qs, c->d_q, sizeof(double) * 4 * c->M, cudaMemcpyDeviceToDevice, c->stream));
+  double* acc = c->d_H + c->maxit_alloc + 1;
+  FCM_CUDA(cudaMemsetAsync(acc, 0, sizeof(double), c->stream));
+  for (int i = 0; i < 6; ++i) {
+    double e[6] = {0, 0, 0, 0, 0, 0};
+    e[i] = (i < 3) ? c->p.fd_delta * c->p.blob_radius : c->p.fd_delta;
+    FCM_TRY(launch_body_update_uniform(*c, c->d_x, c->d_q, e, c->stream));
+    FCM_TRY(launch_fill_blob_pos(*c, c->d_x, c->d_q, c->d_Y, c->stream));
+    FCM_TRY(set_up_gaussians_dev(c, c->d_Y));
+    FCM_TRY(random_velocities_dev(c, c->d_V));
+    FCM_TRY(launch_rigid_projection(*c, c->d_q, c->d_V, c->d_tmp6, c->stream));
+    FCM_TRY(launch_divU_accumulate(*c, c->d_tmp6, c->d_U0, i, e[i], c->d_tmp3, c->stream));
+    FCM_TRY(blas_sum_accumulate(*c, c->d_tmp3, c->M, acc, c->stream));
+    FCM_CUDA(cudaMemcpyAsync(c->d_x, c->d_xs, sizeof(double) * 3 * c->M, cudaMemcpyDeviceToDevice, c->stream));
+    FCM_CUDA(cudaMemcpyAsync(c->d_q, c->d_qs, sizeof(double) * 4 * c->M, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  FCM_CUDA(cudaMemcpyAsync(c->h_pinned, acc, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  FCM_CUDA(cudaStreamSynchronize(c->stream));
+  *out = c->h_pinned[0];
+  return FCM_OK;
+}
+
+int reference_matrices_dev(Ctx* c) {
+  const int nb = c->nb, n3 = 3 * nb;
+  // Body 0 alone at the box centre with q = 1 (collection_of_rigid_bodies.cpp:132-151).
+  std::vector<double> ref(3 * nb), Y(3 * nb);
+  FCM_CUDA(cudaMemcpyAsync(ref.data(), c->d_ref, sizeof(double) * 3 * nb, cudaMemcpyDeviceToHost, c->stream));
+  FCM_CUDA(cudaStreamSynchronize(c->stream));
+  const double centre[3] = {0.5 * c->g.Lx, 0.5 * c->g.Ly, 0.5 * c->g.Lz};
+  const double L[3] = {c->g.Lx, c->g.Ly, c->g.Lz};
+  for (int m = 0; m < nb; ++m)
+    for (int d = 0; d < 3; ++d) {
+      const double p = centre[d] + ref[3 * m + d];
+      Y[3 * m + d] = p - L[d] * std::floor(p / L[d]);
+    }
+  double *dY = nullptr, *dF = nullptr, *dV = nullptr;
+  FCM_TRY(dev_alloc(&dY, 3 * (size_t)nb));
+  FCM_TRY(dev_alloc(&dF, 3 * (size_t)nb));
+  FCM_TRY(dev_alloc(&dV, 3 * (size_t)nb));
+  int st = FCM_OK;
+  std::vector<double> Mb((size_t)n3 * n3);
+  do {
+    if ((st = copy_in(c, dY, Y.data(), sizeof(double) * 3 * nb)) != FCM_OK) break;
+    if ((st = launch_set_up_gaussians<double>(*c, c->g64.ref_blobs, dY, c->stream)) != FCM_OK) break;
+    std::vector<double> e(n3, 0.0);
+    for (int n = 0; n < n3 && st == FCM_OK; ++n) {
+      std::fill(e.begin(), e.end(), 0.0);
+      e[n] = 1.0;
+      if ((st = copy_in(c, dF, e.data(), sizeof(double) * n3)) != FCM_OK) break;
+      if ((st = spread_t<double>(c, c->g64.ref_blobs, dF)) != FCM_OK) break;
+      if ((st = stokes_t<double>(c)) != FCM_OK) break;
+      if ((st = interp_t<double>(c, c->g64.ref_blobs, c->g64.r, dV)) != FCM_OK) break;
+      if (cudaMemcpyAsync(&Mb[(size_t)n * n3], dV, sizeof(double) * n3, cudaMemcpyDeviceToHost, c->stream) !=
+          cudaSuccess) {
+        st = FCM_ERR_CUDA;
+        break;
+      }
+      if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+        st = FCM_ERR_CUDA;
+        break;
+      }
+    }
+  } while (0);
+  cudaFree(dY);
+  cudaFree(dF);
+  cudaFree(dV);
+  if (st != FCM_OK) return st;
+  // ref_Minv = inv_sympd(M_body); ref_N = inv(K^T ref_Minv K) (fcm_fluid_solver.cpp:866-877)
+  std::vector<double> Minv, N;
+  if (!dense_inv_sympd(Mb, n3, Minv)) {
+    set_error("single-body mobility is not positive definite");
+    return FCM_ERR_NONFINITE;
+  }
+  const std::vector<double> K = reference_K(ref, nb);
+  std::vector<double> KtMK(36, 0.0), t(n3);
+  for (int j = 0; j < 6; ++j) {
+    for (int i = 0; i < n3; ++i) {
+      double s = 0.0;
+      for (int k = 0; k < n3; ++k) s += Minv[(size_t)k * n3 + i] * K[(size_t)j * n3 + k];
+      t[i] = s;
+    }
+    for (int i = 0; i < 6; ++i) {
+      double s = 0.0;
+      for (int r = 0; r < n3; ++r) s += K[(size_t)i * n3 + r] * t[r];
+      KtMK[(size_t)j * 6 + i] = s;
+    }
+  }
+  if (!sym_inv_or_pinv(KtMK, 6, N, nullptr)) {
+    set_error("K^T Minv K could not be inverted");
+    return FCM_ERR_NONFINITE;
+  }
+  c->h_Minv = Minv;
+  c->h_N = N;
+  FCM_CUDA(cudaMemcpyAsync(c->d_Minv, c->h_Minv.data(), sizeof(double) * n3 * n3, cudaMemcpyHostToDevice, c->stream));
+  FCM_CUDA(cudaMemcpyAsync(c->d_N, c->h_N.data(), sizeof(double) * 36, cudaMemcpyHostToDevice, c->stream));
+  FCM_CUDA(cudaStreamSynchronize(c->stream));
+  c->have_ref = true;
+  c->gauss_ready = false;  // the main tables are untouched, but V was not produced for them
+  return FCM_OK;
+}
+
+// Copy between the reference's padded [x][y][pad] layout and the unpadded grid.
+int padded_to_grid(Ctx* c, double* dst, const double* src_padded) {
+  FCM_CUDA(cudaMemcpy2DAsync(dst, sizeof(double) * c->g.nz, src_padded, sizeof(double) * 2 * c->g.nzh,
+                             sizeof(double) * c->g.nz, (size_t)c->g.nx * c->g.ny, cudaMemcpyDefault, c->stream));
+  return FCM_OK;
+}
+
+template <typename T>
+int grid_to_padded(Ctx* c, double* dst_padded, const T* src) {
+  const size_t G = (size_t)c->g.G;
+  const int pad = 2 * c->g.nzh;
+  std::vector<T> h(G);
+  FCM_CUDA(cudaMemcpyAsync(h.data(), src, sizeof(T) * G, cudaMemcpyDeviceToHost, c->stream));
+  FCM_CUDA(cudaStreamSynchronize(c->stream));
+  std::vector<double> out((size_t)c->g.nx * c->g.ny * pad, 0.0);
+  for (size_t l = 0; l < (size_t)c->g.nx * c->g.ny; ++l)
+    for (int k = 0; k < c->g.nz; ++k) out[l * pad + k] = (double)h[l * c->g.nz + k];
+  FCM_CUDA(cudaMemcpyAsync(dst_padded, out.data(), sizeof(double) * out.size(), cudaMemcpyDefault, c->stream));
+  FCM_CUDA(cudaStreamSynchronize(c->stream));
+  return FCM_OK;
+}
+
+int check_params(const fcm_params* p) {
+  if (!p) return FCM_ERR_INVALID;
+  auto bad = [](const char* m) {
+    set_error(m);
+    return FCM_ERR_INVALID;
+  };
+  if (p->nx < 2 || p->ny < 2 || p->nz < 2) return bad("grid dimensions must be >= 2");
+  if (p->ngauss < 1 || p->ngauss > p->nx || p->ngauss > p->ny || p->ngauss > p->nz)
+    return bad("ngauss must be in [1, min(nx,ny,nz)]");
+  if (!(p->dx > 0) || !(p->blob_radius > 0) || !(p->viscosity > 0) || !(p->dt > 0) || !(p->kT >= 0))
+    return bad("dx, blob_radius, viscosity, dt must be > 0 and kT >= 0");
+  if (p->num_bodies < 1 || p->blobs_per_body < 1) return bad("num_bodies and blobs_per_body must be >= 1");
+  if (p->ncells < 3) return bad("ncells must be >= 3 (the 13-cell half shell degenerates below 3)");
+  if (p->potential < 0 || p->potential > 3) return bad("potential must be 0..3");
+  if (p->gmres_max_iter < 1) return bad("gmres_max_iter must be >= 1");
+  if (p->algorithm != 1 && p->algorithm != 2) return bad("algorithm must be 1 (GDC) or 2 (EM)");
+  if (p->precision != 0 && p->precision != 1) return bad("precision must be 0 or 1");
+  const long long G = (long long)p->nx * p->ny * p->nz;
+  if (3 * G > 2000000000LL) return bad("grid too large for 32-bit cuFFT batch strides");
+  return FCM_OK;
+}
+
+void destroy_ctx(Ctx* c) {
+  if (!c) return;
+  double* ptrs[] = {c->d_ref, c->d_x, c->d_q, c->d_xm, c->d_qm, c->d_xs, c->d_qs, c->d_Y, c->d_V, c->d_F,
+                    c->d_fe, c->d_U0, c->d_tmp3, c->d_tmp6, c->d_sys_a, c->d_sys_b, c->d_rhs, c->d_soln, c->d_res, c->d_dx, c->d_Minv, c->d_N,
+                    c->d_KTKinv, c->d_Qm, c->d_H, c->d_y, c->d_partials, c->d_stress};
+  for (double* p : ptrs) cudaFree(p);
+  cudaFree(c->d_counter);
+  cudaFree(c->d_cell);
+  cudaFree(c->d_cell_start);
+  cudaFree(c->d_cell_count);
+  cudaFree(c->d_cell_sorted);
+  cudaFree(c->d_cell_cursor);
+  cudaFree(c->d_flag);
+  cudaFree(c->d_pair_count);
+  cudaFree(c->d_stress_c);
+  if (c->plan_r2c6) cufftDestroy(c->plan_r2c6);
+  if (c->h_pinned) cudaFreeHost(c->h_pinned);
+  free_grid(c->g64);
+  free_grid(c->g32);
+  delete c;
+}
+
+int create_ctx(const fcm_params* p, const double* ref, Ctx** out) {
+  FCM_TRY(check_params(p));
+  if (!ref) {
+    set_error("blob_ref_pos is null");
+    return FCM_ERR_INVALID;
+  }
+  Ctx* c = new Ctx();
+  c->p = *p;
+  cudaGetDevice(&c->device);
+  c->M = p->num_bodies;
+  c->nb = p->blobs_per_body;
+  c->Nb = c->M * c->nb;
+  c->nsys = 3 * c->Nb + 6 * c->M;
+  c->g.nx = p->nx;
+  c->g.ny = p->ny;
+  c->g.nz = p->nz;
+  c->g.nzh = p->nz / 2 + 1;
+  c->g.G = (long long)p->nx * p->ny * p->nz;
+  c->g.Gc = (long long)p->nx * p->ny * c->g.nzh;
+  c->g.dx = p->dx;
+  c->g.Lx = p->dx * p->nx;  // config.hpp:89-91
+  c->g.Ly = p->dx * p->ny;
+  c->g.Lz = p->dx * p->nz;
+  int st = FCM_OK;
+  auto fail = [&](int s) {
+    destroy_ctx(c);
+    return s;
+  };
+  const int M = c->M, Nb = c->Nb, nb = c->nb;
+  const long long n = c->nsys;
+  if ((st = dev_alloc(&c->d_ref, 3 * (size_t)nb)) || (st = dev_alloc(&c->d_x, 3 * (size_t)M)) ||
+      (st = dev_alloc(&c->d_q, 4 * (size_t)M)) || (st = dev_alloc(&c->d_xm, 3 * (size_t)M)) ||
+      (st = dev_alloc(&c->d_qm, 4 * (size_t)M)) || (st = dev_alloc(&c->d_xs, 3 * (size_t)M)) ||
+      (st = dev_alloc(&c->d_qs, 4 * (size_t)M)) || (st = dev_alloc(&c->d_Y, 3 * (size_t)Nb)) ||
+      (st = dev_alloc(&c->d_V, 3 * (size_t)Nb)) || (st = dev_alloc(&c->d_F, 3 * (size_t)Nb)) ||
+      (st = dev_alloc(&c->d_fe, 6 * (size_t)M)) || (st = dev_alloc(&c->d_U0, 6 * (size_t)M)) ||
+      (st = dev_alloc(&c->d_tmp3, std::max<size_t>(3 * (size_t)Nb, (size_t)M))) ||
+      (st = dev_alloc(&c->d_tmp6, 6 * (size_t)M)) || (st = dev_alloc(&c->d_sys_a, n)) ||
+      (st = dev_alloc(&c->d_sys_b, n)) || (st = dev_alloc(&c->d_rhs, n)) ||
+      (st = dev_alloc(&c->d_soln, n)) || (st = dev_alloc(&c->d_res, n)) || (st = dev_alloc(&c->d_dx, n)) ||
+      (st = dev_alloc(&c->d_Minv, 9 * (size_t)nb * nb)) || (st = dev_alloc(&c->d_N, 36)) ||
+      (st = dev_alloc(&c->d_KTKinv, 36)))
+    return fail(st);
+  c->maxit_alloc = (int)std::min<long long>(n, p->gmres_max_iter);
+  if ((st = dev_alloc(&c->d_Qm, n * (size_t)(c->maxit_alloc + 1))) ||
+      (st = dev_alloc(&c->d_H, (size_t)c->maxit_alloc + 4)) || (st = dev_alloc(&c->d_y, (size_t)c->maxit_alloc + 1)))
+    return fail(st);
+  c->red_blocks = (int)std::max<long long>(1, std::min<long long>(296, (n + 1023) / 1024));
+  if ((st = dev_alloc(&c->d_partials, (size_t)c->red_blocks)) ||
+      (st = dev_alloc(&c->d_counter, 1)))
+    return fail(st);
+  if (cudaMallocHost(&c->h_pinned, sizeof(double) * std::max(256, c->maxit_alloc + 8)) != cudaSuccess)
+    return fail(FCM_ERR_NOMEM);
+  c->ncell_total = p->ncells * p->ncells * p->ncells;
+  if ((st = dev_alloc(&c->d_cell, (size_t)Nb)) || (st = dev_alloc(&c->d_cell_start, (size_t)c->ncell_total + 1)) ||
+      (st = dev_alloc(&c->d_cell_count, (size_t)c->ncell_total)) ||
+      (st = dev_alloc(&c->d_cell_sorted, (size_t)Nb)) || (st = dev_alloc(&c->d_cell_cursor, (size_t)c->ncell_total)) ||
+      (st = dev_alloc(&c->d_flag, 1)) || (st = dev_alloc(&c->d_pair_count, 1)))
+    return fail(st);
+  if (cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned int), c->stream) != cudaSuccess ||
+      cudaMemsetAsync(c->d_fe, 0, sizeof(double) * 6 * M, c->stream) != cudaSuccess ||
+      cudaMemsetAsync(c->d_V, 0, sizeof(double) * 3 * Nb, c->stream) != cudaSuccess ||
+      cudaMemsetAsync(c->d_F, 0, sizeof(double) * 3 * Nb, c->stream) != cudaSuccess ||
+      cudaMemsetAsync(c->d_U0, 0, sizeof(double) * 6 * M, c->stream) != cudaSuccess) {
+    set_error("cudaMemsetAsync failed");
+    return fail(FCM_ERR_CUDA);
+  }
+  // shape, identity bodies, reference matrices (identity until produced)
+  std::vector<double> href(ref, ref + 3 * nb);
+  if (cudaMemcpy(c->d_ref, href.data(), sizeof(double) * 3 * nb, cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(FCM_ERR_CUDA);
+  std::vector<double> hx(3 * (size_t)M, 0.0), hq(4 * (size_t)M, 0.0);
+  for (int i = 0; i < M; ++i) hq[4 * i] = 1.0;
+  for (double* d : {c->d_x, c->d_xm, c->d_xs})
+    if (cudaMemcpy(d, hx.data(), sizeof(double) * hx.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(FCM_ERR_CUDA);
+  for (double* d : {c->d_q, c->d_qm, c->d_qs})
+    if (cudaMemcpy(d, hq.data(), sizeof(double) * hq.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(FCM_ERR_CUDA);
+  const int n3 = 3 * nb;
+  c->h_Minv.assign((size_t)n3 * n3, 0.0);
+  for (int i = 0; i < n3; ++i) c->h_Minv[(size_t)i * n3 + i] = 1.0;
+  c->h_N.assign(36, 0.0);
+  for (int i = 0; i < 6; ++i) c->h_N[i * 6 + i] = 1.0;
+  // ref_KTKinv = inv(K^T K) (collection_of_rigid_bodies.cpp:117-130)
+  {
+    const std::vector<double> K = reference_K(href, nb);
+    std::vector<double> KTK(36, 0.0);
+    for (int i = 0; i < 6; ++i)
+      for (int j = 0; j < 6; ++j) {
+        double s = 0.0;
+        for (int t = 0; t < n3; ++t) s += K[(size_t)i * n3 + t] * K[(size_t)j * n3 + t];
+        KTK[(size_t)j * 6 + i] = s;
+      }
+    if (!sym_inv_or_pinv(KTK, 6, c->h_KTKinv, nullptr)) {
+      set_error("K^T K of the body shape could not be inverted");
+      return fail(FCM_ERR_INVALID);
+    }
+  }
+  if (cudaMemcpy(c->d_Minv, c->h_Minv.data(), sizeof(double) * n3 * n3, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->d_N, c->h_N.data(), sizeof(double) * 36, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->d_KTKinv, c->h_KTKinv.data(), sizeof(double) * 36, cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(FCM_ERR_CUDA);
+  if ((st = ensure_grid<double>(c)) != FCM_OK) return fail(st);
+  if (p->precision == 1 && (st = ensure_grid<float>(c)) != FCM_OK) return fail(st);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(FCM_ERR_CUDA);
+  *out = c;
+  return FCM_OK;
+}
+
+template <class F>
+int guard(F&& f) {
+  try {
+    return f();
+  } catch (const std::bad_alloc&) {
+    set_error("host allocation failed");
+    return FCM_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return FCM_ERR_INVALID;
+  } catch (...) {
+    set_error("unknown exception");
+    return FCM_ERR_INVALID;
+  }
+}
+
+#define CTX_CHECK(ctx)                   \
+  if (!(ctx)) {                          \
+    ::fcm::set_error("null context");    \
+    return FCM_ERR_INVALID;              \
+  }
+
+}  // namespace
+}  // namespace fcm
+
+struct fcm_ctx {
+  fcm::Ctx* c;
+};
+
+using namespace fcm;
+
+extern "C" {
+
+void fcm_default_params(fcm_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  const double a = 1.0, eta = 1.0, kT = 1.0;
+  p->nx = p->ny = p->nz = 256;  // config.hpp:65-67
+  p->ngauss = 20;               // :69
+  p->dx = a * 0.3033277330901916;
+  p->blob_radius = a;
+  p->viscosity = eta;
+  p->kT = kT;
+  p->dt = (PI * eta * a * a * a / kT) / 100.0;
+  p->num_bodies = 3;
+  p->blobs_per_body = 22;
+  p->ncells = 6;
+  p->potential = 0;
+  p->steric_fs = 40.0 * kT / a;
+  p->steric_rc = 2.2 * a;
+  p->gmres_max_iter = 40;
+  p->gmres_tol = 1e-3;
+  p->fd_delta = 1e-5;
+  p->algorithm = 2;
+  p->precision = 0;
+  p->noise = 1;
+  p->skip_on_overlap = 0;
+}
+
+const char* fcm_last_error(void) { return g_err.c_str(); }
+const char* fcm_version(void) { return "fcm_b200 0.1 (sm_100a)"; }
+
+int fcm_create(const fcm_params* p, const double* blob_ref_pos, fcm_ctx** out) {
+  return guard([&] {
+    if (!out) return (int)FCM_ERR_INVALID;
+    *out = nullptr;
+    Ctx* c = nullptr;
+    const int st = create_ctx(p, blob_ref_pos, &c);
+    if (st != FCM_OK) return st;
+    *out = new fcm_ctx{c};
+    return (int)FCM_OK;
+  });
+}
+
+int fcm_destroy(fcm_ctx* ctx) {
+  if (!ctx) return FCM_OK;
+  if (ctx->c) cudaStreamSynchronize(ctx->c->stream);
+  destroy_ctx(ctx->c);
+  delete ctx;
+  return FCM_OK;
+}
+
+int fcm_set_stream(fcm_ctx* ctx, void* stream) {
+  CTX_CHECK(ctx);
+  ctx->c->stream = (cudaStream_t)stream;
+  return set_stream_all(ctx->c);
+}
+
+int fcm_get_params(const fcm_ctx* ctx, fcm_params* p) {
+  CTX_CHECK(ctx);
+  if (!p) return FCM_ERR_INVALID;
+  *p = ctx->c->p;
+  return FCM_OK;
+}
+
+// ------------------------------------------------------------------ bodies
+int fcm_set_bodies(fcm_ctx* ctx, const double* x, const double* q) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  FCM_TRY(copy_in(c, c->d_x, x, sizeof(double) * 3 * c->M));
+  FCM_TRY(copy_in(c, c->d_q, q, sizeof(double) * 4 * c->M));
+  FCM_CUDA(cudaMemcpyAsync(c->d_xm, c->d_x, sizeof(double) * 3 * c->M, cudaMemcpyDeviceToDevice, c->stream));
+  FCM_CUDA(cudaMemcpyAsync(c->d_qm, c->d_q, sizeof(double) * 4 * c->M, cudaMemcpyDeviceToDevice, c->stream));
+  return FCM_OK;
+}
+
+int fcm_get_bodies(fcm_ctx* ctx, double* x, double* q) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  FCM_TRY(copy_out(c, x, c->d_x, sizeof(double) * 3 * c->M));
+  FCM_TRY(copy_out(c, q, c->d_q, sizeof(double) * 4 * c->M));
+  return FCM_OK;
+}
+
+int fcm_get_midstep_bodies(fcm_ctx* ctx, double* x, double* q) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  FCM_TRY(copy_out(c, x, c->d_xm, sizeof(double) * 3 * c->M));
+  FCM_TRY(copy_out(c, q, c->d_qm, sizeof(double) * 4 * c->M));
+  return FCM_OK;
+}
+
+int fcm_set_external_forces(fcm_ctx* ctx, const double* fe) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  if (!fe) {
+    FCM_CUDA(cudaMemsetAsync(c->d_fe, 0, sizeof(double) * 6 * c->M, c->stream));
+    return FCM_OK;
+  }
+  return copy_in(c, c->d_fe, fe, sizeof(double) * 6 * c->M);
+}
+
+int fcm_fill_all_blob_pos(fcm_ctx* ctx, int32_t at_midstep) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  return launch_fill_blob_pos(*c, at_midstep ? c->d_xm : c->d_x, at_midstep ? c->d_qm : c->d_q, c->d_Y, c->stream);
+}
+
+int fcm_set_all_blob_pos(fcm_ctx* ctx, const double* Y) {
+  CTX_CHECK(ctx);
+  return copy_in(ctx->c, ctx->c->d_Y, Y, sizeof(double) * 3 * ctx->c->Nb);
+}
+
+int fcm_get_all_blob_pos(fcm_ctx* ctx, double* Y) {
+  CTX_CHECK(ctx);
+  return copy_out(ctx->c, Y, ctx->c->d_Y, sizeof(double) * 3 * ctx->c->Nb);
+}
+
+int fcm_multiply_by_K_at_midstep(fcm_ctx* ctx, const double* in, double* out) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  FCM_TRY(copy_in(c, c->d_tmp6, in, sizeof(double) * 6 * c->M));
+  FCM_TRY(launch_multiply_K(*c, c->d_qm, c->d_tmp6, c->d_tmp3, 0.0, c->stream));
+  return copy_out(c, out, c->d_tmp3, sizeof(double) * 3 * c->Nb);
+}
+
+int fcm_multiply_by_KT_at_midstep(fcm_ctx* ctx, const double* in, double* out) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  FCM_TRY(copy_in(c, c->d_tmp3, in, sizeof(double) * 3 * c->Nb));
+  FCM_TRY(launch_multiply_KT(*c, c->d_qm, c->d_tmp3, c->d_tmp6, 1.0, nullptr, 0.0, c->stream));
+  return copy_out(c, out, c->d_tmp6, sizeof(double) * 6 * c->M);
+}
+
+int fcm_calculate_forces(fcm_ctx* ctx) {
+  CTX_CHECK(ctx);
+  return calculate_forces_dev(ctx->c);
+}
+
+int fcm_get_blob_forces(fcm_ctx* ctx, double* F) {
+  CTX_CHECK(ctx);
+  return copy_out(ctx->c, F, ctx->c->d_F, sizeof(double) * 3 * ctx->c->Nb);
+}
+
+int fcm_set_blob_forces(fcm_ctx* ctx, const double* F) {
+  CTX_CHECK(ctx);
+  return copy_in(ctx->c, ctx->c->d_F, F, sizeof(double) * 3 * ctx->c->Nb);
+}
+
+int fcm_advance_to_midstep(fcm_ctx* ctx, const double* V, int32_t* overlap) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  if (V) FCM_TRY(copy_in(c, c->d_V, V, sizeof(double) * 3 * c->Nb));
+  int ov = 0;
+  FCM_TRY(advance_to_midstep_dev(c, c->d_V, &ov));
+  if (overlap) *overlap = ov;
+  return FCM_OK;
+}
+
+int fcm_calculate_divU(fcm_ctx* ctx, double* divU) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  if (!c->urand_ready) {
+    set_error("calculate_divU needs a random velocity field");
+    return FCM_ERR_STATE;
+  }
+  double d = 0.0;
+  FCM_TRY(divU_dev(c, &d));
+  if (divU) *divU = d;
+  return FCM_OK;
+}
+
+int fcm_end_of_step_update(fcm_ctx* ctx, const double* U, double nu, int32_t* overlap) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  FCM_TRY(copy_in(c, c->d_tmp6, U, sizeof(double) * 6 * c->M));
+  int ov = 0;
+  FCM_TRY(end_of_step_update_dev(c, c->d_tmp6, nu, &ov));
+  if (overlap) *overlap = ov;
+  return FCM_OK;
+}
+
+int fcm_reset_to_start_of_step(fcm_ctx* ctx) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  FCM_CUDA(cudaMemcpyAsync(c->d_x, c->d_xs, sizeof(double) * 3 * c->M, cudaMemcpyDeviceToDevice, c->stream));
+  FCM_CUDA(cudaMemcpyAsync(c->d_q, c->d_qs, sizeof(double) * 4 * c->M, cudaMemcpyDeviceToDevice, c->stream));
+  return FCM_OK;
+}
+
+int fcm_check_for_overlap(fcm_ctx* ctx, int32_t* overlap) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  FCM_TRY(cells_build(*c, c->stream));
+  int ov = 0;
+  FCM_TRY(overlap_dev(c, &ov));
+  if (overlap) *overlap = ov;
+  return FCM_OK;
+}
+
+// ------------------------------------------------------------------ linked_list
+int fcm_list_populate(fcm_ctx* ctx) {
+  CTX_CHECK(ctx);
+  return cells_build(*ctx->c, ctx->c->stream);
+}
+
+int fcm_list_get_cells(fcm_ctx* ctx, int32_t* cell) {
+  CTX_CHECK(ctx);
+  return copy_out(ctx->c, cell, ctx->c->d_cell, sizeof(int) * ctx->c->Nb);
+}
+
+int fcm_list_get_pairs(fcm_ctx* ctx, int32_t* pairs, int64_t cap, int64_t* npairs) {
+  CTX_CHECK(ctx);
+  return guard([&] {
+    Ctx* c = ctx->c;
+    FCM_TRY(cells_count_pairs(*c, c->d_pair_count, nullptr, 0, c->stream));
+    long long n = 0;
+    FCM_CUDA(cudaMemcpyAsync(&n, c->d_pair_count, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+    FCM_CUDA(cudaStreamSynchronize(c->stream));
+    if (npairs) *npairs = n;
+    if (!pairs) return (int)FCM_OK;
+    if (n > cap) {
+      set_error("pair buffer too small");
+      return (int)FCM_ERR_CAPACITY;
+    }
+    int* dp = nullptr;
+    FCM_TRY(dev_alloc(&dp, 2 * (size_t)std::max<long long>(n, 1)));
+    int st = cells_count_pairs(*c, c->d_pair_count, dp, n, c->stream);
+    std::vector<int> h(2 * (size_t)n);
+    if (st == FCM_OK && n > 0 &&
+        cudaMemcpyAsync(h.data(), dp, sizeof(int) * 2 * n, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
+      st = FCM_ERR_CUDA;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) st = FCM_ERR_CUDA;
+    cudaFree(dp);
+    if (st != FCM_OK) return st;
+    std::vector<std::pair<int, int>> v((size_t)n);
+    for (long long i = 0; i < n; ++i) v[i] = std::make_pair(h[2 * i], h[2 * i + 1]);
+    std::sort(v.begin(), v.end());
+    std::vector<int> outv(2 * (size_t)n);
+    for (long long i = 0; i < n; ++i) {
+      outv[2 * i] = v[i].first;
+      outv[2 * i + 1] = v[i].second;
+    }
+    if (n > 0) {
+      FCM_CUDA(cudaMemcpyAsync(pairs, outv.data(), sizeof(int) * 2 * n, cudaMemcpyDefault, c->stream));
+      FCM_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    return (int)FCM_OK;
+  });
+}
+
+int fcm_apply_barrier_forces(fcm_ctx* ctx, double* blob_forces) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  if (!blob_forces) return FCM_ERR_INVALID;
+  FCM_TRY(copy_in(c, c->d_tmp3, blob_forces, sizeof(double) * 3 * c->Nb));
+  FCM_TRY(cells_steric_forces(*c, c->d_tmp3, true, c->stream));
+  return copy_out(c, blob_forces, c->d_tmp3, sizeof(double) * 3 * c->Nb);
+}
+
+// ------------------------------------------------------------------ fcm_fluid_solver
+int fcm_set_up_gaussians(fcm_ctx* ctx, const double* Y) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  if (Y) FCM_TRY(copy_in(c, c->d_Y, Y, sizeof(double) * 3 * c->Nb));
+  return set_up_gaussians_dev(c, c->d_Y);
+}
+
+int fcm_produce_random_velocity_field(fcm_ctx* ctx, uint64_t seed, uint64_t counter) {
+  CTX_CHECK(ctx);
+  return noise_dev(ctx->c, seed, counter);
+}
+
+int fcm_inject_random_stress(fcm_ctx* ctx, const double* sxx, const double* syy, const double* szz,
+                             const double* sxy, const double* sxz, const double* syz) {
+  CTX_CHECK(ctx);
+  return guard([&] {
+    Ctx* c = ctx->c;
+    const double* s[6] = {sxx, syy, szz, sxy, sxz, syz};
+    for (int i = 0; i < 6; ++i)
+      if (!s[i]) {
+        set_error("null stress array");
+        return (int)FCM_ERR_INVALID;
+      }
+    if (!c->d_stress) {
+      FCM_TRY(dev_alloc(&c->d_stress, 6 * (size_t)c->g.G));
+      FCM_TRY(dev_alloc(&c->d_stress_c, 6 * (size_t)c->g.Gc));
+      int n[3] = {c->g.nx, c->g.ny, c->g.nz};
+      FCM_CUFFT(cufftPlanMany(&c->plan_r2c6, 3, n, nullptr, 1, (int)c->g.G, nullptr, 1, (int)c->g.Gc, CUFFT_D2Z, 6));
+      FCM_CUFFT(cufftSetStream(c->plan_r2c6, c->stream));
+    }
+    for (int i = 0; i < 6; ++i) FCM_TRY(padded_to_grid(c, c->d_stress + (size_t)i * c->g.G, s[i]));
+    FCM_CUFFT(cufftExecD2Z(c->plan_r2c6, c->d_stress, c->d_stress_c));
+    FCM_TRY(launch_stress_divergence_project(*c, c->d_stress_c, c->g64.c, c->stream));
+    FCM_CUFFT(cufftExecZ2D(c->g64.c2r, c->g64.c, c->g64.urand));
+    c->urand_prec = 0;
+    c->urand_ready = true;
+    FCM_CUDA(cudaStreamSynchronize(c->stream));  // host stress arrays are borrowed
+    return (int)FCM_OK;
+  });
+}
+
+int fcm_calculate_random_blob_velocities(fcm_ctx* ctx, double* V) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  if (!c->gauss_ready) {
+    set_error("set_up_gaussians must precede interpolation");
+    return FCM_ERR_STATE;
+  }
+  FCM_TRY(random_velocities_dev(c, c->d_V));
+  return copy_out(c, V, c->d_V, sizeof(double) * 3 * c->Nb);
+}
+
+int fcm_set_up_force_distribution(fcm_ctx* ctx, const double* F) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  if (!c->gauss_ready) {
+    set_error("set_up_gaussians must precede spreading");
+    return FCM_ERR_STATE;
+  }
+  FCM_TRY(copy_in(c, c->d_tmp3, F, sizeof(double) * 3 * c->Nb));
+  c->det_ready = false;
+  return spread_t<double>(c, c->g64.blobs, c->d_tmp3);
+}
+
+int fcm_produce_deterministic_velocity_field(fcm_ctx* ctx) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  FCM_TRY(stokes_t<double>(c));
+  c->det_ready = true;
+  return FCM_OK;
+}
+
+int fcm_calculate_deterministic_blob_velocities(fcm_ctx* ctx, double* V) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  if (!c->gauss_ready) {
+    set_error("set_up_gaussians must precede interpolation");
+    return FCM_ERR_STATE;
+  }
+  FCM_TRY(interp_t<double>(c, c->g64.blobs, c->g64.r, c->d_V));
+  return copy_out(c, V, c->d_V, sizeof(double) * 3 * c->Nb);
+}
+
+int fcm_get_V(fcm_ctx* ctx, double* V) {
+  CTX_CHECK(ctx);
+  return copy_out(ctx->c, V, ctx->c->d_V, sizeof(double) * 3 * ctx->c->Nb);
+}
+
+int fcm_get_velocity_field(fcm_ctx* ctx, int32_t which, double* ux, double* uy, double* uz) {
+  CTX_CHECK(ctx);
+  return guard([&] {
+    Ctx* c = ctx->c;
+    double* outs[3] = {ux, uy, uz};
+    const size_t G = (size_t)c->g.G;
+    for (int k = 0; k < 3; ++k) {
+      if (!outs[k]) continue;
+      if (which == 1 && c->urand_prec == 1)
+        FCM_TRY(grid_to_padded<float>(c, outs[k], c->g32.urand + k * G));
+      else
+        FCM_TRY(grid_to_padded<double>(c, outs[k], (which == 1 ? c->g64.urand : c->g64.r) + k * G));
+    }
+    return (int)FCM_OK;
+  });
+}
+
+int fcm_apply_mobility(fcm_ctx* ctx, const double* F, double* V) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  if (!c->gauss_ready) {
+    set_error("set_up_gaussians must precede fcm_apply_mobility");
+    return FCM_ERR_STATE;
+  }
+  FCM_TRY(copy_in(c, c->d_tmp3, F, sizeof(double) * 3 * c->Nb));
+  FCM_TRY(mobility_dev(c, c->p.precision, c->d_tmp3, c->d_V));
+  return copy_out(c, V, c->d_V, sizeof(double) * 3 * c->Nb);
+}
+
+int fcm_produce_reference_matrices(fcm_ctx* ctx) {
+  CTX_CHECK(ctx);
+  return guard([&] { return reference_matrices_dev(ctx->c); });
+}
+
+int fcm_get_reference_matrices(fcm_ctx* ctx, double* Minv, double* N, double* KTKinv) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  const int n3 = 3 * c->nb;
+  if (Minv) std::memcpy(Minv, c->h_Minv.data(), sizeof(double) * n3 * n3);
+  if (N) std::memcpy(N, c->h_N.data(), sizeof(double) * 36);
+  if (KTKinv) std::memcpy(KTKinv, c->h_KTKinv.data(), sizeof(double) * 36);
+  return FCM_OK;
+}
+
+int fcm_set_reference_matrices(fcm_ctx* ctx, const double* Minv, const double* N) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  const int n3 = 3 * c->nb;
+  FCM_CUDA(cudaStreamSynchronize(c->stream));
+  if (Minv) {
+    c->h_Minv.assign(Minv, Minv + (size_t)n3 * n3);
+    FCM_CUDA(cudaMemcpyAsync(c->d_Minv, c->h_Minv.data(), sizeof(double) * n3 * n3, cudaMemcpyHostToDevice, c->stream));
+  }
+  if (N) {
+    c->h_N.assign(N, N + 36);
+    FCM_CUDA(cudaMemcpyAsync(c->d_N, c->h_N.data(), sizeof(double) * 36, cudaMemcpyHostToDevice, c->stream));
+  }
+  FCM_CUDA(cudaStreamSynchronize(c->stream));
+  c->have_ref = true;
+  return FCM_OK;
+}
+
+// ------------------------------------------------------------------ gmres_solver
+int fcm_assemble_RHS(fcm_ctx* ctx) {
+  CTX_CHECK(ctx);
+  return assemble_rhs_dev(ctx->c);
+}
+
+int fcm_get_RHS(fcm_ctx* ctx, double* rhs) {
+  CTX_CHECK(ctx);
+  return copy_out(ctx->c, rhs, ctx->c->d_rhs, sizeof(double) * ctx->c->nsys);
+}
+
+int fcm_set_RHS(fcm_ctx* ctx, const double* rhs) {
+  CTX_CHECK(ctx);
+  return copy_in(ctx->c, ctx->c->d_rhs, rhs, sizeof(double) * ctx->c->nsys);
+}
+
+int fcm_multiply_by_Pinv(fcm_ctx* ctx, const double* in, double* out) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  FCM_TRY(copy_in(c, c->d_sys_b, in, sizeof(double) * c->nsys));
+  FCM_TRY(launch_pinv(*c, c->d_qm, c->d_sys_b, c->d_sys_a, c->stream));
+  return copy_out(c, out, c->d_sys_a, sizeof(double) * c->nsys);
+}
+
+int fcm_multiply_by_saddle_point_matrix(fcm_ctx* ctx, const double* in, double* out) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  if (!c->gauss_ready) {
+    set_error("set_up_gaussians must precede the saddle-point product");
+    return FCM_ERR_STATE;
+  }
+  FCM_TRY(copy_in(c, c->d_sys_b, in, sizeof(double) * c->nsys));
+  FCM_TRY(saddle_matvec(c, 0, c->d_sys_b, c->d_sys_a));
+  return copy_out(c, out, c->d_sys_a, sizeof(double) * c->nsys);
+}
+
+int fcm_invert_saddle_point_system(fcm_ctx* ctx, double* soln, int32_t* iters, double* rel_residual) {
+  CTX_CHECK(ctx);
+  return guard([&] {
+    Ctx* c = ctx->c;
+    if (!c->gauss_ready) {
+      set_error("set_up_gaussians must precede the saddle-point solve");
+      return (int)FCM_ERR_STATE;
+    }
+    int it = 0, sw = 0;
+    double rel = 0.0;
+    double* x = c->d_soln;
+    int st = solve_dev(c, c->d_rhs, x, &it, &rel, &sw);
+    if (st == FCM_OK || st == FCM_ERR_NOT_CONVERGED) {
+      const int s2 = copy_out(c, soln, x, sizeof(double) * c->nsys);
+      if (s2 != FCM_OK) st = s2;
+    }
+    if (iters) *iters = it;
+    if (rel_residual) *rel_residual = rel;
+    return st;
+  });
+}
+
+// ------------------------------------------------------------------ time step
+int fcm_step(fcm_ctx* ctx, uint64_t seed, uint64_t step_index, fcm_step_info* info) {
+  CTX_CHECK(ctx);
+  return guard([&] {
+    Ctx* c = ctx->c;
+    fcm_step_info inf;
+    std::memset(&inf, 0, sizeof(inf));
+    const bool noise = c->p.noise != 0;
+    // main.cpp:230-233
+    FCM_TRY(launch_fill_blob_pos(*c, c->d_x, c->d_q, c->d_Y, c->stream));
+    if (noise) FCM_TRY(noise_dev(c, seed, step_index));
+    else c->urand_ready = false;
+    FCM_TRY(set_up_gaussians_dev(c, c->d_Y));
+    FCM_TRY(random_velocities_dev(c, c->d_V));
+    double nu = 1.0;
+    if (c->p.algorithm == 1) {  // main.cpp:235-268
+      int ov = 0;
+      FCM_TRY(advance_to_midstep_dev(c, c->d_V, &ov));
+      if (ov) {
+        inf.overlap = 1;
+        if (info) *info = inf;
+        return (int)FCM_ERR_OVERLAP;
+      }
+      double divU = 0.0;
+      if (noise) FCM_TRY(divU_dev(c, &divU));
+      inf.divU = divU;
+      nu = 1.0 + 0.5 * c->p.dt * divU;
+      FCM_TRY(launch_fill_blob_pos(*c, c->d_xm, c->d_qm, c->d_Y, c->stream));
+      FCM_TRY(set_up_gaussians_dev(c, c->d_Y));
+      FCM_TRY(random_velocities_dev(c, c->d_V));
+    }
+    FCM_TRY(calculate_forces_dev(c));  // main.cpp:282
+    FCM_TRY(assemble_rhs_dev(c));      // main.cpp:308
+    int it = 0, sw = 0;
+    double rel = 0.0;
+    const int st = solve_dev(c, c->d_rhs, c->d_soln, &it, &rel, &sw);  // main.cpp:310
+    inf.gmres_iters = it;
+    inf.refinement_sweeps = sw;
+    inf.gmres_rel_residual = rel;
+    inf.status = st;
+    if (st != FCM_OK && st != FCM_ERR_NOT_CONVERGED) {
+      if (info) *info = inf;
+      return st;
+    }
+    int ov = 0;
+    FCM_TRY(end_of_step_update_dev(c, c->d_soln + 3 * (size_t)c->Nb, nu, &ov));  // main.cpp:312
+    if (ov) {  // main.cpp:316-328
+      FCM_CUDA(cudaMemcpyAsync(c->d_x, c->d_xs, sizeof(double) * 3 * c->M, cudaMemcpyDeviceToDevice, c->stream));
+      FCM_CUDA(cudaMemcpyAsync(c->d_q, c->d_qs, sizeof(double) * 4 * c->M, cudaMemcpyDeviceToDevice, c->stream));
+      inf.overlap = 1;
+      if (info) *info = inf;
+      return (int)FCM_ERR_OVERLAP;
+    }
+    if (info) *info = inf;
+    return (int)FCM_OK;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,216 @@
+// fcm_internal.cuh -- shared declarations of the B200 FCM library (not part of
+// the public C-ABI; see include/fcm_b200.h).
+//
+// Device data layout (one suspension, one GPU):
+//   real grid    T[3][nx][ny][nz]        (component-major, z fastest, unpadded)
+//   spectrum     complex T[3][nx][ny][nzh], nzh = nz/2+1 (cuFFT R2C layout)
+//   blob tables  base int[Nb][3] (first stencil point per dim, unwrapped),
+//                weights T[Nb][3][W]
+//   system vecs  double[3Nb + 6M]       ([lambda ; U], as the reference)
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/fcm_b200.h"
+
+namespace fcm {
+
+// ------------------------------------------------------------------ errors
+void set_error(const std::string& msg);
+struct Status {
+  int code;
+};
+
+#define FCM_CUDA(call)                                                          \
+  do {                                                                          \
+    cudaError_t e_ = (call);                                                    \
+    if (e_ != cudaSuccess) {                                                    \
+      ::fcm::set_error(std::string(#call) + ": " + cudaGetErrorString(e_));     \
+      return (int)FCM_ERR_CUDA;                                                    \
+    }                                                                           \
+  } while (0)
+
+#define FCM_CUFFT(call)                                                         \
+  do {                                                                          \
+    cufftResult r_ = (call);                                                    \
+    if (r_ != CUFFT_SUCCESS) {                                                  \
+      ::fcm::set_error(std::string(#call) + ": cufft error " + std::to_string((int)r_)); \
+      return (int)FCM_ERR_CUFFT;                                                \
+    }                                                                           \
+  } while (0)
+
+#define FCM_TRY(expr)                 \
+  do {                                \
+    int s_ = (expr);                  \
+    if (s_ != FCM_OK) return s_;      \
+  } while (0)
+
+#define FCM_LAUNCH_CHECK()                                                      \
+  do {                                                                          \
+    cudaError_t e_ = cudaGetLastError();                                        \
+    if (e_ != cudaSuccess) {                                                    \
+      ::fcm::set_error(std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+      return (int)FCM_ERR_CUDA;                                                    \
+    }                                                                           \
+  } while (0)
+
+template <typename T>
+struct cplx_t;
+template <>
+struct cplx_t<double> {
+  typedef cufftDoubleComplex type;
+};
+template <>
+struct cplx_t<float> {
+  typedef cufftComplex type;
+};
+
+// ------------------------------------------------------------------ geometry
+struct GridDims {
+  int nx, ny, nz, nzh;
+  long long G;   // nx*ny*nz
+  long long Gc;  // nx*ny*nzh
+  double dx, Lx, Ly, Lz;
+};
+
+// Precomputed separable Gaussian stencil of a set of blobs
+// (fcm_fluid_solver.cpp:131-165 gaussx/y/z and indx/y/z).
+template <typename T>
+struct BlobTable {
+  int n = 0;         // blobs
+  int W = 0;         // stencil width
+  int* base = nullptr;   // [n][3] unwrapped first grid index per dim
+  T* w = nullptr;        // [n][3][W]
+  // tile binning for the tiled spread / interpolation
+  int ntiles = 0;
+  int* tile_count = nullptr;   // [ntiles+1] counts then exclusive offsets
+  int* tile_blobs = nullptr;   // [cap] blob ids grouped by tile
+  long long tile_cap = 0;
+  int* tile_cursor = nullptr;  // [ntiles]
+  int* tile_total = nullptr;   // [1] device total of (blob,tile) overlaps
+};
+
+// Grid buffers and cuFFT plans of one precision.
+template <typename T>
+struct GridBufs {
+  bool ready = false;
+  T* r = nullptr;                              // 3*G real
+  typename cplx_t<T>::type* c = nullptr;       // 3*Gc spectrum
+  T* urand = nullptr;                          // 3*G random velocity field
+  cufftHandle r2c = 0, c2r = 0;
+  BlobTable<T> blobs;                          // all blobs of the suspension
+  BlobTable<T> ref_blobs;                      // single body (reference matrices)
+};
+
+// Tile shape of the tiled spread / interpolation kernels.
+constexpr int TILE_X = 8, TILE_Y = 8, TILE_Z = 8;
+
+// ------------------------------------------------------------------ context
+struct Ctx {
+  fcm_params p;
+  int M = 0, nb = 0, Nb = 0, nsys = 0;
+  GridDims g;
+  cudaStream_t stream = 0;
+  int device = 0;
+
+  // shape
+  double* d_ref = nullptr;   // 3*nb
+  // bodies (x 3M, q 4M) current / midstep / saved start of step
+  double *d_x = nullptr, *d_q = nullptr, *d_xm = nullptr, *d_qm = nullptr, *d_xs = nullptr, *d_qs = nullptr;
+  double *d_Y = nullptr;     // all_blob_pos Nb*3
+  double *d_V = nullptr;     // fcm.V 3Nb
+  double *d_F = nullptr;     // blob_forces 3Nb
+  double *d_fe = nullptr;    // external body forces 6M
+  double *d_U0 = nullptr;    // rigid projection of the random velocities 6M
+  double *d_tmp3 = nullptr;  // 3Nb scratch
+  double *d_tmp6 = nullptr;  // 6M scratch
+  double *d_sys_a = nullptr, *d_sys_b = nullptr;   // system-size scratch
+  double *d_rhs = nullptr;   // RHS
+  double *d_soln = nullptr;  // saddle-point solution
+  double *d_res = nullptr, *d_dx = nullptr;  // refinement residual / correction
+  // preconditioner
+  double *d_Minv = nullptr, *d_N = nullptr, *d_KTKinv = nullptr;
+  std::vector<double> h_Minv, h_N, h_KTKinv;
+  bool have_ref = false;
+  // GMRES
+  double *d_Qm = nullptr;    // nsys * (maxit+1)
+  double *d_H = nullptr;     // (maxit+1) column scratch
+  double *d_y = nullptr;     // maxit coefficients
+  double *d_partials = nullptr;
+  unsigned int* d_counter = nullptr;
+  int red_blocks = 0;
+  int maxit_alloc = 0;
+  double* h_pinned = nullptr;  // small pinned host staging (>= 256 doubles)
+  // cells
+  int ncell_total = 0;
+  int *d_cell = nullptr, *d_cell_start = nullptr, *d_cell_count = nullptr, *d_cell_sorted = nullptr, *d_cell_cursor = nullptr;
+  int *d_flag = nullptr;     // overlap flag
+  long long *d_pair_count = nullptr;
+  // grids
+  GridBufs<double> g64;
+  GridBufs<float> g32;
+  // injected stress (FP64): 6*G real + 6*Gc complex
+  double* d_stress = nullptr;
+  cufftDoubleComplex* d_stress_c = nullptr;
+  cufftHandle plan_r2c6 = 0;
+  // state flags
+  bool gauss_ready = false;
+  bool urand_ready = false;
+  bool det_ready = false;   // deterministic velocity grid holds u
+  int urand_prec = 0;       // precision of the random field last produced
+};
+
+// ------------------------------------------------------------------ launchers
+// gaussians + binning (fcm_grid.cu)
+template <typename T>
+int blob_table_alloc(BlobTable<T>& t, int n, int W, const GridDims& g);
+template <typename T>
+void blob_table_free(BlobTable<T>& t);
+template <typename T>
+int launch_set_up_gaussians(const Ctx& c, BlobTable<T>& t, const double* dY, cudaStream_t s);
+template <typename T>
+int launch_spread(const Ctx& c, const BlobTable<T>& t, const double* dF, T* grid, cudaStream_t s);
+template <typename T>
+int launch_interp(const Ctx& c, const BlobTable<T>& t, const T* grid, double* dV, cudaStream_t s);
+// k-space (fcm_kspace.cu)
+template <typename T>
+int launch_project(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s);
+template <typename T>
+int launch_noise_kspace(const Ctx& c, typename cplx_t<T>::type* spec, uint64_t seed, uint64_t counter, cudaStream_t s);
+int launch_stress_divergence_project(const Ctx& c, const cufftDoubleComplex* sigma6, cufftDoubleComplex* spec, cudaStream_t s);
+int launch_unpad_copy(const double* src_padded, double* dst, int nx, int ny, int nz, int pad, int ncomp_stride_dst, cudaStream_t s);
+// bodies (fcm_bodies.cu)
+int launch_fill_blob_pos(const Ctx& c, const double* x, const double* q, double* Y, cudaStream_t s);
+int launch_multiply_K(const Ctx& c, const double* qm, const double* in6, double* out3, double scale_acc, cudaStream_t s);
+int launch_multiply_KT(const Ctx& c, const double* qm, const double* in3, double* out6, double scale, const double* add6, double add_scale, cudaStream_t s);
+int launch_pinv(const Ctx& c, const double* qm, const double* in, double* out, cudaStream_t s);
+int launch_rigid_projection(const Ctx& c, const double* q, const double* V, double* U6, cudaStream_t s);
+int launch_body_update(const Ctx& c, double* x, double* q, const double* U6, double scale, cudaStream_t s);
+int launch_body_update_uniform(const Ctx& c, double* x, double* q, const double* e6, cudaStream_t s);
+int launch_divU_accumulate(const Ctx& c, const double* U6, const double* U0, int component, double delta, double* acc, cudaStream_t s);
+// cells (fcm_cells.cu)
+int cells_build(Ctx& c, cudaStream_t s);
+int cells_steric_forces(const Ctx& c, double* F, bool accumulate, cudaStream_t s);
+int cells_overlap(const Ctx& c, int* d_flag, cudaStream_t s);
+int cells_count_pairs(const Ctx& c, long long* d_count, int* pairs, long long cap, cudaStream_t s);
+// vector ops (fcm_blas.cu)
+int blas_dot(const Ctx& c, const double* a, const double* b, long long n, double* d_out, cudaStream_t s);
+int blas_mgs_step(const Ctx& c, double* w, const double* q_prev, const double* h_prev, const double* q_i, long long n, double* d_hout, cudaStream_t s);
+int blas_scale(double* v, const double* d_num, int invert, long long n, cudaStream_t s);
+int blas_axpby(double* y, const double* x, double a, double b, long long n, cudaStream_t s);
+int blas_combine(double* out, const double* Q, const double* d_y, int k, long long n, cudaStream_t s);
+int blas_copy_scaled(double* dst, const double* src, const double* d_num, int invert, long long n, cudaStream_t s);
+int blas_norm_sq_partial(const Ctx& c, const double* a, long long n, double* d_out, cudaStream_t s);
+int blas_f64_to_f32(float* dst, const double* src, long long n, cudaStream_t s);
+int blas_sum_accumulate(const Ctx& c, const double* a, long long n, double* d_out, cudaStream_t s);
+
+// symmetric inverse: inv() when well conditioned, otherwise the pseudo-inverse
+// (fcm_linalg.cpp)
+bool sym_inv_or_pinv(const std::vector<double>& A, int n, std::vector<double>& out, bool* used_pinv);
+
+}  // namespace fcm

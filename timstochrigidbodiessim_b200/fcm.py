@@ -1,0 +1,332 @@
+"""Python mirror of the reference's C++ interface over the C-ABI.
+
+``Suspension`` owns one ``fcm_ctx`` (one suspension on one GPU).  Its methods
+carry the names of the reference's methods (fcm_fluid_solver,
+collection_of_rigid_bodies, linked_list, gmres_solver); the thin classes at the
+end expose the same methods under the reference's class names.  Inputs may be
+numpy arrays (host) or CUDA torch tensors (device); outputs are numpy arrays
+unless an ``out=`` tensor is given.
+"""
+import ctypes
+
+import numpy as np
+
+from . import capi
+from .params import FcmParams, FcmStepInfo
+
+
+def _in(a, n, dtype=np.float64):
+    """(keep-alive object, pointer) for an input array of n elements."""
+    if a is None:
+        return None, None
+    if hasattr(a, "data_ptr"):  # torch tensor
+        assert a.is_contiguous() and a.numel() == n, (a.shape, n)
+        return a, ctypes.c_void_p(a.data_ptr())
+    arr = np.ascontiguousarray(a, dtype=dtype)
+    assert arr.size == n, (arr.size, n)
+    return arr, ctypes.c_void_p(arr.ctypes.data)
+
+
+def _out(out, n, dtype=np.float64):
+    if out is not None:
+        if hasattr(out, "data_ptr"):
+            assert out.is_contiguous() and out.numel() == n
+            return out, ctypes.c_void_p(out.data_ptr())
+        assert out.size == n and out.dtype == dtype and out.flags.c_contiguous
+        return out, ctypes.c_void_p(out.ctypes.data)
+    arr = np.zeros(n, dtype=dtype)
+    return arr, ctypes.c_void_p(arr.ctypes.data)
+
+
+class Suspension:
+    """One suspension of rigid multi-blob bodies on the GPU."""
+
+    def __init__(self, params: FcmParams, blob_ref_pos, stream=None):
+        self.L = capi.load()
+        self.p = params.copy()
+        self.M = params.num_bodies
+        self.nb = params.blobs_per_body
+        self.Nb = params.num_blobs
+        self.n = params.system_size
+        self.P = params.nx * params.ny * params.pad
+        keep, ref = _in(blob_ref_pos, 3 * self.nb)
+        h = ctypes.c_void_p()
+        capi.check(self.L.fcm_create(ctypes.byref(self.p), ref, ctypes.byref(h)), "fcm_create")
+        self.h = h
+        if stream is not None:
+            self.set_stream(stream)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.fcm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _c(self, st, where, ok=(0,)):
+        return capi.check(st, where, ok)
+
+    def set_stream(self, stream):
+        """stream: a torch.cuda.Stream or a raw cudaStream_t integer."""
+        s = getattr(stream, "cuda_stream", stream)
+        self._c(self.L.fcm_set_stream(self.h, ctypes.c_void_p(int(s))), "fcm_set_stream")
+
+    # -------------------------------------------------- collection_of_rigid_bodies
+    def set_bodies(self, x, q):
+        kx, px = _in(x, 3 * self.M)
+        kq, pq = _in(q, 4 * self.M)
+        self._c(self.L.fcm_set_bodies(self.h, px, pq), "fcm_set_bodies")
+
+    def get_bodies(self):
+        x, px = _out(None, 3 * self.M)
+        q, pq = _out(None, 4 * self.M)
+        self._c(self.L.fcm_get_bodies(self.h, px, pq), "fcm_get_bodies")
+        return x, q
+
+    def get_midstep_bodies(self):
+        x, px = _out(None, 3 * self.M)
+        q, pq = _out(None, 4 * self.M)
+        self._c(self.L.fcm_get_midstep_bodies(self.h, px, pq), "fcm_get_midstep_bodies")
+        return x, q
+
+    def set_external_forces(self, fe):
+        k, p = _in(fe, 6 * self.M)
+        self._c(self.L.fcm_set_external_forces(self.h, p), "fcm_set_external_forces")
+
+    def fill_all_blob_pos(self, at_midstep=False):
+        self._c(self.L.fcm_fill_all_blob_pos(self.h, int(at_midstep)), "fcm_fill_all_blob_pos")
+
+    def set_all_blob_pos(self, Y):
+        k, p = _in(Y, 3 * self.Nb)
+        self._c(self.L.fcm_set_all_blob_pos(self.h, p), "fcm_set_all_blob_pos")
+
+    def get_all_blob_pos(self, out=None):
+        Y, p = _out(out, 3 * self.Nb)
+        self._c(self.L.fcm_get_all_blob_pos(self.h, p), "fcm_get_all_blob_pos")
+        return Y
+
+    def multiply_by_K_at_midstep(self, U, out=None):
+        k, pi = _in(U, 6 * self.M)
+        o, po = _out(out, 3 * self.Nb)
+        self._c(self.L.fcm_multiply_by_K_at_midstep(self.h, pi, po), "fcm_multiply_by_K_at_midstep")
+        return o
+
+    def multiply_by_KT_at_midstep(self, lam, out=None):
+        k, pi = _in(lam, 3 * self.Nb)
+        o, po = _out(out, 6 * self.M)
+        self._c(self.L.fcm_multiply_by_KT_at_midstep(self.h, pi, po), "fcm_multiply_by_KT_at_midstep")
+        return o
+
+    def calculate_forces(self):
+        self._c(self.L.fcm_calculate_forces(self.h), "fcm_calculate_forces")
+
+    def get_blob_forces(self, out=None):
+        F, p = _out(out, 3 * self.Nb)
+        self._c(self.L.fcm_get_blob_forces(self.h, p), "fcm_get_blob_forces")
+        return F
+
+    def set_blob_forces(self, F):
+        k, p = _in(F, 3 * self.Nb)
+        self._c(self.L.fcm_set_blob_forces(self.h, p), "fcm_set_blob_forces")
+
+    def advance_to_midstep(self, V=None):
+        k, p = _in(V, 3 * self.Nb)
+        ov = ctypes.c_int32(0)
+        self._c(self.L.fcm_advance_to_midstep(self.h, p, ctypes.byref(ov)), "fcm_advance_to_midstep")
+        return bool(ov.value)
+
+    def calculate_divU(self):
+        d = ctypes.c_double(0.0)
+        self._c(self.L.fcm_calculate_divU(self.h, ctypes.byref(d)), "fcm_calculate_divU")
+        return d.value
+
+    def end_of_step_update(self, U, nu=1.0):
+        k, p = _in(U, 6 * self.M)
+        ov = ctypes.c_int32(0)
+        self._c(self.L.fcm_end_of_step_update(self.h, p, float(nu), ctypes.byref(ov)), "fcm_end_of_step_update")
+        return bool(ov.value)
+
+    def reset_to_start_of_step(self):
+        self._c(self.L.fcm_reset_to_start_of_step(self.h), "fcm_reset_to_start_of_step")
+
+    def check_for_overlap(self):
+        ov = ctypes.c_int32(0)
+        self._c(self.L.fcm_check_for_overlap(self.h, ctypes.byref(ov)), "fcm_check_for_overlap")
+        return bool(ov.value)
+
+    # -------------------------------------------------- linked_list
+    def list_populate(self):
+        self._c(self.L.fcm_list_populate(self.h), "fcm_list_populate")
+
+    def list_get_cells(self):
+        c, p = _out(None, self.Nb, np.int32)
+        self._c(self.L.fcm_list_get_cells(self.h, p), "fcm_list_get_cells")
+        return c
+
+    def list_get_pairs(self):
+        n = ctypes.c_int64(0)
+        self._c(self.L.fcm_list_get_pairs(self.h, None, 0, ctypes.byref(n)), "fcm_list_get_pairs")
+        out = np.zeros(2 * max(n.value, 1), dtype=np.int32)
+        n2 = ctypes.c_int64(0)
+        self._c(self.L.fcm_list_get_pairs(self.h, ctypes.c_void_p(out.ctypes.data), n.value, ctypes.byref(n2)),
+                "fcm_list_get_pairs")
+        return out[: 2 * n2.value].reshape(-1, 2)
+
+    def apply_barrier_forces(self, F=None):
+        F = np.zeros(3 * self.Nb) if F is None else np.array(F, dtype=np.float64)
+        self._c(self.L.fcm_apply_barrier_forces(self.h, ctypes.c_void_p(F.ctypes.data)), "fcm_apply_barrier_forces")
+        return F
+
+    # -------------------------------------------------- fcm_fluid_solver
+    def set_up_gaussians(self, Y=None):
+        k, p = _in(Y, 3 * self.Nb)
+        self._c(self.L.fcm_set_up_gaussians(self.h, p), "fcm_set_up_gaussians")
+
+    def produce_random_velocity_field(self, seed, counter):
+        self._c(self.L.fcm_produce_random_velocity_field(self.h, seed, counter), "fcm_produce_random_velocity_field")
+
+    def inject_random_stress(self, s6):
+        ks = [_in(s, self.P) for s in s6]
+        self._c(self.L.fcm_inject_random_stress(self.h, *[p for _, p in ks]), "fcm_inject_random_stress")
+
+    def calculate_random_blob_velocities(self, out=None):
+        V, p = _out(out, 3 * self.Nb)
+        self._c(self.L.fcm_calculate_random_blob_velocities(self.h, p), "fcm_calculate_random_blob_velocities")
+        return V
+
+    def set_up_force_distribution(self, F):
+        k, p = _in(F, 3 * self.Nb)
+        self._c(self.L.fcm_set_up_force_distribution(self.h, p), "fcm_set_up_force_distribution")
+
+    def produce_deterministic_velocity_field(self):
+        self._c(self.L.fcm_produce_deterministic_velocity_field(self.h), "fcm_produce_deterministic_velocity_field")
+
+    def calculate_deterministic_blob_velocities(self, out=None):
+        V, p = _out(out, 3 * self.Nb)
+        self._c(self.L.fcm_calculate_deterministic_blob_velocities(self.h, p),
+                "fcm_calculate_deterministic_blob_velocities")
+        return V
+
+    def get_V(self, out=None):
+        V, p = _out(out, 3 * self.Nb)
+        self._c(self.L.fcm_get_V(self.h, p), "fcm_get_V")
+        return V
+
+    def get_velocity_field(self, which=0):
+        outs = [np.zeros(self.P) for _ in range(3)]
+        self._c(self.L.fcm_get_velocity_field(self.h, which, *[ctypes.c_void_p(o.ctypes.data) for o in outs]),
+                "fcm_get_velocity_field")
+        return outs
+
+    def apply_mobility(self, F, out=None):
+        k, p = _in(F, 3 * self.Nb)
+        V, po = _out(out, 3 * self.Nb)
+        self._c(self.L.fcm_apply_mobility(self.h, p, po), "fcm_apply_mobility")
+        return V
+
+    def produce_reference_matrices(self):
+        self._c(self.L.fcm_produce_reference_matrices(self.h), "fcm_produce_reference_matrices")
+
+    def get_reference_matrices(self):
+        n3 = 3 * self.nb
+        Minv = np.zeros(n3 * n3); N = np.zeros(36); KTKinv = np.zeros(36)
+        self._c(self.L.fcm_get_reference_matrices(self.h, *[ctypes.c_void_p(a.ctypes.data) for a in (Minv, N, KTKinv)]),
+                "fcm_get_reference_matrices")
+        return (Minv.reshape(n3, n3, order="F"), N.reshape(6, 6, order="F"), KTKinv.reshape(6, 6, order="F"))
+
+    def set_reference_matrices(self, Minv, N):
+        a = np.ascontiguousarray(np.asarray(Minv).ravel(order="F"), dtype=np.float64)
+        b = np.ascontiguousarray(np.asarray(N).ravel(order="F"), dtype=np.float64)
+        self._c(self.L.fcm_set_reference_matrices(self.h, ctypes.c_void_p(a.ctypes.data), ctypes.c_void_p(b.ctypes.data)),
+                "fcm_set_reference_matrices")
+
+    # -------------------------------------------------- gmres_solver
+    def assemble_RHS(self):
+        self._c(self.L.fcm_assemble_RHS(self.h), "fcm_assemble_RHS")
+
+    def get_RHS(self, out=None):
+        r, p = _out(out, self.n)
+        self._c(self.L.fcm_get_RHS(self.h, p), "fcm_get_RHS")
+        return r
+
+    def set_RHS(self, r):
+        k, p = _in(r, self.n)
+        self._c(self.L.fcm_set_RHS(self.h, p), "fcm_set_RHS")
+
+    def multiply_by_Pinv(self, v, out=None):
+        k, pi = _in(v, self.n)
+        o, po = _out(out, self.n)
+        self._c(self.L.fcm_multiply_by_Pinv(self.h, pi, po), "fcm_multiply_by_Pinv")
+        return o
+
+    def multiply_by_saddle_point_matrix(self, v, out=None):
+        k, pi = _in(v, self.n)
+        o, po = _out(out, self.n)
+        self._c(self.L.fcm_multiply_by_saddle_point_matrix(self.h, pi, po), "fcm_multiply_by_saddle_point_matrix")
+        return o
+
+    def invert_saddle_point_system(self, out=None):
+        """Returns (status, solution, iterations, relative residual); status is
+        FCM_OK or FCM_ERR_NOT_CONVERGED (the iterate is still returned)."""
+        o, po = _out(out, self.n)
+        it = ctypes.c_int32(0)
+        rel = ctypes.c_double(0.0)
+        st = self.L.fcm_invert_saddle_point_system(self.h, po, ctypes.byref(it), ctypes.byref(rel))
+        self._c(st, "fcm_invert_saddle_point_system", ok=(0, 5))
+        return st, o, it.value, rel.value
+
+    # -------------------------------------------------- time step
+    def step(self, seed, step_index):
+        """One time step (main.cpp:222-451); returns (status, FcmStepInfo);
+        status FCM_ERR_OVERLAP means the step was rejected and bodies restored."""
+        info = FcmStepInfo()
+        st = self.L.fcm_step(self.h, seed, step_index, ctypes.byref(info))
+        self._c(st, "fcm_step", ok=(0, 7))
+        return st, info
+
+
+class fft_solver:
+    """fft_solver.hpp:10-31 on the GPU (in-place transforms of padded arrays)."""
+
+    def __init__(self, nx, ny, nz):
+        self.L = capi.load()
+        self.nx, self.ny, self.nz = nx, ny, nz
+        h = ctypes.c_void_p()
+        capi.check(self.L.fcm_fft_create(nx, ny, nz, ctypes.byref(h)), "fcm_fft_create")
+        self.h = h
+        a = [ctypes.c_int32() for _ in range(4)]
+        tot = ctypes.c_int64()
+        pad = ctypes.c_int32()
+        capi.check(self.L.fcm_fft_local_sizes(self.h, *[ctypes.byref(x) for x in a], ctypes.byref(tot),
+                                              ctypes.byref(pad)), "fcm_fft_local_sizes")
+        (self.local_nx, self.local_x_start, self.local_ny_after_transpose,
+         self.local_y_start_after_transpose) = [x.value for x in a]
+        self.total_local_size = tot.value
+        self.pad = pad.value
+
+    def transform(self, arr):
+        assert arr.dtype == np.float64 and arr.flags.c_contiguous and arr.size == self.total_local_size
+        capi.check(self.L.fcm_fft_transform(self.h, ctypes.c_void_p(arr.ctypes.data)), "fcm_fft_transform")
+
+    def inverse_transform(self, arr):
+        assert arr.dtype == np.float64 and arr.flags.c_contiguous and arr.size == self.total_local_size
+        capi.check(self.L.fcm_fft_inverse_transform(self.h, ctypes.c_void_p(arr.ctypes.data)),
+                   "fcm_fft_inverse_transform")
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.L.fcm_fft_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
