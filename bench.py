@@ -1,0 +1,393 @@
+"""Benchmark: Brownian rigid-rod time steps (body-steps/s) of the FCM mobility
+solve on B200, headline = mixed-precision solver, beside the plain FP64 GPU path.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload rods2048_phi0.10_g256] [--algorithm em|gdc]
+
+One step = one Euler-Maruyama time step (main.cpp:222-451): Philox
+fluctuating field, random blob velocities, steric forces, right-preconditioned
+GMRES of the rigid saddle-point system to the workload's tolerance, body
+update.  N > 1 runs N independent replicas, one per GPU (the solve does not
+shard; no collective on the data path), value = all replicas' body-steps / the
+slowest rank's time.  --impl reference times the CPU FP64 oracle (the
+reference's algorithm restated, all host threads) on the same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "body-steps/s, mixed vs FP64 GPU at <=1e-6 rel vel error; spread/interp HBM GB/s"
+UNIT = "body-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="rods2048_phi0.10_g256")
+    ap.add_argument("--algorithm", default="em", choices=["em", "gdc"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------- ours
+def setup_suspension(p, ref, x, q, fe, stream):
+    from timstochrigidbodiessim_b200.fcm import Suspension
+    s = Suspension(p, ref, stream=stream)
+    s.set_bodies(x, q)
+    s.set_external_forces(fe)
+    s.produce_reference_matrices()
+    return s
+
+
+def timed_steps(s, K, seed, start_index, stream):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    iters = []
+    e0.record(stream)
+    for i in range(K):
+        st, info = s.step(seed, start_index + i)
+        iters.append(info.gmres_iters)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / 1e3, iters
+
+
+def kernel_roofline(s, p, stream, reps=20):
+    """Per-launch durations of the FP64 spread and interpolation, CUDA events on
+    the context's stream; algorithmic bytes 3*G*8 + 6*Nb*8 per launch."""
+    import torch
+    Nb = p.num_blobs
+    F = torch.randn(3 * Nb, dtype=torch.float64, device="cuda")
+    s.fill_all_blob_pos()
+    s.set_up_gaussians()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    for _ in range(3):
+        s.set_up_force_distribution(F)
+        s.calculate_deterministic_blob_velocities(out=torch.empty(3 * Nb, dtype=torch.float64, device="cuda"))
+    torch.cuda.synchronize()
+    ts, ti = [], []
+    for _ in range(reps):
+        ev[0].record(stream)
+        s.set_up_force_distribution(F)
+        ev[1].record(stream)
+        s.L.fcm_calculate_deterministic_blob_velocities(s.h, None)
+        ev[2].record(stream)
+        ev[2].synchronize()
+        ts.append(ev[0].elapsed_time(ev[1]) / 1e3)
+        ti.append(ev[1].elapsed_time(ev[2]) / 1e3)
+    G = p.nx * p.ny * p.nz
+    bytes_ = 3 * G * 8 + 6 * Nb * 8
+    return bytes_, float(np.mean(ts)), float(np.mean(ti))
+
+
+def rel_vel_error(p, ref, x, q, fe, stream):
+    """Body (and blob) velocity error of the mixed-precision solve against the
+    FP64 solve on the same deterministic right-hand side."""
+    sols = []
+    for prec in (0, 1):
+        s = setup_suspension(p.copy(precision=prec, noise=0), ref, x, q, fe, stream)
+        s.fill_all_blob_pos()
+        s.set_up_gaussians()
+        s.calculate_forces()
+        s.assemble_RHS()
+        st, soln, it, rel = s.invert_saddle_point_system()
+        sols.append(soln)
+        s.close()
+    Nb = p.num_blobs
+    U64, U32 = sols[0][3 * Nb:], sols[1][3 * Nb:]
+    L64, L32 = sols[0][:3 * Nb], sols[1][:3 * Nb]
+    return (float(np.linalg.norm(U32 - U64) / np.linalg.norm(U64)),
+            float(np.linalg.norm(L32 - L64) / np.linalg.norm(L64)))
+
+
+def cpu_baseline(p, ref, x, q, fe, gmres_iters):
+    """The CPU oracle (the reference's algorithm restated, FP64) on a bounded
+    sample of the same workload: one fluctuating-field solve plus one saddle-point
+    product (spread, FFT solve, interpolation, K, K^T, P^-1).  A step is
+    estimated as noise + (iters + 2) products, iters = the FP64 GPU path's GMRES
+    iteration count on this workload."""
+    from tests.oracle_lib import Oracle, lib
+    threads = os.cpu_count() or 1
+    lib().orc_set_threads(threads)
+    o = Oracle(p, ref)
+    o.set_bodies(x, q)
+    o.set_external_forces(fe)
+    o.fill_all_blob_pos()
+    o.set_up_gaussians()
+    n = p.system_size
+    v = np.random.default_rng(0).standard_normal(n)
+    t0 = time.perf_counter()
+    o.produce_random_velocity_field(1234, 0)
+    o.calculate_random_blob_velocities()
+    o.calculate_forces()
+    t1 = time.perf_counter()
+    o.multiply_by_saddle_point_matrix(o.multiply_by_Pinv(v))
+    t2 = time.perf_counter()
+    t_step = (t1 - t0) + (gmres_iters + 2) * (t2 - t1)
+    o.close()
+    return {"value": p.num_bodies / t_step, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "1 fluctuating field + forces (%.2fs) and 1 preconditioned saddle-point product (%.2fs) of "
+                      "the same workload, FP64, step = noise + (%.1f GMRES iters + 2) products" %
+                      (t1 - t0, t2 - t1, gmres_iters)}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from timstochrigidbodiessim_b200 import capi, configs
+
+    rank, world, local = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    lib = capi.load()
+    algorithm = 1 if args.algorithm == "gdc" else 2
+    wl = configs.WORKLOADS[args.workload]
+    seed = 1234 + rank
+    p, ref, x, q, fe = configs.rod_suspension(**wl, seed=seed, algorithm=algorithm)
+    results = {}
+    for tag, prec in (("fp64", 0), ("mixed", 1)):
+        pp = p.copy(precision=prec)
+        if prec == 1:
+            pp.gmres_tol = max(p.gmres_tol, 1e-10)
+        s = setup_suspension(pp, ref, x, q, fe, stream)
+        for i in range(args.warmup):
+            s.step(seed, i)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        sampler = ClockSampler(local)
+        if tag == "mixed":
+            sampler.start()
+        l0 = lib.fcm_kernel_launch_count()
+        t, iters = timed_steps(s, args.steps, seed, args.warmup, stream)
+        l1 = lib.fcm_kernel_launch_count()
+        clocks = sampler.stop() if tag == "mixed" else None
+        torch.cuda.synchronize()
+        if world > 1:
+            tt = torch.tensor([t], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+            dist.barrier()
+        results[tag] = dict(t=t, iters=float(np.mean(iters)), launches=l1 - l0, clocks=clocks, s=s)
+    # roofline of the FP64 spread / interpolation kernels (the FP64 context)
+    s64 = results["fp64"]["s"]
+    bytes_, t_spread, t_interp = kernel_roofline(s64, p, stream)
+    # end to end through the C-ABI with host buffers: H2D bodies, step, D2H bodies
+    sm = results["mixed"]["s"]
+    xs, qs = sm.get_bodies()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    K2 = max(2, args.steps // 2)
+    e0.record(stream)
+    for i in range(K2):
+        sm.set_bodies(xs, qs)
+        sm.step(seed, 10000 + i)
+        xs, qs = sm.get_bodies()
+    e1.record(stream)
+    e1.synchronize()
+    t_e2e = e0.elapsed_time(e1) / 1e3
+    if world > 1:
+        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = float(tt.item())
+    err_U, err_l = rel_vel_error(p, ref, x, q, fe, stream) if rank == 0 else (None, None)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs")
+    peak_src = "measured"
+    if not hbm:
+        hbm, peak_src = 6650.0, "fallback"
+    M, K = p.num_bodies, args.steps
+    value = world * M * K / results["mixed"]["t"]
+    fp64_value = world * M * K / results["fp64"]["t"]
+    if rank == 0:
+        ach_s = bytes_ / t_spread / 1e9
+        ach_i = bytes_ / t_interp / 1e9
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline(p, ref, x, q, fe, results["fp64"]["iters"])
+        traffic = None
+        try:
+            prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+            traffic = prof.get(args.workload, {}).get("spread_dram_bytes")
+        except Exception:
+            pass
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": K,
+            "warmup": args.warmup,
+            "ms_per_step": 1e3 * results["mixed"]["t"] / K,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 grid + f64 refinement",
+            "data": "synthetic (seeded random rods, Philox noise)",
+            "config": {"workload": args.workload, "bodies": M, "blobs_per_body": p.blobs_per_body,
+                       "grid": [p.nx, p.ny, p.nz], "box": p.box[0], "algorithm": args.algorithm,
+                       "gmres_tol": p.gmres_tol, "parallelism": "replicas x%d" % world,
+                       "l2": "grid fields (3x%d^3) exceed L2; no flush needed" % p.nx},
+            "fp64": {"value": fp64_value, "ms_per_step": 1e3 * results["fp64"]["t"] / K,
+                     "gmres_iters": results["fp64"]["iters"]},
+            "mixed_over_fp64": value / fp64_value,
+            "gmres_iters_mixed": results["mixed"]["iters"],
+            "rel_vel_error_mixed_vs_fp64": {"bodies": err_U, "blobs": err_l},
+            "roofline": {"kernel": "fcm spread (fp64)", "bound": "hbm", "achieved": ach_s, "peak": hbm,
+                         "unit": "GB/s", "frac": ach_s / hbm, "traffic": traffic,
+                         "bytes_per_launch": bytes_, "ms_per_launch": 1e3 * t_spread, "peak_source": peak_src},
+            "roofline_interp": {"kernel": "fcm interp (fp64)", "achieved": ach_i, "frac": ach_i / hbm,
+                                "ms_per_launch": 1e3 * t_interp},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * M * K2 / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 7 * 8 * M,
+                    "d2h_bytes_per_step": 7 * 8 * M},
+            "gpu_launches": results["mixed"]["launches"],
+            "clocks": results["mixed"]["clocks"],
+        }
+        print(json.dumps(line))
+    for r in results.values():
+        r["s"].close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------- reference
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    from tests.oracle_lib import Oracle, lib
+    from timstochrigidbodiessim_b200 import configs
+    threads = os.cpu_count() or 1
+    lib().orc_set_threads(threads)
+    algorithm = 1 if args.algorithm == "gdc" else 2
+    p, ref, x, q, fe = configs.workload(args.workload, algorithm=algorithm)
+    o = Oracle(p, ref)
+    o.set_bodies(x, q)
+    o.set_external_forces(fe)
+    o.produce_reference_matrices()
+    # GMRES iterations of this workload (one full deterministic solve, untimed)
+    o.fill_all_blob_pos()
+    o.set_up_gaussians()
+    o.calculate_forces()
+    o.assemble_RHS()
+    st, soln, iters, rel = o.invert_saddle_point_system()
+    n = p.system_size
+    v = np.random.default_rng(0).standard_normal(n)
+
+    def sample(i):
+        t0 = time.perf_counter()
+        o.produce_random_velocity_field(1234, i)
+        o.calculate_random_blob_velocities()
+        o.calculate_forces()
+        t1 = time.perf_counter()
+        o.multiply_by_saddle_point_matrix(o.multiply_by_Pinv(v))
+        t2 = time.perf_counter()
+        return (t1 - t0) + (iters + 2) * (t2 - t1)
+
+    for i in range(args.warmup):
+        sample(i)
+    ts = [sample(args.warmup + i) for i in range(args.steps)]
+    t_step = float(np.mean(ts))
+    value = p.num_bodies / t_step
+    desc = ("per step: 1 fluctuating field + forces and 1 preconditioned saddle-point product, FP64, "
+            "scaled to noise + (%d GMRES iterations + 2) products; iterations from one full solve" % iters)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded random rods)",
+        "config": {"workload": args.workload, "bodies": p.num_bodies, "grid": [p.nx, p.ny, p.nz],
+                   "algorithm": args.algorithm, "gmres_tol": p.gmres_tol},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -109,6 +109,10 @@ const char* fcm_last_error(void);
 /* Library version string. */
 const char* fcm_version(void);
 
+/* Number of this library's own kernel launches so far in the process (cuFFT's
+ * kernels are not included); a diagnostic counter. */
+int64_t fcm_kernel_launch_count(void);
+
 /* ================================================================ fft_solver
  * fft_solver.hpp:10-31.  In-place 3-D real transforms on an array of
  * total_local_size = nx*ny*pad doubles, unnormalised, forward sign e^{-iqx},

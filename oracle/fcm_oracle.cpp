@@ -1460,13 +1460,17 @@ void orc_inject_random_stress(orc* o, const double* sxx, const double* syy, cons
 }
 
 // fcm_fluid_solver.cpp:167-234 (SLIP_CHANNEL false): fill order i, k, j; one
-// normal per array per index, in the order sxx, syy, szz, sxy, sxz, syz.
+// normal per array per index, in the order sxx, syy, szz, sxy, sxz, syz.  Each
+// x-plane i draws from its own stream (seed; counter*2^20 + i), as each
+// reference MPI rank draws its x-slab from its own SPRNG stream, so the planes
+// fill in parallel.
 void orc_produce_random_velocity_field(orc* o, uint64_t seed, uint64_t counter) {
   const double var1 = std::sqrt(2.0 * o->kT * o->eta / (o->DX * o->DX * o->DX * o->DT));
   const double var2 = std::sqrt(2.0) * var1;
-  UniformStream rng(seed, counter);
   const int Ny = o->Ny, pad = o->pad;
+#pragma omp parallel for num_threads(g_threads) schedule(static)
   for (int i = 0; i < o->Nx; i++) {
+    UniformStream rng(seed, (counter << 20) + (uint64_t)i);
     const size_t x_index = (size_t)i * Ny * pad;
     for (int k = 0; k < pad; k++)
       for (int j = 0; j < Ny; j++) {

@@ -1,0 +1,49 @@
+import os
+import shutil
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden", "golden.npz")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
+
+
+@pytest.fixture(scope="session")
+def golden():
+    return dict(np.load(GOLDEN))
+
+
+def _cuda_available():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.fixture(scope="session")
+def gpu():
+    """The GPU library, loaded.  A GPU test fails (it is not skipped) when a GPU
+    driver is present but CUDA is unusable; it is skipped only on machines
+    without any NVIDIA driver."""
+    if not _cuda_available():
+        if shutil.which("nvidia-smi") is None:
+            pytest.skip("no GPU on this machine")
+        pytest.fail("nvidia-smi exists but CUDA is unavailable")
+    from timstochrigidbodiessim_b200 import capi
+    return capi.load()
+
+
+def rel_err(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))

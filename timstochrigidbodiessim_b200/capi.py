@@ -21,6 +21,7 @@ SIGNATURES = {
     "fcm_default_params": (None, [ctypes.POINTER(FcmParams)]),
     "fcm_last_error": (ctypes.c_char_p, []),
     "fcm_version": (ctypes.c_char_p, []),
+    "fcm_kernel_launch_count": (ctypes.c_int64, []),
     "fcm_fft_create": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(VP)]),
     "fcm_fft_destroy": (ctypes.c_int, [VP]),
     "fcm_fft_local_sizes": (ctypes.c_int, [VP, I32, I32, I32, I32, I64, I32]),

@@ -2,6 +2,7 @@
 // include/fcm_b200.h.  Every entry point catches C++ exceptions, records the
 // error text (fcm_last_error) and returns a status code.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -15,6 +16,8 @@ namespace fcm {
 
 static thread_local std::string g_err;
 void set_error(const std::string& m) { g_err = m; }
+static std::atomic<long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 namespace {
 bool dense_inv(const std::vector<double>& A, int n, std::vector<double>& out);
@@ -885,6 +888,7 @@ void fcm_default_params(fcm_params* p) {
 
 const char* fcm_last_error(void) { return g_err.c_str(); }
 const char* fcm_version(void) { return "fcm_b200 0.1 (sm_100a)"; }
+int64_t fcm_kernel_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 int fcm_create(const fcm_params* p, const double* blob_ref_pos, fcm_ctx** out) {
   return guard([&] {

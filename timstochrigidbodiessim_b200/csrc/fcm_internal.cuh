@@ -50,8 +50,11 @@ struct Status {
     if (s_ != FCM_OK) return s_;      \
   } while (0)
 
+void count_launch();
+
 #define FCM_LAUNCH_CHECK()                                                      \
   do {                                                                          \
+    ::fcm::count_launch();                                                      \
     cudaError_t e_ = cudaGetLastError();                                        \
     if (e_ != cudaSuccess) {                                                    \
       ::fcm::set_error(std::string("kernel launch: ") + cudaGetErrorString(e_)); \
