@@ -32,18 +32,36 @@ UNIT = "body-steps/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rods2048_phi0.10_g256")
     ap.add_argument("--algorithm", default="em", choices=["em", "gdc"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernels-only", type=int, default=0, metavar="R",
+                    help="profiling mode: R FP64 spread+interp launches and R FP32 mobility products, no steps")
     return ap.parse_args()
 
 
 def dist_env():
     return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
             int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def max_over_ranks(t, device="cuda"):
+    """Slowest rank's time (all_reduce MAX); t itself when not distributed."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(t)
+    tt = torch.tensor([float(t)], device=device, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def replica_throughput(bodies_per_replica, steps, world, t_max):
+    """Whole-job body-steps/s of `world` independent replicas."""
+    return world * bodies_per_replica * steps / t_max
 
 
 # ----------------------------------------------------------------- clocks
@@ -62,7 +80,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -236,10 +254,8 @@ def run_ours(args):
         l1 = lib.fcm_kernel_launch_count()
         clocks = sampler.stop() if tag == "mixed" else None
         torch.cuda.synchronize()
+        t = max_over_ranks(t)
         if world > 1:
-            tt = torch.tensor([t], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t = float(tt.item())
             dist.barrier()
         results[tag] = dict(t=t, iters=float(np.mean(iters)), launches=l1 - l0, clocks=clocks, s=s)
     # roofline of the FP64 spread / interpolation kernels (the FP64 context)
@@ -258,11 +274,7 @@ def run_ours(args):
         xs, qs = sm.get_bodies()
     e1.record(stream)
     e1.synchronize()
-    t_e2e = e0.elapsed_time(e1) / 1e3
-    if world > 1:
-        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_e2e = float(tt.item())
+    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
     err_U, err_l = rel_vel_error(p, ref, x, q, fe, stream) if rank == 0 else (None, None)
     peaks = {}
     try:
@@ -274,8 +286,8 @@ def run_ours(args):
     if not hbm:
         hbm, peak_src = 6650.0, "fallback"
     M, K = p.num_bodies, args.steps
-    value = world * M * K / results["mixed"]["t"]
-    fp64_value = world * M * K / results["fp64"]["t"]
+    value = replica_throughput(M, K, world, results["mixed"]["t"])
+    fp64_value = replica_throughput(M, K, world, results["fp64"]["t"])
     if rank == 0:
         ach_s = bytes_ / t_spread / 1e9
         ach_i = bytes_ / t_interp / 1e9
@@ -316,7 +328,7 @@ def run_ours(args):
             "roofline_interp": {"kernel": "fcm interp (fp64)", "achieved": ach_i, "frac": ach_i / hbm,
                                 "ms_per_launch": 1e3 * t_interp},
             "cpu_baseline": cpu,
-            "e2e": {"value": world * M * K2 / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 7 * 8 * M,
+            "e2e": {"value": replica_throughput(M, K2, world, t_e2e), "unit": UNIT, "h2d_bytes_per_step": 7 * 8 * M,
                     "d2h_bytes_per_step": 7 * 8 * M},
             "gpu_launches": results["mixed"]["launches"],
             "clocks": results["mixed"]["clocks"],
@@ -381,8 +393,37 @@ def run_reference(args):
     }))
 
 
+def run_kernels_only(args):
+    import torch
+    from timstochrigidbodiessim_b200 import configs
+    from timstochrigidbodiessim_b200.fcm import Suspension
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    p, ref, x, q, fe = configs.workload(args.workload)
+    for prec in (0, 1):
+        s = Suspension(p.copy(precision=prec), ref, stream=stream)
+        s.set_bodies(x, q)
+        s.fill_all_blob_pos()
+        s.set_up_gaussians()
+        F = torch.randn(3 * p.num_blobs, dtype=torch.float64, device="cuda")
+        V = torch.empty_like(F)
+        for _ in range(args.kernels_only):
+            if prec == 0:
+                s.set_up_force_distribution(F)
+                s.produce_deterministic_velocity_field()
+                s.calculate_deterministic_blob_velocities(out=V)
+            else:
+                s.apply_mobility(F, out=V)
+        torch.cuda.synchronize()
+        s.close()
+    print(json.dumps({"kernels_only": args.kernels_only, "workload": args.workload}))
+
+
 def main():
     args = parse()
+    if args.kernels_only:
+        run_kernels_only(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

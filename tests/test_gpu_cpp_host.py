@@ -1,0 +1,47 @@
+"""The reference-named C++ classes (csrc/host) through the rigid_bodies_sim
+driver, which runs main.cpp's loop on them, against the CPU oracle."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from tests.oracle_lib import Oracle
+from timstochrigidbodiessim_b200 import build, configs
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("algorithm", [2, 1])
+def test_driver_matches_oracle(gpu, tmp_path, algorithm):
+    p, ref, x, q, fe = configs.rod_suspension(M=8, grid=32, L=24.0, nb=6, seed=5, gmres_tol=1e-12, noise=0,
+                                              ngauss=12, algorithm=algorithm)
+    shape = tmp_path / "shape.txt"
+    shape.write_text("\n".join("%.17g %.17g %.17g" % tuple(ref[3 * m:3 * m + 3]) for m in range(p.blobs_per_body)))
+    ic = tmp_path / "ic.dat"
+    ic.write_text("0 " + " ".join("%.17g %.17g %.17g %.17g %.17g %.17g %.17g" % (tuple(x[3 * n:3 * n + 3]) +
+                                                                                tuple(q[4 * n:4 * n + 4]))
+                                  for n in range(p.num_bodies)) + "\n")
+    args = [build.DRIVER, "shape=%s" % shape, "ic=%s" % ic, "steps=3", "name=%s" % (tmp_path / "run"),
+            "digits=17", "body_force_z=-1"]
+    for k in ("nx", "ny", "nz", "ngauss", "dx", "dt", "ncells", "potential", "steric_fs", "steric_rc",
+              "gmres_max_iter", "gmres_tol", "algorithm", "noise"):
+        args.append("%s=%r" % (k, getattr(p, k)))
+    r = subprocess.run(args, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = (tmp_path / "run.dat").read_text().strip().splitlines()
+    assert len(lines) == 3
+    last = np.array([float(v) for v in lines[-1].split()])
+    xg = last[1:].reshape(-1, 7)[:, :3].ravel()
+    qg = last[1:].reshape(-1, 7)[:, 3:].ravel()
+    o = Oracle(p, ref)
+    o.set_bodies(x, q)
+    o.set_external_forces(fe)
+    o.produce_reference_matrices()
+    for i in range(3):
+        st, info = o.step(0, i)
+        assert st == 0
+    xo, qo = o.get_bodies()
+    assert np.abs(xg - xo).max() < 1e-8
+    assert np.abs(qg - qo).max() < 1e-8
+    assert "skipped_steps 0" in r.stdout

@@ -15,6 +15,10 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(PKG, "libfcm_b200.so")
+HOST_LIB = os.path.join(PKG, "libfcm_b200_host.so")
+DRIVER = os.path.join(PKG, "rigid_bodies_sim")
+HOST_DIR = os.path.join(CSRC, "host")
+CXX = "/usr/bin/g++"
 
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
@@ -60,13 +64,35 @@ def build(verbose=False, ptxas_info=False):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (" ".join(cmd), r.stderr))
+    _build_host()
     return LIB
+
+
+def _build_host():
+    """The reference-named C++ classes (libfcm_b200_host.so) and the driver."""
+    hsrc = os.path.join(HOST_DIR, "fcm_host.cpp")
+    hdr = os.path.join(HOST_DIR, "fcm_host.hpp")
+    main = os.path.join(HOST_DIR, "rigid_bodies_main.cpp")
+    flags = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-I" + os.path.join(ROOT, "include")]
+    newest = max(os.path.getmtime(x) for x in (hsrc, hdr, LIB))
+    if not os.path.exists(HOST_LIB) or os.path.getmtime(HOST_LIB) < newest:
+        cmd = [CXX] + flags + ["-shared", "-o", HOST_LIB, hsrc, "-L" + PKG, "-lfcm_b200", "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("host library build failed:\n%s\n%s" % (" ".join(cmd), r.stderr))
+    newest = max(newest, os.path.getmtime(main), os.path.getmtime(HOST_LIB))
+    if not os.path.exists(DRIVER) or os.path.getmtime(DRIVER) < newest:
+        cmd = [CXX] + flags + ["-o", DRIVER, main, "-L" + PKG, "-lfcm_b200_host", "-lfcm_b200", "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("driver build failed:\n%s\n%s" % (" ".join(cmd), r.stderr))
 
 
 def clean():
     shutil.rmtree(BUILD, ignore_errors=True)
-    if os.path.exists(LIB):
-        os.remove(LIB)
+    for f in (LIB, HOST_LIB, DRIVER):
+        if os.path.exists(f):
+            os.remove(f)
 
 
 if __name__ == "__main__":

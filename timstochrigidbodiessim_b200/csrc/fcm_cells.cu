@@ -244,6 +244,12 @@ PairArgs pair_args(const Ctx& c) {
 
 }  // namespace
 
+int launch_exclusive_scan(const int* in, int* out, int n, cudaStream_t s) {
+  k_exclusive_scan<<<1, 1024, 0, s>>>(in, out, n);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
 // linked_list.cpp:80-102 (populate).
 int cells_build(Ctx& c, cudaStream_t s) {
   const int nc = c.ncell_total;

@@ -2,16 +2,31 @@
 //
 // set_up_gaussians restates fcm_fluid_solver.cpp:131-165; spreading restates
 // :552-600 (SLIP_CHANNEL false) and interpolation :363-424 / :426-487.
+//
+// Tiled spreading.  The grid is cut into 8x8x8 tiles.  After set_up_gaussians
+// every (blob, tile) overlap is listed per tile (count, scan, fill, then a
+// per-tile sort by blob id, so every grid point sums its blobs in ascending blob
+// order -- the reference's order).  One CTA per tile stages the weights of its
+// blobs restricted to the tile in shared memory, accumulates its 512 points in
+// registers and writes every point of the tile exactly once (the zero-fill of
+// fcm_fluid_solver.cpp:556-562 is fused: tiles without blobs write zeros).  No
+// atomics touch the grid.  Grids that cannot be tiled (a dimension not a
+// multiple of 8, or W + 8 > n) use the per-blob atomic scatter.
 #include "fcm_internal.cuh"
 
 namespace fcm {
 
 namespace {
 
+constexpr int TE = 8;    // tile edge
+constexpr int SCB = 16;  // blobs staged per chunk
+
 __device__ __forceinline__ int wrap_index(int i, int n) {
   int r = i % n;
   return r < 0 ? r + n : r;
 }
+
+__device__ __forceinline__ int floordiv(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
 // One thread per (blob, dimension): xc = int(Y/DX); stencil start
 // xc - W/2 + 1; weight anorm*exp(-(xg*DX - Y)^2/anorm2), with sigma = a/sqrt(pi)
@@ -33,8 +48,239 @@ __global__ void k_set_up_gaussians(const double* __restrict__ Y, int n, int W, d
   }
 }
 
-// Spreading, one CTA per blob; each thread owns stencil columns (j,k) and walks
-// x.  Scatter with atomics into the zeroed grid.
+struct TileGeom {
+  int ntx, nty, ntz, nx, ny, nz, W;
+};
+
+// (blob, tile) overlaps of a blob: per dimension the tiles first..first+cnt-1.
+__device__ __forceinline__ void blob_tiles(const int* base, int b, const TileGeom& g, int f[3], int cnt[3]) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int lo = base[3 * b + d];
+    f[d] = floordiv(lo, TE);
+    cnt[d] = floordiv(lo + g.W - 1, TE) - f[d] + 1;
+  }
+}
+
+__global__ void k_tile_count(const int* __restrict__ base, int n, TileGeom g, int* __restrict__ count) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  int f[3], cnt[3];
+  blob_tiles(base, b, g, f, cnt);
+  for (int ox = 0; ox < cnt[0]; ++ox)
+    for (int oy = 0; oy < cnt[1]; ++oy)
+      for (int oz = 0; oz < cnt[2]; ++oz) {
+        const int tile = (wrap_index(f[0] + ox, g.ntx) * g.nty + wrap_index(f[1] + oy, g.nty)) * g.ntz +
+                         wrap_index(f[2] + oz, g.ntz);
+        atomicAdd(count + tile, 1);
+      }
+}
+
+__global__ void k_tile_fill(const int* __restrict__ base, int n, TileGeom g, const int* __restrict__ offset,
+                            int* __restrict__ cursor, unsigned* __restrict__ list) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  int f[3], cnt[3];
+  blob_tiles(base, b, g, f, cnt);
+  for (int ox = 0; ox < cnt[0]; ++ox)
+    for (int oy = 0; oy < cnt[1]; ++oy)
+      for (int oz = 0; oz < cnt[2]; ++oz) {
+        const int tile = (wrap_index(f[0] + ox, g.ntx) * g.nty + wrap_index(f[1] + oy, g.nty)) * g.ntz +
+                         wrap_index(f[2] + oz, g.ntz);
+        const unsigned j = (unsigned)((ox * cnt[1] + oy) * cnt[2] + oz);
+        list[offset[tile] + atomicAdd(cursor + tile, 1)] = ((unsigned)b << 6) | j;
+      }
+}
+
+// Ascending blob order within each tile (a blob meets a tile at most once).
+__global__ void k_tile_sort(const int* __restrict__ offset, int ntiles, unsigned* __restrict__ list) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntiles) return;
+  const int b = offset[t], e = offset[t + 1];
+  for (int i = b + 1; i < e; ++i) {
+    const unsigned v = list[i];
+    int j = i - 1;
+    while (j >= b && list[j] > v) {
+      list[j + 1] = list[j];
+      --j;
+    }
+    list[j + 1] = v;
+  }
+}
+
+// Tiled spreading: one CTA (128 threads) per 8x8x8 tile.  Thread t owns the
+// four points x = 4*xh..4*xh+3 of column (y, z), xh = t/64, y = (t/8)%8,
+// z = t%8; warp w covers x-half w/2 and y-half w%2, and skips blobs whose
+// stencil misses that 4x4x8 quarter (a warp-uniform branch).
+template <typename T>
+__global__ void __launch_bounds__(128) k_spread_tiled(const int* __restrict__ base, const T* __restrict__ w,
+                                                      const double* __restrict__ F, TileGeom g,
+                                                      const int* __restrict__ offset,
+                                                      const unsigned* __restrict__ list, long long G,
+                                                      T* __restrict__ grid) {
+  __shared__ T sw[SCB][3][TE];
+  __shared__ T sF[SCB][3];
+  __shared__ int sflag[SCB];
+  const int tile = blockIdx.x;
+  const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
+  const int O[3] = {tx * TE, ty * TE, tz * TE};
+  const int N[3] = {g.nx, g.ny, g.nz};
+  const int t = threadIdx.x;
+  const int z = t & 7, y = (t >> 3) & 7, xh = t >> 6, yh = (t >> 5) & 1;
+  T acc[4][3];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) acc[i][c] = 0;
+  const int b0 = offset[tile], b1 = offset[tile + 1];
+  for (int c0 = b0; c0 < b1; c0 += SCB) {
+    const int nc = min(SCB, b1 - c0);
+    if (t < SCB) sflag[t] = 0;
+    __syncthreads();
+    for (int e = t; e < nc * 3 * TE; e += 128) {
+      const int k = e / (3 * TE), r = e - k * 3 * TE, d = r / TE, i = r - d * TE;
+      const int b = (int)(list[c0 + k] >> 6);
+      const int s = wrap_index(O[d] + i - base[3 * b + d], N[d]);
+      const T v = (s < g.W) ? w[(size_t)(3 * b + d) * g.W + s] : (T)0;
+      sw[k][d][i] = v;
+      if (d < 2 && v != (T)0) atomicOr(&sflag[k], 1 << (2 * d + (i >> 2)));
+    }
+    for (int e = t; e < nc * 3; e += 128) {
+      const int k = e / 3, c = e - 3 * k;
+      sF[k][c] = (T)F[3 * (size_t)(list[c0 + k] >> 6) + c];
+    }
+    __syncthreads();
+    for (int k = 0; k < nc; ++k) {
+      const int fl = sflag[k];
+      if (!((fl >> xh) & 1) || !((fl >> (2 + yh)) & 1)) continue;
+      const T wyz = sw[k][1][y] * sw[k][2][z];
+      const T f0 = sF[k][0] * wyz, f1 = sF[k][1] * wyz, f2 = sF[k][2] * wyz;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const T wx = sw[k][0][4 * xh + i];
+        acc[i][0] += f0 * wx;
+        acc[i][1] += f1 * wx;
+        acc[i][2] += f2 * wx;
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const long long idx = ((long long)(O[0] + 4 * xh + i) * g.ny + (O[1] + y)) * g.nz + (O[2] + z);
+    grid[idx] = acc[i][0];
+    grid[G + idx] = acc[i][1];
+    grid[2 * G + idx] = acc[i][2];
+  }
+}
+
+// Tiled interpolation: one CTA (two warps) per 8x8x8 tile.  The tile's three
+// velocity components are staged in shared memory (x-plane stride padded to 66
+// values so the four x-slabs a warp reads at once fall in distinct banks).  A
+// warp takes eight of the tile's blobs at a time; lane l serves blob l/4 and
+// x-slab l%4 (two x-planes), forms sum u * wx*wy*wz over its 128 points with the
+// blob's restricted weights held in registers, and the four slab partials are
+// combined with two shuffles.  The per-(blob, tile) partial goes to
+// partial[blob][j][3]; k_interp_reduce sums a blob's partials in j order, so
+// the result is deterministic and no atomics are used.
+constexpr int IPS = 66;  // padded x-plane stride of the staged tile
+
+template <typename T>
+__global__ void __launch_bounds__(64) k_interp_tiled(const int* __restrict__ base, const T* __restrict__ w,
+                                                     const T* __restrict__ grid, TileGeom g,
+                                                     const int* __restrict__ offset,
+                                                     const unsigned* __restrict__ list, long long G,
+                                                     T* __restrict__ partial) {
+  __shared__ T su[3][TE * IPS];
+  const int tile = blockIdx.x;
+  const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
+  const int O[3] = {tx * TE, ty * TE, tz * TE};
+  const int N[3] = {g.nx, g.ny, g.nz};
+  const int t = threadIdx.x;
+  const int b0 = offset[tile], b1 = offset[tile + 1];
+  if (b0 == b1) return;  // no blob meets this tile (uniform over the CTA)
+  for (int e = t; e < 3 * 512; e += 64) {
+    const int c = e >> 9, p = e & 511, x = p >> 6, yz = p & 63;
+    const long long idx = ((long long)(O[0] + x) * g.ny + (O[1] + (yz >> 3))) * g.nz + (O[2] + (yz & 7));
+    su[c][x * IPS + yz] = grid[c * G + idx];
+  }
+  __syncthreads();
+  const int lane = t & 31, warp = t >> 5;
+  const int slab = lane & 3, kk = lane >> 2;
+  for (int g0 = b0 + 8 * warp; g0 < b1; g0 += 16) {
+    const int k = g0 + kk;
+    const bool active = k < b1;
+    unsigned v = active ? list[k] : 0u;
+    const int b = (int)(v >> 6);
+    T wy[TE], wz[TE], wx[2];
+#pragma unroll
+    for (int i = 0; i < TE; ++i) {
+      int s = wrap_index(O[1] + i - base[3 * b + 1], N[1]);
+      wy[i] = (active && s < g.W) ? w[(size_t)(3 * b + 1) * g.W + s] : (T)0;
+      s = wrap_index(O[2] + i - base[3 * b + 2], N[2]);
+      wz[i] = (active && s < g.W) ? w[(size_t)(3 * b + 2) * g.W + s] : (T)0;
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int s = wrap_index(O[0] + 2 * slab + i - base[3 * b], N[0]);
+      wx[i] = (active && s < g.W) ? w[(size_t)(3 * b) * g.W + s] : (T)0;
+    }
+    T a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const T* p0 = &su[0][(2 * slab + i) * IPS];
+      const T* p1 = &su[1][(2 * slab + i) * IPS];
+      const T* p2 = &su[2][(2 * slab + i) * IPS];
+#pragma unroll
+      for (int y = 0; y < TE; ++y) {
+        const T wxy = wx[i] * wy[y];
+#pragma unroll
+        for (int z = 0; z < TE; ++z) {
+          const T wt = wxy * wz[z];
+          a0 += p0[y * TE + z] * wt;
+          a1 += p1[y * TE + z] * wt;
+          a2 += p2[y * TE + z] * wt;
+        }
+      }
+    }
+#pragma unroll
+    for (int off = 1; off <= 2; off <<= 1) {
+      a0 += __shfl_xor_sync(0xffffffffu, a0, off);
+      a1 += __shfl_xor_sync(0xffffffffu, a1, off);
+      a2 += __shfl_xor_sync(0xffffffffu, a2, off);
+    }
+    if (active && slab == 0) {
+      T* o = partial + ((size_t)b * 64 + (v & 63u)) * 3;
+      o[0] = a0;
+      o[1] = a1;
+      o[2] = a2;
+    }
+  }
+}
+
+// V = DX^3 * sum over the blob's tiles (in canonical order j) of the partials.
+template <typename T>
+__global__ void k_interp_reduce(const int* __restrict__ base, const T* __restrict__ partial, int n, TileGeom g,
+                                double dx3, double* __restrict__ V) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  int f[3], cnt[3];
+  blob_tiles(base, b, g, f, cnt);
+  const int nj = cnt[0] * cnt[1] * cnt[2];
+  double s0 = 0, s1 = 0, s2 = 0;
+  const T* p = partial + (size_t)b * 64 * 3;
+  for (int j = 0; j < nj; ++j) {
+    s0 += (double)p[3 * j];
+    s1 += (double)p[3 * j + 1];
+    s2 += (double)p[3 * j + 2];
+  }
+  V[3 * b] = s0 * dx3;
+  V[3 * b + 1] = s1 * dx3;
+  V[3 * b + 2] = s2 * dx3;
+}
+
+// Spreading of grids that cannot be tiled: one CTA per blob, each thread owns
+// stencil columns (j,k) and walks x, atomics into the zeroed grid.
 template <typename T>
 __global__ void k_spread_atomic(const int* __restrict__ base, const T* __restrict__ w, const double* __restrict__ F,
                                 int W, int nx, int ny, int nz, long long G, T* __restrict__ grid) {
@@ -90,15 +336,27 @@ __global__ void __launch_bounds__(NT) k_interp_block(const int* __restrict__ bas
     s2 += __shfl_down_sync(0xffffffffu, s2, off);
   }
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (lane == 0) { red[0][wid] = s0; red[1][wid] = s1; red[2][wid] = s2; }
+  if (lane == 0) {
+    red[0][wid] = s0;
+    red[1][wid] = s1;
+    red[2][wid] = s2;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     T a0 = 0, a1 = 0, a2 = 0;
-    for (int i = 0; i < NT / 32; ++i) { a0 += red[0][i]; a1 += red[1][i]; a2 += red[2][i]; }
+    for (int i = 0; i < NT / 32; ++i) {
+      a0 += red[0][i];
+      a1 += red[1][i];
+      a2 += red[2][i];
+    }
     V[3 * np] = (double)a0 * dx3;
     V[3 * np + 1] = (double)a1 * dx3;
     V[3 * np + 2] = (double)a2 * dx3;
   }
+}
+
+TileGeom tile_geom(const GridDims& g, int W) {
+  return TileGeom{g.nx / TE, g.ny / TE, g.nz / TE, g.nx, g.ny, g.nz, W};
 }
 
 }  // namespace
@@ -111,7 +369,22 @@ int blob_table_alloc(BlobTable<T>& t, int n, int W, const GridDims& g) {
   t.W = W;
   FCM_CUDA(cudaMalloc(&t.base, sizeof(int) * 3 * (size_t)(n > 0 ? n : 1)));
   FCM_CUDA(cudaMalloc(&t.w, sizeof(T) * 3 * (size_t)W * (n > 0 ? n : 1)));
-  (void)g;
+  const bool ok = g.nx % TE == 0 && g.ny % TE == 0 && g.nz % TE == 0 && W + TE <= g.nx && W + TE <= g.ny &&
+                  W + TE <= g.nz && n < (1 << 26);
+  if (ok) {
+    t.tiled = true;
+    t.ntx = g.nx / TE;
+    t.nty = g.ny / TE;
+    t.ntz = g.nz / TE;
+    t.ntiles = t.ntx * t.nty * t.ntz;
+    const long long per = (long long)((W + TE - 2) / TE + 1);
+    t.tile_cap = (long long)(n > 0 ? n : 1) * per * per * per;
+    FCM_CUDA(cudaMalloc(&t.tile_count, sizeof(int) * (size_t)t.ntiles));
+    FCM_CUDA(cudaMalloc(&t.tile_offset, sizeof(int) * ((size_t)t.ntiles + 1)));
+    FCM_CUDA(cudaMalloc(&t.tile_cursor, sizeof(int) * (size_t)t.ntiles));
+    FCM_CUDA(cudaMalloc(&t.tile_list, sizeof(unsigned) * (size_t)t.tile_cap));
+    FCM_CUDA(cudaMalloc(&t.partial, sizeof(T) * 64 * 3 * (size_t)(n > 0 ? n : 1)));
+  }
   return FCM_OK;
 }
 
@@ -120,9 +393,10 @@ void blob_table_free(BlobTable<T>& t) {
   cudaFree(t.base);
   cudaFree(t.w);
   cudaFree(t.tile_count);
-  cudaFree(t.tile_blobs);
+  cudaFree(t.tile_offset);
   cudaFree(t.tile_cursor);
-  cudaFree(t.tile_total);
+  cudaFree(t.tile_list);
+  cudaFree(t.partial);
   t = BlobTable<T>();
 }
 
@@ -136,11 +410,29 @@ int launch_set_up_gaussians(const Ctx& c, BlobTable<T>& t, const double* dY, cud
   const int nt = 3 * t.n;
   k_set_up_gaussians<T><<<(nt + 127) / 128, 128, 0, s>>>(dY, t.n, t.W, c.g.dx, anorm, anorm2, t.base, t.w);
   FCM_LAUNCH_CHECK();
+  if (t.tiled) {
+    const TileGeom g = tile_geom(c.g, t.W);
+    FCM_CUDA(cudaMemsetAsync(t.tile_count, 0, sizeof(int) * (size_t)t.ntiles, s));
+    FCM_CUDA(cudaMemsetAsync(t.tile_cursor, 0, sizeof(int) * (size_t)t.ntiles, s));
+    k_tile_count<<<(t.n + 127) / 128, 128, 0, s>>>(t.base, t.n, g, t.tile_count);
+    FCM_LAUNCH_CHECK();
+    FCM_TRY(launch_exclusive_scan(t.tile_count, t.tile_offset, t.ntiles, s));
+    k_tile_fill<<<(t.n + 127) / 128, 128, 0, s>>>(t.base, t.n, g, t.tile_offset, t.tile_cursor, t.tile_list);
+    FCM_LAUNCH_CHECK();
+    k_tile_sort<<<(t.ntiles + 127) / 128, 128, 0, s>>>(t.tile_offset, t.ntiles, t.tile_list);
+    FCM_LAUNCH_CHECK();
+  }
   return FCM_OK;
 }
 
 template <typename T>
 int launch_spread(const Ctx& c, const BlobTable<T>& t, const double* dF, T* grid, cudaStream_t s) {
+  if (t.tiled) {
+    k_spread_tiled<T><<<t.ntiles, 128, 0, s>>>(t.base, t.w, dF, tile_geom(c.g, t.W), t.tile_offset, t.tile_list,
+                                               c.g.G, grid);
+    FCM_LAUNCH_CHECK();
+    return FCM_OK;
+  }
   FCM_CUDA(cudaMemsetAsync(grid, 0, sizeof(T) * 3 * (size_t)c.g.G, s));
   if (t.n == 0) return FCM_OK;
   k_spread_atomic<T><<<t.n, 128, 0, s>>>(t.base, t.w, dF, t.W, c.g.nx, c.g.ny, c.g.nz, c.g.G, grid);
@@ -152,6 +444,14 @@ template <typename T>
 int launch_interp(const Ctx& c, const BlobTable<T>& t, const T* grid, double* dV, cudaStream_t s) {
   if (t.n == 0) return FCM_OK;
   const double dx3 = c.g.dx * c.g.dx * c.g.dx;
+  if (t.tiled) {
+    const TileGeom g = tile_geom(c.g, t.W);
+    k_interp_tiled<T><<<t.ntiles, 64, 0, s>>>(t.base, t.w, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial);
+    FCM_LAUNCH_CHECK();
+    k_interp_reduce<T><<<(t.n + 127) / 128, 128, 0, s>>>(t.base, t.partial, t.n, g, dx3, dV);
+    FCM_LAUNCH_CHECK();
+    return FCM_OK;
+  }
   k_interp_block<T, 256><<<t.n, 256, 0, s>>>(t.base, t.w, grid, t.W, c.g.nx, c.g.ny, c.g.nz, c.g.G, dx3, dV);
   FCM_LAUNCH_CHECK();
   return FCM_OK;

@@ -89,13 +89,17 @@ struct BlobTable {
   int W = 0;         // stencil width
   int* base = nullptr;   // [n][3] unwrapped first grid index per dim
   T* w = nullptr;        // [n][3][W]
-  // tile binning for the tiled spread / interpolation
-  int ntiles = 0;
-  int* tile_count = nullptr;   // [ntiles+1] counts then exclusive offsets
-  int* tile_blobs = nullptr;   // [cap] blob ids grouped by tile
+  // Binning of (blob, tile) overlaps for the tiled spread / interpolation.
+  // Usable when every grid dimension is a multiple of the tile edge and
+  // W + tile edge <= n (a stencil never meets the same tile twice).
+  bool tiled = false;
+  int ntx = 0, nty = 0, ntz = 0, ntiles = 0;
+  int* tile_count = nullptr;      // [ntiles]
+  int* tile_offset = nullptr;     // [ntiles+1] exclusive offsets
+  int* tile_cursor = nullptr;     // [ntiles]
+  unsigned* tile_list = nullptr;  // [cap] (blob << 6) | j, j = canonical tile index of the blob
   long long tile_cap = 0;
-  int* tile_cursor = nullptr;  // [ntiles]
-  int* tile_total = nullptr;   // [1] device total of (blob,tile) overlaps
+  T* partial = nullptr;           // [n][64][3] per-(blob, tile) interpolation partials
 };
 
 // Grid buffers and cuFFT plans of one precision.
@@ -196,6 +200,7 @@ int launch_rigid_projection(const Ctx& c, const double* q, const double* V, doub
 int launch_body_update(const Ctx& c, double* x, double* q, const double* U6, double scale, cudaStream_t s);
 int launch_body_update_uniform(const Ctx& c, double* x, double* q, const double* e6, cudaStream_t s);
 int launch_divU_accumulate(const Ctx& c, const double* U6, const double* U0, int component, double delta, double* acc, cudaStream_t s);
+int launch_exclusive_scan(const int* in, int* out, int n, cudaStream_t s);
 // cells (fcm_cells.cu)
 int cells_build(Ctx& c, cudaStream_t s);
 int cells_steric_forces(const Ctx& c, double* F, bool accumulate, cudaStream_t s);

@@ -40,23 +40,26 @@ struct KParams {
   int nx, ny, nz, nzh;
   long long Gc;
   double fx, fy, fz;  // 2 pi / L
-  double etaG;        // eta * nx*ny*nz
+  double inv_etaG;    // 1 / (eta * nx*ny*nz)
 };
 
-// Projection of one complex mode (re and im share the real factors).
+// Projection of one complex mode (re and im share the real factors).  The
+// reference divides every component by eta*G; here one reciprocal of the
+// mode's |q|^2 and a precomputed 1/(eta*G) are used instead (a last-bit change).
 template <typename T>
 __device__ __forceinline__ void project_mode(double q1, double q2, double q3, const V2<T> f[3], V2<T> u[3],
-                                             T etaG) {
+                                             T inv_etaG) {
   const T t1 = (T)q1, t2 = (T)q2, t3 = (T)q3;
   const T qq = (T)(q2 * q2) + (T)(q1 * q1) + (T)1e-16;
   const T norm = (T)1 / (qq + (T)(q3 * q3));
   const T kr = (t1 * f[0].x + t2 * f[1].x + t3 * f[2].x) * norm;
   const T ki = (t1 * f[0].y + t2 * f[1].y + t3 * f[2].y) * norm;
+  const T sc = norm * inv_etaG;
   const T qv[3] = {t1, t2, t3};
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    u[c].x = norm * (f[c].x - qv[c] * kr) / etaG;
-    u[c].y = norm * (f[c].y - qv[c] * ki) / etaG;
+    u[c].x = sc * (f[c].x - qv[c] * kr);
+    u[c].y = sc * (f[c].y - qv[c] * ki);
   }
 }
 
@@ -103,7 +106,7 @@ __global__ void k_project(C* __restrict__ spec, KParams k) {
   V2<T> f[3], u[3];
   if (!is_plane(kz, k)) {
     load3(spec, k.Gc, t, f);
-    project_mode<T>(q1, q2, q3, f, u, (T)k.etaG);
+    project_mode<T>(q1, q2, q3, f, u, (T)k.inv_etaG);
     store3(spec, k.Gc, t, u);
     return;
   }
@@ -116,7 +119,7 @@ __global__ void k_project(C* __restrict__ spec, KParams k) {
     return;
   }
   load3(spec, k.Gc, t, f);
-  project_mode<T>(q1, q2, q3, f, u, (T)k.etaG);
+  project_mode<T>(q1, q2, q3, f, u, (T)k.inv_etaG);
   if (tp == t) {
     for (int c = 0; c < 3; ++c) u[c].y = 0;
     store3(spec, k.Gc, t, u);
@@ -125,7 +128,7 @@ __global__ void k_project(C* __restrict__ spec, KParams k) {
   V2<T> fp[3], up[3];
   load3(spec, k.Gc, tp, fp);
   const double p1 = wavenumber(xp, k.nx, k.fx), p2 = wavenumber(yp, k.ny, k.fy);
-  project_mode<T>(p1, p2, q3, fp, up, (T)k.etaG);
+  project_mode<T>(p1, p2, q3, fp, up, (T)k.inv_etaG);
   V2<T> us[3], usp[3];
   for (int c = 0; c < 3; ++c) {
     us[c].x = (T)0.5 * (u[c].x + up[c].x);
@@ -259,7 +262,7 @@ __global__ void k_fluct(C* __restrict__ spec, const cufftDoubleComplex* __restri
   V2<T> f[3], u[3];
   stress_divergence<T>(q1, q2, q3, s, f);
   const double r1 = wavenumber(x, k.nx, k.fx), r2 = wavenumber(y, k.ny, k.fy), r3 = (double)kz * k.fz;
-  project_mode<T>(r1, r2, r3, f, u, (T)k.etaG);
+  project_mode<T>(r1, r2, r3, f, u, (T)k.inv_etaG);
   if (!plane) {
     store3(spec, k.Gc, t, u);
     return;
@@ -273,7 +276,7 @@ __global__ void k_fluct(C* __restrict__ spec, const cufftDoubleComplex* __restri
   divergence_q(xp, yp, kz, k, p1, p2, p3);
   V2<T> fp[3], up[3];
   stress_divergence<T>(p1, p2, p3, sp, fp);
-  project_mode<T>(wavenumber(xp, k.nx, k.fx), wavenumber(yp, k.ny, k.fy), r3, fp, up, (T)k.etaG);
+  project_mode<T>(wavenumber(xp, k.nx, k.fx), wavenumber(yp, k.ny, k.fy), r3, fp, up, (T)k.inv_etaG);
   V2<T> us[3], usp[3];
   for (int c = 0; c < 3; ++c) {
     us[c].x = (T)0.5 * (u[c].x + up[c].x);
@@ -293,7 +296,7 @@ KParams make_kparams(const Ctx& c) {
   k.fx = 2.0 * PI / c.g.Lx;
   k.fy = 2.0 * PI / c.g.Ly;
   k.fz = 2.0 * PI / c.g.Lz;
-  k.etaG = c.p.viscosity * ((double)c.g.nx * (double)c.g.ny * (double)c.g.nz);
+  k.inv_etaG = 1.0 / (c.p.viscosity * ((double)c.g.nx * (double)c.g.ny * (double)c.g.nz));
   return k;
 }
 
