@@ -245,6 +245,26 @@ int fcm_invert_saddle_point_system(fcm_ctx* ctx, double* soln, int32_t* iters,
  * params.noise is 1.  Returns FCM_OK or FCM_ERR_OVERLAP (state restored). */
 int fcm_step(fcm_ctx* ctx, uint64_t seed, uint64_t step_index, fcm_step_info* info);
 
+/* ================================================================ allocation-free interpolation
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory -- a time-step loop that must not stall the device (cudaMalloc and
+ * cudaFree synchronise it), or an application whose device memory all belongs to
+ * its own allocator or pool -- this interpolates a caller-owned velocity grid
+ * onto blobs without allocating anything.  Same result as
+ * fcm_calculate_deterministic_blob_velocities on the same grid and positions:
+ *   V(3*nblobs) = DX^3 * sum u * gx*gy*gz   (fcm_fluid_solver.cpp:363-424).
+ * Y (nblobs*3), grid (3*nx*ny*nz, component-major [3][nx][ny][nz], unpadded) and V
+ * must be DEVICE pointers; work is issued on `stream` (a cudaStream_t, 0 = legacy).
+ * Limits: nblobs <= 8192, ngauss <= 24, nx, ny, nz multiples of 8 with
+ * ngauss + 8 <= n, and at most 32768 8^3 tiles (a 256^3 grid); larger inputs are
+ * rejected with FCM_ERR_INVALID.  Scratch is a fixed 20 MiB device array inside the
+ * library, held by every GPU that loads it until exit.  The first call on a device
+ * looks up that array's device address (once per device), so make the first call
+ * before any stream capture.  Every call shares the array: calls that may overlap
+ * on the GPU (different streams, no ordering between them) race. */
+int fcm_interp_noalloc(int32_t nx, int32_t ny, int32_t nz, double dx, double blob_radius, int32_t ngauss,
+                       int32_t nblobs, const double* Y, const double* grid, double* V, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -72,6 +72,8 @@ SIGNATURES = {
     "fcm_multiply_by_saddle_point_matrix": (ctypes.c_int, [VP, VP, VP]),
     "fcm_invert_saddle_point_system": (ctypes.c_int, [VP, VP, I32, D]),
     "fcm_step": (ctypes.c_int, [VP, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(FcmStepInfo)]),
+    "fcm_interp_noalloc": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_int32, ctypes.c_int32, VP, VP, VP, VP]),
 }
 
 _lib = None

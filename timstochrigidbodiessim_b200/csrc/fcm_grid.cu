@@ -12,6 +12,9 @@
 // fcm_fluid_solver.cpp:556-562 is fused: tiles without blobs write zeros).  No
 // atomics touch the grid.  Grids that cannot be tiled (a dimension not a
 // multiple of 8, or W + 8 > n) use the per-blob atomic scatter.
+#include <mutex>
+#include <string>
+
 #include "fcm_internal.cuh"
 
 namespace fcm {
@@ -469,3 +472,143 @@ template int launch_interp<double>(const Ctx&, const BlobTable<double>&, const d
 template int launch_interp<float>(const Ctx&, const BlobTable<float>&, const float*, double*, cudaStream_t);
 
 }  // namespace fcm
+
+// ============================================================ allocation-free interpolation
+// A variant of the tiled interpolation for callers that must not allocate device
+// memory: code that runs between the kernels of a time step and may not stall the
+// device (cudaMalloc and cudaFree synchronise it), or applications whose device
+// memory is owned entirely by their own allocator or memory pool.  Its scratch --
+// Gaussian tables, tile lists and per-(blob, tile) partials -- lives in one
+// file-scope device array of fixed size, held by every GPU that loads the library
+// until the process exits.  Limits: at most NA_MAX_BLOBS blobs, a stencil of at
+// most NA_MAX_W points and at most NA_MAX_TILES 8^3 tiles (a 256^3 grid).
+namespace fcm {
+namespace {
+
+constexpr int NA_MAX_BLOBS = 8192;
+constexpr int NA_MAX_W = 24;
+constexpr int NA_MAX_TILES = 32768;
+constexpr size_t NA_SCRATCH_BYTES = (size_t)20 << 20;  // 20 MiB
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_SCRATCH_BYTES];
+
+inline size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// Device address of g_noalloc_scratch on the current device, looked up once per
+// device (the name is only a host-side stand-in in host code).
+int noalloc_scratch_address(void** out) {
+  static std::mutex mtx;
+  static void* addr[256] = {};
+  int dev = 0;
+  FCM_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256) {
+    set_error("fcm_interp_noalloc: device ordinal out of range");
+    return FCM_ERR_INVALID;
+  }
+  std::lock_guard<std::mutex> lock(mtx);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      set_error(std::string("fcm_interp_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+      return FCM_ERR_CUDA;
+    }
+    addr[dev] = p;
+  }
+  *out = addr[dev];
+  return FCM_OK;
+}
+
+bool on_device(const void* p) {
+  cudaPointerAttributes a;
+  if (!p || cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace
+}  // namespace fcm
+
+extern "C" int fcm_interp_noalloc(int32_t nx, int32_t ny, int32_t nz, double dx, double blob_radius,
+                                  int32_t ngauss, int32_t nblobs, const double* Y, const double* grid, double* V,
+                                  void* stream) {
+  using namespace fcm;
+  const int W = ngauss, n = nblobs;
+  if (n < 1 || n > NA_MAX_BLOBS) {
+    set_error("fcm_interp_noalloc: nblobs must be in [1, " + std::to_string(NA_MAX_BLOBS) + "], got " +
+              std::to_string(n));
+    return FCM_ERR_INVALID;
+  }
+  if (W < 1 || W > NA_MAX_W) {
+    set_error("fcm_interp_noalloc: ngauss must be in [1, " + std::to_string(NA_MAX_W) + "], got " +
+              std::to_string(W));
+    return FCM_ERR_INVALID;
+  }
+  if (nx % TE || ny % TE || nz % TE || W + TE > nx || W + TE > ny || W + TE > nz) {
+    set_error("fcm_interp_noalloc: grid dimensions must be multiples of 8 and at least ngauss + 8");
+    return FCM_ERR_INVALID;
+  }
+  const long long ntiles = (long long)(nx / TE) * (ny / TE) * (nz / TE);
+  if (ntiles > NA_MAX_TILES) {
+    set_error("fcm_interp_noalloc: grid has " + std::to_string(ntiles) + " 8^3 tiles, at most " +
+              std::to_string(NA_MAX_TILES) + " are allowed (a 256^3 grid)");
+    return FCM_ERR_INVALID;
+  }
+  if (!(dx > 0.0) || !(blob_radius > 0.0)) {
+    set_error("fcm_interp_noalloc: dx and blob_radius must be > 0");
+    return FCM_ERR_INVALID;
+  }
+  if (!on_device(Y) || !on_device(grid) || !on_device(V)) {
+    set_error("fcm_interp_noalloc: Y, grid and V must be device pointers");
+    return FCM_ERR_INVALID;
+  }
+  void* base_ptr = nullptr;
+  FCM_TRY(noalloc_scratch_address(&base_ptr));
+  // carve the scratch array
+  const int per = (W + TE - 2) / TE + 1;
+  const size_t cap = (size_t)n * per * per * per;
+  unsigned char* p = (unsigned char*)base_ptr;
+  int* s_base = (int*)p;
+  p += round256(sizeof(int) * 3 * (size_t)n);
+  double* s_w = (double*)p;
+  p += round256(sizeof(double) * 3 * (size_t)W * n);
+  int* s_count = (int*)p;
+  p += round256(sizeof(int) * (size_t)ntiles);
+  int* s_offset = (int*)p;
+  p += round256(sizeof(int) * ((size_t)ntiles + 1));
+  int* s_cursor = (int*)p;
+  p += round256(sizeof(int) * (size_t)ntiles);
+  unsigned* s_list = (unsigned*)p;
+  p += round256(sizeof(unsigned) * cap);
+  double* s_partial = (double*)p;
+  p += round256(sizeof(double) * 64 * 3 * (size_t)n);
+  if ((size_t)(p - (unsigned char*)base_ptr) > NA_SCRATCH_BYTES) {
+    set_error("fcm_interp_noalloc: scratch layout exceeds the static array");
+    return FCM_ERR_INVALID;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const double PI = 3.14159265358979323846264338327950288;
+  const double anorm = 1.0 / (sqrt(2.0) * blob_radius);
+  const double anorm2 = 2.0 * blob_radius * blob_radius / PI;
+  const TileGeom g{nx / TE, ny / TE, nz / TE, nx, ny, nz, W};
+  const long long G = (long long)nx * ny * nz;
+  // the array keeps the previous call's contents: counters start at zero
+  FCM_CUDA(cudaMemsetAsync(s_count, 0, sizeof(int) * (size_t)ntiles, s));
+  FCM_CUDA(cudaMemsetAsync(s_cursor, 0, sizeof(int) * (size_t)ntiles, s));
+  k_set_up_gaussians<double><<<(3 * n + 127) / 128, 128, 0, s>>>(Y, n, W, dx, anorm, anorm2, s_base, s_w);
+  FCM_LAUNCH_CHECK();
+  k_tile_count<<<(n + 127) / 128, 128, 0, s>>>(s_base, n, g, s_count);
+  FCM_LAUNCH_CHECK();
+  FCM_TRY(launch_exclusive_scan(s_count, s_offset, (int)ntiles, s));
+  k_tile_fill<<<(n + 127) / 128, 128, 0, s>>>(s_base, n, g, s_offset, s_cursor, s_list);
+  FCM_LAUNCH_CHECK();
+  k_tile_sort<<<(unsigned)((ntiles + 127) / 128), 128, 0, s>>>(s_offset, (int)ntiles, s_list);
+  FCM_LAUNCH_CHECK();
+  k_interp_tiled<double><<<(unsigned)ntiles, 64, 0, s>>>(s_base, s_w, grid, g, s_offset, s_list, G, s_partial);
+  FCM_LAUNCH_CHECK();
+  k_interp_reduce<double><<<(n + 127) / 128, 128, 0, s>>>(s_base, s_partial, n, g, dx * dx * dx, V);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
