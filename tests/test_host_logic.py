@@ -95,3 +95,22 @@ def test_workload_is_overlap_free(name):
 def test_volume_fraction_box():
     L = configs.box_for_volume_fraction(12288, 0.10)
     assert abs(L - 80.141) < 0.001
+
+
+def test_ensemble_members_are_valid():
+    """Batched-ensemble instances: body counts in [50, 500], volume fraction in
+    [0.05, 0.20], grids 2^k or 3*2^k in [64, 128], no inter-body overlap."""
+    from scipy.spatial import cKDTree
+    for i in (0, 8):  # instance 8 is dense enough to need the compression path
+        p, ref, x, q, fe = configs.ensemble(1, seed0=i)[0]
+        assert 50 <= p.num_bodies <= 500 and p.nx in (64, 96, 128)
+        L = p.box[0]
+        phi = p.num_blobs * 4.0 / 3.0 * np.pi / L ** 3
+        assert 0.05 <= phi <= 0.20
+        R = configs.rotation_matrices(q.reshape(-1, 4))
+        Y = ((x.reshape(-1, 1, 3) + np.einsum("nij,mj->nmi", R, ref.reshape(-1, 3))) % L).reshape(-1, 3)
+        body = np.repeat(np.arange(p.num_bodies), p.blobs_per_body)
+        pr = cKDTree(Y, boxsize=L).query_pairs(2.0, output_type="ndarray")
+        assert not len(pr) or np.all(body[pr[:, 0]] == body[pr[:, 1]])
+    assert configs.nearest_fft_size(117) == 128 and configs.nearest_fft_size(40) == 64
+    assert configs.nearest_fft_size(100) == 96

@@ -43,57 +43,120 @@ def rotation_matrices(q):
     return R
 
 
-def seed_bodies(rng, M, ref, L, min_dist=2.0 * A, max_trials=200000):
-    """Random non-overlapping placement by rejection (cell-hashed blob checks)."""
+def relax_overlaps(x, q, ref, L, min_dist=2.0 * A, max_iter=5000):
+    """Push overlapping bodies apart until no inter-body blob pair is closer than
+    min_dist: the drag relaxation of collection_of_rigid_bodies.cpp:491-615
+    (blob repulsion summed to body force and torque, applied with a drag
+    mobility), with a linear repulsion and a periodic KD-tree for the pairs."""
+    from scipy.spatial import cKDTree
     ref = np.asarray(ref, dtype=np.float64).reshape(-1, 3)
     nb = len(ref)
-    cell = max(min_dist, 1e-9)
-    ncell = max(1, int(L // cell))
-    h = L / ncell
-    grid = {}
-    xs = np.zeros((M, 3))
-    qs = np.zeros((M, 4))
-    placed = 0
-    trials = 0
+    x = x.reshape(-1, 3).copy()
+    q = q.reshape(-1, 4).copy()
+    M = len(x)
+    body = np.repeat(np.arange(M), nb)
+    target = 1.02 * min_dist
+    for _ in range(max_iter):
+        R = rotation_matrices(q)
+        r = np.einsum("nij,mj->nmi", R, ref).reshape(-1, 3)
+        Y = (np.repeat(x, nb, axis=0) + r) % L
+        pairs = cKDTree(Y % L, boxsize=L).query_pairs(target, output_type="ndarray")
+        if len(pairs):
+            pairs = pairs[body[pairs[:, 0]] != body[pairs[:, 1]]]
+        if not len(pairs):
+            break
+        d = Y[pairs[:, 0]] - Y[pairs[:, 1]]
+        d -= L * np.round(d / L)
+        dist = np.linalg.norm(d, axis=1, keepdims=True)
+        if dist.min() >= min_dist:  # pushed towards `target`, done once clear of min_dist
+            break
+        f = (target - dist) * d / np.maximum(dist, 1e-12)
+        Fb = np.zeros_like(Y)
+        np.add.at(Fb, pairs[:, 0], f)
+        np.add.at(Fb, pairs[:, 1], -f)
+        Fbody = np.zeros((M, 3))
+        Tbody = np.zeros((M, 3))
+        np.add.at(Fbody, body, Fb)
+        np.add.at(Tbody, body, np.cross(r, Fb))
+        x = (x + 0.5 * Fbody / nb) % L
+        w = 0.5 * Tbody / (nb * max(1.0, float(np.mean(np.sum(ref ** 2, axis=1)))))
+        th = np.linalg.norm(w, axis=1)
+        ok = th > 1e-12
+        e = np.zeros((M, 4))
+        e[:, 0] = 1.0
+        e[ok, 0] = np.cos(0.5 * th[ok])
+        e[ok, 1:] = np.sin(0.5 * th[ok])[:, None] * w[ok] / th[ok, None]
+        s0, v0 = e[:, 0], e[:, 1:]
+        s1, v1 = q[:, 0], q[:, 1:]
+        q = np.concatenate([(s0 * s1 - np.sum(v0 * v1, axis=1))[:, None],
+                            s0[:, None] * v1 + s1[:, None] * v0 + np.cross(v0, v1)], axis=1)
+        q /= np.linalg.norm(q, axis=1, keepdims=True)
+    else:
+        raise RuntimeError("overlap relaxation did not converge")
+    return x.ravel(), q.ravel()
+
+
+def seed_bodies(rng, M, ref, L, min_dist=2.0 * A, max_trials=200000, max_fail=3000):
+    """Random non-overlapping placement by rejection sampling.  When the box is too
+    crowded for that (rods jam near volume fraction 0.2), place the bodies by
+    rejection in a box of 0.85x the target density and compress it to L in 1%
+    steps of the side, relaxing overlaps after each step."""
+    try:
+        return _rsa(rng, M, ref, L, min_dist, max_trials, max_fail)
+    except RuntimeError:
+        pass
+    L0 = L * (1.0 / 0.85) ** (1.0 / 3.0)
+    x, q = _rsa(rng, M, ref, L0, min_dist, max_trials, max_fail)
+    Lc = L0
+    while Lc > L:
+        Ln = max(L, Lc * 0.99)
+        x = (x * (Ln / Lc)) % Ln
+        x, q = relax_overlaps(x, q, ref, Ln, min_dist)
+        Lc = Ln
+    return x, q
+
+
+def _rsa(rng, M, ref, L, min_dist, max_trials=None, max_fail=None, batch=2048, max_empty=24):
+    """Random sequential addition, vectorised: batches of candidate bodies are
+    checked against the placed blobs with a periodic KD-tree, and accepted one by
+    one against the blobs accepted since the tree was built.  Raises when
+    max_empty consecutive batches add nothing (jammed)."""
+    from scipy.spatial import cKDTree
+    ref = np.asarray(ref, dtype=np.float64).reshape(-1, 3)
+    nb = len(ref)
+    xs, qs = [], []
+    placed_Y = np.zeros((0, 3))
     md2 = min_dist * min_dist
-    while placed < M:
-        trials += 1
-        if trials > max_trials:
-            raise RuntimeError("could not place %d bodies (placed %d)" % (M, placed))
-        x = rng.uniform(0.0, L, 3)
-        q = random_unit_quaternions(rng, 1)[0]
-        R = rotation_matrices(q[None])[0]
-        pos = (x[None, :] + ref @ R.T) % L
-        ok = True
-        for p in pos:
-            ci = (p // h).astype(int) % ncell
-            for dx in (-1, 0, 1):
-                for dy in (-1, 0, 1):
-                    for dz in (-1, 0, 1):
-                        key = ((ci[0] + dx) % ncell, (ci[1] + dy) % ncell, (ci[2] + dz) % ncell)
-                        for o in grid.get(key, ()):
-                            d = p - o
-                            d -= L * np.round(d / L)
-                            if d @ d < md2:
-                                ok = False
-                                break
-                        if not ok:
-                            break
-                    if not ok:
-                        break
-                if not ok:
-                    break
-            if not ok:
+    empty = 0
+    while len(xs) < M:
+        tree = cKDTree(placed_Y % L, boxsize=L) if len(placed_Y) else None
+        cx = rng.uniform(0.0, L, (batch, 3))
+        cq = random_unit_quaternions(rng, batch)
+        cY = ((cx[:, None, :] + np.einsum("nij,mj->nmi", rotation_matrices(cq), ref)) % L)
+        if tree is not None:
+            hit = tree.query_ball_point(cY.reshape(-1, 3), r=min_dist * (1.0 - 1e-12), return_length=True)
+            ok = ~(hit.reshape(batch, nb) > 0).any(axis=1)
+        else:
+            ok = np.ones(batch, dtype=bool)
+        recent = np.zeros((0, 3))
+        added = 0
+        for c in np.nonzero(ok)[0]:
+            if len(recent):
+                d = cY[c][:, None, :] - recent[None, :, :]
+                d -= L * np.round(d / L)
+                if (np.einsum("ijk,ijk->ij", d, d) < md2).any():
+                    continue
+            xs.append(cx[c])
+            qs.append(cq[c])
+            recent = np.concatenate([recent, cY[c]])
+            added += 1
+            if len(xs) == M or added >= 32:
                 break
-        if not ok:
-            continue
-        for p in pos:
-            ci = tuple((p // h).astype(int) % ncell)
-            grid.setdefault(ci, []).append(p)
-        xs[placed] = x
-        qs[placed] = q
-        placed += 1
-    return xs.ravel(), qs.ravel()
+        placed_Y = np.concatenate([placed_Y, recent])
+        empty = 0 if added else empty + 1
+        if empty >= max_empty:
+            raise RuntimeError("could not place %d bodies (placed %d)" % (M, len(xs)))
+    return np.array(xs).ravel(), np.array(qs).ravel()
 
 
 def rod_suspension(M, grid, L=None, phi=None, nb=6, seed=1234, gmres_tol=1e-10, gmres_max_iter=100,
@@ -132,3 +195,39 @@ def workload(name, **overrides):
     kw = dict(WORKLOADS[name])
     kw.update(overrides)
     return rod_suspension(**kw)
+
+
+def nearest_fft_size(n, lo=64, hi=128):
+    """Nearest 2^k or 3*2^k to n, clamped to [lo, hi]."""
+    cands = sorted({2 ** k for k in range(4, 12)} | {3 * 2 ** k for k in range(3, 11)})
+    best = min(cands, key=lambda c: (abs(c - n), c))
+    return int(min(max(best, lo), hi))
+
+
+def ensemble_member(i, seed0=0, nb=6, gmres_tol=1e-10, dt=0.01, precision=0, **kw):
+    """Instance i of the batched ensemble (seed seed0 + i): U[50, 500] rods of nb
+    blobs at volume fraction U[0.05, 0.20]; its grid is the 2^k or 3*2^k nearest
+    to L/(a/1.86), clamped to 64..128 points per side."""
+    rng = np.random.default_rng(seed0 + i)
+    M = int(rng.integers(50, 501))
+    phi = float(rng.uniform(0.05, 0.20))
+    L = box_for_volume_fraction(M * nb, phi)
+    grid = nearest_fft_size(1.86 * L / A)
+    p, ref, x, q, fe = rod_suspension(M=M, grid=grid, L=L, nb=nb, seed=seed0 + i, gmres_tol=gmres_tol, dt=dt,
+                                      precision=precision, **kw)
+    return p.as_dict(), ref, x, q, fe
+
+
+def ensemble(n_instances=64, seed0=0, workers=1, **kw):
+    """The batched ensemble (see ensemble_member), built in `workers` spawned
+    processes when workers > 1."""
+    import functools
+    f = functools.partial(ensemble_member, seed0=seed0, **kw)
+    if workers > 1:
+        import concurrent.futures as cf
+        import multiprocessing as mp
+        with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+            raw = list(ex.map(f, range(n_instances)))
+    else:
+        raw = [f(i) for i in range(n_instances)]
+    return [(FcmParams.defaults(**pd), ref, x, q, fe) for pd, ref, x, q, fe in raw]

@@ -22,7 +22,7 @@ namespace fcm {
 namespace {
 
 constexpr int TE = 8;    // tile edge
-constexpr int SCB = 16;  // blobs staged per chunk
+constexpr int SCB = 32;  // blobs staged per chunk
 
 __device__ __forceinline__ int wrap_index(int i, int n) {
   int r = i % n;
@@ -111,16 +111,45 @@ __global__ void k_tile_sort(const int* __restrict__ offset, int ntiles, unsigned
   }
 }
 
-// Tiled spreading: one CTA (128 threads) per 8x8x8 tile.  Thread t owns the
-// four points x = 4*xh..4*xh+3 of column (y, z), xh = t/64, y = (t/8)%8,
-// z = t%8; warp w covers x-half w/2 and y-half w%2, and skips blobs whose
-// stencil misses that 4x4x8 quarter (a warp-uniform branch).
+// Stage the weights of the blobs list[c0 .. c0+nc) restricted to this tile:
+// sw[k][d][i] = weight of grid coordinate O_d + i along d (zero outside the
+// stencil) and sflag[k] bit h = the blob reaches y-half h of the tile.  One
+// thread per (blob, dimension) copies its 8-weight window.
 template <typename T>
-__global__ void __launch_bounds__(128) k_spread_tiled(const int* __restrict__ base, const T* __restrict__ w,
-                                                      const double* __restrict__ F, TileGeom g,
-                                                      const int* __restrict__ offset,
-                                                      const unsigned* __restrict__ list, long long G,
-                                                      T* __restrict__ grid) {
+__device__ __forceinline__ void stage_weights(const unsigned* __restrict__ list, int c0, int nc,
+                                              const int* __restrict__ base, const T* __restrict__ w, const int O[3],
+                                              const int N[3], int W, T (*sw)[3][TE], int* sflag) {
+  for (int e = threadIdx.x; e < nc * 3; e += blockDim.x) {
+    const int k = e / 3, d = e - 3 * k;
+    const int b = (int)(list[c0 + k] >> 6);
+    const int Od = (d == 0) ? O[0] : ((d == 1) ? O[1] : O[2]);
+    const int Nd = (d == 0) ? N[0] : ((d == 1) ? N[1] : N[2]);
+    int s0 = (Od - base[3 * b + d]) % Nd;
+    if (s0 < 0) s0 += Nd;
+    const T* wb = w + (size_t)(3 * b + d) * W;
+    int fl = 0;
+#pragma unroll
+    for (int i = 0; i < TE; ++i) {
+      int si = s0 + i;
+      if (si >= Nd) si -= Nd;
+      const T v = (si < W) ? wb[si] : (T)0;
+      sw[k][d][i] = v;
+      if (v != (T)0) fl |= 1 << (i >> 2);
+    }
+    if (d == 1) sflag[k] = fl;
+  }
+}
+
+// Tiled spreading: one CTA (64 threads) per 8x8x8 tile.  Thread t owns the
+// x-column (y, z) = (t/8, t%8) of the tile, eight points with three components
+// accumulated in registers; warp h covers y-half h and skips blobs whose
+// stencil misses it (a warp-uniform branch).
+template <typename T>
+__global__ void __launch_bounds__(64) k_spread_tiled(const int* __restrict__ base, const T* __restrict__ w,
+                                                     const double* __restrict__ F, TileGeom g,
+                                                     const int* __restrict__ offset,
+                                                     const unsigned* __restrict__ list, long long G,
+                                                     T* __restrict__ grid) {
   __shared__ T sw[SCB][3][TE];
   __shared__ T sF[SCB][3];
   __shared__ int sflag[SCB];
@@ -129,134 +158,135 @@ __global__ void __launch_bounds__(128) k_spread_tiled(const int* __restrict__ ba
   const int O[3] = {tx * TE, ty * TE, tz * TE};
   const int N[3] = {g.nx, g.ny, g.nz};
   const int t = threadIdx.x;
-  const int z = t & 7, y = (t >> 3) & 7, xh = t >> 6, yh = (t >> 5) & 1;
-  T acc[4][3];
+  const int z = t & 7, y = t >> 3, yh = t >> 5;
+  T acc[TE][3];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int x = 0; x < TE; ++x)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) acc[i][c] = 0;
+    for (int c = 0; c < 3; ++c) acc[x][c] = 0;
   const int b0 = offset[tile], b1 = offset[tile + 1];
   for (int c0 = b0; c0 < b1; c0 += SCB) {
     const int nc = min(SCB, b1 - c0);
-    if (t < SCB) sflag[t] = 0;
-    __syncthreads();
-    for (int e = t; e < nc * 3 * TE; e += 128) {
-      const int k = e / (3 * TE), r = e - k * 3 * TE, d = r / TE, i = r - d * TE;
-      const int b = (int)(list[c0 + k] >> 6);
-      const int s = wrap_index(O[d] + i - base[3 * b + d], N[d]);
-      const T v = (s < g.W) ? w[(size_t)(3 * b + d) * g.W + s] : (T)0;
-      sw[k][d][i] = v;
-      if (d < 2 && v != (T)0) atomicOr(&sflag[k], 1 << (2 * d + (i >> 2)));
-    }
-    for (int e = t; e < nc * 3; e += 128) {
+    if (c0 != b0) __syncthreads();
+    stage_weights<T>(list, c0, nc, base, w, O, N, g.W, sw, sflag);
+    for (int e = t; e < nc * 3; e += 64) {
       const int k = e / 3, c = e - 3 * k;
       sF[k][c] = (T)F[3 * (size_t)(list[c0 + k] >> 6) + c];
     }
     __syncthreads();
     for (int k = 0; k < nc; ++k) {
-      const int fl = sflag[k];
-      if (!((fl >> xh) & 1) || !((fl >> (2 + yh)) & 1)) continue;
+      if (!((sflag[k] >> yh) & 1)) continue;
       const T wyz = sw[k][1][y] * sw[k][2][z];
       const T f0 = sF[k][0] * wyz, f1 = sF[k][1] * wyz, f2 = sF[k][2] * wyz;
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const T wx = sw[k][0][4 * xh + i];
-        acc[i][0] += f0 * wx;
-        acc[i][1] += f1 * wx;
-        acc[i][2] += f2 * wx;
+      for (int x = 0; x < TE; ++x) {
+        const T wx = sw[k][0][x];
+        acc[x][0] += f0 * wx;
+        acc[x][1] += f1 * wx;
+        acc[x][2] += f2 * wx;
       }
     }
-    __syncthreads();
   }
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const long long idx = ((long long)(O[0] + 4 * xh + i) * g.ny + (O[1] + y)) * g.nz + (O[2] + z);
-    grid[idx] = acc[i][0];
-    grid[G + idx] = acc[i][1];
-    grid[2 * G + idx] = acc[i][2];
+  for (int x = 0; x < TE; ++x) {
+    const long long idx = ((long long)(O[0] + x) * g.ny + (O[1] + y)) * g.nz + (O[2] + z);
+    grid[idx] = acc[x][0];
+    grid[G + idx] = acc[x][1];
+    grid[2 * G + idx] = acc[x][2];
   }
 }
 
-// Tiled interpolation: one CTA (two warps) per 8x8x8 tile.  The tile's three
-// velocity components are staged in shared memory (x-plane stride padded to 66
-// values so the four x-slabs a warp reads at once fall in distinct banks).  A
-// warp takes eight of the tile's blobs at a time; lane l serves blob l/4 and
-// x-slab l%4 (two x-planes), forms sum u * wx*wy*wz over its 128 points with the
-// blob's restricted weights held in registers, and the four slab partials are
-// combined with two shuffles.  The per-(blob, tile) partial goes to
-// partial[blob][j][3]; k_interp_reduce sums a blob's partials in j order, so
-// the result is deterministic and no atomics are used.
-constexpr int IPS = 66;  // padded x-plane stride of the staged tile
+// Sum of v[0..31] over the 32 lanes of a warp, scattered: afterwards lane l
+// holds in v[0] the warp total of value l (31 shuffles for 32 values).
+template <typename T>
+__device__ __forceinline__ T warp_reduce_scatter32(T v[32], int lane) {
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) {
+    const bool upper = (lane & off) != 0;
+#pragma unroll
+    for (int i = 0; i < off; ++i) {
+      const T send = upper ? v[i] : v[i + off];
+      const T keep = upper ? v[i + off] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+    }
+  }
+  return v[0];
+}
 
+// Tiled interpolation: one CTA (64 threads) per 8x8x8 tile.  Thread (y, z) =
+// (t/8, t%8) loads the eight points of its x-column (three components) into
+// registers once.  Blobs are taken eight at a time: each thread forms
+// wyz * sum_x wx * u for the blobs its warp's y-half meets, the warp reduces the
+// 8x(3+1) values with one scatter-reduction, the two warps' sums are added in
+// shared memory, and the per-(blob, tile) partial goes to partial[blob][j][3];
+// k_interp_reduce then sums a blob's partials in j order (deterministic, no
+// atomics).
 template <typename T>
 __global__ void __launch_bounds__(64) k_interp_tiled(const int* __restrict__ base, const T* __restrict__ w,
                                                      const T* __restrict__ grid, TileGeom g,
                                                      const int* __restrict__ offset,
                                                      const unsigned* __restrict__ list, long long G,
                                                      T* __restrict__ partial) {
-  __shared__ T su[3][TE * IPS];
+  __shared__ T sw[SCB][3][TE];
+  __shared__ int sflag[SCB];
+  __shared__ T sred[2][32];
   const int tile = blockIdx.x;
+  const int b0 = offset[tile], b1 = offset[tile + 1];
+  if (b0 == b1) return;  // no blob meets this tile (uniform over the CTA)
   const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
   const int O[3] = {tx * TE, ty * TE, tz * TE};
   const int N[3] = {g.nx, g.ny, g.nz};
   const int t = threadIdx.x;
-  const int b0 = offset[tile], b1 = offset[tile + 1];
-  if (b0 == b1) return;  // no blob meets this tile (uniform over the CTA)
-  for (int e = t; e < 3 * 512; e += 64) {
-    const int c = e >> 9, p = e & 511, x = p >> 6, yz = p & 63;
-    const long long idx = ((long long)(O[0] + x) * g.ny + (O[1] + (yz >> 3))) * g.nz + (O[2] + (yz & 7));
-    su[c][x * IPS + yz] = grid[c * G + idx];
+  const int z = t & 7, y = t >> 3, yh = t >> 5, lane = t & 31;
+  T u[TE][3];
+#pragma unroll
+  for (int x = 0; x < TE; ++x) {
+    const long long idx = ((long long)(O[0] + x) * g.ny + (O[1] + y)) * g.nz + (O[2] + z);
+    u[x][0] = grid[idx];
+    u[x][1] = grid[G + idx];
+    u[x][2] = grid[2 * G + idx];
   }
-  __syncthreads();
-  const int lane = t & 31, warp = t >> 5;
-  const int slab = lane & 3, kk = lane >> 2;
-  for (int g0 = b0 + 8 * warp; g0 < b1; g0 += 16) {
-    const int k = g0 + kk;
-    const bool active = k < b1;
-    unsigned v = active ? list[k] : 0u;
-    const int b = (int)(v >> 6);
-    T wy[TE], wz[TE], wx[2];
+  for (int c0 = b0; c0 < b1; c0 += SCB) {
+    const int nc = min(SCB, b1 - c0);
+    if (c0 != b0) __syncthreads();
+    stage_weights<T>(list, c0, nc, base, w, O, N, g.W, sw, sflag);
+    __syncthreads();
+    for (int k0 = 0; k0 < nc; k0 += 8) {
+      T v[32];
 #pragma unroll
-    for (int i = 0; i < TE; ++i) {
-      int s = wrap_index(O[1] + i - base[3 * b + 1], N[1]);
-      wy[i] = (active && s < g.W) ? w[(size_t)(3 * b + 1) * g.W + s] : (T)0;
-      s = wrap_index(O[2] + i - base[3 * b + 2], N[2]);
-      wz[i] = (active && s < g.W) ? w[(size_t)(3 * b + 2) * g.W + s] : (T)0;
-    }
+      for (int j = 0; j < 8; ++j) {
+        const int k = k0 + j;
+        T p0 = 0, p1 = 0, p2 = 0;
+        if (k < nc && ((sflag[k] >> yh) & 1)) {
+          T s0 = 0, s1 = 0, s2 = 0;
 #pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const int s = wrap_index(O[0] + 2 * slab + i - base[3 * b], N[0]);
-      wx[i] = (active && s < g.W) ? w[(size_t)(3 * b) * g.W + s] : (T)0;
-    }
-    T a0 = 0, a1 = 0, a2 = 0;
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const T* p0 = &su[0][(2 * slab + i) * IPS];
-      const T* p1 = &su[1][(2 * slab + i) * IPS];
-      const T* p2 = &su[2][(2 * slab + i) * IPS];
-#pragma unroll
-      for (int y = 0; y < TE; ++y) {
-        const T wxy = wx[i] * wy[y];
-#pragma unroll
-        for (int z = 0; z < TE; ++z) {
-          const T wt = wxy * wz[z];
-          a0 += p0[y * TE + z] * wt;
-          a1 += p1[y * TE + z] * wt;
-          a2 += p2[y * TE + z] * wt;
+          for (int x = 0; x < TE; ++x) {
+            const T wx = sw[k][0][x];
+            s0 += wx * u[x][0];
+            s1 += wx * u[x][1];
+            s2 += wx * u[x][2];
+          }
+          const T wyz = sw[k][1][y] * sw[k][2][z];
+          p0 = s0 * wyz;
+          p1 = s1 * wyz;
+          p2 = s2 * wyz;
+        }
+        v[4 * j] = p0;
+        v[4 * j + 1] = p1;
+        v[4 * j + 2] = p2;
+        v[4 * j + 3] = 0;
+      }
+      const T r = warp_reduce_scatter32<T>(v, lane);
+      sred[yh][lane] = r;
+      __syncthreads();
+      if (t < 32) {
+        const int j = t >> 2, c = t & 3, k = k0 + j;
+        if (c < 3 && k < nc) {
+          const unsigned e = list[c0 + k];
+          partial[((size_t)(e >> 6) * 64 + (e & 63u)) * 3 + c] = sred[0][t] + sred[1][t];
         }
       }
-    }
-#pragma unroll
-    for (int off = 1; off <= 2; off <<= 1) {
-      a0 += __shfl_xor_sync(0xffffffffu, a0, off);
-      a1 += __shfl_xor_sync(0xffffffffu, a1, off);
-      a2 += __shfl_xor_sync(0xffffffffu, a2, off);
-    }
-    if (active && slab == 0) {
-      T* o = partial + ((size_t)b * 64 + (v & 63u)) * 3;
-      o[0] = a0;
-      o[1] = a1;
-      o[2] = a2;
+      __syncthreads();
     }
   }
 }
@@ -431,7 +461,7 @@ int launch_set_up_gaussians(const Ctx& c, BlobTable<T>& t, const double* dY, cud
 template <typename T>
 int launch_spread(const Ctx& c, const BlobTable<T>& t, const double* dF, T* grid, cudaStream_t s) {
   if (t.tiled) {
-    k_spread_tiled<T><<<t.ntiles, 128, 0, s>>>(t.base, t.w, dF, tile_geom(c.g, t.W), t.tile_offset, t.tile_list,
+    k_spread_tiled<T><<<t.ntiles, 64, 0, s>>>(t.base, t.w, dF, tile_geom(c.g, t.W), t.tile_offset, t.tile_list,
                                                c.g.G, grid);
     FCM_LAUNCH_CHECK();
     return FCM_OK;

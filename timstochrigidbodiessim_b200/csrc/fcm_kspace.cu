@@ -97,7 +97,7 @@ __device__ __forceinline__ void load3(const C* spec, long long Gc, long long t, 
 
 // Deterministic projection in place (fcm_fluid_solver.cpp:642-695).
 template <typename T, typename C>
-__global__ void k_project(C* __restrict__ spec, KParams k) {
+__global__ void __launch_bounds__(256, 4) k_project(C* __restrict__ spec, KParams k) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= k.Gc) return;
   int x, y, kz;
