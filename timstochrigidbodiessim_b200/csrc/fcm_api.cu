@@ -17,7 +17,16 @@ namespace fcm {
 static thread_local std::string g_err;
 void set_error(const std::string& m) { g_err = m; }
 static std::atomic<long long> g_launches{0};
-void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+static thread_local long long t_launches = 0;  // this thread's launches (graph capture bookkeeping)
+void count_launch() {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  ++t_launches;
+}
+void count_launches(long long n) {
+  g_launches.fetch_add(n, std::memory_order_relaxed);
+  t_launches += n;
+}
+long long launch_count() { return t_launches; }
 
 namespace {
 bool dense_inv(const std::vector<double>& A, int n, std::vector<double>& out);
@@ -356,93 +365,81 @@ int saddle_matvec(Ctx* c, int prec, const double* in, double* out) {
   return FCM_OK;
 }
 
-// gmres_solver.cpp:148-306 (right preconditioning, MGS, Givens, no restarts)
-// on the device vector d_b; the solution is written to d_x.
+// One Arnoldi iteration of the device-side GMRES, captured once per precision
+// in a CUDA graph on the private capture stream:
+//   z_in = Q[k]; z = P^-1 z_in; w = A z; orthogonalise, normalise, Givens.
+int capture_iteration(Ctx* c, int prec) {
+  cudaGraphExec_t& ex = c->iter_graph[prec];
+  if (ex) return FCM_OK;
+  const cudaStream_t orig = c->stream;
+  c->stream = c->cap_stream;
+  FCM_TRY(set_stream_all(c));
+  int st = FCM_OK;
+  cudaGraph_t g = nullptr;
+  const long long l0 = launch_count();
+  cudaError_t e = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    do {
+      if ((st = gm_fetch(*c, c->d_sys_b, c->cap_stream)) != FCM_OK) break;
+      if ((st = launch_pinv(*c, c->d_qm, c->d_sys_b, c->d_sys_a, c->cap_stream)) != FCM_OK) break;
+      if ((st = saddle_matvec(c, prec, c->d_sys_a, c->d_sys_b)) != FCM_OK) break;
+      if ((st = gm_orthogonalize(*c, c->d_sys_b, c->cap_stream)) != FCM_OK) break;
+    } while (0);
+    const cudaError_t e2 = cudaStreamEndCapture(c->cap_stream, &g);
+    if (st == FCM_OK && e2 != cudaSuccess) {
+      set_error(std::string("GMRES iteration capture: ") + cudaGetErrorString(e2));
+      st = FCM_ERR_CUDA;
+    }
+  } else {
+    set_error(std::string("cudaStreamBeginCapture: ") + cudaGetErrorString(e));
+    st = FCM_ERR_CUDA;
+  }
+  // captured kernels are counted when the graph is launched, not here
+  c->iter_graph_kernels[prec] = launch_count() - l0;
+  count_launches(-(launch_count() - l0));
+  if (st == FCM_OK) {
+    e = cudaGraphInstantiate(&ex, g, 0);
+    if (e != cudaSuccess) {
+      set_error(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+      ex = nullptr;
+      st = FCM_ERR_CUDA;
+    }
+  }
+  if (g) cudaGraphDestroy(g);
+  cudaGetLastError();
+  c->stream = orig;
+  const int s2 = set_stream_all(c);
+  return st != FCM_OK ? st : s2;
+}
+
+// gmres_solver.cpp:148-306 (right preconditioning, Givens, no restarts) on the
+// device vector d_b; the solution is written to d_x.  The Krylov basis, the
+// Hessenberg matrix, the rotations and the convergence test stay on the device;
+// each iteration is one graph launch followed by a 32-byte state read.
 int gmres_dev(Ctx* c, int prec, const double* d_b, double* d_x, double tol, int maxit_req, int* iters_out,
               double* rel_out) {
   const long long n = c->nsys;
-  const int max_iter = std::min<long long>(n, std::min(maxit_req, c->maxit_alloc)) > 0
-                           ? (int)std::min<long long>(n, std::min(maxit_req, c->maxit_alloc))
-                           : 1;
-  double* Q = c->d_Qm;
-  auto Qc = [&](int i) { return Q + (size_t)i * n; };
-  double* hbuf = c->h_pinned;
-  FCM_TRY(blas_norm_sq_partial(*c, d_b, n, c->d_H, c->stream));
-  FCM_CUDA(cudaMemcpyAsync(hbuf, c->d_H, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  const int max_iter = (int)std::max<long long>(1, std::min<long long>(n, std::min(maxit_req, c->maxit_alloc)));
+  FCM_TRY(capture_iteration(c, prec));
+  FCM_TRY(gm_init(*c, d_b, tol, max_iter, c->stream));
+  FCM_CUDA(cudaMemcpyAsync(c->h_gm, c->gm, sizeof(GmState), cudaMemcpyDeviceToHost, c->stream));
   FCM_CUDA(cudaStreamSynchronize(c->stream));
-  const double norm_of_RHS = hbuf[0];
-  if (!(norm_of_RHS > 0.0)) {
-    FCM_CUDA(cudaMemsetAsync(d_x, 0, sizeof(double) * n, c->stream));
-    if (iters_out) *iters_out = 0;
-    if (rel_out) *rel_out = 0.0;
-    if (norm_of_RHS == 0.0) return FCM_OK;
-    set_error("non-finite right-hand side");
+  for (int it = 0; it < max_iter && !c->h_gm->done; ++it) {
+    FCM_CUDA(cudaGraphLaunch(c->iter_graph[prec], c->stream));
+    count_launches(c->iter_graph_kernels[prec]);
+    FCM_CUDA(cudaMemcpyAsync(c->h_gm, c->gm, sizeof(GmState), cudaMemcpyDeviceToHost, c->stream));
+    FCM_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  const GmState g = *c->h_gm;
+  if (iters_out) *iters_out = g.k;
+  if (rel_out) *rel_out = g.rel;
+  if (g.status == FCM_ERR_NONFINITE) {
+    set_error(g.k == 0 ? "non-finite right-hand side" : "GMRES residual became non-finite");
     return FCM_ERR_NONFINITE;
   }
-  FCM_TRY(blas_copy_scaled(Qc(0), d_b, c->d_H, 1, n, c->stream));
-  const int hn = max_iter + 1;
-  std::vector<double> H((size_t)hn * hn, 0.0), beta(hn, 0.0), CS(max_iter, 0.0), SN(max_iter, 0.0);
-  auto Hm = [&](int i, int j) -> double& { return H[(size_t)j * hn + i]; };
-  beta[0] = norm_of_RHS;
-  double* z = c->d_sys_a;
-  for (int iter = 1; iter <= max_iter; ++iter) {
-    FCM_TRY(launch_pinv(*c, c->d_qm, Qc(iter - 1), z, c->stream));
-    FCM_TRY(saddle_matvec(c, prec, z, Qc(iter)));
-    for (int i = 0; i < iter; ++i)
-      FCM_TRY(blas_mgs_step(*c, Qc(iter), i > 0 ? Qc(i - 1) : nullptr, i > 0 ? c->d_H + (i - 1) : nullptr, Qc(i),
-                            n, c->d_H + i, c->stream));
-    FCM_TRY(blas_mgs_step(*c, Qc(iter), Qc(iter - 1), c->d_H + (iter - 1), nullptr, n, c->d_H + iter, c->stream));
-    FCM_TRY(blas_scale(Qc(iter), c->d_H + iter, 1, n, c->stream));
-    FCM_CUDA(cudaMemcpyAsync(hbuf, c->d_H, sizeof(double) * (iter + 1), cudaMemcpyDeviceToHost, c->stream));
-    FCM_CUDA(cudaStreamSynchronize(c->stream));
-    for (int i = 0; i <= iter; ++i) Hm(i, iter - 1) = hbuf[i];
-    for (int i = 1; i < iter; i++) {
-      const double temp = CS[i - 1] * Hm(i - 1, iter - 1) + SN[i - 1] * Hm(i, iter - 1);
-      Hm(i, iter - 1) = CS[i - 1] * Hm(i, iter - 1) - SN[i - 1] * Hm(i - 1, iter - 1);
-      Hm(i - 1, iter - 1) = temp;
-    }
-    if (Hm(iter, iter - 1) == 0.0) {
-      CS[iter - 1] = 1.0;
-      SN[iter - 1] = 0.0;
-    } else if (std::fabs(Hm(iter, iter - 1)) > std::fabs(Hm(iter - 1, iter - 1))) {
-      const double temp = Hm(iter - 1, iter - 1) / Hm(iter, iter - 1);
-      SN[iter - 1] = (2.0 * double(Hm(iter, iter - 1) > 0) - 1.0) / std::sqrt(1.0 + temp * temp);
-      CS[iter - 1] = temp * SN[iter - 1];
-    } else {
-      const double temp = Hm(iter, iter - 1) / Hm(iter - 1, iter - 1);
-      CS[iter - 1] = (2.0 * double(Hm(iter - 1, iter - 1) > 0) - 1.0) / std::sqrt(1.0 + temp * temp);
-      SN[iter - 1] = temp * CS[iter - 1];
-    }
-    Hm(iter - 1, iter - 1) = CS[iter - 1] * Hm(iter - 1, iter - 1) + SN[iter - 1] * Hm(iter, iter - 1);
-    Hm(iter, iter - 1) = 0.0;
-    beta[iter] = -SN[iter - 1] * beta[iter - 1];
-    beta[iter - 1] = CS[iter - 1] * beta[iter - 1];
-    const double relative_error = std::fabs(beta[iter]) / norm_of_RHS;
-    if (!std::isfinite(relative_error)) {
-      set_error("GMRES residual became non-finite");
-      if (iters_out) *iters_out = iter;
-      if (rel_out) *rel_out = relative_error;
-      return FCM_ERR_NONFINITE;
-    }
-    if (relative_error < tol || iter == max_iter) {
-      std::vector<double> y(iter, 0.0);
-      y[iter - 1] = beta[iter - 1] / Hm(iter - 1, iter - 1);
-      for (int i = iter - 2; i >= 0; i--) {
-        y[i] = beta[i];
-        for (int j = iter - 1; j > i; j--) y[i] -= Hm(i, j) * y[j];
-        y[i] /= Hm(i, i);
-      }
-      for (int i = 0; i < iter; ++i) hbuf[i] = y[i];
-      FCM_CUDA(cudaMemcpyAsync(c->d_y, hbuf, sizeof(double) * iter, cudaMemcpyHostToDevice, c->stream));
-      FCM_TRY(blas_combine(c->d_sys_b, Q, c->d_y, iter, n, c->stream));
-      FCM_TRY(launch_pinv(*c, c->d_qm, c->d_sys_b, d_x, c->stream));
-      FCM_CUDA(cudaStreamSynchronize(c->stream));  // hbuf is reused by the caller
-      if (iters_out) *iters_out = iter;
-      if (rel_out) *rel_out = relative_error;
-      return relative_error < tol ? FCM_OK : FCM_ERR_NOT_CONVERGED;
-    }
-  }
-  return FCM_ERR_STATE;
+  FCM_TRY(gm_finish(*c, c->d_sys_b, c->stream));
+  FCM_TRY(launch_pinv(*c, c->d_qm, c->d_sys_b, d_x, c->stream));
+  return g.status;
 }
 
 // Saddle-point solve of d_rhs into d_soln.  precision 0: one GMRES; precision 1:
@@ -704,6 +701,14 @@ void destroy_ctx(Ctx* c) {
                     c->d_KTKinv, c->d_Qm, c->d_H, c->d_y, c->d_partials, c->d_stress};
   for (double* p : ptrs) cudaFree(p);
   cudaFree(c->d_counter);
+  for (int i = 0; i < 2; ++i)
+    if (c->iter_graph[i]) cudaGraphExecDestroy(c->iter_graph[i]);
+  cudaFree(c->gm);
+  double* gptrs[] = {c->d_Hd, c->d_beta, c->d_CS, c->d_SN, c->d_hA, c->d_hB, c->d_hnorm, c->d_mdpart};
+  for (double* p : gptrs) cudaFree(p);
+  cudaFree(c->d_mdcount);
+  if (c->h_gm) cudaFreeHost(c->h_gm);
+  if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   cudaFree(c->d_cell);
   cudaFree(c->d_cell_start);
   cudaFree(c->d_cell_count);
@@ -767,6 +772,22 @@ int create_ctx(const fcm_params* p, const double* ref, Ctx** out) {
       (st = dev_alloc(&c->d_H, (size_t)c->maxit_alloc + 4)) || (st = dev_alloc(&c->d_y, (size_t)c->maxit_alloc + 1)))
     return fail(st);
   c->red_blocks = (int)std::max<long long>(1, std::min<long long>(296, (n + 1023) / 1024));
+  c->md_blocks = (int)std::max<long long>(1, std::min<long long>(148, (n + 2047) / 2048));
+  {
+    const size_t hn = (size_t)c->maxit_alloc + 1;
+    if ((st = dev_alloc(&c->gm, 1)) || (st = dev_alloc(&c->d_Hd, hn * hn)) || (st = dev_alloc(&c->d_beta, hn)) ||
+        (st = dev_alloc(&c->d_CS, hn)) || (st = dev_alloc(&c->d_SN, hn)) || (st = dev_alloc(&c->d_hA, hn)) ||
+        (st = dev_alloc(&c->d_hB, hn)) || (st = dev_alloc(&c->d_hnorm, 1)) ||
+        (st = dev_alloc(&c->d_mdpart, hn * c->md_blocks)) || (st = dev_alloc(&c->d_mdcount, hn)))
+      return fail(st);
+    if (cudaMemset(c->d_mdcount, 0, sizeof(unsigned int) * hn) != cudaSuccess ||
+        cudaMemset(c->d_Hd, 0, sizeof(double) * hn * hn) != cudaSuccess ||
+        cudaMallocHost(&c->h_gm, sizeof(GmState)) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      set_error("GMRES state allocation failed");
+      return fail(FCM_ERR_NOMEM);
+    }
+  }
   if ((st = dev_alloc(&c->d_partials, (size_t)c->red_blocks)) ||
       (st = dev_alloc(&c->d_counter, 1)))
     return fail(st);

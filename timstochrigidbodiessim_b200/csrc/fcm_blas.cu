@@ -184,3 +184,217 @@ int blas_f64_to_f32(float* dst, const double* src, long long n, cudaStream_t s) 
 }
 
 }  // namespace fcm
+
+// ============================================================ device-side GMRES
+// The Arnoldi/Givens process of gmres_solver.cpp:193-306 kept on the device, so
+// one iteration is a fixed sequence of kernels (captured once in a CUDA graph):
+//   z_in = Q[k]; z = P^-1 z_in; w = A z                       (caller)
+//   h  = Q[0..k]^T w, w -= Q h   twice (classical Gram-Schmidt with one
+//        re-orthogonalisation, the same projections as the reference's modified
+//        Gram-Schmidt in exact arithmetic)
+//   Q[k+1] = w / |w|; Givens rotations, residual, convergence   (one thread)
+// k, the rotations, beta and the Hessenberg matrix live in device memory.
+namespace fcm {
+namespace {
+
+constexpr int MDT = 256;
+
+__global__ void k_gm_fetch(const GmState* __restrict__ st, const double* __restrict__ Q, long long n,
+                           double* __restrict__ dst) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n || st->done) return;
+  dst[t] = Q[(size_t)st->k * n + t];
+}
+
+// h[i] = Q[:, i] . w for i <= k; grid (nblk, maxcols); deterministic two-level sum
+// (one partial per block and column, the last block of a column adds them in order).
+__global__ void __launch_bounds__(MDT) k_multidot(const GmState* __restrict__ st, const double* __restrict__ Q,
+                                                  const double* __restrict__ w, long long n,
+                                                  double* __restrict__ partials, unsigned int* __restrict__ counters,
+                                                  double* __restrict__ h) {
+  __shared__ double sh[MDT / 32];
+  __shared__ bool last;
+  const int col = blockIdx.y;
+  if (st->done || col > st->k) return;
+  const double* q = Q + (size_t)col * n;
+  double s = 0.0;
+  for (long long i = blockIdx.x * (long long)MDT + threadIdx.x; i < n; i += (long long)gridDim.x * MDT)
+    s += q[i] * w[i];
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double b = 0.0;
+    for (int i = 0; i < MDT / 32; ++i) b += sh[i];
+    partials[(size_t)col * gridDim.x + blockIdx.x] = b;
+    __threadfence();
+    last = (atomicAdd(counters + col, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    const volatile double* p = partials + (size_t)col * gridDim.x;
+    for (unsigned int b = 0; b < gridDim.x; ++b) tot += p[b];
+    h[col] = tot;
+    counters[col] = 0u;
+  }
+}
+
+// w -= sum_{i<=k} h[i] Q[:, i]
+__global__ void k_gs_update(const GmState* __restrict__ st, const double* __restrict__ Q,
+                            const double* __restrict__ h, long long n, double* __restrict__ w) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n || st->done) return;
+  const int k = st->k;
+  double v = w[t];
+  for (int i = 0; i <= k; ++i) v -= h[i] * Q[(size_t)i * n + t];
+  w[t] = v;
+}
+
+// Q[k+1] = w / |w| (|w| = 0: a happy breakdown, the column is left as w)
+__global__ void k_gm_normalize(const GmState* __restrict__ st, const double* __restrict__ w,
+                               const double* __restrict__ hnorm, long long n, double* __restrict__ Q) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n || st->done) return;
+  const double s = *hnorm;
+  Q[(size_t)(st->k + 1) * n + t] = (s != 0.0) ? w[t] / s : w[t];
+}
+
+// gmres_solver.cpp:248-300 for column k+1 (one thread).
+__global__ void k_gm_givens(GmState* st, double* __restrict__ H, int hn, double* __restrict__ beta,
+                            double* __restrict__ CS, double* __restrict__ SN, const double* __restrict__ hA,
+                            const double* __restrict__ hB, const double* __restrict__ hnorm) {
+  if (threadIdx.x != 0 || blockIdx.x != 0 || st->done) return;
+  const int iter = st->k + 1;
+  double* col = H + (size_t)(iter - 1) * hn;
+  for (int i = 0; i < iter; ++i) col[i] = hA[i] + hB[i];
+  col[iter] = *hnorm;
+  for (int i = 1; i < iter; i++) {
+    const double temp = CS[i - 1] * col[i - 1] + SN[i - 1] * col[i];
+    col[i] = CS[i - 1] * col[i] - SN[i - 1] * col[i - 1];
+    col[i - 1] = temp;
+  }
+  const double a = col[iter - 1], b = col[iter];
+  if (b == 0.0) {
+    CS[iter - 1] = 1.0;
+    SN[iter - 1] = 0.0;
+  } else if (fabs(b) > fabs(a)) {
+    const double temp = a / b;
+    SN[iter - 1] = (2.0 * double(b > 0) - 1.0) / sqrt(1.0 + temp * temp);
+    CS[iter - 1] = temp * SN[iter - 1];
+  } else {
+    const double temp = b / a;
+    CS[iter - 1] = (2.0 * double(a > 0) - 1.0) / sqrt(1.0 + temp * temp);
+    SN[iter - 1] = temp * CS[iter - 1];
+  }
+  col[iter - 1] = CS[iter - 1] * a + SN[iter - 1] * b;
+  col[iter] = 0.0;
+  beta[iter] = -SN[iter - 1] * beta[iter - 1];
+  beta[iter - 1] = CS[iter - 1] * beta[iter - 1];
+  const double rel = fabs(beta[iter]) / st->normb;
+  st->k = iter;
+  st->rel = rel;
+  if (!isfinite(rel)) {
+    st->done = 1;
+    st->status = FCM_ERR_NONFINITE;
+  } else if (rel < st->tol || iter >= st->maxit) {
+    st->done = 1;
+    st->status = rel < st->tol ? FCM_OK : FCM_ERR_NOT_CONVERGED;
+  }
+}
+
+// beta[0] = |b|, k = 0 (one thread); |b| == 0 or non-finite ends the solve.
+__global__ void k_gm_init(GmState* st, const double* __restrict__ normb, double* __restrict__ beta, double tol,
+                          int maxit) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double nb = *normb;
+  st->k = 0;
+  st->tol = tol;
+  st->maxit = maxit;
+  st->normb = nb;
+  st->rel = 0.0;
+  beta[0] = nb;
+  if (nb > 0.0 && isfinite(nb)) {
+    st->done = 0;
+    st->status = FCM_OK;
+  } else {
+    st->done = 1;
+    st->status = (nb == 0.0) ? FCM_OK : FCM_ERR_NONFINITE;
+  }
+}
+
+// y = R^-1 beta (gmres_solver.cpp:302-318), one thread; k = 0 gives y = 0.
+__global__ void k_gm_backsub(const GmState* __restrict__ st, const double* __restrict__ H, int hn,
+                             const double* __restrict__ beta, double* __restrict__ y) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int iter = st->k;
+  if (iter == 0) return;
+  auto Hm = [&](int i, int j) { return H[(size_t)j * hn + i]; };
+  y[iter - 1] = beta[iter - 1] / Hm(iter - 1, iter - 1);
+  for (int i = iter - 2; i >= 0; i--) {
+    double v = beta[i];
+    for (int j = iter - 1; j > i; j--) v -= Hm(i, j) * y[j];
+    y[i] = v / Hm(i, i);
+  }
+}
+
+// soln = sum_{i<k} y_i Q[:, i] (gmres_solver.cpp:320-326), k from the state.
+__global__ void k_gm_combine(const GmState* __restrict__ st, const double* __restrict__ Q,
+                             const double* __restrict__ y, long long n, double* __restrict__ out) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int k = st->k;
+  double s = 0.0;
+  for (int i = 0; i < k; ++i) s += y[i] * Q[(size_t)i * n + t];
+  out[t] = s;
+}
+
+}  // namespace
+
+int gm_fetch(const Ctx& c, double* dst, cudaStream_t s) {
+  const long long n = c.nsys;
+  k_gm_fetch<<<nblk(n, 256), 256, 0, s>>>(c.gm, c.d_Qm, n, dst);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+int gm_orthogonalize(const Ctx& c, double* w, cudaStream_t s) {
+  const long long n = c.nsys;
+  const dim3 grid(c.md_blocks, c.maxit_alloc + 1);
+  double* hab[2] = {c.d_hA, c.d_hB};
+  for (int pass = 0; pass < 2; ++pass) {
+    k_multidot<<<grid, MDT, 0, s>>>(c.gm, c.d_Qm, w, n, c.d_mdpart, c.d_mdcount, hab[pass]);
+    FCM_LAUNCH_CHECK();
+    k_gs_update<<<nblk(n, 256), 256, 0, s>>>(c.gm, c.d_Qm, hab[pass], n, w);
+    FCM_LAUNCH_CHECK();
+  }
+  FCM_TRY(blas_norm_sq_partial(c, w, n, c.d_hnorm, s));
+  k_gm_normalize<<<nblk(n, 256), 256, 0, s>>>(c.gm, w, c.d_hnorm, n, c.d_Qm);
+  FCM_LAUNCH_CHECK();
+  k_gm_givens<<<1, 32, 0, s>>>(c.gm, c.d_Hd, c.maxit_alloc + 1, c.d_beta, c.d_CS, c.d_SN, c.d_hA, c.d_hB,
+                               c.d_hnorm);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+int gm_init(const Ctx& c, const double* b, double tol, int maxit, cudaStream_t s) {
+  const long long n = c.nsys;
+  FCM_TRY(blas_norm_sq_partial(c, b, n, c.d_hnorm, s));
+  k_gm_init<<<1, 32, 0, s>>>(c.gm, c.d_hnorm, c.d_beta, tol, maxit);
+  FCM_LAUNCH_CHECK();
+  FCM_TRY(blas_copy_scaled(c.d_Qm, b, c.d_hnorm, 1, n, s));
+  return FCM_OK;
+}
+
+int gm_finish(const Ctx& c, double* soln_pre, cudaStream_t s) {
+  const long long n = c.nsys;
+  k_gm_backsub<<<1, 32, 0, s>>>(c.gm, c.d_Hd, c.maxit_alloc + 1, c.d_beta, c.d_y);
+  FCM_LAUNCH_CHECK();
+  k_gm_combine<<<nblk(n, 256), 256, 0, s>>>(c.gm, c.d_Qm, c.d_y, n, soln_pre);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+}  // namespace fcm

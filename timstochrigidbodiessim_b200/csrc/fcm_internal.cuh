@@ -51,6 +51,8 @@ struct Status {
   } while (0)
 
 void count_launch();
+void count_launches(long long n);
+long long launch_count();
 
 #define FCM_LAUNCH_CHECK()                                                      \
   do {                                                                          \
@@ -117,6 +119,15 @@ struct GridBufs {
 // Tile shape of the tiled spread / interpolation kernels.
 constexpr int TILE_X = 8, TILE_Y = 8, TILE_Z = 8;
 
+// Device-resident state of one GMRES solve (gmres_solver.cpp:148-306).
+struct GmState {
+  int k;        // Arnoldi columns completed (the reference's `iter`)
+  int done;     // 1 once converged, out of iterations or non-finite
+  int status;   // FCM_OK / FCM_ERR_NOT_CONVERGED / FCM_ERR_NONFINITE
+  int maxit;
+  double normb, rel, tol;
+};
+
 // ------------------------------------------------------------------ context
 struct Ctx {
   fcm_params p;
@@ -153,6 +164,17 @@ struct Ctx {
   int red_blocks = 0;
   int maxit_alloc = 0;
   double* h_pinned = nullptr;  // small pinned host staging (>= 256 doubles)
+  // device-side GMRES
+  GmState* gm = nullptr;        // device state
+  GmState* h_gm = nullptr;      // pinned host copy
+  double *d_Hd = nullptr, *d_beta = nullptr, *d_CS = nullptr, *d_SN = nullptr;
+  double *d_hA = nullptr, *d_hB = nullptr, *d_hnorm = nullptr;
+  double* d_mdpart = nullptr;   // multidot partials [(maxit+1) * md_blocks]
+  unsigned int* d_mdcount = nullptr;
+  int md_blocks = 0;
+  cudaStream_t cap_stream = 0;  // private stream for graph capture
+  cudaGraphExec_t iter_graph[2] = {nullptr, nullptr};  // one Arnoldi iteration, per precision
+  long long iter_graph_kernels[2] = {0, 0};           // kernels in each graph
   // cells
   int ncell_total = 0;
   int *d_cell = nullptr, *d_cell_start = nullptr, *d_cell_count = nullptr, *d_cell_sorted = nullptr, *d_cell_cursor = nullptr;
@@ -216,6 +238,11 @@ int blas_copy_scaled(double* dst, const double* src, const double* d_num, int in
 int blas_norm_sq_partial(const Ctx& c, const double* a, long long n, double* d_out, cudaStream_t s);
 int blas_f64_to_f32(float* dst, const double* src, long long n, cudaStream_t s);
 int blas_sum_accumulate(const Ctx& c, const double* a, long long n, double* d_out, cudaStream_t s);
+// device-side GMRES pieces (fcm_blas.cu)
+int gm_init(const Ctx& c, const double* b, double tol, int maxit, cudaStream_t s);
+int gm_fetch(const Ctx& c, double* dst, cudaStream_t s);
+int gm_orthogonalize(const Ctx& c, double* w, cudaStream_t s);
+int gm_finish(const Ctx& c, double* soln_pre, cudaStream_t s);
 
 // symmetric inverse: inv() when well conditioned, otherwise the pseudo-inverse
 // (fcm_linalg.cpp)
