@@ -88,6 +88,9 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 5.0:  # first sample before the timed region
+                time.sleep(0.01)
         except Exception:
             self.proc = None
 
@@ -131,45 +134,57 @@ def setup_suspension(p, ref, x, q, fe, stream):
     return s
 
 
-def timed_steps(s, K, seed, start_index, stream):
+def run_step(s, seed, index, mode):
+    """One step: host-driven (fcm_step) or device-resident (fcm_step_async + wait)."""
+    if mode == "graph":
+        s.step_async(seed, index)
+        return s.step_wait()
+    return s.step(seed, index)
+
+
+def timed_steps(s, K, seed, start_index, stream, mode="host"):
     import torch
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     iters = []
     e0.record(stream)
     for i in range(K):
-        st, info = s.step(seed, start_index + i)
+        st, info = run_step(s, seed, start_index + i, mode)
         iters.append(info.gmres_iters)
     e1.record(stream)
     e1.synchronize()
     return e0.elapsed_time(e1) / 1e3, iters
 
 
-def kernel_roofline(s, p, stream, reps=20):
-    """Per-launch durations of the FP64 spread and interpolation, CUDA events on
-    the context's stream; algorithmic bytes 3*G*8 + 6*Nb*8 per launch."""
+def kernel_roofline(s, p, stream, precision, reps=20):
+    """Per-launch durations of the spread and the interpolation on the grid of one
+    precision (0 FP64, 1 FP32), CUDA events on the context's stream around the
+    stage calls fcm_spread / fcm_interp (device F and V, no copies inside);
+    algorithmic bytes 3*G*s + 6*Nb*s per launch (s = 8 or 4)."""
     import torch
     Nb = p.num_blobs
     F = torch.randn(3 * Nb, dtype=torch.float64, device="cuda")
+    V = torch.empty(3 * Nb, dtype=torch.float64, device="cuda")
     s.fill_all_blob_pos()
     s.set_up_gaussians()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
     for _ in range(3):
-        s.set_up_force_distribution(F)
-        s.calculate_deterministic_blob_velocities(out=torch.empty(3 * Nb, dtype=torch.float64, device="cuda"))
+        s.spread(F, precision)
+        s.interp(precision, out=V)
     torch.cuda.synchronize()
     ts, ti = [], []
     for _ in range(reps):
         ev[0].record(stream)
-        s.set_up_force_distribution(F)
+        s.spread(F, precision)
         ev[1].record(stream)
-        s.L.fcm_calculate_deterministic_blob_velocities(s.h, None)
+        s.interp(precision, out=V)
         ev[2].record(stream)
         ev[2].synchronize()
         ts.append(ev[0].elapsed_time(ev[1]) / 1e3)
         ti.append(ev[1].elapsed_time(ev[2]) / 1e3)
     G = p.nx * p.ny * p.nz
-    bytes_ = 3 * G * 8 + 6 * Nb * 8
+    sz = 8 if precision == 0 else 4
+    bytes_ = 3 * G * sz + 6 * Nb * sz
     return bytes_, float(np.mean(ts)), float(np.mean(ti))
 
 
@@ -243,13 +258,13 @@ def run_ours(args):
     seed = 1234 + rank
     p, ref, x, q, fe = configs.rod_suspension(**wl, seed=seed, algorithm=algorithm)
     results = {}
-    for tag, prec in (("fp64", 0), ("mixed", 1)):
+    for tag, prec, mode in (("fp64", 0, "host"), ("fp64_graph", 0, "graph"), ("mixed", 1, "graph")):
         pp = p.copy(precision=prec)
         if prec == 1:
             pp.gmres_tol = MIXED_TOL
         s = setup_suspension(pp, ref, x, q, fe, stream)
         for i in range(args.warmup):
-            s.step(seed, i)
+            run_step(s, seed, i, mode)
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
@@ -257,7 +272,7 @@ def run_ours(args):
         if tag == "mixed":
             sampler.start()
         l0 = lib.fcm_kernel_launch_count()
-        t, iters = timed_steps(s, args.steps, seed, args.warmup, stream)
+        t, iters = timed_steps(s, args.steps, seed, args.warmup, stream, mode)
         l1 = lib.fcm_kernel_launch_count()
         clocks = sampler.stop() if tag == "mixed" else None
         torch.cuda.synchronize()
@@ -265,9 +280,10 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
         results[tag] = dict(t=t, iters=float(np.mean(iters)), launches=l1 - l0, clocks=clocks, s=s)
-    # roofline of the FP64 spread / interpolation kernels (the FP64 context)
-    s64 = results["fp64"]["s"]
-    bytes_, t_spread, t_interp = kernel_roofline(s64, p, stream)
+    # rooflines of the spread / interpolation kernels on the FP32 grid (the mixed
+    # path's) and the FP64 grid
+    kr = {"fp32": kernel_roofline(results["mixed"]["s"], p, stream, 1),
+          "fp64": kernel_roofline(results["fp64"]["s"], p, stream, 0)}
     # end to end through the C-ABI with host buffers: H2D bodies, step, D2H bodies
     sm = results["mixed"]["s"]
     xs, qs = sm.get_bodies()
@@ -277,7 +293,7 @@ def run_ours(args):
     e0.record(stream)
     for i in range(K2):
         sm.set_bodies(xs, qs)
-        sm.step(seed, 10000 + i)
+        run_step(sm, seed, 10000 + i, "graph")
         xs, qs = sm.get_bodies()
     e1.record(stream)
     e1.synchronize()
@@ -295,9 +311,15 @@ def run_ours(args):
     M, K = p.num_bodies, args.steps
     value = replica_throughput(M, K, world, results["mixed"]["t"])
     fp64_value = replica_throughput(M, K, world, results["fp64"]["t"])
+    fp64g_value = replica_throughput(M, K, world, results["fp64_graph"]["t"])
     if rank == 0:
-        ach_s = bytes_ / t_spread / 1e9
-        ach_i = bytes_ / t_interp / 1e9
+        kernels = []
+        for tag in ("fp32", "fp64"):
+            bytes_, t_spread, t_interp = kr[tag]
+            for name, t_k in (("spread", t_spread), ("interp", t_interp)):
+                ach = bytes_ / t_k / 1e9
+                kernels.append({"kernel": "fcm %s (%s)" % (name, tag), "bytes_per_launch": bytes_,
+                                "ms_per_launch": 1e3 * t_k, "achieved": ach, "frac": ach / hbm})
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             cpu = cpu_baseline(p, ref, x, q, fe, results["fp64"]["iters"])
@@ -325,16 +347,17 @@ def run_ours(args):
                        "gmres_tol": p.gmres_tol, "parallelism": "replicas x%d" % world,
                        "l2": "grid fields (3x%d^3) exceed L2; no flush needed" % p.nx},
             "fp64": {"value": fp64_value, "ms_per_step": 1e3 * results["fp64"]["t"] / K,
-                     "gmres_iters": results["fp64"]["iters"]},
+                     "gmres_iters": results["fp64"]["iters"], "mode": "host-driven fcm_step"},
+            "fp64_graph": {"value": fp64g_value, "ms_per_step": 1e3 * results["fp64_graph"]["t"] / K,
+                           "mode": "device-resident graph steps"},
             "mixed_over_fp64": value / fp64_value,
+            "mixed_over_fp64_graph": value / fp64g_value,
             "gmres_iters_mixed": results["mixed"]["iters"],
             "mixed_gmres_tol": MIXED_TOL,
             "rel_vel_error_mixed_vs_fp64": {"bodies": err_U, "blobs": err_l},
-            "roofline": {"kernel": "fcm spread (fp64)", "bound": "hbm", "achieved": ach_s, "peak": hbm,
-                         "unit": "GB/s", "frac": ach_s / hbm, "traffic": traffic,
-                         "bytes_per_launch": bytes_, "ms_per_launch": 1e3 * t_spread, "peak_source": peak_src},
-            "roofline_interp": {"kernel": "fcm interp (fp64)", "achieved": ach_i, "frac": ach_i / hbm,
-                                "ms_per_launch": 1e3 * t_interp},
+            "roofline": dict(kernels[0], bound="hbm", peak=hbm, unit="GB/s", traffic=traffic,
+                             peak_source=peak_src),
+            "roofline_kernels": kernels,
             "cpu_baseline": cpu,
             "e2e": {"value": replica_throughput(M, K2, world, t_e2e), "unit": UNIT, "h2d_bytes_per_step": 7 * 8 * M,
                     "d2h_bytes_per_step": 7 * 8 * M},
@@ -416,78 +439,93 @@ def run_kernels_only(args):
         F = torch.randn(3 * p.num_blobs, dtype=torch.float64, device="cuda")
         V = torch.empty_like(F)
         for _ in range(args.kernels_only):
-            if prec == 0:
-                s.set_up_force_distribution(F)
-                s.produce_deterministic_velocity_field()
-                s.calculate_deterministic_blob_velocities(out=V)
-            else:
-                s.apply_mobility(F, out=V)
+            s.spread(F, prec)
+            s.stokes_solve(prec)
+            s.interp(prec, out=V)
         torch.cuda.synchronize()
         s.close()
     print(json.dumps({"kernels_only": args.kernels_only, "workload": args.workload}))
 
 
 def run_ensemble(args):
-    """Batched ensemble of 64 independent suspensions.  Plain FP64 GPU path: the
-    instances one after another on one stream.  Mixed-precision batched path: all
-    instances at once, each on its own CUDA stream driven by its own host thread
-    (the library releases the interpreter lock), so their kernels overlap on the
-    GPU.  Device time: events on a root stream that every instance stream joins."""
-    import concurrent.futures as cf
-
+    """Batched ensemble of 64 independent suspensions (seeds 0..63).  Plain FP64
+    GPU path: the instances one after another on one stream, host-driven steps
+    (fcm_step).  Also timed, for reference: the same FP64 instances with
+    device-resident (graph) steps, still one after another.  Mixed-precision
+    batched path: every instance on its own CUDA stream, one step of all of them
+    per fcm_step_many call (one CUDA-graph launch per instance, the GMRES loops on
+    the device), so their kernels overlap on the GPU.  Device time: events on a
+    root stream that every instance stream joins."""
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")  # streams -> hardware queues
     from timstochrigidbodiessim_b200 import configs
     insts = configs.ensemble(64, workers=min(16, os.cpu_count() or 1))  # before any CUDA call
     import torch
     from timstochrigidbodiessim_b200 import capi
+    from timstochrigidbodiessim_b200.fcm import step_many
     torch.cuda.set_device(0)
     lib = capi.load()
     root = torch.cuda.current_stream()
     total_bodies = sum(p.num_bodies for p, *_ in insts)
+    seeds = list(range(len(insts)))
     res = {}
-    for tag, prec in (("fp64", 0), ("mixed", 1)):
-        streams = [torch.cuda.Stream() for _ in insts] if prec == 1 else [torch.cuda.Stream()] * len(insts)
+    for tag, prec, mode in (("fp64", 0, "host"), ("fp64_graph", 0, "graph"), ("mixed", 1, "many")):
+        streams = [torch.cuda.Stream() for _ in insts] if mode == "many" else [torch.cuda.Stream()] * len(insts)
         ss = []
         for (p, ref, x, q, fe), st in zip(insts, streams):
             pp = p.copy(precision=prec)
             if prec == 1:
                 pp.gmres_tol = MIXED_TOL
             ss.append(setup_suspension(pp, ref, x, q, fe, st))
-        for s in ss:
-            for i in range(args.warmup):
-                s.step(1234, i)
+        for i in range(args.warmup):
+            if mode == "many":
+                step_many(ss, seeds, i)
+            else:
+                for k, s in enumerate(ss):
+                    if mode == "graph":
+                        s.step_async(seeds[k], i)
+                        s.step_wait()
+                    else:
+                        s.step(seeds[k], i)
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
+        sampler = ClockSampler(0)
+        if mode == "many":
+            sampler.start()
         l0 = lib.fcm_kernel_launch_count()
         e0.record(root)
         for st in set(streams):
             st.wait_event(e0)
-
-        def run(i):
-            its = []
-            for k in range(args.steps):
-                _, info = ss[i].step(1234, args.warmup + k)
-                its.append(info.gmres_iters)
-            return its
-
-        if prec == 1:
-            with cf.ThreadPoolExecutor(max_workers=len(ss)) as ex:
-                iters = list(ex.map(run, range(len(ss))))
-        else:
-            iters = [run(i) for i in range(len(ss))]
+        iters = []
+        for j in range(args.steps):
+            step = args.warmup + j
+            if mode == "many":
+                iters += [inf.gmres_iters for inf in step_many(ss, seeds, step)]
+            else:
+                for k, s in enumerate(ss):
+                    if mode == "graph":
+                        s.step_async(seeds[k], step)
+                        _, inf = s.step_wait()
+                    else:
+                        _, inf = s.step(seeds[k], step)
+                    iters.append(inf.gmres_iters)
         for st in set(streams):
             ev = torch.cuda.Event()
             ev.record(st)
             root.wait_event(ev)
         e1.record(root)
         e1.synchronize()
+        clocks = sampler.stop() if mode == "many" else None
         t = e0.elapsed_time(e1) / 1e3
-        res[tag] = dict(t=t, iters=float(np.mean([np.mean(i) for i in iters])),
-                        launches=lib.fcm_kernel_launch_count() - l0)
+        res[tag] = dict(t=t, iters=float(np.mean(iters)), launches=lib.fcm_kernel_launch_count() - l0,
+                        clocks=clocks)
         for s in ss:
             s.close()
+    # velocity error of the mixed solve against the FP64 solve, every instance
+    errs = [rel_vel_error(p, ref, x, q, fe, root) for p, ref, x, q, fe in insts]
     value = total_bodies * args.steps / res["mixed"]["t"]
     fp64 = total_bodies * args.steps / res["fp64"]["t"]
+    fp64g = total_bodies * args.steps / res["fp64_graph"]["t"]
     grids = sorted({p.nx for p, *_ in insts})
     print(json.dumps({
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
@@ -495,11 +533,16 @@ def run_ensemble(args):
         "vs_baseline": None, "dtype": "f32 grid + f64 refinement", "data": "synthetic (seeded random rods, Philox noise)",
         "config": {"workload": "ensemble64_rods50-500_g64-128", "instances": len(insts), "bodies": total_bodies,
                    "grids": grids, "gmres_tol_fp64": insts[0][0].gmres_tol, "mixed_gmres_tol": MIXED_TOL,
-                   "parallelism": "64 concurrent instances, 1 stream + 1 host thread each"},
+                   "seeds": "0..63", "parallelism": "64 instances, 1 stream each, one fcm_step_many call per step"},
         "fp64": {"value": fp64, "ms_per_step": 1e3 * res["fp64"]["t"] / args.steps, "gmres_iters": res["fp64"]["iters"],
-                 "mode": "instances one after another"},
-        "mixed_over_fp64": value / fp64, "gmres_iters_mixed": res["mixed"]["iters"],
+                 "mode": "instances one after another, host-driven fcm_step"},
+        "fp64_graph": {"value": fp64g, "ms_per_step": 1e3 * res["fp64_graph"]["t"] / args.steps,
+                       "mode": "instances one after another, device-resident graph steps"},
+        "mixed_over_fp64": value / fp64, "mixed_over_fp64_graph": value / fp64g,
+        "gmres_iters_mixed": res["mixed"]["iters"],
+        "rel_vel_error_mixed_vs_fp64_max": {"bodies": max(e[0] for e in errs), "blobs": max(e[1] for e in errs)},
         "gpu_launches": res["mixed"]["launches"],
+        "clocks": res["mixed"]["clocks"],
     }))
 
 

@@ -217,6 +217,15 @@ int fcm_get_V(fcm_ctx* ctx, double* V);
 int fcm_get_velocity_field(fcm_ctx* ctx, int32_t which, double* ux, double* uy, double* uz);
 /* M*F in one call: spread, Stokes solve, interpolation (V = 3Nb). */
 int fcm_apply_mobility(fcm_ctx* ctx, const double* F, double* V);
+/* The three stages of M*F one at a time on the working grid of one precision
+ * (0 = FP64, 1 = FP32, which needs a context of precision 1): spread F (3Nb),
+ * Stokes solve of that grid in place, interpolation of it into V (3Nb).  The
+ * FP64 stages are those of fcm_set_up_force_distribution,
+ * fcm_produce_deterministic_velocity_field and
+ * fcm_calculate_deterministic_blob_velocities; no reference counterpart for FP32. */
+int fcm_spread(fcm_ctx* ctx, int32_t precision, const double* F);
+int fcm_stokes_solve(fcm_ctx* ctx, int32_t precision);
+int fcm_interp(fcm_ctx* ctx, int32_t precision, double* V);
 /* fcm_fluid_solver.cpp:842-881: single-body mobility at the box centre,
  * ref_Minv = inv_sympd(M_body) ((3nb)^2), ref_N = inv(K^T ref_Minv K) (6x6). */
 int fcm_produce_reference_matrices(fcm_ctx* ctx);
@@ -245,6 +254,26 @@ int fcm_invert_saddle_point_system(fcm_ctx* ctx, double* soln, int32_t* iters,
  * params.noise is 1.  Returns FCM_OK or FCM_ERR_OVERLAP (state restored). */
 int fcm_step(fcm_ctx* ctx, uint64_t seed, uint64_t step_index, fcm_step_info* info);
 
+/* Asynchronous steps.  fcm_step_async issues the step of fcm_step without
+ * waiting for it; fcm_step_wait waits and returns its status and record (one step
+ * in flight per context; fcm_step refuses while one is).  The first step issued
+ * on a context runs host-driven, after which the whole step is captured in one
+ * CUDA graph whose GMRES iterations and refinement sweeps are device-side
+ * conditional loops (at most gmres_max_iter iterations per solve and 8 sweeps),
+ * and later steps launch that graph on the context's stream: no host round trip
+ * inside a step.  Contexts with skip_on_overlap = 1 keep host-driven steps.  A
+ * step whose solve fails (non-finite residual) leaves the bodies as they were,
+ * as fcm_step does.  No reference counterpart (main.cpp:222-451 steps
+ * synchronously). */
+int fcm_step_async(fcm_ctx* ctx, uint64_t seed, uint64_t step_index);
+int fcm_step_wait(fcm_ctx* ctx, fcm_step_info* info);
+/* One step of each of n independent suspensions (seeds[i] for context i, the
+ * same step_index): all issued, then all awaited, so contexts on different
+ * streams run concurrently.  infos (n records) may be NULL.  Returns FCM_OK or
+ * the first failing status. */
+int fcm_step_many(fcm_ctx* const* ctxs, int32_t n, const uint64_t* seeds, uint64_t step_index,
+                  fcm_step_info* infos);
+
 /* ================================================================ allocation-free interpolation
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory -- a time-step loop that must not stall the device (cudaMalloc and
@@ -257,7 +286,7 @@ int fcm_step(fcm_ctx* ctx, uint64_t seed, uint64_t step_index, fcm_step_info* in
  * must be DEVICE pointers; work is issued on `stream` (a cudaStream_t, 0 = legacy).
  * Limits: nblobs <= 8192, ngauss <= 24, nx, ny, nz multiples of 8 with
  * ngauss + 8 <= n, and at most 32768 8^3 tiles (a 256^3 grid); larger inputs are
- * rejected with FCM_ERR_INVALID.  Scratch is a fixed 20 MiB device array inside the
+ * rejected with FCM_ERR_INVALID.  Scratch is a fixed 32 MiB device array inside the
  * library, held by every GPU that loads it until exit.  The first call on a device
  * looks up that array's device address (once per device), so make the first call
  * before any stream capture.  Every call shares the array: calls that may overlap

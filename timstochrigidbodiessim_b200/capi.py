@@ -62,6 +62,9 @@ SIGNATURES = {
     "fcm_get_V": (ctypes.c_int, [VP, VP]),
     "fcm_get_velocity_field": (ctypes.c_int, [VP, ctypes.c_int32, VP, VP, VP]),
     "fcm_apply_mobility": (ctypes.c_int, [VP, VP, VP]),
+    "fcm_spread": (ctypes.c_int, [VP, ctypes.c_int32, VP]),
+    "fcm_stokes_solve": (ctypes.c_int, [VP, ctypes.c_int32]),
+    "fcm_interp": (ctypes.c_int, [VP, ctypes.c_int32, VP]),
     "fcm_produce_reference_matrices": (ctypes.c_int, [VP]),
     "fcm_get_reference_matrices": (ctypes.c_int, [VP, VP, VP, VP]),
     "fcm_set_reference_matrices": (ctypes.c_int, [VP, VP, VP]),
@@ -72,6 +75,10 @@ SIGNATURES = {
     "fcm_multiply_by_saddle_point_matrix": (ctypes.c_int, [VP, VP, VP]),
     "fcm_invert_saddle_point_system": (ctypes.c_int, [VP, VP, I32, D]),
     "fcm_step": (ctypes.c_int, [VP, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(FcmStepInfo)]),
+    "fcm_step_async": (ctypes.c_int, [VP, ctypes.c_uint64, ctypes.c_uint64]),
+    "fcm_step_wait": (ctypes.c_int, [VP, ctypes.POINTER(FcmStepInfo)]),
+    "fcm_step_many": (ctypes.c_int, [ctypes.POINTER(VP), ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64),
+                                     ctypes.c_uint64, ctypes.POINTER(FcmStepInfo)]),
     "fcm_interp_noalloc": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_int32, ctypes.c_int32, VP, VP, VP, VP]),
 }

@@ -343,13 +343,13 @@ int random_velocities_dev(Ctx* c, double* dV) {
   return interp_t<float>(c, c->g32.blobs, c->g32.urand, dV);
 }
 
-int noise_dev(Ctx* c, uint64_t seed, uint64_t counter) {
+int noise_dev(Ctx* c, uint64_t seed, uint64_t counter, const uint64_t* d_args = nullptr) {
   if (c->p.precision == 1) {
-    FCM_TRY(launch_noise_kspace<float>(*c, c->g32.c, seed, counter, c->stream));
+    FCM_TRY(launch_noise_kspace<float>(*c, c->g32.c, seed, counter, d_args, c->stream));
     FCM_CUFFT(exec_c2r(c->g32.c2r, c->g32.c, c->g32.urand));
     c->urand_prec = 1;
   } else {
-    FCM_TRY(launch_noise_kspace<double>(*c, c->g64.c, seed, counter, c->stream));
+    FCM_TRY(launch_noise_kspace<double>(*c, c->g64.c, seed, counter, d_args, c->stream));
     FCM_CUFFT(exec_c2r(c->g64.c2r, c->g64.c, c->g64.urand));
     c->urand_prec = 0;
   }
@@ -365,9 +365,18 @@ int saddle_matvec(Ctx* c, int prec, const double* in, double* out) {
   return FCM_OK;
 }
 
-// One Arnoldi iteration of the device-side GMRES, captured once per precision
-// in a CUDA graph on the private capture stream:
+// One Arnoldi iteration of the device-side GMRES on c->stream:
 //   z_in = Q[k]; z = P^-1 z_in; w = A z; orthogonalise, normalise, Givens.
+int enqueue_gm_iteration(Ctx* c, int prec) {
+  FCM_TRY(gm_fetch(*c, c->d_sys_b, c->stream));
+  FCM_TRY(launch_pinv(*c, c->d_qm, c->d_sys_b, c->d_sys_a, c->stream));
+  FCM_TRY(saddle_matvec(c, prec, c->d_sys_a, c->d_sys_b));
+  FCM_TRY(gm_orthogonalize(*c, c->d_sys_b, c->stream));
+  return FCM_OK;
+}
+
+// The Arnoldi iteration captured once per precision in a CUDA graph on the
+// private capture stream.
 int capture_iteration(Ctx* c, int prec) {
   cudaGraphExec_t& ex = c->iter_graph[prec];
   if (ex) return FCM_OK;
@@ -379,12 +388,7 @@ int capture_iteration(Ctx* c, int prec) {
   const long long l0 = launch_count();
   cudaError_t e = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    do {
-      if ((st = gm_fetch(*c, c->d_sys_b, c->cap_stream)) != FCM_OK) break;
-      if ((st = launch_pinv(*c, c->d_qm, c->d_sys_b, c->d_sys_a, c->cap_stream)) != FCM_OK) break;
-      if ((st = saddle_matvec(c, prec, c->d_sys_a, c->d_sys_b)) != FCM_OK) break;
-      if ((st = gm_orthogonalize(*c, c->d_sys_b, c->cap_stream)) != FCM_OK) break;
-    } while (0);
+    st = enqueue_gm_iteration(c, prec);
     const cudaError_t e2 = cudaStreamEndCapture(c->cap_stream, &g);
     if (st == FCM_OK && e2 != cudaSuccess) {
       set_error(std::string("GMRES iteration capture: ") + cudaGetErrorString(e2));
@@ -521,11 +525,12 @@ int overlap_dev(Ctx* c, int* ov) {
   return FCM_OK;
 }
 
-int end_of_step_update_dev(Ctx* c, const double* dU, double nu, int* overlap) {
+// The body update scales by nu * dt, with nu read from *d_nu when d_nu is given.
+int end_of_step_update_dev(Ctx* c, const double* dU, double nu, int* overlap, const double* d_nu = nullptr) {
   FCM_CUDA(cudaMemcpyAsync(c->d_xs, c->d_x, sizeof(double) * 3 * c->M, cudaMemcpyDeviceToDevice, c->stream));
   FCM_CUDA(cudaMemcpyAsync(c->d_qs, c->d_q, sizeof(double) * 4 * c->M, cudaMemcpyDeviceToDevice, c->stream));
-  const double scale = nu * c->p.dt;
-  FCM_TRY(launch_body_update(*c, c->d_x, c->d_q, dU, scale, c->stream));
+  const double scale = d_nu ? c->p.dt : nu * c->p.dt;
+  FCM_TRY(launch_body_update(*c, c->d_x, c->d_q, dU, scale, c->stream, d_nu));
   FCM_TRY(launch_fill_blob_pos(*c, c->d_x, c->d_q, c->d_Y, c->stream));
   FCM_TRY(cells_build(*c, c->stream));
   int ov = 0;
@@ -547,10 +552,10 @@ int advance_to_midstep_dev(Ctx* c, const double* dV, int* overlap) {
   return FCM_OK;
 }
 
-int divU_dev(Ctx* c, double* out) {
+// collection_of_rigid_bodies.cpp:869-953 with the sum left in *acc (device).
+int divU_enqueue(Ctx* c, double* acc) {
   FCM_CUDA(cudaMemcpyAsync(c->d_xs, c->d_x, sizeof(double) * 3 * c->M, cudaMemcpyDeviceToDevice, c->stream));
   FCM_CUDA(cudaMemcpyAsync(c->d_qs, c->d_q, sizeof(double) * 4 * c->M, cudaMemcpyDeviceToDevice, c->stream));
-  double* acc = c->d_H + c->maxit_alloc + 1;
   FCM_CUDA(cudaMemsetAsync(acc, 0, sizeof(double), c->stream));
   for (int i = 0; i < 6; ++i) {
     double e[6] = {0, 0, 0, 0, 0, 0};
@@ -565,9 +570,340 @@ int divU_dev(Ctx* c, double* out) {
     FCM_CUDA(cudaMemcpyAsync(c->d_x, c->d_xs, sizeof(double) * 3 * c->M, cudaMemcpyDeviceToDevice, c->stream));
     FCM_CUDA(cudaMemcpyAsync(c->d_q, c->d_qs, sizeof(double) * 4 * c->M, cudaMemcpyDeviceToDevice, c->stream));
   }
+  return FCM_OK;
+}
+
+int divU_dev(Ctx* c, double* out) {
+  double* acc = c->d_H + c->maxit_alloc + 1;
+  FCM_TRY(divU_enqueue(c, acc));
   FCM_CUDA(cudaMemcpyAsync(c->h_pinned, acc, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   FCM_CUDA(cudaStreamSynchronize(c->stream));
   *out = c->h_pinned[0];
+  return FCM_OK;
+}
+
+// ------------------------------------------------------------------ device-resident step
+// The whole time step as one CUDA graph.  The GMRES iterations and the FP64
+// refinement sweeps are conditional while-nodes whose conditions the device sets
+// from the GMRES state (cudaGraphSetConditional), so a step runs from launch to
+// completion with no host round trip; the host reads one StepRecord at the end.
+// The per-step inputs (noise seed and step index) are read from device memory.
+// Built once per context, after a host-driven step has allocated every buffer.
+
+// Condition of a GMRES while-loop: go on while the solve is not done, for at
+// most `limit` iterations of this loop.
+__global__ void k_gm_loop_cond(cudaGraphConditionalHandle h, const GmState* __restrict__ gm, StepRecord* sd,
+                               int enter, int limit) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (enter) sd->guard = 0;
+  else ++sd->guard;
+  cudaGraphSetConditional(h, (!gm->done && sd->guard < limit) ? 1u : 0u);
+}
+
+__global__ void k_step_begin(StepRecord* sd) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  sd->iters = 0;
+  sd->sweeps = 0;
+  sd->status = FCM_OK;
+  sd->guard = 0;
+  sd->rel = 0.0;
+  sd->divU = 0.0;
+  sd->normb = 0.0;
+  sd->relr = 1.0;
+}
+
+// FP64 solve: record the GMRES result.
+__global__ void k_gm_record(StepRecord* sd, const GmState* __restrict__ gm) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  sd->iters = gm->k;
+  sd->sweeps = 1;
+  sd->rel = gm->rel;
+  sd->status = gm->status;
+}
+
+// GDC: nu = 1 + dt/2 divU (main.cpp:265-268), divU = 0 without noise.
+__global__ void k_gdc_nu(StepRecord* sd, const double* __restrict__ acc, int noise, double dt, double* __restrict__ nu) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double divU = noise ? *acc : 0.0;
+  sd->divU = divU;
+  *nu = __dadd_rn(1.0, __dmul_rn(__dmul_rn(0.5, dt), divU));
+}
+
+// Refinement loop entry: ||b|| from rs[0], enter the loop.
+__global__ void k_ref_enter(cudaGraphConditionalHandle h, StepRecord* sd, const double* __restrict__ rs) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  sd->normb = rs[0];
+  sd->relr = 1.0;
+  sd->sweeps = 0;
+  sd->iters = 0;
+  sd->status = FCM_OK;
+  cudaGraphSetConditional(h, 1u);
+}
+
+// Inner tolerance of the next FP32-grid sweep: it only has to shrink the
+// current residual by the remaining factor (clamped to [1e-6, 0.5]).
+__global__ void k_ref_tol(const StepRecord* __restrict__ sd, double tol, double* __restrict__ rs) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  rs[2] = fmin(0.5, fmax(1e-6, 0.3 * tol / sd->relr));
+}
+
+// After a sweep: relative residual ||r|| / ||b|| (rs[1] / normb) and the loop
+// condition; at most `max_sweeps` sweeps.
+__global__ void k_ref_next(cudaGraphConditionalHandle h, StepRecord* sd, const GmState* __restrict__ gm,
+                           const double* __restrict__ rs, double tol, int max_sweeps) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  sd->sweeps += 1;
+  sd->iters += gm->k;
+  unsigned go = 0u;
+  if (gm->status == FCM_ERR_NONFINITE) {
+    sd->status = FCM_ERR_NONFINITE;
+    sd->rel = gm->rel;
+  } else {
+    const double relr = sd->normb > 0.0 ? rs[1] / sd->normb : 0.0;
+    sd->relr = relr;
+    sd->rel = relr;
+    if (!isfinite(relr)) {
+      sd->status = FCM_ERR_NONFINITE;
+    } else if (relr < tol) {
+      sd->status = FCM_OK;
+    } else {
+      sd->status = FCM_ERR_NOT_CONVERGED;
+      go = sd->sweeps < max_sweeps ? 1u : 0u;
+    }
+  }
+  cudaGraphSetConditional(h, go);
+}
+
+constexpr int kMaxSweeps = 8;
+
+// Capture scope: c->stream and the cuFFT plans follow stream `s` until restored.
+struct StreamSwap {
+  Ctx* c;
+  cudaStream_t old;
+  StreamSwap(Ctx* c_, cudaStream_t s) : c(c_), old(c_->stream) {
+    c->stream = s;
+    set_stream_all(c);
+  }
+  ~StreamSwap() {
+    c->stream = old;
+    set_stream_all(c);
+  }
+};
+
+// A conditional while-node appended to the graph being captured on `s`; its
+// condition handle `h` must have been created on that graph (new_handle) and set
+// by a kernel captured before.  Returns the (empty) body graph.
+int add_while_node(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraph_t* body) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  FCM_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+  if (cs != cudaStreamCaptureStatusActive) {
+    set_error("step graph: stream is not capturing");
+    return FCM_ERR_CUDA;
+  }
+  cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node = nullptr;
+  FCM_CUDA(cudaGraphAddNode(&node, g, deps, nd, &np));
+  *body = np.conditional.phGraph_out[0];
+  FCM_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+  return FCM_OK;
+}
+
+// A condition handle on the graph being captured on `s`.
+int new_handle(cudaStream_t s, cudaGraphConditionalHandle* h) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaGraph_t g = nullptr;
+  FCM_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, nullptr, nullptr));
+  if (cs != cudaStreamCaptureStatusActive) {
+    set_error("step graph: stream is not capturing");
+    return FCM_ERR_CUDA;
+  }
+  // default 0 at every launch of the owning graph: a loop runs only once a
+  // kernel has set its condition
+  FCM_CUDA(cudaGraphConditionalHandleCreate(h, g, 0, cudaGraphCondAssignDefault));
+  return FCM_OK;
+}
+
+// Capture into `body` on stream `bs` whatever `fn` enqueues on c->stream.
+template <typename F>
+int capture_body(Ctx* c, cudaGraph_t body, cudaStream_t bs, F&& fn) {
+  FCM_CUDA(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  int st = FCM_OK;
+  {
+    StreamSwap sw(c, bs);
+    st = fn();
+  }
+  cudaGraph_t out = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(bs, &out);
+  if (st == FCM_OK && e != cudaSuccess) {
+    set_error(std::string("step graph body capture: ") + cudaGetErrorString(e));
+    st = FCM_ERR_CUDA;
+  }
+  return st;
+}
+
+// GMRES on c->stream as a device loop: init (tolerance `tol`, or *d_tol), the
+// iterations as a while-node whose body is captured on `bs`, then the solution
+// P^-1 sum y_i q_i into d_x.  *iter_kernels receives the kernels of one iteration.
+int enqueue_gmres_loop(Ctx* c, int prec, const double* d_b, double* d_x, double tol, const double* d_tol,
+                       cudaStream_t bs, long long* iter_kernels) {
+  const long long n = c->nsys;
+  const int max_iter =
+      (int)std::max<long long>(1, std::min<long long>(n, std::min(c->p.gmres_max_iter, c->maxit_alloc)));
+  FCM_TRY(gm_init(*c, d_b, tol, max_iter, c->stream, d_tol));
+  cudaGraphConditionalHandle h;
+  FCM_TRY(new_handle(c->stream, &h));
+  k_gm_loop_cond<<<1, 32, 0, c->stream>>>(h, c->gm, c->d_step, 1, max_iter);
+  FCM_LAUNCH_CHECK();
+  cudaGraph_t body = nullptr;
+  FCM_TRY(add_while_node(c->stream, h, &body));
+  const long long l0 = launch_count();
+  FCM_TRY(capture_body(c, body, bs, [&] {
+    FCM_TRY(enqueue_gm_iteration(c, prec));
+    k_gm_loop_cond<<<1, 32, 0, c->stream>>>(h, c->gm, c->d_step, 0, max_iter);
+    FCM_LAUNCH_CHECK();
+    return (int)FCM_OK;
+  }));
+  *iter_kernels = launch_count() - l0;
+  FCM_TRY(gm_finish(*c, c->d_sys_b, c->stream));
+  FCM_TRY(launch_pinv(*c, c->d_qm, c->d_sys_b, d_x, c->stream));
+  return FCM_OK;
+}
+
+// Enqueue one whole time step (the sequence of fcm_step) on c->stream, with the
+// solve as device loops.  Requires skip_on_overlap = 0 (no host decision).
+int enqueue_resident_step(Ctx* c, long long* k_top, long long* k_sweep, long long* k_iter) {
+  const long long l_start = launch_count();
+  long long l_loops = 0;  // kernels captured inside loop bodies
+  const bool noise = c->p.noise != 0;
+  k_step_begin<<<1, 32, 0, c->stream>>>(c->d_step);
+  FCM_LAUNCH_CHECK();
+  FCM_TRY(launch_fill_blob_pos(*c, c->d_x, c->d_q, c->d_Y, c->stream));
+  if (noise) FCM_TRY(noise_dev(c, 0, 0, c->d_stepargs));
+  else c->urand_ready = false;
+  FCM_TRY(set_up_gaussians_dev(c, c->d_Y));
+  FCM_TRY(random_velocities_dev(c, c->d_V));
+  const double* d_nu = nullptr;
+  if (c->p.algorithm == 1) {
+    int ov = 0;
+    FCM_TRY(advance_to_midstep_dev(c, c->d_V, &ov));
+    double* acc = c->d_H + c->maxit_alloc + 1;
+    if (noise) FCM_TRY(divU_enqueue(c, acc));
+    k_gdc_nu<<<1, 32, 0, c->stream>>>(c->d_step, acc, noise ? 1 : 0, c->p.dt, c->d_rs + 3);
+    FCM_LAUNCH_CHECK();
+    d_nu = c->d_rs + 3;
+    FCM_TRY(launch_fill_blob_pos(*c, c->d_xm, c->d_qm, c->d_Y, c->stream));
+    FCM_TRY(set_up_gaussians_dev(c, c->d_Y));
+    FCM_TRY(random_velocities_dev(c, c->d_V));
+  }
+  FCM_TRY(calculate_forces_dev(c));
+  FCM_TRY(assemble_rhs_dev(c));
+  const long long n = c->nsys;
+  *k_sweep = 0;
+  if (c->p.precision == 0) {
+    FCM_TRY(enqueue_gmres_loop(c, 0, c->d_rhs, c->d_soln, c->p.gmres_tol, nullptr, c->cap_body[0], k_iter));
+    l_loops += *k_iter;
+    k_gm_record<<<1, 32, 0, c->stream>>>(c->d_step, c->gm);
+    FCM_LAUNCH_CHECK();
+  } else {
+    // r = b; x = 0; repeat: dx = GMRES32(r); x += dx; r = b - A64 x (solve_dev).
+    double* x = c->d_soln;
+    FCM_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, c->stream));
+    FCM_CUDA(cudaMemcpyAsync(c->d_res, c->d_rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream));
+    FCM_TRY(blas_norm_sq_partial(*c, c->d_rhs, n, c->d_rs + 0, c->stream));
+    cudaGraphConditionalHandle h;
+    FCM_TRY(new_handle(c->stream, &h));
+    k_ref_enter<<<1, 32, 0, c->stream>>>(h, c->d_step, c->d_rs);
+    FCM_LAUNCH_CHECK();
+    cudaGraph_t body = nullptr;
+    FCM_TRY(add_while_node(c->stream, h, &body));
+    const long long l0 = launch_count();
+    FCM_TRY(capture_body(c, body, c->cap_body[0], [&] {
+      k_ref_tol<<<1, 32, 0, c->stream>>>(c->d_step, c->p.gmres_tol, c->d_rs);
+      FCM_LAUNCH_CHECK();
+      FCM_TRY(enqueue_gmres_loop(c, 1, c->d_res, c->d_dx, 0.0, c->d_rs + 2, c->cap_body[1], k_iter));
+      FCM_TRY(blas_axpby(x, c->d_dx, 1.0, 1.0, n, c->stream));
+      FCM_TRY(saddle_matvec(c, 0, x, c->d_res));
+      FCM_TRY(blas_axpby(c->d_res, c->d_rhs, 1.0, -1.0, n, c->stream));
+      FCM_TRY(blas_norm_sq_partial(*c, c->d_res, n, c->d_rs + 1, c->stream));
+      k_ref_next<<<1, 32, 0, c->stream>>>(h, c->d_step, c->gm, c->d_rs, c->p.gmres_tol, kMaxSweeps);
+      FCM_LAUNCH_CHECK();
+      return (int)FCM_OK;
+    }));
+    *k_sweep = launch_count() - l0 - *k_iter;
+    l_loops += launch_count() - l0;
+  }
+  int ov = 0;
+  FCM_TRY(end_of_step_update_dev(c, c->d_soln + 3 * (size_t)c->Nb, 1.0, &ov, d_nu));
+  FCM_CUDA(cudaMemcpyAsync(c->h_step, c->d_step, sizeof(StepRecord), cudaMemcpyDeviceToHost, c->stream));
+  *k_top = launch_count() - l_start - l_loops;
+  return FCM_OK;
+}
+
+// Capture the resident step into c->step_graph (state 1), or mark the context
+// for host-driven steps (state -1) when the step cannot be a graph.
+int build_step_graph(Ctx* c) {
+  if (c->p.skip_on_overlap) {
+    c->step_graph_state = -1;
+    return FCM_OK;
+  }
+  if (!c->d_step) {
+    if (cudaMalloc(&c->d_step, sizeof(StepRecord)) != cudaSuccess ||
+        cudaMallocHost(&c->h_step, sizeof(StepRecord)) != cudaSuccess ||
+        cudaMalloc(&c->d_stepargs, 2 * sizeof(uint64_t)) != cudaSuccess ||
+        cudaMallocHost(&c->h_stepargs, 2 * sizeof(uint64_t)) != cudaSuccess ||
+        cudaMalloc(&c->d_rs, 8 * sizeof(double)) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->cap_body[0], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->cap_body[1], cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("step graph: buffer allocation failed");
+      c->step_graph_state = -1;
+      return FCM_ERR_NOMEM;
+    }
+  }
+  const long long l0 = launch_count();
+  int st = FCM_OK;
+  cudaGraph_t g = nullptr;
+  long long kt = 0, ks = 0, ki = 0;
+  cudaError_t e = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    {
+      StreamSwap sw(c, c->cap_stream);
+      st = enqueue_resident_step(c, &kt, &ks, &ki);
+    }
+    const cudaError_t e2 = cudaStreamEndCapture(c->cap_stream, &g);
+    if (st == FCM_OK && e2 != cudaSuccess) {
+      set_error(std::string("step graph capture: ") + cudaGetErrorString(e2));
+      st = FCM_ERR_CUDA;
+    }
+  } else {
+    set_error(std::string("cudaStreamBeginCapture: ") + cudaGetErrorString(e));
+    st = FCM_ERR_CUDA;
+  }
+  count_launches(-(launch_count() - l0));  // counted per executed step instead
+  if (st == FCM_OK) {
+    e = cudaGraphInstantiate(&c->step_graph, g, 0);
+    if (e != cudaSuccess) {
+      set_error(std::string("step graph instantiate: ") + cudaGetErrorString(e));
+      c->step_graph = nullptr;
+      st = FCM_ERR_CUDA;
+    }
+  }
+  if (g) cudaGraphDestroy(g);
+  cudaGetLastError();
+  if (st != FCM_OK) {
+    c->step_graph_state = -1;
+    return st;
+  }
+  c->step_kernels_top = kt;
+  c->step_kernels_sweep = ks;
+  c->step_kernels_iter = ki;
+  c->step_graph_state = 1;
   return FCM_OK;
 }
 
@@ -709,6 +1045,14 @@ void destroy_ctx(Ctx* c) {
   cudaFree(c->d_mdcount);
   if (c->h_gm) cudaFreeHost(c->h_gm);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+  if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+  cudaFree(c->d_step);
+  cudaFree(c->d_stepargs);
+  cudaFree(c->d_rs);
+  if (c->h_step) cudaFreeHost(c->h_step);
+  if (c->h_stepargs) cudaFreeHost(c->h_stepargs);
+  for (int i = 0; i < 2; ++i)
+    if (c->cap_body[i]) cudaStreamDestroy(c->cap_body[i]);
   cudaFree(c->d_cell);
   cudaFree(c->d_cell_start);
   cudaFree(c->d_cell_count);
@@ -871,6 +1215,131 @@ int guard(F&& f) {
     ::fcm::set_error("null context");    \
     return FCM_ERR_INVALID;              \
   }
+
+// main.cpp:222-451, one step driven from the host.
+int step_host(Ctx* c, uint64_t seed, uint64_t step_index, fcm_step_info* info) {
+  {
+    fcm_step_info inf;
+    std::memset(&inf, 0, sizeof(inf));
+    const bool noise = c->p.noise != 0;
+    // main.cpp:230-233
+    FCM_TRY(launch_fill_blob_pos(*c, c->d_x, c->d_q, c->d_Y, c->stream));
+    if (noise) FCM_TRY(noise_dev(c, seed, step_index));
+    else c->urand_ready = false;
+    FCM_TRY(set_up_gaussians_dev(c, c->d_Y));
+    FCM_TRY(random_velocities_dev(c, c->d_V));
+    double nu = 1.0;
+    if (c->p.algorithm == 1) {  // main.cpp:235-268
+      int ov = 0;
+      FCM_TRY(advance_to_midstep_dev(c, c->d_V, &ov));
+      if (ov) {
+        inf.overlap = 1;
+        if (info) *info = inf;
+        return (int)FCM_ERR_OVERLAP;
+      }
+      double divU = 0.0;
+      if (noise) FCM_TRY(divU_dev(c, &divU));
+      inf.divU = divU;
+      nu = 1.0 + 0.5 * c->p.dt * divU;
+      FCM_TRY(launch_fill_blob_pos(*c, c->d_xm, c->d_qm, c->d_Y, c->stream));
+      FCM_TRY(set_up_gaussians_dev(c, c->d_Y));
+      FCM_TRY(random_velocities_dev(c, c->d_V));
+    }
+    FCM_TRY(calculate_forces_dev(c));  // main.cpp:282
+    FCM_TRY(assemble_rhs_dev(c));      // main.cpp:308
+    int it = 0, sw = 0;
+    double rel = 0.0;
+    const int st = solve_dev(c, c->d_rhs, c->d_soln, &it, &rel, &sw);  // main.cpp:310
+    inf.gmres_iters = it;
+    inf.refinement_sweeps = sw;
+    inf.gmres_rel_residual = rel;
+    inf.status = st;
+    if (st != FCM_OK && st != FCM_ERR_NOT_CONVERGED) {
+      if (info) *info = inf;
+      return st;
+    }
+    int ov = 0;
+    FCM_TRY(end_of_step_update_dev(c, c->d_soln + 3 * (size_t)c->Nb, nu, &ov));  // main.cpp:312
+    if (ov) {  // main.cpp:316-328
+      FCM_CUDA(cudaMemcpyAsync(c->d_x, c->d_xs, sizeof(double) * 3 * c->M, cudaMemcpyDeviceToDevice, c->stream));
+      FCM_CUDA(cudaMemcpyAsync(c->d_q, c->d_qs, sizeof(double) * 4 * c->M, cudaMemcpyDeviceToDevice, c->stream));
+      inf.overlap = 1;
+      if (info) *info = inf;
+      return (int)FCM_ERR_OVERLAP;
+    }
+    if (info) *info = inf;
+    return (int)FCM_OK;
+  }
+}
+
+// Issue one step on c->stream: a launch of the step graph when the context has
+// one; otherwise (first step, or skip_on_overlap) a host-driven step whose
+// result step_wait returns.  The first host-driven step allocates every buffer,
+// after which the step graph is captured.
+int step_issue(Ctx* c, uint64_t seed, uint64_t step_index) {
+  if (c->step_pending) {
+    set_error("a step is already in flight on this context: call fcm_step_wait first");
+    return FCM_ERR_STATE;
+  }
+  if (c->step_graph_state == 1) {
+    c->h_stepargs[0] = seed;
+    c->h_stepargs[1] = step_index;
+    FCM_CUDA(cudaMemcpyAsync(c->d_stepargs, c->h_stepargs, 2 * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+    FCM_CUDA(cudaGraphLaunch(c->step_graph, c->stream));
+    c->step_pending = true;
+    c->step_pending_graph = true;
+    return FCM_OK;
+  }
+  fcm_step_info inf;
+  std::memset(&inf, 0, sizeof(inf));
+  const int st = step_host(c, seed, step_index, &inf);
+  if (st != FCM_OK && st != FCM_ERR_OVERLAP) return st;
+  c->step_pending = true;
+  c->step_pending_graph = false;
+  c->step_pending_status = st;
+  c->step_pending_info = inf;
+  if (c->step_graph_state == 0 && st == FCM_OK) {
+    const std::string keep = g_err;
+    if (build_step_graph(c) != FCM_OK) set_error(keep);  // host-driven steps from now on
+  }
+  return FCM_OK;
+}
+
+int step_wait(Ctx* c, fcm_step_info* info) {
+  if (!c->step_pending) {
+    set_error("no step in flight on this context");
+    return FCM_ERR_STATE;
+  }
+  c->step_pending = false;
+  if (!c->step_pending_graph) {
+    if (info) *info = c->step_pending_info;
+    return c->step_pending_status;
+  }
+  FCM_CUDA(cudaStreamSynchronize(c->stream));
+  const StepRecord r = *c->h_step;
+  count_launches(c->step_kernels_top + (long long)r.sweeps * c->step_kernels_sweep +
+                 (long long)r.iters * c->step_kernels_iter);
+  c->gauss_ready = true;
+  c->urand_ready = c->p.noise != 0;
+  c->urand_prec = c->p.precision;
+  fcm_step_info inf;
+  std::memset(&inf, 0, sizeof(inf));
+  inf.gmres_iters = r.iters;
+  inf.refinement_sweeps = r.sweeps;
+  inf.gmres_rel_residual = r.rel;
+  inf.divU = r.divU;
+  inf.status = r.status;
+  if (info) *info = inf;
+  if (r.status != FCM_OK && r.status != FCM_ERR_NOT_CONVERGED) {
+    // the host-driven step stops before the body update: put the bodies back
+    FCM_CUDA(cudaMemcpyAsync(c->d_x, c->d_xs, sizeof(double) * 3 * c->M, cudaMemcpyDeviceToDevice, c->stream));
+    FCM_CUDA(cudaMemcpyAsync(c->d_q, c->d_qs, sizeof(double) * 4 * c->M, cudaMemcpyDeviceToDevice, c->stream));
+    FCM_CUDA(cudaStreamSynchronize(c->stream));
+    set_error(r.status == FCM_ERR_NONFINITE ? "GMRES residual became non-finite" : "step failed");
+    return r.status;
+  }
+  return FCM_OK;
+}
 
 }  // namespace
 }  // namespace fcm
@@ -1259,6 +1728,63 @@ int fcm_apply_mobility(fcm_ctx* ctx, const double* F, double* V) {
   return copy_out(c, V, c->d_V, sizeof(double) * 3 * c->Nb);
 }
 
+static int check_stage_precision(Ctx* c, int32_t precision) {
+  if (precision != 0 && precision != 1) {
+    set_error("precision must be 0 (FP64) or 1 (FP32)");
+    return FCM_ERR_INVALID;
+  }
+  if (precision == 1 && c->p.precision != 1) {
+    set_error("the FP32 grid needs a context created with precision 1");
+    return FCM_ERR_INVALID;
+  }
+  if (!c->gauss_ready) {
+    set_error("set_up_gaussians must precede the grid stages");
+    return FCM_ERR_STATE;
+  }
+  return FCM_OK;
+}
+
+int fcm_spread(fcm_ctx* ctx, int32_t precision, const double* F) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  FCM_TRY(check_stage_precision(c, precision));
+  const double* dF = F;  // device input is read in place
+  if (!is_device_ptr(F)) {
+    FCM_TRY(copy_in(c, c->d_tmp3, F, sizeof(double) * 3 * c->Nb));
+    dF = c->d_tmp3;
+  }
+  if (precision == 0) {
+    c->det_ready = false;
+    return spread_t<double>(c, c->g64.blobs, dF);
+  }
+  return spread_t<float>(c, c->g32.blobs, dF);
+}
+
+int fcm_stokes_solve(fcm_ctx* ctx, int32_t precision) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  FCM_TRY(check_stage_precision(c, precision));
+  if (precision == 0) {
+    FCM_TRY(stokes_t<double>(c));
+    c->det_ready = true;
+    return FCM_OK;
+  }
+  return stokes_t<float>(c);
+}
+
+int fcm_interp(fcm_ctx* ctx, int32_t precision, double* V) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  FCM_TRY(check_stage_precision(c, precision));
+  double* dV = (V && is_device_ptr(V)) ? V : c->d_V;  // device output is written in place
+  if (precision == 0)
+    FCM_TRY(interp_t<double>(c, c->g64.blobs, c->g64.r, dV));
+  else
+    FCM_TRY(interp_t<float>(c, c->g32.blobs, c->g32.r, dV));
+  if (dV == V) return FCM_OK;
+  return copy_out(c, V, c->d_V, sizeof(double) * 3 * c->Nb);
+}
+
 int fcm_produce_reference_matrices(fcm_ctx* ctx) {
   CTX_CHECK(ctx);
   return guard([&] { return reference_matrices_dev(ctx->c); });
@@ -1353,58 +1879,53 @@ int fcm_invert_saddle_point_system(fcm_ctx* ctx, double* soln, int32_t* iters, d
 // ------------------------------------------------------------------ time step
 int fcm_step(fcm_ctx* ctx, uint64_t seed, uint64_t step_index, fcm_step_info* info) {
   CTX_CHECK(ctx);
+  if (ctx->c->step_pending) {
+    set_error("a step issued by fcm_step_async is in flight: call fcm_step_wait first");
+    return FCM_ERR_STATE;
+  }
+  return guard([&] { return step_host(ctx->c, seed, step_index, info); });
+}
+
+int fcm_step_async(fcm_ctx* ctx, uint64_t seed, uint64_t step_index) {
+  CTX_CHECK(ctx);
+  return guard([&] { return step_issue(ctx->c, seed, step_index); });
+}
+
+int fcm_step_wait(fcm_ctx* ctx, fcm_step_info* info) {
+  CTX_CHECK(ctx);
+  return guard([&] { return step_wait(ctx->c, info); });
+}
+
+int fcm_step_many(fcm_ctx* const* ctxs, int32_t n, const uint64_t* seeds, uint64_t step_index,
+                  fcm_step_info* infos) {
+  if (n < 0 || (n > 0 && (!ctxs || !seeds))) {
+    set_error("fcm_step_many: n >= 0 contexts and seeds required");
+    return FCM_ERR_INVALID;
+  }
+  for (int i = 0; i < n; ++i) CTX_CHECK(ctxs[i]);
   return guard([&] {
-    Ctx* c = ctx->c;
-    fcm_step_info inf;
-    std::memset(&inf, 0, sizeof(inf));
-    const bool noise = c->p.noise != 0;
-    // main.cpp:230-233
-    FCM_TRY(launch_fill_blob_pos(*c, c->d_x, c->d_q, c->d_Y, c->stream));
-    if (noise) FCM_TRY(noise_dev(c, seed, step_index));
-    else c->urand_ready = false;
-    FCM_TRY(set_up_gaussians_dev(c, c->d_Y));
-    FCM_TRY(random_velocities_dev(c, c->d_V));
-    double nu = 1.0;
-    if (c->p.algorithm == 1) {  // main.cpp:235-268
-      int ov = 0;
-      FCM_TRY(advance_to_midstep_dev(c, c->d_V, &ov));
-      if (ov) {
-        inf.overlap = 1;
-        if (info) *info = inf;
-        return (int)FCM_ERR_OVERLAP;
+    int first = FCM_OK;
+    std::string err;
+    int issued = 0;
+    for (; issued < n; ++issued) {
+      const int st = step_issue(ctxs[issued]->c, seeds[issued], step_index);
+      if (st != FCM_OK) {
+        first = st;
+        err = g_err;
+        break;
       }
-      double divU = 0.0;
-      if (noise) FCM_TRY(divU_dev(c, &divU));
-      inf.divU = divU;
-      nu = 1.0 + 0.5 * c->p.dt * divU;
-      FCM_TRY(launch_fill_blob_pos(*c, c->d_xm, c->d_qm, c->d_Y, c->stream));
-      FCM_TRY(set_up_gaussians_dev(c, c->d_Y));
-      FCM_TRY(random_velocities_dev(c, c->d_V));
     }
-    FCM_TRY(calculate_forces_dev(c));  // main.cpp:282
-    FCM_TRY(assemble_rhs_dev(c));      // main.cpp:308
-    int it = 0, sw = 0;
-    double rel = 0.0;
-    const int st = solve_dev(c, c->d_rhs, c->d_soln, &it, &rel, &sw);  // main.cpp:310
-    inf.gmres_iters = it;
-    inf.refinement_sweeps = sw;
-    inf.gmres_rel_residual = rel;
-    inf.status = st;
-    if (st != FCM_OK && st != FCM_ERR_NOT_CONVERGED) {
-      if (info) *info = inf;
-      return st;
+    for (int i = 0; i < issued; ++i) {
+      fcm_step_info inf;
+      const int st = step_wait(ctxs[i]->c, &inf);
+      if (infos) infos[i] = inf;
+      if (st != FCM_OK && first == FCM_OK) {
+        first = st;
+        err = g_err;
+      }
     }
-    int ov = 0;
-    FCM_TRY(end_of_step_update_dev(c, c->d_soln + 3 * (size_t)c->Nb, nu, &ov));  // main.cpp:312
-    if (ov) {  // main.cpp:316-328
-      FCM_CUDA(cudaMemcpyAsync(c->d_x, c->d_xs, sizeof(double) * 3 * c->M, cudaMemcpyDeviceToDevice, c->stream));
-      FCM_CUDA(cudaMemcpyAsync(c->d_q, c->d_qs, sizeof(double) * 4 * c->M, cudaMemcpyDeviceToDevice, c->stream));
-      inf.overlap = 1;
-      if (info) *info = inf;
-      return (int)FCM_ERR_OVERLAP;
-    }
-    if (info) *info = inf;
-    return (int)FCM_OK;
+    if (first != FCM_OK) set_error(err);
+    return first;
   });
 }
 

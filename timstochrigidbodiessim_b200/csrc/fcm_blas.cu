@@ -307,9 +307,10 @@ __global__ void k_gm_givens(GmState* st, double* __restrict__ H, int hn, double*
 
 // beta[0] = |b|, k = 0 (one thread); |b| == 0 or non-finite ends the solve.
 __global__ void k_gm_init(GmState* st, const double* __restrict__ normb, double* __restrict__ beta, double tol,
-                          int maxit) {
+                          const double* __restrict__ d_tol, int maxit) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const double nb = *normb;
+  if (d_tol) tol = *d_tol;
   st->k = 0;
   st->tol = tol;
   st->maxit = maxit;
@@ -379,10 +380,10 @@ int gm_orthogonalize(const Ctx& c, double* w, cudaStream_t s) {
   return FCM_OK;
 }
 
-int gm_init(const Ctx& c, const double* b, double tol, int maxit, cudaStream_t s) {
+int gm_init(const Ctx& c, const double* b, double tol, int maxit, cudaStream_t s, const double* d_tol) {
   const long long n = c.nsys;
   FCM_TRY(blas_norm_sq_partial(c, b, n, c.d_hnorm, s));
-  k_gm_init<<<1, 32, 0, s>>>(c.gm, c.d_hnorm, c.d_beta, tol, maxit);
+  k_gm_init<<<1, 32, 0, s>>>(c.gm, c.d_hnorm, c.d_beta, tol, d_tol, maxit);
   FCM_LAUNCH_CHECK();
   FCM_TRY(blas_copy_scaled(c.d_Qm, b, c.d_hnorm, 1, n, s));
   return FCM_OK;

@@ -247,9 +247,10 @@ __device__ void body_update_one(double* x, double* q, const double u[6], double 
 }
 
 __global__ void k_body_update(double* __restrict__ x, double* __restrict__ q, const double* __restrict__ U, int M,
-                              double scale, double Lx, double Ly, double Lz) {
+                              double scale, const double* __restrict__ d_nu, double Lx, double Ly, double Lz) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= M) return;
+  if (d_nu) scale = __dmul_rn(*d_nu, scale);  // nu * dt with nu from device memory
   double u[6];
   for (int d = 0; d < 6; ++d) u[d] = scale * U[6 * n + d];
   body_update_one(x + 3 * n, q + 4 * n, u, Lx, Ly, Lz);
@@ -313,9 +314,10 @@ int launch_rigid_projection(const Ctx& c, const double* q, const double* V, doub
   return FCM_OK;
 }
 
-int launch_body_update(const Ctx& c, double* x, double* q, const double* U6, double scale, cudaStream_t s) {
+int launch_body_update(const Ctx& c, double* x, double* q, const double* U6, double scale, cudaStream_t s,
+                       const double* d_nu) {
   if (c.M == 0) return FCM_OK;
-  k_body_update<<<(c.M + 127) / 128, 128, 0, s>>>(x, q, U6, c.M, scale, c.g.Lx, c.g.Ly, c.g.Lz);
+  k_body_update<<<(c.M + 127) / 128, 128, 0, s>>>(x, q, U6, c.M, scale, d_nu, c.g.Lx, c.g.Ly, c.g.Lz);
   FCM_LAUNCH_CHECK();
   return FCM_OK;
 }

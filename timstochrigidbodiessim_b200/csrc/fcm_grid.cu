@@ -3,15 +3,20 @@
 // set_up_gaussians restates fcm_fluid_solver.cpp:131-165; spreading restates
 // :552-600 (SLIP_CHANNEL false) and interpolation :363-424 / :426-487.
 //
-// Tiled spreading.  The grid is cut into 8x8x8 tiles.  After set_up_gaussians
-// every (blob, tile) overlap is listed per tile (count, scan, fill, then a
-// per-tile sort by blob id, so every grid point sums its blobs in ascending blob
-// order -- the reference's order).  One CTA per tile stages the weights of its
-// blobs restricted to the tile in shared memory, accumulates its 512 points in
-// registers and writes every point of the tile exactly once (the zero-fill of
+// Tiled spreading.  The grid is cut into 8x8x8 tiles.  Once per position set
+// (set_up_gaussians) every blob's weights are also laid out on the 8-aligned
+// grid chunks its stencil meets -- per dimension four chunks of eight weights,
+// zero outside the stencil -- and every (blob, tile) overlap is listed per tile
+// as one 64-bit entry: blob id, the chunk index per dimension, the blob's
+// canonical tile index j and which halves of the tile the stencil reaches (count,
+// scan, fill, then a per-tile sort by blob id, so every grid point sums its blobs
+// in ascending blob order -- the reference's order).  One CTA per tile copies the
+// three 8-weight chunks of each of its blobs into shared memory with vector loads
+// (no index arithmetic beyond the entry), accumulates its 512 points in registers
+// and writes every point of the tile exactly once (the zero-fill of
 // fcm_fluid_solver.cpp:556-562 is fused: tiles without blobs write zeros).  No
-// atomics touch the grid.  Grids that cannot be tiled (a dimension not a
-// multiple of 8, or W + 8 > n) use the per-blob atomic scatter.
+// atomics touch the grid.  Grids that cannot be tiled (a dimension not a multiple
+// of 8, W + 8 > n, or W > 25) use the per-blob atomic scatter.
 #include <mutex>
 #include <string>
 
@@ -22,7 +27,14 @@ namespace fcm {
 namespace {
 
 constexpr int TE = 8;    // tile edge
-constexpr int SCB = 32;  // blobs staged per chunk
+constexpr int NCH = 4;   // 8-aligned chunks a stencil of at most 25 points meets per dimension
+constexpr int MAXW = 25;
+constexpr int SCB = 16;  // blobs staged per round (four staging lanes per blob, 64 threads)
+
+// Entry layout (low word): bits 0-5 chunk index per dimension (2 bits each),
+// 6-11 canonical tile index j of the blob, 12-13 / 14-15 / 16-17 x / y / z
+// halves of the tile the stencil reaches.  The blob id is the high word.
+constexpr int EJ = 6, EXM = 12, EYM = 14, EZM = 16;
 
 __device__ __forceinline__ int wrap_index(int i, int n) {
   int r = i % n;
@@ -34,9 +46,11 @@ __device__ __forceinline__ int floordiv(int a, int b) { return a >= 0 ? a / b : 
 // One thread per (blob, dimension): xc = int(Y/DX); stencil start
 // xc - W/2 + 1; weight anorm*exp(-(xg*DX - Y)^2/anorm2), with sigma = a/sqrt(pi)
 // implicit in anorm = 1/(sqrt(2) a), anorm2 = 2a^2/pi (fcm_fluid_solver.cpp:135-136).
+// With wc given, the weights are also written on the NCH 8-aligned chunks from
+// floor(base/8)*8 on (zero outside the stencil).
 template <typename T>
 __global__ void k_set_up_gaussians(const double* __restrict__ Y, int n, int W, double dx, double anorm,
-                                   double anorm2, int* __restrict__ base, T* __restrict__ w) {
+                                   double anorm2, int* __restrict__ base, T* __restrict__ w, T* __restrict__ wc) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= 3 * n) return;
   const double y = Y[t];
@@ -48,6 +62,14 @@ __global__ void k_set_up_gaussians(const double* __restrict__ Y, int n, int W, d
     const double xx = __dsub_rn(__dmul_rn((double)(b + i), dx), y);
     const double e = exp(__ddiv_rn(-__dmul_rn(xx, xx), anorm2));
     wt[i] = (T)(anorm * e);
+  }
+  if (wc) {
+    const int c0 = floordiv(b, TE) * TE;
+    T* ct = wc + (size_t)t * NCH * TE;
+    for (int i = 0; i < NCH * TE; ++i) {
+      const int s = c0 + i - b;
+      ct[i] = (s >= 0 && s < W) ? wt[s] : (T)0;
+    }
   }
 }
 
@@ -65,6 +87,12 @@ __device__ __forceinline__ void blob_tiles(const int* base, int b, const TileGeo
   }
 }
 
+// Bit h (h = 0, 1) set when the stencil [lo, lo + W) meets half h of the chunk
+// starting at s.
+__device__ __forceinline__ unsigned half_mask(int lo, int W, int s) {
+  return (lo < s + 4 && lo + W > s ? 1u : 0u) | (lo < s + 8 && lo + W > s + 4 ? 2u : 0u);
+}
+
 __global__ void k_tile_count(const int* __restrict__ base, int n, TileGeom g, int* __restrict__ count) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n) return;
@@ -80,28 +108,33 @@ __global__ void k_tile_count(const int* __restrict__ base, int n, TileGeom g, in
 }
 
 __global__ void k_tile_fill(const int* __restrict__ base, int n, TileGeom g, const int* __restrict__ offset,
-                            int* __restrict__ cursor, unsigned* __restrict__ list) {
+                            int* __restrict__ cursor, unsigned long long* __restrict__ list) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n) return;
   int f[3], cnt[3];
   blob_tiles(base, b, g, f, cnt);
+  const int lx = base[3 * b], ly = base[3 * b + 1], lz = base[3 * b + 2];
   for (int ox = 0; ox < cnt[0]; ++ox)
     for (int oy = 0; oy < cnt[1]; ++oy)
       for (int oz = 0; oz < cnt[2]; ++oz) {
         const int tile = (wrap_index(f[0] + ox, g.ntx) * g.nty + wrap_index(f[1] + oy, g.nty)) * g.ntz +
                          wrap_index(f[2] + oz, g.ntz);
         const unsigned j = (unsigned)((ox * cnt[1] + oy) * cnt[2] + oz);
-        list[offset[tile] + atomicAdd(cursor + tile, 1)] = ((unsigned)b << 6) | j;
+        const unsigned lo = (unsigned)ox | ((unsigned)oy << 2) | ((unsigned)oz << 4) | (j << EJ) |
+                            (half_mask(lx, g.W, (f[0] + ox) * TE) << EXM) |
+                            (half_mask(ly, g.W, (f[1] + oy) * TE) << EYM) |
+                            (half_mask(lz, g.W, (f[2] + oz) * TE) << EZM);
+        list[offset[tile] + atomicAdd(cursor + tile, 1)] = ((unsigned long long)b << 32) | lo;
       }
 }
 
 // Ascending blob order within each tile (a blob meets a tile at most once).
-__global__ void k_tile_sort(const int* __restrict__ offset, int ntiles, unsigned* __restrict__ list) {
+__global__ void k_tile_sort(const int* __restrict__ offset, int ntiles, unsigned long long* __restrict__ list) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ntiles) return;
   const int b = offset[t], e = offset[t + 1];
   for (int i = b + 1; i < e; ++i) {
-    const unsigned v = list[i];
+    const unsigned long long v = list[i];
     int j = i - 1;
     while (j >= b && list[j] > v) {
       list[j + 1] = list[j];
@@ -111,52 +144,89 @@ __global__ void k_tile_sort(const int* __restrict__ offset, int ntiles, unsigned
   }
 }
 
-// Stage the weights of the blobs list[c0 .. c0+nc) restricted to this tile:
-// sw[k][d][i] = weight of grid coordinate O_d + i along d (zero outside the
-// stencil) and sflag[k] bit h = the blob reaches y-half h of the tile.  One
-// thread per (blob, dimension) copies its 8-weight window.
+// Eight consecutive T from global (aligned to 8*sizeof(T)) to shared memory.
+__device__ __forceinline__ void copy8(double* dst, const double* __restrict__ src) {
+  const double2* s = reinterpret_cast<const double2*>(src);
+  double2* d = reinterpret_cast<double2*>(dst);
+  const double2 a = __ldg(s), b = __ldg(s + 1), c = __ldg(s + 2), e = __ldg(s + 3);
+  d[0] = a;
+  d[1] = b;
+  d[2] = c;
+  d[3] = e;
+}
+__device__ __forceinline__ void copy8(float* dst, const float* __restrict__ src) {
+  const float4* s = reinterpret_cast<const float4*>(src);
+  float4* d = reinterpret_cast<float4*>(dst);
+  const float4 a = __ldg(s), b = __ldg(s + 1);
+  d[0] = a;
+  d[1] = b;
+}
+
+// Stage blobs list[c0 .. c0+nc) (nc <= SCB) of a tile: lane (k, d) = (t/4, t%4)
+// copies chunk d of blob k for d < 3; lane d = 3 copies the entry's low word and,
+// when F is given, the blob's force.
 template <typename T>
-__device__ __forceinline__ void stage_weights(const unsigned* __restrict__ list, int c0, int nc,
-                                              const int* __restrict__ base, const T* __restrict__ w, const int O[3],
-                                              const int N[3], int W, T (*sw)[3][TE], int* sflag) {
-  for (int e = threadIdx.x; e < nc * 3; e += blockDim.x) {
-    const int k = e / 3, d = e - 3 * k;
-    const int b = (int)(list[c0 + k] >> 6);
-    const int Od = (d == 0) ? O[0] : ((d == 1) ? O[1] : O[2]);
-    const int Nd = (d == 0) ? N[0] : ((d == 1) ? N[1] : N[2]);
-    int s0 = (Od - base[3 * b + d]) % Nd;
-    if (s0 < 0) s0 += Nd;
-    const T* wb = w + (size_t)(3 * b + d) * W;
-    int fl = 0;
-#pragma unroll
-    for (int i = 0; i < TE; ++i) {
-      int si = s0 + i;
-      if (si >= Nd) si -= Nd;
-      const T v = (si < W) ? wb[si] : (T)0;
-      sw[k][d][i] = v;
-      if (v != (T)0) fl |= 1 << (i >> 2);
+__device__ __forceinline__ void stage_blobs(const unsigned long long* __restrict__ list, int c0, int nc,
+                                            const T* __restrict__ wc, const double* __restrict__ F,
+                                            T (*sw)[3][TE], T (*sF)[4], unsigned* sflag) {
+  const int k = threadIdx.x >> 2, d = threadIdx.x & 3;
+  if (k >= nc) return;
+  const unsigned long long e = list[c0 + k];
+  const unsigned b = (unsigned)(e >> 32), lo = (unsigned)e;
+  if (d < 3) {
+    copy8(sw[k][d], wc + ((size_t)(3 * b + d) * NCH + ((lo >> (2 * d)) & 3u)) * TE);
+  } else {
+    sflag[k] = lo;
+    if (F) {
+      sF[k][0] = (T)F[3 * (size_t)b];
+      sF[k][1] = (T)F[3 * (size_t)b + 1];
+      sF[k][2] = (T)F[3 * (size_t)b + 2];
     }
-    if (d == 1) sflag[k] = fl;
   }
+}
+
+template <typename T>
+struct V4 {};
+template <>
+struct V4<double> {
+  // two doubles
+  static __device__ __forceinline__ void ld(const double* p, double& a, double& b) {
+    const double2 v = *reinterpret_cast<const double2*>(p);
+    a = v.x;
+    b = v.y;
+  }
+};
+template <>
+struct V4<float> {
+  static __device__ __forceinline__ void ld(const float* p, float& a, float& b) {
+    const float2 v = *reinterpret_cast<const float2*>(p);
+    a = v.x;
+    b = v.y;
+  }
+};
+
+// x-weights xs..xs+3 of a staged chunk into registers.
+template <typename T>
+__device__ __forceinline__ void load_wx4(const T* row, int xs, T wx[4]) {
+  V4<T>::ld(row + xs, wx[0], wx[1]);
+  V4<T>::ld(row + xs + 2, wx[2], wx[3]);
 }
 
 // Tiled spreading: one CTA (64 threads) per 8x8x8 tile.  Thread t owns the
 // x-column (y, z) = (t/8, t%8) of the tile, eight points with three components
-// accumulated in registers; warp h covers y-half h and skips blobs whose
-// stencil misses it (a warp-uniform branch).
+// accumulated in registers.  Warp h covers y-half h and skips blobs whose
+// stencil misses it; an x-half the stencil misses is skipped by the whole CTA
+// (both branches are uniform).
 template <typename T>
-__global__ void __launch_bounds__(64) k_spread_tiled(const int* __restrict__ base, const T* __restrict__ w,
-                                                     const double* __restrict__ F, TileGeom g,
-                                                     const int* __restrict__ offset,
-                                                     const unsigned* __restrict__ list, long long G,
+__global__ void __launch_bounds__(64) k_spread_tiled(const T* __restrict__ wc, const double* __restrict__ F,
+                                                     TileGeom g, const int* __restrict__ offset,
+                                                     const unsigned long long* __restrict__ list, long long G,
                                                      T* __restrict__ grid) {
-  __shared__ T sw[SCB][3][TE];
-  __shared__ T sF[SCB][3];
-  __shared__ int sflag[SCB];
+  __shared__ __align__(16) T sw[SCB][3][TE];
+  __shared__ __align__(16) T sF[SCB][4];
+  __shared__ unsigned sflag[SCB];
   const int tile = blockIdx.x;
   const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
-  const int O[3] = {tx * TE, ty * TE, tz * TE};
-  const int N[3] = {g.nx, g.ny, g.nz};
   const int t = threadIdx.x;
   const int z = t & 7, y = t >> 3, yh = t >> 5;
   T acc[TE][3];
@@ -168,103 +238,114 @@ __global__ void __launch_bounds__(64) k_spread_tiled(const int* __restrict__ bas
   for (int c0 = b0; c0 < b1; c0 += SCB) {
     const int nc = min(SCB, b1 - c0);
     if (c0 != b0) __syncthreads();
-    stage_weights<T>(list, c0, nc, base, w, O, N, g.W, sw, sflag);
-    for (int e = t; e < nc * 3; e += 64) {
-      const int k = e / 3, c = e - 3 * k;
-      sF[k][c] = (T)F[3 * (size_t)(list[c0 + k] >> 6) + c];
-    }
+    stage_blobs<T>(list, c0, nc, wc, F, sw, sF, sflag);
     __syncthreads();
     for (int k = 0; k < nc; ++k) {
-      if (!((sflag[k] >> yh) & 1)) continue;
+      const unsigned fl = sflag[k];
+      if (!((fl >> (EYM + yh)) & 1u)) continue;
       const T wyz = sw[k][1][y] * sw[k][2][z];
       const T f0 = sF[k][0] * wyz, f1 = sF[k][1] * wyz, f2 = sF[k][2] * wyz;
 #pragma unroll
-      for (int x = 0; x < TE; ++x) {
-        const T wx = sw[k][0][x];
-        acc[x][0] += f0 * wx;
-        acc[x][1] += f1 * wx;
-        acc[x][2] += f2 * wx;
+      for (int h = 0; h < 2; ++h) {
+        if (!((fl >> (EXM + h)) & 1u)) continue;
+        T wx[4];
+        load_wx4<T>(sw[k][0], 4 * h, wx);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          acc[4 * h + i][0] += f0 * wx[i];
+          acc[4 * h + i][1] += f1 * wx[i];
+          acc[4 * h + i][2] += f2 * wx[i];
+        }
       }
     }
   }
+  const int ox = tx * TE, oy = ty * TE + y, oz = tz * TE + z;
 #pragma unroll
   for (int x = 0; x < TE; ++x) {
-    const long long idx = ((long long)(O[0] + x) * g.ny + (O[1] + y)) * g.nz + (O[2] + z);
+    const long long idx = ((long long)(ox + x) * g.ny + oy) * g.nz + oz;
     grid[idx] = acc[x][0];
     grid[G + idx] = acc[x][1];
     grid[2 * G + idx] = acc[x][2];
   }
 }
 
-// Sum of v[0..31] over the 32 lanes of a warp, scattered: afterwards lane l
-// holds in v[0] the warp total of value l (31 shuffles for 32 values).
+// Sum of v[0..15] over the 32 lanes of a warp, scattered: afterwards lanes 2i
+// and 2i+1 hold in v[0] the warp total of value i (16 shuffles for 16 values).
 template <typename T>
-__device__ __forceinline__ T warp_reduce_scatter32(T v[32], int lane) {
+__device__ __forceinline__ T warp_reduce_scatter16(T v[16], int lane) {
 #pragma unroll
-  for (int off = 16; off >= 1; off >>= 1) {
+  for (int off = 16, m = 8; off >= 2; off >>= 1, m >>= 1) {
     const bool upper = (lane & off) != 0;
 #pragma unroll
-    for (int i = 0; i < off; ++i) {
-      const T send = upper ? v[i] : v[i + off];
-      const T keep = upper ? v[i + off] : v[i];
+    for (int i = 0; i < m; ++i) {
+      const T send = upper ? v[i] : v[i + m];
+      const T keep = upper ? v[i + m] : v[i];
       v[i] = keep + __shfl_xor_sync(0xffffffffu, send, off);
     }
   }
-  return v[0];
+  return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
 }
 
 // Tiled interpolation: one CTA (64 threads) per 8x8x8 tile.  Thread (y, z) =
 // (t/8, t%8) loads the eight points of its x-column (three components) into
-// registers once.  Blobs are taken eight at a time: each thread forms
-// wyz * sum_x wx * u for the blobs its warp's y-half meets, the warp reduces the
-// 8x(3+1) values with one scatter-reduction, the two warps' sums are added in
-// shared memory, and the per-(blob, tile) partial goes to partial[blob][j][3];
-// k_interp_reduce then sums a blob's partials in j order (deterministic, no
-// atomics).
+// registers once.  Blobs are taken four at a time: each thread forms
+// wyz * sum_x wx * u for the blobs its warp's y-half meets (x-halves the
+// stencil misses are skipped), the warp reduces the 4x(3+1) values with one
+// scatter-reduction, the two warps' sums are added in shared memory, and the
+// per-(blob, tile) partial goes to partial[blob][j][3]; k_interp_reduce then
+// sums a blob's partials in j order (deterministic, no atomics).
 template <typename T>
-__global__ void __launch_bounds__(64) k_interp_tiled(const int* __restrict__ base, const T* __restrict__ w,
-                                                     const T* __restrict__ grid, TileGeom g,
-                                                     const int* __restrict__ offset,
-                                                     const unsigned* __restrict__ list, long long G,
+__global__ void __launch_bounds__(64) k_interp_tiled(const T* __restrict__ wc, const T* __restrict__ grid,
+                                                     TileGeom g, const int* __restrict__ offset,
+                                                     const unsigned long long* __restrict__ list, long long G,
                                                      T* __restrict__ partial) {
-  __shared__ T sw[SCB][3][TE];
-  __shared__ int sflag[SCB];
-  __shared__ T sred[2][32];
+  __shared__ __align__(16) T sw[SCB][3][TE];
+  __shared__ unsigned sflag[SCB];
+  __shared__ unsigned sblob[SCB];
+  __shared__ T sred[SCB / 4][2][16];
   const int tile = blockIdx.x;
   const int b0 = offset[tile], b1 = offset[tile + 1];
   if (b0 == b1) return;  // no blob meets this tile (uniform over the CTA)
   const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
-  const int O[3] = {tx * TE, ty * TE, tz * TE};
-  const int N[3] = {g.nx, g.ny, g.nz};
   const int t = threadIdx.x;
   const int z = t & 7, y = t >> 3, yh = t >> 5, lane = t & 31;
   T u[TE][3];
+  {
+    const int ox = tx * TE, oy = ty * TE + y, oz = tz * TE + z;
 #pragma unroll
-  for (int x = 0; x < TE; ++x) {
-    const long long idx = ((long long)(O[0] + x) * g.ny + (O[1] + y)) * g.nz + (O[2] + z);
-    u[x][0] = grid[idx];
-    u[x][1] = grid[G + idx];
-    u[x][2] = grid[2 * G + idx];
+    for (int x = 0; x < TE; ++x) {
+      const long long idx = ((long long)(ox + x) * g.ny + oy) * g.nz + oz;
+      u[x][0] = grid[idx];
+      u[x][1] = grid[G + idx];
+      u[x][2] = grid[2 * G + idx];
+    }
   }
   for (int c0 = b0; c0 < b1; c0 += SCB) {
     const int nc = min(SCB, b1 - c0);
     if (c0 != b0) __syncthreads();
-    stage_weights<T>(list, c0, nc, base, w, O, N, g.W, sw, sflag);
+    stage_blobs<T>(list, c0, nc, wc, nullptr, sw, nullptr, sflag);
+    if ((t & 3) == 3 && (t >> 2) < nc) sblob[t >> 2] = (unsigned)(list[c0 + (t >> 2)] >> 32);
     __syncthreads();
-    for (int k0 = 0; k0 < nc; k0 += 8) {
-      T v[32];
+    for (int k0 = 0; k0 < nc; k0 += 4) {
+      T v[16];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
+      for (int j = 0; j < 4; ++j) {
         const int k = k0 + j;
         T p0 = 0, p1 = 0, p2 = 0;
-        if (k < nc && ((sflag[k] >> yh) & 1)) {
+        const unsigned fl = k < nc ? sflag[k] : 0u;
+        if ((fl >> (EYM + yh)) & 1u) {
           T s0 = 0, s1 = 0, s2 = 0;
 #pragma unroll
-          for (int x = 0; x < TE; ++x) {
-            const T wx = sw[k][0][x];
-            s0 += wx * u[x][0];
-            s1 += wx * u[x][1];
-            s2 += wx * u[x][2];
+          for (int h = 0; h < 2; ++h) {
+            if (!((fl >> (EXM + h)) & 1u)) continue;
+            T wx[4];
+            load_wx4<T>(sw[k][0], 4 * h, wx);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              s0 += wx[i] * u[4 * h + i][0];
+              s1 += wx[i] * u[4 * h + i][1];
+              s2 += wx[i] * u[4 * h + i][2];
+            }
           }
           const T wyz = sw[k][1][y] * sw[k][2][z];
           p0 = s0 * wyz;
@@ -276,17 +357,17 @@ __global__ void __launch_bounds__(64) k_interp_tiled(const int* __restrict__ bas
         v[4 * j + 2] = p2;
         v[4 * j + 3] = 0;
       }
-      const T r = warp_reduce_scatter32<T>(v, lane);
-      sred[yh][lane] = r;
-      __syncthreads();
-      if (t < 32) {
-        const int j = t >> 2, c = t & 3, k = k0 + j;
-        if (c < 3 && k < nc) {
-          const unsigned e = list[c0 + k];
-          partial[((size_t)(e >> 6) * 64 + (e & 63u)) * 3 + c] = sred[0][t] + sred[1][t];
-        }
+      const T r = warp_reduce_scatter16<T>(v, lane);
+      if (!(lane & 1)) sred[k0 >> 2][yh][lane >> 1] = r;
+    }
+    __syncthreads();
+    // thread t: group t/16 of four blobs, value t%16 = (blob, component)
+    {
+      const int grp = t >> 4, i = t & 15, c = i & 3, k = 4 * grp + (i >> 2);
+      if (c < 3 && k < nc) {
+        const unsigned jt = (sflag[k] >> EJ) & 63u;
+        partial[((size_t)sblob[k] * 64 + jt) * 3 + c] = sred[grp][0][i] + sred[grp][1][i];
       }
-      __syncthreads();
     }
   }
 }
@@ -403,7 +484,7 @@ int blob_table_alloc(BlobTable<T>& t, int n, int W, const GridDims& g) {
   FCM_CUDA(cudaMalloc(&t.base, sizeof(int) * 3 * (size_t)(n > 0 ? n : 1)));
   FCM_CUDA(cudaMalloc(&t.w, sizeof(T) * 3 * (size_t)W * (n > 0 ? n : 1)));
   const bool ok = g.nx % TE == 0 && g.ny % TE == 0 && g.nz % TE == 0 && W + TE <= g.nx && W + TE <= g.ny &&
-                  W + TE <= g.nz && n < (1 << 26);
+                  W + TE <= g.nz && W <= MAXW && n < (1 << 30);
   if (ok) {
     t.tiled = true;
     t.ntx = g.nx / TE;
@@ -412,10 +493,11 @@ int blob_table_alloc(BlobTable<T>& t, int n, int W, const GridDims& g) {
     t.ntiles = t.ntx * t.nty * t.ntz;
     const long long per = (long long)((W + TE - 2) / TE + 1);
     t.tile_cap = (long long)(n > 0 ? n : 1) * per * per * per;
+    FCM_CUDA(cudaMalloc(&t.wc, sizeof(T) * 3 * NCH * TE * (size_t)(n > 0 ? n : 1)));
     FCM_CUDA(cudaMalloc(&t.tile_count, sizeof(int) * (size_t)t.ntiles));
     FCM_CUDA(cudaMalloc(&t.tile_offset, sizeof(int) * ((size_t)t.ntiles + 1)));
     FCM_CUDA(cudaMalloc(&t.tile_cursor, sizeof(int) * (size_t)t.ntiles));
-    FCM_CUDA(cudaMalloc(&t.tile_list, sizeof(unsigned) * (size_t)t.tile_cap));
+    FCM_CUDA(cudaMalloc(&t.tile_list, sizeof(unsigned long long) * (size_t)t.tile_cap));
     FCM_CUDA(cudaMalloc(&t.partial, sizeof(T) * 64 * 3 * (size_t)(n > 0 ? n : 1)));
   }
   return FCM_OK;
@@ -425,6 +507,7 @@ template <typename T>
 void blob_table_free(BlobTable<T>& t) {
   cudaFree(t.base);
   cudaFree(t.w);
+  cudaFree(t.wc);
   cudaFree(t.tile_count);
   cudaFree(t.tile_offset);
   cudaFree(t.tile_cursor);
@@ -441,7 +524,8 @@ int launch_set_up_gaussians(const Ctx& c, BlobTable<T>& t, const double* dY, cud
   const double anorm = 1.0 / (sqrt(2.0) * a);
   const double anorm2 = 2.0 * a * a / PI;
   const int nt = 3 * t.n;
-  k_set_up_gaussians<T><<<(nt + 127) / 128, 128, 0, s>>>(dY, t.n, t.W, c.g.dx, anorm, anorm2, t.base, t.w);
+  k_set_up_gaussians<T><<<(nt + 127) / 128, 128, 0, s>>>(dY, t.n, t.W, c.g.dx, anorm, anorm2, t.base, t.w,
+                                                          t.tiled ? t.wc : nullptr);
   FCM_LAUNCH_CHECK();
   if (t.tiled) {
     const TileGeom g = tile_geom(c.g, t.W);
@@ -461,8 +545,8 @@ int launch_set_up_gaussians(const Ctx& c, BlobTable<T>& t, const double* dY, cud
 template <typename T>
 int launch_spread(const Ctx& c, const BlobTable<T>& t, const double* dF, T* grid, cudaStream_t s) {
   if (t.tiled) {
-    k_spread_tiled<T><<<t.ntiles, 64, 0, s>>>(t.base, t.w, dF, tile_geom(c.g, t.W), t.tile_offset, t.tile_list,
-                                               c.g.G, grid);
+    k_spread_tiled<T><<<t.ntiles, 64, 0, s>>>(t.wc, dF, tile_geom(c.g, t.W), t.tile_offset, t.tile_list, c.g.G,
+                                               grid);
     FCM_LAUNCH_CHECK();
     return FCM_OK;
   }
@@ -479,7 +563,7 @@ int launch_interp(const Ctx& c, const BlobTable<T>& t, const T* grid, double* dV
   const double dx3 = c.g.dx * c.g.dx * c.g.dx;
   if (t.tiled) {
     const TileGeom g = tile_geom(c.g, t.W);
-    k_interp_tiled<T><<<t.ntiles, 64, 0, s>>>(t.base, t.w, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial);
+    k_interp_tiled<T><<<t.ntiles, 64, 0, s>>>(t.wc, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial);
     FCM_LAUNCH_CHECK();
     k_interp_reduce<T><<<(t.n + 127) / 128, 128, 0, s>>>(t.base, t.partial, t.n, g, dx3, dV);
     FCM_LAUNCH_CHECK();
@@ -518,7 +602,7 @@ namespace {
 constexpr int NA_MAX_BLOBS = 8192;
 constexpr int NA_MAX_W = 24;
 constexpr int NA_MAX_TILES = 32768;
-constexpr size_t NA_SCRATCH_BYTES = (size_t)20 << 20;  // 20 MiB
+constexpr size_t NA_SCRATCH_BYTES = (size_t)32 << 20;  // 32 MiB
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_SCRATCH_BYTES];
 
@@ -604,14 +688,16 @@ extern "C" int fcm_interp_noalloc(int32_t nx, int32_t ny, int32_t nz, double dx,
   p += round256(sizeof(int) * 3 * (size_t)n);
   double* s_w = (double*)p;
   p += round256(sizeof(double) * 3 * (size_t)W * n);
+  double* s_wc = (double*)p;
+  p += round256(sizeof(double) * 3 * NCH * TE * (size_t)n);
   int* s_count = (int*)p;
   p += round256(sizeof(int) * (size_t)ntiles);
   int* s_offset = (int*)p;
   p += round256(sizeof(int) * ((size_t)ntiles + 1));
   int* s_cursor = (int*)p;
   p += round256(sizeof(int) * (size_t)ntiles);
-  unsigned* s_list = (unsigned*)p;
-  p += round256(sizeof(unsigned) * cap);
+  unsigned long long* s_list = (unsigned long long*)p;
+  p += round256(sizeof(unsigned long long) * cap);
   double* s_partial = (double*)p;
   p += round256(sizeof(double) * 64 * 3 * (size_t)n);
   if ((size_t)(p - (unsigned char*)base_ptr) > NA_SCRATCH_BYTES) {
@@ -627,7 +713,7 @@ extern "C" int fcm_interp_noalloc(int32_t nx, int32_t ny, int32_t nz, double dx,
   // the array keeps the previous call's contents: counters start at zero
   FCM_CUDA(cudaMemsetAsync(s_count, 0, sizeof(int) * (size_t)ntiles, s));
   FCM_CUDA(cudaMemsetAsync(s_cursor, 0, sizeof(int) * (size_t)ntiles, s));
-  k_set_up_gaussians<double><<<(3 * n + 127) / 128, 128, 0, s>>>(Y, n, W, dx, anorm, anorm2, s_base, s_w);
+  k_set_up_gaussians<double><<<(3 * n + 127) / 128, 128, 0, s>>>(Y, n, W, dx, anorm, anorm2, s_base, s_w, s_wc);
   FCM_LAUNCH_CHECK();
   k_tile_count<<<(n + 127) / 128, 128, 0, s>>>(s_base, n, g, s_count);
   FCM_LAUNCH_CHECK();
@@ -636,7 +722,7 @@ extern "C" int fcm_interp_noalloc(int32_t nx, int32_t ny, int32_t nz, double dx,
   FCM_LAUNCH_CHECK();
   k_tile_sort<<<(unsigned)((ntiles + 127) / 128), 128, 0, s>>>(s_offset, (int)ntiles, s_list);
   FCM_LAUNCH_CHECK();
-  k_interp_tiled<double><<<(unsigned)ntiles, 64, 0, s>>>(s_base, s_w, grid, g, s_offset, s_list, G, s_partial);
+  k_interp_tiled<double><<<(unsigned)ntiles, 64, 0, s>>>(s_wc, grid, g, s_offset, s_list, G, s_partial);
   FCM_LAUNCH_CHECK();
   k_interp_reduce<double><<<(n + 127) / 128, 128, 0, s>>>(s_base, s_partial, n, g, dx * dx * dx, V);
   FCM_LAUNCH_CHECK();

@@ -5,7 +5,8 @@
 //   real grid    T[3][nx][ny][nz]        (component-major, z fastest, unpadded)
 //   spectrum     complex T[3][nx][ny][nzh], nzh = nz/2+1 (cuFFT R2C layout)
 //   blob tables  base int[Nb][3] (first stencil point per dim, unwrapped),
-//                weights T[Nb][3][W]
+//                weights T[Nb][3][W], and the same weights on the four
+//                8-aligned grid chunks the stencil meets, T[Nb][3][4][8]
 //   system vecs  double[3Nb + 6M]       ([lambda ; U], as the reference)
 #pragma once
 
@@ -96,10 +97,11 @@ struct BlobTable {
   // W + tile edge <= n (a stencil never meets the same tile twice).
   bool tiled = false;
   int ntx = 0, nty = 0, ntz = 0, ntiles = 0;
+  T* wc = nullptr;                // [n][3][4][8] weights on the 8-aligned grid chunks a stencil meets
   int* tile_count = nullptr;      // [ntiles]
   int* tile_offset = nullptr;     // [ntiles+1] exclusive offsets
   int* tile_cursor = nullptr;     // [ntiles]
-  unsigned* tile_list = nullptr;  // [cap] (blob << 6) | j, j = canonical tile index of the blob
+  unsigned long long* tile_list = nullptr;  // [cap] (blob << 32) | chunk indices, j and half masks
   long long tile_cap = 0;
   T* partial = nullptr;           // [n][64][3] per-(blob, tile) interpolation partials
 };
@@ -118,6 +120,18 @@ struct GridBufs {
 
 // Tile shape of the tiled spread / interpolation kernels.
 constexpr int TILE_X = 8, TILE_Y = 8, TILE_Z = 8;
+
+// Record of one device-resident (graph) time step, written by the device.
+struct StepRecord {
+  int iters;     // GMRES iterations, summed over refinement sweeps
+  int sweeps;    // refinement sweeps (1 for an FP64 solve)
+  int status;    // FCM_OK / FCM_ERR_NOT_CONVERGED / FCM_ERR_NONFINITE
+  int guard;     // iterations of the loop in progress (bounds every device loop)
+  double rel;    // final relative residual
+  double divU;   // GDC divergence term (0 for EM or without noise)
+  double normb;  // ||RHS|| of the refinement
+  double relr;   // refinement residual of the last sweep
+};
 
 // Device-resident state of one GMRES solve (gmres_solver.cpp:148-306).
 struct GmState {
@@ -175,6 +189,20 @@ struct Ctx {
   cudaStream_t cap_stream = 0;  // private stream for graph capture
   cudaGraphExec_t iter_graph[2] = {nullptr, nullptr};  // one Arnoldi iteration, per precision
   long long iter_graph_kernels[2] = {0, 0};           // kernels in each graph
+  // device-resident step: the whole step as one graph with conditional loops
+  StepRecord* d_step = nullptr;     // written by the step's kernels
+  StepRecord* h_step = nullptr;     // pinned copy, the graph's last node
+  uint64_t* d_stepargs = nullptr;   // (seed, counter) of the step in flight
+  uint64_t* h_stepargs = nullptr;   // pinned staging of d_stepargs
+  double* d_rs = nullptr;           // [0] ||b|| [1] ||r|| [2] inner tolerance [3] nu
+  cudaStream_t cap_body[2] = {0, 0};  // capture streams of the loop bodies
+  cudaGraphExec_t step_graph = nullptr;
+  int step_graph_state = 0;         // 0 not built yet, 1 built, -1 unavailable (host-driven steps)
+  long long step_kernels_top = 0, step_kernels_sweep = 0, step_kernels_iter = 0;
+  bool step_pending = false;        // fcm_step_async issued, fcm_step_wait not yet called
+  bool step_pending_graph = false;  // ... and it was a graph launch
+  int step_pending_status = 0;      // host-driven pending step: its status and record
+  fcm_step_info step_pending_info{};
   // cells
   int ncell_total = 0;
   int *d_cell = nullptr, *d_cell_start = nullptr, *d_cell_count = nullptr, *d_cell_sorted = nullptr, *d_cell_cursor = nullptr;
@@ -209,8 +237,10 @@ int launch_interp(const Ctx& c, const BlobTable<T>& t, const T* grid, double* dV
 // k-space (fcm_kspace.cu)
 template <typename T>
 int launch_project(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s);
+// (seed, counter) are read from d_args[0..1] instead when d_args is given.
 template <typename T>
-int launch_noise_kspace(const Ctx& c, typename cplx_t<T>::type* spec, uint64_t seed, uint64_t counter, cudaStream_t s);
+int launch_noise_kspace(const Ctx& c, typename cplx_t<T>::type* spec, uint64_t seed, uint64_t counter,
+                        const uint64_t* d_args, cudaStream_t s);
 int launch_stress_divergence_project(const Ctx& c, const cufftDoubleComplex* sigma6, cufftDoubleComplex* spec, cudaStream_t s);
 int launch_unpad_copy(const double* src_padded, double* dst, int nx, int ny, int nz, int pad, int ncomp_stride_dst, cudaStream_t s);
 // bodies (fcm_bodies.cu)
@@ -219,7 +249,9 @@ int launch_multiply_K(const Ctx& c, const double* qm, const double* in6, double*
 int launch_multiply_KT(const Ctx& c, const double* qm, const double* in3, double* out6, double scale, const double* add6, double add_scale, cudaStream_t s);
 int launch_pinv(const Ctx& c, const double* qm, const double* in, double* out, cudaStream_t s);
 int launch_rigid_projection(const Ctx& c, const double* q, const double* V, double* U6, cudaStream_t s);
-int launch_body_update(const Ctx& c, double* x, double* q, const double* U6, double scale, cudaStream_t s);
+// U scaled by `scale`, times *d_nu when d_nu is given.
+int launch_body_update(const Ctx& c, double* x, double* q, const double* U6, double scale, cudaStream_t s,
+                       const double* d_nu = nullptr);
 int launch_body_update_uniform(const Ctx& c, double* x, double* q, const double* e6, cudaStream_t s);
 int launch_divU_accumulate(const Ctx& c, const double* U6, const double* U0, int component, double delta, double* acc, cudaStream_t s);
 int launch_exclusive_scan(const int* in, int* out, int n, cudaStream_t s);
@@ -239,7 +271,8 @@ int blas_norm_sq_partial(const Ctx& c, const double* a, long long n, double* d_o
 int blas_f64_to_f32(float* dst, const double* src, long long n, cudaStream_t s);
 int blas_sum_accumulate(const Ctx& c, const double* a, long long n, double* d_out, cudaStream_t s);
 // device-side GMRES pieces (fcm_blas.cu)
-int gm_init(const Ctx& c, const double* b, double tol, int maxit, cudaStream_t s);
+// tol is read from *d_tol instead when d_tol is given.
+int gm_init(const Ctx& c, const double* b, double tol, int maxit, cudaStream_t s, const double* d_tol = nullptr);
 int gm_fetch(const Ctx& c, double* dst, cudaStream_t s);
 int gm_orthogonalize(const Ctx& c, double* w, cudaStream_t s);
 int gm_finish(const Ctx& c, double* soln_pre, cudaStream_t s);

@@ -209,9 +209,13 @@ __device__ __forceinline__ void mode_normals(unsigned long long m, uint64_t seed
 // s(-k) = conj(s(k)); the Fourier-space draw reproduces exactly that law.
 template <typename T, typename C, int SOURCE>
 __global__ void k_fluct(C* __restrict__ spec, const cufftDoubleComplex* __restrict__ sig, KParams k, uint64_t seed,
-                        uint64_t counter, double amp_diag, double amp_off) {
+                        uint64_t counter, const uint64_t* __restrict__ dargs, double amp_diag, double amp_off) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= k.Gc) return;
+  if (dargs) {  // (seed, counter) from device memory (a captured step reads them there)
+    seed = dargs[0];
+    counter = dargs[1];
+  }
   int x, y, kz;
   mode_coords(t, k, x, y, kz);
   const bool plane = is_plane(kz, k);
@@ -324,13 +328,14 @@ static void stress_amplitudes(const Ctx& c, double& diag, double& off) {
 }
 
 template <typename T>
-int launch_noise_kspace(const Ctx& c, typename cplx_t<T>::type* spec, uint64_t seed, uint64_t counter, cudaStream_t s) {
+int launch_noise_kspace(const Ctx& c, typename cplx_t<T>::type* spec, uint64_t seed, uint64_t counter,
+                        const uint64_t* d_args, cudaStream_t s) {
   const KParams k = make_kparams(c);
   double ad, ao;
   stress_amplitudes(c, ad, ao);
   const int nt = 256;
   k_fluct<T, typename cplx_t<T>::type, 1><<<(unsigned)((k.Gc + nt - 1) / nt), nt, 0, s>>>(spec, nullptr, k, seed,
-                                                                                          counter, ad, ao);
+                                                                                          counter, d_args, ad, ao);
   FCM_LAUNCH_CHECK();
   return FCM_OK;
 }
@@ -339,15 +344,16 @@ int launch_stress_divergence_project(const Ctx& c, const cufftDoubleComplex* sig
                                      cudaStream_t s) {
   const KParams k = make_kparams(c);
   const int nt = 256;
-  k_fluct<double, cufftDoubleComplex, 0><<<(unsigned)((k.Gc + nt - 1) / nt), nt, 0, s>>>(spec, sigma6, k, 0, 0, 0,
-                                                                                         0);
+  k_fluct<double, cufftDoubleComplex, 0><<<(unsigned)((k.Gc + nt - 1) / nt), nt, 0, s>>>(spec, sigma6, k, 0, 0,
+                                                                                         nullptr, 0, 0);
   FCM_LAUNCH_CHECK();
   return FCM_OK;
 }
 
 template int launch_project<double>(const Ctx&, cufftDoubleComplex*, cudaStream_t);
 template int launch_project<float>(const Ctx&, cufftComplex*, cudaStream_t);
-template int launch_noise_kspace<double>(const Ctx&, cufftDoubleComplex*, uint64_t, uint64_t, cudaStream_t);
-template int launch_noise_kspace<float>(const Ctx&, cufftComplex*, uint64_t, uint64_t, cudaStream_t);
+template int launch_noise_kspace<double>(const Ctx&, cufftDoubleComplex*, uint64_t, uint64_t, const uint64_t*,
+                                         cudaStream_t);
+template int launch_noise_kspace<float>(const Ctx&, cufftComplex*, uint64_t, uint64_t, const uint64_t*, cudaStream_t);
 
 }  // namespace fcm

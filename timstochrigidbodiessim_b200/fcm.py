@@ -234,6 +234,19 @@ class Suspension:
         self._c(self.L.fcm_apply_mobility(self.h, p, po), "fcm_apply_mobility")
         return V
 
+    # The stages of apply_mobility one at a time, on the FP64 (0) or FP32 (1) grid.
+    def spread(self, F, precision=0):
+        k, p = _in(F, 3 * self.Nb)
+        self._c(self.L.fcm_spread(self.h, precision, p), "fcm_spread")
+
+    def stokes_solve(self, precision=0):
+        self._c(self.L.fcm_stokes_solve(self.h, precision), "fcm_stokes_solve")
+
+    def interp(self, precision=0, out=None):
+        V, po = _out(out, 3 * self.Nb)
+        self._c(self.L.fcm_interp(self.h, precision, po), "fcm_interp")
+        return V
+
     def produce_reference_matrices(self):
         self._c(self.L.fcm_produce_reference_matrices(self.h), "fcm_produce_reference_matrices")
 
@@ -293,6 +306,30 @@ class Suspension:
         st = self.L.fcm_step(self.h, seed, step_index, ctypes.byref(info))
         self._c(st, "fcm_step", ok=(0, 7))
         return st, info
+
+    def step_async(self, seed, step_index):
+        """Issue a step without waiting (a CUDA-graph launch after the first step)."""
+        self._c(self.L.fcm_step_async(self.h, seed, step_index), "fcm_step_async")
+
+    def step_wait(self):
+        """Wait for the step issued by step_async; returns (status, FcmStepInfo)."""
+        info = FcmStepInfo()
+        st = self.L.fcm_step_wait(self.h, ctypes.byref(info))
+        self._c(st, "fcm_step_wait", ok=(0, 7))
+        return st, info
+
+
+def step_many(suspensions, seeds, step_index):
+    """One step of each suspension (fcm_step_many): all issued, then all awaited.
+    Returns the list of FcmStepInfo."""
+    n = len(suspensions)
+    L = suspensions[0].L if n else capi.load()
+    hs = (ctypes.c_void_p * n)(*[s.h.value for s in suspensions])
+    sd = (ctypes.c_uint64 * n)(*[int(x) for x in seeds])
+    infos = (FcmStepInfo * n)()
+    st = L.fcm_step_many(hs, n, sd, step_index, infos)
+    capi.check(st, "fcm_step_many", (0,))
+    return list(infos)
 
 
 class fft_solver:
