@@ -450,34 +450,51 @@ def run_kernels_only(args):
 def run_ensemble(args):
     """Batched ensemble of 64 independent suspensions (seeds 0..63).  Plain FP64
     GPU path: the instances one after another on one stream, host-driven steps
-    (fcm_step).  Also timed, for reference: the same FP64 instances with
-    device-resident (graph) steps, still one after another.  Mixed-precision
-    batched path: every instance on its own CUDA stream, one step of all of them
-    per fcm_step_many call (one CUDA-graph launch per instance, the GMRES loops on
-    the device), so their kernels overlap on the GPU.  Device time: events on a
-    root stream that every instance stream joins."""
+    (fcm_step).  Mixed-precision batched path: one fcm_batch of the 64 instances
+    (per-instance work as concurrent graph branches, the solves in lockstep as
+    batched kernels, one CUDA graph per step).  Also timed, for reference: FP64
+    device-resident graph steps one instance after another, and the mixed
+    instances as 64 contexts on 64 streams (fcm_step_many).  Device time: events
+    on a root stream that every instance stream joins."""
     os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")  # streams -> hardware queues
     from timstochrigidbodiessim_b200 import configs
     insts = configs.ensemble(64, workers=min(16, os.cpu_count() or 1))  # before any CUDA call
     import torch
     from timstochrigidbodiessim_b200 import capi
-    from timstochrigidbodiessim_b200.fcm import step_many
+    from timstochrigidbodiessim_b200.fcm import Batch, step_many
     torch.cuda.set_device(0)
     lib = capi.load()
     root = torch.cuda.current_stream()
     total_bodies = sum(p.num_bodies for p, *_ in insts)
     seeds = list(range(len(insts)))
     res = {}
-    for tag, prec, mode in (("fp64", 0, "host"), ("fp64_graph", 0, "graph"), ("mixed", 1, "many")):
+    modes = (("fp64", 0, "host"), ("fp64_graph", 0, "graph"), ("mixed_streams", 1, "many"), ("mixed", 1, "batch"))
+    for tag, prec, mode in modes:
         streams = [torch.cuda.Stream() for _ in insts] if mode == "many" else [torch.cuda.Stream()] * len(insts)
-        ss = []
-        for (p, ref, x, q, fe), st in zip(insts, streams):
-            pp = p.copy(precision=prec)
-            if prec == 1:
+        batch = None
+        if mode == "batch":
+            pps = []
+            for p, ref, x, q, fe in insts:
+                pp = p.copy(precision=prec)
                 pp.gmres_tol = MIXED_TOL
-            ss.append(setup_suspension(pp, ref, x, q, fe, st))
+                pps.append((pp, ref))
+            batch = Batch(pps, stream=streams[0])
+            for m, (p, ref, x, q, fe) in zip(batch.members, insts):
+                m.set_bodies(x, q)
+                m.set_external_forces(fe)
+                m.produce_reference_matrices()
+            ss = batch.members
+        else:
+            ss = []
+            for (p, ref, x, q, fe), st in zip(insts, streams):
+                pp = p.copy(precision=prec)
+                if prec == 1:
+                    pp.gmres_tol = MIXED_TOL
+                ss.append(setup_suspension(pp, ref, x, q, fe, st))
         for i in range(args.warmup):
-            if mode == "many":
+            if mode == "batch":
+                batch.step(seeds, i)
+            elif mode == "many":
                 step_many(ss, seeds, i)
             else:
                 for k, s in enumerate(ss):
@@ -490,7 +507,7 @@ def run_ensemble(args):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         sampler = ClockSampler(0)
-        if mode == "many":
+        if mode == "batch":
             sampler.start()
         l0 = lib.fcm_kernel_launch_count()
         e0.record(root)
@@ -499,7 +516,9 @@ def run_ensemble(args):
         iters = []
         for j in range(args.steps):
             step = args.warmup + j
-            if mode == "many":
+            if mode == "batch":
+                iters += [inf.gmres_iters for inf in batch.step(seeds, step)]
+            elif mode == "many":
                 iters += [inf.gmres_iters for inf in step_many(ss, seeds, step)]
             else:
                 for k, s in enumerate(ss):
@@ -515,12 +534,15 @@ def run_ensemble(args):
             root.wait_event(ev)
         e1.record(root)
         e1.synchronize()
-        clocks = sampler.stop() if mode == "many" else None
+        clocks = sampler.stop() if mode == "batch" else None
         t = e0.elapsed_time(e1) / 1e3
         res[tag] = dict(t=t, iters=float(np.mean(iters)), launches=lib.fcm_kernel_launch_count() - l0,
                         clocks=clocks)
-        for s in ss:
-            s.close()
+        if batch is not None:
+            batch.close()
+        else:
+            for s in ss:
+                s.close()
     # velocity error of the mixed solve against the FP64 solve, every instance
     errs = [rel_vel_error(p, ref, x, q, fe, root) for p, ref, x, q, fe in insts]
     value = total_bodies * args.steps / res["mixed"]["t"]
@@ -533,11 +555,15 @@ def run_ensemble(args):
         "vs_baseline": None, "dtype": "f32 grid + f64 refinement", "data": "synthetic (seeded random rods, Philox noise)",
         "config": {"workload": "ensemble64_rods50-500_g64-128", "instances": len(insts), "bodies": total_bodies,
                    "grids": grids, "gmres_tol_fp64": insts[0][0].gmres_tol, "mixed_gmres_tol": MIXED_TOL,
-                   "seeds": "0..63", "parallelism": "64 instances, 1 stream each, one fcm_step_many call per step"},
+                   "seeds": "0..63",
+                   "parallelism": "one batch of 64 instances: lockstep batched solve, one CUDA graph per step"},
         "fp64": {"value": fp64, "ms_per_step": 1e3 * res["fp64"]["t"] / args.steps, "gmres_iters": res["fp64"]["iters"],
                  "mode": "instances one after another, host-driven fcm_step"},
         "fp64_graph": {"value": fp64g, "ms_per_step": 1e3 * res["fp64_graph"]["t"] / args.steps,
                        "mode": "instances one after another, device-resident graph steps"},
+        "mixed_streams": {"value": total_bodies * args.steps / res["mixed_streams"]["t"],
+                          "ms_per_step": 1e3 * res["mixed_streams"]["t"] / args.steps,
+                          "mode": "64 contexts on 64 streams, one graph per instance step (fcm_step_many)"},
         "mixed_over_fp64": value / fp64, "mixed_over_fp64_graph": value / fp64g,
         "gmres_iters_mixed": res["mixed"]["iters"],
         "rel_vel_error_mixed_vs_fp64_max": {"bodies": max(e[0] for e in errs), "blobs": max(e[1] for e in errs)},

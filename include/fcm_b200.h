@@ -267,6 +267,31 @@ int fcm_step(fcm_ctx* ctx, uint64_t seed, uint64_t step_index, fcm_step_info* in
  * synchronously). */
 int fcm_step_async(fcm_ctx* ctx, uint64_t seed, uint64_t step_index);
 int fcm_step_wait(fcm_ctx* ctx, fcm_step_info* info);
+/* Batches: n independent suspensions (members, each with its own params and
+ * blob_ref_pos; body counts and grids may differ, precision and gmres_tol are
+ * common, skip_on_overlap must be 0) stepped together.  Per-member work runs
+ * concurrently; the saddle-point solves run in lockstep as batched kernels
+ * (one spread, projection and interpolation launch over every member, one
+ * cuFFT plan per group of members with equal grids, the GMRES vector work of
+ * all members per launch), members whose solve is done being skipped, and a
+ * step is one CUDA graph whose GMRES iterations and refinement sweeps loop on
+ * the device until every member is done.  The first fcm_batch_step runs the
+ * members host-driven and captures that graph.  Each member's solve and
+ * trajectory are those of fcm_step on the same member.  No reference
+ * counterpart. */
+typedef struct fcm_batch fcm_batch;
+int fcm_batch_create(int32_t n, const fcm_params* params, const double* const* blob_ref_pos, fcm_batch** out);
+int fcm_batch_destroy(fcm_batch* b);
+/* Member i as a context (owned by the batch: set bodies, forces, reference
+ * matrices, read results through it; fcm_destroy refuses it). NULL if out of range. */
+fcm_ctx* fcm_batch_member(fcm_batch* b, int32_t i);
+/* Stream of the batch's graph launches (a cudaStream_t, 0 = legacy). */
+int fcm_batch_set_stream(fcm_batch* b, void* stream);
+/* One step of every member: seeds[i] for member i, the same step_index; infos
+ * (n records) may be NULL.  Returns FCM_OK or the first failing status (a member
+ * whose solve failed keeps its bodies). */
+int fcm_batch_step(fcm_batch* b, const uint64_t* seeds, uint64_t step_index, fcm_step_info* infos);
+
 /* One step of each of n independent suspensions (seeds[i] for context i, the
  * same step_index): all issued, then all awaited, so contexts on different
  * streams run concurrently.  infos (n records) may be NULL.  Returns FCM_OK or

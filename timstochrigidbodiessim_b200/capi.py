@@ -75,6 +75,13 @@ SIGNATURES = {
     "fcm_multiply_by_saddle_point_matrix": (ctypes.c_int, [VP, VP, VP]),
     "fcm_invert_saddle_point_system": (ctypes.c_int, [VP, VP, I32, D]),
     "fcm_step": (ctypes.c_int, [VP, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(FcmStepInfo)]),
+    "fcm_batch_create": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(FcmParams), ctypes.POINTER(VP),
+                                        ctypes.POINTER(VP)]),
+    "fcm_batch_destroy": (ctypes.c_int, [VP]),
+    "fcm_batch_member": (VP, [VP, ctypes.c_int32]),
+    "fcm_batch_set_stream": (ctypes.c_int, [VP, VP]),
+    "fcm_batch_step": (ctypes.c_int, [VP, ctypes.POINTER(ctypes.c_uint64), ctypes.c_uint64,
+                                      ctypes.POINTER(FcmStepInfo)]),
     "fcm_step_async": (ctypes.c_int, [VP, ctypes.c_uint64, ctypes.c_uint64]),
     "fcm_step_wait": (ctypes.c_int, [VP, ctypes.POINTER(FcmStepInfo)]),
     "fcm_step_many": (ctypes.c_int, [ctypes.POINTER(VP), ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64),

@@ -269,9 +269,11 @@ int ensure_grid(Ctx* c) {
 
 template <typename T>
 void free_grid(GridBufs<T>& gb) {
-  cudaFree(gb.r);
-  cudaFree(gb.c);
-  cudaFree(gb.urand);
+  if (!gb.borrowed) {
+    cudaFree(gb.r);
+    cudaFree(gb.c);
+    cudaFree(gb.urand);
+  }
   if (gb.r2c) cufftDestroy(gb.r2c);
   if (gb.c2r) cufftDestroy(gb.c2r);
   blob_table_free(gb.blobs);
@@ -1046,8 +1048,10 @@ void destroy_ctx(Ctx* c) {
   if (c->h_gm) cudaFreeHost(c->h_gm);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
-  cudaFree(c->d_step);
-  cudaFree(c->d_stepargs);
+  if (!c->in_batch) {
+    cudaFree(c->d_step);
+    cudaFree(c->d_stepargs);
+  }
   cudaFree(c->d_rs);
   if (c->h_step) cudaFreeHost(c->h_step);
   if (c->h_stepargs) cudaFreeHost(c->h_stepargs);
@@ -1341,11 +1345,697 @@ int step_wait(Ctx* c, fcm_step_info* info) {
   return FCM_OK;
 }
 
+// ------------------------------------------------------------------ batches
+// A batch steps many independent suspensions (its members) together.  The
+// per-member work of a step (blob positions, noise, Gaussian tables, cells and
+// forces, right-hand side, body update) runs as one graph branch per member;
+// the saddle-point solves run in lockstep as batched kernels: every member's
+// tiles in one spread / interpolation launch, every member's modes in one
+// projection launch, one cuFFT plan per group of members with equal grids (their
+// grids are contiguous), and the GMRES vector work of all members per launch.
+// Members whose solve has finished are skipped inside the kernels.  The step is
+// one CUDA graph whose GMRES iterations and refinement sweeps are conditional
+// loops that run until every member is done.
+struct BatchGroup {
+  int nx = 0, ny = 0, nz = 0;
+  std::vector<int> idx;                   // members
+  void* r[2] = {nullptr, nullptr};        // [precision] 3G per member, contiguous
+  void* c[2] = {nullptr, nullptr};        // 3Gc per member
+  void* urand[2] = {nullptr, nullptr};
+  cufftHandle r2c[2] = {0, 0}, c2r[2] = {0, 0};
+};
+
+struct Batch {
+  BatchGeom geom;
+  std::vector<Ctx*> m;
+  int precision = 0;
+  BMember* d_mem = nullptr;
+  int2* d_tile_map = nullptr;
+  int2* d_kblock_map = nullptr;
+  double* d_partials = nullptr;
+  unsigned* d_counter = nullptr;
+  double* d_mdpart = nullptr;
+  unsigned* d_mdcount = nullptr;
+  StepRecord* d_rec = nullptr;
+  StepRecord* h_rec = nullptr;
+  uint64_t* d_args = nullptr;
+  uint64_t* h_args = nullptr;
+  int* d_loop = nullptr;  // [0] inner-loop guard [1] inner iterations run [2] sweeps run
+  int* h_loop = nullptr;
+  std::vector<BatchGroup> groups;
+  cudaStream_t stream = 0;
+  cudaStream_t cap = 0, cap_body[2] = {0, 0};
+  std::vector<cudaStream_t> branch;
+  std::vector<cudaEvent_t> events;  // 2 forks + 2n joins
+  cudaGraphExec_t graph = nullptr;
+  int state = 0;  // 0 not built, 1 built, -1 host-driven
+  long long k_top = 0, k_sweep = 0, k_iter = 0;
+};
+
+__global__ void k_b_step_begin(const BMember* __restrict__ mem, int n, int* __restrict__ loop) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    StepRecord* sd = mem[i].sd;
+    sd->iters = 0;
+    sd->sweeps = 0;
+    sd->status = FCM_OK;
+    sd->guard = 0;
+    sd->rel = 0.0;
+    sd->divU = 0.0;
+    sd->normb = 0.0;
+    sd->relr = 1.0;
+    sd->ref_active = 0;
+  }
+  if (threadIdx.x == 0) loop[0] = loop[1] = loop[2] = 0;
+}
+
+// Lockstep GMRES loop condition: some member not done, at most `limit` rounds.
+__global__ void k_b_loop_cond(cudaGraphConditionalHandle h, const BMember* __restrict__ mem, int n,
+                              int* __restrict__ loop, int enter, int limit) {
+  __shared__ int any;
+  if (threadIdx.x == 0) {
+    any = 0;
+    if (enter) {
+      loop[0] = 0;
+    } else {
+      loop[0] += 1;
+      loop[1] += 1;
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    if (!mem[i].gm->done) atomicOr(&any, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, (any && loop[0] < limit) ? 1u : 0u);
+}
+
+__global__ void k_b_gm_record(const BMember* __restrict__ mem, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const BMember& m = mem[i];
+    m.sd->iters = m.gm->k;
+    m.sd->sweeps = 1;
+    m.sd->rel = m.gm->rel;
+    m.sd->status = m.gm->status;
+  }
+}
+
+// soln = 0, res = rhs
+__global__ void k_b_refine_start(const BMember* __restrict__ mem) {
+  const BMember& m = mem[blockIdx.y];
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= m.nsys) return;
+  m.soln[i] = 0.0;
+  m.res[i] = m.rhs[i];
+}
+
+__global__ void k_b_ref_enter(cudaGraphConditionalHandle h, const BMember* __restrict__ mem, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    StepRecord* sd = mem[i].sd;
+    sd->normb = mem[i].rs[0];
+    sd->relr = 1.0;
+    sd->sweeps = 0;
+    sd->iters = 0;
+    sd->status = FCM_OK;
+    sd->ref_active = 1;
+  }
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, n > 0 ? 1u : 0u);
+}
+
+__global__ void k_b_ref_tol(const BMember* __restrict__ mem, int n, double tol) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const BMember& m = mem[i];
+    if (m.sd->ref_active) m.rs[2] = fmin(0.5, fmax(1e-6, 0.3 * tol / m.sd->relr));
+  }
+}
+
+// k_ref_next for every member still sweeping; the loop goes on while any does.
+__global__ void k_b_ref_next(cudaGraphConditionalHandle h, const BMember* __restrict__ mem, int n, double tol,
+                             int max_sweeps, int* __restrict__ loop) {
+  __shared__ int any;
+  if (threadIdx.x == 0) {
+    any = 0;
+    loop[2] += 1;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const BMember& m = mem[i];
+    StepRecord* sd = m.sd;
+    if (!sd->ref_active) continue;
+    const GmState* gm = m.gm;
+    sd->sweeps += 1;
+    sd->iters += gm->k;
+    int go = 0;
+    if (gm->status == FCM_ERR_NONFINITE) {
+      sd->status = FCM_ERR_NONFINITE;
+      sd->rel = gm->rel;
+    } else {
+      const double relr = sd->normb > 0.0 ? m.rs[1] / sd->normb : 0.0;
+      sd->relr = relr;
+      sd->rel = relr;
+      if (!isfinite(relr)) {
+        sd->status = FCM_ERR_NONFINITE;
+      } else if (relr < tol) {
+        sd->status = FCM_OK;
+      } else {
+        sd->status = FCM_ERR_NOT_CONVERGED;
+        go = sd->sweeps < max_sweeps ? 1 : 0;
+      }
+    }
+    sd->ref_active = go;
+    if (go) atomicOr(&any, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, any ? 1u : 0u);
+}
+
+// Batched saddle-point product out = A in on the grids of precision T.
+template <typename T>
+int batch_saddle(Batch* B, int in, int out, int mask, cudaStream_t s) {
+  constexpr int P = sizeof(T) == 8 ? 0 : 1;
+  FCM_TRY(b_spread<T>(B->geom, in, mask, s));
+  for (BatchGroup& g : B->groups) {
+    FCM_CUFFT(cufftSetStream(g.r2c[P], s));
+    FCM_CUFFT(exec_r2c(g.r2c[P], (T*)g.r[P], (typename cplx_t<T>::type*)g.c[P]));
+  }
+  FCM_TRY(b_project<T>(B->geom, mask, s));
+  for (BatchGroup& g : B->groups) {
+    FCM_CUFFT(cufftSetStream(g.c2r[P], s));
+    FCM_CUFFT(exec_c2r(g.c2r[P], (typename cplx_t<T>::type*)g.c[P], (T*)g.r[P]));
+  }
+  FCM_TRY(b_interp<T>(B->geom, out, mask, s));
+  FCM_TRY(b_multiply_K_KT(B->geom, in, out, mask, s));
+  return FCM_OK;
+}
+
+// Lockstep GMRES of every member (on stream s, body captured on bs): init from
+// vector `vec`, iterations until all are done, solution P^-1 sum y_i q_i in out.
+int batch_gmres_loop(Batch* B, int prec, int vec, double tol, int use_rs, int mask, int out, cudaStream_t s,
+                     cudaStream_t bs) {
+  const BatchGeom& G = B->geom;
+  FCM_TRY(b_gm_init(G, vec, tol, use_rs, mask, s));
+  cudaGraphConditionalHandle h;
+  FCM_TRY(new_handle(s, &h));
+  const int limit = G.max_hn - 1;
+  k_b_loop_cond<<<1, 256, 0, s>>>(h, G.mem, G.n, B->d_loop, 1, limit);
+  FCM_LAUNCH_CHECK();
+  cudaGraph_t body = nullptr;
+  FCM_TRY(add_while_node(s, h, &body));
+  const long long l0 = launch_count();
+  FCM_CUDA(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  auto iteration = [&]() -> int {
+    FCM_TRY(b_gm_fetch(G, bs));
+    FCM_TRY(b_pinv(G, BV_SYS_B, BV_SYS_A, BM_GM, bs));
+    if (prec == 0) FCM_TRY(batch_saddle<double>(B, BV_SYS_A, BV_SYS_B, BM_GM, bs));
+    else FCM_TRY(batch_saddle<float>(B, BV_SYS_A, BV_SYS_B, BM_GM, bs));
+    FCM_TRY(b_gm_orthogonalize(G, bs));
+    k_b_loop_cond<<<1, 256, 0, bs>>>(h, G.mem, G.n, B->d_loop, 0, limit);
+    FCM_LAUNCH_CHECK();
+    return (int)FCM_OK;
+  };
+  const int st = iteration();
+  cudaGraph_t tmp = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(bs, &tmp);
+  if (st != FCM_OK) return st;
+  if (e2 != cudaSuccess) {
+    set_error(std::string("batch GMRES body capture: ") + cudaGetErrorString(e2));
+    return FCM_ERR_CUDA;
+  }
+  B->k_iter = launch_count() - l0;
+  FCM_TRY(b_gm_finish(G, s));
+  FCM_TRY(b_pinv(G, BV_SYS_B, out, mask == BM_REF ? BM_REF : BM_ALL, s));
+  return FCM_OK;
+}
+
+// Fork the members' branches off `s`, run fn(member index) on each branch
+// (the member's c->stream swapped to the branch), join back into `s`.
+template <typename F>
+int batch_branches(Batch* B, cudaStream_t s, int fork_id, F&& fn) {
+  const int n = B->geom.n;
+  cudaEvent_t fork = B->events[fork_id];
+  FCM_CUDA(cudaEventRecord(fork, s));
+  for (int i = 0; i < n; ++i) {
+    FCM_CUDA(cudaStreamWaitEvent(B->branch[i], fork, 0));
+    {
+      StreamSwap sw(B->m[i], B->branch[i]);
+      FCM_TRY(fn(i));
+    }
+    cudaEvent_t join = B->events[2 + (size_t)fork_id * n + i];
+    FCM_CUDA(cudaEventRecord(join, B->branch[i]));
+    FCM_CUDA(cudaStreamWaitEvent(s, join, 0));
+  }
+  return FCM_OK;
+}
+
+// The pre-solve part of a step for one member (as enqueue_resident_step).
+int member_pre_solve(Ctx* c) {
+  const bool noise = c->p.noise != 0;
+  FCM_TRY(launch_fill_blob_pos(*c, c->d_x, c->d_q, c->d_Y, c->stream));
+  if (noise) FCM_TRY(noise_dev(c, 0, 0, c->d_stepargs));
+  else c->urand_ready = false;
+  FCM_TRY(set_up_gaussians_dev(c, c->d_Y));
+  FCM_TRY(random_velocities_dev(c, c->d_V));
+  if (c->p.algorithm == 1) {
+    int ov = 0;
+    FCM_TRY(advance_to_midstep_dev(c, c->d_V, &ov));
+    double* acc = c->d_H + c->maxit_alloc + 1;
+    if (noise) FCM_TRY(divU_enqueue(c, acc));
+    k_gdc_nu<<<1, 32, 0, c->stream>>>(c->d_step, acc, noise ? 1 : 0, c->p.dt, c->d_rs + 3);
+    FCM_LAUNCH_CHECK();
+    FCM_TRY(launch_fill_blob_pos(*c, c->d_xm, c->d_qm, c->d_Y, c->stream));
+    FCM_TRY(set_up_gaussians_dev(c, c->d_Y));
+    FCM_TRY(random_velocities_dev(c, c->d_V));
+  }
+  FCM_TRY(calculate_forces_dev(c));
+  FCM_TRY(assemble_rhs_dev(c));
+  return FCM_OK;
+}
+
+int enqueue_batch_step(Batch* B, cudaStream_t s) {
+  const BatchGeom& G = B->geom;
+  const int n = G.n;
+  const long long l_start = launch_count();
+  long long l_loops = 0;
+  k_b_step_begin<<<1, 256, 0, s>>>(G.mem, n, B->d_loop);
+  FCM_LAUNCH_CHECK();
+  FCM_TRY(batch_branches(B, s, 0, [&](int i) { return member_pre_solve(B->m[i]); }));
+  const double tol = B->m[0]->p.gmres_tol;
+  if (B->precision == 0) {
+    FCM_TRY(batch_gmres_loop(B, 0, BV_RHS, tol, 0, BM_ALL, BV_SOLN, s, B->cap_body[0]));
+    l_loops += B->k_iter;
+    B->k_sweep = 0;
+    k_b_gm_record<<<1, 256, 0, s>>>(G.mem, n);
+    FCM_LAUNCH_CHECK();
+  } else {
+    // r = b; x = 0; repeat: dx = GMRES32(r); x += dx; r = b - A64 x (solve_dev).
+    k_b_refine_start<<<dim3(G.max_sys_blocks, n), 256, 0, s>>>(G.mem);
+    FCM_LAUNCH_CHECK();
+    FCM_TRY(b_norm(G, BV_RHS, BO_RS0, BM_ALL, s));
+    cudaGraphConditionalHandle h;
+    FCM_TRY(new_handle(s, &h));
+    k_b_ref_enter<<<1, 256, 0, s>>>(h, G.mem, n);
+    FCM_LAUNCH_CHECK();
+    cudaGraph_t body = nullptr;
+    FCM_TRY(add_while_node(s, h, &body));
+    const long long l0 = launch_count();
+    const cudaStream_t bs = B->cap_body[0];
+    FCM_CUDA(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    auto sweep = [&]() -> int {
+      k_b_ref_tol<<<1, 256, 0, bs>>>(G.mem, n, tol);
+      FCM_LAUNCH_CHECK();
+      FCM_TRY(batch_gmres_loop(B, 1, BV_RES, 0.0, 1, BM_REF, BV_DX, bs, B->cap_body[1]));
+      FCM_TRY(b_axpby(G, BV_SOLN, BV_DX, 1.0, 1.0, BM_REF, bs));
+      FCM_TRY(batch_saddle<double>(B, BV_SOLN, BV_RES, BM_REF, bs));
+      FCM_TRY(b_axpby(G, BV_RES, BV_RHS, 1.0, -1.0, BM_REF, bs));
+      FCM_TRY(b_norm(G, BV_RES, BO_RS1, BM_REF, bs));
+      k_b_ref_next<<<1, 256, 0, bs>>>(h, G.mem, n, tol, kMaxSweeps, B->d_loop);
+      FCM_LAUNCH_CHECK();
+      return (int)FCM_OK;
+    };
+    const int st = sweep();
+    cudaGraph_t tmp = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(bs, &tmp);
+    if (st != FCM_OK) return st;
+    if (e2 != cudaSuccess) {
+      set_error(std::string("batch refinement body capture: ") + cudaGetErrorString(e2));
+      return FCM_ERR_CUDA;
+    }
+    B->k_sweep = launch_count() - l0 - B->k_iter;
+    l_loops += launch_count() - l0;
+  }
+  FCM_TRY(batch_branches(B, s, 1, [&](int i) {
+    Ctx* c = B->m[i];
+    int ov = 0;
+    return end_of_step_update_dev(c, c->d_soln + 3 * (size_t)c->Nb, 1.0, &ov,
+                                  c->p.algorithm == 1 ? c->d_rs + 3 : nullptr);
+  }));
+  FCM_CUDA(cudaMemcpyAsync(B->h_rec, B->d_rec, sizeof(StepRecord) * n, cudaMemcpyDeviceToHost, s));
+  FCM_CUDA(cudaMemcpyAsync(B->h_loop, B->d_loop, sizeof(int) * 4, cudaMemcpyDeviceToHost, s));
+  B->k_top = launch_count() - l_start - l_loops;
+  return FCM_OK;
+}
+
+int build_batch_graph(Batch* B) {
+  const long long l0 = launch_count();
+  int st = FCM_OK;
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(B->cap, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    st = enqueue_batch_step(B, B->cap);
+    const cudaError_t e2 = cudaStreamEndCapture(B->cap, &g);
+    if (st == FCM_OK && e2 != cudaSuccess) {
+      set_error(std::string("batch step capture: ") + cudaGetErrorString(e2));
+      st = FCM_ERR_CUDA;
+    }
+  } else {
+    set_error(std::string("cudaStreamBeginCapture: ") + cudaGetErrorString(e));
+    st = FCM_ERR_CUDA;
+  }
+  count_launches(-(launch_count() - l0));  // counted per executed step instead
+  if (st == FCM_OK) {
+    e = cudaGraphInstantiate(&B->graph, g, 0);
+    if (e != cudaSuccess) {
+      set_error(std::string("batch step graph instantiate: ") + cudaGetErrorString(e));
+      B->graph = nullptr;
+      st = FCM_ERR_CUDA;
+    }
+  }
+  if (g) cudaGraphDestroy(g);
+  cudaGetLastError();
+  B->state = st == FCM_OK ? 1 : -1;
+  return st;
+}
+
+// The members' grids of precision T moved into one contiguous array per group
+// of equal grids, with one cuFFT plan per group over all of them.
+template <typename T>
+int rehome_grids(Batch* B, int P) {
+  for (BatchGroup& grp : B->groups) {
+    const Ctx* c0 = B->m[grp.idx[0]];
+    const size_t G = (size_t)c0->g.G, Gc = (size_t)c0->g.Gc, k = grp.idx.size();
+    T* r = nullptr;
+    typename cplx_t<T>::type* sp = nullptr;
+    T* ur = nullptr;
+    FCM_TRY(dev_alloc(&r, 3 * G * k));
+    FCM_TRY(dev_alloc(&sp, 3 * Gc * k));
+    FCM_TRY(dev_alloc(&ur, 3 * G * k));
+    grp.r[P] = r;
+    grp.c[P] = sp;
+    grp.urand[P] = ur;
+    FCM_CUDA(cudaMemset(ur, 0, sizeof(T) * 3 * G * k));
+    for (size_t j = 0; j < k; ++j) {
+      GridBufs<T>& gb = grid_of<T>(B->m[grp.idx[j]]);
+      if (!gb.borrowed) {
+        cudaFree(gb.r);
+        cudaFree(gb.c);
+        cudaFree(gb.urand);
+      }
+      gb.r = r + 3 * G * j;
+      gb.c = sp + 3 * Gc * j;
+      gb.urand = ur + 3 * G * j;
+      gb.borrowed = true;
+    }
+    int nn[3] = {grp.nx, grp.ny, grp.nz};
+    FCM_CUFFT(cufftPlanMany(&grp.r2c[P], 3, nn, nullptr, 1, (int)G, nullptr, 1, (int)Gc, r2c_type<T>(), (int)(3 * k)));
+    FCM_CUFFT(cufftPlanMany(&grp.c2r[P], 3, nn, nullptr, 1, (int)Gc, nullptr, 1, (int)G, c2r_type<T>(), (int)(3 * k)));
+  }
+  return FCM_OK;
+}
+
+void destroy_batch(Batch* B) {
+  if (!B) return;
+  if (B->graph) cudaGraphExecDestroy(B->graph);
+  for (Ctx* c : B->m) {
+    c->d_step = nullptr;
+    c->d_stepargs = nullptr;
+    c->in_batch = false;
+    destroy_ctx(c);
+  }
+  for (BatchGroup& g : B->groups)
+    for (int P = 0; P < 2; ++P) {
+      cudaFree(g.r[P]);
+      cudaFree(g.c[P]);
+      cudaFree(g.urand[P]);
+      if (g.r2c[P]) cufftDestroy(g.r2c[P]);
+      if (g.c2r[P]) cufftDestroy(g.c2r[P]);
+    }
+  cudaFree(B->d_mem);
+  cudaFree(B->d_tile_map);
+  cudaFree(B->d_kblock_map);
+  cudaFree(B->d_partials);
+  cudaFree(B->d_counter);
+  cudaFree(B->d_mdpart);
+  cudaFree(B->d_mdcount);
+  cudaFree(B->d_rec);
+  cudaFree(B->d_args);
+  cudaFree(B->d_loop);
+  if (B->h_rec) cudaFreeHost(B->h_rec);
+  if (B->h_args) cudaFreeHost(B->h_args);
+  if (B->h_loop) cudaFreeHost(B->h_loop);
+  if (B->cap) cudaStreamDestroy(B->cap);
+  for (int i = 0; i < 2; ++i)
+    if (B->cap_body[i]) cudaStreamDestroy(B->cap_body[i]);
+  for (cudaStream_t s : B->branch)
+    if (s) cudaStreamDestroy(s);
+  for (cudaEvent_t e : B->events)
+    if (e) cudaEventDestroy(e);
+  delete B;
+}
+
+int create_batch(int n, const fcm_params* params, const double* const* refs, Batch** out) {
+  if (n < 1 || n > 4096 || !params || !refs) {
+    set_error("batch: 1 <= n <= 4096 members with params and blob_ref_pos each");
+    return FCM_ERR_INVALID;
+  }
+  for (int i = 0; i < n; ++i) {
+    if (params[i].precision != params[0].precision || params[i].gmres_tol != params[0].gmres_tol) {
+      set_error("batch: every member needs the same precision and gmres_tol");
+      return FCM_ERR_INVALID;
+    }
+    if (params[i].skip_on_overlap) {
+      set_error("batch: members step without overlap rejection (skip_on_overlap = 0)");
+      return FCM_ERR_INVALID;
+    }
+  }
+  Batch* B = new Batch();
+  auto fail = [&](int s) {
+    destroy_batch(B);
+    return s;
+  };
+  B->precision = params[0].precision;
+  for (int i = 0; i < n; ++i) {
+    Ctx* c = nullptr;
+    const int st = create_ctx(&params[i], refs[i], &c);
+    if (st != FCM_OK) return fail(st);
+    B->m.push_back(c);
+    c->in_batch = true;
+    c->step_graph_state = -1;
+    if (!c->g64.blobs.tiled || (B->precision == 1 && !c->g32.blobs.tiled)) {
+      set_error("batch: member " + std::to_string(i) +
+                " has a grid the tiled kernels cannot take (dimensions multiples of 8, at least ngauss + 8, "
+                "ngauss <= 25)");
+      return fail(FCM_ERR_INVALID);
+    }
+  }
+  for (int i = 0; i < n; ++i) {  // groups of equal grids
+    const Ctx* c = B->m[i];
+    BatchGroup* g = nullptr;
+    for (BatchGroup& x : B->groups)
+      if (x.nx == c->g.nx && x.ny == c->g.ny && x.nz == c->g.nz) g = &x;
+    if (!g) {
+      B->groups.emplace_back();
+      g = &B->groups.back();
+      g->nx = c->g.nx;
+      g->ny = c->g.ny;
+      g->nz = c->g.nz;
+    }
+    g->idx.push_back(i);
+  }
+  int st = rehome_grids<double>(B, 0);
+  if (st == FCM_OK && B->precision == 1) st = rehome_grids<float>(B, 1);
+  if (st != FCM_OK) return fail(st);
+  BatchGeom& G = B->geom;
+  G.n = n;
+  long long max_sys = 1, max_Nb = 1, max_M = 1;
+  for (const Ctx* c : B->m) {
+    max_sys = std::max<long long>(max_sys, c->nsys);
+    max_Nb = std::max<long long>(max_Nb, c->Nb);
+    max_M = std::max<long long>(max_M, c->M);
+    G.max_nb = std::max(G.max_nb, c->nb);
+    G.max_hn = std::max(G.max_hn, c->maxit_alloc + 1);
+    G.red_blocks = std::max(G.red_blocks, c->red_blocks);
+    G.md_blocks = std::max(G.md_blocks, c->md_blocks);
+    G.total_tiles += c->g64.blobs.ntiles;
+    G.total_kblocks += (int)((c->g.Gc + 255) / 256);
+  }
+  G.max_sys_blocks = (int)((max_sys + 255) / 256);
+  G.max_blob_blocks = (int)((max_Nb + 127) / 128);
+  G.max_body_blocks = (int)((max_M + 127) / 128);
+  G.max_pinv_blocks = (int)((max_M + 3) / 4);
+  if ((st = dev_alloc(&B->d_mem, (size_t)n)) || (st = dev_alloc(&B->d_tile_map, (size_t)G.total_tiles)) ||
+      (st = dev_alloc(&B->d_kblock_map, (size_t)G.total_kblocks)) ||
+      (st = dev_alloc(&B->d_partials, (size_t)n * G.red_blocks)) || (st = dev_alloc(&B->d_counter, (size_t)n)) ||
+      (st = dev_alloc(&B->d_mdpart, (size_t)n * G.max_hn * G.md_blocks)) ||
+      (st = dev_alloc(&B->d_mdcount, (size_t)n * G.max_hn)) || (st = dev_alloc(&B->d_rec, (size_t)n)) ||
+      (st = dev_alloc(&B->d_args, 2 * (size_t)n)) || (st = dev_alloc(&B->d_loop, 4)))
+    return fail(st);
+  if (cudaMemset(B->d_counter, 0, sizeof(unsigned) * n) != cudaSuccess ||
+      cudaMemset(B->d_mdcount, 0, sizeof(unsigned) * n * G.max_hn) != cudaSuccess ||
+      cudaMemset(B->d_rec, 0, sizeof(StepRecord) * n) != cudaSuccess ||
+      cudaMallocHost(&B->h_rec, sizeof(StepRecord) * n) != cudaSuccess ||
+      cudaMallocHost(&B->h_args, 2 * sizeof(uint64_t) * n) != cudaSuccess ||
+      cudaMallocHost(&B->h_loop, 4 * sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("batch: allocation failed");
+    return fail(FCM_ERR_NOMEM);
+  }
+  std::vector<BMember> hm(n);
+  std::vector<int2> tmap, kmap;
+  tmap.reserve(G.total_tiles);
+  kmap.reserve(G.total_kblocks);
+  for (int i = 0; i < n; ++i) {
+    Ctx* c = B->m[i];
+    if ((st = dev_alloc(&c->d_rs, 8)) != FCM_OK) return fail(st);
+    c->d_step = B->d_rec + i;
+    c->d_stepargs = B->d_args + 2 * i;
+    BMember& m = hm[i];
+    std::memset(&m, 0, sizeof(m));
+    m.Nb = c->Nb;
+    m.M = c->M;
+    m.nb = c->nb;
+    m.nsys = c->nsys;
+    m.hn = c->maxit_alloc + 1;
+    m.red_blocks = c->red_blocks;
+    m.md_blocks = c->md_blocks;
+    m.qm = c->d_qm;
+    m.ref = c->d_ref;
+    m.Minv = c->d_Minv;
+    m.N = c->d_N;
+    m.sys_a = c->d_sys_a;
+    m.sys_b = c->d_sys_b;
+    m.rhs = c->d_rhs;
+    m.soln = c->d_soln;
+    m.res = c->d_res;
+    m.dx = c->d_dx;
+    m.gm = c->gm;
+    m.Qm = c->d_Qm;
+    m.Hd = c->d_Hd;
+    m.beta = c->d_beta;
+    m.CS = c->d_CS;
+    m.SN = c->d_SN;
+    m.hA = c->d_hA;
+    m.hB = c->d_hB;
+    m.hnorm = c->d_hnorm;
+    m.y = c->d_y;
+    m.partials = B->d_partials + (size_t)i * G.red_blocks;
+    m.counter = B->d_counter + i;
+    m.mdpart = B->d_mdpart + (size_t)i * G.max_hn * G.md_blocks;
+    m.mdcount = B->d_mdcount + (size_t)i * G.max_hn;
+    m.sd = B->d_rec + i;
+    m.rs = c->d_rs;
+    m.wc[0] = c->g64.blobs.wc;
+    m.toff[0] = c->g64.blobs.tile_offset;
+    m.tlist[0] = c->g64.blobs.tile_list;
+    m.base[0] = c->g64.blobs.base;
+    m.grid[0] = c->g64.r;
+    m.spec[0] = c->g64.c;
+    m.partial[0] = c->g64.blobs.partial;
+    if (B->precision == 1) {
+      m.wc[1] = c->g32.blobs.wc;
+      m.toff[1] = c->g32.blobs.tile_offset;
+      m.tlist[1] = c->g32.blobs.tile_list;
+      m.base[1] = c->g32.blobs.base;
+      m.grid[1] = c->g32.r;
+      m.spec[1] = c->g32.c;
+      m.partial[1] = c->g32.blobs.partial;
+    }
+    m.tg = tile_geom(c->g, c->p.ngauss);
+    m.kp = make_kparams(*c);
+    m.dx3 = c->g.dx * c->g.dx * c->g.dx;
+    for (int t = 0; t < c->g64.blobs.ntiles; ++t) tmap.push_back(make_int2(i, t));
+    const int kb = (int)((c->g.Gc + 255) / 256);
+    for (int t = 0; t < kb; ++t) kmap.push_back(make_int2(i, t));
+  }
+  if (cudaMemcpy(B->d_mem, hm.data(), sizeof(BMember) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(B->d_tile_map, tmap.data(), sizeof(int2) * tmap.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(B->d_kblock_map, kmap.data(), sizeof(int2) * kmap.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+    set_error("batch: descriptor upload failed");
+    return fail(FCM_ERR_CUDA);
+  }
+  G.mem = B->d_mem;
+  G.tile_map = B->d_tile_map;
+  G.kblock_map = B->d_kblock_map;
+  B->branch.assign(n, nullptr);
+  B->events.assign(2 + 2 * (size_t)n, nullptr);
+  bool ok = cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&B->cap_body[0], cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&B->cap_body[1], cudaStreamNonBlocking) == cudaSuccess;
+  for (int i = 0; ok && i < n; ++i) ok = cudaStreamCreateWithFlags(&B->branch[i], cudaStreamNonBlocking) == cudaSuccess;
+  for (size_t i = 0; ok && i < B->events.size(); ++i)
+    ok = cudaEventCreateWithFlags(&B->events[i], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    set_error("batch: stream or event creation failed");
+    return fail(FCM_ERR_CUDA);
+  }
+  *out = B;
+  return FCM_OK;
+}
+
+// One step of every member.  The first call steps the members host-driven
+// (allocating what they need) and then captures the batch graph.
+int batch_step(Batch* B, const uint64_t* seeds, uint64_t step_index, fcm_step_info* infos) {
+  const int n = B->geom.n;
+  if (B->state != 1) {
+    int first = FCM_OK;
+    std::string err;
+    for (int i = 0; i < n; ++i) {
+      fcm_step_info inf;
+      std::memset(&inf, 0, sizeof(inf));
+      const int st = step_host(B->m[i], seeds[i], step_index, &inf);
+      if (infos) infos[i] = inf;
+      if (st != FCM_OK && first == FCM_OK) {
+        first = st;
+        err = g_err;
+      }
+    }
+    for (int i = 0; i < n; ++i) FCM_CUDA(cudaStreamSynchronize(B->m[i]->stream));
+    if (first != FCM_OK) {
+      set_error(err);
+      return first;
+    }
+    if (B->state == 0) {
+      const std::string keep = g_err;
+      if (build_batch_graph(B) != FCM_OK) set_error(keep);  // host-driven steps from now on
+    }
+    return FCM_OK;
+  }
+  for (int i = 0; i < n; ++i) {
+    B->h_args[2 * i] = seeds[i];
+    B->h_args[2 * i + 1] = step_index;
+  }
+  FCM_CUDA(cudaMemcpyAsync(B->d_args, B->h_args, 2 * sizeof(uint64_t) * n, cudaMemcpyHostToDevice, B->stream));
+  FCM_CUDA(cudaGraphLaunch(B->graph, B->stream));
+  FCM_CUDA(cudaStreamSynchronize(B->stream));
+  count_launches(B->k_top + (long long)B->h_loop[2] * B->k_sweep + (long long)B->h_loop[1] * B->k_iter);
+  int first = FCM_OK;
+  for (int i = 0; i < n; ++i) {
+    Ctx* c = B->m[i];
+    const StepRecord& r = B->h_rec[i];
+    c->gauss_ready = true;
+    c->urand_ready = c->p.noise != 0;
+    c->urand_prec = c->p.precision;
+    if (infos) {
+      fcm_step_info& inf = infos[i];
+      std::memset(&inf, 0, sizeof(inf));
+      inf.gmres_iters = r.iters;
+      inf.refinement_sweeps = r.sweeps;
+      inf.gmres_rel_residual = r.rel;
+      inf.divU = r.divU;
+      inf.status = r.status;
+    }
+    if (r.status != FCM_OK && r.status != FCM_ERR_NOT_CONVERGED) {
+      // as in a host-driven step, a failed solve leaves the bodies where they were
+      FCM_CUDA(cudaMemcpyAsync(c->d_x, c->d_xs, sizeof(double) * 3 * c->M, cudaMemcpyDeviceToDevice, B->stream));
+      FCM_CUDA(cudaMemcpyAsync(c->d_q, c->d_qs, sizeof(double) * 4 * c->M, cudaMemcpyDeviceToDevice, B->stream));
+      if (first == FCM_OK) first = r.status;
+    }
+  }
+  if (first != FCM_OK) {
+    FCM_CUDA(cudaStreamSynchronize(B->stream));
+    set_error("a batch member's solve failed (non-finite residual); its bodies were left unchanged");
+  }
+  return first;
+}
+
 }  // namespace
 }  // namespace fcm
 
 struct fcm_ctx {
   fcm::Ctx* c;
+};
+
+struct fcm_batch {
+  fcm::Batch* b;
+  std::vector<fcm_ctx> members;
 };
 
 using namespace fcm;
@@ -1396,6 +2086,10 @@ int fcm_create(const fcm_params* p, const double* blob_ref_pos, fcm_ctx** out) {
 
 int fcm_destroy(fcm_ctx* ctx) {
   if (!ctx) return FCM_OK;
+  if (ctx->c && ctx->c->in_batch) {
+    set_error("this context belongs to a batch: destroy the batch instead");
+    return FCM_ERR_INVALID;
+  }
   if (ctx->c) cudaStreamSynchronize(ctx->c->stream);
   destroy_ctx(ctx->c);
   delete ctx;
@@ -1884,6 +2578,56 @@ int fcm_step(fcm_ctx* ctx, uint64_t seed, uint64_t step_index, fcm_step_info* in
     return FCM_ERR_STATE;
   }
   return guard([&] { return step_host(ctx->c, seed, step_index, info); });
+}
+
+int fcm_batch_create(int32_t n, const fcm_params* params, const double* const* blob_ref_pos, fcm_batch** out) {
+  return guard([&] {
+    if (!out) return (int)FCM_ERR_INVALID;
+    *out = nullptr;
+    Batch* B = nullptr;
+    const int st = create_batch(n, params, blob_ref_pos, &B);
+    if (st != FCM_OK) return st;
+    fcm_batch* h = new fcm_batch{B, {}};
+    h->members.resize(n);
+    for (int i = 0; i < n; ++i) h->members[i].c = B->m[i];
+    *out = h;
+    return (int)FCM_OK;
+  });
+}
+
+int fcm_batch_destroy(fcm_batch* b) {
+  if (!b) return FCM_OK;
+  if (b->b) {
+    cudaStreamSynchronize(b->b->stream);
+    destroy_batch(b->b);
+  }
+  delete b;
+  return FCM_OK;
+}
+
+fcm_ctx* fcm_batch_member(fcm_batch* b, int32_t i) {
+  if (!b || i < 0 || i >= (int32_t)b->members.size()) {
+    set_error("fcm_batch_member: index out of range");
+    return nullptr;
+  }
+  return &b->members[i];
+}
+
+int fcm_batch_set_stream(fcm_batch* b, void* stream) {
+  if (!b) {
+    set_error("null batch");
+    return FCM_ERR_INVALID;
+  }
+  b->b->stream = (cudaStream_t)stream;
+  return FCM_OK;
+}
+
+int fcm_batch_step(fcm_batch* b, const uint64_t* seeds, uint64_t step_index, fcm_step_info* infos) {
+  if (!b || !seeds) {
+    set_error("fcm_batch_step: null batch or seeds");
+    return FCM_ERR_INVALID;
+  }
+  return guard([&] { return batch_step(b->b, seeds, step_index, infos); });
 }
 
 int fcm_step_async(fcm_ctx* ctx, uint64_t seed, uint64_t step_index) {

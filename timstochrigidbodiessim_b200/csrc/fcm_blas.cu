@@ -27,21 +27,22 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
 
 // Finish a reduction: the last block sums `partials` in order into *out.
 // mode 0: *out = total, 1: *out += total, 2: *out = sqrt(total).
+// nblocks: blocks taking part (gridDim.x for a single reduction).
 __device__ __forceinline__ void finish(double my_partial, double* partials, unsigned int* counter, double* out,
-                                       int mode, double* sh) {
+                                       int mode, double* sh, unsigned nblocks) {
   __shared__ bool last;
   if (threadIdx.x == 0) {
     partials[blockIdx.x] = my_partial;
     __threadfence();
     const unsigned int ticket = atomicAdd(counter, 1u);
-    last = (ticket == gridDim.x - 1);
+    last = (ticket == nblocks - 1);
   }
   __syncthreads();
   if (!last) return;
   __threadfence();
   double v = 0.0;
   // fixed assignment of partials to threads, then a fixed-order block sum
-  for (int i = threadIdx.x; i < (int)gridDim.x; i += RT) v += ((volatile double*)partials)[i];
+  for (int i = threadIdx.x; i < (int)nblocks; i += RT) v += ((volatile double*)partials)[i];
   const double total = block_sum(v, sh);
   if (threadIdx.x == 0) {
     if (mode == 0) *out = total;
@@ -59,7 +60,7 @@ __global__ void __launch_bounds__(RT) k_dot(const double* __restrict__ a, const 
   for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)gridDim.x * RT)
     s += b ? a[i] * b[i] : a[i];
   const double bs = block_sum(s, sh);
-  finish(bs, partials, counter, out, mode, sh);
+  finish(bs, partials, counter, out, mode, sh, gridDim.x);
 }
 
 // One modified-Gram-Schmidt step (gmres_solver.cpp:198-206): w -= h_prev*q_prev
@@ -79,7 +80,7 @@ __global__ void __launch_bounds__(RT) k_mgs(double* __restrict__ w, const double
     s += q_i ? v * q_i[i] : v * v;
   }
   const double bs = block_sum(s, sh);
-  finish(bs, partials, counter, hout, q_i ? 0 : 2, sh);
+  finish(bs, partials, counter, hout, q_i ? 0 : 2, sh, gridDim.x);
 }
 
 __global__ void k_scale(double* __restrict__ v, const double* __restrict__ num, int invert, long long n) {
@@ -263,10 +264,11 @@ __global__ void k_gm_normalize(const GmState* __restrict__ st, const double* __r
 }
 
 // gmres_solver.cpp:248-300 for column k+1 (one thread).
-__global__ void k_gm_givens(GmState* st, double* __restrict__ H, int hn, double* __restrict__ beta,
-                            double* __restrict__ CS, double* __restrict__ SN, const double* __restrict__ hA,
-                            const double* __restrict__ hB, const double* __restrict__ hnorm) {
-  if (threadIdx.x != 0 || blockIdx.x != 0 || st->done) return;
+__device__ __forceinline__ void givens_step(GmState* st, double* __restrict__ H, int hn, double* __restrict__ beta,
+                                            double* __restrict__ CS, double* __restrict__ SN,
+                                            const double* __restrict__ hA, const double* __restrict__ hB,
+                                            const double* __restrict__ hnorm) {
+  if (st->done) return;
   const int iter = st->k + 1;
   double* col = H + (size_t)(iter - 1) * hn;
   for (int i = 0; i < iter; ++i) col[i] = hA[i] + hB[i];
@@ -305,6 +307,13 @@ __global__ void k_gm_givens(GmState* st, double* __restrict__ H, int hn, double*
   }
 }
 
+__global__ void k_gm_givens(GmState* st, double* __restrict__ H, int hn, double* __restrict__ beta,
+                            double* __restrict__ CS, double* __restrict__ SN, const double* __restrict__ hA,
+                            const double* __restrict__ hB, const double* __restrict__ hnorm) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  givens_step(st, H, hn, beta, CS, SN, hA, hB, hnorm);
+}
+
 // beta[0] = |b|, k = 0 (one thread); |b| == 0 or non-finite ends the solve.
 __global__ void k_gm_init(GmState* st, const double* __restrict__ normb, double* __restrict__ beta, double tol,
                           const double* __restrict__ d_tol, int maxit) {
@@ -327,9 +336,8 @@ __global__ void k_gm_init(GmState* st, const double* __restrict__ normb, double*
 }
 
 // y = R^-1 beta (gmres_solver.cpp:302-318), one thread; k = 0 gives y = 0.
-__global__ void k_gm_backsub(const GmState* __restrict__ st, const double* __restrict__ H, int hn,
-                             const double* __restrict__ beta, double* __restrict__ y) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ void backsub_step(const GmState* __restrict__ st, const double* __restrict__ H, int hn,
+                                             const double* __restrict__ beta, double* __restrict__ y) {
   const int iter = st->k;
   if (iter == 0) return;
   auto Hm = [&](int i, int j) { return H[(size_t)j * hn + i]; };
@@ -339,6 +347,12 @@ __global__ void k_gm_backsub(const GmState* __restrict__ st, const double* __res
     for (int j = iter - 1; j > i; j--) v -= Hm(i, j) * y[j];
     y[i] = v / Hm(i, i);
   }
+}
+
+__global__ void k_gm_backsub(const GmState* __restrict__ st, const double* __restrict__ H, int hn,
+                             const double* __restrict__ beta, double* __restrict__ y) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  backsub_step(st, H, hn, beta, y);
 }
 
 // soln = sum_{i<k} y_i Q[:, i] (gmres_solver.cpp:320-326), k from the state.
@@ -394,6 +408,214 @@ int gm_finish(const Ctx& c, double* soln_pre, cudaStream_t s) {
   k_gm_backsub<<<1, 32, 0, s>>>(c.gm, c.d_Hd, c.maxit_alloc + 1, c.d_beta, c.d_y);
   FCM_LAUNCH_CHECK();
   k_gm_combine<<<nblk(n, 256), 256, 0, s>>>(c.gm, c.d_Qm, c.d_y, n, soln_pre);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+}  // namespace fcm
+
+// ============================================================ batched GMRES
+// The same steps for every member of a batch in one launch: blockIdx.y (or .z
+// for the multidot) selects the member, blockIdx.x keeps its single-member
+// meaning, and each member's reductions use its own block count and ticket
+// counter (the sums of its single solve).  Masks skip members whose solve is
+// done (BM_GM) or whose refinement has finished (BM_REF).
+namespace fcm {
+namespace {
+
+__global__ void __launch_bounds__(RT) k_b_norm(const BMember* __restrict__ mem, int vec, int out, int mask) {
+  __shared__ double sh[RT / 32];
+  const BMember& m = mem[blockIdx.y];
+  if ((int)blockIdx.x >= m.red_blocks || bskip(m, mask)) return;
+  const double* w = bvec(m, vec);
+  const long long n = m.nsys;
+  double s = 0.0;
+  for (long long i = blockIdx.x * (long long)RT + threadIdx.x; i < n; i += (long long)m.red_blocks * RT)
+    s += w[i] * w[i];
+  const double bs = block_sum(s, sh);
+  finish(bs, m.partials, m.counter, bout(m, out), 2, sh, (unsigned)m.red_blocks);
+}
+
+// y = a x + b y
+__global__ void k_b_axpby(const BMember* __restrict__ mem, int yv, int xv, double a, double b, int mask) {
+  const BMember& m = mem[blockIdx.y];
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= m.nsys || bskip(m, mask)) return;
+  double* y = bvec(m, yv);
+  const double* x = bvec(m, xv);
+  y[i] = a * x[i] + b * y[i];
+}
+
+// Start of a solve (k_gm_init per member): tolerance from rs[2] when use_rs;
+// members the mask excludes get an empty, finished solve.
+__global__ void k_b_gm_init(const BMember* __restrict__ mem, double tol, int use_rs, int mask) {
+  if (threadIdx.x != 0) return;
+  const BMember& m = mem[blockIdx.x];
+  GmState* st = m.gm;
+  st->k = 0;
+  st->maxit = m.hn - 1;
+  st->rel = 0.0;
+  if (mask == BM_REF && !m.sd->ref_active) {
+    st->tol = tol;
+    st->normb = 0.0;
+    st->done = 1;
+    st->status = FCM_OK;
+    return;
+  }
+  const double nb = *m.hnorm;
+  st->tol = use_rs ? m.rs[2] : tol;
+  st->normb = nb;
+  m.beta[0] = nb;
+  if (nb > 0.0 && isfinite(nb)) {
+    st->done = 0;
+    st->status = FCM_OK;
+  } else {
+    st->done = 1;
+    st->status = (nb == 0.0) ? FCM_OK : FCM_ERR_NONFINITE;
+  }
+}
+
+// Q[:, 0] = b / ||b||
+__global__ void k_b_first_column(const BMember* __restrict__ mem, int vec) {
+  const BMember& m = mem[blockIdx.y];
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= m.nsys || m.gm->done) return;
+  m.Qm[i] = bvec(m, vec)[i] / *m.hnorm;
+}
+
+__global__ void k_b_fetch(const BMember* __restrict__ mem) {
+  const BMember& m = mem[blockIdx.y];
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= m.nsys || m.gm->done) return;
+  m.sys_b[t] = m.Qm[(size_t)m.gm->k * m.nsys + t];
+}
+
+__global__ void __launch_bounds__(MDT) k_b_multidot(const BMember* __restrict__ mem, int pass) {
+  __shared__ double sh[MDT / 32];
+  __shared__ bool last;
+  const BMember& m = mem[blockIdx.z];
+  const GmState* st = m.gm;
+  const int col = blockIdx.y;
+  const unsigned nbk = (unsigned)m.md_blocks;
+  if (blockIdx.x >= nbk || st->done || col > st->k) return;
+  const long long n = m.nsys;
+  const double* q = m.Qm + (size_t)col * n;
+  const double* w = m.sys_b;
+  double s = 0.0;
+  for (long long i = blockIdx.x * (long long)MDT + threadIdx.x; i < n; i += (long long)nbk * MDT)
+    s += q[i] * w[i];
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double b = 0.0;
+    for (int i = 0; i < MDT / 32; ++i) b += sh[i];
+    m.mdpart[(size_t)col * nbk + blockIdx.x] = b;
+    __threadfence();
+    last = (atomicAdd(m.mdcount + col, 1u) == nbk - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    const volatile double* p = m.mdpart + (size_t)col * nbk;
+    for (unsigned int b = 0; b < nbk; ++b) tot += p[b];
+    (pass == 0 ? m.hA : m.hB)[col] = tot;
+    m.mdcount[col] = 0u;
+  }
+}
+
+__global__ void k_b_gs_update(const BMember* __restrict__ mem, int pass) {
+  const BMember& m = mem[blockIdx.y];
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= m.nsys || m.gm->done) return;
+  const int k = m.gm->k;
+  const double* h = pass == 0 ? m.hA : m.hB;
+  double v = m.sys_b[t];
+  for (int i = 0; i <= k; ++i) v -= h[i] * m.Qm[(size_t)i * m.nsys + t];
+  m.sys_b[t] = v;
+}
+
+__global__ void k_b_normalize(const BMember* __restrict__ mem) {
+  const BMember& m = mem[blockIdx.y];
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= m.nsys || m.gm->done) return;
+  const double s = *m.hnorm;
+  m.Qm[(size_t)(m.gm->k + 1) * m.nsys + t] = (s != 0.0) ? m.sys_b[t] / s : m.sys_b[t];
+}
+
+__global__ void k_b_givens(const BMember* __restrict__ mem) {
+  if (threadIdx.x != 0) return;
+  const BMember& m = mem[blockIdx.x];
+  givens_step(m.gm, m.Hd, m.hn, m.beta, m.CS, m.SN, m.hA, m.hB, m.hnorm);
+}
+
+__global__ void k_b_backsub(const BMember* __restrict__ mem) {
+  if (threadIdx.x != 0) return;
+  const BMember& m = mem[blockIdx.x];
+  backsub_step(m.gm, m.Hd, m.hn, m.beta, m.y);
+}
+
+// sys_b = sum_{i<k} y_i Q[:, i]
+__global__ void k_b_combine(const BMember* __restrict__ mem) {
+  const BMember& m = mem[blockIdx.y];
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= m.nsys) return;
+  const int k = m.gm->k;
+  double s = 0.0;
+  for (int i = 0; i < k; ++i) s += m.y[i] * m.Qm[(size_t)i * m.nsys + t];
+  m.sys_b[t] = s;
+}
+
+}  // namespace
+
+int b_norm(const BatchGeom& b, int vec, int out, int mask, cudaStream_t s) {
+  k_b_norm<<<dim3(b.red_blocks, b.n), RT, 0, s>>>(b.mem, vec, out, mask);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+int b_axpby(const BatchGeom& b, int y, int x, double a, double bb, int mask, cudaStream_t s) {
+  k_b_axpby<<<dim3(b.max_sys_blocks, b.n), 256, 0, s>>>(b.mem, y, x, a, bb, mask);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+int b_gm_init(const BatchGeom& b, int vec, double tol, int use_rs_tol, int mask, cudaStream_t s) {
+  FCM_TRY(b_norm(b, vec, BO_HNORM, mask, s));
+  k_b_gm_init<<<b.n, 32, 0, s>>>(b.mem, tol, use_rs_tol, mask);
+  FCM_LAUNCH_CHECK();
+  k_b_first_column<<<dim3(b.max_sys_blocks, b.n), 256, 0, s>>>(b.mem, vec);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+int b_gm_fetch(const BatchGeom& b, cudaStream_t s) {
+  k_b_fetch<<<dim3(b.max_sys_blocks, b.n), 256, 0, s>>>(b.mem);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+int b_gm_orthogonalize(const BatchGeom& b, cudaStream_t s) {
+  for (int pass = 0; pass < 2; ++pass) {
+    k_b_multidot<<<dim3(b.md_blocks, b.max_hn, b.n), MDT, 0, s>>>(b.mem, pass);
+    FCM_LAUNCH_CHECK();
+    k_b_gs_update<<<dim3(b.max_sys_blocks, b.n), 256, 0, s>>>(b.mem, pass);
+    FCM_LAUNCH_CHECK();
+  }
+  FCM_TRY(b_norm(b, BV_SYS_B, BO_HNORM, BM_GM, s));
+  k_b_normalize<<<dim3(b.max_sys_blocks, b.n), 256, 0, s>>>(b.mem);
+  FCM_LAUNCH_CHECK();
+  k_b_givens<<<b.n, 32, 0, s>>>(b.mem);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+int b_gm_finish(const BatchGeom& b, cudaStream_t s) {
+  k_b_backsub<<<b.n, 32, 0, s>>>(b.mem);
+  FCM_LAUNCH_CHECK();
+  k_b_combine<<<dim3(b.max_sys_blocks, b.n), 256, 0, s>>>(b.mem);
   FCM_LAUNCH_CHECK();
   return FCM_OK;
 }

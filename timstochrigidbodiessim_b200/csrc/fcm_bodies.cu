@@ -73,10 +73,9 @@ __global__ void k_fill_blob_pos(const double* __restrict__ x, const double* __re
 }
 
 // collection_of_rigid_bodies.cpp:707-731: out_m (+)= U + Omega x (R r_m).
-__global__ void k_multiply_K(const double* __restrict__ q, const double* __restrict__ ref, const double* __restrict__ in,
-                             double* __restrict__ out, int Nb, int nb, int subtract) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= Nb) return;
+__device__ __forceinline__ void multiply_K_one(const double* __restrict__ q, const double* __restrict__ ref,
+                                               const double* __restrict__ in, double* __restrict__ out, int i,
+                                               int nb, int subtract) {
   const int n = i / nb, m = i - n * nb;
   double R[3][3];
   quat_matrix(q + 4 * n, R);
@@ -90,13 +89,19 @@ __global__ void k_multiply_K(const double* __restrict__ q, const double* __restr
   }
 }
 
+__global__ void k_multiply_K(const double* __restrict__ q, const double* __restrict__ ref, const double* __restrict__ in,
+                             double* __restrict__ out, int Nb, int nb, int subtract) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= Nb) return;
+  multiply_K_one(q, ref, in, out, i, nb, subtract);
+}
+
 // collection_of_rigid_bodies.cpp:733-757: F = sum lambda_m, T = sum (R r_m) x lambda_m;
 // out = scale * K^T in + add_scale * add.
-__global__ void k_multiply_KT(const double* __restrict__ q, const double* __restrict__ ref,
-                              const double* __restrict__ in, double* __restrict__ out, int M, int nb, double scale,
-                              const double* __restrict__ add, double add_scale) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= M) return;
+__device__ __forceinline__ void multiply_KT_one(const double* __restrict__ q, const double* __restrict__ ref,
+                                                const double* __restrict__ in, double* __restrict__ out, int n,
+                                                int nb, double scale, const double* __restrict__ add,
+                                                double add_scale) {
   double R[3][3];
   quat_matrix(q + 4 * n, R);
   double acc[6] = {0, 0, 0, 0, 0, 0};
@@ -115,16 +120,24 @@ __global__ void k_multiply_KT(const double* __restrict__ q, const double* __rest
   for (int d = 0; d < 6; ++d) out[6 * n + d] = scale * acc[d] + (add ? add_scale * add[6 * n + d] : 0.0);
 }
 
+__global__ void k_multiply_KT(const double* __restrict__ q, const double* __restrict__ ref,
+                              const double* __restrict__ in, double* __restrict__ out, int M, int nb, double scale,
+                              const double* __restrict__ add, double add_scale) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= M) return;
+  multiply_KT_one(q, ref, in, out, n, nb, scale, add, add_scale);
+}
+
 // gmres_solver.cpp:85-146, one warp per body, applied in the body frame:
 // with B = blockdiag(R) and C = diag(R^T, R^T), the reference's rotated
 // matrices are B ref_Minv B^T, K_rot = B K_ref C and C^T ref_N C, so
 //   U' = ref_N (-C in_U - K_ref^T ref_Minv B^T in_l),   out_U = C^T U'
 //   out_l = B ref_Minv (K_ref U' + B^T in_l).
 // Shared memory per warp: 2*(3nb) + 12 doubles.
-__global__ void k_pinv(const double* __restrict__ q, const double* __restrict__ ref, const double* __restrict__ Minv,
-                       const double* __restrict__ Nm, const double* __restrict__ in, double* __restrict__ out, int M,
-                       int nb, int Nb) {
-  extern __shared__ double sm[];
+__device__ __forceinline__ void pinv_block(const double* __restrict__ q, const double* __restrict__ ref,
+                                           const double* __restrict__ Minv, const double* __restrict__ Nm,
+                                           const double* __restrict__ in, double* __restrict__ out, int M, int nb,
+                                           int Nb, double* sm) {
   const int warps = blockDim.x >> 5;
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int n = blockIdx.x * warps + wid;
@@ -185,6 +198,13 @@ __global__ void k_pinv(const double* __restrict__ q, const double* __restrict__ 
   __syncwarp();
   double* ol = out + (size_t)n3 * n;
   for (int m = lane; m < nb; m += 32) rot(R, t + 3 * m, ol + 3 * m);
+}
+
+__global__ void k_pinv(const double* __restrict__ q, const double* __restrict__ ref, const double* __restrict__ Minv,
+                       const double* __restrict__ Nm, const double* __restrict__ in, double* __restrict__ out, int M,
+                       int nb, int Nb) {
+  extern __shared__ double sm[];
+  pinv_block(q, ref, Minv, Nm, in, out, M, nb, Nb, sm);
 }
 
 // Rigid projection of blob velocities with ref_KTKinv
@@ -334,6 +354,51 @@ int launch_divU_accumulate(const Ctx& c, const double* U6, const double* U0, int
                            double* acc, cudaStream_t s) {
   if (c.M == 0) return FCM_OK;
   k_divU_terms<<<(c.M + 127) / 128, 128, 0, s>>>(U6, U0, c.M, component, delta, acc);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+}  // namespace fcm
+
+// ============================================================ batched
+namespace fcm {
+namespace {
+
+__global__ void k_b_pinv(const BMember* __restrict__ mem, int in, int out, int mask) {
+  extern __shared__ double sm[];
+  const BMember& m = mem[blockIdx.y];
+  if (bskip(m, mask)) return;
+  pinv_block(m.qm, m.ref, m.Minv, m.N, bvec(m, in), bvec(m, out), m.M, m.nb, m.Nb, sm);
+}
+
+// out[lambda] -= K in[U] (blocks [0, blob_blocks)) and out[U] = -K^T in[lambda]
+// (the rest): the rigid-body part of the saddle-point product.
+__global__ void k_b_K_KT(const BMember* __restrict__ mem, int in, int out, int blob_blocks, int mask) {
+  const BMember& m = mem[blockIdx.y];
+  if (bskip(m, mask)) return;
+  const double* x = bvec(m, in);
+  double* y = bvec(m, out);
+  if ((int)blockIdx.x < blob_blocks) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m.Nb) multiply_K_one(m.qm, m.ref, x + 3 * (size_t)m.Nb, y, i, m.nb, 1);
+  } else {
+    const int n = (blockIdx.x - blob_blocks) * blockDim.x + threadIdx.x;
+    if (n < m.M) multiply_KT_one(m.qm, m.ref, x, y + 3 * (size_t)m.Nb, n, m.nb, -1.0, nullptr, 0.0);
+  }
+}
+
+}  // namespace
+
+int b_pinv(const BatchGeom& b, int in, int out, int mask, cudaStream_t s) {
+  const int warps = 4;
+  const size_t shm = sizeof(double) * warps * (size_t)(6 * b.max_nb + 12);
+  k_b_pinv<<<dim3(b.max_pinv_blocks, b.n), 32 * warps, shm, s>>>(b.mem, in, out, mask);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+int b_multiply_K_KT(const BatchGeom& b, int in, int out, int mask, cudaStream_t s) {
+  k_b_K_KT<<<dim3(b.max_blob_blocks + b.max_body_blocks, b.n), 128, 0, s>>>(b.mem, in, out, b.max_blob_blocks, mask);
   FCM_LAUNCH_CHECK();
   return FCM_OK;
 }

@@ -73,10 +73,6 @@ __global__ void k_set_up_gaussians(const double* __restrict__ Y, int n, int W, d
   }
 }
 
-struct TileGeom {
-  int ntx, nty, ntz, nx, ny, nz, W;
-};
-
 // (blob, tile) overlaps of a blob: per dimension the tiles first..first+cnt-1.
 __device__ __forceinline__ void blob_tiles(const int* base, int b, const TileGeom& g, int f[3], int cnt[3]) {
 #pragma unroll
@@ -218,14 +214,13 @@ __device__ __forceinline__ void load_wx4(const T* row, int xs, T wx[4]) {
 // stencil misses it; an x-half the stencil misses is skipped by the whole CTA
 // (both branches are uniform).
 template <typename T>
-__global__ void __launch_bounds__(64) k_spread_tiled(const T* __restrict__ wc, const double* __restrict__ F,
-                                                     TileGeom g, const int* __restrict__ offset,
-                                                     const unsigned long long* __restrict__ list, long long G,
-                                                     T* __restrict__ grid) {
+__device__ __forceinline__ void spread_tile(const T* __restrict__ wc, const double* __restrict__ F,
+                                            const TileGeom& g, const int* __restrict__ offset,
+                                            const unsigned long long* __restrict__ list, long long G,
+                                            T* __restrict__ grid, int tile) {
   __shared__ __align__(16) T sw[SCB][3][TE];
   __shared__ __align__(16) T sF[SCB][4];
   __shared__ unsigned sflag[SCB];
-  const int tile = blockIdx.x;
   const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
   const int t = threadIdx.x;
   const int z = t & 7, y = t >> 3, yh = t >> 5;
@@ -269,6 +264,14 @@ __global__ void __launch_bounds__(64) k_spread_tiled(const T* __restrict__ wc, c
   }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(64) k_spread_tiled(const T* __restrict__ wc, const double* __restrict__ F,
+                                                     TileGeom g, const int* __restrict__ offset,
+                                                     const unsigned long long* __restrict__ list, long long G,
+                                                     T* __restrict__ grid) {
+  spread_tile<T>(wc, F, g, offset, list, G, grid, blockIdx.x);
+}
+
 // Sum of v[0..15] over the 32 lanes of a warp, scattered: afterwards lanes 2i
 // and 2i+1 hold in v[0] the warp total of value i (16 shuffles for 16 values).
 template <typename T>
@@ -295,15 +298,14 @@ __device__ __forceinline__ T warp_reduce_scatter16(T v[16], int lane) {
 // per-(blob, tile) partial goes to partial[blob][j][3]; k_interp_reduce then
 // sums a blob's partials in j order (deterministic, no atomics).
 template <typename T>
-__global__ void __launch_bounds__(64) k_interp_tiled(const T* __restrict__ wc, const T* __restrict__ grid,
-                                                     TileGeom g, const int* __restrict__ offset,
-                                                     const unsigned long long* __restrict__ list, long long G,
-                                                     T* __restrict__ partial) {
+__device__ __forceinline__ void interp_tile(const T* __restrict__ wc, const T* __restrict__ grid, const TileGeom& g,
+                                            const int* __restrict__ offset,
+                                            const unsigned long long* __restrict__ list, long long G,
+                                            T* __restrict__ partial, int tile) {
   __shared__ __align__(16) T sw[SCB][3][TE];
   __shared__ unsigned sflag[SCB];
   __shared__ unsigned sblob[SCB];
   __shared__ T sred[SCB / 4][2][16];
-  const int tile = blockIdx.x;
   const int b0 = offset[tile], b1 = offset[tile + 1];
   if (b0 == b1) return;  // no blob meets this tile (uniform over the CTA)
   const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
@@ -372,12 +374,18 @@ __global__ void __launch_bounds__(64) k_interp_tiled(const T* __restrict__ wc, c
   }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(64) k_interp_tiled(const T* __restrict__ wc, const T* __restrict__ grid,
+                                                     TileGeom g, const int* __restrict__ offset,
+                                                     const unsigned long long* __restrict__ list, long long G,
+                                                     T* __restrict__ partial) {
+  interp_tile<T>(wc, grid, g, offset, list, G, partial, blockIdx.x);
+}
+
 // V = DX^3 * sum over the blob's tiles (in canonical order j) of the partials.
 template <typename T>
-__global__ void k_interp_reduce(const int* __restrict__ base, const T* __restrict__ partial, int n, TileGeom g,
-                                double dx3, double* __restrict__ V) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= n) return;
+__device__ __forceinline__ void interp_reduce_one(const int* __restrict__ base, const T* __restrict__ partial,
+                                                  const TileGeom& g, double dx3, double* __restrict__ V, int b) {
   int f[3], cnt[3];
   blob_tiles(base, b, g, f, cnt);
   const int nj = cnt[0] * cnt[1] * cnt[2];
@@ -391,6 +399,14 @@ __global__ void k_interp_reduce(const int* __restrict__ base, const T* __restric
   V[3 * b] = s0 * dx3;
   V[3 * b + 1] = s1 * dx3;
   V[3 * b + 2] = s2 * dx3;
+}
+
+template <typename T>
+__global__ void k_interp_reduce(const int* __restrict__ base, const T* __restrict__ partial, int n, TileGeom g,
+                                double dx3, double* __restrict__ V) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  interp_reduce_one<T>(base, partial, g, dx3, V, b);
 }
 
 // Spreading of grids that cannot be tiled: one CTA per blob, each thread owns
@@ -469,11 +485,11 @@ __global__ void __launch_bounds__(NT) k_interp_block(const int* __restrict__ bas
   }
 }
 
+}  // namespace
+
 TileGeom tile_geom(const GridDims& g, int W) {
   return TileGeom{g.nx / TE, g.ny / TE, g.nz / TE, g.nx, g.ny, g.nz, W};
 }
-
-}  // namespace
 
 template <typename T>
 int blob_table_alloc(BlobTable<T>& t, int n, int W, const GridDims& g) {
@@ -584,6 +600,64 @@ template int launch_spread<double>(const Ctx&, const BlobTable<double>&, const d
 template int launch_spread<float>(const Ctx&, const BlobTable<float>&, const double*, float*, cudaStream_t);
 template int launch_interp<double>(const Ctx&, const BlobTable<double>&, const double*, double*, cudaStream_t);
 template int launch_interp<float>(const Ctx&, const BlobTable<float>&, const float*, double*, cudaStream_t);
+
+// ------------------------------------------------------------------ batched
+// One launch over the tiles of every member: tile_map[blockIdx.x] = (member,
+// tile).  P selects the member's grid of that precision (0 FP64, 1 FP32).
+namespace {
+
+template <typename T, int P>
+__global__ void __launch_bounds__(64) k_b_spread(const BMember* __restrict__ mem, const int2* __restrict__ tile_map,
+                                                 int in, int mask) {
+  const int2 mt = tile_map[blockIdx.x];
+  const BMember& m = mem[mt.x];
+  if (bskip(m, mask)) return;
+  spread_tile<T>((const T*)m.wc[P], bvec(m, in), m.tg, m.toff[P], m.tlist[P], (long long)m.tg.nx * m.tg.ny * m.tg.nz,
+                 (T*)m.grid[P], mt.y);
+}
+
+template <typename T, int P>
+__global__ void __launch_bounds__(64) k_b_interp(const BMember* __restrict__ mem, const int2* __restrict__ tile_map,
+                                                 int mask) {
+  const int2 mt = tile_map[blockIdx.x];
+  const BMember& m = mem[mt.x];
+  if (bskip(m, mask)) return;
+  interp_tile<T>((const T*)m.wc[P], (const T*)m.grid[P], m.tg, m.toff[P], m.tlist[P],
+                 (long long)m.tg.nx * m.tg.ny * m.tg.nz, (T*)m.partial[P], mt.y);
+}
+
+template <typename T, int P>
+__global__ void k_b_interp_reduce(const BMember* __restrict__ mem, int out, int mask) {
+  const BMember& m = mem[blockIdx.y];
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= m.Nb || bskip(m, mask)) return;
+  interp_reduce_one<T>(m.base[P], (const T*)m.partial[P], m.tg, m.dx3, bvec(m, out), b);
+}
+
+}  // namespace
+
+template <typename T>
+int b_spread(const BatchGeom& b, int in, int mask, cudaStream_t s) {
+  constexpr int P = sizeof(T) == 8 ? 0 : 1;
+  k_b_spread<T, P><<<b.total_tiles, 64, 0, s>>>(b.mem, b.tile_map, in, mask);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+template <typename T>
+int b_interp(const BatchGeom& b, int out, int mask, cudaStream_t s) {
+  constexpr int P = sizeof(T) == 8 ? 0 : 1;
+  k_b_interp<T, P><<<b.total_tiles, 64, 0, s>>>(b.mem, b.tile_map, mask);
+  FCM_LAUNCH_CHECK();
+  k_b_interp_reduce<T, P><<<dim3(b.max_blob_blocks, b.n), 128, 0, s>>>(b.mem, out, mask);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+template int b_spread<double>(const BatchGeom&, int, int, cudaStream_t);
+template int b_spread<float>(const BatchGeom&, int, int, cudaStream_t);
+template int b_interp<double>(const BatchGeom&, int, int, cudaStream_t);
+template int b_interp<float>(const BatchGeom&, int, int, cudaStream_t);
 
 }  // namespace fcm
 

@@ -110,6 +110,7 @@ struct BlobTable {
 template <typename T>
 struct GridBufs {
   bool ready = false;
+  bool borrowed = false;                       // r, c, urand are slices of a batch's group arrays
   T* r = nullptr;                              // 3*G real
   typename cplx_t<T>::type* c = nullptr;       // 3*Gc spectrum
   T* urand = nullptr;                          // 3*G random velocity field
@@ -121,6 +122,19 @@ struct GridBufs {
 // Tile shape of the tiled spread / interpolation kernels.
 constexpr int TILE_X = 8, TILE_Y = 8, TILE_Z = 8;
 
+// Tile grid of the tiled spread / interpolation (fcm_grid.cu).
+struct TileGeom {
+  int ntx, nty, ntz, nx, ny, nz, W;
+};
+
+// k-space geometry of the projection (fcm_kspace.cu).
+struct KParams {
+  int nx, ny, nz, nzh;
+  long long Gc;
+  double fx, fy, fz;  // 2 pi / L
+  double inv_etaG;    // 1 / (eta * nx*ny*nz)
+};
+
 // Record of one device-resident (graph) time step, written by the device.
 struct StepRecord {
   int iters;     // GMRES iterations, summed over refinement sweeps
@@ -131,6 +145,8 @@ struct StepRecord {
   double divU;   // GDC divergence term (0 for EM or without noise)
   double normb;  // ||RHS|| of the refinement
   double relr;   // refinement residual of the last sweep
+  int ref_active;  // batched refinement: this member still sweeps
+  int pad_;
 };
 
 // Device-resident state of one GMRES solve (gmres_solver.cpp:148-306).
@@ -203,6 +219,7 @@ struct Ctx {
   bool step_pending_graph = false;  // ... and it was a graph launch
   int step_pending_status = 0;      // host-driven pending step: its status and record
   fcm_step_info step_pending_info{};
+  bool in_batch = false;            // owned by a batch (its step record and arguments too)
   // cells
   int ncell_total = 0;
   int *d_cell = nullptr, *d_cell_start = nullptr, *d_cell_count = nullptr, *d_cell_sorted = nullptr, *d_cell_cursor = nullptr;
@@ -221,6 +238,101 @@ struct Ctx {
   bool det_ready = false;   // deterministic velocity grid holds u
   int urand_prec = 0;       // precision of the random field last produced
 };
+
+// ------------------------------------------------------------------ batches
+// One member suspension of a batch as the batched kernels see it (a device
+// array, one entry per member; blockIdx.y or .z selects the member).
+struct BMember {
+  int Nb, M, nb, nsys;
+  int hn;  // columns of the member's Krylov basis (maxit_alloc + 1)
+  int red_blocks, md_blocks;  // the member's own reduction grids (same sums as its single solve)
+  const double *qm, *ref, *Minv, *N;
+  double *sys_a, *sys_b, *rhs, *soln, *res, *dx;
+  GmState* gm;
+  double *Qm, *Hd, *beta, *CS, *SN, *hA, *hB, *hnorm, *y;
+  double* partials;    // [max red blocks] batch reduction scratch
+  unsigned* counter;   // [1]
+  double* mdpart;      // [hn * max md blocks]
+  unsigned* mdcount;   // [hn]
+  StepRecord* sd;
+  double* rs;          // [0] ||b|| [1] ||r|| [2] inner tolerance [3] nu
+  // grid of each precision, [0] FP64 and [1] FP32
+  const void* wc[2];
+  const int* toff[2];
+  const unsigned long long* tlist[2];
+  const int* base[2];
+  void* grid[2];
+  void* spec[2];
+  void* partial[2];
+  TileGeom tg;
+  KParams kp;
+  double dx3;
+};
+
+// Which members a batched kernel works on.
+enum BMask { BM_ALL = 0, BM_GM = 1, BM_REF = 2 };  // all / GMRES not done / refinement active
+// Member vectors addressed by batched kernels.
+enum BVec { BV_SYS_A = 0, BV_SYS_B, BV_RHS, BV_SOLN, BV_RES, BV_DX };
+// Member scalars written by batched reductions.
+enum BOut { BO_HNORM = 0, BO_RS0, BO_RS1 };
+
+#ifdef __CUDACC__
+__device__ __forceinline__ double* bvec(const BMember& m, int v) {
+  switch (v) {
+    case BV_SYS_A: return m.sys_a;
+    case BV_SYS_B: return m.sys_b;
+    case BV_RHS: return m.rhs;
+    case BV_SOLN: return m.soln;
+    case BV_RES: return m.res;
+    default: return m.dx;
+  }
+}
+
+__device__ __forceinline__ double* bout(const BMember& m, int o) {
+  return o == BO_HNORM ? m.hnorm : (o == BO_RS0 ? m.rs : m.rs + 1);
+}
+
+__device__ __forceinline__ bool bskip(const BMember& m, int mask) {
+  return (mask == BM_GM && m.gm->done) || (mask == BM_REF && !m.sd->ref_active);
+}
+#endif
+
+// Launch geometry of a batch (host side).
+struct BatchGeom {
+  int n = 0;                   // members
+  int max_sys_blocks = 1;      // ceil(max nsys / 256)
+  int max_blob_blocks = 1;     // ceil(max Nb / 128)
+  int max_body_blocks = 1;     // ceil(max M / 128)
+  int max_pinv_blocks = 1;     // ceil(max M / 4) (4 warps per block)
+  int max_nb = 1;              // blobs per body (shared memory of the preconditioner)
+  int red_blocks = 1;          // reduction blocks per member (the largest)
+  int md_blocks = 1;           // multidot blocks per member (the largest)
+  int max_hn = 1;              // multidot columns
+  int total_tiles = 0;         // sum of the members' tiles
+  int total_kblocks = 0;       // sum of the members' k-space blocks (256 modes)
+  const BMember* mem = nullptr;      // device array [n]
+  const int2* tile_map = nullptr;    // [total_tiles] (member, tile)
+  const int2* kblock_map = nullptr;  // [total_kblocks] (member, block)
+};
+
+KParams make_kparams(const Ctx& c);
+TileGeom tile_geom(const GridDims& g, int W);
+
+// batched kernels (fcm_blas.cu, fcm_bodies.cu, fcm_grid.cu, fcm_kspace.cu)
+int b_gm_init(const BatchGeom& b, int vec, double tol, int use_rs_tol, int mask, cudaStream_t s);
+int b_gm_fetch(const BatchGeom& b, cudaStream_t s);
+int b_gm_orthogonalize(const BatchGeom& b, cudaStream_t s);
+int b_gm_finish(const BatchGeom& b, cudaStream_t s);
+int b_norm(const BatchGeom& b, int vec, int out, int mask, cudaStream_t s);
+int b_axpby(const BatchGeom& b, int y, int x, double a, double bb, int mask, cudaStream_t s);
+int b_pinv(const BatchGeom& b, int in, int out, int mask, cudaStream_t s);
+int b_multiply_K_KT(const BatchGeom& b, int in, int out, int mask, cudaStream_t s);
+template <typename T>
+int b_spread(const BatchGeom& b, int in, int mask, cudaStream_t s);
+template <typename T>
+int b_interp(const BatchGeom& b, int out, int mask, cudaStream_t s);
+template <typename T>
+int b_project(const BatchGeom& b, int mask, cudaStream_t s);
 
 // ------------------------------------------------------------------ launchers
 // gaussians + binning (fcm_grid.cu)

@@ -36,13 +36,6 @@ __device__ __forceinline__ double wavenumber(int i, int n, double fac) {
   return (i <= n / 2) ? (double)i * fac : (double)(i - n) * fac;
 }
 
-struct KParams {
-  int nx, ny, nz, nzh;
-  long long Gc;
-  double fx, fy, fz;  // 2 pi / L
-  double inv_etaG;    // 1 / (eta * nx*ny*nz)
-};
-
 // Projection of one complex mode (re and im share the real factors).  The
 // reference divides every component by eta*G; here one reciprocal of the
 // mode's |q|^2 and a precomputed 1/(eta*G) are used instead (a last-bit change).
@@ -97,8 +90,7 @@ __device__ __forceinline__ void load3(const C* spec, long long Gc, long long t, 
 
 // Deterministic projection in place (fcm_fluid_solver.cpp:642-695).
 template <typename T, typename C>
-__global__ void __launch_bounds__(256, 4) k_project(C* __restrict__ spec, KParams k) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void project_one(C* __restrict__ spec, const KParams& k, long long t) {
   if (t >= k.Gc) return;
   int x, y, kz;
   mode_coords(t, k, x, y, kz);
@@ -138,6 +130,21 @@ __global__ void __launch_bounds__(256, 4) k_project(C* __restrict__ spec, KParam
   }
   store3(spec, k.Gc, t, us);
   store3(spec, k.Gc, tp, usp);
+}
+
+template <typename T, typename C>
+__global__ void __launch_bounds__(256, 4) k_project(C* __restrict__ spec, KParams k) {
+  project_one<T, C>(spec, k, blockIdx.x * (long long)blockDim.x + threadIdx.x);
+}
+
+// Batched: kblock_map[blockIdx.x] = (member, block of 256 modes).
+template <typename T, typename C, int P>
+__global__ void __launch_bounds__(256, 4) k_b_project(const BMember* __restrict__ mem,
+                                                      const int2* __restrict__ kblock_map, int mask) {
+  const int2 mb = kblock_map[blockIdx.x];
+  const BMember& m = mem[mb.x];
+  if (bskip(m, mask)) return;
+  project_one<T, C>((C*)m.spec[P], m.kp, (long long)mb.y * 256 + threadIdx.x);
 }
 
 // f = i (q~ . sigma) for one mode; sigma order xx, yy, zz, xy, xz, yz.
@@ -292,6 +299,8 @@ __global__ void k_fluct(C* __restrict__ spec, const cufftDoubleComplex* __restri
   store3(spec, k.Gc, tp, usp);
 }
 
+}  // namespace
+
 KParams make_kparams(const Ctx& c) {
   const double PI = 3.14159265358979323846264338327950288;
   KParams k;
@@ -304,7 +313,6 @@ KParams make_kparams(const Ctx& c) {
   return k;
 }
 
-}  // namespace
 
 template <typename T>
 int launch_project(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s) {
@@ -350,6 +358,16 @@ int launch_stress_divergence_project(const Ctx& c, const cufftDoubleComplex* sig
   return FCM_OK;
 }
 
+template <typename T>
+int b_project(const BatchGeom& b, int mask, cudaStream_t s) {
+  constexpr int P = sizeof(T) == 8 ? 0 : 1;
+  k_b_project<T, typename cplx_t<T>::type, P><<<b.total_kblocks, 256, 0, s>>>(b.mem, b.kblock_map, mask);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+template int b_project<double>(const BatchGeom&, int, cudaStream_t);
+template int b_project<float>(const BatchGeom&, int, cudaStream_t);
 template int launch_project<double>(const Ctx&, cufftDoubleComplex*, cudaStream_t);
 template int launch_project<float>(const Ctx&, cufftComplex*, cudaStream_t);
 template int launch_noise_kspace<double>(const Ctx&, cufftDoubleComplex*, uint64_t, uint64_t, const uint64_t*,

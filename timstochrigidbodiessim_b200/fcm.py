@@ -41,7 +41,7 @@ def _out(out, n, dtype=np.float64):
 class Suspension:
     """One suspension of rigid multi-blob bodies on the GPU."""
 
-    def __init__(self, params: FcmParams, blob_ref_pos, stream=None):
+    def __init__(self, params: FcmParams, blob_ref_pos, stream=None, _handle=None):
         self.L = capi.load()
         self.p = params.copy()
         self.M = params.num_bodies
@@ -49,16 +49,21 @@ class Suspension:
         self.Nb = params.num_blobs
         self.n = params.system_size
         self.P = params.nx * params.ny * params.pad
-        keep, ref = _in(blob_ref_pos, 3 * self.nb)
-        h = ctypes.c_void_p()
-        capi.check(self.L.fcm_create(ctypes.byref(self.p), ref, ctypes.byref(h)), "fcm_create")
-        self.h = h
+        self._owned = _handle is None
+        if _handle is None:
+            keep, ref = _in(blob_ref_pos, 3 * self.nb)
+            h = ctypes.c_void_p()
+            capi.check(self.L.fcm_create(ctypes.byref(self.p), ref, ctypes.byref(h)), "fcm_create")
+            self.h = h
+        else:  # a member of a Batch, owned by it
+            self.h = ctypes.c_void_p(_handle)
         if stream is not None:
             self.set_stream(stream)
 
     def close(self):
         if getattr(self, "h", None):
-            self.L.fcm_destroy(self.h)
+            if self._owned:
+                self.L.fcm_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -317,6 +322,51 @@ class Suspension:
         st = self.L.fcm_step_wait(self.h, ctypes.byref(info))
         self._c(st, "fcm_step_wait", ok=(0, 7))
         return st, info
+
+
+class Batch:
+    """Many independent suspensions stepped together (fcm_batch_*): members[i]
+    is a Suspension view of member i (owned by the batch)."""
+
+    def __init__(self, members, stream=None):
+        """members: list of (FcmParams, blob_ref_pos)."""
+        self.L = capi.load()
+        n = len(members)
+        self.n = n
+        self._params = (FcmParams * n)(*[p.copy() for p, _ in members])
+        self._refs = [np.ascontiguousarray(r, dtype=np.float64).ravel() for _, r in members]
+        ptrs = (ctypes.c_void_p * n)(*[r.ctypes.data for r in self._refs])
+        h = ctypes.c_void_p()
+        capi.check(self.L.fcm_batch_create(n, self._params, ptrs, ctypes.byref(h)), "fcm_batch_create")
+        self.h = h
+        self.members = [Suspension(p, r, _handle=self.L.fcm_batch_member(h, i))
+                        for i, (p, r) in enumerate(members)]
+        if stream is not None:
+            self.set_stream(stream)
+
+    def set_stream(self, stream):
+        s = getattr(stream, "cuda_stream", stream)
+        capi.check(self.L.fcm_batch_set_stream(self.h, ctypes.c_void_p(int(s))), "fcm_batch_set_stream")
+
+    def step(self, seeds, step_index):
+        """One step of every member; returns the list of FcmStepInfo."""
+        sd = (ctypes.c_uint64 * self.n)(*[int(x) for x in seeds])
+        infos = (FcmStepInfo * self.n)()
+        capi.check(self.L.fcm_batch_step(self.h, sd, step_index, infos), "fcm_batch_step")
+        return list(infos)
+
+    def close(self):
+        if getattr(self, "h", None):
+            for m in self.members:
+                m.h = None
+            self.L.fcm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def step_many(suspensions, seeds, step_index):
