@@ -42,6 +42,9 @@ def parse():
     ap.add_argument("--workload", default="rods2048_phi0.10_g256")
     ap.add_argument("--algorithm", default="em", choices=["em", "gdc"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ens-modes", default="fp64,fp64_graph,mixed_streams,mixed",
+                    help="ensemble arms to time (the JSON line needs fp64, fp64_graph and mixed)")
+    ap.add_argument("--nvtx", action="store_true", help="mark the timed region with an NVTX range 'timed'")
     ap.add_argument("--kernels-only", type=int, default=0, metavar="R",
                     help="profiling mode: R FP64 spread+interp launches and R FP32 mobility products, no steps")
     return ap.parse_args()
@@ -469,7 +472,10 @@ def run_ensemble(args):
     seeds = list(range(len(insts)))
     res = {}
     modes = (("fp64", 0, "host"), ("fp64_graph", 0, "graph"), ("mixed_streams", 1, "many"), ("mixed", 1, "batch"))
+    wanted = set(args.ens_modes.split(","))
     for tag, prec, mode in modes:
+        if tag not in wanted:
+            continue
         streams = [torch.cuda.Stream() for _ in insts] if mode == "many" else [torch.cuda.Stream()] * len(insts)
         batch = None
         if mode == "batch":
@@ -510,14 +516,18 @@ def run_ensemble(args):
         if mode == "batch":
             sampler.start()
         l0 = lib.fcm_kernel_launch_count()
+        if args.nvtx:
+            torch.cuda.nvtx.range_push("timed")
         e0.record(root)
         for st in set(streams):
             st.wait_event(e0)
         iters = []
+        rounds = []
         for j in range(args.steps):
             step = args.warmup + j
             if mode == "batch":
                 iters += [inf.gmres_iters for inf in batch.step(seeds, step)]
+                rounds.append(batch.last_rounds())
             elif mode == "many":
                 iters += [inf.gmres_iters for inf in step_many(ss, seeds, step)]
             else:
@@ -534,15 +544,21 @@ def run_ensemble(args):
             root.wait_event(ev)
         e1.record(root)
         e1.synchronize()
+        if args.nvtx:
+            torch.cuda.nvtx.range_pop()
         clocks = sampler.stop() if mode == "batch" else None
         t = e0.elapsed_time(e1) / 1e3
         res[tag] = dict(t=t, iters=float(np.mean(iters)), launches=lib.fcm_kernel_launch_count() - l0,
-                        clocks=clocks)
+                        clocks=clocks, rounds=[float(np.mean([r[i] for r in rounds])) for i in (0, 1)] if rounds else None)
         if batch is not None:
             batch.close()
         else:
             for s in ss:
                 s.close()
+    if not {"fp64", "fp64_graph", "mixed"} <= set(res):
+        print(json.dumps({"ensemble_partial": {k: {"ms_per_step": 1e3 * v["t"] / args.steps, "iters": v["iters"],
+                                                    "rounds": v["rounds"]} for k, v in res.items()}}))
+        return
     # velocity error of the mixed solve against the FP64 solve, every instance
     errs = [rel_vel_error(p, ref, x, q, fe, root) for p, ref, x, q, fe in insts]
     value = total_bodies * args.steps / res["mixed"]["t"]
@@ -566,6 +582,7 @@ def run_ensemble(args):
                           "mode": "64 contexts on 64 streams, one graph per instance step (fcm_step_many)"},
         "mixed_over_fp64": value / fp64, "mixed_over_fp64_graph": value / fp64g,
         "gmres_iters_mixed": res["mixed"]["iters"],
+        "lockstep_rounds_mixed": {"gmres_iters": res["mixed"]["rounds"][0], "sweeps": res["mixed"]["rounds"][1]},
         "rel_vel_error_mixed_vs_fp64_max": {"bodies": max(e[0] for e in errs), "blobs": max(e[1] for e in errs)},
         "gpu_launches": res["mixed"]["launches"],
         "clocks": res["mixed"]["clocks"],

@@ -217,6 +217,23 @@ int fcm_get_V(fcm_ctx* ctx, double* V);
 int fcm_get_velocity_field(fcm_ctx* ctx, int32_t which, double* ux, double* uy, double* uz);
 /* M*F in one call: spread, Stokes solve, interpolation (V = 3Nb). */
 int fcm_apply_mobility(fcm_ctx* ctx, const double* F, double* V);
+/* Force dipoles -- no reference counterpart (the reference spreads forces only).
+ * The FCM dipole terms (Lomholt & Maxey, J. Comput. Phys. 184 (2003)) on the FP64
+ * deterministic grid: blob forces F (3Nb), torques T (3Nb) and stresslets S
+ * (9Nb, row-major, symmetric) -- each may be NULL for zero -- spread with the force
+ * envelope (F) and the dipole envelope sigma_D = a / (6 sqrt(pi))^(1/3) (the
+ * dipole D = S - 1/2 eps.T as f_i = D_ij (x_j - Y_j)/sigma_D^2 Delta_D).  After
+ * fcm_produce_deterministic_velocity_field, V comes from
+ * fcm_calculate_deterministic_blob_velocities and the blob rotation rates Omega
+ * (3Nb) and strain rates E (9Nb, row-major) from
+ * fcm_calculate_deterministic_blob_rotations (either output may be NULL).
+ * Positions are those of the last fcm_set_up_gaussians; the grid must be one the
+ * tiled kernels take (dimensions multiples of 8, ngauss + 8 <= n, ngauss <= 25).
+ * The dipole envelope is narrower than the force envelope: resolve it with
+ * dx <= a/2 or finer for accurate rotation rates. */
+int fcm_set_up_dipole_distribution(fcm_ctx* ctx, const double* F, const double* T, const double* S);
+int fcm_calculate_deterministic_blob_rotations(fcm_ctx* ctx, double* Omega, double* E);
+
 /* The three stages of M*F one at a time on the working grid of one precision
  * (0 = FP64, 1 = FP32, which needs a context of precision 1): spread F (3Nb),
  * Stokes solve of that grid in place, interpolation of it into V (3Nb).  The
@@ -291,6 +308,10 @@ int fcm_batch_set_stream(fcm_batch* b, void* stream);
  * (n records) may be NULL.  Returns FCM_OK or the first failing status (a member
  * whose solve failed keeps its bodies). */
 int fcm_batch_step(fcm_batch* b, const uint64_t* seeds, uint64_t step_index, fcm_step_info* infos);
+/* Lockstep rounds of the last graph step: rounds[0] GMRES iterations (summed
+ * over sweeps), rounds[1] refinement sweeps (0 for FP64 batches); both 0 before
+ * the first graph step.  A member's own counts are in its fcm_step_info. */
+int fcm_batch_last_rounds(const fcm_batch* b, int32_t* rounds);
 
 /* One step of each of n independent suspensions (seeds[i] for context i, the
  * same step_index): all issued, then all awaited, so contexts on different

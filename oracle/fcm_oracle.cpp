@@ -625,6 +625,7 @@ struct orc {
   std::vector<double> gaussx, gaussy, gaussz;  // [np*W + i]
   std::vector<int> indx, indy, indz;
   int ngauss_rows = 0;
+  std::vector<double> gauss_Y;  // the positions of the current Gaussian tables
   Mat ref_Minv, ref_N;
   // collection_of_rigid_bodies fields (collection_of_rigid_bodies.hpp:25-37)
   std::vector<double> blob_ref_pos;  // 3*nb
@@ -788,6 +789,7 @@ void set_up_gaussians(orc* o, const double* Y, int nrows) {
   const double anorm2 = 2.0 * o->a * o->a / PI;
   const double DX = o->DX;
   o->ngauss_rows = nrows;
+  o->gauss_Y.assign(Y, Y + 3 * (size_t)nrows);
   o->gaussx.assign((size_t)nrows * W, 0.0); o->gaussy.assign((size_t)nrows * W, 0.0); o->gaussz.assign((size_t)nrows * W, 0.0);
   o->indx.assign((size_t)nrows * W, 0); o->indy.assign((size_t)nrows * W, 0); o->indz.assign((size_t)nrows * W, 0);
   for (int np = 0; np < nrows; np++) {
@@ -1638,6 +1640,127 @@ int orc_step(orc* o, uint64_t seed, uint64_t step_index, fcm_step_info* info) {
 }
 int orc_step_injected(orc* o, const double* s6, fcm_step_info* info) {
   return step_impl(o, true, s6, 0, 0, info);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ force dipoles
+// No reference code: the FCM force-dipole (stresslet and torque) terms named
+// for this project, restated from the published FCM dipole formulation (Lomholt
+// & Maxey, J. Comput. Phys. 184 (2003) 381-405) on the reference's grid
+// conventions.  Dipole envelope: a Gaussian of width sigma_D = a / (6 sqrt(pi))^(1/3)
+// on the same W-point stencil as the force envelope (fcm_fluid_solver.cpp:131-165).
+// Blob dipole D_ij = S_ij - 1/2 eps_ijk T_k (S symmetric, row-major 9 per blob);
+// force density f_i = F_i Delta + D_ij (x_j - Y_j) / sigma_D^2 Delta_D, whose
+// first moment is D (torque T, stresslet S).  Moments of the velocity,
+// M_kj = DX^3 sum u_k (x_j - Y_j) / sigma_D^2 Delta_D (= the average of du_k/dx_j):
+// Omega_i = 1/2 eps_ijk M_kj, E_ij = (M_ij + M_ji) / 2.
+namespace {
+
+// Dipole weights of blob np, dimension d: g = Delta_D factor, h = g (x - Y) / sigma_D^2,
+// on the stencil points ind[] of set_up_gaussians.
+void dipole_weights(const orc* o, const double* Y, int np, int d, double* g, double* h) {
+  const int W = o->W, ngdh = W / 2;
+  const double sD = o->a / std::cbrt(6.0 * std::sqrt(PI));
+  const double anorm = 1.0 / (std::sqrt(2.0 * PI) * sD);
+  const double anorm2 = 2.0 * sD * sD;
+  const int c = int(Y[3 * np + d] / o->DX);
+  for (int i = 0; i < W; i++) {
+    const int xg = c - ngdh + (i + 1);
+    const double xx = xg * o->DX - Y[3 * np + d];
+    g[i] = anorm * std::exp(-xx * xx / anorm2);
+    h[i] = g[i] * xx / (sD * sD);
+  }
+}
+
+void blob_dipole(const double* T, const double* S, int np, double D[3][3]) {
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) D[i][j] = S ? S[9 * np + 3 * i + j] : 0.0;
+  if (T) {
+    const double* t = T + 3 * np;
+    // -1/2 eps_ijk T_k
+    D[0][1] += -0.5 * t[2];
+    D[1][0] += 0.5 * t[2];
+    D[0][2] += 0.5 * t[1];
+    D[2][0] += -0.5 * t[1];
+    D[1][2] += -0.5 * t[0];
+    D[2][1] += 0.5 * t[0];
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void orc_set_up_dipole_distribution(orc* o, const double* F, const double* T, const double* S) {
+  const int W = o->W, Ny = o->Ny, pad = o->pad, nrows = o->ngauss_rows;
+  std::vector<double> zero;
+  if (!F) {
+    zero.assign(3 * (size_t)nrows, 0.0);
+    F = zero.data();
+  }
+  spread(o, F);
+  if (!T && !S) return;
+  const double* Y = o->gauss_Y.data();
+  std::vector<double> gx(W), hx(W), gy(W), hy(W), gz(W), hz(W);
+  for (int np = 0; np < nrows; np++) {
+    double D[3][3];
+    blob_dipole(T, S, np, D);
+    dipole_weights(o, Y, np, 0, gx.data(), hx.data());
+    dipole_weights(o, Y, np, 1, gy.data(), hy.data());
+    dipole_weights(o, Y, np, 2, gz.data(), hz.data());
+    for (int i = 0; i < W; i++) {
+      const size_t x_index = (size_t)o->indx[np * W + i] * Ny * pad;
+      for (int j = 0; j < W; j++) {
+        const size_t y_index = (size_t)o->indy[np * W + j] * pad;
+        for (int k = 0; k < W; k++) {
+          const size_t index = x_index + y_index + o->indz[np * W + k];
+          const double r[3] = {hx[i] * gy[j] * gz[k], gx[i] * hy[j] * gz[k], gx[i] * gy[j] * hz[k]};
+          o->fx[index] += D[0][0] * r[0] + D[0][1] * r[1] + D[0][2] * r[2];
+          o->fy[index] += D[1][0] * r[0] + D[1][1] * r[1] + D[1][2] * r[2];
+          o->fz[index] += D[2][0] * r[0] + D[2][1] * r[1] + D[2][2] * r[2];
+        }
+      }
+    }
+  }
+}
+
+// Omega (3 per blob) and E (9 per blob, row-major) of the deterministic field.
+void orc_calculate_deterministic_blob_rotations(orc* o, double* Om, double* E) {
+  const int W = o->W, Ny = o->Ny, pad = o->pad, nrows = o->ngauss_rows;
+  const double norm = o->DX * o->DX * o->DX;
+  const double* Y = o->gauss_Y.data();
+  const double* u[3] = {o->ux.data(), o->uy.data(), o->uz.data()};
+#pragma omp parallel for num_threads(g_threads) schedule(dynamic, 16)
+  for (int np = 0; np < nrows; np++) {
+    std::vector<double> gx(W), hx(W), gy(W), hy(W), gz(W), hz(W);
+    dipole_weights(o, Y, np, 0, gx.data(), hx.data());
+    dipole_weights(o, Y, np, 1, gy.data(), hy.data());
+    dipole_weights(o, Y, np, 2, gz.data(), hz.data());
+    double M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int i = 0; i < W; i++) {
+      const size_t x_index = (size_t)o->indx[np * W + i] * Ny * pad;
+      for (int j = 0; j < W; j++) {
+        const size_t y_index = (size_t)o->indy[np * W + j] * pad;
+        for (int k = 0; k < W; k++) {
+          const size_t index = x_index + y_index + o->indz[np * W + k];
+          const double r[3] = {hx[i] * gy[j] * gz[k], gx[i] * hy[j] * gz[k], gx[i] * gy[j] * hz[k]};
+          for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) M[a][b] += u[a][index] * r[b];
+        }
+      }
+    }
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++) M[a][b] *= norm;
+    if (Om) {
+      Om[3 * np] = 0.5 * (M[2][1] - M[1][2]);
+      Om[3 * np + 1] = 0.5 * (M[0][2] - M[2][0]);
+      Om[3 * np + 2] = 0.5 * (M[1][0] - M[0][1]);
+    }
+    if (E)
+      for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) E[9 * np + 3 * a + b] = 0.5 * (M[a][b] + M[b][a]);
+  }
 }
 
 }  // extern "C"

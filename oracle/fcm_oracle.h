@@ -76,6 +76,11 @@ void orc_calculate_random_blob_velocities(orc* o, double* V);
 void orc_set_up_force_distribution(orc* o, const double* F);
 void orc_produce_deterministic_velocity_field(orc* o);
 void orc_calculate_deterministic_blob_velocities(orc* o, double* V);
+/* Force dipoles (no reference code): forces F (3Nb or NULL), torques T (3Nb or
+ * NULL) and stresslets S (9Nb row-major, or NULL) spread with the dipole envelope;
+ * then Omega (3Nb) and E (9Nb) of the deterministic field. */
+void orc_set_up_dipole_distribution(orc* o, const double* F, const double* T, const double* S);
+void orc_calculate_deterministic_blob_rotations(orc* o, double* Om, double* E);
 void orc_get_V(orc* o, double* V);
 void orc_get_grid(orc* o, int which, double* out);  /* 0..2 fx,fy,fz 3..5 ux,uy,uz 6..8 u*_rand */
 void orc_produce_reference_matrices(orc* o);

@@ -68,6 +68,8 @@ def lib():
             "orc_set_up_force_distribution": (None, [vp, D]),
             "orc_produce_deterministic_velocity_field": (None, [vp]),
             "orc_calculate_deterministic_blob_velocities": (None, [vp, D]),
+            "orc_set_up_dipole_distribution": (None, [vp, D, D, D]),
+            "orc_calculate_deterministic_blob_rotations": (None, [vp, D, D]),
             "orc_get_V": (None, [vp, D]),
             "orc_get_grid": (None, [vp, ctypes.c_int, D]),
             "orc_produce_reference_matrices": (None, [vp]),
@@ -259,6 +261,18 @@ class Oracle:
         V = np.zeros(3 * self.Nb)
         lib().orc_calculate_deterministic_blob_velocities(self.h, _dp(V))
         return V
+
+    def set_up_dipole_distribution(self, F=None, T=None, S=None):
+        """Forces, torques and stresslets (9 per blob) spread together (no reference code)."""
+        arr = [None if v is None else _f64(v, (9 if k == 2 else 3) * self.Nb) for k, v in enumerate((F, T, S))]
+        lib().orc_set_up_dipole_distribution(self.h, *[None if a is None else _dp(a) for a in arr])
+
+    def calculate_deterministic_blob_rotations(self):
+        """(Omega (3Nb), E (9Nb)) of the deterministic field."""
+        Om = np.zeros(3 * self.Nb)
+        E = np.zeros(9 * self.Nb)
+        lib().orc_calculate_deterministic_blob_rotations(self.h, _dp(Om), _dp(E))
+        return Om, E
 
     def apply_mobility(self, F):
         self.set_up_force_distribution(F)

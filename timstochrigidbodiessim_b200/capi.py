@@ -62,6 +62,8 @@ SIGNATURES = {
     "fcm_get_V": (ctypes.c_int, [VP, VP]),
     "fcm_get_velocity_field": (ctypes.c_int, [VP, ctypes.c_int32, VP, VP, VP]),
     "fcm_apply_mobility": (ctypes.c_int, [VP, VP, VP]),
+    "fcm_set_up_dipole_distribution": (ctypes.c_int, [VP, VP, VP, VP]),
+    "fcm_calculate_deterministic_blob_rotations": (ctypes.c_int, [VP, VP, VP]),
     "fcm_spread": (ctypes.c_int, [VP, ctypes.c_int32, VP]),
     "fcm_stokes_solve": (ctypes.c_int, [VP, ctypes.c_int32]),
     "fcm_interp": (ctypes.c_int, [VP, ctypes.c_int32, VP]),
@@ -80,6 +82,7 @@ SIGNATURES = {
     "fcm_batch_destroy": (ctypes.c_int, [VP]),
     "fcm_batch_member": (VP, [VP, ctypes.c_int32]),
     "fcm_batch_set_stream": (ctypes.c_int, [VP, VP]),
+    "fcm_batch_last_rounds": (ctypes.c_int, [VP, ctypes.POINTER(ctypes.c_int32)]),
     "fcm_batch_step": (ctypes.c_int, [VP, ctypes.POINTER(ctypes.c_uint64), ctypes.c_uint64,
                                       ctypes.POINTER(FcmStepInfo)]),
     "fcm_step_async": (ctypes.c_int, [VP, ctypes.c_uint64, ctypes.c_uint64]),

@@ -1047,6 +1047,7 @@ void destroy_ctx(Ctx* c) {
   cudaFree(c->d_mdcount);
   if (c->h_gm) cudaFreeHost(c->h_gm);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+  cudaFree(c->d_dip);
   if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
   if (!c->in_batch) {
     cudaFree(c->d_step);
@@ -1858,6 +1859,7 @@ int create_batch(int n, const fcm_params* params, const double* const* refs, Bat
       (st = dev_alloc(&B->d_args, 2 * (size_t)n)) || (st = dev_alloc(&B->d_loop, 4)))
     return fail(st);
   if (cudaMemset(B->d_counter, 0, sizeof(unsigned) * n) != cudaSuccess ||
+      cudaMemset(B->d_loop, 0, sizeof(int) * 4) != cudaSuccess ||
       cudaMemset(B->d_mdcount, 0, sizeof(unsigned) * n * G.max_hn) != cudaSuccess ||
       cudaMemset(B->d_rec, 0, sizeof(StepRecord) * n) != cudaSuccess ||
       cudaMallocHost(&B->h_rec, sizeof(StepRecord) * n) != cudaSuccess ||
@@ -2422,6 +2424,49 @@ int fcm_apply_mobility(fcm_ctx* ctx, const double* F, double* V) {
   return copy_out(c, V, c->d_V, sizeof(double) * 3 * c->Nb);
 }
 
+// Force dipoles on the FP64 deterministic grid (no reference counterpart).
+int fcm_set_up_dipole_distribution(fcm_ctx* ctx, const double* F, const double* T, const double* S) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  if (!c->gauss_ready) {
+    set_error("set_up_gaussians must precede spreading");
+    return FCM_ERR_STATE;
+  }
+  const size_t Nb = (size_t)c->Nb;
+  if (!c->d_dip) FCM_TRY(dev_alloc(&c->d_dip, 33 * (Nb > 0 ? Nb : 1)));
+  double* dT = c->d_dip;
+  double* dS = dT + 3 * Nb;
+  double* dD = dS + 9 * Nb;
+  if (F) {
+    FCM_TRY(copy_in(c, c->d_tmp3, F, sizeof(double) * 3 * Nb));
+  } else {
+    FCM_CUDA(cudaMemsetAsync(c->d_tmp3, 0, sizeof(double) * 3 * Nb, c->stream));
+  }
+  c->det_ready = false;
+  FCM_TRY(spread_t<double>(c, c->g64.blobs, c->d_tmp3));
+  if (!T && !S) return FCM_OK;
+  if (T) FCM_TRY(copy_in(c, dT, T, sizeof(double) * 3 * Nb));
+  if (S) FCM_TRY(copy_in(c, dS, S, sizeof(double) * 9 * Nb));
+  FCM_TRY(launch_blob_dipoles(T ? dT : nullptr, S ? dS : nullptr, c->Nb, dD, c->stream));
+  return launch_spread_dipoles<double>(*c, c->g64.blobs, dD, c->g64.r, c->stream);
+}
+
+int fcm_calculate_deterministic_blob_rotations(fcm_ctx* ctx, double* Omega, double* E) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  if (!c->gauss_ready) {
+    set_error("set_up_gaussians must precede interpolation");
+    return FCM_ERR_STATE;
+  }
+  const size_t Nb = (size_t)c->Nb;
+  if (!c->d_dip) FCM_TRY(dev_alloc(&c->d_dip, 33 * (Nb > 0 ? Nb : 1)));
+  double* dOm = c->d_dip + 21 * Nb;
+  double* dE = dOm + 3 * Nb;
+  FCM_TRY(launch_interp_dipoles<double>(*c, c->g64.blobs, c->g64.r, dOm, dE, c->stream));
+  FCM_TRY(copy_out(c, Omega, dOm, sizeof(double) * 3 * Nb));
+  return copy_out(c, E, dE, sizeof(double) * 9 * Nb);
+}
+
 static int check_stage_precision(Ctx* c, int32_t precision) {
   if (precision != 0 && precision != 1) {
     set_error("precision must be 0 (FP64) or 1 (FP32)");
@@ -2619,6 +2664,17 @@ int fcm_batch_set_stream(fcm_batch* b, void* stream) {
     return FCM_ERR_INVALID;
   }
   b->b->stream = (cudaStream_t)stream;
+  return FCM_OK;
+}
+
+int fcm_batch_last_rounds(const fcm_batch* b, int32_t* rounds) {
+  if (!b || !rounds) {
+    set_error("fcm_batch_last_rounds: null batch or output");
+    return FCM_ERR_INVALID;
+  }
+  const bool graph = b->b->state == 1;
+  rounds[0] = graph ? b->b->h_loop[1] : 0;
+  rounds[1] = graph ? b->b->h_loop[2] : 0;
   return FCM_OK;
 }
 

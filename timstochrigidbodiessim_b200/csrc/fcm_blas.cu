@@ -5,6 +5,8 @@
 // Reductions are single-launch and deterministic: a fixed grid writes one
 // partial per block, and the last block to finish (ticket counter, no waiting)
 // sums the partials in index order.
+#include <algorithm>
+
 #include "fcm_internal.cuh"
 
 namespace fcm {
@@ -490,39 +492,44 @@ __global__ void k_b_fetch(const BMember* __restrict__ mem) {
   m.sys_b[t] = m.Qm[(size_t)m.gm->k * m.nsys + t];
 }
 
+// Columns col = blockIdx.y, blockIdx.y + gridDim.y, ... <= k of each member:
+// a fixed grid whatever k is, so few blocks exit idle.
 __global__ void __launch_bounds__(MDT) k_b_multidot(const BMember* __restrict__ mem, int pass) {
   __shared__ double sh[MDT / 32];
   __shared__ bool last;
   const BMember& m = mem[blockIdx.z];
   const GmState* st = m.gm;
-  const int col = blockIdx.y;
   const unsigned nbk = (unsigned)m.md_blocks;
-  if (blockIdx.x >= nbk || st->done || col > st->k) return;
+  if (blockIdx.x >= nbk || st->done) return;
+  const int k = st->k;
   const long long n = m.nsys;
-  const double* q = m.Qm + (size_t)col * n;
   const double* w = m.sys_b;
-  double s = 0.0;
-  for (long long i = blockIdx.x * (long long)MDT + threadIdx.x; i < n; i += (long long)nbk * MDT)
-    s += q[i] * w[i];
-  for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double b = 0.0;
-    for (int i = 0; i < MDT / 32; ++i) b += sh[i];
-    m.mdpart[(size_t)col * nbk + blockIdx.x] = b;
-    __threadfence();
-    last = (atomicAdd(m.mdcount + col, 1u) == nbk - 1);
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  if (threadIdx.x == 0) {
-    double tot = 0.0;
-    const volatile double* p = m.mdpart + (size_t)col * nbk;
-    for (unsigned int b = 0; b < nbk; ++b) tot += p[b];
-    (pass == 0 ? m.hA : m.hB)[col] = tot;
-    m.mdcount[col] = 0u;
+  double* h = pass == 0 ? m.hA : m.hB;
+  for (int col = blockIdx.y; col <= k; col += gridDim.y) {
+    const double* q = m.Qm + (size_t)col * n;
+    double s = 0.0;
+    for (long long i = blockIdx.x * (long long)MDT + threadIdx.x; i < n; i += (long long)nbk * MDT)
+      s += q[i] * w[i];
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double b = 0.0;
+      for (int i = 0; i < MDT / 32; ++i) b += sh[i];
+      m.mdpart[(size_t)col * nbk + blockIdx.x] = b;
+      __threadfence();
+      last = (atomicAdd(m.mdcount + col, 1u) == nbk - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+      __threadfence();
+      double tot = 0.0;
+      const volatile double* p = m.mdpart + (size_t)col * nbk;
+      for (unsigned int b = 0; b < nbk; ++b) tot += p[b];
+      h[col] = tot;
+      m.mdcount[col] = 0u;
+    }
+    __syncthreads();
   }
 }
 
@@ -599,7 +606,7 @@ int b_gm_fetch(const BatchGeom& b, cudaStream_t s) {
 
 int b_gm_orthogonalize(const BatchGeom& b, cudaStream_t s) {
   for (int pass = 0; pass < 2; ++pass) {
-    k_b_multidot<<<dim3(b.md_blocks, b.max_hn, b.n), MDT, 0, s>>>(b.mem, pass);
+    k_b_multidot<<<dim3(b.md_blocks, std::min(b.max_hn, 8), b.n), MDT, 0, s>>>(b.mem, pass);
     FCM_LAUNCH_CHECK();
     k_b_gs_update<<<dim3(b.max_sys_blocks, b.n), 256, 0, s>>>(b.mem, pass);
     FCM_LAUNCH_CHECK();

@@ -50,10 +50,12 @@ __device__ __forceinline__ int floordiv(int a, int b) { return a >= 0 ? a / b : 
 // floor(base/8)*8 on (zero outside the stencil).
 template <typename T>
 __global__ void k_set_up_gaussians(const double* __restrict__ Y, int n, int W, double dx, double anorm,
-                                   double anorm2, int* __restrict__ base, T* __restrict__ w, T* __restrict__ wc) {
+                                   double anorm2, int* __restrict__ base, T* __restrict__ w, T* __restrict__ wc,
+                                   double* __restrict__ ypos) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= 3 * n) return;
   const double y = Y[t];
+  if (ypos) ypos[t] = y;
   const int xc = (int)__ddiv_rn(y, dx);
   const int b = xc - W / 2 + 1;
   base[t] = b;
@@ -499,6 +501,7 @@ int blob_table_alloc(BlobTable<T>& t, int n, int W, const GridDims& g) {
   t.W = W;
   FCM_CUDA(cudaMalloc(&t.base, sizeof(int) * 3 * (size_t)(n > 0 ? n : 1)));
   FCM_CUDA(cudaMalloc(&t.w, sizeof(T) * 3 * (size_t)W * (n > 0 ? n : 1)));
+  FCM_CUDA(cudaMalloc(&t.ypos, sizeof(double) * 3 * (size_t)(n > 0 ? n : 1)));
   const bool ok = g.nx % TE == 0 && g.ny % TE == 0 && g.nz % TE == 0 && W + TE <= g.nx && W + TE <= g.ny &&
                   W + TE <= g.nz && W <= MAXW && n < (1 << 30);
   if (ok) {
@@ -524,6 +527,10 @@ void blob_table_free(BlobTable<T>& t) {
   cudaFree(t.base);
   cudaFree(t.w);
   cudaFree(t.wc);
+  cudaFree(t.ypos);
+  cudaFree(t.wd);
+  cudaFree(t.hd);
+  cudaFree(t.partial9);
   cudaFree(t.tile_count);
   cudaFree(t.tile_offset);
   cudaFree(t.tile_cursor);
@@ -541,7 +548,7 @@ int launch_set_up_gaussians(const Ctx& c, BlobTable<T>& t, const double* dY, cud
   const double anorm2 = 2.0 * a * a / PI;
   const int nt = 3 * t.n;
   k_set_up_gaussians<T><<<(nt + 127) / 128, 128, 0, s>>>(dY, t.n, t.W, c.g.dx, anorm, anorm2, t.base, t.w,
-                                                          t.tiled ? t.wc : nullptr);
+                                                          t.tiled ? t.wc : nullptr, t.ypos);
   FCM_LAUNCH_CHECK();
   if (t.tiled) {
     const TileGeom g = tile_geom(c.g, t.W);
@@ -600,6 +607,308 @@ template int launch_spread<double>(const Ctx&, const BlobTable<double>&, const d
 template int launch_spread<float>(const Ctx&, const BlobTable<float>&, const double*, float*, cudaStream_t);
 template int launch_interp<double>(const Ctx&, const BlobTable<double>&, const double*, double*, cudaStream_t);
 template int launch_interp<float>(const Ctx&, const BlobTable<float>&, const float*, double*, cudaStream_t);
+
+// ------------------------------------------------------------------ force dipoles
+// No reference code: the FCM force-dipole terms (Lomholt & Maxey, J. Comput.
+// Phys. 184 (2003) 381-405) on the grid conventions above.  Dipole envelope of
+// width sigma_D = a / (6 sqrt(pi))^(1/3) on the same stencils and tiles as the
+// force envelope; per (blob, dimension) the chunk tables hold
+// gD = exp(-xx^2 / (2 sigma_D^2)) / (sqrt(2 pi) sigma_D) and hD = gD xx / sigma_D^2
+// (xx = x - Y).  A blob dipole D_ij = S_ij - 1/2 eps_ijk T_k adds
+// f_i = D_ij (x_j - Y_j) / sigma_D^2 Delta_D to the force grid; the velocity
+// moments M_kj = DX^3 sum u_k (x_j - Y_j) / sigma_D^2 Delta_D give
+// Omega_i = 1/2 eps_ijk M_kj and E_ij = (M_ij + M_ji) / 2.
+namespace {
+
+template <typename T>
+__global__ void k_set_up_dipoles(const double* __restrict__ ypos, const int* __restrict__ base, int n, int W,
+                                 double dx, double anorm, double anorm2, double inv_s2, T* __restrict__ wd,
+                                 T* __restrict__ hd) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 3 * n) return;
+  const double y = ypos[t];
+  const int b = base[t];
+  const int c0 = floordiv(b, TE) * TE;
+  T* g = wd + (size_t)t * NCH * TE;
+  T* h = hd + (size_t)t * NCH * TE;
+  for (int i = 0; i < NCH * TE; ++i) {
+    const int s = c0 + i - b;
+    if (s >= 0 && s < W) {
+      const double xx = __dsub_rn(__dmul_rn((double)(c0 + i), dx), y);
+      const double e = anorm * exp(__ddiv_rn(-__dmul_rn(xx, xx), anorm2));
+      g[i] = (T)e;
+      h[i] = (T)(e * xx * inv_s2);
+    } else {
+      g[i] = (T)0;
+      h[i] = (T)0;
+    }
+  }
+}
+
+__global__ void k_blob_dipoles(const double* __restrict__ T3, const double* __restrict__ S9, int n,
+                               double* __restrict__ D9) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  double D[9];
+  for (int v = 0; v < 9; ++v) D[v] = S9 ? S9[9 * (size_t)b + v] : 0.0;
+  if (T3) {
+    const double t0 = T3[3 * (size_t)b], t1 = T3[3 * (size_t)b + 1], t2 = T3[3 * (size_t)b + 2];
+    D[1] += -0.5 * t2;  // D_01
+    D[3] += 0.5 * t2;   // D_10
+    D[2] += 0.5 * t1;   // D_02
+    D[6] += -0.5 * t1;  // D_20
+    D[5] += -0.5 * t0;  // D_12
+    D[7] += 0.5 * t0;   // D_21
+  }
+  for (int v = 0; v < 9; ++v) D9[9 * (size_t)b + v] = D[v];
+}
+
+// Stage the dipole chunks of blobs list[c0 .. c0+nc): lane (k, d) copies the
+// envelope and derivative chunks of dimension d < 3; lane d = 3 the entry's
+// low word, the blob id and, when D9 is given, the blob's dipole.
+template <typename T>
+__device__ __forceinline__ void stage_dipoles(const unsigned long long* __restrict__ list, int c0, int nc,
+                                              const T* __restrict__ wd, const T* __restrict__ hd,
+                                              const double* __restrict__ D9, T (*sg)[3][TE], T (*sh)[3][TE],
+                                              T (*sD)[9], unsigned* sflag, unsigned* sblob) {
+  const int k = threadIdx.x >> 2, d = threadIdx.x & 3;
+  if (k >= nc) return;
+  const unsigned long long e = list[c0 + k];
+  const unsigned b = (unsigned)(e >> 32), lo = (unsigned)e;
+  if (d < 3) {
+    const size_t off = ((size_t)(3 * b + d) * NCH + ((lo >> (2 * d)) & 3u)) * TE;
+    copy8(sg[k][d], wd + off);
+    copy8(sh[k][d], hd + off);
+  } else {
+    sflag[k] = lo;
+    sblob[k] = b;
+    if (D9)
+      for (int v = 0; v < 9; ++v) sD[k][v] = (T)D9[9 * (size_t)b + v];
+  }
+}
+
+// Adds the dipole force density of the tile's blobs to its points (each CTA
+// owns its tile, so no atomics; tiles without blobs are untouched).
+template <typename T>
+__global__ void __launch_bounds__(64) k_spread_dipole_tiled(const T* __restrict__ wd, const T* __restrict__ hd,
+                                                            const double* __restrict__ D9, TileGeom g,
+                                                            const int* __restrict__ offset,
+                                                            const unsigned long long* __restrict__ list, long long G,
+                                                            T* __restrict__ grid) {
+  __shared__ __align__(16) T sg[SCB][3][TE];
+  __shared__ __align__(16) T sh[SCB][3][TE];
+  __shared__ T sD[SCB][9];
+  __shared__ unsigned sflag[SCB], sblob[SCB];
+  const int tile = blockIdx.x;
+  const int b0 = offset[tile], b1 = offset[tile + 1];
+  if (b0 == b1) return;
+  const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
+  const int t = threadIdx.x;
+  const int z = t & 7, y = t >> 3, yh = t >> 5;
+  T acc[TE][3];
+#pragma unroll
+  for (int x = 0; x < TE; ++x)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) acc[x][c] = 0;
+  for (int c0 = b0; c0 < b1; c0 += SCB) {
+    const int nc = min(SCB, b1 - c0);
+    if (c0 != b0) __syncthreads();
+    stage_dipoles<T>(list, c0, nc, wd, hd, D9, sg, sh, sD, sflag, sblob);
+    __syncthreads();
+    for (int k = 0; k < nc; ++k) {
+      const unsigned fl = sflag[k];
+      if (!((fl >> (EYM + yh)) & 1u)) continue;
+      const T gy = sg[k][1][y], hy = sh[k][1][y], gz = sg[k][2][z], hz = sh[k][2][z];
+      const T gyz = gy * gz, hygz = hy * gz, gyhz = gy * hz;
+      T ca[3], cb[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        ca[c] = sD[k][3 * c] * gyz;                             // times hD_x
+        cb[c] = sD[k][3 * c + 1] * hygz + sD[k][3 * c + 2] * gyhz;  // times gD_x
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (!((fl >> (EXM + h)) & 1u)) continue;
+        T wg[4], wh[4];
+        load_wx4<T>(sg[k][0], 4 * h, wg);
+        load_wx4<T>(sh[k][0], 4 * h, wh);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) acc[4 * h + i][c] += ca[c] * wh[i] + cb[c] * wg[i];
+      }
+    }
+  }
+  const int ox = tx * TE, oy = ty * TE + y, oz = tz * TE + z;
+#pragma unroll
+  for (int x = 0; x < TE; ++x) {
+    const long long idx = ((long long)(ox + x) * g.ny + oy) * g.nz + oz;
+    grid[idx] += acc[x][0];
+    grid[G + idx] += acc[x][1];
+    grid[2 * G + idx] += acc[x][2];
+  }
+}
+
+// Per-(blob, tile) velocity moments M_kj (9 values) into partial9[blob][j][9].
+template <typename T>
+__global__ void __launch_bounds__(64) k_interp_dipole_tiled(const T* __restrict__ wd, const T* __restrict__ hd,
+                                                            const T* __restrict__ grid, TileGeom g,
+                                                            const int* __restrict__ offset,
+                                                            const unsigned long long* __restrict__ list, long long G,
+                                                            T* __restrict__ partial9) {
+  __shared__ __align__(16) T sg[SCB][3][TE];
+  __shared__ __align__(16) T sh[SCB][3][TE];
+  __shared__ unsigned sflag[SCB], sblob[SCB];
+  __shared__ T sred[SCB][2][16];
+  const int tile = blockIdx.x;
+  const int b0 = offset[tile], b1 = offset[tile + 1];
+  if (b0 == b1) return;
+  const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
+  const int t = threadIdx.x;
+  const int z = t & 7, y = t >> 3, yh = t >> 5, lane = t & 31;
+  T u[TE][3];
+  {
+    const int ox = tx * TE, oy = ty * TE + y, oz = tz * TE + z;
+#pragma unroll
+    for (int x = 0; x < TE; ++x) {
+      const long long idx = ((long long)(ox + x) * g.ny + oy) * g.nz + oz;
+      u[x][0] = grid[idx];
+      u[x][1] = grid[G + idx];
+      u[x][2] = grid[2 * G + idx];
+    }
+  }
+  for (int c0 = b0; c0 < b1; c0 += SCB) {
+    const int nc = min(SCB, b1 - c0);
+    if (c0 != b0) __syncthreads();
+    stage_dipoles<T>(list, c0, nc, wd, hd, nullptr, sg, sh, nullptr, sflag, sblob);
+    __syncthreads();
+    for (int k = 0; k < nc; ++k) {
+      const unsigned fl = sflag[k];
+      T v[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) v[i] = 0;
+      if ((fl >> (EYM + yh)) & 1u) {
+        T sx[3] = {0, 0, 0}, tx3[3] = {0, 0, 0};
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          if (!((fl >> (EXM + h)) & 1u)) continue;
+          T wg[4], wh[4];
+          load_wx4<T>(sg[k][0], 4 * h, wg);
+          load_wx4<T>(sh[k][0], 4 * h, wh);
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              sx[c] += u[4 * h + i][c] * wh[i];
+              tx3[c] += u[4 * h + i][c] * wg[i];
+            }
+        }
+        const T gy = sg[k][1][y], hy = sh[k][1][y], gz = sg[k][2][z], hz = sh[k][2][z];
+        const T gyz = gy * gz, hygz = hy * gz, gyhz = gy * hz;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          v[3 * c] = sx[c] * gyz;
+          v[3 * c + 1] = tx3[c] * hygz;
+          v[3 * c + 2] = tx3[c] * gyhz;
+        }
+      }
+      const T r = warp_reduce_scatter16<T>(v, lane);
+      if (!(lane & 1)) sred[k][yh][lane >> 1] = r;
+    }
+    __syncthreads();
+    for (int e = t; e < nc * 9; e += 64) {
+      const int k = e / 9, vv = e - 9 * k;
+      const unsigned jt = (sflag[k] >> EJ) & 63u;
+      partial9[((size_t)sblob[k] * 64 + jt) * 9 + vv] = sred[k][0][vv] + sred[k][1][vv];
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_interp_dipole_reduce(const int* __restrict__ base, const T* __restrict__ partial9, int n,
+                                       TileGeom g, double dx3, double* __restrict__ Om, double* __restrict__ E) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  int f[3], cnt[3];
+  blob_tiles(base, b, g, f, cnt);
+  const int nj = cnt[0] * cnt[1] * cnt[2];
+  double M[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const T* p = partial9 + (size_t)b * 64 * 9;
+  for (int j = 0; j < nj; ++j)
+    for (int v = 0; v < 9; ++v) M[v] += (double)p[9 * j + v];
+  for (int v = 0; v < 9; ++v) M[v] *= dx3;
+  if (Om) {
+    Om[3 * (size_t)b] = 0.5 * (M[7] - M[5]);
+    Om[3 * (size_t)b + 1] = 0.5 * (M[2] - M[6]);
+    Om[3 * (size_t)b + 2] = 0.5 * (M[3] - M[1]);
+  }
+  if (E)
+    for (int a = 0; a < 3; ++a)
+      for (int c = 0; c < 3; ++c) E[9 * (size_t)b + 3 * a + c] = 0.5 * (M[3 * a + c] + M[3 * c + a]);
+}
+
+template <typename T>
+int ensure_dipole_tables(const Ctx& c, BlobTable<T>& t, cudaStream_t s) {
+  if (!t.tiled) {
+    set_error("force dipoles need a grid the tiled kernels take (dimensions multiples of 8, at least ngauss + 8, "
+              "ngauss <= 25)");
+    return FCM_ERR_INVALID;
+  }
+  const size_t nn = (size_t)(t.n > 0 ? t.n : 1);
+  if (!t.wd) FCM_CUDA(cudaMalloc(&t.wd, sizeof(T) * 3 * NCH * TE * nn));
+  if (!t.hd) FCM_CUDA(cudaMalloc(&t.hd, sizeof(T) * 3 * NCH * TE * nn));
+  if (!t.partial9) FCM_CUDA(cudaMalloc(&t.partial9, sizeof(T) * 64 * 9 * nn));
+  if (t.n == 0) return FCM_OK;
+  const double PI = 3.14159265358979323846264338327950288;
+  const double a = c.p.blob_radius;
+  const double sD = a / cbrt(6.0 * sqrt(PI));
+  const double anorm = 1.0 / (sqrt(2.0 * PI) * sD);
+  const double anorm2 = 2.0 * sD * sD;
+  k_set_up_dipoles<T><<<(3 * t.n + 127) / 128, 128, 0, s>>>(t.ypos, t.base, t.n, t.W, c.g.dx, anorm, anorm2,
+                                                          1.0 / (sD * sD), t.wd, t.hd);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+}  // namespace
+
+int launch_blob_dipoles(const double* T3, const double* S9, int n, double* D9, cudaStream_t s) {
+  if (n == 0) return FCM_OK;
+  k_blob_dipoles<<<(n + 127) / 128, 128, 0, s>>>(T3, S9, n, D9);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+template <typename T>
+int launch_spread_dipoles(const Ctx& c, BlobTable<T>& t, const double* dD, T* grid, cudaStream_t s) {
+  FCM_TRY(ensure_dipole_tables<T>(c, t, s));
+  if (t.n == 0) return FCM_OK;
+  k_spread_dipole_tiled<T><<<t.ntiles, 64, 0, s>>>(t.wd, t.hd, dD, tile_geom(c.g, t.W), t.tile_offset, t.tile_list,
+                                                   c.g.G, grid);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+template <typename T>
+int launch_interp_dipoles(const Ctx& c, BlobTable<T>& t, const T* grid, double* dOm, double* dE, cudaStream_t s) {
+  FCM_TRY(ensure_dipole_tables<T>(c, t, s));
+  if (t.n == 0) return FCM_OK;
+  const TileGeom g = tile_geom(c.g, t.W);
+  k_interp_dipole_tiled<T><<<t.ntiles, 64, 0, s>>>(t.wd, t.hd, grid, g, t.tile_offset, t.tile_list, c.g.G,
+                                                   t.partial9);
+  FCM_LAUNCH_CHECK();
+  k_interp_dipole_reduce<T><<<(t.n + 127) / 128, 128, 0, s>>>(t.base, t.partial9, t.n, g,
+                                                              c.g.dx * c.g.dx * c.g.dx, dOm, dE);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+template int launch_spread_dipoles<double>(const Ctx&, BlobTable<double>&, const double*, double*, cudaStream_t);
+template int launch_spread_dipoles<float>(const Ctx&, BlobTable<float>&, const double*, float*, cudaStream_t);
+template int launch_interp_dipoles<double>(const Ctx&, BlobTable<double>&, const double*, double*, double*,
+                                           cudaStream_t);
+template int launch_interp_dipoles<float>(const Ctx&, BlobTable<float>&, const float*, double*, double*,
+                                          cudaStream_t);
 
 // ------------------------------------------------------------------ batched
 // One launch over the tiles of every member: tile_map[blockIdx.x] = (member,
@@ -787,7 +1096,8 @@ extern "C" int fcm_interp_noalloc(int32_t nx, int32_t ny, int32_t nz, double dx,
   // the array keeps the previous call's contents: counters start at zero
   FCM_CUDA(cudaMemsetAsync(s_count, 0, sizeof(int) * (size_t)ntiles, s));
   FCM_CUDA(cudaMemsetAsync(s_cursor, 0, sizeof(int) * (size_t)ntiles, s));
-  k_set_up_gaussians<double><<<(3 * n + 127) / 128, 128, 0, s>>>(Y, n, W, dx, anorm, anorm2, s_base, s_w, s_wc);
+  k_set_up_gaussians<double><<<(3 * n + 127) / 128, 128, 0, s>>>(Y, n, W, dx, anorm, anorm2, s_base, s_w, s_wc,
+                                                                 nullptr);
   FCM_LAUNCH_CHECK();
   k_tile_count<<<(n + 127) / 128, 128, 0, s>>>(s_base, n, g, s_count);
   FCM_LAUNCH_CHECK();

@@ -104,6 +104,12 @@ struct BlobTable {
   unsigned long long* tile_list = nullptr;  // [cap] (blob << 32) | chunk indices, j and half masks
   long long tile_cap = 0;
   T* partial = nullptr;           // [n][64][3] per-(blob, tile) interpolation partials
+  double* ypos = nullptr;         // [n][3] positions of the current tables
+  // force dipoles (allocated on first use): dipole-envelope weights and their
+  // x-derivative factors on the chunks, per-(blob, tile) velocity moments
+  T* wd = nullptr;                // [n][3][4][8]
+  T* hd = nullptr;                // [n][3][4][8]
+  T* partial9 = nullptr;          // [n][64][9]
 };
 
 // Grid buffers and cuFFT plans of one precision.
@@ -220,6 +226,8 @@ struct Ctx {
   int step_pending_status = 0;      // host-driven pending step: its status and record
   fcm_step_info step_pending_info{};
   bool in_batch = false;            // owned by a batch (its step record and arguments too)
+  // force dipoles (allocated on first use): T 3Nb, S 9Nb, D 9Nb, Omega 3Nb, E 9Nb
+  double* d_dip = nullptr;
   // cells
   int ncell_total = 0;
   int *d_cell = nullptr, *d_cell_start = nullptr, *d_cell_count = nullptr, *d_cell_sorted = nullptr, *d_cell_cursor = nullptr;
@@ -346,6 +354,13 @@ template <typename T>
 int launch_spread(const Ctx& c, const BlobTable<T>& t, const double* dF, T* grid, cudaStream_t s);
 template <typename T>
 int launch_interp(const Ctx& c, const BlobTable<T>& t, const T* grid, double* dV, cudaStream_t s);
+// force dipoles (fcm_grid.cu): D (9 per blob) added to the force grid; moments
+// of the velocity grid into Omega (3 per blob) and E (9 per blob)
+template <typename T>
+int launch_spread_dipoles(const Ctx& c, BlobTable<T>& t, const double* dD, T* grid, cudaStream_t s);
+template <typename T>
+int launch_interp_dipoles(const Ctx& c, BlobTable<T>& t, const T* grid, double* dOm, double* dE, cudaStream_t s);
+int launch_blob_dipoles(const double* T3, const double* S9, int n, double* D9, cudaStream_t s);
 // k-space (fcm_kspace.cu)
 template <typename T>
 int launch_project(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s);

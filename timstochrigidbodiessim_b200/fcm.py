@@ -239,6 +239,21 @@ class Suspension:
         self._c(self.L.fcm_apply_mobility(self.h, p, po), "fcm_apply_mobility")
         return V
 
+    # Force dipoles (no reference counterpart): F, T (3 per blob), S (9 per blob).
+    def set_up_dipole_distribution(self, F=None, T=None, S=None):
+        kf, pf = _in(F, 3 * self.Nb)
+        kt, pt = _in(T, 3 * self.Nb)
+        ks, ps = _in(S, 9 * self.Nb)
+        self._c(self.L.fcm_set_up_dipole_distribution(self.h, pf, pt, ps), "fcm_set_up_dipole_distribution")
+
+    def calculate_deterministic_blob_rotations(self):
+        """(Omega (3Nb), E (9Nb)) of the deterministic velocity grid."""
+        Om, po = _out(None, 3 * self.Nb)
+        E, pe = _out(None, 9 * self.Nb)
+        self._c(self.L.fcm_calculate_deterministic_blob_rotations(self.h, po, pe),
+                "fcm_calculate_deterministic_blob_rotations")
+        return Om, E
+
     # The stages of apply_mobility one at a time, on the FP64 (0) or FP32 (1) grid.
     def spread(self, F, precision=0):
         k, p = _in(F, 3 * self.Nb)
@@ -354,6 +369,12 @@ class Batch:
         infos = (FcmStepInfo * self.n)()
         capi.check(self.L.fcm_batch_step(self.h, sd, step_index, infos), "fcm_batch_step")
         return list(infos)
+
+    def last_rounds(self):
+        """(lockstep GMRES iterations, refinement sweeps) of the last graph step."""
+        r = (ctypes.c_int32 * 2)()
+        capi.check(self.L.fcm_batch_last_rounds(self.h, r), "fcm_batch_last_rounds")
+        return int(r[0]), int(r[1])
 
     def close(self):
         if getattr(self, "h", None):
