@@ -257,9 +257,14 @@ def run_ours(args):
     stream = torch.cuda.Stream()
     lib = capi.load()
     algorithm = 1 if args.algorithm == "gdc" else 2
-    wl = configs.WORKLOADS[args.workload]
     seed = 1234 + rank
-    p, ref, x, q, fe = configs.rod_suspension(**wl, seed=seed, algorithm=algorithm)
+    p, ref, x, q, fe = configs.workload(args.workload, seed=seed, algorithm=algorithm)
+    mcmc = None
+    steps_eq = configs.WORKLOADS[args.workload].get("mcmc_steps", 0)
+    if steps_eq:  # Metropolis equilibration of the start (untimed)
+        x, q, st = configs.equilibrate(p, ref, x, q, steps_eq, seed=seed, stream=stream)
+        mcmc = {"steps": int(st.steps), "scale": st.scale, "acceptance_ratio": st.acceptance_ratio,
+                "potential": st.potential}
     results = {}
     for tag, prec, mode in (("fp64", 0, "host"), ("fp64_graph", 0, "graph"), ("mixed", 1, "graph")):
         pp = p.copy(precision=prec)
@@ -348,7 +353,8 @@ def run_ours(args):
             "config": {"workload": args.workload, "bodies": M, "blobs_per_body": p.blobs_per_body,
                        "grid": [p.nx, p.ny, p.nz], "box": p.box[0], "algorithm": args.algorithm,
                        "gmres_tol": p.gmres_tol, "parallelism": "replicas x%d" % world,
-                       "l2": "grid fields (3x%d^3) exceed L2; no flush needed" % p.nx},
+                       "l2": "grid fields (3x%d^3) exceed L2; no flush needed" % p.nx,
+                       "mcmc_equilibration": mcmc},
             "fp64": {"value": fp64_value, "ms_per_step": 1e3 * results["fp64"]["t"] / K,
                      "gmres_iters": results["fp64"]["iters"], "mode": "host-driven fcm_step"},
             "fp64_graph": {"value": fp64g_value, "ms_per_step": 1e3 * results["fp64_graph"]["t"] / K,

@@ -97,6 +97,16 @@ typedef struct fcm_step_info {
   int32_t status;            /* status of the GMRES solve                          */
 } fcm_step_info;
 
+/* State of a Metropolis Monte Carlo run (main.cpp:113-210), carried across calls. */
+typedef struct fcm_mcmc_state {
+  double scale;             /* proposal scale (main.cpp:120 starts at 0.1 a)           */
+  double acceptance_ratio;  /* running acceptance ratio (main.cpp:121 starts at 0.5)   */
+  double potential;         /* energy of the current configuration (output)            */
+  int64_t steps;            /* Metropolis steps done (n of main.cpp; overlap retries
+                               excluded)                                               */
+  int64_t attempts;         /* proposals drawn: the position in the random stream      */
+} fcm_mcmc_state;
+
 typedef struct fcm_ctx fcm_ctx;   /* opaque solver context: one suspension */
 typedef struct fcm_fft fcm_fft;   /* opaque standalone 3-D real FFT        */
 
@@ -284,6 +294,24 @@ int fcm_step(fcm_ctx* ctx, uint64_t seed, uint64_t step_index, fcm_step_info* in
  * synchronously). */
 int fcm_step_async(fcm_ctx* ctx, uint64_t seed, uint64_t step_index);
 int fcm_step_wait(fcm_ctx* ctx, fcm_step_info* info);
+/* collection_of_rigid_bodies.cpp:666-705 with linked_list.cpp:283-360: the
+ * pair potential of the current bodies (blob positions and cells refreshed),
+ * using the MARKOV_CHAIN_MONTE_CARLO energy forms of linked_list.cpp:362-497 for
+ * potentials 0-2 and, for potential 3, the energy whose force is that potential's
+ * polynomial.  Each pair of blobs of different bodies in adjacent cells counts once. */
+int fcm_calculate_potential(fcm_ctx* ctx, double* U);
+/* main.cpp:113-210: n_steps Metropolis steps of global rigid-body moves, on the
+ * device (one CUDA graph, the loop conditional on the device).  Each step moves
+ * every body by dt * scale * (2u - 1) per component (rotations divided by the
+ * body radius), accepts with probability min(1, exp((U_old - U)/kT)), updates the
+ * running acceptance ratio over 20 steps and scales `scale` by 1.02 above a
+ * ratio of 0.5 and 0.98 otherwise.  With skip_on_overlap a proposal that
+ * overlaps is undone and drawn again without counting.  The uniforms are
+ * Philox4x32-10 (seed, state->attempts), so runs continue exactly across calls.
+ * fcm_mcmc_state_init sets the reference's starting scale and ratio. */
+int fcm_mcmc_state_init(const fcm_ctx* ctx, fcm_mcmc_state* state);
+int fcm_mcmc_run(fcm_ctx* ctx, uint64_t seed, int64_t n_steps, fcm_mcmc_state* state);
+
 /* Batches: n independent suspensions (members, each with its own params and
  * blob_ref_pos; body counts and grids may differ, precision and gmres_tol are
  * common, skip_on_overlap must be 0) stepped together.  Per-member work runs

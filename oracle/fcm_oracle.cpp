@@ -1764,3 +1764,134 @@ void orc_calculate_deterministic_blob_rotations(orc* o, double* Om, double* E) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ Metropolis Monte Carlo
+namespace {
+
+// linked_list.cpp:362-497, MARKOV_CHAIN_MONTE_CARLO branches (pair energies);
+// potential 3: U(r) = int_r^rc F_s ((rc^2 - s^2)/(rc^2 - 4a^2))^4 ds.
+double interaction_energy(const orc* o, double r) {
+  const double a = o->a, kT = o->kT;
+  if (o->p.potential == 3) {
+    // degree-8 polynomial integrand: 5-point Gauss-Legendre is exact, all terms positive
+    const double rc = o->p.steric_rc;
+    if (r >= rc) return 0.0;
+    const double xg[5] = {-0.9061798459386640, -0.5384693101056831, 0.0, 0.5384693101056831, 0.9061798459386640};
+    const double wg[5] = {0.2369268850561891, 0.4786286704993665, 0.5688888888888889, 0.4786286704993665,
+                          0.2369268850561891};
+    const double D = rc * rc - 4.0 * a * a, mid = 0.5 * (rc + r), half = 0.5 * (rc - r);
+    double u = 0.0;
+    for (int k = 0; k < 5; ++k) {
+      const double s = mid + half * xg[k];
+      const double t = (rc * rc - s * s) / D;
+      const double t2 = t * t;
+      u += wg[k] * (t2 * t2);
+    }
+    return o->p.steric_fs * half * u;
+  }
+  const double U0 = 20.0 * kT, b = 0.5 * a;
+  double e = (r < 2.0 * a) ? U0 + U0 * (2.0 * a - r) / b : U0 * std::exp((2.0 * a - r) / b);
+  if (o->p.potential == 1 || o->p.potential == 2) {
+    const double A = 5.0 * kT, lambda = 0.5 * a;
+    if (r < 2.0 * a) {
+      double temp = a / lambda;
+      temp = A * std::exp(-temp * temp);
+      e -= temp;
+      e += 2.0 * a * (2.0 * a - r) * temp / (lambda * lambda);
+      if (o->p.potential == 2) {
+        temp = 1.5 * a / lambda;
+        temp = A * std::exp(-temp * temp);
+        e += temp;
+        e -= 3.0 * a * (2.0 * a - r) * temp / (lambda * lambda);
+      }
+    } else {
+      double temp = (r - 3.0 * a) / lambda;
+      e -= A * std::exp(-temp * temp);
+      if (o->p.potential == 2) {
+        temp = (r - 3.5 * a) / lambda;
+        e += A * std::exp(-temp * temp);
+      }
+    }
+  }
+  return e;
+}
+
+// linked_list.cpp:283-360 on the current list.
+double barrier_potential(const orc* o) {
+  double U = 0.0;
+  list_visit(o, o->all_blob_pos, [&](int, int, double dx, double dy, double dz) {
+    U += interaction_energy(o, std::sqrt(dx * dx + dy * dy + dz * dz));
+  });
+  return U;
+}
+
+// Uniform in [0, 1) with 53 bits from Philox4x32-10, counter (i, 0x4D434D43,
+// attempt), key seed: the same numbers as the GPU's Metropolis kernels.
+double mcmc_uniform(uint64_t seed, uint64_t attempt, uint32_t i) {
+  const uint32_t ctr[4] = {i, 0x4D434D43u, (uint32_t)attempt, (uint32_t)(attempt >> 32)};
+  uint32_t out[4];
+  Philox::gen(ctr, (uint32_t)seed, (uint32_t)(seed >> 32), out);
+  return ((double)(out[0] >> 5) * 67108864.0 + (double)(out[1] >> 6)) * (1.0 / 9007199254740992.0);
+}
+
+}  // namespace
+
+extern "C" {
+
+// collection_of_rigid_bodies.cpp:666-705 for the current bodies.
+double orc_calculate_potential(orc* o) {
+  orc_fill_all_blob_pos(o, 0);
+  orc_list_populate(o);
+  return barrier_potential(o);
+}
+
+// main.cpp:113-210 with Philox uniforms (see mcmc_uniform).
+int orc_mcmc_run(orc* o, uint64_t seed, int64_t n_steps, fcm_mcmc_state* st) {
+  double body_radius = 0.0;  // collection_of_rigid_bodies.cpp:110-114
+  for (int m = 0; m < o->nb; ++m) {
+    const double* r = &o->blob_ref_pos[3 * m];
+    body_radius = std::max(body_radius, std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]));
+  }
+  if (body_radius == 0.0) body_radius = o->a;
+  double U_old = orc_calculate_potential(o);
+  const double rs = 20.0;
+  int64_t n = st->steps, attempt = st->attempts;
+  const int64_t target = n + n_steps, cap = attempt + 100 * n_steps + 1000;
+  double scale = st->scale, acc = st->acceptance_ratio;
+  std::vector<double> move(6 * (size_t)o->M);
+  while (n < target && attempt < cap) {
+    for (int b = 0; b < o->M; ++b)
+      for (int d = 0; d < 6; ++d) {
+        double mv = scale * (2.0 * mcmc_uniform(seed, (uint64_t)attempt, (uint32_t)(6 * b + d)) - 1.0);
+        if (d >= 3) mv /= body_radius;
+        move[6 * b + d] = mv;
+      }
+    if (orc_end_of_step_update(o, move.data(), 1.0)) {
+      orc_reset_to_start_of_step(o);
+      ++attempt;
+      continue;
+    }
+    const double U = barrier_potential(o);
+    const double u = mcmc_uniform(seed, (uint64_t)attempt, (uint32_t)(6 * o->M));
+    if (u < std::exp((U_old - U) / o->kT)) {
+      U_old = U;
+      acc = ((rs - 1.0) * acc + 1.0) / rs;
+    } else {
+      orc_reset_to_start_of_step(o);
+      acc *= (rs - 1.0) / rs;
+    }
+    ++n;
+    scale *= acc > 0.5 ? 1.02 : 0.98;
+    ++attempt;
+  }
+  orc_fill_all_blob_pos(o, 0);
+  orc_list_populate(o);
+  st->scale = scale;
+  st->acceptance_ratio = acc;
+  st->potential = U_old;
+  st->steps = n;
+  st->attempts = attempt;
+  return n < target ? FCM_ERR_OVERLAP : FCM_OK;
+}
+
+}  // extern "C"

@@ -81,6 +81,10 @@ void orc_calculate_deterministic_blob_velocities(orc* o, double* V);
  * then Omega (3Nb) and E (9Nb) of the deterministic field. */
 void orc_set_up_dipole_distribution(orc* o, const double* F, const double* T, const double* S);
 void orc_calculate_deterministic_blob_rotations(orc* o, double* Om, double* E);
+/* Pair potential of the current bodies, and Metropolis runs (main.cpp:113-210)
+ * with the same Philox uniforms as the GPU library. */
+double orc_calculate_potential(orc* o);
+int orc_mcmc_run(orc* o, uint64_t seed, int64_t n_steps, fcm_mcmc_state* st);
 void orc_get_V(orc* o, double* V);
 void orc_get_grid(orc* o, int which, double* out);  /* 0..2 fx,fy,fz 3..5 ux,uy,uz 6..8 u*_rand */
 void orc_produce_reference_matrices(orc* o);

@@ -9,7 +9,7 @@ import subprocess
 
 import numpy as np
 
-from timstochrigidbodiessim_b200.params import FcmParams, FcmStepInfo
+from timstochrigidbodiessim_b200.params import FcmMcmcState, FcmParams, FcmStepInfo
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_DIR = os.path.join(ROOT, "oracle")
@@ -69,6 +69,8 @@ def lib():
             "orc_produce_deterministic_velocity_field": (None, [vp]),
             "orc_calculate_deterministic_blob_velocities": (None, [vp, D]),
             "orc_set_up_dipole_distribution": (None, [vp, D, D, D]),
+            "orc_calculate_potential": (ctypes.c_double, [vp]),
+            "orc_mcmc_run": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.c_int64, ctypes.POINTER(FcmMcmcState)]),
             "orc_calculate_deterministic_blob_rotations": (None, [vp, D, D]),
             "orc_get_V": (None, [vp, D]),
             "orc_get_grid": (None, [vp, ctypes.c_int, D]),
@@ -261,6 +263,16 @@ class Oracle:
         V = np.zeros(3 * self.Nb)
         lib().orc_calculate_deterministic_blob_velocities(self.h, _dp(V))
         return V
+
+    def calculate_potential(self):
+        return lib().orc_calculate_potential(self.h)
+
+    def mcmc_run(self, seed, n_steps, state=None):
+        """Metropolis steps (main.cpp:113-210); state defaults to the reference's start."""
+        if state is None:
+            state = FcmMcmcState(scale=0.1 * self.p.blob_radius, acceptance_ratio=0.5)
+        st = lib().orc_mcmc_run(self.h, seed, n_steps, ctypes.byref(state))
+        return st, state
 
     def set_up_dipole_distribution(self, F=None, T=None, S=None):
         """Forces, torques and stresslets (9 per blob) spread together (no reference code)."""

@@ -7,7 +7,7 @@ There is no CPU fallback.
 import ctypes
 import os
 
-from .params import FcmParams, FcmStepInfo
+from .params import FcmMcmcState, FcmParams, FcmStepInfo
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libfcm_b200.so")
 
@@ -77,6 +77,9 @@ SIGNATURES = {
     "fcm_multiply_by_saddle_point_matrix": (ctypes.c_int, [VP, VP, VP]),
     "fcm_invert_saddle_point_system": (ctypes.c_int, [VP, VP, I32, D]),
     "fcm_step": (ctypes.c_int, [VP, ctypes.c_uint64, ctypes.c_uint64, ctypes.POINTER(FcmStepInfo)]),
+    "fcm_calculate_potential": (ctypes.c_int, [VP, D]),
+    "fcm_mcmc_state_init": (ctypes.c_int, [VP, ctypes.POINTER(FcmMcmcState)]),
+    "fcm_mcmc_run": (ctypes.c_int, [VP, ctypes.c_uint64, ctypes.c_int64, ctypes.POINTER(FcmMcmcState)]),
     "fcm_batch_create": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(FcmParams), ctypes.POINTER(VP),
                                         ctypes.POINTER(VP)]),
     "fcm_batch_destroy": (ctypes.c_int, [VP]),

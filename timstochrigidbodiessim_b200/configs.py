@@ -180,6 +180,53 @@ def rod_suspension(M, grid, L=None, phi=None, nb=6, seed=1234, gmres_tol=1e-10, 
     return p, ref, x, q, fe
 
 
+def random_walk_cluster(rng, nb=12, bond=2.2 * A, min_dist=2.0 * A, max_tries=10000):
+    """A rigid cluster shape: a self-avoiding random walk of nb blobs with bonds
+    of length `bond` (each new blob at distance >= min_dist from all earlier
+    ones), re-centred on its centroid.  Returns (nb, 3)."""
+    pts = [np.zeros(3)]
+    tries = 0
+    while len(pts) < nb:
+        tries += 1
+        if tries > max_tries:
+            raise RuntimeError("random-walk cluster could not grow")
+        v = rng.standard_normal(3)
+        c = pts[-1] + bond * v / np.linalg.norm(v)
+        if min(np.linalg.norm(c - p) for p in pts) >= min_dist * (1.0 - 1e-12):
+            pts.append(c)
+    P = np.array(pts)
+    return P - P.mean(axis=0)
+
+
+def cluster_suspension(M, grid, phi, nb=12, seed=1234, gmres_tol=1e-10, gmres_max_iter=100, dt=0.01, kT=1.0,
+                       noise=1, algorithm=2, precision=0, ngauss=20):
+    """M rigid bodies of one random-walk cluster shape (random_walk_cluster; the
+    bodies of a collection share blob_ref_pos, as collection_of_rigid_bodies.hpp
+    has one) at volume fraction phi: centres on a cubic lattice (side M^(1/3)),
+    orientations uniform random; overlaps are allowed and left to the
+    Metropolis equilibration.  Params, blob_ref_pos, x, q and external forces."""
+    rng = np.random.default_rng(seed)
+    ref = random_walk_cluster(rng, nb)
+    Nb = M * nb
+    L = box_for_volume_fraction(Nb, phi)
+    rc = 2.2 * A
+    ncells = max(3, int(L // rc))
+    p = FcmParams.defaults(nx=grid, ny=grid, nz=grid, ngauss=ngauss, dx=L / grid, blob_radius=A,
+                           viscosity=1.0, kT=kT, dt=dt, num_bodies=M, blobs_per_body=nb, ncells=ncells,
+                           potential=3, steric_fs=40.0 * kT / A, steric_rc=rc, gmres_max_iter=gmres_max_iter,
+                           gmres_tol=gmres_tol, fd_delta=1e-5, algorithm=algorithm, precision=precision,
+                           noise=noise, skip_on_overlap=0)
+    side = int(round(M ** (1.0 / 3.0)))
+    if side ** 3 != M:
+        raise ValueError("M must be a cube for the lattice start")
+    g = (np.arange(side) + 0.5) * (L / side)
+    x = np.stack(np.meshgrid(g, g, g, indexing="ij"), axis=-1).reshape(-1, 3)
+    q = random_unit_quaternions(rng, M)
+    fe = np.zeros(6 * M)
+    fe[2::6] = -1.0
+    return p, ref.ravel(), x.ravel(), q.ravel(), fe
+
+
 # The benchmark workloads (sizes as stated; synthetic, seeded).
 WORKLOADS = {
     # 32 rods, L = 64a, 64^3 grid: the CPU-runnable case
@@ -188,13 +235,37 @@ WORKLOADS = {
     "rods2048_phi0.10_g256": dict(M=2048, grid=256, phi=0.10),
     # 8192 rods (49,152 blobs), volume fraction 0.15, 384^3 grid
     "rods8192_phi0.15_g384": dict(M=8192, grid=384, phi=0.15),
+    # 32,768 rigid 12-blob random-walk clusters (393,216 blobs), volume fraction
+    # 0.20, 512^3 grid; started on a lattice, equilibrated by Metropolis steps
+    "clusters32768_phi0.20_g512": dict(kind="clusters", M=32768, grid=512, phi=0.20, mcmc_steps=10000),
 }
 
 
 def workload(name, **overrides):
+    """(params, blob_ref_pos, x, q, forces) of a named workload.  For cluster
+    workloads the Metropolis equilibration (WORKLOADS[name]["mcmc_steps"]) is
+    run separately (equilibrate), since it needs the GPU library."""
     kw = dict(WORKLOADS[name])
     kw.update(overrides)
+    kind = kw.pop("kind", "rods")
+    kw.pop("mcmc_steps", None)
+    if kind == "clusters":
+        return cluster_suspension(**kw)
     return rod_suspension(**kw)
+
+
+def equilibrate(p, ref, x, q, steps, seed=1234, stream=None):
+    """Metropolis equilibration on the GPU (fcm_mcmc_run, main.cpp:113-210) of
+    bodies x, q; returns the new (x, q) and the final fcm_mcmc_state."""
+    from .fcm import Suspension
+    s = Suspension(p, ref, stream=stream)
+    try:
+        s.set_bodies(x, q)
+        st = s.mcmc_run(seed, steps)
+        x2, q2 = s.get_bodies()
+    finally:
+        s.close()
+    return x2, q2, st
 
 
 def nearest_fft_size(n, lo=64, hi=128):

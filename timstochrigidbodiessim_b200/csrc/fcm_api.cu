@@ -248,6 +248,16 @@ GridBufs<double>& grid_of<double>(Ctx* c) { return c->g64; }
 template <>
 GridBufs<float>& grid_of<float>(Ctx* c) { return c->g32; }
 
+// Stencil width of the FP32 tables: the reference's W, narrowed where it reaches
+// beyond 6.5 sigma on each side (weights below 7e-10 of the peak, under the
+// FP32 path's accuracy; the FP64 residual of the refinement keeps the full W).
+int fp32_stencil(const Ctx* c) {
+  const double PI = 3.14159265358979323846264338327950288;
+  const double sigma = c->p.blob_radius / std::sqrt(PI);
+  const int half = (int)std::ceil(6.5 * sigma / c->g.dx);
+  return std::min(c->p.ngauss, 2 * half + 2);
+}
+
 template <typename T>
 int ensure_grid(Ctx* c) {
   GridBufs<T>& gb = grid_of<T>(c);
@@ -261,8 +271,9 @@ int ensure_grid(Ctx* c) {
   FCM_CUFFT(cufftPlanMany(&gb.c2r, 3, n, nullptr, 1, (int)c->g.Gc, nullptr, 1, (int)c->g.G, c2r_type<T>(), 3));
   FCM_CUFFT(cufftSetStream(gb.r2c, c->stream));
   FCM_CUFFT(cufftSetStream(gb.c2r, c->stream));
-  FCM_TRY(blob_table_alloc(gb.blobs, c->Nb, c->p.ngauss, c->g));
-  FCM_TRY(blob_table_alloc(gb.ref_blobs, c->nb, c->p.ngauss, c->g));
+  const int W = sizeof(T) == 4 ? fp32_stencil(c) : c->p.ngauss;
+  FCM_TRY(blob_table_alloc(gb.blobs, c->Nb, W, c->g));
+  FCM_TRY(blob_table_alloc(gb.ref_blobs, c->nb, W, c->g));
   gb.ready = true;
   return FCM_OK;
 }
@@ -860,8 +871,8 @@ int build_step_graph(Ctx* c) {
         cudaMalloc(&c->d_stepargs, 2 * sizeof(uint64_t)) != cudaSuccess ||
         cudaMallocHost(&c->h_stepargs, 2 * sizeof(uint64_t)) != cudaSuccess ||
         cudaMalloc(&c->d_rs, 8 * sizeof(double)) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&c->cap_body[0], cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&c->cap_body[1], cudaStreamNonBlocking) != cudaSuccess) {
+        (!c->cap_body[0] && cudaStreamCreateWithFlags(&c->cap_body[0], cudaStreamNonBlocking) != cudaSuccess) ||
+        (!c->cap_body[1] && cudaStreamCreateWithFlags(&c->cap_body[1], cudaStreamNonBlocking) != cudaSuccess)) {
       cudaGetLastError();
       set_error("step graph: buffer allocation failed");
       c->step_graph_state = -1;
@@ -1048,6 +1059,9 @@ void destroy_ctx(Ctx* c) {
   if (c->h_gm) cudaFreeHost(c->h_gm);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   cudaFree(c->d_dip);
+  cudaFree(c->d_mcmc);
+  cudaFree(c->d_usum);
+  if (c->mcmc_graph) cudaGraphExecDestroy(c->mcmc_graph);
   if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
   if (!c->in_batch) {
     cudaFree(c->d_step);
@@ -1142,6 +1156,10 @@ int create_ctx(const fcm_params* p, const double* ref, Ctx** out) {
     return fail(st);
   if (cudaMallocHost(&c->h_pinned, sizeof(double) * std::max(256, c->maxit_alloc + 8)) != cudaSuccess)
     return fail(FCM_ERR_NOMEM);
+  for (int m = 0; m < nb; ++m) {
+    const double* r = ref + 3 * m;
+    c->body_radius = std::max(c->body_radius, std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]));
+  }
   c->ncell_total = p->ncells * p->ncells * p->ncells;
   if ((st = dev_alloc(&c->d_cell, (size_t)Nb)) || (st = dev_alloc(&c->d_cell_start, (size_t)c->ncell_total + 1)) ||
       (st = dev_alloc(&c->d_cell_count, (size_t)c->ncell_total)) ||
@@ -1342,6 +1360,158 @@ int step_wait(Ctx* c, fcm_step_info* info) {
     FCM_CUDA(cudaStreamSynchronize(c->stream));
     set_error(r.status == FCM_ERR_NONFINITE ? "GMRES residual became non-finite" : "step failed");
     return r.status;
+  }
+  return FCM_OK;
+}
+
+// ------------------------------------------------------------------ Metropolis
+__global__ void k_mcmc_enter(cudaGraphConditionalHandle h, const McmcDev* __restrict__ st) {
+  if (threadIdx.x == 0)
+    cudaGraphSetConditional(h, (st->n < st->n_target && st->attempt < st->attempt_cap) ? 1u : 0u);
+}
+
+__global__ void k_mcmc_set_energy(McmcDev* st, const double* __restrict__ usum) {
+  if (threadIdx.x == 0) st->U_old = 0.5 * *usum;
+}
+
+// main.cpp:162-200: Metropolis test, running acceptance ratio (20 steps), scale.
+__global__ void k_mcmc_decide(cudaGraphConditionalHandle h, McmcDev* st, const double* __restrict__ usum,
+                              const int* __restrict__ ovflag, unsigned int i_acc) {
+  if (threadIdx.x != 0) return;
+  const double rs = 20.0;
+  if (st->skip_on_overlap && *ovflag) {
+    st->restore = 1;
+  } else {
+    const double U = 0.5 * *usum;
+    const double u = mcmc_uniform(st->seed, (uint64_t)st->attempt, i_acc);
+    if (u < exp((st->U_old - U) / st->kT)) {
+      st->U_old = U;
+      st->acc = ((rs - 1.0) * st->acc + 1.0) / rs;
+      st->restore = 0;
+    } else {
+      st->restore = 1;
+      st->acc *= (rs - 1.0) / rs;
+    }
+    st->n += 1;
+    st->scale *= st->acc > 0.5 ? 1.02 : 0.98;
+  }
+  st->attempt += 1;
+  cudaGraphSetConditional(h, (st->n < st->n_target && st->attempt < st->attempt_cap) ? 1u : 0u);
+}
+
+// Energy of the current bodies into *d_usum (twice the potential).
+int potential_sum_dev(Ctx* c) {
+  FCM_TRY(launch_fill_blob_pos(*c, c->d_x, c->d_q, c->d_Y, c->stream));
+  FCM_TRY(cells_build(*c, c->stream));
+  FCM_TRY(cells_potential_terms(*c, c->d_tmp3, c->stream));
+  FCM_TRY(blas_dot(*c, c->d_tmp3, nullptr, c->Nb, c->d_usum, c->stream));
+  return FCM_OK;
+}
+
+int mcmc_alloc(Ctx* c) {
+  if (c->d_mcmc) return FCM_OK;
+  FCM_TRY(dev_alloc(&c->d_mcmc, 1));
+  FCM_TRY(dev_alloc(&c->d_usum, 1));
+  return FCM_OK;
+}
+
+// The Metropolis loop as one graph: while (n < n_target) { propose, positions,
+// cells, [overlap], energy, decide, undo if rejected }.
+int build_mcmc_graph(Ctx* c) {
+  if (c->mcmc_graph) return FCM_OK;
+  if (!c->cap_body[0] && cudaStreamCreateWithFlags(&c->cap_body[0], cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("MCMC graph: stream creation failed");
+    return FCM_ERR_CUDA;
+  }
+  const long long l0 = launch_count();
+  int st = FCM_OK;
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    {
+      StreamSwap sw(c, c->cap_stream);
+      do {
+        cudaGraphConditionalHandle h;
+        if ((st = new_handle(c->stream, &h)) != FCM_OK) break;
+        k_mcmc_enter<<<1, 32, 0, c->stream>>>(h, c->d_mcmc);
+        count_launch();
+        cudaGraph_t body = nullptr;
+        if ((st = add_while_node(c->stream, h, &body)) != FCM_OK) break;
+        const long long lb = launch_count();
+        st = capture_body(c, body, c->cap_body[0], [&] {
+          FCM_TRY(launch_mcmc_propose(*c, c->d_mcmc, c->stream));
+          FCM_TRY(launch_fill_blob_pos(*c, c->d_x, c->d_q, c->d_Y, c->stream));
+          FCM_TRY(cells_build(*c, c->stream));
+          if (c->p.skip_on_overlap) FCM_TRY(cells_overlap(*c, c->d_flag, c->stream));
+          FCM_TRY(cells_potential_terms(*c, c->d_tmp3, c->stream));
+          FCM_TRY(blas_dot(*c, c->d_tmp3, nullptr, c->Nb, c->d_usum, c->stream));
+          k_mcmc_decide<<<1, 32, 0, c->stream>>>(h, c->d_mcmc, c->d_usum, c->d_flag, (unsigned int)(6 * c->M));
+          FCM_LAUNCH_CHECK();
+          FCM_TRY(launch_mcmc_restore(*c, c->d_mcmc, c->stream));
+          return (int)FCM_OK;
+        });
+        c->mcmc_kernels = launch_count() - lb;
+      } while (0);
+    }
+    const cudaError_t e2 = cudaStreamEndCapture(c->cap_stream, &g);
+    if (st == FCM_OK && e2 != cudaSuccess) {
+      set_error(std::string("MCMC graph capture: ") + cudaGetErrorString(e2));
+      st = FCM_ERR_CUDA;
+    }
+  } else {
+    set_error(std::string("cudaStreamBeginCapture: ") + cudaGetErrorString(e));
+    st = FCM_ERR_CUDA;
+  }
+  count_launches(-(launch_count() - l0));
+  if (st == FCM_OK) {
+    e = cudaGraphInstantiate(&c->mcmc_graph, g, 0);
+    if (e != cudaSuccess) {
+      set_error(std::string("MCMC graph instantiate: ") + cudaGetErrorString(e));
+      c->mcmc_graph = nullptr;
+      st = FCM_ERR_CUDA;
+    }
+  }
+  if (g) cudaGraphDestroy(g);
+  cudaGetLastError();
+  return st;
+}
+
+int mcmc_run_dev(Ctx* c, uint64_t seed, long long n_steps, fcm_mcmc_state* state) {
+  FCM_TRY(mcmc_alloc(c));
+  FCM_TRY(build_mcmc_graph(c));
+  McmcDev h;
+  std::memset(&h, 0, sizeof(h));
+  h.seed = seed;
+  h.n = state->steps;
+  h.n_target = state->steps + n_steps;
+  h.attempt = state->attempts;
+  h.attempt_cap = state->attempts + 100 * n_steps + 1000;
+  h.scale = state->scale;
+  h.acc = state->acceptance_ratio;
+  h.body_radius = c->body_radius > 0.0 ? c->body_radius : c->p.blob_radius;
+  h.dt = c->p.dt;
+  h.kT = c->p.kT;
+  h.skip_on_overlap = c->p.skip_on_overlap;
+  FCM_CUDA(cudaMemcpyAsync(c->d_mcmc, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+  FCM_TRY(potential_sum_dev(c));  // U_old of main.cpp:116
+  k_mcmc_set_energy<<<1, 32, 0, c->stream>>>(c->d_mcmc, c->d_usum);
+  FCM_LAUNCH_CHECK();
+  if (n_steps > 0) FCM_CUDA(cudaGraphLaunch(c->mcmc_graph, c->stream));
+  FCM_CUDA(cudaMemcpyAsync(&h, c->d_mcmc, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  FCM_CUDA(cudaStreamSynchronize(c->stream));
+  count_launches((h.attempt - state->attempts) * c->mcmc_kernels + (n_steps > 0 ? 1 : 0));
+  // leave positions and cells of the accepted configuration
+  FCM_TRY(launch_fill_blob_pos(*c, c->d_x, c->d_q, c->d_Y, c->stream));
+  FCM_TRY(cells_build(*c, c->stream));
+  state->scale = h.scale;
+  state->acceptance_ratio = h.acc;
+  state->potential = h.U_old;
+  state->steps = h.n;
+  state->attempts = h.attempt;
+  if (h.n < h.n_target) {
+    set_error("MCMC: too many overlapping proposals (attempt bound reached)");
+    return FCM_ERR_OVERLAP;
   }
   return FCM_OK;
 }
@@ -1929,7 +2099,8 @@ int create_batch(int n, const fcm_params* params, const double* const* refs, Bat
       m.spec[1] = c->g32.c;
       m.partial[1] = c->g32.blobs.partial;
     }
-    m.tg = tile_geom(c->g, c->p.ngauss);
+    m.tg[0] = tile_geom(c->g, c->g64.blobs.W);
+    m.tg[1] = tile_geom(c->g, B->precision == 1 ? c->g32.blobs.W : c->g64.blobs.W);
     m.kp = make_kparams(*c);
     m.dx3 = c->g.dx * c->g.dx * c->g.dx;
     for (int t = 0; t < c->g64.blobs.ntiles; ++t) tmap.push_back(make_int2(i, t));
@@ -2623,6 +2794,42 @@ int fcm_step(fcm_ctx* ctx, uint64_t seed, uint64_t step_index, fcm_step_info* in
     return FCM_ERR_STATE;
   }
   return guard([&] { return step_host(ctx->c, seed, step_index, info); });
+}
+
+int fcm_calculate_potential(fcm_ctx* ctx, double* U) {
+  CTX_CHECK(ctx);
+  if (!U) {
+    set_error("fcm_calculate_potential: null output");
+    return FCM_ERR_INVALID;
+  }
+  return guard([&] {
+    Ctx* c = ctx->c;
+    FCM_TRY(mcmc_alloc(c));
+    FCM_TRY(potential_sum_dev(c));
+    double sum = 0.0;
+    FCM_CUDA(cudaMemcpyAsync(&sum, c->d_usum, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    FCM_CUDA(cudaStreamSynchronize(c->stream));
+    *U = 0.5 * sum;
+    return (int)FCM_OK;
+  });
+}
+
+int fcm_mcmc_state_init(const fcm_ctx* ctx, fcm_mcmc_state* state) {
+  CTX_CHECK(ctx);
+  if (!state) return FCM_ERR_INVALID;
+  std::memset(state, 0, sizeof(*state));
+  state->scale = 0.1 * ctx->c->p.blob_radius;  // main.cpp:120
+  state->acceptance_ratio = 0.5;              // main.cpp:121
+  return FCM_OK;
+}
+
+int fcm_mcmc_run(fcm_ctx* ctx, uint64_t seed, int64_t n_steps, fcm_mcmc_state* state) {
+  CTX_CHECK(ctx);
+  if (!state || n_steps < 0) {
+    set_error("fcm_mcmc_run: a state and n_steps >= 0 are required");
+    return FCM_ERR_INVALID;
+  }
+  return guard([&] { return mcmc_run_dev(ctx->c, seed, n_steps, state); });
 }
 
 int fcm_batch_create(int32_t n, const fcm_params* params, const double* const* blob_ref_pos, fcm_batch** out) {

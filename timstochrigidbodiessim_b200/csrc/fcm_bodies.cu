@@ -284,6 +284,35 @@ __global__ void k_body_update_uniform(double* __restrict__ x, double* __restrict
   body_update_one(x + 3 * n, q + 4 * n, u, Lx, Ly, Lz);
 }
 
+// main.cpp:126-150 and collection_of_rigid_bodies.cpp:759-776: save the body,
+// draw the proposal scale (2u - 1) per component (rotations divided by the body
+// radius) and apply bodies[n].update(nu DT move) with nu = 1.
+__global__ void k_mcmc_propose(double* __restrict__ x, double* __restrict__ q, double* __restrict__ xs,
+                               double* __restrict__ qs, int M, const McmcDev* __restrict__ st, double Lx, double Ly,
+                               double Lz) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= M) return;
+  for (int d = 0; d < 3; ++d) xs[3 * n + d] = x[3 * n + d];
+  for (int d = 0; d < 4; ++d) qs[4 * n + d] = q[4 * n + d];
+  const uint64_t seed = st->seed, attempt = (uint64_t)st->attempt;
+  const double scale = st->scale, dt = st->dt;
+  double u[6];
+  for (int d = 0; d < 6; ++d) {
+    double mv = scale * (2.0 * mcmc_uniform(seed, attempt, (unsigned int)(6 * n + d)) - 1.0);
+    if (d >= 3) mv /= st->body_radius;
+    u[d] = dt * mv;
+  }
+  body_update_one(x + 3 * n, q + 4 * n, u, Lx, Ly, Lz);
+}
+
+__global__ void k_mcmc_restore(double* __restrict__ x, double* __restrict__ q, const double* __restrict__ xs,
+                               const double* __restrict__ qs, int M, const McmcDev* __restrict__ st) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= M || !st->restore) return;
+  for (int d = 0; d < 3; ++d) x[3 * n + d] = xs[3 * n + d];
+  for (int d = 0; d < 4; ++d) q[4 * n + d] = qs[4 * n + d];
+}
+
 // contribution of every body to div(U) for perturbation `comp`
 // (collection_of_rigid_bodies.cpp:941-948).
 __global__ void k_divU_terms(const double* __restrict__ U, const double* __restrict__ U0, int M, int comp,
@@ -338,6 +367,20 @@ int launch_body_update(const Ctx& c, double* x, double* q, const double* U6, dou
                        const double* d_nu) {
   if (c.M == 0) return FCM_OK;
   k_body_update<<<(c.M + 127) / 128, 128, 0, s>>>(x, q, U6, c.M, scale, d_nu, c.g.Lx, c.g.Ly, c.g.Lz);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+int launch_mcmc_propose(const Ctx& c, const McmcDev* st, cudaStream_t s) {
+  if (c.M == 0) return FCM_OK;
+  k_mcmc_propose<<<(c.M + 127) / 128, 128, 0, s>>>(c.d_x, c.d_q, c.d_xs, c.d_qs, c.M, st, c.g.Lx, c.g.Ly, c.g.Lz);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+int launch_mcmc_restore(const Ctx& c, const McmcDev* st, cudaStream_t s) {
+  if (c.M == 0) return FCM_OK;
+  k_mcmc_restore<<<(c.M + 127) / 128, 128, 0, s>>>(c.d_x, c.d_q, c.d_xs, c.d_qs, c.M, st);
   FCM_LAUNCH_CHECK();
   return FCM_OK;
 }

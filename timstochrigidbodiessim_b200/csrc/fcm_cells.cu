@@ -136,6 +136,54 @@ __device__ __forceinline__ double interaction_magnitude(double r, int type, doub
   return mag;
 }
 
+// linked_list.cpp:362-497, the MARKOV_CHAIN_MONTE_CARLO branches (pair
+// energies), and for potential 3 the energy whose force is the polynomial
+// F_s t^4, t = (rc^2 - r^2)/(rc^2 - 4a^2): U(r) = int_r^rc F ds (zero beyond rc).
+__device__ __forceinline__ double interaction_energy(double r, int type, double a, double kT, double fs, double rc) {
+  if (type == 3) {
+    // the integrand is a degree-8 polynomial: 5-point Gauss-Legendre is exact,
+    // and its terms are all positive (no cancellation)
+    if (r >= rc) return 0.0;
+    const double xg[5] = {-0.9061798459386640, -0.5384693101056831, 0.0, 0.5384693101056831, 0.9061798459386640};
+    const double wg[5] = {0.2369268850561891, 0.4786286704993665, 0.5688888888888889, 0.4786286704993665,
+                          0.2369268850561891};
+    const double D = rc * rc - 4.0 * a * a, mid = 0.5 * (rc + r), half = 0.5 * (rc - r);
+    double u = 0.0;
+    for (int k = 0; k < 5; ++k) {
+      const double s = mid + half * xg[k];
+      const double t = (rc * rc - s * s) / D;
+      const double t2 = t * t;
+      u += wg[k] * (t2 * t2);
+    }
+    return fs * half * u;
+  }
+  const double U0 = 20.0 * kT, b = 0.5 * a;
+  double e = (r < 2.0 * a) ? U0 + U0 * (2.0 * a - r) / b : U0 * exp((2.0 * a - r) / b);
+  if (type == 1 || type == 2) {
+    const double A = 5.0 * kT, lambda = 0.5 * a;
+    if (r < 2.0 * a) {
+      double temp = a / lambda;
+      temp = A * exp(-temp * temp);
+      e -= temp;
+      e += 2.0 * a * (2.0 * a - r) * temp / (lambda * lambda);
+      if (type == 2) {
+        temp = 1.5 * a / lambda;
+        temp = A * exp(-temp * temp);
+        e += temp;
+        e -= 3.0 * a * (2.0 * a - r) * temp / (lambda * lambda);
+      }
+    } else {
+      double temp = (r - 3.0 * a) / lambda;
+      e -= A * exp(-temp * temp);
+      if (type == 2) {
+        temp = (r - 3.5 * a) / lambda;
+        e += A * exp(-temp * temp);
+      }
+    }
+  }
+  return e;
+}
+
 // Minimum image d - L trunc(2d/L) (linked_list.cpp:253-256).
 __device__ __forceinline__ double min_image(double d, double L) {
   return __dsub_rn(d, __dmul_rn(L, trunc(__ddiv_rn(__dmul_rn(2.0, d), L))));
@@ -200,6 +248,19 @@ __global__ void k_steric(PairArgs a, int type, double rad, double kT, double fs,
     F[3 * i + 1] = f1;
     F[3 * i + 2] = f2;
   }
+}
+
+// Energy of blob i with all its partners (each pair is seen from both blobs, so
+// the total is half the sum over blobs; linked_list.cpp:283-360).
+__global__ void k_potential_terms(PairArgs a, int type, double rad, double kT, double fs, double rc,
+                                  double* __restrict__ Ui) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.Nb) return;
+  double u = 0.0;
+  visit_partners(a, i, [&](int, double xd, double yd, double zd) {
+    u += interaction_energy(sqrt(xd * xd + yd * yd + zd * zd), type, rad, kT, fs, rc);
+  });
+  Ui[i] = u;
 }
 
 __global__ void k_overlap(PairArgs a, double lim, int* __restrict__ flag) {
@@ -276,6 +337,14 @@ int cells_steric_forces(const Ctx& c, double* F, bool accumulate, cudaStream_t s
   if (c.Nb == 0) return FCM_OK;
   k_steric<<<(c.Nb + 127) / 128, 128, 0, s>>>(pair_args(c), c.p.potential, c.p.blob_radius, c.p.kT, c.p.steric_fs,
                                               c.p.steric_rc, F, accumulate ? 1 : 0);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+int cells_potential_terms(const Ctx& c, double* Ui, cudaStream_t s) {
+  if (c.Nb == 0) return FCM_OK;
+  k_potential_terms<<<(c.Nb + 127) / 128, 128, 0, s>>>(pair_args(c), c.p.potential, c.p.blob_radius, c.p.kT,
+                                                       c.p.steric_fs, c.p.steric_rc, Ui);
   FCM_LAUNCH_CHECK();
   return FCM_OK;
 }

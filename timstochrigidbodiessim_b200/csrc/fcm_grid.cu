@@ -921,7 +921,8 @@ __global__ void __launch_bounds__(64) k_b_spread(const BMember* __restrict__ mem
   const int2 mt = tile_map[blockIdx.x];
   const BMember& m = mem[mt.x];
   if (bskip(m, mask)) return;
-  spread_tile<T>((const T*)m.wc[P], bvec(m, in), m.tg, m.toff[P], m.tlist[P], (long long)m.tg.nx * m.tg.ny * m.tg.nz,
+  spread_tile<T>((const T*)m.wc[P], bvec(m, in), m.tg[P], m.toff[P], m.tlist[P],
+                 (long long)m.tg[P].nx * m.tg[P].ny * m.tg[P].nz,
                  (T*)m.grid[P], mt.y);
 }
 
@@ -931,8 +932,8 @@ __global__ void __launch_bounds__(64) k_b_interp(const BMember* __restrict__ mem
   const int2 mt = tile_map[blockIdx.x];
   const BMember& m = mem[mt.x];
   if (bskip(m, mask)) return;
-  interp_tile<T>((const T*)m.wc[P], (const T*)m.grid[P], m.tg, m.toff[P], m.tlist[P],
-                 (long long)m.tg.nx * m.tg.ny * m.tg.nz, (T*)m.partial[P], mt.y);
+  interp_tile<T>((const T*)m.wc[P], (const T*)m.grid[P], m.tg[P], m.toff[P], m.tlist[P],
+                 (long long)m.tg[P].nx * m.tg[P].ny * m.tg[P].nz, (T*)m.partial[P], mt.y);
 }
 
 template <typename T, int P>
@@ -940,7 +941,7 @@ __global__ void k_b_interp_reduce(const BMember* __restrict__ mem, int out, int 
   const BMember& m = mem[blockIdx.y];
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= m.Nb || bskip(m, mask)) return;
-  interp_reduce_one<T>(m.base[P], (const T*)m.partial[P], m.tg, m.dx3, bvec(m, out), b);
+  interp_reduce_one<T>(m.base[P], (const T*)m.partial[P], m.tg[P], m.dx3, bvec(m, out), b);
 }
 
 }  // namespace

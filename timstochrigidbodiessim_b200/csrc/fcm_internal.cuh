@@ -155,6 +155,20 @@ struct StepRecord {
   int pad_;
 };
 
+// Device-resident state of a Metropolis run (main.cpp:113-210).
+struct McmcDev {
+  uint64_t seed;
+  long long n_target;     // accepted + rejected steps to reach
+  long long n;            // steps done (overlap retries excluded)
+  long long attempt;      // proposals drawn (the random stream position)
+  long long attempt_cap;  // bound on proposals in this run
+  double scale, acc;      // proposal scale, running acceptance ratio
+  double U_old;           // energy of the current configuration
+  double body_radius, dt, kT;
+  int restore;            // the last proposal is undone
+  int skip_on_overlap;
+};
+
 // Device-resident state of one GMRES solve (gmres_solver.cpp:148-306).
 struct GmState {
   int k;        // Arnoldi columns completed (the reference's `iter`)
@@ -217,6 +231,12 @@ struct Ctx {
   uint64_t* d_stepargs = nullptr;   // (seed, counter) of the step in flight
   uint64_t* h_stepargs = nullptr;   // pinned staging of d_stepargs
   double* d_rs = nullptr;           // [0] ||b|| [1] ||r|| [2] inner tolerance [3] nu
+  // Metropolis runs (allocated on first use)
+  McmcDev* d_mcmc = nullptr;
+  double* d_usum = nullptr;         // sum of the per-blob pair energies
+  cudaGraphExec_t mcmc_graph = nullptr;
+  long long mcmc_kernels = 0;       // kernels of one proposal in mcmc_graph
+  double body_radius = 0.0;         // largest |blob_ref_pos| (collection_of_rigid_bodies.cpp:110-114)
   cudaStream_t cap_body[2] = {0, 0};  // capture streams of the loop bodies
   cudaGraphExec_t step_graph = nullptr;
   int step_graph_state = 0;         // 0 not built yet, 1 built, -1 unavailable (host-driven steps)
@@ -272,7 +292,7 @@ struct BMember {
   void* grid[2];
   void* spec[2];
   void* partial[2];
-  TileGeom tg;
+  TileGeom tg[2];  // tile geometry of each precision's tables (their stencil widths differ)
   KParams kp;
   double dx3;
 };
@@ -285,6 +305,30 @@ enum BVec { BV_SYS_A = 0, BV_SYS_B, BV_RHS, BV_SOLN, BV_RES, BV_DX };
 enum BOut { BO_HNORM = 0, BO_RS0, BO_RS1 };
 
 #ifdef __CUDACC__
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy
+// as 1, 2, 3", SC'11): 10 rounds, multipliers 0xD2511F53 / 0xCD9E8D57, Weyl key
+// increments 0x9E3779B9 / 0xBB67AE85.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const unsigned int lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+    const unsigned int lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    k.x += 0x9E3779B9u;
+    k.y += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// Uniform double in [0, 1) with 53 random bits: Philox block with counter
+// (i, 0x4D434D43, attempt_lo, attempt_hi) and key (seed_lo, seed_hi); the top
+// 27 bits of word 0 and the top 26 bits of word 1.
+__device__ __forceinline__ double mcmc_uniform(uint64_t seed, uint64_t attempt, unsigned int i) {
+  const uint4 r = philox4x32_10(make_uint4(i, 0x4D434D43u, (unsigned int)attempt, (unsigned int)(attempt >> 32)),
+                                make_uint2((unsigned int)seed, (unsigned int)(seed >> 32)));
+  return ((double)(r.x >> 5) * 67108864.0 + (double)(r.y >> 6)) * (1.0 / 9007199254740992.0);
+}
+
 __device__ __forceinline__ double* bvec(const BMember& m, int v) {
   switch (v) {
     case BV_SYS_A: return m.sys_a;
@@ -380,12 +424,18 @@ int launch_rigid_projection(const Ctx& c, const double* q, const double* V, doub
 int launch_body_update(const Ctx& c, double* x, double* q, const double* U6, double scale, cudaStream_t s,
                        const double* d_nu = nullptr);
 int launch_body_update_uniform(const Ctx& c, double* x, double* q, const double* e6, cudaStream_t s);
+// Metropolis proposal for every body (bodies saved to xs, qs first) and the
+// undo of a rejected proposal (main.cpp:126-160, :170-185).
+int launch_mcmc_propose(const Ctx& c, const McmcDev* st, cudaStream_t s);
+int launch_mcmc_restore(const Ctx& c, const McmcDev* st, cudaStream_t s);
 int launch_divU_accumulate(const Ctx& c, const double* U6, const double* U0, int component, double delta, double* acc, cudaStream_t s);
 int launch_exclusive_scan(const int* in, int* out, int n, cudaStream_t s);
 // cells (fcm_cells.cu)
 int cells_build(Ctx& c, cudaStream_t s);
 int cells_steric_forces(const Ctx& c, double* F, bool accumulate, cudaStream_t s);
 int cells_overlap(const Ctx& c, int* d_flag, cudaStream_t s);
+// per-blob pair energies (half their sum is the potential of linked_list.cpp:283-360)
+int cells_potential_terms(const Ctx& c, double* Ui, cudaStream_t s);
 int cells_count_pairs(const Ctx& c, long long* d_count, int* pairs, long long cap, cudaStream_t s);
 // vector ops (fcm_blas.cu)
 int blas_dot(const Ctx& c, const double* a, const double* b, long long n, double* d_out, cudaStream_t s);

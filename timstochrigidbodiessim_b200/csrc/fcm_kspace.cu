@@ -168,22 +168,6 @@ __device__ __forceinline__ void divergence_q(int x, int y, int kz, const KParams
   q3 = (kz == k.nzh - 1) ? 0.0 : (double)kz * k.fz;
 }
 
-// ---------------------------------------------------------- Philox4x32-10
-// Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3",
-// SC'11: 10 rounds, multipliers 0xD2511F53 / 0xCD9E8D57, Weyl key increments
-// 0x9E3779B9 / 0xBB67AE85.
-__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
-#pragma unroll
-  for (int r = 0; r < 10; ++r) {
-    const unsigned int lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
-    const unsigned int lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
-    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
-    k.x += 0x9E3779B9u;
-    k.y += 0xBB67AE85u;
-  }
-  return c;
-}
-
 // Two standard normals from two 32-bit words (Box-Muller, single precision).
 __device__ __forceinline__ void box_muller(unsigned int a, unsigned int b, float& n1, float& n2) {
   const float u1 = ((float)a + 0.5f) * 2.3283064365386963e-10f;

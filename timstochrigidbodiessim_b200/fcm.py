@@ -12,7 +12,7 @@ import ctypes
 import numpy as np
 
 from . import capi
-from .params import FcmParams, FcmStepInfo
+from .params import FcmMcmcState, FcmParams, FcmStepInfo
 
 
 def _in(a, n, dtype=np.float64):
@@ -238,6 +238,24 @@ class Suspension:
         V, po = _out(out, 3 * self.Nb)
         self._c(self.L.fcm_apply_mobility(self.h, p, po), "fcm_apply_mobility")
         return V
+
+    # -------------------------------------------------- Metropolis Monte Carlo (main.cpp:113-210)
+    def calculate_potential(self):
+        U = ctypes.c_double(0.0)
+        self._c(self.L.fcm_calculate_potential(self.h, ctypes.byref(U)), "fcm_calculate_potential")
+        return U.value
+
+    def mcmc_state(self):
+        """The reference's starting state: scale 0.1a, acceptance ratio 0.5."""
+        st = FcmMcmcState()
+        self._c(self.L.fcm_mcmc_state_init(self.h, ctypes.byref(st)), "fcm_mcmc_state_init")
+        return st
+
+    def mcmc_run(self, seed, n_steps, state=None):
+        """n_steps Metropolis steps on the device; returns the updated state."""
+        st = self.mcmc_state() if state is None else state
+        self._c(self.L.fcm_mcmc_run(self.h, seed, n_steps, ctypes.byref(st)), "fcm_mcmc_run")
+        return st
 
     # Force dipoles (no reference counterpart): F, T (3 per blob), S (9 per blob).
     def set_up_dipole_distribution(self, F=None, T=None, S=None):

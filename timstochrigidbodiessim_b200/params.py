@@ -80,6 +80,20 @@ class FcmParams(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class FcmMcmcState(ctypes.Structure):
+    """fcm_mcmc_state: a Metropolis run's state, carried across calls."""
+    _fields_ = [
+        ("scale", ctypes.c_double),
+        ("acceptance_ratio", ctypes.c_double),
+        ("potential", ctypes.c_double),
+        ("steps", ctypes.c_int64),
+        ("attempts", ctypes.c_int64),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class FcmStepInfo(ctypes.Structure):
     _fields_ = [
         ("gmres_iters", ctypes.c_int32),
