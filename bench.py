@@ -42,9 +42,14 @@ def parse():
     ap.add_argument("--workload", default="rods2048_phi0.10_g256")
     ap.add_argument("--algorithm", default="em", choices=["em", "gdc"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--ens-modes", default="fp64,fp64_graph,mixed_streams,mixed",
+    ap.add_argument("--ens-modes", default="fp64,fp64_graph,mixed_batch,mixed",
                     help="ensemble arms to time (the JSON line needs fp64, fp64_graph and mixed)")
     ap.add_argument("--nvtx", action="store_true", help="mark the timed region with an NVTX range 'timed'")
+    ap.add_argument("--mixed-tol", type=float, default=None,
+                    help="refinement tolerance of the mixed-precision solver (default %g)" % MIXED_TOL)
+    ap.add_argument("--step-mode", default="graph", choices=["graph", "host"],
+                    help="mixed arm: device-resident graph steps (default) or host-driven fcm_step, whose "
+                         "kernels a profiler can list one by one")
     ap.add_argument("--kernels-only", type=int, default=0, metavar="R",
                     help="profiling mode: R FP64 spread+interp launches and R FP32 mobility products, no steps")
     return ap.parse_args()
@@ -159,6 +164,20 @@ def timed_steps(s, K, seed, start_index, stream, mode="host"):
     return e0.elapsed_time(e1) / 1e3, iters
 
 
+def profiled_traffic(workload):
+    """DRAM bytes per launch of each spread / interpolation kernel of `workload`
+    from the ncu capture summarised in profiles/traffic.txt ({kernel: bytes})."""
+    out = {}
+    try:
+        for line in open(os.path.join(ROOT, "profiles", "traffic.txt")):
+            f = line.split()
+            if len(f) == 3 and not line.startswith("#") and f[0] == workload:
+                out[f[1]] = float(f[2])
+    except OSError:
+        pass
+    return out
+
+
 def kernel_roofline(s, p, stream, precision, reps=20):
     """Per-launch durations of the spread and the interpolation on the grid of one
     precision (0 FP64, 1 FP32), CUDA events on the context's stream around the
@@ -266,7 +285,7 @@ def run_ours(args):
         mcmc = {"steps": int(st.steps), "scale": st.scale, "acceptance_ratio": st.acceptance_ratio,
                 "potential": st.potential}
     results = {}
-    for tag, prec, mode in (("fp64", 0, "host"), ("fp64_graph", 0, "graph"), ("mixed", 1, "graph")):
+    for tag, prec, mode in (("fp64", 0, "host"), ("fp64_graph", 0, "graph"), ("mixed", 1, args.step_mode)):
         pp = p.copy(precision=prec)
         if prec == 1:
             pp.gmres_tol = MIXED_TOL
@@ -301,7 +320,7 @@ def run_ours(args):
     e0.record(stream)
     for i in range(K2):
         sm.set_bodies(xs, qs)
-        run_step(sm, seed, 10000 + i, "graph")
+        run_step(sm, seed, 10000 + i, args.step_mode)
         xs, qs = sm.get_bodies()
     e1.record(stream)
     e1.synchronize()
@@ -321,22 +340,18 @@ def run_ours(args):
     fp64_value = replica_throughput(M, K, world, results["fp64"]["t"])
     fp64g_value = replica_throughput(M, K, world, results["fp64_graph"]["t"])
     if rank == 0:
+        traffic = profiled_traffic(args.workload)
         kernels = []
         for tag in ("fp32", "fp64"):
             bytes_, t_spread, t_interp = kr[tag]
             for name, t_k in (("spread", t_spread), ("interp", t_interp)):
                 ach = bytes_ / t_k / 1e9
                 kernels.append({"kernel": "fcm %s (%s)" % (name, tag), "bytes_per_launch": bytes_,
-                                "ms_per_launch": 1e3 * t_k, "achieved": ach, "frac": ach / hbm})
+                                "ms_per_launch": 1e3 * t_k, "achieved": ach, "frac": ach / hbm,
+                                "traffic": traffic.get("%s_%s" % (name, tag))})
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             cpu = cpu_baseline(p, ref, x, q, fe, results["fp64"]["iters"])
-        traffic = None
-        try:
-            prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
-            traffic = prof.get(args.workload, {}).get("spread_dram_bytes")
-        except Exception:
-            pass
         line = {
             "metric": METRIC,
             "value": value,
@@ -364,8 +379,7 @@ def run_ours(args):
             "gmres_iters_mixed": results["mixed"]["iters"],
             "mixed_gmres_tol": MIXED_TOL,
             "rel_vel_error_mixed_vs_fp64": {"bodies": err_U, "blobs": err_l},
-            "roofline": dict(kernels[0], bound="hbm", peak=hbm, unit="GB/s", traffic=traffic,
-                             peak_source=peak_src),
+            "roofline": dict(kernels[0], bound="hbm", peak=hbm, unit="GB/s", peak_source=peak_src),
             "roofline_kernels": kernels,
             "cpu_baseline": cpu,
             "e2e": {"value": replica_throughput(M, K2, world, t_e2e), "unit": UNIT, "h2d_bytes_per_step": 7 * 8 * M,
@@ -477,7 +491,7 @@ def run_ensemble(args):
     total_bodies = sum(p.num_bodies for p, *_ in insts)
     seeds = list(range(len(insts)))
     res = {}
-    modes = (("fp64", 0, "host"), ("fp64_graph", 0, "graph"), ("mixed_streams", 1, "many"), ("mixed", 1, "batch"))
+    modes = (("fp64", 0, "host"), ("fp64_graph", 0, "graph"), ("mixed_batch", 1, "batch"), ("mixed", 1, "many"))
     wanted = set(args.ens_modes.split(","))
     for tag, prec, mode in modes:
         if tag not in wanted:
@@ -519,7 +533,7 @@ def run_ensemble(args):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         sampler = ClockSampler(0)
-        if mode == "batch":
+        if tag == "mixed":
             sampler.start()
         l0 = lib.fcm_kernel_launch_count()
         if args.nvtx:
@@ -552,7 +566,7 @@ def run_ensemble(args):
         e1.synchronize()
         if args.nvtx:
             torch.cuda.nvtx.range_pop()
-        clocks = sampler.stop() if mode == "batch" else None
+        clocks = sampler.stop() if tag == "mixed" else None
         t = e0.elapsed_time(e1) / 1e3
         res[tag] = dict(t=t, iters=float(np.mean(iters)), launches=lib.fcm_kernel_launch_count() - l0,
                         clocks=clocks, rounds=[float(np.mean([r[i] for r in rounds])) for i in (0, 1)] if rounds else None)
@@ -578,17 +592,18 @@ def run_ensemble(args):
         "config": {"workload": "ensemble64_rods50-500_g64-128", "instances": len(insts), "bodies": total_bodies,
                    "grids": grids, "gmres_tol_fp64": insts[0][0].gmres_tol, "mixed_gmres_tol": MIXED_TOL,
                    "seeds": "0..63",
-                   "parallelism": "one batch of 64 instances: lockstep batched solve, one CUDA graph per step"},
+                   "parallelism": "64 contexts on 64 streams, one CUDA graph per instance step (fcm_step_many)"},
         "fp64": {"value": fp64, "ms_per_step": 1e3 * res["fp64"]["t"] / args.steps, "gmres_iters": res["fp64"]["iters"],
                  "mode": "instances one after another, host-driven fcm_step"},
         "fp64_graph": {"value": fp64g, "ms_per_step": 1e3 * res["fp64_graph"]["t"] / args.steps,
                        "mode": "instances one after another, device-resident graph steps"},
-        "mixed_streams": {"value": total_bodies * args.steps / res["mixed_streams"]["t"],
-                          "ms_per_step": 1e3 * res["mixed_streams"]["t"] / args.steps,
-                          "mode": "64 contexts on 64 streams, one graph per instance step (fcm_step_many)"},
+        "mixed_batch": {"value": total_bodies * args.steps / res["mixed_batch"]["t"],
+                        "ms_per_step": 1e3 * res["mixed_batch"]["t"] / args.steps,
+                        "lockstep_rounds": {"gmres_iters": res["mixed_batch"]["rounds"][0],
+                                            "sweeps": res["mixed_batch"]["rounds"][1]},
+                        "mode": "one fcm_batch: lockstep batched solve, one CUDA graph per step"},
         "mixed_over_fp64": value / fp64, "mixed_over_fp64_graph": value / fp64g,
         "gmres_iters_mixed": res["mixed"]["iters"],
-        "lockstep_rounds_mixed": {"gmres_iters": res["mixed"]["rounds"][0], "sweeps": res["mixed"]["rounds"][1]},
         "rel_vel_error_mixed_vs_fp64_max": {"bodies": max(e[0] for e in errs), "blobs": max(e[1] for e in errs)},
         "gpu_launches": res["mixed"]["launches"],
         "clocks": res["mixed"]["clocks"],
@@ -596,7 +611,10 @@ def run_ensemble(args):
 
 
 def main():
+    global MIXED_TOL
     args = parse()
+    if args.mixed_tol:
+        MIXED_TOL = args.mixed_tol
     if args.workload.startswith("ensemble"):
         run_ensemble(args)
         return

@@ -180,31 +180,91 @@ def rod_suspension(M, grid, L=None, phi=None, nb=6, seed=1234, gmres_tol=1e-10, 
     return p, ref, x, q, fe
 
 
-def random_walk_cluster(rng, nb=12, bond=2.2 * A, min_dist=2.0 * A, max_tries=10000):
-    """A rigid cluster shape: a self-avoiding random walk of nb blobs with bonds
-    of length `bond` (each new blob at distance >= min_dist from all earlier
-    ones), re-centred on its centroid.  Returns (nb, 3)."""
-    pts = [np.zeros(3)]
+def random_walk_cluster(rng, nb=12, bond=2.2 * A, min_dist=2.0 * A, draws=32, max_tries=100000):
+    """A rigid cluster shape grown from a seed blob: each new blob is bonded at
+    distance `bond` to a randomly chosen earlier blob, at least min_dist from all
+    of them; of `draws` such clusters the most compact (smallest largest distance
+    from the centroid) is kept, re-centred on its centroid.  Returns (nb, 3)."""
+    best, best_r = None, np.inf
     tries = 0
-    while len(pts) < nb:
-        tries += 1
-        if tries > max_tries:
-            raise RuntimeError("random-walk cluster could not grow")
-        v = rng.standard_normal(3)
-        c = pts[-1] + bond * v / np.linalg.norm(v)
-        if min(np.linalg.norm(c - p) for p in pts) >= min_dist * (1.0 - 1e-12):
-            pts.append(c)
-    P = np.array(pts)
-    return P - P.mean(axis=0)
+    for _ in range(draws):
+        pts = [np.zeros(3)]
+        while len(pts) < nb:
+            tries += 1
+            if tries > max_tries:
+                raise RuntimeError("cluster could not grow")
+            v = rng.standard_normal(3)
+            c = pts[rng.integers(len(pts))] + bond * v / np.linalg.norm(v)
+            if min(np.linalg.norm(c - p) for p in pts) >= min_dist * (1.0 - 1e-12):
+                pts.append(c)
+        P = np.array(pts)
+        P -= P.mean(axis=0)
+        r = np.linalg.norm(P, axis=1).max()
+        if r < best_r:
+            best, best_r = P, r
+    return best
+
+
+def lattice_start(rng, M, ref, L, min_dist=2.0 * A, tries=16, rounds=12, jitter=0.0):
+    """Bodies of shape ref (nb, 3) near the sites of a cubic lattice of side
+    M^(1/3) in the box L (each centre within +-jitter spacings of its site),
+    each placed and turned to keep its blobs at least min_dist from the blobs of
+    the bodies placed before it.  Sites are filled in 27 classes
+    (i, j, k mod 3), so bodies of one class (three spacings apart) are placed
+    together against a periodic KD-tree of the placed blobs; a site with no clear
+    orientation after `rounds` batches of `tries` draws keeps the draw with the
+    largest clearance.  Returns x (M, 3), q (M, 4)."""
+    from scipy.spatial import cKDTree
+    ref = np.asarray(ref, dtype=np.float64).reshape(-1, 3)
+    nb = len(ref)
+    side = int(round(M ** (1.0 / 3.0)))
+    if side ** 3 != M:
+        raise ValueError("M must be a cube for the lattice start")
+    idx = np.arange(M)
+    ijk = np.stack([idx // (side * side), (idx // side) % side, idx % side], axis=1)
+    sp = L / side
+    x = (ijk + 0.5) * sp
+    q = np.zeros((M, 4))
+    placed_Y = np.zeros((0, 3))
+    cls = (ijk % 3) @ np.array([9, 3, 1])
+    for c in range(27):
+        mem = np.nonzero(cls == c)[0]
+        tree = cKDTree(placed_Y % L, boxsize=L) if len(placed_Y) else None
+        best_q = random_unit_quaternions(rng, len(mem))
+        best_x = x[mem].copy()
+        best_d = np.full(len(mem), -1.0)
+        todo = np.ones(len(mem), dtype=bool)
+        for _ in range(rounds):
+            if tree is None or not todo.any():
+                break
+            sel = np.nonzero(todo)[0]
+            qs = random_unit_quaternions(rng, len(sel) * tries)
+            xs = np.repeat(x[mem[sel]], tries, axis=0) + rng.uniform(-jitter, jitter, (len(sel) * tries, 3)) * sp
+            cb = (xs[:, None, :] + np.einsum("tij,nj->tni", rotation_matrices(qs), ref)) % L   # (s*t, nb, 3)
+            dist, _ = tree.query(cb.reshape(-1, 3), k=1)
+            dist = dist.reshape(len(sel), tries, nb).min(axis=2)
+            k = dist.argmax(axis=1)
+            dk = dist[np.arange(len(sel)), k]
+            better = dk > best_d[sel]
+            best_d[sel[better]] = dk[better]
+            best_q[sel[better]] = qs.reshape(len(sel), tries, 4)[better, k[better]]
+            best_x[sel[better]] = xs.reshape(len(sel), tries, 3)[better, k[better]]
+            todo[sel] = best_d[sel] < min_dist
+        q[mem] = best_q
+        x[mem] = best_x % L
+        Yc = (x[mem][:, None, :] + np.einsum("mij,nj->mni", rotation_matrices(best_q), ref)).reshape(-1, 3)
+        placed_Y = np.concatenate([placed_Y, Yc])
+    return x, q
 
 
 def cluster_suspension(M, grid, phi, nb=12, seed=1234, gmres_tol=1e-10, gmres_max_iter=100, dt=0.01, kT=1.0,
                        noise=1, algorithm=2, precision=0, ngauss=20):
-    """M rigid bodies of one random-walk cluster shape (random_walk_cluster; the
+    """M rigid bodies of one random cluster shape (random_walk_cluster; the
     bodies of a collection share blob_ref_pos, as collection_of_rigid_bodies.hpp
     has one) at volume fraction phi: centres on a cubic lattice (side M^(1/3)),
-    orientations uniform random; overlaps are allowed and left to the
-    Metropolis equilibration.  Params, blob_ref_pos, x, q and external forces."""
+    orientations drawn to clear the neighbours (lattice_start); what overlap
+    remains is left to the Metropolis equilibration.  Params, blob_ref_pos, x,
+    q and external forces."""
     rng = np.random.default_rng(seed)
     ref = random_walk_cluster(rng, nb)
     Nb = M * nb
@@ -216,12 +276,7 @@ def cluster_suspension(M, grid, phi, nb=12, seed=1234, gmres_tol=1e-10, gmres_ma
                            potential=3, steric_fs=40.0 * kT / A, steric_rc=rc, gmres_max_iter=gmres_max_iter,
                            gmres_tol=gmres_tol, fd_delta=1e-5, algorithm=algorithm, precision=precision,
                            noise=noise, skip_on_overlap=0)
-    side = int(round(M ** (1.0 / 3.0)))
-    if side ** 3 != M:
-        raise ValueError("M must be a cube for the lattice start")
-    g = (np.arange(side) + 0.5) * (L / side)
-    x = np.stack(np.meshgrid(g, g, g, indexing="ij"), axis=-1).reshape(-1, 3)
-    q = random_unit_quaternions(rng, M)
+    x, q = lattice_start(rng, M, ref, L)
     fe = np.zeros(6 * M)
     fe[2::6] = -1.0
     return p, ref.ravel(), x.ravel(), q.ravel(), fe
@@ -235,7 +290,7 @@ WORKLOADS = {
     "rods2048_phi0.10_g256": dict(M=2048, grid=256, phi=0.10),
     # 8192 rods (49,152 blobs), volume fraction 0.15, 384^3 grid
     "rods8192_phi0.15_g384": dict(M=8192, grid=384, phi=0.15),
-    # 32,768 rigid 12-blob random-walk clusters (393,216 blobs), volume fraction
+    # 32,768 rigid 12-blob random clusters (393,216 blobs), volume fraction
     # 0.20, 512^3 grid; started on a lattice, equilibrated by Metropolis steps
     "clusters32768_phi0.20_g512": dict(kind="clusters", M=32768, grid=512, phi=0.20, mcmc_steps=10000),
 }

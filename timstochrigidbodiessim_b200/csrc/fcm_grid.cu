@@ -194,27 +194,34 @@ struct V4<double> {
     b = v.y;
   }
 };
-template <>
-struct V4<float> {
-  static __device__ __forceinline__ void ld(const float* p, float& a, float& b) {
-    const float2 v = *reinterpret_cast<const float2*>(p);
-    a = v.x;
-    b = v.y;
-  }
-};
-
-// x-weights xs..xs+3 of a staged chunk into registers.
+// x-weights xs..xs+3 (xs = 0 or 4) of a staged chunk into registers: two
+// 16-byte shared loads for doubles, one for floats.
 template <typename T>
 __device__ __forceinline__ void load_wx4(const T* row, int xs, T wx[4]) {
   V4<T>::ld(row + xs, wx[0], wx[1]);
   V4<T>::ld(row + xs + 2, wx[2], wx[3]);
 }
+template <>
+__device__ __forceinline__ void load_wx4<float>(const float* row, int xs, float wx[4]) {
+  const float4 v = *reinterpret_cast<const float4*>(row + xs);
+  wx[0] = v.x;
+  wx[1] = v.y;
+  wx[2] = v.z;
+  wx[3] = v.w;
+}
+
+// Whether to skip an x-half the stencil misses: worth its test for FP64 (the
+// FP64 pipe is the tighter limit); in FP32 the test costs about what it saves.
+template <typename T>
+__device__ __forceinline__ bool skip_x_half(unsigned fl, int h) {
+  return sizeof(T) == 8 && !((fl >> (EXM + h)) & 1u);
+}
 
 // Tiled spreading: one CTA (64 threads) per 8x8x8 tile.  Thread t owns the
 // x-column (y, z) = (t/8, t%8) of the tile, eight points with three components
 // accumulated in registers.  Warp h covers y-half h and skips blobs whose
-// stencil misses it; an x-half the stencil misses is skipped by the whole CTA
-// (both branches are uniform).
+// stencil misses it; in FP64 an x-half the stencil misses is skipped by the
+// whole CTA (both branches are uniform).
 template <typename T>
 __device__ __forceinline__ void spread_tile(const T* __restrict__ wc, const double* __restrict__ F,
                                             const TileGeom& g, const int* __restrict__ offset,
@@ -244,7 +251,7 @@ __device__ __forceinline__ void spread_tile(const T* __restrict__ wc, const doub
       const T f0 = sF[k][0] * wyz, f1 = sF[k][1] * wyz, f2 = sF[k][2] * wyz;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        if (!((fl >> (EXM + h)) & 1u)) continue;
+        if (skip_x_half<T>(fl, h)) continue;
         T wx[4];
         load_wx4<T>(sw[k][0], 4 * h, wx);
 #pragma unroll
@@ -341,7 +348,7 @@ __device__ __forceinline__ void interp_tile(const T* __restrict__ wc, const T* _
           T s0 = 0, s1 = 0, s2 = 0;
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
-            if (!((fl >> (EXM + h)) & 1u)) continue;
+            if (skip_x_half<T>(fl, h)) continue;
             T wx[4];
             load_wx4<T>(sw[k][0], 4 * h, wx);
 #pragma unroll
@@ -728,7 +735,7 @@ __global__ void __launch_bounds__(64) k_spread_dipole_tiled(const T* __restrict_
       }
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        if (!((fl >> (EXM + h)) & 1u)) continue;
+        if (skip_x_half<T>(fl, h)) continue;
         T wg[4], wh[4];
         load_wx4<T>(sg[k][0], 4 * h, wg);
         load_wx4<T>(sh[k][0], 4 * h, wh);
@@ -791,7 +798,7 @@ __global__ void __launch_bounds__(64) k_interp_dipole_tiled(const T* __restrict_
         T sx[3] = {0, 0, 0}, tx3[3] = {0, 0, 0};
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          if (!((fl >> (EXM + h)) & 1u)) continue;
+          if (skip_x_half<T>(fl, h)) continue;
           T wg[4], wh[4];
           load_wx4<T>(sg[k][0], 4 * h, wg);
           load_wx4<T>(sh[k][0], 4 * h, wh);
