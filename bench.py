@@ -597,11 +597,12 @@ def run_ensemble(args):
                  "mode": "instances one after another, host-driven fcm_step"},
         "fp64_graph": {"value": fp64g, "ms_per_step": 1e3 * res["fp64_graph"]["t"] / args.steps,
                        "mode": "instances one after another, device-resident graph steps"},
-        "mixed_batch": {"value": total_bodies * args.steps / res["mixed_batch"]["t"],
-                        "ms_per_step": 1e3 * res["mixed_batch"]["t"] / args.steps,
-                        "lockstep_rounds": {"gmres_iters": res["mixed_batch"]["rounds"][0],
-                                            "sweeps": res["mixed_batch"]["rounds"][1]},
-                        "mode": "one fcm_batch: lockstep batched solve, one CUDA graph per step"},
+        "mixed_batch": None if "mixed_batch" not in res else {
+            "value": total_bodies * args.steps / res["mixed_batch"]["t"],
+            "ms_per_step": 1e3 * res["mixed_batch"]["t"] / args.steps,
+            "lockstep_rounds": {"gmres_iters": res["mixed_batch"]["rounds"][0],
+                                "sweeps": res["mixed_batch"]["rounds"][1]},
+            "mode": "one fcm_batch: lockstep batched solve, one CUDA graph per step"},
         "mixed_over_fp64": value / fp64, "mixed_over_fp64_graph": value / fp64g,
         "gmres_iters_mixed": res["mixed"]["iters"],
         "rel_vel_error_mixed_vs_fp64_max": {"bodies": max(e[0] for e in errs), "blobs": max(e[1] for e in errs)},

@@ -17,6 +17,7 @@
 // fcm_fluid_solver.cpp:556-562 is fused: tiles without blobs write zeros).  No
 // atomics touch the grid.  Grids that cannot be tiled (a dimension not a multiple
 // of 8, W + 8 > n, or W > 25) use the per-blob atomic scatter.
+#include <algorithm>
 #include <mutex>
 #include <string>
 
@@ -281,6 +282,187 @@ __global__ void __launch_bounds__(64) k_spread_tiled(const T* __restrict__ wc, c
   spread_tile<T>(wc, F, g, offset, list, G, grid, blockIdx.x);
 }
 
+// ------------------------------------------------------------------ persistent pipelined tiles
+// Work items of a persistent CTA: its tiles blockIdx.x, +gridDim.x, ..., each cut
+// into staging rounds of SCB blobs (one empty round for a tile without blobs).
+// The tile offsets are loaded two tiles ahead, so the generator never waits.
+struct TileItem {
+  int tile, c0, nc, last;
+};
+
+struct ItemGen {
+  const int* __restrict__ offset;
+  int ntiles, stride;
+  int tile, c0, b1;
+  int o1a, o1b, o2a, o2b;  // offsets of tile + stride and tile + 2 stride
+
+  __device__ __forceinline__ void load_off(int tl, int& a, int& b) const {
+    if (tl < ntiles) {
+      a = offset[tl];
+      b = offset[tl + 1];
+    } else {
+      a = b = 0;
+    }
+  }
+  __device__ __forceinline__ bool first() {
+    tile = blockIdx.x;
+    if (tile >= ntiles) return false;
+    c0 = offset[tile];
+    b1 = offset[tile + 1];
+    load_off(tile + stride, o1a, o1b);
+    load_off(tile + 2 * stride, o2a, o2b);
+    return true;
+  }
+  __device__ __forceinline__ bool next() {
+    if (c0 + SCB < b1) {
+      c0 += SCB;
+      return true;
+    }
+    tile += stride;
+    if (tile >= ntiles) return false;
+    c0 = o1a;
+    b1 = o1b;
+    o1a = o2a;
+    o1b = o2b;
+    load_off(tile + 2 * stride, o2a, o2b);
+    return true;
+  }
+  __device__ __forceinline__ TileItem item() const {
+    return TileItem{tile, c0, min(SCB, b1 - c0), (c0 + SCB >= b1) ? 1 : 0};
+  }
+};
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Asynchronous copy of one 8-weight chunk (32 B float, 64 B double) to shared memory.
+template <typename T>
+__device__ __forceinline__ void chunk_async(T* dst, const T* __restrict__ src) {
+#pragma unroll
+  for (int i = 0; i < (int)(TE * sizeof(T) / 16); ++i) cp_async16(reinterpret_cast<char*>(dst) + 16 * i,
+                                                                  reinterpret_cast<const char*>(src) + 16 * i);
+}
+
+// Persistent, software-pipelined tiled spreading: the arithmetic of
+// k_spread_tiled (each point sums its blobs in the same order), but a CTA walks
+// over many tiles and, while it accumulates one staging round, the weight
+// chunks of the next round are already on their way to the other shared buffer
+// (cp.async) and the list entries of the round after that are being loaded.
+template <typename T>
+__global__ void __launch_bounds__(64) k_spread_pipe(const T* __restrict__ wc, const double* __restrict__ F, TileGeom g,
+                                                    const int* __restrict__ offset,
+                                                    const unsigned long long* __restrict__ list, long long G,
+                                                    T* __restrict__ grid, int ntiles) {
+  __shared__ __align__(16) T sw[2][SCB][3][TE];
+  __shared__ __align__(16) T sF[2][SCB][4];
+  __shared__ unsigned sflag[2][SCB];
+  const int t = threadIdx.x, k = t >> 2, d = t & 3;
+  const int z = t & 7, y = t >> 3, yh = t >> 5;
+  ItemGen gen{offset, ntiles, (int)gridDim.x, 0, 0, 0, 0, 0, 0, 0};
+  if (!gen.first()) return;  // uniform over the CTA
+  TileItem cur = gen.item();
+  bool v1 = gen.next();
+  TileItem nx1 = v1 ? gen.item() : TileItem{0, 0, 0, 0};
+  bool v2 = v1 && gen.next();
+  TileItem nx2 = v2 ? gen.item() : TileItem{0, 0, 0, 0};
+  // prologue: the first round straight into buffer 0
+  if (k < cur.nc) {
+    const unsigned long long e = list[cur.c0 + k];
+    const unsigned b = (unsigned)(e >> 32), lo = (unsigned)e;
+    if (d < 3) {
+      chunk_async<T>(sw[0][k][d], wc + ((size_t)(3 * b + d) * NCH + ((lo >> (2 * d)) & 3u)) * TE);
+    } else {
+      sflag[0][k] = lo;
+      sF[0][k][0] = (T)F[3 * (size_t)b];
+      sF[0][k][1] = (T)F[3 * (size_t)b + 1];
+      sF[0][k][2] = (T)F[3 * (size_t)b + 2];
+    }
+  }
+  cp_async_commit();
+  unsigned long long e1 = (v1 && k < nx1.nc) ? list[nx1.c0 + k] : 0ull;
+  cp_async_wait_all();
+  __syncthreads();
+  T acc[TE][3];
+#pragma unroll
+  for (int x = 0; x < TE; ++x)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) acc[x][c] = 0;
+  int buf = 0;
+  while (true) {
+    // the next round's weights into the other buffer, its forces into registers
+    double fn0 = 0, fn1 = 0, fn2 = 0;
+    unsigned fln = 0;
+    if (v1 && k < nx1.nc) {
+      const unsigned b = (unsigned)(e1 >> 32), lo = (unsigned)e1;
+      if (d < 3) {
+        chunk_async<T>(sw[buf ^ 1][k][d], wc + ((size_t)(3 * b + d) * NCH + ((lo >> (2 * d)) & 3u)) * TE);
+      } else {
+        fln = lo;
+        fn0 = F[3 * (size_t)b];
+        fn1 = F[3 * (size_t)b + 1];
+        fn2 = F[3 * (size_t)b + 2];
+      }
+    }
+    cp_async_commit();
+    // the entries of the round after
+    const unsigned long long e2 = (v2 && k < nx2.nc) ? list[nx2.c0 + k] : 0ull;
+    // accumulate this round
+    for (int kk = 0; kk < cur.nc; ++kk) {
+      const unsigned fl = sflag[buf][kk];
+      if (!((fl >> (EYM + yh)) & 1u)) continue;
+      const T wyz = sw[buf][kk][1][y] * sw[buf][kk][2][z];
+      const T f0 = sF[buf][kk][0] * wyz, f1 = sF[buf][kk][1] * wyz, f2 = sF[buf][kk][2] * wyz;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (skip_x_half<T>(fl, h)) continue;
+        T wx[4];
+        load_wx4<T>(sw[buf][kk][0], 4 * h, wx);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          acc[4 * h + i][0] += f0 * wx[i];
+          acc[4 * h + i][1] += f1 * wx[i];
+          acc[4 * h + i][2] += f2 * wx[i];
+        }
+      }
+    }
+    if (v1 && k < nx1.nc && d == 3) {
+      sflag[buf ^ 1][k] = fln;
+      sF[buf ^ 1][k][0] = (T)fn0;
+      sF[buf ^ 1][k][1] = (T)fn1;
+      sF[buf ^ 1][k][2] = (T)fn2;
+    }
+    if (cur.last) {  // the tile is complete: every point written once
+      const int tz = cur.tile % g.ntz, ty = (cur.tile / g.ntz) % g.nty, tx = cur.tile / (g.ntz * g.nty);
+      const int ox = tx * TE, oy = ty * TE + y, oz = tz * TE + z;
+#pragma unroll
+      for (int x = 0; x < TE; ++x) {
+        const long long idx = ((long long)(ox + x) * g.ny + oy) * g.nz + oz;
+        grid[idx] = acc[x][0];
+        grid[G + idx] = acc[x][1];
+        grid[2 * G + idx] = acc[x][2];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[x][c] = 0;
+      }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    if (!v1) break;
+    cur = nx1;
+    nx1 = nx2;
+    v1 = v2;
+    e1 = e2;
+    buf ^= 1;
+    v2 = v2 && gen.next();
+    if (v2) nx2 = gen.item();
+  }
+}
+
 // Sum of v[0..15] over the 32 lanes of a warp, scattered: afterwards lanes 2i
 // and 2i+1 hold in v[0] the warp total of value i (16 shuffles for 16 values).
 template <typename T>
@@ -500,6 +682,25 @@ TileGeom tile_geom(const GridDims& g, int W) {
   return TileGeom{g.nx / TE, g.ny / TE, g.nz / TE, g.nx, g.ny, g.nz, W};
 }
 
+// CTAs of a persistent kernel: as many as fit on the device at once
+// (resident CTAs per SM x SMs), looked up once per kernel and device.
+template <typename K>
+int persistent_ctas(K kernel, int threads, int device) {
+  static std::mutex mtx;
+  static int cache[64] = {0};
+  std::lock_guard<std::mutex> lock(mtx);
+  const int dev = (device >= 0 && device < 64) ? device : 0;
+  if (!cache[dev]) {
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm < 1)
+      per_sm = 1;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 1;
+    cudaGetLastError();
+    cache[dev] = per_sm * sms;
+  }
+  return cache[dev];
+}
+
 template <typename T>
 int blob_table_alloc(BlobTable<T>& t, int n, int W, const GridDims& g) {
   if (t.n == n && t.W == W && t.base) return FCM_OK;
@@ -575,8 +776,16 @@ int launch_set_up_gaussians(const Ctx& c, BlobTable<T>& t, const double* dY, cud
 template <typename T>
 int launch_spread(const Ctx& c, const BlobTable<T>& t, const double* dF, T* grid, cudaStream_t s) {
   if (t.tiled) {
-    k_spread_tiled<T><<<t.ntiles, 64, 0, s>>>(t.wc, dF, tile_geom(c.g, t.W), t.tile_offset, t.tile_list, c.g.G,
-                                               grid);
+    // FP64: the persistent pipelined kernel (its staging latency is the limit);
+    // FP32: one CTA per tile (issue-bound; more resident CTAs hide the latency)
+    if (sizeof(T) == 8) {
+      const int ctas = std::min(t.ntiles, persistent_ctas(k_spread_pipe<T>, 64, c.device));
+      k_spread_pipe<T><<<ctas, 64, 0, s>>>(t.wc, dF, tile_geom(c.g, t.W), t.tile_offset, t.tile_list, c.g.G, grid,
+                                          t.ntiles);
+    } else {
+      k_spread_tiled<T><<<t.ntiles, 64, 0, s>>>(t.wc, dF, tile_geom(c.g, t.W), t.tile_offset, t.tile_list, c.g.G,
+                                                 grid);
+    }
     FCM_LAUNCH_CHECK();
     return FCM_OK;
   }
