@@ -45,3 +45,34 @@ def test_driver_matches_oracle(gpu, tmp_path, algorithm):
     assert np.abs(xg - xo).max() < 1e-8
     assert np.abs(qg - qo).max() < 1e-8
     assert "skipped_steps 0" in r.stdout
+
+
+def test_driver_mcmc_matches_oracle(gpu, tmp_path):
+    """The driver's MARKOV_CHAIN_MONTE_CARLO mode (main.cpp:113-210): samples
+    every 200 steps once past mcmc_save_after, the last one equal to the
+    oracle's run of the same length and seed; also writes the blob forces file
+    in time-stepping mode."""
+    p, ref, x, q, fe = configs.rod_suspension(M=32, grid=32, L=24.0, seed=3)
+    p = p.copy(potential=0, ncells=3)
+    shape = tmp_path / "shape.txt"
+    shape.write_text("\n".join("%.17g %.17g %.17g" % tuple(ref[3 * m:3 * m + 3]) for m in range(p.blobs_per_body)))
+    ic = tmp_path / "ic.dat"
+    ic.write_text("0 " + " ".join("%.17g %.17g %.17g %.17g %.17g %.17g %.17g" % (tuple(x[3 * n:3 * n + 3]) +
+                                                                                tuple(q[4 * n:4 * n + 4]))
+                                  for n in range(p.num_bodies)) + "\n")
+    args = [build.DRIVER, "shape=%s" % shape, "ic=%s" % ic, "mcmc=400", "mcmc_save_after=0", "seed=9",
+            "name=%s" % (tmp_path / "mc"), "digits=17"]
+    for k in ("nx", "ny", "nz", "ngauss", "dx", "dt", "ncells", "potential", "kT"):
+        args.append("%s=%r" % (k, getattr(p, k)))
+    r = subprocess.run(args, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = (tmp_path / "mc.dat").read_text().strip().splitlines()
+    assert len(lines) == 2 and lines[-1].split()[0].startswith("4")
+    last = np.array([float(v) for v in lines[-1].split()])
+    o = Oracle(p, ref)
+    o.set_bodies(x, q)
+    st, state = o.mcmc_run(9, 400)
+    xo, qo = o.get_bodies()
+    assert np.abs(last[1:].reshape(-1, 7)[:, :3].ravel() - xo).max() < 1e-12
+    assert np.abs(last[1:].reshape(-1, 7)[:, 3:].ravel() - qo).max() < 1e-12
+    assert "Saved sample 400" in r.stdout

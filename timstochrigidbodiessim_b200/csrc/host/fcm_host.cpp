@@ -168,6 +168,20 @@ void collection_of_rigid_bodies::write_data_to_file(double t, const std::string&
   f << std::endl;
 }
 
+void collection_of_rigid_bodies::write_blob_forces_to_file(double t, const std::string& name, int digits) const {
+  std::ofstream f(name, std::ios::app);
+  f << std::scientific << std::setprecision(digits) << t << " ";
+  for (size_t i = 0; i < blob_forces.n_elem(); ++i) f << blob_forces(i) << " ";
+  f << std::endl;
+}
+
+double collection_of_rigid_bodies::calculate_potential() {
+  double U = 0.0;
+  check(fcm_calculate_potential(ctx_, &U), "calculate_potential");
+  pull_blob_pos();
+  return U;
+}
+
 // ------------------------------------------------------------------ linked_list
 void linked_list::initialise(int, int, int) {}  // the cell map is built with the context
 

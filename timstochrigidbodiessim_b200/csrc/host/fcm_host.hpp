@@ -144,8 +144,11 @@ class collection_of_rigid_bodies {
   void reset_to_start_of_step();                         // :792-796
   double calculate_divU(fcm_fluid_solver& fcm);          // :869-953
   bool check_for_overlap();                              // :195-205
+  double calculate_potential();                          // :666-705
   // :798-814 (state part); the reference writes 6 significant digits
   void write_data_to_file(double t, const std::string& name, int digits = 6) const;
+  // :816-833, the blob forces of the last calculate_forces
+  void write_blob_forces_to_file(double t, const std::string& name, int digits = 6) const;
 
   fcm_ctx* ctx() const { return ctx_; }
   void pull_bodies();

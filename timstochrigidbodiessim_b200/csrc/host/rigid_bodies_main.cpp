@@ -17,12 +17,20 @@
 //                    and <prefix>_velocities.dat (body velocities, main.cpp:343-367)
 //   save_every=<n>   steps between saves (default 1)
 //   digits=<n>       significant digits of the saved states (default 6, the reference's)
+//   ic_pick=last|random  which state of the ic file to start from (IC_READ_IN_LAST /
+//                    IC_READ_IN_RANDOM, collection_of_rigid_bodies.cpp:265-339)
+//   mcmc=<n>         Metropolis sampling instead of time stepping (MARKOV_CHAIN_MONTE_CARLO,
+//                    main.cpp:113-210): n steps, reported every 200 and saved to
+//                    <prefix>.dat every 200 once past mcmc_save_after (default 100000)
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <iomanip>
 #include <map>
+#include <random>
+#include <stdexcept>
+#include <algorithm>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -48,6 +56,22 @@ static bool set_param(fcm_params& p, const std::string& k, const std::string& v)
 #undef I
 #undef F
   return false;
+}
+
+// The non-empty lines of a state file, each as its numbers.
+static std::vector<std::vector<double>> read_states(const std::string& path) {
+  std::ifstream f(path);
+  std::string line;
+  std::vector<std::vector<double>> out;
+  while (std::getline(f, line)) {
+    if (line.find_first_not_of(" \t\r") == std::string::npos) continue;
+    std::istringstream is(line);
+    std::vector<double> v;
+    double x;
+    while (is >> x) v.push_back(x);
+    out.push_back(v);
+  }
+  return out;
 }
 
 static std::vector<double> read_numbers_last_line(const std::string& path) {
@@ -94,7 +118,15 @@ int main(int argc, char** argv) {
     while (f >> v) ref.push_back(v);
   }
   p.blobs_per_body = (int32_t)(ref.size() / 3);
-  const std::vector<double> ic = read_numbers_last_line(opt["ic"]);
+  std::vector<double> ic = read_numbers_last_line(opt["ic"]);
+  if (opt.count("ic_pick") && opt["ic_pick"] == "random") {  // IC_READ_IN_RANDOM
+    const std::vector<std::vector<double>> states = read_states(opt["ic"]);
+    if (!states.empty()) {
+      std::mt19937_64 rng(seed);
+      ic = states[std::uniform_int_distribution<size_t>(0, states.size() - 1)(rng)];
+      std::printf("Input file contains %zu state(s); one was selected at random.\n", states.size());
+    }
+  }
   p.num_bodies = (int32_t)((ic.size() - 1) / 7);
   try {
     // main.cpp:73-109
@@ -114,6 +146,28 @@ int main(int argc, char** argv) {
     fcm.produce_reference_matrices(all_bodies);
     gmres_solver gmres;
     gmres.initialise(all_bodies);
+    if (opt.count("mcmc")) {  // main.cpp:113-210
+      const long long n_total = std::atoll(opt["mcmc"].c_str());
+      const long long save_after = opt.count("mcmc_save_after") ? std::atoll(opt["mcmc_save_after"].c_str()) : 100000;
+      fcm_mcmc_state st;
+      if (fcm_mcmc_state_init(all_bodies.ctx(), &st) != 0) throw std::runtime_error(fcm_last_error());
+      while (st.steps < n_total) {
+        const long long chunk = std::min<long long>(200 - st.steps % 200, n_total - st.steps);
+        const int rc = fcm_mcmc_run(all_bodies.ctx(), seed, chunk, &st);
+        if (rc != 0) throw std::runtime_error(fcm_last_error());
+        if (st.steps % 200 == 0) {
+          all_bodies.pull_bodies();
+          if (st.steps > save_after) {
+            all_bodies.write_data_to_file((double)st.steps, name + ".dat", digits);
+            std::printf("[scale/a = %g, U = %g] Saved sample %lld\n", st.scale / p.blob_radius, st.potential,
+                        st.steps);
+          } else {
+            std::printf("[scale/a = %g, U = %g]\n", st.scale / p.blob_radius, st.potential);
+          }
+        }
+      }
+      return 0;
+    }
     // main.cpp:212-451
     int skipped_steps = 0, accepted = 0, plotting_step = 0;
     unsigned long long counter = 0;
@@ -151,6 +205,7 @@ int main(int argc, char** argv) {
       if (++plotting_step == save_every) {
         plotting_step = 0;
         all_bodies.write_data_to_file(t, name + ".dat", digits);
+        all_bodies.write_blob_forces_to_file(t, name + "_blob_forces.dat", digits);
         std::ofstream vf(name + "_velocities.dat", std::ios::app);
         vf << std::scientific << std::setprecision(digits) << t << " ";
         for (size_t i = 0; i < U.n_elem(); ++i) vf << U(i) << " ";
