@@ -222,8 +222,9 @@ int fcm_produce_deterministic_velocity_field(fcm_ctx* ctx);
 int fcm_calculate_deterministic_blob_velocities(fcm_ctx* ctx, double* V);
 /* The context's last interpolated velocities (fcm.V) to V (3Nb). */
 int fcm_get_V(fcm_ctx* ctx, double* V);
-/* Velocity grids u{x,y,z} (deterministic: which=0, random: which=1) in the
- * reference's padded [x][y][pad] layout, 3 arrays of nx*ny*pad doubles. */
+/* Velocity grids u{x,y,z} (deterministic: which=0, random: which=1, imposed shear
+ * flow: which=2) in the reference's padded [x][y][pad] layout, 3 arrays of
+ * nx*ny*pad doubles. */
 int fcm_get_velocity_field(fcm_ctx* ctx, int32_t which, double* ux, double* uy, double* uz);
 /* M*F in one call: spread, Stokes solve, interpolation (V = 3Nb). */
 int fcm_apply_mobility(fcm_ctx* ctx, const double* F, double* V);
@@ -243,6 +244,26 @@ int fcm_apply_mobility(fcm_ctx* ctx, const double* F, double* V);
  * dx <= a/2 or finer for accurate rotation rates. */
 int fcm_set_up_dipole_distribution(fcm_ctx* ctx, const double* F, const double* T, const double* S);
 int fcm_calculate_deterministic_blob_rotations(fcm_ctx* ctx, double* Omega, double* E);
+
+/* Shear forcing (SHEARING_FORCES, config.hpp:32, :52-56).
+ * fcm_produce_shear_velocity_field replaces fcm_fluid_solver.cpp:703-842: the
+ * Stokes flow u_shear driven by the body force
+ * fx = scale * kT * sin(wavenumber * 2 pi j / ny) / a (fy = fz = 0) on every grid
+ * point -- scale and wavenumber are SHEAR_FORCE_SCALE and SHEAR_WAVENUMBER -- solved
+ * once, as main.cpp:98-100 does at start-up.  From then on every RHS subtracts
+ * Vshear (gmres_solver.cpp:62-64), and a GDC step interpolates u_shear at the
+ * midstep (main.cpp:270-272) before its solve; an EM step, like the reference's,
+ * never does, so it uses the Vshear last computed (zero until
+ * fcm_calculate_shear_blob_velocities is called).  The deterministic grids are
+ * left holding the shear solve.
+ * fcm_calculate_shear_blob_velocities replaces fcm_fluid_solver.cpp:489-550:
+ * Vshear (3Nb, may be NULL) = J u_shear on the current Gaussians; fcm.V is kept.
+ * fcm_fluid_x_velocity_in_y replaces main.cpp:371-433: spread F (3Nb) on the
+ * current Gaussians, solve, and write profile[j] (ny doubles) = the mean over x
+ * and z of ux + ux_shear at y index j (ux alone without a shear flow). */
+int fcm_produce_shear_velocity_field(fcm_ctx* ctx, double scale, double wavenumber);
+int fcm_calculate_shear_blob_velocities(fcm_ctx* ctx, double* Vshear);
+int fcm_fluid_x_velocity_in_y(fcm_ctx* ctx, const double* F, double* profile);
 
 /* The three stages of M*F one at a time on the working grid of one precision
  * (0 = FP64, 1 = FP32, which needs a context of precision 1): spread F (3Nb),

@@ -621,6 +621,10 @@ struct orc {
   // fcm_fluid_solver fields (fcm_fluid_solver.hpp:20-56)
   std::vector<double> ux, uy, uz, fx, fy, fz, sxx, syy, szz, sxy, sxz, syz;
   std::vector<double> V, Vtemp, ux_rand, uy_rand, uz_rand;
+  // SHEARING_FORCES fields (fcm_fluid_solver.cpp:53-61): the imposed flow and its
+  // blob velocities; shear is set once the flow has been produced
+  std::vector<double> ux_shear, uy_shear, uz_shear, Vshear;
+  bool shear = false;
   std::vector<double> qx, qxsq, qy, qysq, qpad, qpadsq;
   std::vector<double> gaussx, gaussy, gaussz;  // [np*W + i]
   std::vector<int> indx, indy, indz;
@@ -1234,6 +1238,7 @@ orc* orc_create(const fcm_params* p, const double* ref) {
   for (auto* v : {&o->ux, &o->uy, &o->uz, &o->fx, &o->fy, &o->fz, &o->sxx, &o->syy, &o->szz, &o->sxy, &o->sxz, &o->syz, &o->ux_rand, &o->uy_rand, &o->uz_rand})
     v->assign(o->P, 0.0);
   o->V.assign(3 * (size_t)o->Nb, 0.0);
+  o->Vshear.assign(3 * (size_t)o->Nb, 0.0);
   // fcm_fluid_solver.cpp:71-127 wavenumber tables
   auto qtab = [](int N, double L, std::vector<double>& q, std::vector<double>& qsq) {
     q.resize(N); qsq.resize(N);
@@ -1568,6 +1573,8 @@ void orc_set_reference_matrices(orc* o, const double* Minv, const double* N) {
 void orc_assemble_RHS(orc* o) {
   const int Nb = o->Nb;
   for (int i = 0; i < 3 * Nb; ++i) o->RHS[i] = -o->V[i];
+  if (o->shear)  // gmres_solver.cpp:62-64
+    for (int i = 0; i < 3 * Nb; ++i) o->RHS[i] -= o->Vshear[i];
   std::vector<double> kt(6 * o->M);
   mult_KT(o, o->blob_forces.data(), kt.data());
   for (int i = 0; i < 6 * o->M; ++i) o->RHS[3 * Nb + i] = -kt[i] - o->ext_forces[i];
@@ -1614,6 +1621,7 @@ static int step_impl(orc* o, bool injected, const double* s6, uint64_t seed, uin
     orc_fill_all_blob_pos(o, 1);
     set_up_gaussians(o, o->all_blob_pos.data(), o->Nb);
     interp(o, o->ux_rand.data(), o->uy_rand.data(), o->uz_rand.data());
+    if (o->shear) orc_calculate_shear_blob_velocities(o, nullptr);  // main.cpp:270-272
   }
   calculate_forces(o);
   orc_assemble_RHS(o);
@@ -1892,6 +1900,69 @@ int orc_mcmc_run(orc* o, uint64_t seed, int64_t n_steps, fcm_mcmc_state* st) {
   st->steps = n;
   st->attempts = attempt;
   return n < target ? FCM_ERR_OVERLAP : FCM_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ shear forcing
+// fcm_fluid_solver.cpp:703-842 (SHEARING_FORCES, SLIP_CHANNEL false): the Stokes
+// flow driven by the body force fx(j) = scale*kT*sin(wavenumber*2*pi*j/Ny)/a,
+// fy = fz = 0, on every grid point.  Its k-space steps (:771-833) are those of
+// produce_deterministic_velocity_field (:636-701); the result is kept as
+// u*_shear and the force and velocity grids are left holding this solve, as in
+// the reference.
+extern "C" {
+
+void orc_produce_shear_velocity_field(orc* o, double scale, double wavenumber) {
+  const int Nx = o->Nx, Ny = o->Ny, Nz = o->Nz, pad = o->pad;
+  std::fill(o->fx.begin(), o->fx.end(), 0.0);
+  std::fill(o->fy.begin(), o->fy.end(), 0.0);
+  std::fill(o->fz.begin(), o->fz.end(), 0.0);
+  for (int i = 0; i < Nx; i++) {
+    const size_t x_index = (size_t)i * Ny * pad;
+    for (int j = 0; j < Ny; j++) {
+      const size_t y_index = (size_t)j * pad;
+      const double f = scale * o->kT * std::sin(wavenumber * 2.0 * PI * double(j) / double(Ny)) / o->a;
+      for (int k = 0; k < Nz; k++) o->fx[x_index + y_index + k] = f;
+    }
+  }
+  produce_deterministic_velocity_field(o);
+  o->ux_shear = o->ux;
+  o->uy_shear = o->uy;
+  o->uz_shear = o->uz;
+  o->shear = true;
+}
+
+// fcm_fluid_solver.cpp:489-550: Vshear = J u_shear on the current Gaussians
+// (V itself is left as it was).
+void orc_calculate_shear_blob_velocities(orc* o, double* Vshear) {
+  if (!o->shear) return;
+  const std::vector<double> keep = o->V;
+  interp(o, o->ux_shear.data(), o->uy_shear.data(), o->uz_shear.data());
+  o->Vshear = o->V;
+  o->V = keep;
+  if (Vshear) std::copy(o->Vshear.begin(), o->Vshear.end(), Vshear);
+}
+
+// main.cpp:371-433: the deterministic flow of blob forces F (3Nb) on the current
+// Gaussians plus the imposed flow, x-velocity averaged over x and z for every y
+// (profile: Ny values).  The force and velocity grids keep that solve.
+void orc_fluid_x_velocity_in_y(orc* o, const double* F, double* profile) {
+  orc_set_up_force_distribution(o, F);
+  produce_deterministic_velocity_field(o);
+  const int Nx = o->Nx, Ny = o->Ny, Nz = o->Nz, pad = o->pad;
+  for (int j = 0; j < Ny; j++) {
+    const size_t y_index = (size_t)j * pad;
+    double u_local = 0.0;
+    for (int i = 0; i < Nx; i++) {
+      const size_t x_index = (size_t)i * Ny * pad;
+      for (int k = 0; k < Nz; k++) {
+        const size_t index = x_index + y_index + k;
+        u_local += o->ux[index] + (o->shear ? o->ux_shear[index] : 0.0);
+      }
+    }
+    profile[j] = u_local / (Nx * Nz);
+  }
 }
 
 }  // extern "C"

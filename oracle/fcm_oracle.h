@@ -81,6 +81,12 @@ void orc_calculate_deterministic_blob_velocities(orc* o, double* V);
  * then Omega (3Nb) and E (9Nb) of the deterministic field. */
 void orc_set_up_dipole_distribution(orc* o, const double* F, const double* T, const double* S);
 void orc_calculate_deterministic_blob_rotations(orc* o, double* Om, double* E);
+/* Shear forcing (fcm_fluid_solver.cpp:703-842, :489-550; main.cpp:371-433):
+ * produce the imposed flow once; afterwards GDC steps interpolate it at the
+ * midstep and every RHS subtracts Vshear. */
+void orc_produce_shear_velocity_field(orc* o, double scale, double wavenumber);
+void orc_calculate_shear_blob_velocities(orc* o, double* Vshear);
+void orc_fluid_x_velocity_in_y(orc* o, const double* F, double* profile);
 /* Pair potential of the current bodies, and Metropolis runs (main.cpp:113-210)
  * with the same Philox uniforms as the GPU library. */
 double orc_calculate_potential(orc* o);

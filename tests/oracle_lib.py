@@ -70,6 +70,9 @@ def lib():
             "orc_calculate_deterministic_blob_velocities": (None, [vp, D]),
             "orc_set_up_dipole_distribution": (None, [vp, D, D, D]),
             "orc_calculate_potential": (ctypes.c_double, [vp]),
+            "orc_produce_shear_velocity_field": (None, [vp, ctypes.c_double, ctypes.c_double]),
+            "orc_calculate_shear_blob_velocities": (None, [vp, D]),
+            "orc_fluid_x_velocity_in_y": (None, [vp, D, D]),
             "orc_mcmc_run": (ctypes.c_int, [vp, ctypes.c_uint64, ctypes.c_int64, ctypes.POINTER(FcmMcmcState)]),
             "orc_calculate_deterministic_blob_rotations": (None, [vp, D, D]),
             "orc_get_V": (None, [vp, D]),
@@ -266,6 +269,25 @@ class Oracle:
 
     def calculate_potential(self):
         return lib().orc_calculate_potential(self.h)
+
+    def get_V(self):
+        V = np.zeros(3 * self.Nb)
+        lib().orc_get_V(self.h, _dp(V))
+        return V
+
+    def produce_shear_velocity_field(self, scale=1.0, wavenumber=1.0):
+        """fcm_fluid_solver.cpp:703-842 with SHEAR_FORCE_SCALE and SHEAR_WAVENUMBER."""
+        lib().orc_produce_shear_velocity_field(self.h, float(scale), float(wavenumber))
+
+    def calculate_shear_blob_velocities(self):
+        Vs = np.zeros(3 * self.Nb)
+        lib().orc_calculate_shear_blob_velocities(self.h, _dp(Vs))
+        return Vs
+
+    def fluid_x_velocity_in_y(self, F):
+        prof = np.zeros(self.p.ny)
+        lib().orc_fluid_x_velocity_in_y(self.h, _dp(_f64(F, 3 * self.Nb)), _dp(prof))
+        return prof
 
     def mcmc_run(self, seed, n_steps, state=None):
         """Metropolis steps (main.cpp:113-210); state defaults to the reference's start."""

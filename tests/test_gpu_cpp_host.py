@@ -76,3 +76,45 @@ def test_driver_mcmc_matches_oracle(gpu, tmp_path):
     assert np.abs(last[1:].reshape(-1, 7)[:, :3].ravel() - xo).max() < 1e-12
     assert np.abs(last[1:].reshape(-1, 7)[:, 3:].ravel() - qo).max() < 1e-12
     assert "Saved sample 400" in r.stdout
+
+
+def test_driver_shear_matches_oracle(gpu, tmp_path):
+    """The driver with SHEARING_FORCES (shear=1): GDC steps on the oracle's
+    trajectory with the imposed flow on, and one x-velocity profile per save
+    (main.cpp:371-433), whose mean over y is zero (the k = 0 mode is removed)
+    and which follows the imposed sin profile."""
+    p, ref, x, q, fe = configs.rod_suspension(M=8, grid=32, L=24.0, nb=6, seed=5, gmres_tol=1e-12, noise=0,
+                                              ngauss=12, algorithm=1)
+    shape = tmp_path / "shape.txt"
+    shape.write_text("\n".join("%.17g %.17g %.17g" % tuple(ref[3 * m:3 * m + 3]) for m in range(p.blobs_per_body)))
+    ic = tmp_path / "ic.dat"
+    ic.write_text("0 " + " ".join("%.17g %.17g %.17g %.17g %.17g %.17g %.17g" % (tuple(x[3 * n:3 * n + 3]) +
+                                                                                tuple(q[4 * n:4 * n + 4]))
+                                  for n in range(p.num_bodies)) + "\n")
+    args = [build.DRIVER, "shape=%s" % shape, "ic=%s" % ic, "steps=3", "name=%s" % (tmp_path / "sh"),
+            "digits=17", "body_force_z=-1", "shear=1", "shear_scale=2.0", "shear_wavenumber=1.0"]
+    for k in ("nx", "ny", "nz", "ngauss", "dx", "dt", "ncells", "potential", "steric_fs", "steric_rc",
+              "gmres_max_iter", "gmres_tol", "algorithm", "noise"):
+        args.append("%s=%r" % (k, getattr(p, k)))
+    r = subprocess.run(args, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    last = np.array([float(v) for v in (tmp_path / "sh.dat").read_text().strip().splitlines()[-1].split()])
+    o = Oracle(p, ref)
+    o.set_bodies(x, q)
+    o.set_external_forces(fe)
+    o.produce_reference_matrices()
+    o.produce_shear_velocity_field(2.0, 1.0)
+    for i in range(3):
+        assert o.step(0, i)[0] == 0
+    xo, qo = o.get_bodies()
+    assert np.abs(last[1:].reshape(-1, 7)[:, :3].ravel() - xo).max() < 1e-8
+    assert np.abs(last[1:].reshape(-1, 7)[:, 3:].ravel() - qo).max() < 1e-8
+    prof = (tmp_path / "sh_fluid_x_velocity_in_y.dat").read_text().strip().splitlines()
+    assert len(prof) == 3
+    u = np.array([float(v) for v in prof[-1].split()[1:]])
+    assert u.size == p.ny
+    L = p.ny * p.dx
+    k = 2 * np.pi / L
+    amp = 2.0 * p.kT / (p.blob_radius * p.viscosity * k * k)
+    assert abs(u.mean()) < 1e-5 * amp  # the saved values carry 6 digits
+    assert np.corrcoef(u, np.sin(k * np.arange(p.ny) * p.dx))[0, 1] > 0.99

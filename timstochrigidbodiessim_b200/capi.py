@@ -64,6 +64,9 @@ SIGNATURES = {
     "fcm_apply_mobility": (ctypes.c_int, [VP, VP, VP]),
     "fcm_set_up_dipole_distribution": (ctypes.c_int, [VP, VP, VP, VP]),
     "fcm_calculate_deterministic_blob_rotations": (ctypes.c_int, [VP, VP, VP]),
+    "fcm_produce_shear_velocity_field": (ctypes.c_int, [VP, ctypes.c_double, ctypes.c_double]),
+    "fcm_calculate_shear_blob_velocities": (ctypes.c_int, [VP, VP]),
+    "fcm_fluid_x_velocity_in_y": (ctypes.c_int, [VP, VP, VP]),
     "fcm_spread": (ctypes.c_int, [VP, ctypes.c_int32, VP]),
     "fcm_stokes_solve": (ctypes.c_int, [VP, ctypes.c_int32]),
     "fcm_interp": (ctypes.c_int, [VP, ctypes.c_int32, VP]),

@@ -258,6 +258,32 @@ int fp32_stencil(const Ctx* c) {
   return std::min(c->p.ngauss, 2 * half + 2);
 }
 
+// The fused x-transform path of the Stokes solve (stokes_t) when nx has a kernel
+// and nz is even: the twiddles exp(-2 pi i j / nx) of both precisions.
+int setup_xfft(Ctx* c) {
+  int n1 = 0, n2 = 0;
+  c->xfft = xfft_factor(c->g.nx, &n1, &n2) && c->g.nz % 2 == 0;
+  if (!c->xfft) return FCM_OK;
+  FCM_TRY(xfft_tables_init());
+  const int n = c->g.nx;
+  const double PI = 3.14159265358979323846264338327950288;
+  std::vector<double2> wd(n);
+  std::vector<float2> wf(n);
+  for (int j = 0; j < n; ++j) {
+    wd[j] = make_double2(std::cos(2.0 * PI * j / n), -std::sin(2.0 * PI * j / n));
+    wf[j] = make_float2((float)wd[j].x, (float)wd[j].y);
+  }
+  double2* d64 = nullptr;
+  float2* d32 = nullptr;
+  FCM_TRY(dev_alloc(&d64, (size_t)n));
+  c->d_xtw64 = d64;
+  FCM_TRY(dev_alloc(&d32, (size_t)n));
+  c->d_xtw32 = d32;
+  FCM_CUDA(cudaMemcpy(d64, wd.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
+  FCM_CUDA(cudaMemcpy(d32, wf.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+  return FCM_OK;
+}
+
 template <typename T>
 int ensure_grid(Ctx* c) {
   GridBufs<T>& gb = grid_of<T>(c);
@@ -271,6 +297,17 @@ int ensure_grid(Ctx* c) {
   FCM_CUFFT(cufftPlanMany(&gb.c2r, 3, n, nullptr, 1, (int)c->g.Gc, nullptr, 1, (int)c->g.G, c2r_type<T>(), 3));
   FCM_CUFFT(cufftSetStream(gb.r2c, c->stream));
   FCM_CUFFT(cufftSetStream(gb.c2r, c->stream));
+  if (c->xfft) {  // (y, z) transforms of the 3 nx planes of each component
+    int n2[2] = {c->g.ny, c->g.nz};
+    const int planes = 3 * c->g.nx;
+    FCM_CUFFT(cufftPlanMany(&gb.r2c2d, 2, n2, nullptr, 1, c->g.ny * c->g.nz, nullptr, 1, c->g.ny * c->g.nzh,
+                            r2c_type<T>(), planes));
+    FCM_CUFFT(cufftPlanMany(&gb.c2r2d, 2, n2, nullptr, 1, c->g.ny * c->g.nzh, nullptr, 1, c->g.ny * c->g.nz,
+                            c2r_type<T>(), planes));
+    FCM_CUFFT(cufftSetStream(gb.r2c2d, c->stream));
+    FCM_CUFFT(cufftSetStream(gb.c2r2d, c->stream));
+    FCM_TRY(xfft_prepare<T>(*c));
+  }
   const int W = sizeof(T) == 4 ? fp32_stencil(c) : c->p.ngauss;
   FCM_TRY(blob_table_alloc(gb.blobs, c->Nb, W, c->g));
   FCM_TRY(blob_table_alloc(gb.ref_blobs, c->nb, W, c->g));
@@ -287,6 +324,8 @@ void free_grid(GridBufs<T>& gb) {
   }
   if (gb.r2c) cufftDestroy(gb.r2c);
   if (gb.c2r) cufftDestroy(gb.c2r);
+  if (gb.r2c2d) cufftDestroy(gb.r2c2d);
+  if (gb.c2r2d) cufftDestroy(gb.c2r2d);
   blob_table_free(gb.blobs);
   blob_table_free(gb.ref_blobs);
   gb = GridBufs<T>();
@@ -296,10 +335,14 @@ int set_stream_all(Ctx* c) {
   if (c->g64.ready) {
     FCM_CUFFT(cufftSetStream(c->g64.r2c, c->stream));
     FCM_CUFFT(cufftSetStream(c->g64.c2r, c->stream));
+    if (c->g64.r2c2d) FCM_CUFFT(cufftSetStream(c->g64.r2c2d, c->stream));
+    if (c->g64.c2r2d) FCM_CUFFT(cufftSetStream(c->g64.c2r2d, c->stream));
   }
   if (c->g32.ready) {
     FCM_CUFFT(cufftSetStream(c->g32.r2c, c->stream));
     FCM_CUFFT(cufftSetStream(c->g32.c2r, c->stream));
+    if (c->g32.r2c2d) FCM_CUFFT(cufftSetStream(c->g32.r2c2d, c->stream));
+    if (c->g32.c2r2d) FCM_CUFFT(cufftSetStream(c->g32.c2r2d, c->stream));
   }
   if (c->plan_r2c6) FCM_CUFFT(cufftSetStream(c->plan_r2c6, c->stream));
   return FCM_OK;
@@ -322,6 +365,12 @@ int spread_t(Ctx* c, const BlobTable<T>& t, const double* dF) {
 template <typename T>
 int stokes_t(Ctx* c) {
   GridBufs<T>& gb = grid_of<T>(c);
+  if (c->xfft) {  // (y, z) transforms, then x-transform + projection + inverse in one kernel
+    FCM_CUFFT(exec_r2c(gb.r2c2d, gb.r, gb.c));
+    FCM_TRY(launch_xfft_project<T>(*c, gb.c, c->stream));
+    FCM_CUFFT(exec_c2r(gb.c2r2d, gb.c, gb.r));
+    return FCM_OK;
+  }
   FCM_CUFFT(exec_r2c(gb.r2c, gb.r, gb.c));
   FCM_TRY(launch_project<T>(*c, gb.c, c->stream));
   FCM_CUFFT(exec_c2r(gb.c2r, gb.c, gb.r));
@@ -525,8 +574,14 @@ int assemble_rhs_dev(Ctx* c) {
   const size_t n3 = 3 * (size_t)c->Nb;
   FCM_CUDA(cudaMemcpyAsync(c->d_rhs, c->d_V, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->stream));
   FCM_TRY(blas_axpby(c->d_rhs, c->d_rhs, 0.0, -1.0, (long long)n3, c->stream));
+  if (c->shear) FCM_TRY(blas_axpby(c->d_rhs, c->d_vshear, -1.0, 1.0, (long long)n3, c->stream));  // :62-64
   FCM_TRY(launch_multiply_KT(*c, c->d_qm, c->d_F, c->d_rhs + n3, -1.0, c->d_fe, -1.0, c->stream));
   return FCM_OK;
+}
+
+// fcm_fluid_solver.cpp:489-550: Vshear = J u_shear on the current Gaussians.
+int shear_velocities_dev(Ctx* c) {
+  return launch_interp<double>(*c, c->g64.blobs, c->d_ushear, c->d_vshear, c->stream);
 }
 
 int overlap_dev(Ctx* c, int* ov) {
@@ -813,6 +868,7 @@ int enqueue_resident_step(Ctx* c, long long* k_top, long long* k_sweep, long lon
     FCM_TRY(launch_fill_blob_pos(*c, c->d_xm, c->d_qm, c->d_Y, c->stream));
     FCM_TRY(set_up_gaussians_dev(c, c->d_Y));
     FCM_TRY(random_velocities_dev(c, c->d_V));
+    if (c->shear) FCM_TRY(shear_velocities_dev(c));  // main.cpp:270-272
   }
   FCM_TRY(calculate_forces_dev(c));
   FCM_TRY(assemble_rhs_dev(c));
@@ -1059,6 +1115,10 @@ void destroy_ctx(Ctx* c) {
   if (c->h_gm) cudaFreeHost(c->h_gm);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   cudaFree(c->d_dip);
+  cudaFree(c->d_xtw64);
+  cudaFree(c->d_xtw32);
+  cudaFree(c->d_ushear);
+  cudaFree(c->d_vshear);
   cudaFree(c->d_mcmc);
   cudaFree(c->d_usum);
   if (c->mcmc_graph) cudaGraphExecDestroy(c->mcmc_graph);
@@ -1210,6 +1270,7 @@ int create_ctx(const fcm_params* p, const double* ref, Ctx** out) {
       cudaMemcpy(c->d_N, c->h_N.data(), sizeof(double) * 36, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(c->d_KTKinv, c->h_KTKinv.data(), sizeof(double) * 36, cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(FCM_ERR_CUDA);
+  if ((st = setup_xfft(c)) != FCM_OK) return fail(st);
   if ((st = ensure_grid<double>(c)) != FCM_OK) return fail(st);
   if (p->precision == 1 && (st = ensure_grid<float>(c)) != FCM_OK) return fail(st);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(FCM_ERR_CUDA);
@@ -1267,6 +1328,7 @@ int step_host(Ctx* c, uint64_t seed, uint64_t step_index, fcm_step_info* info) {
       FCM_TRY(launch_fill_blob_pos(*c, c->d_xm, c->d_qm, c->d_Y, c->stream));
       FCM_TRY(set_up_gaussians_dev(c, c->d_Y));
       FCM_TRY(random_velocities_dev(c, c->d_V));
+      if (c->shear) FCM_TRY(shear_velocities_dev(c));  // main.cpp:270-272
     }
     FCM_TRY(calculate_forces_dev(c));  // main.cpp:282
     FCM_TRY(assemble_rhs_dev(c));      // main.cpp:308
@@ -1303,6 +1365,12 @@ int step_issue(Ctx* c, uint64_t seed, uint64_t step_index) {
   if (c->step_pending) {
     set_error("a step is already in flight on this context: call fcm_step_wait first");
     return FCM_ERR_STATE;
+  }
+  if (c->graph_stale && !c->in_batch) {  // recapture after a change of the step's work
+    if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+    c->step_graph = nullptr;
+    if (c->step_graph_state == 1) c->step_graph_state = 0;
+    c->graph_stale = false;
   }
   if (c->step_graph_state == 1) {
     c->h_stepargs[0] = seed;
@@ -1534,6 +1602,9 @@ struct BatchGroup {
   void* c[2] = {nullptr, nullptr};        // 3Gc per member
   void* urand[2] = {nullptr, nullptr};
   cufftHandle r2c[2] = {0, 0}, c2r[2] = {0, 0};
+  // fused x-transform path: (y, z) transforms of every member's planes, member ids
+  cufftHandle r2c2d[2] = {0, 0}, c2r2d[2] = {0, 0};
+  int* d_gidx = nullptr;
 };
 
 struct Batch {
@@ -1683,14 +1754,21 @@ template <typename T>
 int batch_saddle(Batch* B, int in, int out, int mask, cudaStream_t s) {
   constexpr int P = sizeof(T) == 8 ? 0 : 1;
   FCM_TRY(b_spread<T>(B->geom, in, mask, s));
+  bool any3d = false;  // groups without the fused x-transform
   for (BatchGroup& g : B->groups) {
-    FCM_CUFFT(cufftSetStream(g.r2c[P], s));
-    FCM_CUFFT(exec_r2c(g.r2c[P], (T*)g.r[P], (typename cplx_t<T>::type*)g.c[P]));
+    const bool fused = g.r2c2d[P] != 0;
+    any3d = any3d || !fused;
+    const cufftHandle h = fused ? g.r2c2d[P] : g.r2c[P];
+    FCM_CUFFT(cufftSetStream(h, s));
+    FCM_CUFFT(exec_r2c(h, (T*)g.r[P], (typename cplx_t<T>::type*)g.c[P]));
+    if (fused)
+      FCM_TRY(b_xfft_project<T>(B->geom, *B->m[g.idx[0]], g.d_gidx, (int)g.idx.size(), mask, s));
   }
-  FCM_TRY(b_project<T>(B->geom, mask, s));
+  if (any3d) FCM_TRY(b_project<T>(B->geom, mask, s));  // members of the other groups
   for (BatchGroup& g : B->groups) {
-    FCM_CUFFT(cufftSetStream(g.c2r[P], s));
-    FCM_CUFFT(exec_c2r(g.c2r[P], (typename cplx_t<T>::type*)g.c[P], (T*)g.r[P]));
+    const cufftHandle h = g.c2r2d[P] ? g.c2r2d[P] : g.c2r[P];
+    FCM_CUFFT(cufftSetStream(h, s));
+    FCM_CUFFT(exec_c2r(h, (typename cplx_t<T>::type*)g.c[P], (T*)g.r[P]));
   }
   FCM_TRY(b_interp<T>(B->geom, out, mask, s));
   FCM_TRY(b_multiply_K_KT(B->geom, in, out, mask, s));
@@ -1774,6 +1852,7 @@ int member_pre_solve(Ctx* c) {
     FCM_TRY(launch_fill_blob_pos(*c, c->d_xm, c->d_qm, c->d_Y, c->stream));
     FCM_TRY(set_up_gaussians_dev(c, c->d_Y));
     FCM_TRY(random_velocities_dev(c, c->d_V));
+    if (c->shear) FCM_TRY(shear_velocities_dev(c));  // main.cpp:270-272
   }
   FCM_TRY(calculate_forces_dev(c));
   FCM_TRY(assemble_rhs_dev(c));
@@ -1907,6 +1986,16 @@ int rehome_grids(Batch* B, int P) {
     int nn[3] = {grp.nx, grp.ny, grp.nz};
     FCM_CUFFT(cufftPlanMany(&grp.r2c[P], 3, nn, nullptr, 1, (int)G, nullptr, 1, (int)Gc, r2c_type<T>(), (int)(3 * k)));
     FCM_CUFFT(cufftPlanMany(&grp.c2r[P], 3, nn, nullptr, 1, (int)Gc, nullptr, 1, (int)G, c2r_type<T>(), (int)(3 * k)));
+    if (c0->xfft) {
+      int n2[2] = {grp.ny, grp.nz};
+      const int pz = grp.ny * grp.nz, pc = grp.ny * (grp.nz / 2 + 1), planes = (int)(3 * grp.nx * k);
+      FCM_CUFFT(cufftPlanMany(&grp.r2c2d[P], 2, n2, nullptr, 1, pz, nullptr, 1, pc, r2c_type<T>(), planes));
+      FCM_CUFFT(cufftPlanMany(&grp.c2r2d[P], 2, n2, nullptr, 1, pc, nullptr, 1, pz, c2r_type<T>(), planes));
+      if (!grp.d_gidx) {
+        FCM_TRY(dev_alloc(&grp.d_gidx, k));
+        FCM_CUDA(cudaMemcpy(grp.d_gidx, grp.idx.data(), sizeof(int) * k, cudaMemcpyHostToDevice));
+      }
+    }
   }
   return FCM_OK;
 }
@@ -1927,7 +2016,10 @@ void destroy_batch(Batch* B) {
       cudaFree(g.urand[P]);
       if (g.r2c[P]) cufftDestroy(g.r2c[P]);
       if (g.c2r[P]) cufftDestroy(g.c2r[P]);
+      if (g.r2c2d[P]) cufftDestroy(g.r2c2d[P]);
+      if (g.c2r2d[P]) cufftDestroy(g.c2r2d[P]);
     }
+  for (BatchGroup& g : B->groups) cudaFree(g.d_gidx);
   cudaFree(B->d_mem);
   cudaFree(B->d_tile_map);
   cudaFree(B->d_kblock_map);
@@ -2015,7 +2107,7 @@ int create_batch(int n, const fcm_params* params, const double* const* refs, Bat
     G.red_blocks = std::max(G.red_blocks, c->red_blocks);
     G.md_blocks = std::max(G.md_blocks, c->md_blocks);
     G.total_tiles += c->g64.blobs.ntiles;
-    G.total_kblocks += (int)((c->g.Gc + 255) / 256);
+    if (!c->xfft) G.total_kblocks += (int)((c->g.Gc + 255) / 256);  // the fused path projects the others
   }
   G.max_sys_blocks = (int)((max_sys + 255) / 256);
   G.max_blob_blocks = (int)((max_Nb + 127) / 128);
@@ -2104,7 +2196,7 @@ int create_batch(int n, const fcm_params* params, const double* const* refs, Bat
     m.kp = make_kparams(*c);
     m.dx3 = c->g.dx * c->g.dx * c->g.dx;
     for (int t = 0; t < c->g64.blobs.ntiles; ++t) tmap.push_back(make_int2(i, t));
-    const int kb = (int)((c->g.Gc + 255) / 256);
+    const int kb = c->xfft ? 0 : (int)((c->g.Gc + 255) / 256);
     for (int t = 0; t < kb; ++t) kmap.push_back(make_int2(i, t));
   }
   if (cudaMemcpy(B->d_mem, hm.data(), sizeof(BMember) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -2137,6 +2229,16 @@ int create_batch(int n, const fcm_params* params, const double* const* refs, Bat
 // (allocating what they need) and then captures the batch graph.
 int batch_step(Batch* B, const uint64_t* seeds, uint64_t step_index, fcm_step_info* infos) {
   const int n = B->geom.n;
+  bool stale = false;
+  for (Ctx* c : B->m) {
+    stale = stale || c->graph_stale;
+    c->graph_stale = false;
+  }
+  if (stale && B->state == 1) {  // recapture after a change of a member's step
+    cudaGraphExecDestroy(B->graph);
+    B->graph = nullptr;
+    B->state = 0;
+  }
   if (B->state != 1) {
     int first = FCM_OK;
     std::string err;
@@ -2574,7 +2676,13 @@ int fcm_get_velocity_field(fcm_ctx* ctx, int32_t which, double* ux, double* uy, 
     const size_t G = (size_t)c->g.G;
     for (int k = 0; k < 3; ++k) {
       if (!outs[k]) continue;
-      if (which == 1 && c->urand_prec == 1)
+      if (which == 2 && !c->shear) {
+        set_error("no shear flow: call fcm_produce_shear_velocity_field first");
+        return (int)FCM_ERR_STATE;
+      }
+      if (which == 2)
+        FCM_TRY(grid_to_padded<double>(c, outs[k], c->d_ushear + k * G));
+      else if (which == 1 && c->urand_prec == 1)
         FCM_TRY(grid_to_padded<float>(c, outs[k], c->g32.urand + k * G));
       else
         FCM_TRY(grid_to_padded<double>(c, outs[k], (which == 1 ? c->g64.urand : c->g64.r) + k * G));
@@ -2593,6 +2701,83 @@ int fcm_apply_mobility(fcm_ctx* ctx, const double* F, double* V) {
   FCM_TRY(copy_in(c, c->d_tmp3, F, sizeof(double) * 3 * c->Nb));
   FCM_TRY(mobility_dev(c, c->p.precision, c->d_tmp3, c->d_V));
   return copy_out(c, V, c->d_V, sizeof(double) * 3 * c->Nb);
+}
+
+// Shear forcing (SHEARING_FORCES of the reference).
+int fcm_produce_shear_velocity_field(fcm_ctx* ctx, double scale, double wavenumber) {
+  CTX_CHECK(ctx);
+  return guard([&] {
+    Ctx* c = ctx->c;
+    if (c->step_pending) {
+      set_error("a step is in flight on this context: call fcm_step_wait first");
+      return (int)FCM_ERR_STATE;
+    }
+    if (!std::isfinite(scale) || !std::isfinite(wavenumber)) {
+      set_error("shear scale and wavenumber must be finite");
+      return (int)FCM_ERR_INVALID;
+    }
+    // fx(j) of fcm_fluid_solver.cpp:727, evaluated on the host once per y index
+    const double PI = 3.14159265358979323846264338327950288;
+    const int ny = c->g.ny;
+    std::vector<double> row(ny);
+    for (int j = 0; j < ny; ++j)
+      row[j] = scale * c->p.kT * std::sin(wavenumber * 2.0 * PI * double(j) / double(ny)) / c->p.blob_radius;
+    if (!c->d_ushear) {
+      FCM_TRY(dev_alloc(&c->d_ushear, 3 * (size_t)c->g.G));
+      FCM_TRY(dev_alloc(&c->d_vshear, 3 * (size_t)(c->Nb > 0 ? c->Nb : 1)));
+      FCM_CUDA(cudaMemsetAsync(c->d_vshear, 0, sizeof(double) * 3 * (size_t)(c->Nb > 0 ? c->Nb : 1), c->stream));
+    }
+    // the spectrum array holds the row until the forward transform overwrites it
+    double* d_row = reinterpret_cast<double*>(c->g64.c);
+    FCM_CUDA(cudaMemcpyAsync(d_row, row.data(), sizeof(double) * ny, cudaMemcpyHostToDevice, c->stream));
+    FCM_TRY(launch_shear_forcing(*c, d_row, c->g64.r, c->stream));
+    FCM_TRY(stokes_t<double>(c));  // :771-841, the steps of :636-701
+    FCM_CUDA(cudaMemcpyAsync(c->d_ushear, c->g64.r, sizeof(double) * 3 * (size_t)c->g.G, cudaMemcpyDeviceToDevice,
+                             c->stream));
+    c->det_ready = true;
+    c->shear = true;
+    c->graph_stale = true;
+    FCM_CUDA(cudaStreamSynchronize(c->stream));
+    return (int)FCM_OK;
+  });
+}
+
+int fcm_calculate_shear_blob_velocities(fcm_ctx* ctx, double* Vshear) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  if (!c->shear) {
+    set_error("no shear flow: call fcm_produce_shear_velocity_field first");
+    return FCM_ERR_STATE;
+  }
+  if (!c->gauss_ready) {
+    set_error("set_up_gaussians must precede interpolation");
+    return FCM_ERR_STATE;
+  }
+  FCM_TRY(shear_velocities_dev(c));
+  return copy_out(c, Vshear, c->d_vshear, sizeof(double) * 3 * c->Nb);
+}
+
+int fcm_fluid_x_velocity_in_y(fcm_ctx* ctx, const double* F, double* profile) {
+  CTX_CHECK(ctx);
+  return guard([&] {
+    Ctx* c = ctx->c;
+    if (!profile) {
+      set_error("fcm_fluid_x_velocity_in_y: null output");
+      return (int)FCM_ERR_INVALID;
+    }
+    if (!c->gauss_ready) {
+      set_error("set_up_gaussians must precede spreading");
+      return (int)FCM_ERR_STATE;
+    }
+    FCM_TRY(copy_in(c, c->d_tmp3, F, sizeof(double) * 3 * c->Nb));
+    FCM_TRY(spread_t<double>(c, c->g64.blobs, c->d_tmp3));
+    FCM_TRY(stokes_t<double>(c));
+    c->det_ready = true;
+    // the profile (ny doubles) goes through the spectrum array, free after the solve
+    double* d_prof = reinterpret_cast<double*>(c->g64.c);
+    FCM_TRY(launch_x_profile(*c, c->g64.r, c->shear ? c->d_ushear : nullptr, d_prof, c->stream));
+    return copy_out(c, profile, d_prof, sizeof(double) * c->g.ny);
+  });
 }
 
 // Force dipoles on the FP64 deterministic grid (no reference counterpart).

@@ -121,6 +121,7 @@ struct GridBufs {
   typename cplx_t<T>::type* c = nullptr;       // 3*Gc spectrum
   T* urand = nullptr;                          // 3*G random velocity field
   cufftHandle r2c = 0, c2r = 0;
+  cufftHandle r2c2d = 0, c2r2d = 0;            // (y, z) transforms of every x-plane (fused x path)
   BlobTable<T> blobs;                          // all blobs of the suspension
   BlobTable<T> ref_blobs;                      // single body (reference matrices)
 };
@@ -248,6 +249,17 @@ struct Ctx {
   bool in_batch = false;            // owned by a batch (its step record and arguments too)
   // force dipoles (allocated on first use): T 3Nb, S 9Nb, D 9Nb, Omega 3Nb, E 9Nb
   double* d_dip = nullptr;
+  // shear forcing (fcm_fluid_solver.hpp SHEARING_FORCES fields), allocated when
+  // the imposed flow is produced: u_shear 3G (the grid layout of g64.r), Vshear 3Nb
+  // fused x-transform of the Stokes solve: on when nx is a supported length and nz
+  // is even; twiddles exp(-2 pi i j / nx), j < nx, as double2 and float2
+  bool xfft = false;
+  void* d_xtw64 = nullptr;
+  void* d_xtw32 = nullptr;
+  double* d_ushear = nullptr;
+  double* d_vshear = nullptr;
+  bool shear = false;
+  bool graph_stale = false;         // a captured step graph predates a change of the step's work
   // cells
   int ncell_total = 0;
   int *d_cell = nullptr, *d_cell_start = nullptr, *d_cell_count = nullptr, *d_cell_sorted = nullptr, *d_cell_cursor = nullptr;
@@ -408,11 +420,26 @@ int launch_blob_dipoles(const double* T3, const double* S9, int n, double* D9, c
 // k-space (fcm_kspace.cu)
 template <typename T>
 int launch_project(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s);
+// the x-transform, projection and inverse x-transform of a spectrum holding the
+// (y, z) transforms of every x-plane (fcm_kspace.cu)
+bool xfft_factor(int n, int* n1, int* n2);
+int xfft_tables_init();
+template <typename T>
+int xfft_prepare(const Ctx& c);
+template <typename T>
+int launch_xfft_project(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s);
+// the same for the members gidx[0..nm) of a batch group whose grids equal c0's
+template <typename T>
+int b_xfft_project(const BatchGeom& b, const Ctx& c0, const int* gidx, int nm, int mask, cudaStream_t s);
 // (seed, counter) are read from d_args[0..1] instead when d_args is given.
 template <typename T>
 int launch_noise_kspace(const Ctx& c, typename cplx_t<T>::type* spec, uint64_t seed, uint64_t counter,
                         const uint64_t* d_args, cudaStream_t s);
 int launch_stress_divergence_project(const Ctx& c, const cufftDoubleComplex* sigma6, cufftDoubleComplex* spec, cudaStream_t s);
+// shear forcing (fcm_kspace.cu): grid x-component = row[j] on every (i, k),
+// y and z components zero; and out[j] = mean over (i, k) of u[i][j][k] + add[i][j][k]
+int launch_shear_forcing(const Ctx& c, const double* d_row, double* grid, cudaStream_t s);
+int launch_x_profile(const Ctx& c, const double* u, const double* add, double* d_out, cudaStream_t s);
 int launch_unpad_copy(const double* src_padded, double* dst, int nx, int ny, int nz, int pad, int ncomp_stride_dst, cudaStream_t s);
 // bodies (fcm_bodies.cu)
 int launch_fill_blob_pos(const Ctx& c, const double* x, const double* q, double* Y, cudaStream_t s);

@@ -15,6 +15,10 @@
 // planes, u_sym(k) = (u(k) + conj(u(-k)))/2, with u(-k) computed from the
 // partner mode; cuFFT's C2R of a Hermitian-consistent spectrum then equals the
 // reference's transform.  One thread handles each {k, -k} pair.
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+
 #include "fcm_internal.cuh"
 
 namespace fcm {
@@ -283,6 +287,270 @@ __global__ void k_fluct(C* __restrict__ spec, const cufftDoubleComplex* __restri
   store3(spec, k.Gc, tp, usp);
 }
 
+// ------------------------------------------------------------------ fused x-transform
+// The Stokes solve of a force grid as 2D transforms over (y, z) for every x-plane
+// (cuFFT) with the transform along x, the projection and the inverse transform
+// along x fused into one kernel: each CTA holds the x-pencils of one y row and TK
+// consecutive kz (all three components) in shared memory, transforms them along x,
+// projects every mode and transforms back.  A 3D DFT is the x-DFT of the (y, z)
+// DFTs, so this is the transform pair of the 3D path with the projection between.
+// Pencils are transformed in two register-resident steps, N = N1 * N2 (both
+// divisors of 96 up to 32); in the chunks holding the kz = 0 and kz = nz/2 planes a
+// CTA takes the rows y and -y together and symmetrises each {k, -k} pair there.
+
+template <typename T, typename C>
+__device__ __forceinline__ V2<T> ldt(const C& v) {
+  return V2<T>{(T)v.x, (T)v.y};
+}
+
+__constant__ double2 c_w96d[96];  // exp(-2 pi i k / 96)
+__constant__ float2 c_w96f[96];
+
+template <typename T>
+__device__ __forceinline__ V2<T> w96(int k);
+template <>
+__device__ __forceinline__ V2<double> w96<double>(int k) {
+  const double2 w = c_w96d[k];
+  return V2<double>{w.x, w.y};
+}
+template <>
+__device__ __forceinline__ V2<float> w96<float>(int k) {
+  const float2 w = c_w96f[k];
+  return V2<float>{w.x, w.y};
+}
+
+template <typename T>
+__device__ __forceinline__ V2<T> cadd(V2<T> a, V2<T> b) { return V2<T>{a.x + b.x, a.y + b.y}; }
+template <typename T>
+__device__ __forceinline__ V2<T> csub(V2<T> a, V2<T> b) { return V2<T>{a.x - b.x, a.y - b.y}; }
+template <typename T>
+__device__ __forceinline__ V2<T> cmul(V2<T> a, V2<T> b) { return V2<T>{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
+template <typename T>
+__device__ __forceinline__ V2<T> cmulc(V2<T> a, V2<T> b) { return V2<T>{a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y}; }
+// -i z (forward) or +i z (inverse)
+template <typename T, bool INV>
+__device__ __forceinline__ V2<T> rot(V2<T> z) { return INV ? V2<T>{-z.y, z.x} : V2<T>{z.y, -z.x}; }
+
+// In-register DFT of R points, R a divisor of 96: forward exp(-2 pi i n k / R),
+// inverse exp(+2 pi i n k / R), unnormalised.  Decimation in time, R = P * Q.
+template <typename T, int R, bool INV>
+__device__ __forceinline__ void dft(V2<T> (&a)[R]) {
+  if constexpr (R == 1) {
+    return;
+  } else if constexpr (R == 2) {
+    const V2<T> t = a[1];
+    a[1] = csub(a[0], t);
+    a[0] = cadd(a[0], t);
+  } else if constexpr (R == 3) {
+    // W_3 = -1/2 -+ i sqrt(3)/2
+    const T h = (T)0.86602540378443864676;
+    const V2<T> t1 = cadd(a[1], a[2]);
+    const V2<T> t2 = V2<T>{a[0].x - (T)0.5 * t1.x, a[0].y - (T)0.5 * t1.y};
+    const V2<T> d = rot<T, INV>(csub(a[1], a[2]));
+    a[0] = cadd(a[0], t1);
+    a[1] = V2<T>{t2.x + h * d.x, t2.y + h * d.y};
+    a[2] = V2<T>{t2.x - h * d.x, t2.y - h * d.y};
+  } else if constexpr (R == 4) {
+    const V2<T> s0 = cadd(a[0], a[2]), s1 = csub(a[0], a[2]);
+    const V2<T> s2 = cadd(a[1], a[3]), s3 = rot<T, INV>(csub(a[1], a[3]));
+    a[0] = cadd(s0, s2);
+    a[2] = csub(s0, s2);
+    a[1] = cadd(s1, s3);
+    a[3] = csub(s1, s3);
+  } else {
+    constexpr int P = (R % 4 == 0) ? 4 : ((R % 2 == 0) ? 2 : 3);
+    constexpr int Q = R / P;
+    static_assert(96 % R == 0, "register DFT sizes divide 96");
+    V2<T> b[P][Q];
+#pragma unroll
+    for (int p = 0; p < P; ++p)
+#pragma unroll
+      for (int m = 0; m < Q; ++m) b[p][m] = a[P * m + p];
+#pragma unroll
+    for (int p = 0; p < P; ++p) dft<T, Q, INV>(b[p]);
+#pragma unroll
+    for (int p = 1; p < P; ++p)
+#pragma unroll
+      for (int m = 1; m < Q; ++m) {
+        const V2<T> w = w96<T>(((p * m) % R) * (96 / R));
+        b[p][m] = INV ? cmulc(b[p][m], w) : cmul(b[p][m], w);
+      }
+#pragma unroll
+    for (int m = 0; m < Q; ++m) {
+      V2<T> c[P];
+#pragma unroll
+      for (int p = 0; p < P; ++p) c[p] = b[p][m];
+      dft<T, P, INV>(c);
+#pragma unroll
+      for (int j = 0; j < P; ++j) a[m + Q * j] = c[j];
+    }
+  }
+}
+
+// Step over n1 (or k1) of every column: positions j*N2 + n2, j < N1.  Forward: DFT,
+// then the twiddle W_N^(n2 k1); inverse: DFT only (its twiddle came in step b).
+template <typename T, int N1, int N2, bool INV>
+__device__ __forceinline__ void xpass_a(V2<T>* __restrict__ s, const V2<T>* __restrict__ tw, int ncol, int NC) {
+  for (int i = threadIdx.x; i < N2 * ncol; i += blockDim.x) {
+    const int col = i % ncol, n2 = i / ncol;
+    V2<T> a[N1];
+#pragma unroll
+    for (int j = 0; j < N1; ++j) a[j] = s[(j * N2 + n2) * NC + col];
+    dft<T, N1, INV>(a);
+    if (!INV) {
+#pragma unroll
+      for (int j = 1; j < N1; ++j) a[j] = cmul(a[j], tw[n2 * j]);
+    }
+#pragma unroll
+    for (int j = 0; j < N1; ++j) s[(j * N2 + n2) * NC + col] = a[j];
+  }
+}
+
+// Step over n2 (or k2) of every column: positions k1*N2 + j, j < N2.  Inverse: DFT,
+// then the twiddle W_N^(-n2 k1).
+template <typename T, int N1, int N2, bool INV>
+__device__ __forceinline__ void xpass_b(V2<T>* __restrict__ s, const V2<T>* __restrict__ tw, int ncol, int NC) {
+  for (int i = threadIdx.x; i < N1 * ncol; i += blockDim.x) {
+    const int col = i % ncol, k1 = i / ncol;
+    V2<T> b[N2];
+#pragma unroll
+    for (int j = 0; j < N2; ++j) b[j] = s[(k1 * N2 + j) * NC + col];
+    dft<T, N2, INV>(b);
+    if (INV) {
+#pragma unroll
+      for (int j = 1; j < N2; ++j) b[j] = cmulc(b[j], tw[j * k1]);
+    }
+#pragma unroll
+    for (int j = 0; j < N2; ++j) s[(k1 * N2 + j) * NC + col] = b[j];
+  }
+}
+
+// One CTA: kz in [blockIdx.x*TK, +TK) of row y = blockIdx.y.  A chunk that holds a
+// Hermitian plane (kz = 0 or nz/2) pairs mode k with -k of row -y, so the CTA of the
+// smaller of {y, -y} takes both rows and the other returns: every {k, -k} pair is
+// read and written by one thread, as in k_project (the spectrum is updated in place).
+// Shared memory: pencils [N][6 TK] (column (row*3 + c)*TK + kz_local), twiddles W_N^j.
+template <typename T, typename C, int N1, int N2, int TK>
+__device__ __forceinline__ void xfft_project_cta(C* __restrict__ spec, const KParams& k, const C* __restrict__ twN) {
+  constexpr int N = N1 * N2;
+  constexpr int NC = 6 * TK;
+  extern __shared__ __align__(16) unsigned char xfft_smem[];
+  V2<T>* s = reinterpret_cast<V2<T>*>(xfft_smem);
+  V2<T>* tw = s + N * NC;
+  const int y = blockIdx.y;
+  const int yp = (k.ny - y) % k.ny;
+  const int k0 = blockIdx.x * TK;
+  const int kzn = k.nz / 2;  // nz is even on this path
+  const bool planes = k0 == 0 || (kzn >= k0 && kzn < k0 + TK);
+  if (planes && yp < y) return;  // row y is done by the CTA of row yp
+  const int rows = (planes && yp != y) ? 2 : 1;
+  const int ncol = rows * 3 * TK;
+  const long long xs = (long long)k.ny * k.nzh;  // x stride of the spectrum
+  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = ldt<T>(twN[i]);
+  for (int i = threadIdx.x; i < N * ncol; i += blockDim.x) {
+    const int kzl = i % TK, rc = (i / TK) % (3 * rows), x = i / (TK * 3 * rows);
+    const int kz = k0 + kzl, c = rc % 3, yr = rc < 3 ? y : yp;
+    V2<T> v{(T)0, (T)0};
+    if (kz < k.nzh) v = ldt<T>(spec[c * k.Gc + x * xs + (long long)yr * k.nzh + kz]);
+    s[x * NC + rc * TK + kzl] = v;
+  }
+  __syncthreads();
+  xpass_a<T, N1, N2, false>(s, tw, ncol, NC);
+  __syncthreads();
+  xpass_b<T, N1, N2, false>(s, tw, ncol, NC);
+  __syncthreads();
+  // projection; position k1*N2 + k2 holds mode kx = k1 + N1*k2
+  const T ie = (T)k.inv_etaG;
+  for (int i = threadIdx.x; i < N * TK * rows; i += blockDim.x) {
+    const int kzl = i % TK, pos = (i / TK) % N, r = i / (TK * N);
+    const int kz = k0 + kzl;
+    if (kz >= k.nzh) continue;
+    const int yr = r ? yp : y, ypr = r ? y : yp;
+    const int kx = pos / N2 + N1 * (pos % N2);
+    const double q1 = wavenumber(kx, k.nx, k.fx), q2 = wavenumber(yr, k.ny, k.fy), q3 = (double)kz * k.fz;
+    const int cb = 3 * r * TK + kzl;  // column of component 0 of this mode
+    V2<T> f[3], u[3];
+    const bool plane = kz == 0 || kz == kzn;
+    if (!plane) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) f[c] = s[pos * NC + cb + c * TK];
+      project_mode<T>(q1, q2, q3, f, u, ie);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) s[pos * NC + cb + c * TK] = u[c];
+      continue;
+    }
+    if (kz == 0 && kx == 0 && yr == 0) {  // f(0) = 0 and u(0) = 0
+#pragma unroll
+      for (int c = 0; c < 3; ++c) s[pos * NC + cb + c * TK] = V2<T>{(T)0, (T)0};
+      continue;
+    }
+    const int kxp = (k.nx - kx) % k.nx;
+    const int posp = (kxp % N1) * N2 + kxp / N1;
+    int pb;  // column of the partner mode -k
+    if (rows == 2) {
+      if (r == 1) continue;  // row 0's thread writes the pair
+      pb = 3 * TK + kzl;
+    } else {
+      if (kxp < kx) continue;  // the partner's thread writes the pair
+      pb = cb;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) f[c] = s[pos * NC + cb + c * TK];
+    project_mode<T>(q1, q2, q3, f, u, ie);
+    if (rows == 1 && kxp == kx) {  // self-conjugate mode
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        u[c].y = (T)0;
+        s[pos * NC + cb + c * TK] = u[c];
+      }
+      continue;
+    }
+    V2<T> fp[3], up[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) fp[c] = s[posp * NC + pb + c * TK];
+    project_mode<T>(wavenumber(kxp, k.nx, k.fx), wavenumber(ypr, k.ny, k.fy), q3, fp, up, ie);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      V2<T> us;
+      us.x = (T)0.5 * (u[c].x + up[c].x);
+      us.y = (T)0.5 * (u[c].y - up[c].y);
+      s[pos * NC + cb + c * TK] = us;
+      s[posp * NC + pb + c * TK] = V2<T>{us.x, -us.y};
+    }
+  }
+  __syncthreads();
+  xpass_b<T, N1, N2, true>(s, tw, ncol, NC);
+  __syncthreads();
+  xpass_a<T, N1, N2, true>(s, tw, ncol, NC);
+  __syncthreads();
+  for (int i = threadIdx.x; i < N * ncol; i += blockDim.x) {
+    const int kzl = i % TK, rc = (i / TK) % (3 * rows), x = i / (TK * 3 * rows);
+    const int kz = k0 + kzl, c = rc % 3, yr = rc < 3 ? y : yp;
+    if (kz >= k.nzh) continue;
+    const V2<T> v = s[x * NC + rc * TK + kzl];
+    C o;
+    o.x = v.x;
+    o.y = v.y;
+    spec[c * k.Gc + x * xs + (long long)yr * k.nzh + kz] = o;
+  }
+}
+
+template <typename T, typename C, int N1, int N2, int TK>
+__global__ void __launch_bounds__(256, (sizeof(T) == 8 && N1 * N2 >= 384) ? 1 : 2)
+    k_xfft_project(C* __restrict__ spec, KParams k, const C* __restrict__ twN) {
+  xfft_project_cta<T, C, N1, N2, TK>(spec, k, twN);
+}
+
+// Batched: blockIdx.z = member gidx[blockIdx.z] of a group of equal grids.
+template <typename T, typename C, int P, int N1, int N2, int TK>
+__global__ void __launch_bounds__(256, (sizeof(T) == 8 && N1 * N2 >= 384) ? 1 : 2)
+    k_b_xfft_project(const BMember* __restrict__ mem, const int* __restrict__ gidx, int mask,
+                     const C* __restrict__ twN) {
+  const BMember& m = mem[gidx[blockIdx.z]];
+  if (bskip(m, mask)) return;
+  xfft_project_cta<T, C, N1, N2, TK>((C*)m.spec[P], m.kp, twN);
+}
+
 }  // namespace
 
 KParams make_kparams(const Ctx& c) {
@@ -297,6 +565,126 @@ KParams make_kparams(const Ctx& c) {
   return k;
 }
 
+
+// ------------------------------------------------------------------ fused x-transform (host)
+// (N1, N2) of the x-transform length n, both divisors of 96 up to 32; false when
+// n is not one of the supported lengths.
+bool xfft_factor(int n, int* n1, int* n2) {
+  static const int tab[][3] = {{8, 2, 4},    {12, 3, 4},   {16, 4, 4},   {24, 4, 6},    {32, 4, 8},
+                               {48, 6, 8},   {64, 8, 8},   {96, 8, 12},  {128, 8, 16},  {192, 12, 16},
+                               {256, 16, 16}, {384, 16, 24}, {512, 16, 32}};
+  for (const auto& t : tab)
+    if (t[0] == n) {
+      *n1 = t[1];
+      *n2 = t[2];
+      return true;
+    }
+  return false;
+}
+
+namespace {
+
+// kz per CTA: shared memory N * (6 TK + 1) elements at most ~110 KB (two CTAs per SM).
+template <typename T>
+constexpr int xfft_tk(int n) {
+  return sizeof(T) == 4 ? (n <= 256 ? 8 : 4) : (n <= 128 ? 8 : (n <= 256 ? 4 : 2));
+}
+
+// One launch: the context's own spectrum (b == nullptr), or the members gidx[0..nm)
+// of a batch group (all with c's grid) when b is given.
+template <typename T, int N1, int N2>
+int xfft_run(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s, bool prepare, const BatchGeom* b,
+             const int* gidx, int nm, int mask) {
+  using C = typename cplx_t<T>::type;
+  constexpr int N = N1 * N2;
+  constexpr int TK = xfft_tk<T>(N);
+  constexpr int P = sizeof(T) == 8 ? 0 : 1;
+  const size_t smem = (size_t)N * (6 * TK + 1) * sizeof(C);
+  if (prepare) {
+    FCM_CUDA(cudaFuncSetAttribute(k_xfft_project<T, C, N1, N2, TK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    FCM_CUDA(cudaFuncSetAttribute(k_b_xfft_project<T, C, P, N1, N2, TK>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    return FCM_OK;
+  }
+  const C* tw = (const C*)(sizeof(T) == 4 ? c.d_xtw32 : c.d_xtw64);
+  const dim3 grid((unsigned)((c.g.nzh + TK - 1) / TK), (unsigned)c.g.ny, (unsigned)(b ? nm : 1));
+  if (b)
+    k_b_xfft_project<T, C, P, N1, N2, TK><<<grid, 256, smem, s>>>(b->mem, gidx, mask, tw);
+  else
+    k_xfft_project<T, C, N1, N2, TK><<<grid, 256, smem, s>>>(spec, make_kparams(c), tw);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+template <typename T>
+int xfft_dispatch(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s, bool prepare,
+                  const BatchGeom* b = nullptr, const int* gidx = nullptr, int nm = 0, int mask = 0) {
+  switch (c.g.nx) {
+    case 8: return xfft_run<T, 2, 4>(c, spec, s, prepare, b, gidx, nm, mask);
+    case 12: return xfft_run<T, 3, 4>(c, spec, s, prepare, b, gidx, nm, mask);
+    case 16: return xfft_run<T, 4, 4>(c, spec, s, prepare, b, gidx, nm, mask);
+    case 24: return xfft_run<T, 4, 6>(c, spec, s, prepare, b, gidx, nm, mask);
+    case 32: return xfft_run<T, 4, 8>(c, spec, s, prepare, b, gidx, nm, mask);
+    case 48: return xfft_run<T, 6, 8>(c, spec, s, prepare, b, gidx, nm, mask);
+    case 64: return xfft_run<T, 8, 8>(c, spec, s, prepare, b, gidx, nm, mask);
+    case 96: return xfft_run<T, 8, 12>(c, spec, s, prepare, b, gidx, nm, mask);
+    case 128: return xfft_run<T, 8, 16>(c, spec, s, prepare, b, gidx, nm, mask);
+    case 192: return xfft_run<T, 12, 16>(c, spec, s, prepare, b, gidx, nm, mask);
+    case 256: return xfft_run<T, 16, 16>(c, spec, s, prepare, b, gidx, nm, mask);
+    case 384: return xfft_run<T, 16, 24>(c, spec, s, prepare, b, gidx, nm, mask);
+    case 512: return xfft_run<T, 16, 32>(c, spec, s, prepare, b, gidx, nm, mask);
+    default: break;
+  }
+  set_error("fused x-transform: unsupported length " + std::to_string(c.g.nx));
+  return FCM_ERR_INVALID;
+}
+
+}  // namespace
+
+// exp(-2 pi i k / 96) into the constant tables of the current device (once per device).
+int xfft_tables_init() {
+  static std::mutex mu;
+  static std::vector<bool> done;
+  int dev = 0;
+  FCM_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if ((int)done.size() <= dev) done.resize(dev + 1, false);
+  if (done[dev]) return FCM_OK;
+  const double PI = 3.14159265358979323846264338327950288;
+  double2 wd[96];
+  float2 wf[96];
+  for (int j = 0; j < 96; ++j) {
+    wd[j] = make_double2(std::cos(2.0 * PI * j / 96.0), -std::sin(2.0 * PI * j / 96.0));
+    wf[j] = make_float2((float)wd[j].x, (float)wd[j].y);
+  }
+  FCM_CUDA(cudaMemcpyToSymbol(c_w96d, wd, sizeof(wd)));
+  FCM_CUDA(cudaMemcpyToSymbol(c_w96f, wf, sizeof(wf)));
+  done[dev] = true;
+  return FCM_OK;
+}
+
+template <typename T>
+int launch_xfft_project(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s) {
+  return xfft_dispatch<T>(c, spec, s, false);
+}
+
+template <typename T>
+int xfft_prepare(const Ctx& c) {
+  return xfft_dispatch<T>(c, nullptr, 0, true);
+}
+
+template <typename T>
+int b_xfft_project(const BatchGeom& b, const Ctx& c0, const int* gidx, int nm, int mask, cudaStream_t s) {
+  return xfft_dispatch<T>(c0, nullptr, s, false, &b, gidx, nm, mask);
+}
+template int b_xfft_project<double>(const BatchGeom&, const Ctx&, const int*, int, int, cudaStream_t);
+template int b_xfft_project<float>(const BatchGeom&, const Ctx&, const int*, int, int, cudaStream_t);
+
+template int launch_xfft_project<double>(const Ctx&, cufftDoubleComplex*, cudaStream_t);
+template int launch_xfft_project<float>(const Ctx&, cufftComplex*, cudaStream_t);
+template int xfft_prepare<double>(const Ctx&);
+template int xfft_prepare<float>(const Ctx&);
 
 template <typename T>
 int launch_project(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s) {
@@ -338,6 +726,54 @@ int launch_stress_divergence_project(const Ctx& c, const cufftDoubleComplex* sig
   const int nt = 256;
   k_fluct<double, cufftDoubleComplex, 0><<<(unsigned)((k.Gc + nt - 1) / nt), nt, 0, s>>>(spec, sigma6, k, 0, 0,
                                                                                          nullptr, 0, 0);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+// Body force of the imposed shear flow (fcm_fluid_solver.cpp:713-734): fx takes
+// the value row[j] of its y index everywhere, fy = fz = 0.
+__global__ void k_shear_forcing(const double* __restrict__ row, double* __restrict__ grid, int ny, int nz,
+                                long long G) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < G; t += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)((t / nz) % ny);
+    grid[t] = row[j];
+    grid[G + t] = 0.0;
+    grid[2 * G + t] = 0.0;
+  }
+}
+
+int launch_shear_forcing(const Ctx& c, const double* d_row, double* grid, cudaStream_t s) {
+  const long long G = c.g.G;
+  const int nt = 256;
+  const long long nb = std::min<long long>((G + nt - 1) / nt, 148LL * 16);
+  k_shear_forcing<<<(unsigned)nb, nt, 0, s>>>(d_row, grid, c.g.ny, c.g.nz, G);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+// x-velocity profile along y (main.cpp:395-429): one block per y index sums
+// u + add over the nx*nz points of that plane, divided by nx*nz.
+__global__ void __launch_bounds__(256) k_x_profile(const double* __restrict__ u, const double* __restrict__ add,
+                                                   int nx, int ny, int nz, double* __restrict__ out) {
+  const int j = blockIdx.x;
+  double acc = 0.0;
+  for (long long t = threadIdx.x; t < (long long)nx * nz; t += blockDim.x) {
+    const int i = (int)(t / nz), k = (int)(t % nz);
+    const long long idx = ((long long)i * ny + j) * nz + k;
+    acc += u[idx] + (add ? add[idx] : 0.0);
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[j] = red[0] / (double)(nx * nz);
+}
+
+int launch_x_profile(const Ctx& c, const double* u, const double* add, double* d_out, cudaStream_t s) {
+  k_x_profile<<<(unsigned)c.g.ny, 256, 0, s>>>(u, add, c.g.nx, c.g.ny, c.g.nz, d_out);
   FCM_LAUNCH_CHECK();
   return FCM_OK;
 }

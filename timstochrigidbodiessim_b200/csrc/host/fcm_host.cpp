@@ -252,6 +252,22 @@ void fcm_fluid_solver::calculate_deterministic_blob_velocities() {
   check(fcm_calculate_deterministic_blob_velocities(ctx(), V.memptr()), "calculate_deterministic_blob_velocities");
 }
 
+void fcm_fluid_solver::produce_shear_velocity_field(double scale, double wavenumber) {
+  check(fcm_produce_shear_velocity_field(ctx(), scale, wavenumber), "produce_shear_velocity_field");
+  Vshear = vec(3 * (size_t)bodies_->total_num_blobs);
+}
+
+void fcm_fluid_solver::calculate_shear_blob_velocities() {
+  Vshear = vec(3 * (size_t)bodies_->total_num_blobs);
+  check(fcm_calculate_shear_blob_velocities(ctx(), Vshear.memptr()), "calculate_shear_blob_velocities");
+}
+
+std::vector<double> fcm_fluid_solver::fluid_x_velocity_in_y(const vec& F) {
+  std::vector<double> prof((size_t)bodies_->params.ny, 0.0);
+  check(fcm_fluid_x_velocity_in_y(ctx(), F.memptr(), prof.data()), "fluid_x_velocity_in_y");
+  return prof;
+}
+
 void fcm_fluid_solver::produce_reference_matrices(collection_of_rigid_bodies& c) {
   bodies_ = &c;
   check(fcm_produce_reference_matrices(ctx()), "produce_reference_matrices");

@@ -175,7 +175,12 @@ class fcm_fluid_solver {
   void produce_deterministic_velocity_field();                // :636-701
   void calculate_deterministic_blob_velocities();             // :363-424
   void produce_reference_matrices(collection_of_rigid_bodies& c);  // :842-881
-  void fetch_velocity_field(int which);                       // ux/uy/uz host mirrors
+  void fetch_velocity_field(int which);                       // ux/uy/uz host mirrors (2 = u_shear)
+  // SHEARING_FORCES (config.hpp:52-56 values as arguments)
+  vec Vshear;                                                  // 3 Nb
+  void produce_shear_velocity_field(double scale, double wavenumber);  // :703-842
+  void calculate_shear_blob_velocities();                      // :489-550
+  std::vector<double> fluid_x_velocity_in_y(const vec& F);     // main.cpp:371-433 (ny values)
 
  private:
   collection_of_rigid_bodies* bodies_;

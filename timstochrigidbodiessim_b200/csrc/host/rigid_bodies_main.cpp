@@ -22,6 +22,9 @@
 //   mcmc=<n>         Metropolis sampling instead of time stepping (MARKOV_CHAIN_MONTE_CARLO,
 //                    main.cpp:113-210): n steps, reported every 200 and saved to
 //                    <prefix>.dat every 200 once past mcmc_save_after (default 100000)
+//   shear=1          sinusoidal shear forcing (SHEARING_FORCES, main.cpp:98-100, :270-272,
+//                    :371-433) with shear_scale=<S> and shear_wavenumber=<w> (default 1 and 1,
+//                    config.hpp:54-55); saves add <prefix>_fluid_x_velocity_in_y.dat
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -146,6 +149,10 @@ int main(int argc, char** argv) {
     fcm.produce_reference_matrices(all_bodies);
     gmres_solver gmres;
     gmres.initialise(all_bodies);
+    const bool shear = opt.count("shear") && std::atoi(opt["shear"].c_str()) != 0;
+    if (shear)  // main.cpp:98-100
+      fcm.produce_shear_velocity_field(opt.count("shear_scale") ? std::atof(opt["shear_scale"].c_str()) : 1.0,
+                                       opt.count("shear_wavenumber") ? std::atof(opt["shear_wavenumber"].c_str()) : 1.0);
     if (opt.count("mcmc")) {  // main.cpp:113-210
       const long long n_total = std::atoll(opt["mcmc"].c_str());
       const long long save_after = opt.count("mcmc_save_after") ? std::atoll(opt["mcmc_save_after"].c_str()) : 100000;
@@ -189,6 +196,7 @@ int main(int argc, char** argv) {
         all_bodies.fill_all_blob_pos_at_midstep();
         fcm.set_up_gaussians(all_bodies.all_blob_pos);
         if (p.noise) fcm.calculate_random_blob_velocities();
+        if (shear) fcm.calculate_shear_blob_velocities();  // main.cpp:270-272
       }
       all_bodies.calculate_forces(t);
       gmres.assemble_RHS(all_bodies, fcm);
@@ -210,6 +218,16 @@ int main(int argc, char** argv) {
         vf << std::scientific << std::setprecision(digits) << t << " ";
         for (size_t i = 0; i < U.n_elem(); ++i) vf << U(i) << " ";
         vf << std::endl;
+        if (shear) {  // main.cpp:371-433: the flow of the constraint forces plus u_shear
+          all_bodies.fill_all_blob_pos_at_midstep();
+          fcm.set_up_gaussians(all_bodies.all_blob_pos);
+          const std::vector<double> prof =
+              fcm.fluid_x_velocity_in_y(soln.subvec(0, 3 * (size_t)all_bodies.total_num_blobs - 1));
+          std::ofstream ff(name + "_fluid_x_velocity_in_y.dat", std::ios::app);
+          ff << t << " ";
+          for (double u : prof) ff << u << " ";
+          ff << std::endl;
+        }
       }
       std::printf("step %d gmres_iters %d rel %.3e status %d\n", accepted, gmres.last_iterations,
                   gmres.last_relative_error, gmres.last_status);

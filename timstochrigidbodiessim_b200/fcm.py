@@ -239,6 +239,29 @@ class Suspension:
         self._c(self.L.fcm_apply_mobility(self.h, p, po), "fcm_apply_mobility")
         return V
 
+    # -------------------------------------------------- shear forcing (SHEARING_FORCES)
+    def produce_shear_velocity_field(self, scale=1.0, wavenumber=1.0):
+        """fcm_fluid_solver.cpp:703-842 with SHEAR_FORCE_SCALE = scale and
+        SHEAR_WAVENUMBER = wavenumber; later RHS assemblies subtract Vshear and
+        GDC steps interpolate it at the midstep."""
+        self._c(self.L.fcm_produce_shear_velocity_field(self.h, float(scale), float(wavenumber)),
+                "fcm_produce_shear_velocity_field")
+
+    def calculate_shear_blob_velocities(self, out=None):
+        """fcm_fluid_solver.cpp:489-550: Vshear (3Nb) on the current Gaussians."""
+        V, p = _out(out, 3 * self.Nb)
+        self._c(self.L.fcm_calculate_shear_blob_velocities(self.h, p), "fcm_calculate_shear_blob_velocities")
+        return V
+
+    def fluid_x_velocity_in_y(self, F):
+        """main.cpp:371-433: mean over x and z of ux + ux_shear for every y index,
+        ux the flow of blob forces F on the current Gaussians."""
+        k, p = _in(F, 3 * self.Nb)
+        prof = np.zeros(self.p.ny)
+        self._c(self.L.fcm_fluid_x_velocity_in_y(self.h, p, ctypes.c_void_p(prof.ctypes.data)),
+                "fcm_fluid_x_velocity_in_y")
+        return prof
+
     # -------------------------------------------------- Metropolis Monte Carlo (main.cpp:113-210)
     def calculate_potential(self):
         U = ctypes.c_double(0.0)
