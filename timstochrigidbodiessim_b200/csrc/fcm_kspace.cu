@@ -425,25 +425,26 @@ __device__ __forceinline__ void xpass_b(V2<T>* __restrict__ s, const V2<T>* __re
   }
 }
 
-// One CTA: kz in [blockIdx.x*TK, +TK) of row y = blockIdx.y.  A chunk that holds a
-// Hermitian plane (kz = 0 or nz/2) pairs mode k with -k of row -y, so the CTA of the
-// smaller of {y, -y} takes both rows and the other returns: every {k, -k} pair is
-// read and written by one thread, as in k_project (the spectrum is updated in place).
-// Shared memory: pencils [N][6 TK] (column (row*3 + c)*TK + kz_local), twiddles W_N^j.
-template <typename T, typename C, int N1, int N2, int TK>
+// Two kernels share this body.  Interior (PLANES false): one CTA per (TK kz, row y),
+// every kz except the Hermitian planes kz = 0 and nz/2, where modes have no
+// partner.  Planes (PLANES true, TK = 1): one CTA per (plane, {y, -y}): the mode
+// k pairs with -k of row -y, so the CTA of the smaller of y and -y takes both rows
+// and each {k, -k} pair is read and written by one thread, as in k_project (the
+// spectrum is updated in place).  Shared memory: pencils [N][NC] (column
+// (row*3 + c)*TK + kz_local) and the twiddles W_N^j.
+template <typename T, typename C, int N1, int N2, int TK, bool PLANES>
 __device__ __forceinline__ void xfft_project_cta(C* __restrict__ spec, const KParams& k, const C* __restrict__ twN) {
   constexpr int N = N1 * N2;
-  constexpr int NC = 6 * TK;
+  constexpr int NC = (PLANES ? 6 : 3) * TK;
   extern __shared__ __align__(16) unsigned char xfft_smem[];
   V2<T>* s = reinterpret_cast<V2<T>*>(xfft_smem);
   V2<T>* tw = s + N * NC;
   const int y = blockIdx.y;
   const int yp = (k.ny - y) % k.ny;
-  const int k0 = blockIdx.x * TK;
   const int kzn = k.nz / 2;  // nz is even on this path
-  const bool planes = k0 == 0 || (kzn >= k0 && kzn < k0 + TK);
-  if (planes && yp < y) return;  // row y is done by the CTA of row yp
-  const int rows = (planes && yp != y) ? 2 : 1;
+  const int k0 = PLANES ? (blockIdx.x == 0 ? 0 : kzn) : (int)blockIdx.x * TK;
+  if (PLANES && yp < y) return;  // row y is done by the CTA of row yp
+  const int rows = (PLANES && yp != y) ? 2 : 1;
   const int ncol = rows * 3 * TK;
   const long long xs = (long long)k.ny * k.nzh;  // x stride of the spectrum
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = ldt<T>(twN[i]);
@@ -451,7 +452,7 @@ __device__ __forceinline__ void xfft_project_cta(C* __restrict__ spec, const KPa
     const int kzl = i % TK, rc = (i / TK) % (3 * rows), x = i / (TK * 3 * rows);
     const int kz = k0 + kzl, c = rc % 3, yr = rc < 3 ? y : yp;
     V2<T> v{(T)0, (T)0};
-    if (kz < k.nzh) v = ldt<T>(spec[c * k.Gc + x * xs + (long long)yr * k.nzh + kz]);
+    if (PLANES || (kz != 0 && kz < kzn)) v = ldt<T>(spec[c * k.Gc + x * xs + (long long)yr * k.nzh + kz]);
     s[x * NC + rc * TK + kzl] = v;
   }
   __syncthreads();
@@ -464,14 +465,13 @@ __device__ __forceinline__ void xfft_project_cta(C* __restrict__ spec, const KPa
   for (int i = threadIdx.x; i < N * TK * rows; i += blockDim.x) {
     const int kzl = i % TK, pos = (i / TK) % N, r = i / (TK * N);
     const int kz = k0 + kzl;
-    if (kz >= k.nzh) continue;
+    if (!PLANES && (kz == 0 || kz >= kzn)) continue;
     const int yr = r ? yp : y, ypr = r ? y : yp;
     const int kx = pos / N2 + N1 * (pos % N2);
     const double q1 = wavenumber(kx, k.nx, k.fx), q2 = wavenumber(yr, k.ny, k.fy), q3 = (double)kz * k.fz;
     const int cb = 3 * r * TK + kzl;  // column of component 0 of this mode
     V2<T> f[3], u[3];
-    const bool plane = kz == 0 || kz == kzn;
-    if (!plane) {
+    if (!PLANES) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) f[c] = s[pos * NC + cb + c * TK];
       project_mode<T>(q1, q2, q3, f, u, ie);
@@ -526,7 +526,7 @@ __device__ __forceinline__ void xfft_project_cta(C* __restrict__ spec, const KPa
   for (int i = threadIdx.x; i < N * ncol; i += blockDim.x) {
     const int kzl = i % TK, rc = (i / TK) % (3 * rows), x = i / (TK * 3 * rows);
     const int kz = k0 + kzl, c = rc % 3, yr = rc < 3 ? y : yp;
-    if (kz >= k.nzh) continue;
+    if (!PLANES && (kz == 0 || kz >= kzn)) continue;
     const V2<T> v = s[x * NC + rc * TK + kzl];
     C o;
     o.x = v.x;
@@ -535,20 +535,37 @@ __device__ __forceinline__ void xfft_project_cta(C* __restrict__ spec, const KPa
   }
 }
 
-template <typename T, typename C, int N1, int N2, int TK>
-__global__ void __launch_bounds__(256, (sizeof(T) == 8 && N1 * N2 >= 384) ? 1 : 2)
+// Threads per CTA (a CTA sized to one pencil DFT per thread and step, 384 threads
+// at 256 points, measured slower than 256 threads).
+template <typename T, int N1, int N2, int TK, bool PLANES>
+constexpr int xfft_block() {
+  return 256;
+}
+
+// CTAs per SM the register allocation must allow: three for the FP32 transforms up
+// to 256 points, fewer for the longer ones and for FP64, whose pencils need more
+// registers.
+template <typename T, int N, int BLOCK>
+constexpr int xfft_min_blocks() {
+  return sizeof(T) == 4 ? (N <= 256 ? 3 : 2) : (N <= 256 ? 2 : 1);
+}
+
+template <typename T, typename C, int N1, int N2, int TK, bool PLANES>
+__global__ void __launch_bounds__(xfft_block<T, N1, N2, TK, PLANES>(),
+                                  (xfft_min_blocks<T, N1 * N2, xfft_block<T, N1, N2, TK, PLANES>()>()))
     k_xfft_project(C* __restrict__ spec, KParams k, const C* __restrict__ twN) {
-  xfft_project_cta<T, C, N1, N2, TK>(spec, k, twN);
+  xfft_project_cta<T, C, N1, N2, TK, PLANES>(spec, k, twN);
 }
 
 // Batched: blockIdx.z = member gidx[blockIdx.z] of a group of equal grids.
-template <typename T, typename C, int P, int N1, int N2, int TK>
-__global__ void __launch_bounds__(256, (sizeof(T) == 8 && N1 * N2 >= 384) ? 1 : 2)
+template <typename T, typename C, int P, int N1, int N2, int TK, bool PLANES>
+__global__ void __launch_bounds__(xfft_block<T, N1, N2, TK, PLANES>(),
+                                  (xfft_min_blocks<T, N1 * N2, xfft_block<T, N1, N2, TK, PLANES>()>()))
     k_b_xfft_project(const BMember* __restrict__ mem, const int* __restrict__ gidx, int mask,
                      const C* __restrict__ twN) {
   const BMember& m = mem[gidx[blockIdx.z]];
   if (bskip(m, mask)) return;
-  xfft_project_cta<T, C, N1, N2, TK>((C*)m.spec[P], m.kp, twN);
+  xfft_project_cta<T, C, N1, N2, TK, PLANES>((C*)m.spec[P], m.kp, twN);
 }
 
 }  // namespace
@@ -584,14 +601,20 @@ bool xfft_factor(int n, int* n1, int* n2) {
 
 namespace {
 
-// kz per CTA: shared memory N * (6 TK + 1) elements at most ~110 KB (two CTAs per SM).
+// kz per interior CTA: shared memory N * (3 TK + 1) elements near 50 KB.
 template <typename T>
 constexpr int xfft_tk(int n) {
   return sizeof(T) == 4 ? (n <= 256 ? 8 : 4) : (n <= 128 ? 8 : (n <= 256 ? 4 : 2));
 }
 
-// One launch: the context's own spectrum (b == nullptr), or the members gidx[0..nm)
-// of a batch group (all with c's grid) when b is given.
+template <typename K>
+int xfft_smem_attr(K kernel, size_t smem) {
+  FCM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  return FCM_OK;
+}
+
+// The interior and plane launches: the context's own spectrum (b == nullptr), or
+// the members gidx[0..nm) of a batch group (all with c's grid) when b is given.
 template <typename T, int N1, int N2>
 int xfft_run(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s, bool prepare, const BatchGeom* b,
              const int* gidx, int nm, int mask) {
@@ -599,20 +622,30 @@ int xfft_run(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s, bool 
   constexpr int N = N1 * N2;
   constexpr int TK = xfft_tk<T>(N);
   constexpr int P = sizeof(T) == 8 ? 0 : 1;
-  const size_t smem = (size_t)N * (6 * TK + 1) * sizeof(C);
+  const size_t smem_i = (size_t)N * (3 * TK + 1) * sizeof(C);
+  const size_t smem_p = (size_t)N * 7 * sizeof(C);
   if (prepare) {
-    FCM_CUDA(cudaFuncSetAttribute(k_xfft_project<T, C, N1, N2, TK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
-    FCM_CUDA(cudaFuncSetAttribute(k_b_xfft_project<T, C, P, N1, N2, TK>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FCM_TRY(xfft_smem_attr(k_xfft_project<T, C, N1, N2, TK, false>, smem_i));
+    FCM_TRY(xfft_smem_attr(k_xfft_project<T, C, N1, N2, 1, true>, smem_p));
+    FCM_TRY(xfft_smem_attr(k_b_xfft_project<T, C, P, N1, N2, TK, false>, smem_i));
+    FCM_TRY(xfft_smem_attr(k_b_xfft_project<T, C, P, N1, N2, 1, true>, smem_p));
     return FCM_OK;
   }
   const C* tw = (const C*)(sizeof(T) == 4 ? c.d_xtw32 : c.d_xtw64);
-  const dim3 grid((unsigned)((c.g.nzh + TK - 1) / TK), (unsigned)c.g.ny, (unsigned)(b ? nm : 1));
-  if (b)
-    k_b_xfft_project<T, C, P, N1, N2, TK><<<grid, 256, smem, s>>>(b->mem, gidx, mask, tw);
-  else
-    k_xfft_project<T, C, N1, N2, TK><<<grid, 256, smem, s>>>(spec, make_kparams(c), tw);
+  const int kzn = c.g.nz / 2;
+  const unsigned nb = (unsigned)(b ? nm : 1);
+  const dim3 gi((unsigned)((kzn + TK - 1) / TK), (unsigned)c.g.ny, nb), gp(2u, (unsigned)c.g.ny, nb);
+  constexpr int BI = xfft_block<T, N1, N2, TK, false>(), BP = xfft_block<T, N1, N2, 1, true>();
+  if (b) {
+    k_b_xfft_project<T, C, P, N1, N2, TK, false><<<gi, BI, smem_i, s>>>(b->mem, gidx, mask, tw);
+    FCM_LAUNCH_CHECK();
+    k_b_xfft_project<T, C, P, N1, N2, 1, true><<<gp, BP, smem_p, s>>>(b->mem, gidx, mask, tw);
+  } else {
+    const KParams k = make_kparams(c);
+    k_xfft_project<T, C, N1, N2, TK, false><<<gi, BI, smem_i, s>>>(spec, k, tw);
+    FCM_LAUNCH_CHECK();
+    k_xfft_project<T, C, N1, N2, 1, true><<<gp, BP, smem_p, s>>>(spec, k, tw);
+  }
   FCM_LAUNCH_CHECK();
   return FCM_OK;
 }
