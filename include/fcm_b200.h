@@ -57,7 +57,8 @@ enum fcm_status {
 /* ------------------------------------------------------------------ parameters
  * Runtime replacements for the compile-time macros of config.hpp.  Defaults
  * (fcm_default_params) follow config.hpp with SLIP_CHANNEL false and
- * SIMULATION_ALGORITHM 2 (Euler-Maruyama). */
+ * SIMULATION_ALGORITHM 2 (Euler-Maruyama); set slip_channel = 1 for the
+ * reference's default geometry. */
 typedef struct fcm_params {
   int32_t nx, ny, nz;        /* NUM_FFT_GRID_POINTS_{X,Y,Z} (config.hpp:65-67)     */
   int32_t ngauss;            /* NUM_FCM_GAUSSIAN_POINTS, stencil width W (:69)     */
@@ -85,6 +86,13 @@ typedef struct fcm_params {
   int32_t noise;             /* 1 = fluctuating stress on (main.cpp:231),
                                 0 = noise off (deterministic runs)                  */
   int32_t skip_on_overlap;   /* SKIP_ON_OVERLAP (:35)                              */
+  int32_t slip_channel;      /* SLIP_CHANNEL (:33): free-slip walls at y = 0 and
+                                y = L_y/2 by the image system in y (the bodies live
+                                in 0 < y < L_y/2): mirrored force grids and stress,
+                                Gaussians truncated at ny/2, wall forces and
+                                potential, steps rejected on wall contact.  Not
+                                with batches, force dipoles or skip-free graph steps
+                                (slip-channel steps are host-driven).             */
 } fcm_params;
 
 /* Per-step diagnostics returned by fcm_step. */
@@ -188,6 +196,11 @@ int fcm_end_of_step_update(fcm_ctx* ctx, const double* U, double nu, int32_t* ov
 int fcm_reset_to_start_of_step(fcm_ctx* ctx);
 /* collection_of_rigid_bodies.cpp:195-205 on the current all_blob_pos. */
 int fcm_check_for_overlap(fcm_ctx* ctx, int32_t* overlap);
+/* collection_of_rigid_bodies.cpp:207-239 on the current all_blob_pos: a blob with
+ * y == 0 or y >= L_y/2 (always 0 without a slip channel).  With slip_channel,
+ * fcm_advance_to_midstep and fcm_end_of_step_update report such contacts whatever
+ * skip_on_overlap is (:611-617, :780-786). */
+int fcm_check_for_channel_wall_overlap(fcm_ctx* ctx, int32_t* overlap);
 
 /* ================================================================ linked_list */
 /* linked_list.cpp:74-102: cell of every blob from all_blob_pos. */

@@ -817,9 +817,30 @@ void set_up_gaussians(orc* o, const double* Y, int nrows) {
   }
 }
 
-// fcm_fluid_solver.cpp:552-600 (SLIP_CHANNEL false, so :602-632 is absent).  The
-// x-slab loop mirrors the reference's per-rank slab filter (:568-570); with t
-// threads each owns a slab, so every grid point sums its blobs in blob order.
+// Slip channel (fcm_fluid_solver.cpp:602-632, and :735-760 for the shear forcing):
+// fy = 0 on the wall rows 0 and Ny/2; rows above Ny/2 become mirror images.
+void slip_image(orc* o) {
+  const int Nx = o->Nx, Ny = o->Ny, pad = o->pad, half_y = Ny / 2;
+  for (int i = 0; i < Nx; i++) {
+    const size_t x_index = (size_t)i * Ny * pad;
+    for (int k = 0; k < pad; k++) {
+      const size_t z_index = k;
+      o->fy[x_index + z_index] = 0.0;
+      o->fy[x_index + z_index + (size_t)half_y * pad] = 0.0;
+      for (int j = 1 + half_y; j < Ny; j++) {
+        const size_t index = x_index + z_index + (size_t)j * pad;
+        const size_t image_index = x_index + z_index + (size_t)(Ny - j) * pad;
+        o->fx[index] = o->fx[image_index];
+        o->fy[index] = -o->fy[image_index];
+        o->fz[index] = o->fz[image_index];
+      }
+    }
+  }
+}
+
+// fcm_fluid_solver.cpp:552-632.  The x-slab loop mirrors the reference's per-rank
+// slab filter (:568-570); with t threads each owns a slab, so every grid point sums
+// its blobs in blob order.
 void spread(orc* o, const double* F) {
   const size_t P = o->P;
   std::fill(o->fx.begin(), o->fx.end(), 0.0);
@@ -856,6 +877,7 @@ void spread(orc* o, const double* F) {
       }
     }
   }
+  if (o->p.slip_channel) slip_image(o);
 }
 
 // fcm_fluid_solver.cpp:363-424 / :426-487 (interpolation of ux/uy/uz or u*_rand).
@@ -871,6 +893,7 @@ void interp(orc* o, const double* u1, const double* u2, const double* u3) {
       const size_t x_index = (size_t)ii * Ny * pad;
       for (int j = 0; j < W; j++) {
         const int jj = o->indy[np * W + j];
+        if (o->p.slip_channel && jj >= Ny / 2) continue;  // truncated Gaussians (fcm_fluid_solver.cpp:387-389)
         const size_t y_index = (size_t)jj * pad;
         for (int k = 0; k < W; k++) {
           const int kk = o->indz[np * W + k];
@@ -1195,11 +1218,33 @@ int gmres(orc* o, double* soln_out, int* iters_out, double* rel_out) {
   return FCM_ERR_STATE;
 }
 
-void calculate_forces(orc* o) {  // collection_of_rigid_bodies.cpp:623-664 (EM, no slip channel)
+void calculate_forces(orc* o) {  // collection_of_rigid_bodies.cpp:623-664
   if (o->p.algorithm == 2) o->midstep_bodies = o->bodies;
   orc_list_populate(o);
   std::fill(o->blob_forces.begin(), o->blob_forces.end(), 0.0);
   orc_apply_barrier_forces(o, o->blob_forces.data());
+  if (o->p.slip_channel) {  // :640-662
+    const double L = 2.2 * o->a;
+    const double K = (40.0 * o->kT / o->a) / L;
+    for (int i = 0; i < o->Nb; i++) {
+      const double y = o->all_blob_pos[3 * i + 1];
+      if (y <= L) {
+        o->blob_forces[3 * i + 1] += K * (L - y);
+      } else if ((0.5 * o->LY - y <= L) && (y <= 0.5 * o->LY)) {
+        o->blob_forces[3 * i + 1] -= K * (L - 0.5 * o->LY + y);
+      }
+    }
+  }
+}
+
+// collection_of_rigid_bodies.cpp:207-239
+int wall_overlap(const orc* o) {
+  if (!o->p.slip_channel) return 0;
+  for (int n = 0; n < o->Nb; n++) {
+    const double y = o->all_blob_pos[3 * n + 1];
+    if ((y == 0.0) || (y >= 0.5 * o->LY)) return 1;
+  }
+  return 0;
 }
 
 }  // namespace
@@ -1351,7 +1396,7 @@ int orc_advance_to_midstep(orc* o, const double* V) {
   }
   orc_fill_all_blob_pos(o, 1);
   orc_list_populate(o);
-  return o->p.skip_on_overlap ? orc_check_for_overlap(o) : 0;
+  return (wall_overlap(o) || (o->p.skip_on_overlap && orc_check_for_overlap(o))) ? 1 : 0;  // :611-617
 }
 
 // collection_of_rigid_bodies.cpp:869-953
@@ -1388,7 +1433,7 @@ int orc_end_of_step_update(orc* o, const double* U, double nu) {
   }
   orc_fill_all_blob_pos(o, 0);
   orc_list_populate(o);
-  return o->p.skip_on_overlap ? orc_check_for_overlap(o) : 0;
+  return (wall_overlap(o) || (o->p.skip_on_overlap && orc_check_for_overlap(o))) ? 1 : 0;  // :780-786
 }
 void orc_reset_to_start_of_step(orc* o) { o->bodies = o->temp_bodies; }
 
@@ -1479,9 +1524,36 @@ void orc_produce_random_velocity_field(orc* o, uint64_t seed, uint64_t counter) 
   for (int i = 0; i < o->Nx; i++) {
     UniformStream rng(seed, (counter << 20) + (uint64_t)i);
     const size_t x_index = (size_t)i * Ny * pad;
+    const int half_y = Ny / 2;
     for (int k = 0; k < pad; k++)
       for (int j = 0; j < Ny; j++) {
         const size_t index = x_index + k + (size_t)j * pad;
+        if (o->p.slip_channel) {  // fcm_fluid_solver.cpp:186-217
+          if ((j == 0) || (j == half_y)) {
+            o->sxx[index] = std::sqrt(2.0) * var2 * rng.gaussian_random();
+            o->syy[index] = std::sqrt(2.0) * var2 * rng.gaussian_random();
+            o->szz[index] = std::sqrt(2.0) * var2 * rng.gaussian_random();
+            o->sxz[index] = std::sqrt(2.0) * var1 * rng.gaussian_random();
+            o->sxy[index] = 0.0;
+            o->syz[index] = 0.0;
+          } else if (j < half_y) {
+            o->sxx[index] = var2 * rng.gaussian_random();
+            o->syy[index] = var2 * rng.gaussian_random();
+            o->szz[index] = var2 * rng.gaussian_random();
+            o->sxz[index] = var1 * rng.gaussian_random();
+            o->sxy[index] = var1 * rng.gaussian_random();
+            o->syz[index] = var1 * rng.gaussian_random();
+          } else {
+            const size_t image_index = x_index + k + (size_t)(Ny - j) * pad;
+            o->sxx[index] = o->sxx[image_index];
+            o->syy[index] = o->syy[image_index];
+            o->szz[index] = o->szz[image_index];
+            o->sxz[index] = o->sxz[image_index];
+            o->sxy[index] = -o->sxy[image_index];
+            o->syz[index] = -o->syz[image_index];
+          }
+          continue;
+        }
         o->sxx[index] = var2 * rng.gaussian_random();
         o->syy[index] = var2 * rng.gaussian_random();
         o->szz[index] = var2 * rng.gaussian_random();
@@ -1515,7 +1587,7 @@ void orc_get_grid(orc* o, int which, double* out) {
 void orc_produce_reference_matrices(orc* o) {
   const int nb = o->nb, n3 = 3 * nb;
   Body c;
-  c.x[0] = 0.5 * o->LX; c.x[1] = 0.5 * o->LY; c.x[2] = 0.5 * o->LZ;
+  c.x[0] = 0.5 * o->LX; c.x[1] = (o->p.slip_channel ? 0.25 : 0.5) * o->LY; c.x[2] = 0.5 * o->LZ;  // :139-147
   c.q.s = 1.0; c.q.v[0] = c.q.v[1] = c.q.v[2] = 0.0;
   std::vector<double> Y((size_t)3 * nb);
   for (int m = 0; m < nb; ++m) blob_pos_of(o, c, m, &Y[3 * m]);
@@ -1842,6 +1914,25 @@ double mcmc_uniform(uint64_t seed, uint64_t attempt, uint32_t i) {
   return ((double)(out[0] >> 5) * 67108864.0 + (double)(out[1] >> 6)) * (1.0 / 9007199254740992.0);
 }
 
+// collection_of_rigid_bodies.cpp:666-705: the pair potential, then a slip
+// channel's wall potential blob by blob (:679-700).
+double total_potential(orc* o) {
+  double potential = barrier_potential(o);
+  if (o->p.slip_channel) {
+    const double L = 2.2 * o->a;
+    const double K = 40.0 * o->kT / (L * o->a);
+    for (int i = 0; i < o->Nb; i++) {
+      const double y = o->all_blob_pos[3 * i + 1];
+      if (y <= L) {
+        potential += 0.5 * K * (L - y) * (L - y);
+      } else if ((0.5 * o->LY - y <= L) && (y <= 0.5 * o->LY)) {
+        potential += 0.5 * K * (L - 0.5 * o->LY + y) * (L - 0.5 * o->LY + y);
+      }
+    }
+  }
+  return potential;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1850,7 +1941,7 @@ extern "C" {
 double orc_calculate_potential(orc* o) {
   orc_fill_all_blob_pos(o, 0);
   orc_list_populate(o);
-  return barrier_potential(o);
+  return total_potential(o);
 }
 
 // main.cpp:113-210 with Philox uniforms (see mcmc_uniform).
@@ -1879,7 +1970,7 @@ int orc_mcmc_run(orc* o, uint64_t seed, int64_t n_steps, fcm_mcmc_state* st) {
       ++attempt;
       continue;
     }
-    const double U = barrier_potential(o);
+    const double U = total_potential(o);
     const double u = mcmc_uniform(seed, (uint64_t)attempt, (uint32_t)(6 * o->M));
     if (u < std::exp((U_old - U) / o->kT)) {
       U_old = U;
@@ -1926,6 +2017,7 @@ void orc_produce_shear_velocity_field(orc* o, double scale, double wavenumber) {
       for (int k = 0; k < Nz; k++) o->fx[x_index + y_index + k] = f;
     }
   }
+  if (o->p.slip_channel) slip_image(o);  // :735-760
   produce_deterministic_velocity_field(o);
   o->ux_shear = o->ux;
   o->uy_shear = o->uy;

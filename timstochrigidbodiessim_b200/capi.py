@@ -48,6 +48,7 @@ SIGNATURES = {
     "fcm_end_of_step_update": (ctypes.c_int, [VP, VP, ctypes.c_double, I32]),
     "fcm_reset_to_start_of_step": (ctypes.c_int, [VP]),
     "fcm_check_for_overlap": (ctypes.c_int, [VP, I32]),
+    "fcm_check_for_channel_wall_overlap": (ctypes.c_int, [VP, I32]),
     "fcm_list_populate": (ctypes.c_int, [VP]),
     "fcm_list_get_cells": (ctypes.c_int, [VP, VP]),
     "fcm_list_get_pairs": (ctypes.c_int, [VP, VP, ctypes.c_int64, I64]),

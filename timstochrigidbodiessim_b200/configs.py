@@ -180,6 +180,48 @@ def rod_suspension(M, grid, L=None, phi=None, nb=6, seed=1234, gmres_tol=1e-10, 
     return p, ref, x, q, fe
 
 
+def rod_channel(M, grid, L, nb=6, seed=1234, margin=2.2 * A, gmres_tol=1e-10, gmres_max_iter=100, dt=0.01,
+                kT=1.0, noise=1, algorithm=2, precision=0, ngauss=20, max_trials=200000):
+    """A rod suspension in a slip channel (slip_channel = 1): an L^3 periodic box
+    whose bodies live in 0 < y < L/2, every blob at least `margin` from the walls
+    (outside the walls' spring range 2.2a by default), placed by rejection.
+    Returns params, blob_ref_pos, x, q and external forces (-1 along z, parallel
+    to the walls)."""
+    p, ref, _, _, fe = rod_suspension(M=1, grid=grid, L=L, nb=nb, seed=seed, gmres_tol=gmres_tol,
+                                      gmres_max_iter=gmres_max_iter, dt=dt, kT=kT, noise=noise,
+                                      algorithm=algorithm, precision=precision, ngauss=ngauss)
+    p.num_bodies = M
+    p.slip_channel = 1
+    rng = np.random.default_rng(seed)
+    H = 0.5 * L
+    Y = np.zeros((0, 3))
+    xs, qs = [], []
+    for _ in range(max_trials):
+        if len(xs) == M:
+            break
+        c = rng.uniform(0.0, 1.0, 3) * np.array([L, H, L])
+        qq = random_unit_quaternions(rng, 1)
+        b = c + (rotation_matrices(qq)[0] @ np.asarray(ref).reshape(-1, 3).T).T
+        if b[:, 1].min() < margin or b[:, 1].max() > H - margin:
+            continue
+        b[:, 0] %= L
+        b[:, 2] %= L
+        if len(Y):
+            d = np.abs(Y[None, :, :] - b[:, None, :])
+            d[..., 0] = np.minimum(d[..., 0], L - d[..., 0])
+            d[..., 2] = np.minimum(d[..., 2], L - d[..., 2])
+            if (np.einsum("ijk,ijk->ij", d, d) < (2.0 * A) ** 2).any():
+                continue
+        Y = np.vstack([Y, b])
+        xs.append([c[0] % L, c[1], c[2] % L])
+        qs.append(qq[0])
+    if len(xs) < M:
+        raise RuntimeError("rod_channel: could not place %d rods" % M)
+    fe = np.zeros(6 * M)
+    fe[2::6] = -1.0
+    return p, ref, np.array(xs).ravel(), np.array(qs).ravel(), fe
+
+
 def random_walk_cluster(rng, nb=12, bond=2.2 * A, min_dist=2.0 * A, draws=32, max_tries=100000):
     """A rigid cluster shape grown from a seed blob: each new blob is bonded at
     distance `bond` to a randomly chosen earlier blob, at least min_dist from all

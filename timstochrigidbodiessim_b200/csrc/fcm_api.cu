@@ -359,7 +359,9 @@ int set_up_gaussians_dev(Ctx* c, const double* dY) {
 
 template <typename T>
 int spread_t(Ctx* c, const BlobTable<T>& t, const double* dF) {
-  return launch_spread<T>(*c, t, dF, grid_of<T>(c).r, c->stream);
+  FCM_TRY(launch_spread<T>(*c, t, dF, grid_of<T>(c).r, c->stream));
+  if (c->p.slip_channel) FCM_TRY(launch_slip_image<T>(*c, grid_of<T>(c).r, c->stream));  // :602-632
+  return FCM_OK;
 }
 
 template <typename T>
@@ -566,7 +568,7 @@ int calculate_forces_dev(Ctx* c) {
     FCM_CUDA(cudaMemcpyAsync(c->d_qm, c->d_q, sizeof(double) * 4 * c->M, cudaMemcpyDeviceToDevice, c->stream));
   }
   FCM_TRY(cells_build(*c, c->stream));
-  FCM_TRY(cells_steric_forces(*c, c->d_F, false, c->stream));
+  FCM_TRY(cells_steric_forces(*c, c->d_F, false, c->stream, true));  // + slip-channel walls (:640-662)
   return FCM_OK;
 }
 
@@ -584,8 +586,12 @@ int shear_velocities_dev(Ctx* c) {
   return launch_interp<double>(*c, c->g64.blobs, c->d_ushear, c->d_vshear, c->stream);
 }
 
-int overlap_dev(Ctx* c, int* ov) {
-  FCM_TRY(cells_overlap(*c, c->d_flag, c->stream));
+// Overlaps of all_blob_pos: between bodies (check_for_overlap) and, with walls, a
+// slip channel's wall contacts (check_for_channel_wall_overlap).
+int overlap_dev(Ctx* c, int* ov, bool pairs = true, bool walls = false) {
+  if (pairs) FCM_TRY(cells_overlap(*c, c->d_flag, c->stream));
+  else FCM_CUDA(cudaMemsetAsync(c->d_flag, 0, sizeof(int), c->stream));
+  if (walls) FCM_TRY(cells_wall_overlap(*c, c->d_flag, c->stream));
   int h = 0;
   FCM_CUDA(cudaMemcpyAsync(&h, c->d_flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   FCM_CUDA(cudaStreamSynchronize(c->stream));
@@ -601,8 +607,10 @@ int end_of_step_update_dev(Ctx* c, const double* dU, double nu, int* overlap, co
   FCM_TRY(launch_body_update(*c, c->d_x, c->d_q, dU, scale, c->stream, d_nu));
   FCM_TRY(launch_fill_blob_pos(*c, c->d_x, c->d_q, c->d_Y, c->stream));
   FCM_TRY(cells_build(*c, c->stream));
+  // collection_of_rigid_bodies.cpp:780-786: wall contact always, body overlap with SKIP_ON_OVERLAP
   int ov = 0;
-  if (c->p.skip_on_overlap) FCM_TRY(overlap_dev(c, &ov));
+  if (c->p.skip_on_overlap || c->p.slip_channel)
+    FCM_TRY(overlap_dev(c, &ov, c->p.skip_on_overlap != 0, c->p.slip_channel != 0));
   if (overlap) *overlap = ov;
   return FCM_OK;
 }
@@ -614,8 +622,10 @@ int advance_to_midstep_dev(Ctx* c, const double* dV, int* overlap) {
   FCM_TRY(launch_body_update(*c, c->d_xm, c->d_qm, c->d_U0, 0.5 * c->p.dt, c->stream));
   FCM_TRY(launch_fill_blob_pos(*c, c->d_xm, c->d_qm, c->d_Y, c->stream));
   FCM_TRY(cells_build(*c, c->stream));
+  // collection_of_rigid_bodies.cpp:611-617
   int ov = 0;
-  if (c->p.skip_on_overlap) FCM_TRY(overlap_dev(c, &ov));
+  if (c->p.skip_on_overlap || c->p.slip_channel)
+    FCM_TRY(overlap_dev(c, &ov, c->p.skip_on_overlap != 0, c->p.slip_channel != 0));
   if (overlap) *overlap = ov;
   return FCM_OK;
 }
@@ -917,7 +927,7 @@ int enqueue_resident_step(Ctx* c, long long* k_top, long long* k_sweep, long lon
 // Capture the resident step into c->step_graph (state 1), or mark the context
 // for host-driven steps (state -1) when the step cannot be a graph.
 int build_step_graph(Ctx* c) {
-  if (c->p.skip_on_overlap) {
+  if (c->p.skip_on_overlap || c->p.slip_channel) {  // steps that may be rejected stay host-driven
     c->step_graph_state = -1;
     return FCM_OK;
   }
@@ -978,11 +988,12 @@ int build_step_graph(Ctx* c) {
 
 int reference_matrices_dev(Ctx* c) {
   const int nb = c->nb, n3 = 3 * nb;
-  // Body 0 alone at the box centre with q = 1 (collection_of_rigid_bodies.cpp:132-151).
+  // Body 0 alone at the box centre (in a slip channel at the channel's centre,
+  // y = L_y/4) with q = 1 (collection_of_rigid_bodies.cpp:132-151).
   std::vector<double> ref(3 * nb), Y(3 * nb);
   FCM_CUDA(cudaMemcpyAsync(ref.data(), c->d_ref, sizeof(double) * 3 * nb, cudaMemcpyDeviceToHost, c->stream));
   FCM_CUDA(cudaStreamSynchronize(c->stream));
-  const double centre[3] = {0.5 * c->g.Lx, 0.5 * c->g.Ly, 0.5 * c->g.Lz};
+  const double centre[3] = {0.5 * c->g.Lx, (c->p.slip_channel ? 0.25 : 0.5) * c->g.Ly, 0.5 * c->g.Lz};
   const double L[3] = {c->g.Lx, c->g.Ly, c->g.Lz};
   for (int m = 0; m < nb; ++m)
     for (int d = 0; d < 3; ++d) {
@@ -1094,6 +1105,8 @@ int check_params(const fcm_params* p) {
   if (p->gmres_max_iter < 1) return bad("gmres_max_iter must be >= 1");
   if (p->algorithm != 1 && p->algorithm != 2) return bad("algorithm must be 1 (GDC) or 2 (EM)");
   if (p->precision != 0 && p->precision != 1) return bad("precision must be 0 or 1");
+  if (p->slip_channel != 0 && p->slip_channel != 1) return bad("slip_channel must be 0 or 1");
+  if (p->slip_channel && p->ny % 2) return bad("slip_channel needs an even ny (walls at rows 0 and ny/2)");
   const long long G = (long long)p->nx * p->ny * p->nz;
   if (3 * G > 2000000000LL) return bad("grid too large for 32-bit cuFFT batch strides");
   return FCM_OK;
@@ -1512,6 +1525,8 @@ int build_mcmc_graph(Ctx* c) {
           FCM_TRY(launch_fill_blob_pos(*c, c->d_x, c->d_q, c->d_Y, c->stream));
           FCM_TRY(cells_build(*c, c->stream));
           if (c->p.skip_on_overlap) FCM_TRY(cells_overlap(*c, c->d_flag, c->stream));
+          else if (c->p.slip_channel) FCM_CUDA(cudaMemsetAsync(c->d_flag, 0, sizeof(int), c->stream));
+          FCM_TRY(cells_wall_overlap(*c, c->d_flag, c->stream));  // slip channel (main.cpp:160)
           FCM_TRY(cells_potential_terms(*c, c->d_tmp3, c->stream));
           FCM_TRY(blas_dot(*c, c->d_tmp3, nullptr, c->Nb, c->d_usum, c->stream));
           k_mcmc_decide<<<1, 32, 0, c->stream>>>(h, c->d_mcmc, c->d_usum, c->d_flag, (unsigned int)(6 * c->M));
@@ -1560,7 +1575,7 @@ int mcmc_run_dev(Ctx* c, uint64_t seed, long long n_steps, fcm_mcmc_state* state
   h.body_radius = c->body_radius > 0.0 ? c->body_radius : c->p.blob_radius;
   h.dt = c->p.dt;
   h.kT = c->p.kT;
-  h.skip_on_overlap = c->p.skip_on_overlap;
+  h.skip_on_overlap = c->p.skip_on_overlap || c->p.slip_channel;  // redraw on rejected proposals
   FCM_CUDA(cudaMemcpyAsync(c->d_mcmc, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
   FCM_TRY(potential_sum_dev(c));  // U_old of main.cpp:116
   k_mcmc_set_energy<<<1, 32, 0, c->stream>>>(c->d_mcmc, c->d_usum);
@@ -2053,8 +2068,8 @@ int create_batch(int n, const fcm_params* params, const double* const* refs, Bat
       set_error("batch: every member needs the same precision and gmres_tol");
       return FCM_ERR_INVALID;
     }
-    if (params[i].skip_on_overlap) {
-      set_error("batch: members step without overlap rejection (skip_on_overlap = 0)");
+    if (params[i].skip_on_overlap || params[i].slip_channel) {
+      set_error("batch: members step without overlap rejection (skip_on_overlap = 0, slip_channel = 0)");
       return FCM_ERR_INVALID;
     }
   }
@@ -2341,6 +2356,7 @@ void fcm_default_params(fcm_params* p) {
   p->precision = 0;
   p->noise = 1;
   p->skip_on_overlap = 0;
+  p->slip_channel = 0;
 }
 
 const char* fcm_last_error(void) { return g_err.c_str(); }
@@ -2515,6 +2531,15 @@ int fcm_check_for_overlap(fcm_ctx* ctx, int32_t* overlap) {
   FCM_TRY(cells_build(*c, c->stream));
   int ov = 0;
   FCM_TRY(overlap_dev(c, &ov));
+  if (overlap) *overlap = ov;
+  return FCM_OK;
+}
+
+int fcm_check_for_channel_wall_overlap(fcm_ctx* ctx, int32_t* overlap) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  int ov = 0;
+  if (c->p.slip_channel) FCM_TRY(overlap_dev(c, &ov, false, true));
   if (overlap) *overlap = ov;
   return FCM_OK;
 }
@@ -2731,6 +2756,7 @@ int fcm_produce_shear_velocity_field(fcm_ctx* ctx, double scale, double wavenumb
     double* d_row = reinterpret_cast<double*>(c->g64.c);
     FCM_CUDA(cudaMemcpyAsync(d_row, row.data(), sizeof(double) * ny, cudaMemcpyHostToDevice, c->stream));
     FCM_TRY(launch_shear_forcing(*c, d_row, c->g64.r, c->stream));
+    if (c->p.slip_channel) FCM_TRY(launch_slip_image<double>(*c, c->g64.r, c->stream));  // :735-760
     FCM_TRY(stokes_t<double>(c));  // :771-841, the steps of :636-701
     FCM_CUDA(cudaMemcpyAsync(c->d_ushear, c->g64.r, sizeof(double) * 3 * (size_t)c->g.G, cudaMemcpyDeviceToDevice,
                              c->stream));
@@ -2784,6 +2810,10 @@ int fcm_fluid_x_velocity_in_y(fcm_ctx* ctx, const double* F, double* profile) {
 int fcm_set_up_dipole_distribution(fcm_ctx* ctx, const double* F, const double* T, const double* S) {
   CTX_CHECK(ctx);
   Ctx* c = ctx->c;
+  if (c->p.slip_channel) {
+    set_error("force dipoles have no slip-channel image system");
+    return FCM_ERR_INVALID;
+  }
   if (!c->gauss_ready) {
     set_error("set_up_gaussians must precede spreading");
     return FCM_ERR_STATE;
@@ -2810,6 +2840,10 @@ int fcm_set_up_dipole_distribution(fcm_ctx* ctx, const double* F, const double* 
 int fcm_calculate_deterministic_blob_rotations(fcm_ctx* ctx, double* Omega, double* E) {
   CTX_CHECK(ctx);
   Ctx* c = ctx->c;
+  if (c->p.slip_channel) {
+    set_error("force dipoles have no slip-channel image system");
+    return FCM_ERR_INVALID;
+  }
   if (!c->gauss_ready) {
     set_error("set_up_gaussians must precede interpolation");
     return FCM_ERR_STATE;

@@ -227,8 +227,28 @@ __device__ __forceinline__ void visit_partners(const PairArgs& a, int i, Fn fn) 
   }
 }
 
+// Slip-channel walls at y = 0 and y = L_y/2 (collection_of_rigid_bodies.cpp:640-662,
+// :679-700): within L = 2.2a of a wall a blob feels the spring K (L - d), d its
+// distance to the wall, K = 40 kT / (a L), and has the energy K (L - d)^2 / 2.
+struct Walls {
+  int on;
+  double L, K, Ke, half_ly;  // K of the force (:643), Ke of the energy (:682)
+};
+
+__device__ __forceinline__ double wall_force_y(const Walls& w, double y) {
+  if (y <= w.L) return w.K * (w.L - y);
+  if ((w.half_ly - y <= w.L) && (y <= w.half_ly)) return -(w.K * (w.L - w.half_ly + y));
+  return 0.0;
+}
+
+__device__ __forceinline__ double wall_energy(const Walls& w, double y) {
+  if (y <= w.L) return 0.5 * w.Ke * (w.L - y) * (w.L - y);
+  if ((w.half_ly - y <= w.L) && (y <= w.half_ly)) return 0.5 * w.Ke * (w.L - w.half_ly + y) * (w.L - w.half_ly + y);
+  return 0.0;
+}
+
 __global__ void k_steric(PairArgs a, int type, double rad, double kT, double fs, double rc, double* __restrict__ F,
-                         int accumulate) {
+                         int accumulate, Walls w) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.Nb) return;
   double f0 = 0, f1 = 0, f2 = 0;
@@ -239,6 +259,7 @@ __global__ void k_steric(PairArgs a, int type, double rad, double kT, double fs,
     f1 += mag * (yd / r);
     f2 += mag * (zd / r);
   });
+  if (w.on) f1 += wall_force_y(w, a.Y[3 * i + 1]);  // added after the barrier forces (:640)
   if (accumulate) {
     F[3 * i] += f0;
     F[3 * i + 1] += f1;
@@ -252,15 +273,26 @@ __global__ void k_steric(PairArgs a, int type, double rad, double kT, double fs,
 
 // Energy of blob i with all its partners (each pair is seen from both blobs, so
 // the total is half the sum over blobs; linked_list.cpp:283-360).
+// A slip channel's wall energy enters twice, so that half the sum counts it once.
 __global__ void k_potential_terms(PairArgs a, int type, double rad, double kT, double fs, double rc,
-                                  double* __restrict__ Ui) {
+                                  double* __restrict__ Ui, Walls w) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.Nb) return;
   double u = 0.0;
   visit_partners(a, i, [&](int, double xd, double yd, double zd) {
     u += interaction_energy(sqrt(xd * xd + yd * yd + zd * zd), type, rad, kT, fs, rc);
   });
+  if (w.on) u += 2.0 * wall_energy(w, a.Y[3 * i + 1]);
   Ui[i] = u;
+}
+
+// collection_of_rigid_bodies.cpp:207-239: a blob on the lower wall (y == 0) or at
+// or beyond the upper one (y >= L_y/2).
+__global__ void k_wall_overlap(const double* __restrict__ Y, int Nb, double half_ly, int* __restrict__ flag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= Nb) return;
+  const double y = Y[3 * i + 1];
+  if (y == 0.0 || y >= half_ly) atomicExch(flag, 1);
 }
 
 __global__ void k_overlap(PairArgs a, double lim, int* __restrict__ flag) {
@@ -333,10 +365,16 @@ int cells_build(Ctx& c, cudaStream_t s) {
   return FCM_OK;
 }
 
-int cells_steric_forces(const Ctx& c, double* F, bool accumulate, cudaStream_t s) {
+Walls walls(const Ctx& c, bool on) {
+  const double L = 2.2 * c.p.blob_radius;
+  return Walls{on && c.p.slip_channel ? 1 : 0, L, (40.0 * c.p.kT / c.p.blob_radius) / L,
+               40.0 * c.p.kT / (L * c.p.blob_radius), 0.5 * c.g.Ly};
+}
+
+int cells_steric_forces(const Ctx& c, double* F, bool accumulate, cudaStream_t s, bool with_walls) {
   if (c.Nb == 0) return FCM_OK;
   k_steric<<<(c.Nb + 127) / 128, 128, 0, s>>>(pair_args(c), c.p.potential, c.p.blob_radius, c.p.kT, c.p.steric_fs,
-                                              c.p.steric_rc, F, accumulate ? 1 : 0);
+                                              c.p.steric_rc, F, accumulate ? 1 : 0, walls(c, with_walls));
   FCM_LAUNCH_CHECK();
   return FCM_OK;
 }
@@ -344,7 +382,14 @@ int cells_steric_forces(const Ctx& c, double* F, bool accumulate, cudaStream_t s
 int cells_potential_terms(const Ctx& c, double* Ui, cudaStream_t s) {
   if (c.Nb == 0) return FCM_OK;
   k_potential_terms<<<(c.Nb + 127) / 128, 128, 0, s>>>(pair_args(c), c.p.potential, c.p.blob_radius, c.p.kT,
-                                                       c.p.steric_fs, c.p.steric_rc, Ui);
+                                                       c.p.steric_fs, c.p.steric_rc, Ui, walls(c, true));
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+
+int cells_wall_overlap(const Ctx& c, int* d_flag, cudaStream_t s) {
+  if (c.Nb == 0 || !c.p.slip_channel) return FCM_OK;
+  k_wall_overlap<<<(c.Nb + 127) / 128, 128, 0, s>>>(c.d_Y, c.Nb, 0.5 * c.g.Ly, d_flag);
   FCM_LAUNCH_CHECK();
   return FCM_OK;
 }

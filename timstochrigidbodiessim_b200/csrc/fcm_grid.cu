@@ -505,12 +505,13 @@ __device__ __forceinline__ void interp_tile(const T* __restrict__ wc, const T* _
   T u[TE][3];
   {
     const int ox = tx * TE, oy = ty * TE + y, oz = tz * TE + z;
+    const bool live = oy < g.ycut;  // rows at or above the slip channel's upper wall read as 0
 #pragma unroll
     for (int x = 0; x < TE; ++x) {
       const long long idx = ((long long)(ox + x) * g.ny + oy) * g.nz + oz;
-      u[x][0] = grid[idx];
-      u[x][1] = grid[G + idx];
-      u[x][2] = grid[2 * G + idx];
+      u[x][0] = live ? grid[idx] : (T)0;
+      u[x][1] = live ? grid[G + idx] : (T)0;
+      u[x][2] = live ? grid[2 * G + idx] : (T)0;
     }
   }
   for (int c0 = b0; c0 < b1; c0 += SCB) {
@@ -630,7 +631,7 @@ __global__ void k_spread_atomic(const int* __restrict__ base, const T* __restric
 template <typename T, int NT>
 __global__ void __launch_bounds__(NT) k_interp_block(const int* __restrict__ base, const T* __restrict__ w,
                                                      const T* __restrict__ grid, int W, int nx, int ny, int nz,
-                                                     long long G, double dx3, double* __restrict__ V) {
+                                                     long long G, double dx3, double* __restrict__ V, int ycut) {
   const int np = blockIdx.x;
   const int bx = base[3 * np], by = base[3 * np + 1], bz = base[3 * np + 2];
   const T* gx = w + (size_t)(3 * np) * W;
@@ -640,6 +641,7 @@ __global__ void __launch_bounds__(NT) k_interp_block(const int* __restrict__ bas
   for (int jk = threadIdx.x; jk < W * W; jk += NT) {
     const int j = jk / W, k = jk - j * W;
     const int yy = wrap_index(by + j, ny), zz = wrap_index(bz + k, nz);
+    if (yy >= ycut) continue;  // Gaussians truncated at the slip channel's upper wall
     const T wyz = gy[j] * gz[k];
     for (int i = 0; i < W; ++i) {
       const int xx = wrap_index(bx + i, nx);
@@ -679,7 +681,7 @@ __global__ void __launch_bounds__(NT) k_interp_block(const int* __restrict__ bas
 }  // namespace
 
 TileGeom tile_geom(const GridDims& g, int W) {
-  return TileGeom{g.nx / TE, g.ny / TE, g.nz / TE, g.nx, g.ny, g.nz, W};
+  return TileGeom{g.nx / TE, g.ny / TE, g.nz / TE, g.nx, g.ny, g.nz, W, g.ny};
 }
 
 // CTAs of a persistent kernel: as many as fit on the device at once
@@ -800,18 +802,52 @@ template <typename T>
 int launch_interp(const Ctx& c, const BlobTable<T>& t, const T* grid, double* dV, cudaStream_t s) {
   if (t.n == 0) return FCM_OK;
   const double dx3 = c.g.dx * c.g.dx * c.g.dx;
+  const int ycut = c.p.slip_channel ? c.g.ny / 2 : c.g.ny;  // fcm_fluid_solver.cpp:387-389
   if (t.tiled) {
-    const TileGeom g = tile_geom(c.g, t.W);
+    TileGeom g = tile_geom(c.g, t.W);
+    g.ycut = ycut;
     k_interp_tiled<T><<<t.ntiles, 64, 0, s>>>(t.wc, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial);
     FCM_LAUNCH_CHECK();
     k_interp_reduce<T><<<(t.n + 127) / 128, 128, 0, s>>>(t.base, t.partial, t.n, g, dx3, dV);
     FCM_LAUNCH_CHECK();
     return FCM_OK;
   }
-  k_interp_block<T, 256><<<t.n, 256, 0, s>>>(t.base, t.w, grid, t.W, c.g.nx, c.g.ny, c.g.nz, c.g.G, dx3, dV);
+  k_interp_block<T, 256><<<t.n, 256, 0, s>>>(t.base, t.w, grid, t.W, c.g.nx, c.g.ny, c.g.nz, c.g.G, dx3, dV, ycut);
   FCM_LAUNCH_CHECK();
   return FCM_OK;
 }
+
+// Slip channel (fcm_fluid_solver.cpp:602-632): fy = 0 on the wall rows 0 and ny/2;
+// every row j > ny/2 becomes the mirror image of row ny - j (fx, fz copied, fy
+// negated).  Rows above ny/2 read rows below it, which this kernel does not write.
+template <typename T>
+__global__ void k_slip_image(T* __restrict__ grid, int ny, int nz, long long G) {
+  const int h = ny / 2;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < G; t += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(t % nz);
+    const long long xy = t / nz;
+    const int j = (int)(xy % ny);
+    if (j == 0 || j == h) {
+      grid[G + t] = (T)0;
+    } else if (j > h) {
+      const long long m = (xy - j + (ny - j)) * nz + k;
+      grid[t] = grid[m];
+      grid[G + t] = -grid[G + m];
+      grid[2 * G + t] = grid[2 * G + m];
+    }
+  }
+}
+
+template <typename T>
+int launch_slip_image(const Ctx& c, T* grid, cudaStream_t s) {
+  const long long G = c.g.G;
+  const long long nb = std::min<long long>((G + 255) / 256, 148LL * 16);
+  k_slip_image<T><<<(unsigned)nb, 256, 0, s>>>(grid, c.g.ny, c.g.nz, G);
+  FCM_LAUNCH_CHECK();
+  return FCM_OK;
+}
+template int launch_slip_image<double>(const Ctx&, double*, cudaStream_t);
+template int launch_slip_image<float>(const Ctx&, float*, cudaStream_t);
 
 template int blob_table_alloc<double>(BlobTable<double>&, int, int, const GridDims&);
 template int blob_table_alloc<float>(BlobTable<float>&, int, int, const GridDims&);
@@ -985,12 +1021,13 @@ __global__ void __launch_bounds__(64) k_interp_dipole_tiled(const T* __restrict_
   T u[TE][3];
   {
     const int ox = tx * TE, oy = ty * TE + y, oz = tz * TE + z;
+    const bool live = oy < g.ycut;  // rows at or above the slip channel's upper wall read as 0
 #pragma unroll
     for (int x = 0; x < TE; ++x) {
       const long long idx = ((long long)(ox + x) * g.ny + oy) * g.nz + oz;
-      u[x][0] = grid[idx];
-      u[x][1] = grid[G + idx];
-      u[x][2] = grid[2 * G + idx];
+      u[x][0] = live ? grid[idx] : (T)0;
+      u[x][1] = live ? grid[G + idx] : (T)0;
+      u[x][2] = live ? grid[2 * G + idx] : (T)0;
     }
   }
   for (int c0 = b0; c0 < b1; c0 += SCB) {
@@ -1308,7 +1345,7 @@ extern "C" int fcm_interp_noalloc(int32_t nx, int32_t ny, int32_t nz, double dx,
   const double PI = 3.14159265358979323846264338327950288;
   const double anorm = 1.0 / (sqrt(2.0) * blob_radius);
   const double anorm2 = 2.0 * blob_radius * blob_radius / PI;
-  const TileGeom g{nx / TE, ny / TE, nz / TE, nx, ny, nz, W};
+  const TileGeom g{nx / TE, ny / TE, nz / TE, nx, ny, nz, W, ny};
   const long long G = (long long)nx * ny * nz;
   // the array keeps the previous call's contents: counters start at zero
   FCM_CUDA(cudaMemsetAsync(s_count, 0, sizeof(int) * (size_t)ntiles, s));

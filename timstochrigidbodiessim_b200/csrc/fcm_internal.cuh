@@ -132,6 +132,7 @@ constexpr int TILE_X = 8, TILE_Y = 8, TILE_Z = 8;
 // Tile grid of the tiled spread / interpolation (fcm_grid.cu).
 struct TileGeom {
   int ntx, nty, ntz, nx, ny, nz, W;
+  int ycut;  // interpolation reads rows y < ycut only (ny, or ny/2 in a slip channel)
 };
 
 // k-space geometry of the projection (fcm_kspace.cu).
@@ -140,6 +141,7 @@ struct KParams {
   long long Gc;
   double fx, fy, fz;  // 2 pi / L
   double inv_etaG;    // 1 / (eta * nx*ny*nz)
+  int slip;           // slip channel: image-symmetric fluctuating stress
 };
 
 // Record of one device-resident (graph) time step, written by the device.
@@ -412,6 +414,10 @@ template <typename T>
 int launch_interp(const Ctx& c, const BlobTable<T>& t, const T* grid, double* dV, cudaStream_t s);
 // force dipoles (fcm_grid.cu): D (9 per blob) added to the force grid; moments
 // of the velocity grid into Omega (3 per blob) and E (9 per blob)
+// slip channel: the image of the lower half over the upper half of a force grid
+// (fcm_fluid_solver.cpp:602-632)
+template <typename T>
+int launch_slip_image(const Ctx& c, T* grid, cudaStream_t s);
 template <typename T>
 int launch_spread_dipoles(const Ctx& c, BlobTable<T>& t, const double* dD, T* grid, cudaStream_t s);
 template <typename T>
@@ -459,7 +465,10 @@ int launch_divU_accumulate(const Ctx& c, const double* U6, const double* U0, int
 int launch_exclusive_scan(const int* in, int* out, int n, cudaStream_t s);
 // cells (fcm_cells.cu)
 int cells_build(Ctx& c, cudaStream_t s);
-int cells_steric_forces(const Ctx& c, double* F, bool accumulate, cudaStream_t s);
+// with_walls adds a slip channel's wall forces (collection_of_rigid_bodies.cpp:640-662)
+int cells_steric_forces(const Ctx& c, double* F, bool accumulate, cudaStream_t s, bool with_walls = false);
+// OR-s a slip channel's wall contacts of all_blob_pos into *d_flag (no-op otherwise)
+int cells_wall_overlap(const Ctx& c, int* d_flag, cudaStream_t s);
 int cells_overlap(const Ctx& c, int* d_flag, cudaStream_t s);
 // per-blob pair energies (half their sum is the potential of linked_list.cpp:283-360)
 int cells_potential_terms(const Ctx& c, double* Ui, cudaStream_t s);

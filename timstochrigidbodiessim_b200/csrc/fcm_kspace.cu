@@ -239,6 +239,50 @@ __global__ void k_fluct(C* __restrict__ spec, const cufftDoubleComplex* __restri
         sp[c].y = (T)w.y;
       }
     }
+  } else if (k.slip) {
+    // Image-symmetric stress of a slip channel (fcm_fluid_solver.cpp:186-217): xx, yy,
+    // zz, xz even in y, xy and yz odd, the even ones with twice the variance on the
+    // wall rows 0 and ny/2 and the odd ones zero there.  Its DFT along y is real
+    // and even (odd: imaginary and odd) with independent rows ky = 0..ny/2, those of
+    // the even components of variance ny v^2 (2 ny v^2 on ky = 0, ny/2), those of
+    // the odd ones ny v^2 (0 on ky = 0, ny/2).  So row y takes the draw of row
+    // yr = min(y, ny - y): even components a white (x, z) spectrum of variance
+    // G v^2 (doubled on the wall rows), odd ones -i times one (zero on the wall
+    // rows), negated for y > ny/2.  In the kz = 0 and nz/2 planes (x, yr) pairs
+    // with (-x, yr) as the 2D spectrum of a real field.
+    const int h = k.ny / 2;
+    const int yr = y <= h ? y : k.ny - y;
+    const bool wall = yr == 0 || yr == h;
+    const int xm = (k.nx - x) % k.nx;
+    const int xr = (plane && xm < x) ? xm : x;
+    const bool cj = xr != x, xself = plane && xm == x;
+    float nrm[12];
+    mode_normals((unsigned long long)(((long long)xr * k.ny + yr) * k.nzh + kz), seed, counter, nrm);
+    for (int c = 0; c < 6; ++c) {
+      const double amp = (c < 3) ? amp_diag : amp_off;  // order xx, yy, zz, xy, xz, yz
+      double re, im;
+      if (xself) {
+        re = amp * 1.4142135623730951 * (double)nrm[2 * c];
+        im = 0.0;
+      } else {
+        re = amp * (double)nrm[2 * c];
+        im = amp * (double)nrm[2 * c + 1];
+      }
+      if (cj) im = -im;
+      if (c == 3 || c == 5) {  // odd: -i (re + i im), zero on the walls, negated above ny/2
+        const double sg = wall ? 0.0 : (y > h ? -1.0 : 1.0);
+        const double r2 = sg * im, i2 = -sg * re;
+        re = r2;
+        im = i2;
+      } else if (wall) {
+        re *= 1.4142135623730951;
+        im *= 1.4142135623730951;
+      }
+      s[c].x = (T)re;
+      s[c].y = (T)im;
+      sp[c].x = s[c].x;
+      sp[c].y = -s[c].y;
+    }
   } else {
     float nrm[12];
     mode_normals((unsigned long long)t, seed, counter, nrm);
@@ -579,6 +623,7 @@ KParams make_kparams(const Ctx& c) {
   k.fy = 2.0 * PI / c.g.Ly;
   k.fz = 2.0 * PI / c.g.Lz;
   k.inv_etaG = 1.0 / (c.p.viscosity * ((double)c.g.nx * (double)c.g.ny * (double)c.g.nz));
+  k.slip = c.p.slip_channel;
   return k;
 }
 

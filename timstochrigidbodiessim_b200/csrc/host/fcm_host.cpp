@@ -156,6 +156,12 @@ bool collection_of_rigid_bodies::check_for_overlap() {
   return ov != 0;
 }
 
+bool collection_of_rigid_bodies::check_for_channel_wall_overlap() {
+  int32_t ov = 0;
+  check(fcm_check_for_channel_wall_overlap(ctx_, &ov), "check_for_channel_wall_overlap");
+  return ov != 0;
+}
+
 // collection_of_rigid_bodies.cpp:798-814: "t x y z q0 q1 q2 q3 ..." per line.
 void collection_of_rigid_bodies::write_data_to_file(double t, const std::string& name, int digits) const {
   std::ofstream f(name, std::ios::app);

@@ -144,6 +144,7 @@ class collection_of_rigid_bodies {
   void reset_to_start_of_step();                         // :792-796
   double calculate_divU(fcm_fluid_solver& fcm);          // :869-953
   bool check_for_overlap();                              // :195-205
+  bool check_for_channel_wall_overlap();                 // :207-239
   double calculate_potential();                          // :666-705
   // :798-814 (state part); the reference writes 6 significant digits
   void write_data_to_file(double t, const std::string& name, int digits = 6) const;

@@ -5,7 +5,7 @@
 //
 // keys: the fcm_params fields (nx ny nz ngauss dx blob_radius viscosity kT dt
 // num_bodies blobs_per_body ncells potential steric_fs steric_rc gmres_max_iter
-// gmres_tol fd_delta algorithm noise skip_on_overlap precision), plus
+// gmres_tol fd_delta algorithm noise skip_on_overlap slip_channel precision), plus
 //   shape=<file>     blob reference positions, one "x y z" line per blob
 //   ic=<file>        initial state in the reference's .dat format
 //                    ("t x y z q0 q1 q2 q3 ..." per line; the last line is used,
@@ -55,7 +55,7 @@ static bool set_param(fcm_params& p, const std::string& k, const std::string& v)
   }
   I(nx) I(ny) I(nz) I(ngauss) F(dx) F(blob_radius) F(viscosity) F(kT) F(dt) I(num_bodies) I(blobs_per_body)
   I(ncells) I(potential) F(steric_fs) F(steric_rc) I(gmres_max_iter) F(gmres_tol) F(fd_delta) I(algorithm)
-  I(precision) I(noise) I(skip_on_overlap)
+  I(precision) I(noise) I(skip_on_overlap) I(slip_channel)
 #undef I
 #undef F
   return false;

@@ -169,6 +169,13 @@ class Suspension:
         self._c(self.L.fcm_check_for_overlap(self.h, ctypes.byref(ov)), "fcm_check_for_overlap")
         return bool(ov.value)
 
+    def check_for_channel_wall_overlap(self):
+        """collection_of_rigid_bodies.cpp:207-239 (False without a slip channel)."""
+        ov = ctypes.c_int32(0)
+        self._c(self.L.fcm_check_for_channel_wall_overlap(self.h, ctypes.byref(ov)),
+                "fcm_check_for_channel_wall_overlap")
+        return bool(ov.value)
+
     # -------------------------------------------------- linked_list
     def list_populate(self):
         self._c(self.L.fcm_list_populate(self.h), "fcm_list_populate")

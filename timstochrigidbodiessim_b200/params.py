@@ -32,6 +32,7 @@ class FcmParams(ctypes.Structure):
         ("precision", ctypes.c_int32),
         ("noise", ctypes.c_int32),
         ("skip_on_overlap", ctypes.c_int32),
+        ("slip_channel", ctypes.c_int32),
     ]
 
     @classmethod
@@ -44,7 +45,7 @@ class FcmParams(ctypes.Structure):
                 num_bodies=3, blobs_per_body=22, ncells=6, potential=0,
                 steric_fs=40.0 * kT / a, steric_rc=2.2 * a,
                 gmres_max_iter=40, gmres_tol=1e-3, fd_delta=1e-5,
-                algorithm=2, precision=0, noise=1, skip_on_overlap=0)
+                algorithm=2, precision=0, noise=1, skip_on_overlap=0, slip_channel=0)
         for k, v in kw.items():
             if not hasattr(p, k):
                 raise AttributeError(k)
