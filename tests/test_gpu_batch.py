@@ -4,7 +4,8 @@ follow the trajectory of the same suspension stepped alone with fcm_step: the
 batched kernels run each member's arithmetic in the single-suspension order
 (its own reduction grids included), so the only possible difference is cuFFT's
 choice of kernels for a batch of transforms; positions and quaternions must
-agree to 1e-9 absolute and the GMRES iteration counts to within one."""
+agree to 1e-9 absolute (FP64) or 1e-8 (mixed, refined to 1e-8), and the GMRES
+iteration counts to within one."""
 import numpy as np
 import pytest
 
@@ -49,11 +50,14 @@ def test_batch_members_follow_single_steps(gpu, precision, algorithm):
             st, inf = s.step(seeds[i], k)
             assert abs(inf.gmres_iters - infos[i].gmres_iters) <= 1, (k, i)
             assert infos[i].status in (0, 5)
+    # FP64 solves (tol 1e-10) agree to 1e-9; mixed solves, refined to 1e-8, whose
+    # FP32 arithmetic in the batched kernels rounds differently, to 1e-8
+    tol = 1e-8 if precision == 1 else 1e-9
     for s, m in zip(solo, b.members):
         xs, qs = s.get_bodies()
         xm, qm = m.get_bodies()
-        assert np.max(np.abs(xs - xm)) <= 1e-9
-        assert np.max(np.abs(qs - qm)) <= 1e-9
+        assert np.max(np.abs(xs - xm)) <= tol
+        assert np.max(np.abs(qs - qm)) <= tol
     b.close()
 
 

@@ -407,8 +407,14 @@ int random_velocities_dev(Ctx* c, double* dV) {
   return interp_t<float>(c, c->g32.blobs, c->g32.urand, dV);
 }
 
+// Precision of the random velocity field: FP32 for mixed-precision EM steps; FP64
+// otherwise, and for GDC also in mixed precision, whose div(U) differentiates
+// random velocities over 1e-5 a (collection_of_rigid_bodies.cpp:869-953), which
+// FP32 interpolation rounding would swamp.
+int noise_precision(const Ctx* c) { return (c->p.precision == 1 && c->p.algorithm == 2) ? 1 : 0; }
+
 int noise_dev(Ctx* c, uint64_t seed, uint64_t counter, const uint64_t* d_args = nullptr) {
-  if (c->p.precision == 1) {
+  if (noise_precision(c) == 1) {
     FCM_TRY(launch_noise_kspace<float>(*c, c->g32.c, seed, counter, d_args, c->stream));
     FCM_CUFFT(exec_c2r(c->g32.c2r, c->g32.c, c->g32.urand));
     c->urand_prec = 1;
@@ -1425,7 +1431,7 @@ int step_wait(Ctx* c, fcm_step_info* info) {
                  (long long)r.iters * c->step_kernels_iter);
   c->gauss_ready = true;
   c->urand_ready = c->p.noise != 0;
-  c->urand_prec = c->p.precision;
+  c->urand_prec = noise_precision(c);
   fcm_step_info inf;
   std::memset(&inf, 0, sizeof(inf));
   inf.gmres_iters = r.iters;
@@ -2292,7 +2298,7 @@ int batch_step(Batch* B, const uint64_t* seeds, uint64_t step_index, fcm_step_in
     const StepRecord& r = B->h_rec[i];
     c->gauss_ready = true;
     c->urand_ready = c->p.noise != 0;
-    c->urand_prec = c->p.precision;
+    c->urand_prec = noise_precision(c);
     if (infos) {
       fcm_step_info& inf = infos[i];
       std::memset(&inf, 0, sizeof(inf));

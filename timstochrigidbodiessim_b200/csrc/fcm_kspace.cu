@@ -579,6 +579,103 @@ __device__ __forceinline__ void xfft_project_cta(C* __restrict__ spec, const KPa
   }
 }
 
+// Interior CTA (every kz of the chunk except the Hermitian planes): the step over
+// n1 reads its pencils straight from the spectrum into registers and writes the
+// transformed, twiddled values to shared memory [N][3 TK]; after one barrier each
+// thread takes one (k1, kz) and runs, without barriers, the forward step over n2
+// of the three components, the projection of those N2 modes and the inverse step
+// over n2 with its twiddles; after a second barrier the inverse step over n1 goes
+// from shared memory to registers to the spectrum.  Twiddles W_N^j are read
+// through the cache.
+template <typename T, typename C, int N1, int N2, int TK>
+__device__ __forceinline__ void xfft_interior_cta(C* __restrict__ spec, const KParams& k,
+                                                  const C* __restrict__ twN) {
+  constexpr int N = N1 * N2;
+  constexpr int NC = 3 * TK;
+  extern __shared__ __align__(16) unsigned char xfft_smem[];
+  V2<T>* s = reinterpret_cast<V2<T>*>(xfft_smem);
+  const int y = blockIdx.y;
+  const int k0 = (int)blockIdx.x * TK;
+  const int kzn = k.nz / 2;
+  const long long xs = (long long)k.ny * k.nzh;  // x stride of the spectrum
+  const long long row = (long long)y * k.nzh + k0;
+  // forward step over n1: item (column, n2), column = c*TK + kz_local
+  for (int i = threadIdx.x; i < N2 * NC; i += blockDim.x) {
+    const int col = i % NC, n2 = i / NC, kzl = col % TK, c = col / TK;
+    const int kz = k0 + kzl;
+    const bool mine = kz != 0 && kz < kzn;
+    const C* src = spec + c * k.Gc + row + kzl;
+    V2<T> a[N1];
+#pragma unroll
+    for (int j = 0; j < N1; ++j)
+      a[j] = mine ? ldt<T>(src[(long long)(j * N2 + n2) * xs]) : V2<T>{(T)0, (T)0};
+    dft<T, N1, false>(a);
+#pragma unroll
+    for (int j = 1; j < N1; ++j) a[j] = cmul(a[j], ldt<T>(__ldg(&twN[n2 * j])));
+#pragma unroll
+    for (int j = 0; j < N1; ++j) s[(j * N2 + n2) * NC + col] = a[j];
+  }
+  __syncthreads();
+  // per (k1, kz): forward step over n2, projection, inverse step over n2
+  const double q2 = wavenumber(y, k.ny, k.fy);
+  const T ie = (T)k.inv_etaG;
+  for (int i = threadIdx.x; i < N1 * TK; i += blockDim.x) {
+    const int kzl = i % TK, k1 = i / TK;
+    const int kz = k0 + kzl;
+    if (kz == 0 || kz >= kzn) continue;
+    V2<T>* base = s + (k1 * N2) * NC + kzl;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      V2<T> b[N2];
+#pragma unroll
+      for (int j = 0; j < N2; ++j) b[j] = base[j * NC + c * TK];
+      dft<T, N2, false>(b);
+#pragma unroll
+      for (int j = 0; j < N2; ++j) base[j * NC + c * TK] = b[j];
+    }
+    const double q3 = (double)kz * k.fz;
+#pragma unroll 4
+    for (int j = 0; j < N2; ++j) {  // mode kx = k1 + N1*j
+      V2<T> f[3], u[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) f[c] = base[j * NC + c * TK];
+      project_mode<T>(wavenumber(k1 + N1 * j, k.nx, k.fx), q2, q3, f, u, ie);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) base[j * NC + c * TK] = u[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      V2<T> b[N2];
+#pragma unroll
+      for (int j = 0; j < N2; ++j) b[j] = base[j * NC + c * TK];
+      dft<T, N2, true>(b);
+#pragma unroll
+      for (int j = 1; j < N2; ++j) b[j] = cmulc(b[j], ldt<T>(__ldg(&twN[j * k1])));
+#pragma unroll
+      for (int j = 0; j < N2; ++j) base[j * NC + c * TK] = b[j];
+    }
+  }
+  __syncthreads();
+  // inverse step over n1: shared memory -> registers -> spectrum
+  for (int i = threadIdx.x; i < N2 * NC; i += blockDim.x) {
+    const int col = i % NC, n2 = i / NC, kzl = col % TK, c = col / TK;
+    const int kz = k0 + kzl;
+    if (kz == 0 || kz >= kzn) continue;
+    V2<T> a[N1];
+#pragma unroll
+    for (int j = 0; j < N1; ++j) a[j] = s[(j * N2 + n2) * NC + col];
+    dft<T, N1, true>(a);
+    C* dst = spec + c * k.Gc + row + kzl;
+#pragma unroll
+    for (int j = 0; j < N1; ++j) {
+      C o;
+      o.x = a[j].x;
+      o.y = a[j].y;
+      dst[(long long)(j * N2 + n2) * xs] = o;
+    }
+  }
+}
+
 // Threads per CTA (a CTA sized to one pencil DFT per thread and step, 384 threads
 // at 256 points, measured slower than 256 threads).
 template <typename T, int N1, int N2, int TK, bool PLANES>
@@ -589,27 +686,33 @@ constexpr int xfft_block() {
 // CTAs per SM the register allocation must allow: three for the FP32 transforms up
 // to 256 points, fewer for the longer ones and for FP64, whose pencils need more
 // registers.
-template <typename T, int N, int BLOCK>
+template <typename T, int N, int BLOCK, bool PLANES>
 constexpr int xfft_min_blocks() {
   return sizeof(T) == 4 ? (N <= 256 ? 3 : 2) : (N <= 256 ? 2 : 1);
 }
 
 template <typename T, typename C, int N1, int N2, int TK, bool PLANES>
 __global__ void __launch_bounds__(xfft_block<T, N1, N2, TK, PLANES>(),
-                                  (xfft_min_blocks<T, N1 * N2, xfft_block<T, N1, N2, TK, PLANES>()>()))
+                                  (xfft_min_blocks<T, N1 * N2, xfft_block<T, N1, N2, TK, PLANES>(), PLANES>()))
     k_xfft_project(C* __restrict__ spec, KParams k, const C* __restrict__ twN) {
-  xfft_project_cta<T, C, N1, N2, TK, PLANES>(spec, k, twN);
+  if constexpr (PLANES || sizeof(T) == 8)
+    xfft_project_cta<T, C, N1, N2, TK, PLANES>(spec, k, twN);
+  else
+    xfft_interior_cta<T, C, N1, N2, TK>(spec, k, twN);
 }
 
 // Batched: blockIdx.z = member gidx[blockIdx.z] of a group of equal grids.
 template <typename T, typename C, int P, int N1, int N2, int TK, bool PLANES>
 __global__ void __launch_bounds__(xfft_block<T, N1, N2, TK, PLANES>(),
-                                  (xfft_min_blocks<T, N1 * N2, xfft_block<T, N1, N2, TK, PLANES>()>()))
+                                  (xfft_min_blocks<T, N1 * N2, xfft_block<T, N1, N2, TK, PLANES>(), PLANES>()))
     k_b_xfft_project(const BMember* __restrict__ mem, const int* __restrict__ gidx, int mask,
                      const C* __restrict__ twN) {
   const BMember& m = mem[gidx[blockIdx.z]];
   if (bskip(m, mask)) return;
-  xfft_project_cta<T, C, N1, N2, TK, PLANES>((C*)m.spec[P], m.kp, twN);
+  if constexpr (PLANES || sizeof(T) == 8)
+    xfft_project_cta<T, C, N1, N2, TK, PLANES>((C*)m.spec[P], m.kp, twN);
+  else
+    xfft_interior_cta<T, C, N1, N2, TK>((C*)m.spec[P], m.kp, twN);
 }
 
 }  // namespace
@@ -646,10 +749,13 @@ bool xfft_factor(int n, int* n1, int* n2) {
 
 namespace {
 
-// kz per interior CTA: shared memory N * (3 TK + 1) elements near 50 KB.
+// kz per interior CTA.  FP32 (xfft_interior_cta): shared memory N * 3 TK elements
+// near 100 KB (two CTAs per SM), TK * N1 threads busy in the middle step.  FP64
+// (xfft_project_cta, whose register-resident pencils of the one-step-per-barrier
+// form spill less): N * (3 TK + 1) elements near 50 KB.
 template <typename T>
 constexpr int xfft_tk(int n) {
-  return sizeof(T) == 4 ? (n <= 256 ? 8 : 4) : (n <= 128 ? 8 : (n <= 256 ? 4 : 2));
+  return sizeof(T) == 4 ? (n <= 256 ? 16 : 8) : (n <= 128 ? 8 : (n <= 256 ? 4 : 2));
 }
 
 template <typename K>
@@ -667,7 +773,7 @@ int xfft_run(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s, bool 
   constexpr int N = N1 * N2;
   constexpr int TK = xfft_tk<T>(N);
   constexpr int P = sizeof(T) == 8 ? 0 : 1;
-  const size_t smem_i = (size_t)N * (3 * TK + 1) * sizeof(C);
+  const size_t smem_i = (size_t)N * (3 * TK + (sizeof(T) == 8 ? 1 : 0)) * sizeof(C);
   const size_t smem_p = (size_t)N * 7 * sizeof(C);
   if (prepare) {
     FCM_TRY(xfft_smem_attr(k_xfft_project<T, C, N1, N2, TK, false>, smem_i));
