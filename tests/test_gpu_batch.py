@@ -70,3 +70,34 @@ def test_batch_refuses_bad_members(gpu):
     b = Batch([(p0, r0)])
     assert capi.load().fcm_destroy(b.members[0].h) != 0  # members belong to the batch
     b.close()
+
+
+def test_batch_long_x_grid_mixed_paths(gpu):
+    """Members with nx = 384, whose FP32 solves use the fused x-transform and whose
+    FP64 residuals the 3D transforms with k_b_project: batch steps follow single
+    steps (mixed precision, 1e-8)."""
+    from timstochrigidbodiessim_b200.params import FcmParams, rod_reference_positions
+    ref = np.array(rod_reference_positions(3, 2.2))
+    insts = []
+    for seed in (1, 2):
+        p = FcmParams.defaults(nx=384, ny=16, nz=16, ngauss=8, dx=0.5, num_bodies=8, blobs_per_body=3, ncells=3,
+                               potential=3, gmres_tol=1e-8, gmres_max_iter=100, precision=1, dt=0.01)
+        rng = np.random.default_rng(seed)
+        x = np.column_stack([20.0 * np.arange(8) + rng.uniform(0, 5, 8), rng.uniform(3, 5, 8),
+                             rng.uniform(3, 5, 8)]).ravel()
+        q = configs.random_unit_quaternions(rng, 8).ravel()
+        fe = np.zeros(48)
+        fe[2::6] = -1.0
+        insts.append((p, ref, x, q, fe))
+    solo = [_solo(*i) for i in insts]
+    b = _batch(insts)
+    for k in range(3):
+        infos = b.step([3, 4], k)
+        for i, s in enumerate(solo):
+            st, inf = s.step([3, 4][i], k)
+            assert st == 0 and infos[i].status == 0
+            assert abs(inf.gmres_iters - infos[i].gmres_iters) <= 1
+    for s, m in zip(solo, b.members):
+        assert np.max(np.abs(s.get_bodies()[0] - m.get_bodies()[0])) <= 1e-8
+        assert np.max(np.abs(s.get_bodies()[1] - m.get_bodies()[1])) <= 1e-8
+    b.close()

@@ -304,3 +304,24 @@ def test_device_pointers_through_the_abi(gpu, cfg0):
     g.apply_mobility(torch.tensor(F, device="cuda"), out=Vd)
     torch.cuda.synchronize()
     assert rel_err(Vd.cpu().numpy(), Vh) < 1e-13
+
+
+def test_mobility_parity_long_x_grid(gpu):
+    """nx = 384: the FP32 Stokes solve takes the fused x-transform, the FP64 one the
+    3D transforms (the fused kernel is used for FP64 only up to 256 points)."""
+    from timstochrigidbodiessim_b200.params import FcmParams
+    p = FcmParams.defaults(nx=384, ny=16, nz=16, ngauss=8, dx=0.5, num_bodies=24, blobs_per_body=1, ncells=3,
+                           precision=1)
+    rng = np.random.default_rng(4)
+    Y = (rng.uniform(0, 1, (24, 3)) * np.array([192.0, 8.0, 8.0])).ravel()
+    F = rng.standard_normal(72)
+    g, o = Suspension(p, [0, 0, 0]), Oracle(p.copy(precision=0), [0, 0, 0])
+    for s in (g, o):
+        s.set_up_gaussians(Y)
+    Vo = o.apply_mobility(F)
+    g.spread(F, 0)
+    g.stokes_solve(0)
+    assert rel_err(g.interp(0), Vo) < TOL
+    g.spread(F, 1)
+    g.stokes_solve(1)
+    assert rel_err(g.interp(1), Vo) < 1e-6

@@ -259,11 +259,15 @@ int fp32_stencil(const Ctx* c) {
 }
 
 // The fused x-transform path of the Stokes solve (stokes_t) when nx has a kernel
-// and nz is even: the twiddles exp(-2 pi i j / nx) of both precisions.
+// and nz is even -- for FP64 only up to 256 points, where it measured faster than
+// the 3D transforms (at 512^3 FP64 it was slower) -- and the twiddles
+// exp(-2 pi i j / nx) of both precisions.
 int setup_xfft(Ctx* c) {
   int n1 = 0, n2 = 0;
-  c->xfft = xfft_factor(c->g.nx, &n1, &n2) && c->g.nz % 2 == 0;
-  if (!c->xfft) return FCM_OK;
+  const bool ok = xfft_factor(c->g.nx, &n1, &n2) && c->g.nz % 2 == 0;
+  c->xfft[1] = ok;
+  c->xfft[0] = ok && c->g.nx <= 256;
+  if (!ok) return FCM_OK;
   FCM_TRY(xfft_tables_init());
   const int n = c->g.nx;
   const double PI = 3.14159265358979323846264338327950288;
@@ -297,7 +301,7 @@ int ensure_grid(Ctx* c) {
   FCM_CUFFT(cufftPlanMany(&gb.c2r, 3, n, nullptr, 1, (int)c->g.Gc, nullptr, 1, (int)c->g.G, c2r_type<T>(), 3));
   FCM_CUFFT(cufftSetStream(gb.r2c, c->stream));
   FCM_CUFFT(cufftSetStream(gb.c2r, c->stream));
-  if (c->xfft) {  // (y, z) transforms of the 3 nx planes of each component
+  if (c->xfft[sizeof(T) == 8 ? 0 : 1]) {  // (y, z) transforms of the 3 nx planes of each component
     int n2[2] = {c->g.ny, c->g.nz};
     const int planes = 3 * c->g.nx;
     FCM_CUFFT(cufftPlanMany(&gb.r2c2d, 2, n2, nullptr, 1, c->g.ny * c->g.nz, nullptr, 1, c->g.ny * c->g.nzh,
@@ -367,7 +371,7 @@ int spread_t(Ctx* c, const BlobTable<T>& t, const double* dF) {
 template <typename T>
 int stokes_t(Ctx* c) {
   GridBufs<T>& gb = grid_of<T>(c);
-  if (c->xfft) {  // (y, z) transforms, then x-transform + projection + inverse in one kernel
+  if (c->xfft[sizeof(T) == 8 ? 0 : 1]) {  // (y, z) transforms, then x + projection + inverse x
     FCM_CUFFT(exec_r2c(gb.r2c2d, gb.r, gb.c));
     FCM_TRY(launch_xfft_project<T>(*c, gb.c, c->stream));
     FCM_CUFFT(exec_c2r(gb.c2r2d, gb.c, gb.r));
@@ -2007,7 +2011,7 @@ int rehome_grids(Batch* B, int P) {
     int nn[3] = {grp.nx, grp.ny, grp.nz};
     FCM_CUFFT(cufftPlanMany(&grp.r2c[P], 3, nn, nullptr, 1, (int)G, nullptr, 1, (int)Gc, r2c_type<T>(), (int)(3 * k)));
     FCM_CUFFT(cufftPlanMany(&grp.c2r[P], 3, nn, nullptr, 1, (int)Gc, nullptr, 1, (int)G, c2r_type<T>(), (int)(3 * k)));
-    if (c0->xfft) {
+    if (c0->xfft[P]) {
       int n2[2] = {grp.ny, grp.nz};
       const int pz = grp.ny * grp.nz, pc = grp.ny * (grp.nz / 2 + 1), planes = (int)(3 * grp.nx * k);
       FCM_CUFFT(cufftPlanMany(&grp.r2c2d[P], 2, n2, nullptr, 1, pz, nullptr, 1, pc, r2c_type<T>(), planes));
@@ -2128,7 +2132,7 @@ int create_batch(int n, const fcm_params* params, const double* const* refs, Bat
     G.red_blocks = std::max(G.red_blocks, c->red_blocks);
     G.md_blocks = std::max(G.md_blocks, c->md_blocks);
     G.total_tiles += c->g64.blobs.ntiles;
-    if (!c->xfft) G.total_kblocks += (int)((c->g.Gc + 255) / 256);  // the fused path projects the others
+    if (!(c->xfft[0] && c->xfft[1])) G.total_kblocks += (int)((c->g.Gc + 255) / 256);  // k_b_project's share
   }
   G.max_sys_blocks = (int)((max_sys + 255) / 256);
   G.max_blob_blocks = (int)((max_Nb + 127) / 128);
@@ -2216,8 +2220,10 @@ int create_batch(int n, const fcm_params* params, const double* const* refs, Bat
     m.tg[1] = tile_geom(c->g, B->precision == 1 ? c->g32.blobs.W : c->g64.blobs.W);
     m.kp = make_kparams(*c);
     m.dx3 = c->g.dx * c->g.dx * c->g.dx;
+    m.xfft[0] = c->xfft[0] ? 1 : 0;
+    m.xfft[1] = c->xfft[1] ? 1 : 0;
     for (int t = 0; t < c->g64.blobs.ntiles; ++t) tmap.push_back(make_int2(i, t));
-    const int kb = c->xfft ? 0 : (int)((c->g.Gc + 255) / 256);
+    const int kb = (c->xfft[0] && c->xfft[1]) ? 0 : (int)((c->g.Gc + 255) / 256);
     for (int t = 0; t < kb; ++t) kmap.push_back(make_int2(i, t));
   }
   if (cudaMemcpy(B->d_mem, hm.data(), sizeof(BMember) * n, cudaMemcpyHostToDevice) != cudaSuccess ||

@@ -253,9 +253,10 @@ struct Ctx {
   double* d_dip = nullptr;
   // shear forcing (fcm_fluid_solver.hpp SHEARING_FORCES fields), allocated when
   // the imposed flow is produced: u_shear 3G (the grid layout of g64.r), Vshear 3Nb
-  // fused x-transform of the Stokes solve: on when nx is a supported length and nz
-  // is even; twiddles exp(-2 pi i j / nx), j < nx, as double2 and float2
-  bool xfft = false;
+  // fused x-transform of the Stokes solve, per grid precision ([0] FP64, [1] FP32):
+  // on when nx is a supported length and nz is even (FP64 up to 256 points, beyond
+  // which the 3D transforms are faster); twiddles exp(-2 pi i j / nx), j < nx
+  bool xfft[2] = {false, false};
   void* d_xtw64 = nullptr;
   void* d_xtw32 = nullptr;
   double* d_ushear = nullptr;
@@ -309,6 +310,7 @@ struct BMember {
   TileGeom tg[2];  // tile geometry of each precision's tables (their stencil widths differ)
   KParams kp;
   double dx3;
+  int xfft[2];  // the member's grids of each precision use the fused x-transform
 };
 
 // Which members a batched kernel works on.

@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(256, 4) k_b_project(const BMember* __restrict_
                                                       const int2* __restrict__ kblock_map, int mask) {
   const int2 mb = kblock_map[blockIdx.x];
   const BMember& m = mem[mb.x];
-  if (bskip(m, mask)) return;
+  if (bskip(m, mask) || m.xfft[P]) return;  // that precision's fused x-transform projects it
   project_one<T, C>((C*)m.spec[P], m.kp, (long long)mb.y * 256 + threadIdx.x);
 }
 
@@ -579,6 +579,93 @@ __device__ __forceinline__ void xfft_project_cta(C* __restrict__ spec, const KPa
   }
 }
 
+// Plane CTA: the kz = 0 (blockIdx.x = 0) or kz = nz/2 (blockIdx.x = 1) modes of PP
+// row pairs {y, -y}, y = blockIdx.y * PP + p <= ny/2.  Mode k of row y pairs with -k
+// of row -y (of the same row when y = -y), and one thread projects each {k, -k}
+// pair and writes both, symmetrised as in k_project.  Shared memory: pencils
+// [N][6 PP] (column (2 p + r) * 3 + c, r = 0 for y, 1 for -y) and the twiddles.
+template <typename T, typename C, int N1, int N2, int PP>
+__device__ __forceinline__ void xfft_planes_cta(C* __restrict__ spec, const KParams& k, const C* __restrict__ twN) {
+  constexpr int N = N1 * N2;
+  constexpr int NC = 6 * PP;
+  extern __shared__ __align__(16) unsigned char xfft_smem[];
+  V2<T>* s = reinterpret_cast<V2<T>*>(xfft_smem);
+  V2<T>* tw = s + N * NC;
+  const int h = k.ny / 2;
+  const int kz = blockIdx.x == 0 ? 0 : k.nz / 2;  // nz is even on this path
+  const int y0 = (int)blockIdx.y * PP;
+  const long long xs = (long long)k.ny * k.nzh;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = ldt<T>(twN[i]);
+  for (int i = threadIdx.x; i < N * NC; i += blockDim.x) {
+    const int col = i % NC, x = i / NC, c = col % 3, r = (col / 3) & 1, y = y0 + col / 6;
+    const int yr = r ? (k.ny - y) % k.ny : y;
+    const bool live = y <= h && !(r && yr == y);
+    s[x * NC + col] = live ? ldt<T>(spec[c * k.Gc + x * xs + (long long)yr * k.nzh + kz]) : V2<T>{(T)0, (T)0};
+  }
+  __syncthreads();
+  xpass_a<T, N1, N2, false>(s, tw, NC, NC);
+  __syncthreads();
+  xpass_b<T, N1, N2, false>(s, tw, NC, NC);
+  __syncthreads();
+  const T ie = (T)k.inv_etaG;
+  const double q3 = (double)kz * k.fz;
+  for (int i = threadIdx.x; i < N * PP; i += blockDim.x) {
+    const int pos = i % N, p = i / N, y = y0 + p;
+    if (y > h) continue;
+    const int yp = (k.ny - y) % k.ny;
+    const bool two = yp != y;
+    const int kx = pos / N2 + N1 * (pos % N2);
+    const int kxp = (k.nx - kx) % k.nx;
+    const int posp = (kxp % N1) * N2 + kxp / N1;
+    const int cb = 6 * p, pb = two ? 6 * p + 3 : cb;
+    if (kz == 0 && kx == 0 && y == 0) {  // f(0) = 0 and u(0) = 0
+#pragma unroll
+      for (int c = 0; c < 3; ++c) s[pos * NC + cb + c] = V2<T>{(T)0, (T)0};
+      continue;
+    }
+    if (!two && kxp < kx) continue;  // the partner's thread writes the pair
+    V2<T> f[3], u[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) f[c] = s[pos * NC + cb + c];
+    project_mode<T>(wavenumber(kx, k.nx, k.fx), wavenumber(y, k.ny, k.fy), q3, f, u, ie);
+    if (!two && kxp == kx) {  // self-conjugate mode
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        u[c].y = (T)0;
+        s[pos * NC + cb + c] = u[c];
+      }
+      continue;
+    }
+    V2<T> fp[3], up[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) fp[c] = s[posp * NC + pb + c];
+    project_mode<T>(wavenumber(kxp, k.nx, k.fx), wavenumber(yp, k.ny, k.fy), q3, fp, up, ie);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      V2<T> us;
+      us.x = (T)0.5 * (u[c].x + up[c].x);
+      us.y = (T)0.5 * (u[c].y - up[c].y);
+      s[pos * NC + cb + c] = us;
+      s[posp * NC + pb + c] = V2<T>{us.x, -us.y};
+    }
+  }
+  __syncthreads();
+  xpass_b<T, N1, N2, true>(s, tw, NC, NC);
+  __syncthreads();
+  xpass_a<T, N1, N2, true>(s, tw, NC, NC);
+  __syncthreads();
+  for (int i = threadIdx.x; i < N * NC; i += blockDim.x) {
+    const int col = i % NC, x = i / NC, c = col % 3, r = (col / 3) & 1, y = y0 + col / 6;
+    const int yr = r ? (k.ny - y) % k.ny : y;
+    if (y > h || (r && yr == y)) continue;
+    const V2<T> v = s[x * NC + col];
+    C o;
+    o.x = v.x;
+    o.y = v.y;
+    spec[c * k.Gc + x * xs + (long long)yr * k.nzh + kz] = o;
+  }
+}
+
 // Interior CTA (every kz of the chunk except the Hermitian planes): the step over
 // n1 reads its pencils straight from the spectrum into registers and writes the
 // transformed, twiddled values to shared memory [N][3 TK]; after one barrier each
@@ -590,7 +677,6 @@ __device__ __forceinline__ void xfft_project_cta(C* __restrict__ spec, const KPa
 template <typename T, typename C, int N1, int N2, int TK>
 __device__ __forceinline__ void xfft_interior_cta(C* __restrict__ spec, const KParams& k,
                                                   const C* __restrict__ twN) {
-  constexpr int N = N1 * N2;
   constexpr int NC = 3 * TK;
   extern __shared__ __align__(16) unsigned char xfft_smem[];
   V2<T>* s = reinterpret_cast<V2<T>*>(xfft_smem);
@@ -624,7 +710,7 @@ __device__ __forceinline__ void xfft_interior_cta(C* __restrict__ spec, const KP
     const int kz = k0 + kzl;
     if (kz == 0 || kz >= kzn) continue;
     V2<T>* base = s + (k1 * N2) * NC + kzl;
-#pragma unroll
+#pragma unroll 1
     for (int c = 0; c < 3; ++c) {
       V2<T> b[N2];
 #pragma unroll
@@ -643,7 +729,7 @@ __device__ __forceinline__ void xfft_interior_cta(C* __restrict__ spec, const KP
 #pragma unroll
       for (int c = 0; c < 3; ++c) base[j * NC + c * TK] = u[c];
     }
-#pragma unroll
+#pragma unroll 1
     for (int c = 0; c < 3; ++c) {
       V2<T> b[N2];
 #pragma unroll
@@ -676,11 +762,12 @@ __device__ __forceinline__ void xfft_interior_cta(C* __restrict__ spec, const KP
   }
 }
 
-// Threads per CTA (a CTA sized to one pencil DFT per thread and step, 384 threads
-// at 256 points, measured slower than 256 threads).
+// Threads per CTA: 256 (an FP32 CTA sized to one pencil DFT per thread and step,
+// 384 threads at 256 points, measured slower); 128 for the FP64 interior CTAs,
+// whose register-resident pencils take about 150 registers.
 template <typename T, int N1, int N2, int TK, bool PLANES>
 constexpr int xfft_block() {
-  return 256;
+  return (sizeof(T) == 8 && !PLANES && N1 * N2 <= 256) ? 128 : 256;
 }
 
 // CTAs per SM the register allocation must allow: three for the FP32 transforms up
@@ -695,8 +782,10 @@ template <typename T, typename C, int N1, int N2, int TK, bool PLANES>
 __global__ void __launch_bounds__(xfft_block<T, N1, N2, TK, PLANES>(),
                                   (xfft_min_blocks<T, N1 * N2, xfft_block<T, N1, N2, TK, PLANES>(), PLANES>()))
     k_xfft_project(C* __restrict__ spec, KParams k, const C* __restrict__ twN) {
-  if constexpr (PLANES || sizeof(T) == 8)
-    xfft_project_cta<T, C, N1, N2, TK, PLANES>(spec, k, twN);
+  if constexpr (PLANES)
+    xfft_planes_cta<T, C, N1, N2, TK>(spec, k, twN);
+  else if constexpr (sizeof(T) == 8 && N1 * N2 > 256)
+    xfft_project_cta<T, C, N1, N2, TK, false>(spec, k, twN);
   else
     xfft_interior_cta<T, C, N1, N2, TK>(spec, k, twN);
 }
@@ -709,8 +798,10 @@ __global__ void __launch_bounds__(xfft_block<T, N1, N2, TK, PLANES>(),
                      const C* __restrict__ twN) {
   const BMember& m = mem[gidx[blockIdx.z]];
   if (bskip(m, mask)) return;
-  if constexpr (PLANES || sizeof(T) == 8)
-    xfft_project_cta<T, C, N1, N2, TK, PLANES>((C*)m.spec[P], m.kp, twN);
+  if constexpr (PLANES)
+    xfft_planes_cta<T, C, N1, N2, TK>((C*)m.spec[P], m.kp, twN);
+  else if constexpr (sizeof(T) == 8 && N1 * N2 > 256)
+    xfft_project_cta<T, C, N1, N2, TK, false>((C*)m.spec[P], m.kp, twN);
   else
     xfft_interior_cta<T, C, N1, N2, TK>((C*)m.spec[P], m.kp, twN);
 }
@@ -749,13 +840,20 @@ bool xfft_factor(int n, int* n1, int* n2) {
 
 namespace {
 
-// kz per interior CTA.  FP32 (xfft_interior_cta): shared memory N * 3 TK elements
-// near 100 KB (two CTAs per SM), TK * N1 threads busy in the middle step.  FP64
-// (xfft_project_cta, whose register-resident pencils of the one-step-per-barrier
-// form spill less): N * (3 TK + 1) elements near 50 KB.
+// kz per interior CTA (xfft_interior_cta): shared memory N * 3 TK elements near
+// 100 KB (two CTAs per SM), TK * N1 threads busy in the middle step.  FP64 beyond
+// 256 points keeps the one-step-per-barrier form (xfft_project_cta, N * (3 TK + 1)
+// elements), whose pencils do not need all 255 registers.
 template <typename T>
 constexpr int xfft_tk(int n) {
-  return sizeof(T) == 4 ? (n <= 256 ? 16 : 8) : (n <= 128 ? 8 : (n <= 256 ? 4 : 2));
+  return sizeof(T) == 4 ? (n <= 256 ? 16 : 8) : (n <= 256 ? 8 : 2);
+}
+
+// Row pairs per plane CTA: one (ny/2 + 1 CTAs per plane; four pairs per CTA left
+// most SMs idle at 256 points and took twice as long).
+template <typename T>
+constexpr int xfft_pairs(int n) {
+  return 1;
 }
 
 template <typename K>
@@ -773,29 +871,31 @@ int xfft_run(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s, bool 
   constexpr int N = N1 * N2;
   constexpr int TK = xfft_tk<T>(N);
   constexpr int P = sizeof(T) == 8 ? 0 : 1;
-  const size_t smem_i = (size_t)N * (3 * TK + (sizeof(T) == 8 ? 1 : 0)) * sizeof(C);
-  const size_t smem_p = (size_t)N * 7 * sizeof(C);
+  constexpr int PP = xfft_pairs<T>(N);
+  const size_t smem_i = (size_t)N * (3 * TK + ((sizeof(T) == 8 && N > 256) ? 1 : 0)) * sizeof(C);
+  const size_t smem_p = (size_t)N * (6 * PP + 1) * sizeof(C);
   if (prepare) {
     FCM_TRY(xfft_smem_attr(k_xfft_project<T, C, N1, N2, TK, false>, smem_i));
-    FCM_TRY(xfft_smem_attr(k_xfft_project<T, C, N1, N2, 1, true>, smem_p));
+    FCM_TRY(xfft_smem_attr(k_xfft_project<T, C, N1, N2, PP, true>, smem_p));
     FCM_TRY(xfft_smem_attr(k_b_xfft_project<T, C, P, N1, N2, TK, false>, smem_i));
-    FCM_TRY(xfft_smem_attr(k_b_xfft_project<T, C, P, N1, N2, 1, true>, smem_p));
+    FCM_TRY(xfft_smem_attr(k_b_xfft_project<T, C, P, N1, N2, PP, true>, smem_p));
     return FCM_OK;
   }
   const C* tw = (const C*)(sizeof(T) == 4 ? c.d_xtw32 : c.d_xtw64);
   const int kzn = c.g.nz / 2;
   const unsigned nb = (unsigned)(b ? nm : 1);
-  const dim3 gi((unsigned)((kzn + TK - 1) / TK), (unsigned)c.g.ny, nb), gp(2u, (unsigned)c.g.ny, nb);
-  constexpr int BI = xfft_block<T, N1, N2, TK, false>(), BP = xfft_block<T, N1, N2, 1, true>();
+  const unsigned pair_ctas = (unsigned)((c.g.ny / 2 + 1 + PP - 1) / PP);
+  const dim3 gi((unsigned)((kzn + TK - 1) / TK), (unsigned)c.g.ny, nb), gp(2u, pair_ctas, nb);
+  constexpr int BI = xfft_block<T, N1, N2, TK, false>(), BP = xfft_block<T, N1, N2, PP, true>();
   if (b) {
     k_b_xfft_project<T, C, P, N1, N2, TK, false><<<gi, BI, smem_i, s>>>(b->mem, gidx, mask, tw);
     FCM_LAUNCH_CHECK();
-    k_b_xfft_project<T, C, P, N1, N2, 1, true><<<gp, BP, smem_p, s>>>(b->mem, gidx, mask, tw);
+    k_b_xfft_project<T, C, P, N1, N2, PP, true><<<gp, BP, smem_p, s>>>(b->mem, gidx, mask, tw);
   } else {
     const KParams k = make_kparams(c);
     k_xfft_project<T, C, N1, N2, TK, false><<<gi, BI, smem_i, s>>>(spec, k, tw);
     FCM_LAUNCH_CHECK();
-    k_xfft_project<T, C, N1, N2, 1, true><<<gp, BP, smem_p, s>>>(spec, k, tw);
+    k_xfft_project<T, C, N1, N2, PP, true><<<gp, BP, smem_p, s>>>(spec, k, tw);
   }
   FCM_LAUNCH_CHECK();
   return FCM_OK;
