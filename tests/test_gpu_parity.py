@@ -325,3 +325,26 @@ def test_mobility_parity_long_x_grid(gpu):
     g.spread(F, 1)
     g.stokes_solve(1)
     assert rel_err(g.interp(1), Vo) < 1e-6
+
+
+@pytest.mark.parametrize("shape", [(16, 16, 16), (32, 24, 16), (48, 64, 32), (96, 96, 96), (128, 64, 96)])
+def test_stokes_solve_both_precisions(gpu, shape):
+    """M F through the stage calls on both grids against the oracle: FP64 within
+    1e-10, FP32 within 1e-6 (relative, norm-wise).  These grids take the fused
+    x-transform in both precisions and, in FP32, the library's own (y, z)
+    transforms, with factors 2, 3, 4, 6, 8, 12, 16 and non-cubic shapes."""
+    from timstochrigidbodiessim_b200.params import FcmParams
+    nx, ny, nz = shape
+    p = FcmParams.defaults(nx=nx, ny=ny, nz=nz, ngauss=8, dx=1.0, num_bodies=20, blobs_per_body=1, ncells=3,
+                           precision=1)
+    rng = np.random.default_rng(2)
+    Y = (rng.uniform(0, 1, (20, 3)) * np.array([nx, ny, nz])).ravel()
+    F = rng.standard_normal(60)
+    g, o = Suspension(p, [0, 0, 0]), Oracle(p.copy(precision=0), [0, 0, 0])
+    for s in (g, o):
+        s.set_up_gaussians(Y)
+    Vo = o.apply_mobility(F)
+    for prec, tol in ((0, TOL), (1, 1e-6)):
+        g.spread(F, prec)
+        g.stokes_solve(prec)
+        assert rel_err(g.interp(prec), Vo) < tol, prec

@@ -285,6 +285,23 @@ int setup_xfft(Ctx* c) {
   c->d_xtw32 = d32;
   FCM_CUDA(cudaMemcpy(d64, wd.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
   FCM_CUDA(cudaMemcpy(d32, wf.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+  // FP32 (y, z) transforms by the library's kernels for nz up to 128, where they beat
+  // cuFFT's 2D plans (64^3, 96^3: the 64-suspension ensemble ran 11% faster); at
+  // 256^3 they measured even with cuFFT (373 against 364 us per solve) and cuFFT stays
+  c->yz32 = xfft_factor(c->g.ny, &n1, &n2) && xfft_factor(c->g.nz, &n1, &n2) && c->g.nz <= 128 &&
+            3 * c->g.nx <= 65535;
+  if (c->yz32) {
+    for (int d = 0; d < 2; ++d) {
+      const int m = d == 0 ? c->g.ny : c->g.nz;
+      std::vector<float2> w(m);
+      for (int j = 0; j < m; ++j)
+        w[j] = make_float2((float)std::cos(2.0 * PI * j / m), (float)-std::sin(2.0 * PI * j / m));
+      float2* dw = nullptr;
+      FCM_TRY(dev_alloc(&dw, (size_t)m));
+      (d == 0 ? c->d_ytw32 : c->d_ztw32) = dw;
+      FCM_CUDA(cudaMemcpy(dw, w.data(), sizeof(float2) * m, cudaMemcpyHostToDevice));
+    }
+  }
   return FCM_OK;
 }
 
@@ -372,6 +389,13 @@ template <typename T>
 int stokes_t(Ctx* c) {
   GridBufs<T>& gb = grid_of<T>(c);
   if (c->xfft[sizeof(T) == 8 ? 0 : 1]) {  // (y, z) transforms, then x + projection + inverse x
+    if constexpr (sizeof(T) == 4) {
+      if (c->yz32) {
+        FCM_TRY(launch_yz_forward(*c, gb.r, gb.c, 1, c->stream));
+        FCM_TRY(launch_xfft_project<T>(*c, gb.c, c->stream));
+        return launch_yz_inverse(*c, gb.c, gb.r, 1, c->stream);
+      }
+    }
     FCM_CUFFT(exec_r2c(gb.r2c2d, gb.r, gb.c));
     FCM_TRY(launch_xfft_project<T>(*c, gb.c, c->stream));
     FCM_CUFFT(exec_c2r(gb.c2r2d, gb.c, gb.r));
@@ -1140,6 +1164,8 @@ void destroy_ctx(Ctx* c) {
   cudaFree(c->d_dip);
   cudaFree(c->d_xtw64);
   cudaFree(c->d_xtw32);
+  cudaFree(c->d_ytw32);
+  cudaFree(c->d_ztw32);
   cudaFree(c->d_ushear);
   cudaFree(c->d_vshear);
   cudaFree(c->d_mcmc);
@@ -1783,14 +1809,25 @@ int batch_saddle(Batch* B, int in, int out, int mask, cudaStream_t s) {
   for (BatchGroup& g : B->groups) {
     const bool fused = g.r2c2d[P] != 0;
     any3d = any3d || !fused;
-    const cufftHandle h = fused ? g.r2c2d[P] : g.r2c[P];
-    FCM_CUFFT(cufftSetStream(h, s));
-    FCM_CUFFT(exec_r2c(h, (T*)g.r[P], (typename cplx_t<T>::type*)g.c[P]));
-    if (fused)
-      FCM_TRY(b_xfft_project<T>(B->geom, *B->m[g.idx[0]], g.d_gidx, (int)g.idx.size(), mask, s));
+    const Ctx& c0 = *B->m[g.idx[0]];
+    const int k = (int)g.idx.size();
+    if (P == 1 && fused && c0.yz32 && 3LL * c0.g.nx * k <= 65535) {  // the library's (y, z) transforms
+      FCM_TRY(launch_yz_forward(c0, (const float*)g.r[P], (cufftComplex*)g.c[P], k, s));
+    } else {
+      const cufftHandle h = fused ? g.r2c2d[P] : g.r2c[P];
+      FCM_CUFFT(cufftSetStream(h, s));
+      FCM_CUFFT(exec_r2c(h, (T*)g.r[P], (typename cplx_t<T>::type*)g.c[P]));
+    }
+    if (fused) FCM_TRY(b_xfft_project<T>(B->geom, c0, g.d_gidx, k, mask, s));
   }
   if (any3d) FCM_TRY(b_project<T>(B->geom, mask, s));  // members of the other groups
   for (BatchGroup& g : B->groups) {
+    const Ctx& c0 = *B->m[g.idx[0]];
+    const int k = (int)g.idx.size();
+    if (P == 1 && g.c2r2d[P] && c0.yz32 && 3LL * c0.g.nx * k <= 65535) {
+      FCM_TRY(launch_yz_inverse(c0, (cufftComplex*)g.c[P], (float*)g.r[P], k, s));
+      continue;
+    }
     const cufftHandle h = g.c2r2d[P] ? g.c2r2d[P] : g.c2r[P];
     FCM_CUFFT(cufftSetStream(h, s));
     FCM_CUFFT(exec_c2r(h, (typename cplx_t<T>::type*)g.c[P], (T*)g.r[P]));

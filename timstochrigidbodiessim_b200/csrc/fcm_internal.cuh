@@ -257,6 +257,12 @@ struct Ctx {
   // on when nx is a supported length and nz is even (FP64 up to 256 points, beyond
   // which the 3D transforms are faster); twiddles exp(-2 pi i j / nx), j < nx
   bool xfft[2] = {false, false};
+  // FP32 (y, z) transforms by this library's kernels instead of cuFFT's 2D plans
+  // (fused FP32 grids whose ny and nz are supported lengths, nz even, nz <= 128);
+  // twiddles exp(-2 pi i j / n) for n = ny, nz
+  bool yz32 = false;
+  void* d_ytw32 = nullptr;
+  void* d_ztw32 = nullptr;
   void* d_xtw64 = nullptr;
   void* d_xtw32 = nullptr;
   double* d_ushear = nullptr;
@@ -436,6 +442,9 @@ template <typename T>
 int xfft_prepare(const Ctx& c);
 template <typename T>
 int launch_xfft_project(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s);
+// the FP32 (y, z) transforms of `members` consecutive grids of c's shape (fcm_kspace.cu)
+int launch_yz_forward(const Ctx& c, const float* r, cufftComplex* spec, int members, cudaStream_t s);
+int launch_yz_inverse(const Ctx& c, cufftComplex* spec, float* r, int members, cudaStream_t s);
 // the same for the members gidx[0..nm) of a batch group whose grids equal c0's
 template <typename T>
 int b_xfft_project(const BatchGeom& b, const Ctx& c0, const int* gidx, int nm, int mask, cudaStream_t s);

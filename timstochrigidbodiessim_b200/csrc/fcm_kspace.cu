@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cmath>
 #include <mutex>
+#include <type_traits>
 
 #include "fcm_internal.cuh"
 
@@ -806,6 +807,206 @@ __global__ void __launch_bounds__(xfft_block<T, N1, N2, TK, PLANES>(),
     xfft_interior_cta<T, C, N1, N2, TK>((C*)m.spec[P], m.kp, twN);
 }
 
+// ------------------------------------------------------------------ (y, z) transforms
+// The (y, z) transforms around k_xfft_project for FP32 grids up to 128 points
+// along z, replacing cuFFT's R2C / C2R of every x-plane.  z: the real lines are taken two at a time as the
+// real and imaginary parts of one complex pencil (the DFTs of the two real lines
+// are (Z(k) + conj Z(-k))/2 and (Z(k) - conj Z(-k))/2i), transformed in two
+// register steps with one shared-memory exchange, and written as nz/2 + 1 modes per
+// line; the inverse assembles Z(k) = A(k) + i B(k) from the two half spectra,
+// ignoring the imaginary parts of A, B at kz = 0 and nz/2 as a C2R transform does.
+// y: one CTA per (x-plane, TK kz), the step over n1 straight from global memory,
+// the step over n2 straight back to it, one barrier between.  Unnormalised, with
+// cuFFT's sign convention.
+
+// padded shared-memory index of pencil position pos (one gap after every Z2)
+template <int Z2>
+__device__ __forceinline__ int zpad(int pos) {
+  return pos + pos / Z2;
+}
+
+template <int Z1, int Z2>
+__device__ __forceinline__ int zpos(int k) {  // position of mode k after the two steps
+  return (k % Z1) * Z2 + k / Z1;
+}
+
+template <typename T, typename C, int Z1, int Z2>
+__global__ void __launch_bounds__(256) k_zfft_r2c(const T* __restrict__ in, C* __restrict__ out, long long nlines,
+                                                  int nzh, const C* __restrict__ twZ) {
+  constexpr int N = Z1 * Z2;
+  constexpr int Q = 256 / Z2;        // complex pencils (two lines each) per CTA
+  constexpr int PS = Z1 * (Z2 + 1);  // padded pencil
+  extern __shared__ __align__(16) unsigned char zfft_smem[];
+  V2<T>* s = reinterpret_cast<V2<T>*>(zfft_smem);
+  const long long l0 = (long long)blockIdx.x * 2 * Q;
+  for (int i = threadIdx.x; i < Q * Z2; i += blockDim.x) {
+    const int p = i / Z2, n2 = i % Z2;
+    const long long la = l0 + 2 * p, lb = la + 1;
+    V2<T> a[Z1];
+#pragma unroll
+    for (int j = 0; j < Z1; ++j) {
+      const int z = j * Z2 + n2;
+      a[j].x = la < nlines ? in[la * N + z] : (T)0;
+      a[j].y = lb < nlines ? in[lb * N + z] : (T)0;
+    }
+    dft<T, Z1, false>(a);
+#pragma unroll
+    for (int j = 1; j < Z1; ++j) a[j] = cmul(a[j], ldt<T>(__ldg(&twZ[n2 * j])));
+#pragma unroll
+    for (int j = 0; j < Z1; ++j) s[p * PS + zpad<Z2>(j * Z2 + n2)] = a[j];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < Q * Z1; i += blockDim.x) {
+    const int p = i / Z1, k1 = i % Z1;
+    V2<T> b[Z2];
+#pragma unroll
+    for (int j = 0; j < Z2; ++j) b[j] = s[p * PS + zpad<Z2>(k1 * Z2 + j)];
+    dft<T, Z2, false>(b);
+#pragma unroll
+    for (int j = 0; j < Z2; ++j) s[p * PS + zpad<Z2>(k1 * Z2 + j)] = b[j];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < Q * nzh; i += blockDim.x) {
+    const int p = i / nzh, k = i % nzh;
+    const long long la = l0 + 2 * p, lb = la + 1;
+    const V2<T> zk = s[p * PS + zpad<Z2>(zpos<Z1, Z2>(k))];
+    const V2<T> zm = s[p * PS + zpad<Z2>(zpos<Z1, Z2>((N - k) % N))];
+    if (la < nlines) {
+      C o;
+      o.x = (T)0.5 * (zk.x + zm.x);
+      o.y = (T)0.5 * (zk.y - zm.y);
+      out[la * nzh + k] = o;
+    }
+    if (lb < nlines) {
+      C o;
+      o.x = (T)0.5 * (zk.y + zm.y);
+      o.y = (T)0.5 * (zm.x - zk.x);
+      out[lb * nzh + k] = o;
+    }
+  }
+}
+
+template <typename T, typename C, int Z1, int Z2>
+__global__ void __launch_bounds__(256) k_zfft_c2r(const C* __restrict__ in, T* __restrict__ out, long long nlines,
+                                                  int nzh, const C* __restrict__ twZ) {
+  constexpr int N = Z1 * Z2;
+  constexpr int Q = 256 / Z2;
+  constexpr int PS = Z1 * (Z2 + 1);
+  extern __shared__ __align__(16) unsigned char zfft_smem[];
+  V2<T>* s = reinterpret_cast<V2<T>*>(zfft_smem);
+  const long long l0 = (long long)blockIdx.x * 2 * Q;
+  for (int i = threadIdx.x; i < Q * nzh; i += blockDim.x) {
+    const int p = i / nzh, k = i % nzh;
+    const long long la = l0 + 2 * p, lb = la + 1;
+    V2<T> A = la < nlines ? ldt<T>(in[la * nzh + k]) : V2<T>{(T)0, (T)0};
+    V2<T> B = lb < nlines ? ldt<T>(in[lb * nzh + k]) : V2<T>{(T)0, (T)0};
+    if (k == 0 || 2 * k == N) {
+      A.y = (T)0;
+      B.y = (T)0;
+    }
+    s[p * PS + zpad<Z2>(zpos<Z1, Z2>(k))] = V2<T>{A.x - B.y, A.y + B.x};
+    if (k > 0 && 2 * k < N) s[p * PS + zpad<Z2>(zpos<Z1, Z2>(N - k))] = V2<T>{A.x + B.y, B.x - A.y};
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < Q * Z1; i += blockDim.x) {
+    const int p = i / Z1, k1 = i % Z1;
+    V2<T> b[Z2];
+#pragma unroll
+    for (int j = 0; j < Z2; ++j) b[j] = s[p * PS + zpad<Z2>(k1 * Z2 + j)];
+    dft<T, Z2, true>(b);
+#pragma unroll
+    for (int j = 1; j < Z2; ++j) b[j] = cmulc(b[j], ldt<T>(__ldg(&twZ[j * k1])));
+#pragma unroll
+    for (int j = 0; j < Z2; ++j) s[p * PS + zpad<Z2>(k1 * Z2 + j)] = b[j];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < Q * Z2; i += blockDim.x) {
+    const int p = i / Z2, n2 = i % Z2;
+    const long long la = l0 + 2 * p, lb = la + 1;
+    V2<T> a[Z1];
+#pragma unroll
+    for (int j = 0; j < Z1; ++j) a[j] = s[p * PS + zpad<Z2>(j * Z2 + n2)];
+    dft<T, Z1, true>(a);
+#pragma unroll
+    for (int j = 0; j < Z1; ++j) {
+      const int z = j * Z2 + n2;
+      if (la < nlines) out[la * N + z] = a[j].x;
+      if (lb < nlines) out[lb * N + z] = a[j].y;
+    }
+  }
+}
+
+// C2C along y, in place: blockIdx.y = x-plane (3 nx per grid), TK kz per CTA.
+template <typename T, typename C, int Y1, int Y2, int TK, bool INV>
+__global__ void __launch_bounds__(256) k_yfft(C* __restrict__ spec, int nzh, const C* __restrict__ twY) {
+  constexpr int NY = Y1 * Y2;
+  extern __shared__ __align__(16) unsigned char yfft_smem[];
+  V2<T>* s = reinterpret_cast<V2<T>*>(yfft_smem);  // [NY][TK]
+  const int k0 = (int)blockIdx.x * TK;
+  C* base = spec + (long long)blockIdx.y * NY * nzh + k0;
+  if (!INV) {
+    for (int i = threadIdx.x; i < Y2 * TK; i += blockDim.x) {
+      const int kzl = i % TK, n2 = i / TK;
+      const bool live = k0 + kzl < nzh;
+      V2<T> a[Y1];
+#pragma unroll
+      for (int j = 0; j < Y1; ++j)
+        a[j] = live ? ldt<T>(base[(long long)(j * Y2 + n2) * nzh + kzl]) : V2<T>{(T)0, (T)0};
+      dft<T, Y1, false>(a);
+#pragma unroll
+      for (int j = 1; j < Y1; ++j) a[j] = cmul(a[j], ldt<T>(__ldg(&twY[n2 * j])));
+#pragma unroll
+      for (int j = 0; j < Y1; ++j) s[(j * Y2 + n2) * TK + kzl] = a[j];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < Y1 * TK; i += blockDim.x) {
+      const int kzl = i % TK, k1 = i / TK;
+      if (k0 + kzl >= nzh) continue;
+      V2<T> b[Y2];
+#pragma unroll
+      for (int j = 0; j < Y2; ++j) b[j] = s[(k1 * Y2 + j) * TK + kzl];
+      dft<T, Y2, false>(b);
+#pragma unroll
+      for (int j = 0; j < Y2; ++j) {
+        C o;
+        o.x = b[j].x;
+        o.y = b[j].y;
+        base[(long long)(k1 + Y1 * j) * nzh + kzl] = o;
+      }
+    }
+  } else {
+    for (int i = threadIdx.x; i < Y1 * TK; i += blockDim.x) {
+      const int kzl = i % TK, k1 = i / TK;
+      const bool live = k0 + kzl < nzh;
+      V2<T> b[Y2];
+#pragma unroll
+      for (int j = 0; j < Y2; ++j)
+        b[j] = live ? ldt<T>(base[(long long)(k1 + Y1 * j) * nzh + kzl]) : V2<T>{(T)0, (T)0};
+      dft<T, Y2, true>(b);
+#pragma unroll
+      for (int j = 1; j < Y2; ++j) b[j] = cmulc(b[j], ldt<T>(__ldg(&twY[j * k1])));
+#pragma unroll
+      for (int j = 0; j < Y2; ++j) s[(k1 * Y2 + j) * TK + kzl] = b[j];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < Y2 * TK; i += blockDim.x) {
+      const int kzl = i % TK, n2 = i / TK;
+      if (k0 + kzl >= nzh) continue;
+      V2<T> a[Y1];
+#pragma unroll
+      for (int j = 0; j < Y1; ++j) a[j] = s[(j * Y2 + n2) * TK + kzl];
+      dft<T, Y1, true>(a);
+#pragma unroll
+      for (int j = 0; j < Y1; ++j) {
+        C o;
+        o.x = a[j].x;
+        o.y = a[j].y;
+        base[(long long)(j * Y2 + n2) * nzh + kzl] = o;
+      }
+    }
+  }
+}
+
 }  // namespace
 
 KParams make_kparams(const Ctx& c) {
@@ -946,6 +1147,88 @@ int xfft_tables_init() {
   FCM_CUDA(cudaMemcpyToSymbol(c_w96f, wf, sizeof(wf)));
   done[dev] = true;
   return FCM_OK;
+}
+
+namespace {
+
+// Calls f(integral_constant<N1>, integral_constant<N2>) for a supported length n.
+template <typename F>
+int with_factors(int n, F&& f) {
+  using std::integral_constant;
+  switch (n) {
+    case 8: return f(integral_constant<int, 2>{}, integral_constant<int, 4>{});
+    case 12: return f(integral_constant<int, 3>{}, integral_constant<int, 4>{});
+    case 16: return f(integral_constant<int, 4>{}, integral_constant<int, 4>{});
+    case 24: return f(integral_constant<int, 4>{}, integral_constant<int, 6>{});
+    case 32: return f(integral_constant<int, 4>{}, integral_constant<int, 8>{});
+    case 48: return f(integral_constant<int, 6>{}, integral_constant<int, 8>{});
+    case 64: return f(integral_constant<int, 8>{}, integral_constant<int, 8>{});
+    case 96: return f(integral_constant<int, 8>{}, integral_constant<int, 12>{});
+    case 128: return f(integral_constant<int, 8>{}, integral_constant<int, 16>{});
+    case 192: return f(integral_constant<int, 12>{}, integral_constant<int, 16>{});
+    case 256: return f(integral_constant<int, 16>{}, integral_constant<int, 16>{});
+    case 384: return f(integral_constant<int, 16>{}, integral_constant<int, 24>{});
+    case 512: return f(integral_constant<int, 16>{}, integral_constant<int, 32>{});
+    default: break;
+  }
+  set_error("(y, z) transforms: unsupported length " + std::to_string(n));
+  return FCM_ERR_INVALID;
+}
+
+template <typename T>
+int zfft(const Ctx& c, const T* r, typename cplx_t<T>::type* spec, T* r_out, long long nlines, bool inverse,
+         cudaStream_t s) {
+  using C = typename cplx_t<T>::type;
+  const C* tw = (const C*)c.d_ztw32;
+  const int nzh = c.g.nzh;
+  return with_factors(c.g.nz, [&](auto a, auto b) -> int {
+    constexpr int Z1 = decltype(a)::value, Z2 = decltype(b)::value;
+    constexpr int Q = 256 / Z2;
+    const size_t smem = (size_t)Q * Z1 * (Z2 + 1) * sizeof(C);
+    const unsigned grid = (unsigned)((nlines + 2 * Q - 1) / (2 * Q));
+    if (inverse)
+      k_zfft_c2r<T, C, Z1, Z2><<<grid, 256, smem, s>>>(spec, r_out, nlines, nzh, tw);
+    else
+      k_zfft_r2c<T, C, Z1, Z2><<<grid, 256, smem, s>>>(r, spec, nlines, nzh, tw);
+    FCM_LAUNCH_CHECK();
+    return (int)FCM_OK;
+  });
+}
+
+template <typename T>
+int yfft(const Ctx& c, typename cplx_t<T>::type* spec, int nplanes, bool inverse, cudaStream_t s) {
+  using C = typename cplx_t<T>::type;
+  const C* tw = (const C*)c.d_ytw32;
+  const int nzh = c.g.nzh;
+  return with_factors(c.g.ny, [&](auto a, auto b) -> int {
+    constexpr int Y1 = decltype(a)::value, Y2 = decltype(b)::value;
+    constexpr int TK = Y1 * Y2 <= 256 ? 16 : 8;
+    const size_t smem = (size_t)Y1 * Y2 * TK * sizeof(C);
+    const dim3 grid((unsigned)((nzh + TK - 1) / TK), (unsigned)nplanes);
+    if (inverse)
+      k_yfft<T, C, Y1, Y2, TK, true><<<grid, 256, smem, s>>>(spec, nzh, tw);
+    else
+      k_yfft<T, C, Y1, Y2, TK, false><<<grid, 256, smem, s>>>(spec, nzh, tw);
+    FCM_LAUNCH_CHECK();
+    return (int)FCM_OK;
+  });
+}
+
+}  // namespace
+
+// The (y, z) transforms of `members` consecutive FP32 grids of c's shape: forward
+// from the real grid r into the spectrum, inverse from the spectrum (overwritten)
+// into r.
+int launch_yz_forward(const Ctx& c, const float* r, cufftComplex* spec, int members, cudaStream_t s) {
+  const long long nlines = 3LL * c.g.nx * c.g.ny * members;
+  FCM_TRY(zfft<float>(c, r, spec, nullptr, nlines, false, s));
+  return yfft<float>(c, spec, 3 * c.g.nx * members, false, s);
+}
+
+int launch_yz_inverse(const Ctx& c, cufftComplex* spec, float* r, int members, cudaStream_t s) {
+  const long long nlines = 3LL * c.g.nx * c.g.ny * members;
+  FCM_TRY(yfft<float>(c, spec, 3 * c.g.nx * members, true, s));
+  return zfft<float>(c, nullptr, spec, r, nlines, true, s);
 }
 
 template <typename T>
