@@ -334,14 +334,14 @@ __global__ void k_fluct(C* __restrict__ spec, const cufftDoubleComplex* __restri
 
 // ------------------------------------------------------------------ fused x-transform
 // The Stokes solve of a force grid as 2D transforms over (y, z) for every x-plane
-// (cuFFT) with the transform along x, the projection and the inverse transform
-// along x fused into one kernel: each CTA holds the x-pencils of one y row and TK
-// consecutive kz (all three components) in shared memory, transforms them along x,
-// projects every mode and transforms back.  A 3D DFT is the x-DFT of the (y, z)
-// DFTs, so this is the transform pair of the 3D path with the projection between.
-// Pencils are transformed in two register-resident steps, N = N1 * N2 (both
-// divisors of 96 up to 32); in the chunks holding the kz = 0 and kz = nz/2 planes a
-// CTA takes the rows y and -y together and symmetrises each {k, -k} pair there.
+// (cuFFT, or the library's kernels further below) with the transform along x, the
+// projection and the inverse transform along x fused: interior CTAs take the
+// x-pencils of TK consecutive kz of one y row (all three components), transform
+// them along x, project every mode and transform back; plane CTAs do the same for
+// the kz = 0 and kz = nz/2 modes of a row pair {y, -y}, whose modes pair as
+// {k, -k}.  A 3D DFT is the x-DFT of the (y, z) DFTs, so this is the transform pair
+// of the 3D path with the projection between.  Pencils are transformed in two
+// register steps, N = N1 * N2 (both divisors of 96 up to 32).
 
 template <typename T, typename C>
 __device__ __forceinline__ V2<T> ldt(const C& v) {
@@ -467,116 +467,6 @@ __device__ __forceinline__ void xpass_b(V2<T>* __restrict__ s, const V2<T>* __re
     }
 #pragma unroll
     for (int j = 0; j < N2; ++j) s[(k1 * N2 + j) * NC + col] = b[j];
-  }
-}
-
-// Two kernels share this body.  Interior (PLANES false): one CTA per (TK kz, row y),
-// every kz except the Hermitian planes kz = 0 and nz/2, where modes have no
-// partner.  Planes (PLANES true, TK = 1): one CTA per (plane, {y, -y}): the mode
-// k pairs with -k of row -y, so the CTA of the smaller of y and -y takes both rows
-// and each {k, -k} pair is read and written by one thread, as in k_project (the
-// spectrum is updated in place).  Shared memory: pencils [N][NC] (column
-// (row*3 + c)*TK + kz_local) and the twiddles W_N^j.
-template <typename T, typename C, int N1, int N2, int TK, bool PLANES>
-__device__ __forceinline__ void xfft_project_cta(C* __restrict__ spec, const KParams& k, const C* __restrict__ twN) {
-  constexpr int N = N1 * N2;
-  constexpr int NC = (PLANES ? 6 : 3) * TK;
-  extern __shared__ __align__(16) unsigned char xfft_smem[];
-  V2<T>* s = reinterpret_cast<V2<T>*>(xfft_smem);
-  V2<T>* tw = s + N * NC;
-  const int y = blockIdx.y;
-  const int yp = (k.ny - y) % k.ny;
-  const int kzn = k.nz / 2;  // nz is even on this path
-  const int k0 = PLANES ? (blockIdx.x == 0 ? 0 : kzn) : (int)blockIdx.x * TK;
-  if (PLANES && yp < y) return;  // row y is done by the CTA of row yp
-  const int rows = (PLANES && yp != y) ? 2 : 1;
-  const int ncol = rows * 3 * TK;
-  const long long xs = (long long)k.ny * k.nzh;  // x stride of the spectrum
-  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = ldt<T>(twN[i]);
-  for (int i = threadIdx.x; i < N * ncol; i += blockDim.x) {
-    const int kzl = i % TK, rc = (i / TK) % (3 * rows), x = i / (TK * 3 * rows);
-    const int kz = k0 + kzl, c = rc % 3, yr = rc < 3 ? y : yp;
-    V2<T> v{(T)0, (T)0};
-    if (PLANES || (kz != 0 && kz < kzn)) v = ldt<T>(spec[c * k.Gc + x * xs + (long long)yr * k.nzh + kz]);
-    s[x * NC + rc * TK + kzl] = v;
-  }
-  __syncthreads();
-  xpass_a<T, N1, N2, false>(s, tw, ncol, NC);
-  __syncthreads();
-  xpass_b<T, N1, N2, false>(s, tw, ncol, NC);
-  __syncthreads();
-  // projection; position k1*N2 + k2 holds mode kx = k1 + N1*k2
-  const T ie = (T)k.inv_etaG;
-  for (int i = threadIdx.x; i < N * TK * rows; i += blockDim.x) {
-    const int kzl = i % TK, pos = (i / TK) % N, r = i / (TK * N);
-    const int kz = k0 + kzl;
-    if (!PLANES && (kz == 0 || kz >= kzn)) continue;
-    const int yr = r ? yp : y, ypr = r ? y : yp;
-    const int kx = pos / N2 + N1 * (pos % N2);
-    const double q1 = wavenumber(kx, k.nx, k.fx), q2 = wavenumber(yr, k.ny, k.fy), q3 = (double)kz * k.fz;
-    const int cb = 3 * r * TK + kzl;  // column of component 0 of this mode
-    V2<T> f[3], u[3];
-    if (!PLANES) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) f[c] = s[pos * NC + cb + c * TK];
-      project_mode<T>(q1, q2, q3, f, u, ie);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) s[pos * NC + cb + c * TK] = u[c];
-      continue;
-    }
-    if (kz == 0 && kx == 0 && yr == 0) {  // f(0) = 0 and u(0) = 0
-#pragma unroll
-      for (int c = 0; c < 3; ++c) s[pos * NC + cb + c * TK] = V2<T>{(T)0, (T)0};
-      continue;
-    }
-    const int kxp = (k.nx - kx) % k.nx;
-    const int posp = (kxp % N1) * N2 + kxp / N1;
-    int pb;  // column of the partner mode -k
-    if (rows == 2) {
-      if (r == 1) continue;  // row 0's thread writes the pair
-      pb = 3 * TK + kzl;
-    } else {
-      if (kxp < kx) continue;  // the partner's thread writes the pair
-      pb = cb;
-    }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) f[c] = s[pos * NC + cb + c * TK];
-    project_mode<T>(q1, q2, q3, f, u, ie);
-    if (rows == 1 && kxp == kx) {  // self-conjugate mode
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        u[c].y = (T)0;
-        s[pos * NC + cb + c * TK] = u[c];
-      }
-      continue;
-    }
-    V2<T> fp[3], up[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) fp[c] = s[posp * NC + pb + c * TK];
-    project_mode<T>(wavenumber(kxp, k.nx, k.fx), wavenumber(ypr, k.ny, k.fy), q3, fp, up, ie);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      V2<T> us;
-      us.x = (T)0.5 * (u[c].x + up[c].x);
-      us.y = (T)0.5 * (u[c].y - up[c].y);
-      s[pos * NC + cb + c * TK] = us;
-      s[posp * NC + pb + c * TK] = V2<T>{us.x, -us.y};
-    }
-  }
-  __syncthreads();
-  xpass_b<T, N1, N2, true>(s, tw, ncol, NC);
-  __syncthreads();
-  xpass_a<T, N1, N2, true>(s, tw, ncol, NC);
-  __syncthreads();
-  for (int i = threadIdx.x; i < N * ncol; i += blockDim.x) {
-    const int kzl = i % TK, rc = (i / TK) % (3 * rows), x = i / (TK * 3 * rows);
-    const int kz = k0 + kzl, c = rc % 3, yr = rc < 3 ? y : yp;
-    if (!PLANES && (kz == 0 || kz >= kzn)) continue;
-    const V2<T> v = s[x * NC + rc * TK + kzl];
-    C o;
-    o.x = v.x;
-    o.y = v.y;
-    spec[c * k.Gc + x * xs + (long long)yr * k.nzh + kz] = o;
   }
 }
 
@@ -785,8 +675,6 @@ __global__ void __launch_bounds__(xfft_block<T, N1, N2, TK, PLANES>(),
     k_xfft_project(C* __restrict__ spec, KParams k, const C* __restrict__ twN) {
   if constexpr (PLANES)
     xfft_planes_cta<T, C, N1, N2, TK>(spec, k, twN);
-  else if constexpr (sizeof(T) == 8 && N1 * N2 > 256)
-    xfft_project_cta<T, C, N1, N2, TK, false>(spec, k, twN);
   else
     xfft_interior_cta<T, C, N1, N2, TK>(spec, k, twN);
 }
@@ -801,8 +689,6 @@ __global__ void __launch_bounds__(xfft_block<T, N1, N2, TK, PLANES>(),
   if (bskip(m, mask)) return;
   if constexpr (PLANES)
     xfft_planes_cta<T, C, N1, N2, TK>((C*)m.spec[P], m.kp, twN);
-  else if constexpr (sizeof(T) == 8 && N1 * N2 > 256)
-    xfft_project_cta<T, C, N1, N2, TK, false>((C*)m.spec[P], m.kp, twN);
   else
     xfft_interior_cta<T, C, N1, N2, TK>((C*)m.spec[P], m.kp, twN);
 }
@@ -1041,13 +927,12 @@ bool xfft_factor(int n, int* n1, int* n2) {
 
 namespace {
 
-// kz per interior CTA (xfft_interior_cta): shared memory N * 3 TK elements near
-// 100 KB (two CTAs per SM), TK * N1 threads busy in the middle step.  FP64 beyond
-// 256 points keeps the one-step-per-barrier form (xfft_project_cta, N * (3 TK + 1)
-// elements), whose pencils do not need all 255 registers.
+// kz per interior CTA: shared memory N * 3 TK elements near 100 KB (two CTAs per
+// SM), TK * N1 threads busy in the middle step.  (FP64 grids beyond 256 points use
+// the 3D transforms instead.)
 template <typename T>
 constexpr int xfft_tk(int n) {
-  return sizeof(T) == 4 ? (n <= 256 ? 16 : 8) : (n <= 256 ? 8 : 2);
+  return sizeof(T) == 4 ? (n <= 256 ? 16 : 8) : 8;
 }
 
 // Row pairs per plane CTA: one (ny/2 + 1 CTAs per plane; four pairs per CTA left
@@ -1073,7 +958,7 @@ int xfft_run(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s, bool 
   constexpr int TK = xfft_tk<T>(N);
   constexpr int P = sizeof(T) == 8 ? 0 : 1;
   constexpr int PP = xfft_pairs<T>(N);
-  const size_t smem_i = (size_t)N * (3 * TK + ((sizeof(T) == 8 && N > 256) ? 1 : 0)) * sizeof(C);
+  const size_t smem_i = (size_t)N * 3 * TK * sizeof(C);
   const size_t smem_p = (size_t)N * (6 * PP + 1) * sizeof(C);
   if (prepare) {
     FCM_TRY(xfft_smem_attr(k_xfft_project<T, C, N1, N2, TK, false>, smem_i));
@@ -1117,8 +1002,12 @@ int xfft_dispatch(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s, 
     case 128: return xfft_run<T, 8, 16>(c, spec, s, prepare, b, gidx, nm, mask);
     case 192: return xfft_run<T, 12, 16>(c, spec, s, prepare, b, gidx, nm, mask);
     case 256: return xfft_run<T, 16, 16>(c, spec, s, prepare, b, gidx, nm, mask);
-    case 384: return xfft_run<T, 16, 24>(c, spec, s, prepare, b, gidx, nm, mask);
-    case 512: return xfft_run<T, 16, 32>(c, spec, s, prepare, b, gidx, nm, mask);
+    case 384:
+      if constexpr (sizeof(T) == 4) return xfft_run<T, 16, 24>(c, spec, s, prepare, b, gidx, nm, mask);
+      break;
+    case 512:
+      if constexpr (sizeof(T) == 4) return xfft_run<T, 16, 32>(c, spec, s, prepare, b, gidx, nm, mask);
+      break;
     default: break;
   }
   set_error("fused x-transform: unsupported length " + std::to_string(c.g.nx));
