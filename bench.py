@@ -471,14 +471,14 @@ def run_kernels_only(args):
 
 
 def run_ensemble(args):
-    """Batched ensemble of 64 independent suspensions (seeds 0..63).  Plain FP64
-    GPU path: the instances one after another on one stream, host-driven steps
-    (fcm_step).  Mixed-precision batched path: one fcm_batch of the 64 instances
-    (per-instance work as concurrent graph branches, the solves in lockstep as
-    batched kernels, one CUDA graph per step).  Also timed, for reference: FP64
+    """Ensemble of 64 independent suspensions (seeds 0..63).  Plain FP64 GPU path:
+    the instances one after another on one stream, host-driven steps (fcm_step).
+    Mixed-precision path (the line's value): the 64 instances as 64 contexts on 64
+    streams, one CUDA graph per instance step (fcm_step_many).  Also timed: FP64
     device-resident graph steps one instance after another, and the mixed
-    instances as 64 contexts on 64 streams (fcm_step_many).  Device time: events
-    on a root stream that every instance stream joins."""
+    instances as one fcm_batch (per-instance work as concurrent graph branches,
+    the solves in lockstep as batched kernels, one CUDA graph per step).  Device
+    time: events on a root stream that every instance stream joins."""
     os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")  # streams -> hardware queues
     from timstochrigidbodiessim_b200 import configs
     insts = configs.ensemble(64, workers=min(16, os.cpu_count() or 1))  # before any CUDA call
