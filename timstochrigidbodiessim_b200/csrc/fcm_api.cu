@@ -285,10 +285,10 @@ int setup_xfft(Ctx* c) {
   c->d_xtw32 = d32;
   FCM_CUDA(cudaMemcpy(d64, wd.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
   FCM_CUDA(cudaMemcpy(d32, wf.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
-  // FP32 (y, z) transforms by the library's kernels for nz up to 128, where they beat
-  // cuFFT's 2D plans (64^3, 96^3: the 64-suspension ensemble ran 11% faster); at
-  // 256^3 they measured even with cuFFT (373 against 364 us per solve) and cuFFT stays
-  c->yz32 = xfft_factor(c->g.ny, &n1, &n2) && xfft_factor(c->g.nz, &n1, &n2) && c->g.nz <= 128 &&
+  // FP32 (y, z) transforms by the library's kernels for nz up to 256, where they beat
+  // cuFFT's 2D plans (64^3, 96^3: the 64-suspension ensemble ran 11% faster; 256^3:
+  // 337 against 364 us per solve); longer z lines stay with cuFFT (not measured)
+  c->yz32 = xfft_factor(c->g.ny, &n1, &n2) && xfft_factor(c->g.nz, &n1, &n2) && c->g.nz <= 256 &&
             3 * c->g.nx <= 65535;
   if (c->yz32) {
     for (int d = 0; d < 2; ++d) {

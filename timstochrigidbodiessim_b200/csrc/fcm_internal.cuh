@@ -258,7 +258,7 @@ struct Ctx {
   // which the 3D transforms are faster); twiddles exp(-2 pi i j / nx), j < nx
   bool xfft[2] = {false, false};
   // FP32 (y, z) transforms by this library's kernels instead of cuFFT's 2D plans
-  // (fused FP32 grids whose ny and nz are supported lengths, nz even, nz <= 128);
+  // (fused FP32 grids whose ny and nz are supported lengths, nz even, nz <= 256);
   // twiddles exp(-2 pi i j / n) for n = ny, nz
   bool yz32 = false;
   void* d_ytw32 = nullptr;

@@ -694,7 +694,7 @@ __global__ void __launch_bounds__(xfft_block<T, N1, N2, TK, PLANES>(),
 }
 
 // ------------------------------------------------------------------ (y, z) transforms
-// The (y, z) transforms around k_xfft_project for FP32 grids up to 128 points
+// The (y, z) transforms around k_xfft_project for FP32 grids up to 256 points
 // along z, replacing cuFFT's R2C / C2R of every x-plane.  z: the real lines are taken two at a time as the
 // real and imaginary parts of one complex pencil (the DFTs of the two real lines
 // are (Z(k) + conj Z(-k))/2 and (Z(k) - conj Z(-k))/2i), transformed in two
@@ -781,17 +781,30 @@ __global__ void __launch_bounds__(256) k_zfft_c2r(const C* __restrict__ in, T* _
   extern __shared__ __align__(16) unsigned char zfft_smem[];
   V2<T>* s = reinterpret_cast<V2<T>*>(zfft_smem);
   const long long l0 = (long long)blockIdx.x * 2 * Q;
-  for (int i = threadIdx.x; i < Q * nzh; i += blockDim.x) {
-    const int p = i / nzh, k = i % nzh;
+  // all of a thread's half-spectrum values are loaded before any is stored
+  constexpr int NZH = N / 2 + 1, ITEMS = (Q * NZH + 255) / 256;
+  V2<T> A[ITEMS], B[ITEMS];
+#pragma unroll
+  for (int u = 0; u < ITEMS; ++u) {
+    const int i = threadIdx.x + 256 * u;
+    const int p = i / NZH, k = i % NZH;
     const long long la = l0 + 2 * p, lb = la + 1;
-    V2<T> A = la < nlines ? ldt<T>(in[la * nzh + k]) : V2<T>{(T)0, (T)0};
-    V2<T> B = lb < nlines ? ldt<T>(in[lb * nzh + k]) : V2<T>{(T)0, (T)0};
+    const bool live = i < Q * NZH;
+    A[u] = live && la < nlines ? ldt<T>(in[la * nzh + k]) : V2<T>{(T)0, (T)0};
+    B[u] = live && lb < nlines ? ldt<T>(in[lb * nzh + k]) : V2<T>{(T)0, (T)0};
+  }
+#pragma unroll
+  for (int u = 0; u < ITEMS; ++u) {
+    const int i = threadIdx.x + 256 * u;
+    if (i >= Q * NZH) break;
+    const int p = i / NZH, k = i % NZH;
+    V2<T> a = A[u], bb = B[u];
     if (k == 0 || 2 * k == N) {
-      A.y = (T)0;
-      B.y = (T)0;
+      a.y = (T)0;
+      bb.y = (T)0;
     }
-    s[p * PS + zpad<Z2>(zpos<Z1, Z2>(k))] = V2<T>{A.x - B.y, A.y + B.x};
-    if (k > 0 && 2 * k < N) s[p * PS + zpad<Z2>(zpos<Z1, Z2>(N - k))] = V2<T>{A.x + B.y, B.x - A.y};
+    s[p * PS + zpad<Z2>(zpos<Z1, Z2>(k))] = V2<T>{a.x - bb.y, a.y + bb.x};
+    if (k > 0 && 2 * k < N) s[p * PS + zpad<Z2>(zpos<Z1, Z2>(N - k))] = V2<T>{a.x + bb.y, bb.x - a.y};
   }
   __syncthreads();
   for (int i = threadIdx.x; i < Q * Z1; i += blockDim.x) {
