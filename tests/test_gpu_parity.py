@@ -327,12 +327,15 @@ def test_mobility_parity_long_x_grid(gpu):
     assert rel_err(g.interp(1), Vo) < 1e-6
 
 
-@pytest.mark.parametrize("shape", [(16, 16, 16), (32, 24, 16), (48, 64, 32), (96, 96, 96), (128, 64, 96)])
+@pytest.mark.parametrize("shape", [(16, 16, 16), (32, 24, 16), (48, 64, 32), (96, 96, 96), (128, 64, 96),
+                                   (24, 128, 128), (16, 192, 192), (12, 256, 256)])
 def test_stokes_solve_both_precisions(gpu, shape):
     """M F through the stage calls on both grids against the oracle: FP64 within
     1e-10, FP32 within 1e-6 (relative, norm-wise).  These grids take the fused
     x-transform in both precisions and, in FP32, the library's own (y, z)
-    transforms, with factors 2, 3, 4, 6, 8, 12, 16 and non-cubic shapes."""
+    transforms, with factors 2, 3, 4, 6, 8, 12, 16 and non-cubic shapes: square
+    (y, z) planes up to 96 points by one CTA per plane, the others (and the
+    square 128, 192, 256-point planes) by separate z and y passes."""
     from timstochrigidbodiessim_b200.params import FcmParams
     nx, ny, nz = shape
     p = FcmParams.defaults(nx=nx, ny=ny, nz=nz, ngauss=8, dx=1.0, num_bodies=20, blobs_per_body=1, ncells=3,
