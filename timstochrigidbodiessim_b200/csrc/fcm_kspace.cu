@@ -718,7 +718,7 @@ __device__ __forceinline__ int zpos(int k) {  // position of mode k after the tw
 
 template <typename T, typename C, int Z1, int Z2>
 __global__ void __launch_bounds__(256) k_zfft_r2c(const T* __restrict__ in, C* __restrict__ out, long long nlines,
-                                                  int nzh, const C* __restrict__ twZ) {
+                                                  const C* __restrict__ twZ) {
   constexpr int N = Z1 * Z2;
   constexpr int Q = 256 / Z2;        // complex pencils (two lines each) per CTA
   constexpr int PS = Z1 * (Z2 + 1);  // padded pencil
@@ -752,8 +752,9 @@ __global__ void __launch_bounds__(256) k_zfft_r2c(const T* __restrict__ in, C* _
     for (int j = 0; j < Z2; ++j) s[p * PS + zpad<Z2>(k1 * Z2 + j)] = b[j];
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < Q * nzh; i += blockDim.x) {
-    const int p = i / nzh, k = i % nzh;
+  constexpr int NZH = N / 2 + 1;  // the spectrum's row length (nzh); a constant divisor below
+  for (int i = threadIdx.x; i < Q * NZH; i += blockDim.x) {
+    const int p = i / NZH, k = i % NZH;
     const long long la = l0 + 2 * p, lb = la + 1;
     const V2<T> zk = s[p * PS + zpad<Z2>(zpos<Z1, Z2>(k))];
     const V2<T> zm = s[p * PS + zpad<Z2>(zpos<Z1, Z2>((N - k) % N))];
@@ -761,20 +762,20 @@ __global__ void __launch_bounds__(256) k_zfft_r2c(const T* __restrict__ in, C* _
       C o;
       o.x = (T)0.5 * (zk.x + zm.x);
       o.y = (T)0.5 * (zk.y - zm.y);
-      out[la * nzh + k] = o;
+      out[la * NZH + k] = o;
     }
     if (lb < nlines) {
       C o;
       o.x = (T)0.5 * (zk.y + zm.y);
       o.y = (T)0.5 * (zm.x - zk.x);
-      out[lb * nzh + k] = o;
+      out[lb * NZH + k] = o;
     }
   }
 }
 
 template <typename T, typename C, int Z1, int Z2>
 __global__ void __launch_bounds__(256) k_zfft_c2r(const C* __restrict__ in, T* __restrict__ out, long long nlines,
-                                                  int nzh, const C* __restrict__ twZ) {
+                                                  const C* __restrict__ twZ) {
   constexpr int N = Z1 * Z2;
   constexpr int Q = 256 / Z2;
   constexpr int PS = Z1 * (Z2 + 1);
@@ -790,8 +791,8 @@ __global__ void __launch_bounds__(256) k_zfft_c2r(const C* __restrict__ in, T* _
     const int p = i / NZH, k = i % NZH;
     const long long la = l0 + 2 * p, lb = la + 1;
     const bool live = i < Q * NZH;
-    A[u] = live && la < nlines ? ldt<T>(in[la * nzh + k]) : V2<T>{(T)0, (T)0};
-    B[u] = live && lb < nlines ? ldt<T>(in[lb * nzh + k]) : V2<T>{(T)0, (T)0};
+    A[u] = live && la < nlines ? ldt<T>(in[la * NZH + k]) : V2<T>{(T)0, (T)0};
+    B[u] = live && lb < nlines ? ldt<T>(in[lb * NZH + k]) : V2<T>{(T)0, (T)0};
   }
 #pragma unroll
   for (int u = 0; u < ITEMS; ++u) {
@@ -1256,16 +1257,15 @@ int zfft(const Ctx& c, const T* r, typename cplx_t<T>::type* spec, T* r_out, lon
          cudaStream_t s) {
   using C = typename cplx_t<T>::type;
   const C* tw = (const C*)c.d_ztw32;
-  const int nzh = c.g.nzh;
   return with_factors(c.g.nz, [&](auto a, auto b) -> int {
     constexpr int Z1 = decltype(a)::value, Z2 = decltype(b)::value;
     constexpr int Q = 256 / Z2;
     const size_t smem = (size_t)Q * Z1 * (Z2 + 1) * sizeof(C);
     const unsigned grid = (unsigned)((nlines + 2 * Q - 1) / (2 * Q));
     if (inverse)
-      k_zfft_c2r<T, C, Z1, Z2><<<grid, 256, smem, s>>>(spec, r_out, nlines, nzh, tw);
+      k_zfft_c2r<T, C, Z1, Z2><<<grid, 256, smem, s>>>(spec, r_out, nlines, tw);
     else
-      k_zfft_r2c<T, C, Z1, Z2><<<grid, 256, smem, s>>>(r, spec, nlines, nzh, tw);
+      k_zfft_r2c<T, C, Z1, Z2><<<grid, 256, smem, s>>>(r, spec, nlines, tw);
     FCM_LAUNCH_CHECK();
     return (int)FCM_OK;
   });
