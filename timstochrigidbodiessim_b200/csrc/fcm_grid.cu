@@ -234,12 +234,53 @@ __device__ __forceinline__ void spread_tile(const T* __restrict__ wc, const doub
   const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
   const int t = threadIdx.x;
   const int z = t & 7, y = t >> 3, yh = t >> 5;
+  const int b0 = offset[tile], b1 = offset[tile + 1];
+  if constexpr (sizeof(T) == 4) {
+    // FP32: the x-points in pairs, one packed two-lane FMA (fma.rn.f32x2) per pair
+    // and component; each lane rounds as the scalar FMA does, so the sums are the
+    // same bit for bit.
+    float2 acc2[TE / 2][3];
+#pragma unroll
+    for (int x = 0; x < TE / 2; ++x)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) acc2[x][c] = make_float2(0.f, 0.f);
+    for (int c0 = b0; c0 < b1; c0 += SCB) {
+      const int nc = min(SCB, b1 - c0);
+      if (c0 != b0) __syncthreads();
+      stage_blobs<T>(list, c0, nc, wc, F, sw, sF, sflag);
+      __syncthreads();
+      for (int k = 0; k < nc; ++k) {
+        const unsigned fl = sflag[k];
+        if (!((fl >> (EYM + yh)) & 1u)) continue;
+        const float wyz = sw[k][1][y] * sw[k][2][z];
+        const float f0 = sF[k][0] * wyz, f1 = sF[k][1] * wyz, f2 = sF[k][2] * wyz;
+        const float2 fc[3] = {make_float2(f0, f0), make_float2(f1, f1), make_float2(f2, f2)};
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const float4 v = *reinterpret_cast<const float4*>(&sw[k][0][4 * h]);
+          const float2 wa = make_float2(v.x, v.y), wb = make_float2(v.z, v.w);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            acc2[2 * h][c] = __ffma2_rn(fc[c], wa, acc2[2 * h][c]);
+            acc2[2 * h + 1][c] = __ffma2_rn(fc[c], wb, acc2[2 * h + 1][c]);
+          }
+        }
+      }
+    }
+    const int ox = tx * TE, oy = ty * TE + y, oz = tz * TE + z;
+#pragma unroll
+    for (int x = 0; x < TE; ++x) {
+      const long long idx = ((long long)(ox + x) * g.ny + oy) * g.nz + oz;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) grid[c * G + idx] = (x & 1) ? acc2[x >> 1][c].y : acc2[x >> 1][c].x;
+    }
+    return;
+  }
   T acc[TE][3];
 #pragma unroll
   for (int x = 0; x < TE; ++x)
 #pragma unroll
     for (int c = 0; c < 3; ++c) acc[x][c] = 0;
-  const int b0 = offset[tile], b1 = offset[tile + 1];
   for (int c0 = b0; c0 < b1; c0 += SCB) {
     const int nc = min(SCB, b1 - c0);
     if (c0 != b0) __syncthreads();
