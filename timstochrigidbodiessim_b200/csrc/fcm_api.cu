@@ -287,7 +287,9 @@ int setup_xfft(Ctx* c) {
   FCM_CUDA(cudaMemcpy(d32, wf.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
   // FP32 (y, z) transforms by the library's kernels for nz up to 256, where they beat
   // cuFFT's 2D plans (64^3, 96^3: the 64-suspension ensemble ran 11% faster; 256^3:
-  // 337 against 364 us per solve); longer z lines stay with cuFFT (not measured)
+  // 328 against 364 us per solve); at 512^3 they took 3324 against 3201 us (z passes
+  // 732 + 736 against 919 + 958 us, y passes 783 + 1074 against 662 + 662 us), so
+  // longer lines stay with cuFFT
   c->yz32 = xfft_factor(c->g.ny, &n1, &n2) && xfft_factor(c->g.nz, &n1, &n2) && c->g.nz <= 256 &&
             3 * c->g.nx <= 65535;
   if (c->yz32) {
