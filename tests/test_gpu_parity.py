@@ -328,7 +328,7 @@ def test_mobility_parity_long_x_grid(gpu):
 
 
 @pytest.mark.parametrize("shape", [(16, 16, 16), (32, 24, 16), (48, 64, 32), (96, 96, 96), (128, 64, 96),
-                                   (24, 128, 128), (16, 192, 192), (12, 256, 256)])
+                                   (24, 128, 128), (16, 192, 192), (12, 256, 256), (256, 16, 32)])
 def test_stokes_solve_both_precisions(gpu, shape):
     """M F through the stage calls on both grids against the oracle: FP64 within
     1e-10, FP32 within 1e-6 (relative, norm-wise).  These grids take the fused
