@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--workload", default="rods2048_phi0.10_g256")
     ap.add_argument("--algorithm", default="em", choices=["em", "gdc"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default kernel variants instead of fcm_autotune's choice")
     ap.add_argument("--ens-modes", default="fp64,fp64_graph,mixed_batch,mixed",
                     help="ensemble arms to time (the JSON line needs fp64, fp64_graph and mixed)")
     ap.add_argument("--nvtx", action="store_true", help="mark the timed region with an NVTX range 'timed'")
@@ -133,12 +135,29 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------- ours
+VARIANT_LEGEND = ("variants [FP64 spread, FP64 solve, FP32 spread, FP32 solve]: spread 0 persistent pipelined, "
+                  "1 one CTA per tile; solve 0 cuFFT 3D + projection, 1 cuFFT (y, z) + fused x-transform, "
+                  "2 library (y, z) + fused x-transform.  us[5P + v]: precision P, v 0-1 spread, 2-4 solve "
+                  "variants, microseconds per call, -1 not available")
+
+AUTOTUNE = {"on": True}
+
+
 def setup_suspension(p, ref, x, q, fe, stream):
+    """A context for the workload; unless --no-autotune, its kernel variants are
+    chosen by fcm_autotune on the start configuration (untimed; s.tuning holds the
+    variants and the microseconds per call of each candidate)."""
     from timstochrigidbodiessim_b200.fcm import Suspension
     s = Suspension(p, ref, stream=stream)
     s.set_bodies(x, q)
     s.set_external_forces(fe)
     s.produce_reference_matrices()
+    s.tuning = None
+    if AUTOTUNE["on"]:
+        s.fill_all_blob_pos()
+        s.set_up_gaussians()
+        v, us = s.autotune(reps=3)
+        s.tuning = {"variants": v, "us": [round(float(t), 1) for t in us]}
     return s
 
 
@@ -306,7 +325,7 @@ def run_ours(args):
         t = max_over_ranks(t)
         if world > 1:
             dist.barrier()
-        results[tag] = dict(t=t, iters=float(np.mean(iters)), launches=l1 - l0, clocks=clocks, s=s)
+        results[tag] = dict(t=t, iters=float(np.mean(iters)), launches=l1 - l0, clocks=clocks, s=s, tuning=s.tuning)
     # rooflines of the spread / interpolation kernels on the FP32 grid (the mixed
     # path's) and the FP64 grid
     kr = {"fp32": kernel_roofline(results["mixed"]["s"], p, stream, 1),
@@ -369,7 +388,9 @@ def run_ours(args):
                        "grid": [p.nx, p.ny, p.nz], "box": p.box[0], "algorithm": args.algorithm,
                        "gmres_tol": p.gmres_tol, "parallelism": "replicas x%d" % world,
                        "l2": "grid fields (3x%d^3) exceed L2; no flush needed" % p.nx,
-                       "mcmc_equilibration": mcmc},
+                       "mcmc_equilibration": mcmc,
+                       "kernel_variants": {"legend": VARIANT_LEGEND, "fp64": results["fp64"]["tuning"],
+                                           "mixed": results["mixed"]["tuning"]}},
             "fp64": {"value": fp64_value, "ms_per_step": 1e3 * results["fp64"]["t"] / K,
                      "gmres_iters": results["fp64"]["iters"], "mode": "host-driven fcm_step"},
             "fp64_graph": {"value": fp64g_value, "ms_per_step": 1e3 * results["fp64_graph"]["t"] / K,
@@ -568,8 +589,14 @@ def run_ensemble(args):
             torch.cuda.nvtx.range_pop()
         clocks = sampler.stop() if tag == "mixed" else None
         t = e0.elapsed_time(e1) / 1e3
+        tunings = {}
+        for s in ([] if batch is not None else ss):
+            if s.tuning is not None:
+                key = str(s.tuning["variants"])
+                tunings[key] = tunings.get(key, 0) + 1
         res[tag] = dict(t=t, iters=float(np.mean(iters)), launches=lib.fcm_kernel_launch_count() - l0,
-                        clocks=clocks, rounds=[float(np.mean([r[i] for r in rounds])) for i in (0, 1)] if rounds else None)
+                        clocks=clocks, rounds=[float(np.mean([r[i] for r in rounds])) for i in (0, 1)] if rounds else None,
+                        tunings=tunings or None)
         if batch is not None:
             batch.close()
         else:
@@ -592,7 +619,9 @@ def run_ensemble(args):
         "config": {"workload": "ensemble64_rods50-500_g64-128", "instances": len(insts), "bodies": total_bodies,
                    "grids": grids, "gmres_tol_fp64": insts[0][0].gmres_tol, "mixed_gmres_tol": MIXED_TOL,
                    "seeds": "0..63",
-                   "parallelism": "64 contexts on 64 streams, one CUDA graph per instance step (fcm_step_many)"},
+                   "parallelism": "64 contexts on 64 streams, one CUDA graph per instance step (fcm_step_many)",
+                   "kernel_variants": {"legend": VARIANT_LEGEND, "members_per_choice": {
+                       k: res[k]["tunings"] for k in ("fp64", "mixed") if k in res}}},
         "fp64": {"value": fp64, "ms_per_step": 1e3 * res["fp64"]["t"] / args.steps, "gmres_iters": res["fp64"]["iters"],
                  "mode": "instances one after another, host-driven fcm_step"},
         "fp64_graph": {"value": fp64g, "ms_per_step": 1e3 * res["fp64_graph"]["t"] / args.steps,
@@ -614,6 +643,7 @@ def run_ensemble(args):
 def main():
     global MIXED_TOL
     args = parse()
+    AUTOTUNE["on"] = not args.no_autotune
     if args.mixed_tol:
         MIXED_TOL = args.mixed_tol
     if args.workload.startswith("ensemble"):

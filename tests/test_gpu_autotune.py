@@ -1,0 +1,86 @@
+"""Kernel variants of the grid stages and their autotuner (no reference
+counterpart).  The two spread kernels sum every grid point's blobs in the same
+order, so M F is the same bit for bit whichever runs; the Stokes-solve variants
+(cuFFT 3D + projection, cuFFT (y, z) + fused x-transform, the library's (y, z)
+kernels + fused x-transform) agree with the oracle within 1e-10 (FP64) and 1e-6
+(FP32) relative.  fcm_autotune times what the grid allows, keeps the fastest by
+its own timings, and the results after tuning still match the oracle."""
+import numpy as np
+import pytest
+
+from tests.conftest import rel_err
+from tests.oracle_lib import Oracle
+from timstochrigidbodiessim_b200.capi import FcmError
+from timstochrigidbodiessim_b200.fcm import Suspension
+from timstochrigidbodiessim_b200.params import FcmParams
+
+pytestmark = pytest.mark.gpu
+
+TOL = {0: 1e-10, 1: 1e-6}
+
+
+def _setup(n=(64, 64, 64), nbodies=40):
+    nx, ny, nz = n
+    p = FcmParams.defaults(nx=nx, ny=ny, nz=nz, ngauss=12, dx=1.0, num_bodies=nbodies, blobs_per_body=1, ncells=3,
+                           precision=1)
+    rng = np.random.default_rng(3)
+    Y = (rng.uniform(0, 1, (nbodies, 3)) * np.array([nx, ny, nz])).ravel()
+    F = rng.standard_normal(3 * nbodies)
+    g, o = Suspension(p, [0, 0, 0]), Oracle(p.copy(precision=0), [0, 0, 0])
+    for s in (g, o):
+        s.set_up_gaussians(Y)
+    return g, o.apply_mobility(F), F
+
+
+def _mf(g, F, prec):
+    g.spread(F, prec)
+    g.stokes_solve(prec)
+    return g.interp(prec)
+
+
+def test_variants_agree(gpu):
+    g, Vo, F = _setup()
+    assert g.get_variants() == [0, 1, 1, 2]  # the defaults on a 64^3 grid
+    for prec in (0, 1):
+        for sv in ((0, 1) if prec == 0 else (0, 1, 2)):
+            out = []
+            for sp in (0, 1):
+                v = g.get_variants()
+                v[2 * prec], v[2 * prec + 1] = sp, sv
+                g.set_variants(v)
+                out.append(_mf(g, F, prec))
+            assert np.array_equal(out[0], out[1]), (prec, sv)
+            assert rel_err(out[0], Vo) < TOL[prec], (prec, sv)
+
+
+def test_autotune_keeps_the_fastest(gpu):
+    g, Vo, F = _setup()
+    v, us = g.autotune(reps=3)
+    assert np.all(us[[0, 1, 2, 3]] > 0) and us[4] == -1  # FP64 has no library (y, z) variant
+    assert np.all(us[5:10] > 0)
+    for P in (0, 1):
+        spread, solve = us[5 * P:5 * P + 2], us[5 * P + 2:5 * P + 5]
+        assert v[2 * P] == (0 if spread[0] <= spread[1] else 1)
+        best = min((t, i) for i, t in enumerate(solve) if t >= 0)[1]
+        assert v[2 * P + 1] == best
+    assert g.get_variants() == v
+    for prec in (0, 1):
+        assert rel_err(_mf(g, F, prec), Vo) < TOL[prec], prec
+
+
+def test_variants_refused_where_the_grid_does_not_allow_them(gpu):
+    g, _, _ = _setup()
+    with pytest.raises(FcmError):
+        g.set_variants([0, 2, 1, 2])  # no library (y, z) variant in FP64
+    with pytest.raises(FcmError):
+        g.set_variants([2, 1, 1, 2])  # out of range
+    # 20 points along x: no fused x-transform, so only the 3D solve
+    h, Vo, F = _setup((20, 24, 16), nbodies=12)
+    assert h.get_variants()[1] == 0 and h.get_variants()[3] == 0
+    with pytest.raises(FcmError):
+        h.set_variants([0, 1, 1, 0])
+    v, us = h.autotune(reps=2)
+    assert us[3] == -1 and us[8] == -1 and us[9] == -1
+    assert v[1] == 0 and v[3] == 0
+    for prec in (0, 1):
+        assert rel_err(_mf(h, F, prec), Vo) < TOL[prec], prec

@@ -71,6 +71,9 @@ SIGNATURES = {
     "fcm_spread": (ctypes.c_int, [VP, ctypes.c_int32, VP]),
     "fcm_stokes_solve": (ctypes.c_int, [VP, ctypes.c_int32]),
     "fcm_interp": (ctypes.c_int, [VP, ctypes.c_int32, VP]),
+    "fcm_get_variants": (ctypes.c_int, [VP, VP]),
+    "fcm_set_variants": (ctypes.c_int, [VP, VP]),
+    "fcm_autotune": (ctypes.c_int, [VP, ctypes.c_int32, VP, VP]),
     "fcm_produce_reference_matrices": (ctypes.c_int, [VP]),
     "fcm_get_reference_matrices": (ctypes.c_int, [VP, VP, VP, VP]),
     "fcm_set_reference_matrices": (ctypes.c_int, [VP, VP, VP]),

@@ -267,6 +267,8 @@ int setup_xfft(Ctx* c) {
   const bool ok = xfft_factor(c->g.nx, &n1, &n2) && c->g.nz % 2 == 0;
   c->xfft[1] = ok;
   c->xfft[0] = ok && c->g.nx <= 256;
+  c->xfft_cap[0] = c->xfft[0];
+  c->xfft_cap[1] = c->xfft[1];
   if (!ok) return FCM_OK;
   FCM_TRY(xfft_tables_init());
   const int n = c->g.nx;
@@ -290,9 +292,9 @@ int setup_xfft(Ctx* c) {
   // 328 against 364 us per solve); at 512^3 they took 3324 against 3201 us (z passes
   // 732 + 736 against 919 + 958 us, y passes 783 + 1074 against 662 + 662 us), so
   // longer lines stay with cuFFT
-  c->yz32 = xfft_factor(c->g.ny, &n1, &n2) && xfft_factor(c->g.nz, &n1, &n2) && c->g.nz <= 256 &&
-            3 * c->g.nx <= 65535;
-  if (c->yz32) {
+  c->yz32_cap = xfft_factor(c->g.ny, &n1, &n2) && xfft_factor(c->g.nz, &n1, &n2) && 3 * c->g.nx <= 65535;
+  c->yz32 = c->yz32_cap && c->g.nz <= 256;
+  if (c->yz32_cap) {
     for (int d = 0; d < 2; ++d) {
       const int m = d == 0 ? c->g.ny : c->g.nz;
       std::vector<float2> w(m);
@@ -320,7 +322,7 @@ int ensure_grid(Ctx* c) {
   FCM_CUFFT(cufftPlanMany(&gb.c2r, 3, n, nullptr, 1, (int)c->g.Gc, nullptr, 1, (int)c->g.G, c2r_type<T>(), 3));
   FCM_CUFFT(cufftSetStream(gb.r2c, c->stream));
   FCM_CUFFT(cufftSetStream(gb.c2r, c->stream));
-  if (c->xfft[sizeof(T) == 8 ? 0 : 1]) {  // (y, z) transforms of the 3 nx planes of each component
+  if (c->xfft_cap[sizeof(T) == 8 ? 0 : 1]) {  // (y, z) transforms of the 3 nx planes of each component
     int n2[2] = {c->g.ny, c->g.nz};
     const int planes = 3 * c->g.nx;
     FCM_CUFFT(cufftPlanMany(&gb.r2c2d, 2, n2, nullptr, 1, c->g.ny * c->g.nz, nullptr, 1, c->g.ny * c->g.nzh,
@@ -2381,6 +2383,100 @@ struct fcm_batch {
 
 using namespace fcm;
 
+// ------------------------------------------------------------------ kernel variants
+// Solve variant of precision P: 0 = 3D transforms, 1 = fused x-transform with
+// cuFFT's (y, z) plans, 2 = with the library's (y, z) kernels.
+static int solve_variant(const Ctx* c, int P) {
+  if (!c->xfft[P]) return 0;
+  return (P == 1 && c->yz32) ? 2 : 1;
+}
+
+static void get_variants(const Ctx* c, int32_t* v) {
+  v[0] = c->spread_pipe[0] ? 0 : 1;
+  v[1] = solve_variant(c, 0);
+  v[2] = c->spread_pipe[1] ? 0 : 1;
+  v[3] = solve_variant(c, 1);
+}
+
+static int set_variants(Ctx* c, const int32_t* v) {
+  for (int P = 0; P < 2; ++P) {
+    const int sp = v[2 * P], sv = v[2 * P + 1];
+    if (sp < 0 || sp > 1 || sv < 0 || sv > (P == 1 ? 2 : 1)) {
+      set_error("kernel variant out of range");
+      return FCM_ERR_INVALID;
+    }
+    if (P == 1 && c->p.precision != 1) continue;  // no FP32 grid
+    if ((sv >= 1 && !c->xfft_cap[P]) || (sv == 2 && !c->yz32_cap)) {
+      set_error("this grid does not allow solve variant " + std::to_string(sv));
+      return FCM_ERR_INVALID;
+    }
+  }
+  for (int P = 0; P < 2; ++P) {
+    if (P == 1 && c->p.precision != 1) continue;
+    c->spread_pipe[P] = v[2 * P] == 0;
+    c->xfft[P] = v[2 * P + 1] >= 1;
+    if (P == 1) c->yz32 = v[3] == 2;
+  }
+  c->graph_stale = true;
+  return FCM_OK;
+}
+
+struct EventPair {
+  cudaEvent_t a = nullptr, b = nullptr;
+  ~EventPair() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
+// Mean microseconds of one call of body() on c's stream: one untimed call, then
+// reps timed ones between two events.
+template <class F>
+static int time_calls(Ctx* c, int reps, F&& body, double* out) {
+  FCM_TRY(body());
+  EventPair ev;
+  FCM_CUDA(cudaEventCreate(&ev.a));
+  FCM_CUDA(cudaEventCreate(&ev.b));
+  FCM_CUDA(cudaEventRecord(ev.a, c->stream));
+  for (int i = 0; i < reps; ++i) FCM_TRY(body());
+  FCM_CUDA(cudaEventRecord(ev.b, c->stream));
+  FCM_CUDA(cudaEventSynchronize(ev.b));
+  float ms = 0.f;
+  FCM_CUDA(cudaEventElapsedTime(&ms, ev.a, ev.b));
+  *out = 1e3 * (double)ms / reps;
+  return FCM_OK;
+}
+
+// The spread and solve variants of one precision timed on c's own grid and blob
+// table; the fastest kept.  t[0..1] spread, t[2..4] solve (-1: not available).
+template <typename T>
+static int tune_precision(Ctx* c, int reps, double* t) {
+  constexpr int P = sizeof(T) == 8 ? 0 : 1;
+  GridBufs<T>& gb = grid_of<T>(c);
+  const BlobTable<T>& bt = gb.blobs;
+  FCM_CUDA(cudaMemsetAsync(c->d_tmp3, 0, sizeof(double) * 3 * (size_t)(c->Nb > 0 ? c->Nb : 1), c->stream));
+  if (bt.tiled) {
+    for (int v = 0; v < 2; ++v) {
+      c->spread_pipe[P] = v == 0;
+      FCM_TRY(time_calls(c, reps, [&] { return spread_t<T>(c, bt, c->d_tmp3); }, &t[v]));
+    }
+    c->spread_pipe[P] = t[0] <= t[1];
+  }
+  FCM_CUDA(cudaMemsetAsync(gb.r, 0, sizeof(T) * 3 * (size_t)c->g.G, c->stream));
+  for (int v = 0; v < 3; ++v) {
+    if ((v >= 1 && !c->xfft_cap[P]) || (v == 2 && (P == 0 || !c->yz32_cap))) continue;
+    c->xfft[P] = v >= 1;
+    if (P == 1) c->yz32 = v == 2;
+    FCM_TRY(time_calls(c, reps, [&] { return stokes_t<T>(c); }, &t[2 + v]));
+  }
+  int best = 0;
+  for (int v = 1; v < 3; ++v)
+    if (t[2 + v] >= 0.0 && t[2 + v] < t[2 + best]) best = v;
+  c->xfft[P] = best >= 1;
+  if (P == 1) c->yz32 = best == 2;
+  return FCM_OK;
+}
+
 extern "C" {
 
 void fcm_default_params(fcm_params* p) {
@@ -2963,6 +3059,58 @@ int fcm_interp(fcm_ctx* ctx, int32_t precision, double* V) {
     FCM_TRY(interp_t<float>(c, c->g32.blobs, c->g32.r, dV));
   if (dV == V) return FCM_OK;
   return copy_out(c, V, c->d_V, sizeof(double) * 3 * c->Nb);
+}
+
+int fcm_get_variants(fcm_ctx* ctx, int32_t* variants) {
+  CTX_CHECK(ctx);
+  if (!variants) {
+    set_error("variants is NULL");
+    return FCM_ERR_INVALID;
+  }
+  get_variants(ctx->c, variants);
+  return FCM_OK;
+}
+
+int fcm_set_variants(fcm_ctx* ctx, const int32_t* variants) {
+  CTX_CHECK(ctx);
+  if (!variants) {
+    set_error("variants is NULL");
+    return FCM_ERR_INVALID;
+  }
+  if (ctx->c->in_batch) {
+    set_error("kernel variants of a context owned by a batch are fixed");
+    return FCM_ERR_STATE;
+  }
+  return set_variants(ctx->c, variants);
+}
+
+int fcm_autotune(fcm_ctx* ctx, int32_t reps, double* us, int32_t* variants) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  if (c->in_batch) {
+    set_error("kernel variants of a context owned by a batch are fixed");
+    return FCM_ERR_STATE;
+  }
+  if (!c->gauss_ready) {
+    set_error("set_up_gaussians must precede fcm_autotune");
+    return FCM_ERR_STATE;
+  }
+  return guard([&]() -> int {
+    const int R = reps > 0 ? reps : 5;
+    double t[10];
+    for (double& v : t) v = -1.0;
+    FCM_TRY(ensure_grid<double>(c));
+    FCM_TRY(tune_precision<double>(c, R, t));
+    if (c->p.precision == 1) {
+      FCM_TRY(ensure_grid<float>(c));
+      FCM_TRY(tune_precision<float>(c, R, t + 5));
+    }
+    c->det_ready = false;
+    c->graph_stale = true;
+    if (us) std::memcpy(us, t, sizeof(t));
+    if (variants) get_variants(c, variants);
+    return FCM_OK;
+  });
 }
 
 int fcm_produce_reference_matrices(fcm_ctx* ctx) {

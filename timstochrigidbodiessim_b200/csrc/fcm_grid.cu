@@ -819,9 +819,9 @@ int launch_set_up_gaussians(const Ctx& c, BlobTable<T>& t, const double* dY, cud
 template <typename T>
 int launch_spread(const Ctx& c, const BlobTable<T>& t, const double* dF, T* grid, cudaStream_t s) {
   if (t.tiled) {
-    // FP64: the persistent pipelined kernel (its staging latency is the limit);
-    // FP32: one CTA per tile (issue-bound; more resident CTAs hide the latency)
-    if (sizeof(T) == 8) {
+    // by default FP64 takes the persistent pipelined kernel (its staging latency is
+    // the limit), FP32 one CTA per tile; fcm_autotune may choose the other
+    if (c.spread_pipe[sizeof(T) == 8 ? 0 : 1]) {
       const int ctas = std::min(t.ntiles, persistent_ctas(k_spread_pipe<T>, 64, c.device));
       k_spread_pipe<T><<<ctas, 64, 0, s>>>(t.wc, dF, tile_geom(c.g, t.W), t.tile_offset, t.tile_list, c.g.G, grid,
                                           t.ntiles);

@@ -261,6 +261,13 @@ struct Ctx {
   // (fused FP32 grids whose ny and nz are supported lengths, nz even, nz <= 256);
   // twiddles exp(-2 pi i j / n) for n = ny, nz
   bool yz32 = false;
+  // what the grids allow (fcm_autotune chooses within it): the fused x-transform per
+  // precision (its (y, z) plans exist), the library's (y, z) kernels up to 512 points
+  bool xfft_cap[2] = {false, false};
+  bool yz32_cap = false;
+  // spread kernel per precision: the persistent software-pipelined one (FP64
+  // default) or one CTA per tile (FP32 default); both sum in the same order
+  bool spread_pipe[2] = {true, false};
   void* d_ytw32 = nullptr;
   void* d_ztw32 = nullptr;
   void* d_xtw64 = nullptr;

@@ -1366,7 +1366,7 @@ int launch_xfft_project(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream
 template <typename T>
 int xfft_prepare(const Ctx& c) {
   if constexpr (sizeof(T) == 4)
-    if (c.yz32 && yz_plane_ok(c)) FCM_TRY(yz_plane(c, nullptr, nullptr, nullptr, 0, false, 0, true));
+    if (c.yz32_cap && yz_plane_ok(c)) FCM_TRY(yz_plane(c, nullptr, nullptr, nullptr, 0, false, 0, true));
   return xfft_dispatch<T>(c, nullptr, 0, true);
 }
 
