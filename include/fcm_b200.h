@@ -297,9 +297,9 @@ int fcm_interp(fcm_ctx* ctx, int32_t precision, double* V);
  *       + projection kernel, 2 = the library's own (y, z) transforms around it
  *       (FP32 only).  The solves agree within rounding.
  * A variant the grid does not allow (1 and 2 need supported lengths, 2 also
- * nz <= 512) is refused with FCM_ERR_INVALID; variants 1 for the spread and the
- * FP32 entries are ignored where the grid is not tiled or the context has no FP32
- * grid.  The defaults are those measured fastest on B200: [0, 1 or 0, 1, 2 up to
+ * nz <= 512) or out of range is refused with FCM_ERR_INVALID; the spread entries
+ * have no effect where the grid is not tiled (atomic spreading), the FP32 entries
+ * none in a context without an FP32 grid (they are still range-checked).  The defaults are those measured fastest on B200: [0, 1 or 0, 1, 2 up to
  * 256 points along z else 1 or 0].  Step graphs are rebuilt on the next step.
  * Refused for a context owned by a batch. */
 int fcm_get_variants(fcm_ctx* ctx, int32_t* variants);
