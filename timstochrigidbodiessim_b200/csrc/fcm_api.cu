@@ -10,9 +10,21 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "fcm_internal.cuh"
 
 namespace fcm {
+
+// NVTX range over a scope: host-driven steps, refinement sweeps, GMRES iterations
+// and the grid stages, for Nsight tools and ncu's --nvtx filters (no cost without a
+// tool attached; ranges entered during graph capture mark the capture).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 static thread_local std::string g_err;
 void set_error(const std::string& m) { g_err = m; }
@@ -384,6 +396,7 @@ int set_up_gaussians_dev(Ctx* c, const double* dY) {
 
 template <typename T>
 int spread_t(Ctx* c, const BlobTable<T>& t, const double* dF) {
+  NvtxRange r(sizeof(T) == 8 ? "fcm spread fp64" : "fcm spread fp32");
   FCM_TRY(launch_spread<T>(*c, t, dF, grid_of<T>(c).r, c->stream));
   if (c->p.slip_channel) FCM_TRY(launch_slip_image<T>(*c, grid_of<T>(c).r, c->stream));  // :602-632
   return FCM_OK;
@@ -391,6 +404,7 @@ int spread_t(Ctx* c, const BlobTable<T>& t, const double* dF) {
 
 template <typename T>
 int stokes_t(Ctx* c) {
+  NvtxRange r(sizeof(T) == 8 ? "fcm stokes solve fp64" : "fcm stokes solve fp32");
   GridBufs<T>& gb = grid_of<T>(c);
   if (c->xfft[sizeof(T) == 8 ? 0 : 1]) {  // (y, z) transforms, then x + projection + inverse x
     if constexpr (sizeof(T) == 4) {
@@ -413,6 +427,7 @@ int stokes_t(Ctx* c) {
 
 template <typename T>
 int interp_t(Ctx* c, const BlobTable<T>& t, const T* grid, double* dV) {
+  NvtxRange r(sizeof(T) == 8 ? "fcm interp fp64" : "fcm interp fp32");
   return launch_interp<T>(*c, t, grid, dV, c->stream);
 }
 
@@ -531,6 +546,7 @@ int gmres_dev(Ctx* c, int prec, const double* d_b, double* d_x, double tol, int 
   FCM_CUDA(cudaMemcpyAsync(c->h_gm, c->gm, sizeof(GmState), cudaMemcpyDeviceToHost, c->stream));
   FCM_CUDA(cudaStreamSynchronize(c->stream));
   for (int it = 0; it < max_iter && !c->h_gm->done; ++it) {
+    NvtxRange r(prec ? "fcm gmres iteration fp32 grid" : "fcm gmres iteration fp64");
     FCM_CUDA(cudaGraphLaunch(c->iter_graph[prec], c->stream));
     count_launches(c->iter_graph_kernels[prec]);
     FCM_CUDA(cudaMemcpyAsync(c->h_gm, c->gm, sizeof(GmState), cudaMemcpyDeviceToHost, c->stream));
@@ -569,6 +585,7 @@ int solve_dev(Ctx* c, const double* d_rhs, double* d_soln, int* iters, double* r
   int total = 0, sw = 0, st = FCM_OK;
   double relr = 1.0;
   for (sw = 1; sw <= 8; ++sw) {
+    NvtxRange r("fcm refinement sweep");
     // The FP32-grid inner solve only has to shrink the current residual by the
     // remaining factor; below ~1e-6 the FP32 operator error dominates anyway.
     const double inner_tol = std::min(0.5, std::max(1e-6, 0.3 * c->p.gmres_tol / relr));
@@ -1355,6 +1372,7 @@ int guard(F&& f) {
 
 // main.cpp:222-451, one step driven from the host.
 int step_host(Ctx* c, uint64_t seed, uint64_t step_index, fcm_step_info* info) {
+  NvtxRange range("fcm step");
   {
     fcm_step_info inf;
     std::memset(&inf, 0, sizeof(inf));
