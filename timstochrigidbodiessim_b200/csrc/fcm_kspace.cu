@@ -1116,9 +1116,9 @@ bool xfft_factor(int n, int* n1, int* n2) {
 namespace {
 
 // kz per interior CTA: shared memory N * 3 TK elements near 100 KB (two CTAs per
-// SM), TK * N1 threads busy in the middle step.  (At 256 points in FP32, 12 kz per
-// CTA, three CTAs per SM, took 171 us against 129 us with 16.)  (FP64 grids beyond 256 points use
-// the 3D transforms instead.)
+// SM), TK * N1 threads busy in the middle step.  At 256 points in FP32, 12 kz per
+// CTA (three CTAs per SM) took 171 us against 129 us with 16.  FP64 grids beyond 256
+// points use the 3D transforms instead.
 template <typename T>
 constexpr int xfft_tk(int n) {
   return sizeof(T) == 4 ? (n <= 256 ? 16 : 8) : 8;
