@@ -28,6 +28,44 @@ def test_single_blob_hasimoto(L, N):
     assert abs(V[1]) < 1e-10 * mu0 and abs(V[2]) < 1e-10 * mu0
 
 
+@pytest.mark.parametrize("shape", [(16, 16, 16), (12, 18, 10), (10, 9, 15)])
+def test_stokes_solve_is_the_spectral_projection(shape):
+    """The oracle's Stokes solve against the spectral solution computed here with
+    numpy's FFT: every mode with no Nyquist index satisfies
+    u(q) = (f(q) - q (q.f(q)) / |q|^2) / (eta |q|^2), so u is divergence-free
+    (q.u = 0) and f - eta |q|^2 u is a pure pressure gradient (parallel to q); the
+    mean flow is zero.  (At Nyquist indices the reference's one-sided wavenumber
+    and the C2R's Hermitian part differ from this symmetric form.)"""
+    nx, ny, nz = shape
+    dx = 0.9
+    p = FcmParams.defaults(nx=nx, ny=ny, nz=nz, ngauss=8, dx=dx, num_bodies=5, blobs_per_body=1, ncells=3,
+                           viscosity=1.7)
+    o = Oracle(p, [0, 0, 0])
+    rng = np.random.default_rng(11)
+    o.set_up_gaussians((rng.uniform(0, 1, (5, 3)) * np.array([nx, ny, nz]) * dx).ravel())
+    o.set_up_force_distribution(rng.standard_normal(15))
+    grid = lambda c: o.get_grid(c).reshape(nx, ny, p.pad)[:, :, :nz].copy()
+    Fh = np.array([np.fft.fftn(grid(c)) for c in range(3)])  # before the in-place transforms
+    o.produce_deterministic_velocity_field()
+    Uh = np.array([np.fft.fftn(grid(c)) for c in range(3, 6)])
+    qs = np.meshgrid(*[2 * np.pi * np.fft.fftfreq(n, d=dx) for n in (nx, ny, nz)], indexing="ij")
+    q = np.array(qs)
+    q2 = (q ** 2).sum(0)
+    keep = np.ones((nx, ny, nz), bool)
+    for ax, n in enumerate((nx, ny, nz)):
+        if n % 2 == 0:
+            idx = [slice(None)] * 3
+            idx[ax] = n // 2
+            keep[tuple(idx)] = False
+    keep[0, 0, 0] = False
+    qf = (q * Fh).sum(0)
+    expect = (Fh - q * qf / np.where(q2 > 0, q2, 1)) / (p.viscosity * np.where(q2 > 0, q2, 1))
+    scale = np.abs(expect[:, keep]).max()
+    assert np.abs(Uh[:, keep] - expect[:, keep]).max() < 1e-12 * scale
+    assert np.abs((q * Uh).sum(0)[keep]).max() < 1e-12 * scale * np.sqrt(q2.max())
+    assert np.abs(Uh[:, 0, 0, 0]).max() < 1e-12 * scale
+
+
 def _small_suspension(M=4, nb=3, N=24, L=24.0, seed=3):
     ref = np.array(rod_reference_positions(nb, 2.2))
     p = FcmParams.defaults(nx=N, ny=N, nz=N, ngauss=12, dx=L / N, num_bodies=M, blobs_per_body=nb, ncells=4,
