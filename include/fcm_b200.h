@@ -217,6 +217,13 @@ int fcm_apply_barrier_forces(fcm_ctx* ctx, double* blob_forces);
 /* ================================================================ fcm_fluid_solver */
 /* fcm_fluid_solver.cpp:131-165 on Y (Nb*3; NULL = all_blob_pos). */
 int fcm_set_up_gaussians(fcm_ctx* ctx, const double* Y);
+/* The tables of the last fcm_set_up_gaussians (fcm_fluid_solver.cpp:131-165) on
+ * the grid of one precision (0 = FP64; 1 = FP32, in a context of precision 1,
+ * whose stencil may be narrower): ind (Nb*3*W, may be NULL) the periodic grid
+ * indices indx/indy/indz of every blob, dimension and stencil point, w (Nb*3*W,
+ * may be NULL) the weights gaussx/y/z; W is the stencil width of that grid
+ * (ngauss for FP64). */
+int fcm_get_gaussians(fcm_ctx* ctx, int32_t precision, int32_t* ind, double* w);
 /* fcm_fluid_solver.cpp:167-361 with the stress drawn from a counter-based
  * Philox4x32-10 stream keyed by (seed, counter). */
 int fcm_produce_random_velocity_field(fcm_ctx* ctx, uint64_t seed, uint64_t counter);
@@ -320,6 +327,34 @@ int fcm_produce_reference_matrices(fcm_ctx* ctx);
 int fcm_get_reference_matrices(fcm_ctx* ctx, double* ref_Minv, double* ref_N, double* ref_KTKinv);
 int fcm_set_reference_matrices(fcm_ctx* ctx, const double* ref_Minv, const double* ref_N);
 
+/* Per-body shapes.  No counterpart in the reference: its collection has one
+ * blob_ref_pos for every body (collection_of_rigid_bodies.hpp:24) and one probed
+ * preconditioner reference (fcm_fluid_solver.cpp:842-881).  shapes (3*nb*M)
+ * holds body n's reference blob positions at 3*nb*n (the same blob-major layout
+ * as blob_ref_pos); every body keeps nb blobs, so blob i still belongs to body
+ * i/nb (linked_list.cpp:106,118).  From then on blob positions, K, K^T, the
+ * preconditioner and the GDC rigid projection use each body's own shape, each
+ * body gets its own ref_KTKinv = inv(K^T K) (collection_of_rigid_bodies.cpp:
+ * 117-130 per body), and the Metropolis rotation scale is the largest blob
+ * distance over all shapes.  Probing 3*nb FCM solves per shape
+ * (fcm_produce_reference_matrices) is out of reach for thousands of shapes, so
+ * each body's ref_Minv is the inverse of its blob-blob mobility computed with the
+ * free-space FCM pair mobility of two Gaussian envelopes (sigma = a/sqrt(pi)):
+ *   M(r) = [A I + B rr/r^2] / (8 pi eta r), s^2 = 2 sigma^2,
+ *   A = (1 + s^2/r^2) erf(r/(sqrt2 s)) - sqrt(2/pi)(s/r) exp(-r^2/2s^2),
+ *   B = (1 - 3s^2/r^2) erf(r/(sqrt2 s)) + 3 sqrt(2/pi)(s/r) exp(-r^2/2s^2),
+ *   M(0) = I/(6 pi eta a),
+ * and ref_N = inv(K^T ref_Minv K) (pseudo-inverse for collinear blobs).  The
+ * preconditioner changes GMRES's iteration count, never its solution.
+ * fcm_set_body_preconditioners replaces ref_Minv (M*(3nb)^2, body-major,
+ * column-major blocks) and/or ref_N (36*M); fcm_get_body_preconditioners reads
+ * them and the per-body ref_KTKinv (36*M).  After fcm_set_body_shapes the
+ * single-shape calls fcm_produce/get/set_reference_matrices are refused
+ * (FCM_ERR_STATE); not available to batch members. */
+int fcm_set_body_shapes(fcm_ctx* ctx, const double* shapes);
+int fcm_set_body_preconditioners(fcm_ctx* ctx, const double* Minv, const double* N);
+int fcm_get_body_preconditioners(fcm_ctx* ctx, double* Minv, double* N, double* KTKinv);
+
 /* ================================================================ gmres_solver */
 /* gmres_solver.cpp:58-70: RHS = [-V ; -K^T blob_forces - external]. */
 int fcm_assemble_RHS(fcm_ctx* ctx);
@@ -413,18 +448,25 @@ int fcm_step_many(fcm_ctx* const* ctxs, int32_t n, const uint64_t* seeds, uint64
  * memory -- a time-step loop that must not stall the device (cudaMalloc and
  * cudaFree synchronise it), or an application whose device memory all belongs to
  * its own allocator or pool -- this interpolates a caller-owned velocity grid
- * onto blobs without allocating anything.  Same result as
- * fcm_calculate_deterministic_blob_velocities on the same grid and positions:
- *   V(3*nblobs) = DX^3 * sum u * gx*gy*gz   (fcm_fluid_solver.cpp:363-424).
- * Y (nblobs*3), grid (3*nx*ny*nz, component-major [3][nx][ny][nz], unpadded) and V
- * must be DEVICE pointers; work is issued on `stream` (a cudaStream_t, 0 = legacy).
+ * onto blobs without allocating anything:
+ *   V_c(blob) = DX^3 * sum over the blob's W^3 stencil points of
+ *               u_c(point) * gx(point) * gy(point) * gz(point),
+ * with the separable Gaussian weights g(x) = exp(-pi (x - Y)^2 / (2 a^2)) /
+ * (sqrt(2) a) on the W grid points nearest each blob coordinate Y.  The grid is
+ * fully periodic: there is no slip-channel truncation of the Gaussians, so the
+ * result equals a context's interpolation only for a periodic box (slip_channel
+ * 0).  Y (nblobs*3), grid (3*nx*ny*nz, component-major [3][nx][ny][nz],
+ * unpadded) and V must be DEVICE pointers of the current device (or managed
+ * memory); work is issued on `stream` (a cudaStream_t, 0 = legacy).
  * Limits: nblobs <= 8192, ngauss <= 24, nx, ny, nz multiples of 8 with
  * ngauss + 8 <= n, and at most 32768 8^3 tiles (a 256^3 grid); larger inputs are
  * rejected with FCM_ERR_INVALID.  Scratch is a fixed 32 MiB device array inside the
  * library, held by every GPU that loads it until exit.  The first call on a device
  * looks up that array's device address (once per device), so make the first call
- * before any stream capture.  Every call shares the array: calls that may overlap
- * on the GPU (different streams, no ordering between them) race. */
+ * before any stream capture; the address is kept for the process's lifetime, so
+ * do not use this call after cudaDeviceReset in the same process.  Every call
+ * shares the array: calls that may overlap on the GPU (different streams, no
+ * ordering between them) race. */
 int fcm_interp_noalloc(int32_t nx, int32_t ny, int32_t nz, double dx, double blob_radius, int32_t ngauss,
                        int32_t nblobs, const double* Y, const double* grid, double* V, void* stream);
 

@@ -635,6 +635,11 @@ struct orc {
   std::vector<double> blob_ref_pos;  // 3*nb
   std::vector<double> all_blob_pos;  // Nb*3
   Mat ref_KTKinv;
+  // per-body shapes (no counterpart in the reference, whose bodies share
+  // blob_ref_pos): 3*nb per body, and per body ref_KTKinv (36), ref_Minv
+  // ((3nb)^2) and ref_N (36)
+  bool per_body = false;
+  std::vector<double> shapes, body_KTKinv, body_Minv, body_N;
   std::vector<Body> bodies, midstep_bodies, temp_bodies;
   std::vector<double> blob_forces, ext_forces, U0;
   double body_radius = 0;
@@ -768,11 +773,17 @@ void list_visit(const orc* o, const std::vector<double>& Y, Fn fn) {
   }
 }
 
-void blob_pos_of(const orc* o, const Body& b, int m, double out[3]) {
+// Reference position of blob m of body n: the shared blob_ref_pos, or body n's own
+// shape.
+const double* ref_of(const orc* o, int n, int m) {
+  return o->per_body ? &o->shapes[3 * ((size_t)n * o->nb + m)] : &o->blob_ref_pos[3 * m];
+}
+
+void blob_pos_of(const orc* o, const Body& b, int n, int m, double out[3]) {
   double R[3][3];
   quat_matrix(b.q, R);
   double r[3];
-  matvec3(R, &o->blob_ref_pos[3 * m], r);
+  matvec3(R, ref_of(o, n, m), r);
   const double Lv[3] = {o->LX, o->LY, o->LZ};
   for (int d = 0; d < 3; ++d) {
     const double pd = b.x[d] + r[d];
@@ -782,7 +793,7 @@ void blob_pos_of(const orc* o, const Body& b, int m, double out[3]) {
 
 void fill_pos(orc* o, const std::vector<Body>& bs) {  // collection_of_rigid_bodies.cpp:155-193
   for (int n = 0; n < o->M; n++)
-    for (int m = 0; m < o->nb; m++) blob_pos_of(o, bs[n], m, &o->all_blob_pos[3 * (n * o->nb + m)]);
+    for (int m = 0; m < o->nb; m++) blob_pos_of(o, bs[n], n, m, &o->all_blob_pos[3 * (n * o->nb + m)]);
 }
 
 // fcm_fluid_solver.cpp:131-165
@@ -1013,7 +1024,7 @@ void mult_K(const orc* o, const double* in, double* out) {
     for (int j = 0; j < o->nb; j++) {
       const int jpos = 3 * (o->nb * i + j);
       double r[3], c[3];
-      matvec3(R, &o->blob_ref_pos[3 * j], r);
+      matvec3(R, ref_of(o, i, j), r);
       cross3(in + ipos + 3, r, c);
       for (int d = 0; d < 3; ++d) out[jpos + d] += in[ipos + d] + c[d];
     }
@@ -1030,7 +1041,7 @@ void mult_KT(const orc* o, const double* in, double* out) {
     for (int j = 0; j < o->nb; j++) {
       const int jpos = 3 * (o->nb * i + j);
       double r[3], c[3];
-      matvec3(R, &o->blob_ref_pos[3 * j], r);
+      matvec3(R, ref_of(o, i, j), r);
       cross3(r, in + jpos, c);
       for (int d = 0; d < 3; ++d) {
         out[ipos + d] += in[jpos + d];
@@ -1050,7 +1061,7 @@ void rigid_projection(const orc* o, const Body& body, int n, const double* V, do
     const int id = n * o->nb + i;
     const double* vel = V + 3 * id;
     double r[3], c[3];
-    matvec3(Q, &o->blob_ref_pos[3 * i], r);
+    matvec3(Q, ref_of(o, n, i), r);
     cross3(r, vel, c);
     for (int d = 0; d < 3; ++d) { b[d] += vel[d]; b[3 + d] += c[d]; }
   }
@@ -1058,7 +1069,12 @@ void rigid_projection(const orc* o, const Body& body, int n, const double* V, do
   matTvec3(Q, b, bt);
   matTvec3(Q, b + 3, bt + 3);
   double u[6];
-  gemv(o->ref_KTKinv, 6, 6, bt, u);
+  if (o->per_body) {
+    const Mat KTKinv(o->body_KTKinv.begin() + 36 * (size_t)n, o->body_KTKinv.begin() + 36 * (size_t)(n + 1));
+    gemv(KTKinv, 6, 6, bt, u);
+  } else {
+    gemv(o->ref_KTKinv, 6, 6, bt, u);
+  }
   matvec3(Q, u, U);
   matvec3(Q, u + 3, U + 3);
 }
@@ -1074,13 +1090,19 @@ void mult_Pinv(const orc* o, const double* in, double* out) {
     quat_matrix(o->midstep_bodies[n].q, Q);
     for (int m = 0; m < nb; m++) {
       double r[3], C[3][3];
-      matvec3(Q, &o->blob_ref_pos[3 * m], r);
+      matvec3(Q, ref_of(o, n, m), r);
       rcross(r, C);
       for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) K[(size_t)(3 + j) * n3 + 3 * m + i] = C[i][j];
     }
-    Mat Minv = o->ref_Minv;
-    Mat N = o->ref_N;
+    // the body's own blocks with per-body shapes
+    const size_t mm = (size_t)n3 * n3;
+    const Mat ref_Minv = o->per_body ? Mat(o->body_Minv.begin() + mm * n, o->body_Minv.begin() + mm * (n + 1))
+                                     : o->ref_Minv;
+    const Mat ref_N = o->per_body ? Mat(o->body_N.begin() + 36 * (size_t)n, o->body_N.begin() + 36 * (size_t)(n + 1))
+                                  : o->ref_N;
+    Mat Minv = ref_Minv;
+    Mat N = ref_N;
     auto rot_block = [&](Mat& A, int lda, int r0, int c0, const Mat& src) {
       // A(r0:r0+2, c0:c0+2) = Q * src(r0.., c0..) * Q^T
       double B[3][3], T[3][3];
@@ -1093,14 +1115,14 @@ void mult_Pinv(const orc* o, const double* in, double* out) {
     };
     for (int m = 0; m < nb; m++)
       for (int l = m; l < nb; l++) {
-        rot_block(Minv, n3, 3 * m, 3 * l, o->ref_Minv);
+        rot_block(Minv, n3, 3 * m, 3 * l, ref_Minv);
         for (int i = 0; i < 3; ++i)
           for (int j = 0; j < 3; ++j) Minv[(size_t)(3 * m + j) * n3 + 3 * l + i] = Minv[(size_t)(3 * l + i) * n3 + 3 * m + j];
       }
-    rot_block(N, 6, 0, 0, o->ref_N);
-    rot_block(N, 6, 0, 3, o->ref_N);
-    rot_block(N, 6, 3, 0, o->ref_N);
-    rot_block(N, 6, 3, 3, o->ref_N);
+    rot_block(N, 6, 0, 0, ref_N);
+    rot_block(N, 6, 0, 3, ref_N);
+    rot_block(N, 6, 3, 0, ref_N);
+    rot_block(N, 6, 3, 3, ref_N);
     const double* in_l = in + (size_t)n3 * n;
     const double* in_U = in + (size_t)3 * Nb + 6 * n;
     std::vector<double> t(n3), t2(n3);
@@ -1590,7 +1612,7 @@ void orc_produce_reference_matrices(orc* o) {
   c.x[0] = 0.5 * o->LX; c.x[1] = (o->p.slip_channel ? 0.25 : 0.5) * o->LY; c.x[2] = 0.5 * o->LZ;  // :139-147
   c.q.s = 1.0; c.q.v[0] = c.q.v[1] = c.q.v[2] = 0.0;
   std::vector<double> Y((size_t)3 * nb);
-  for (int m = 0; m < nb; ++m) blob_pos_of(o, c, m, &Y[3 * m]);
+  for (int m = 0; m < nb; ++m) blob_pos_of(o, c, 0, m, &Y[3 * m]);
   // save the blob-table state of the caller
   const std::vector<double> gx = o->gaussx, gy = o->gaussy, gz = o->gaussz, Vs = o->V;
   const std::vector<int> ix = o->indx, iy = o->indy, iz = o->indz;
@@ -1639,6 +1661,116 @@ void orc_get_reference_matrices(orc* o, double* Minv, double* N, double* KTKinv)
 void orc_set_reference_matrices(orc* o, const double* Minv, const double* N) {
   if (Minv) o->ref_Minv.assign(Minv, Minv + (size_t)9 * o->nb * o->nb);
   if (N) o->ref_N.assign(N, N + 36);
+}
+
+// ---------------------------------------------------------------- per-body shapes
+// No counterpart in the reference (one blob_ref_pos per collection).  Each body
+// gets its own shape and ref_KTKinv = inv(K^T K) of that shape
+// (collection_of_rigid_bodies.cpp:117-130 applied per body); the preconditioner
+// blocks start as identities (as the single-shape ones do before
+// produce_reference_matrices).
+void orc_set_body_shapes(orc* o, const double* shapes) {
+  const int nb = o->nb, n3 = 3 * nb, M = o->M;
+  o->shapes.assign(shapes, shapes + (size_t)n3 * M);
+  o->body_KTKinv.assign(36 * (size_t)M, 0.0);
+  o->body_Minv.assign((size_t)n3 * n3 * M, 0.0);
+  o->body_N.assign(36 * (size_t)M, 0.0);
+  for (int n = 0; n < M; ++n) {
+    Mat K((size_t)n3 * 6, 0.0);
+    for (int m = 0; m < nb; m++) {
+      double C[3][3];
+      rcross(&o->shapes[3 * ((size_t)n * nb + m)], C);
+      for (int d = 0; d < 3; ++d) K[(size_t)d * n3 + 3 * m + d] = 1.0;
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) K[(size_t)(3 + j) * n3 + 3 * m + i] = C[i][j];
+    }
+    Mat KTK(36, 0.0), KTKinv;
+    for (int i = 0; i < 6; ++i)
+      for (int j = 0; j < 6; ++j) {
+        double sum = 0.0;
+        for (int t = 0; t < n3; ++t) sum += K[(size_t)i * n3 + t] * K[(size_t)j * n3 + t];
+        KTK[(size_t)j * 6 + i] = sum;
+      }
+    sym_inv_or_pinv(KTK, 6, KTKinv);
+    std::copy(KTKinv.begin(), KTKinv.end(), o->body_KTKinv.begin() + 36 * (size_t)n);
+    for (int i = 0; i < n3; ++i) o->body_Minv[(size_t)n * n3 * n3 + (size_t)i * n3 + i] = 1.0;
+    for (int i = 0; i < 6; ++i) o->body_N[36 * (size_t)n + 7 * i] = 1.0;
+  }
+  o->per_body = true;
+}
+
+void orc_set_body_preconditioners(orc* o, const double* Minv, const double* N) {
+  const size_t n3 = 3 * (size_t)o->nb;
+  if (Minv) o->body_Minv.assign(Minv, Minv + n3 * n3 * o->M);
+  if (N) o->body_N.assign(N, N + 36 * (size_t)o->M);
+}
+
+void orc_get_body_preconditioners(orc* o, double* Minv, double* N, double* KTKinv) {
+  if (Minv) std::copy(o->body_Minv.begin(), o->body_Minv.end(), Minv);
+  if (N) std::copy(o->body_N.begin(), o->body_N.end(), N);
+  if (KTKinv) std::copy(o->body_KTKinv.begin(), o->body_KTKinv.end(), KTKinv);
+}
+
+// The preconditioner blocks of every body from the free-space FCM blob-blob
+// mobility.  Two blobs with Gaussian force envelopes of variance sigma^2 = a^2/pi
+// interact through the Stokeslet smoothed by their convolved envelope (variance
+// s^2 = 2 sigma^2): with g(r) the mean of |x - Z| over Z ~ N(0, s^2 I), the
+// biharmonic part of the Stokes solution is -g/(8 pi) and the flow is
+//   M(r) = [(2 erf/r - g'/r) I + (g'/r - g'') rr/r^2] / (8 pi eta),
+//   g'  = (1 - s^2/r^2) erf + sqrt(2/pi)(s/r) e,   g'' = 2 s^2/r^3 erf - 2 sqrt(2/pi)(s/r^2) e,
+// erf = erf(r/(sqrt2 s)), e = exp(-r^2/(2 s^2)); M(0) = I/(6 pi eta a).  Then
+// ref_Minv = inv(M_body) and ref_N = inv(K^T ref_Minv K) in the body frame.
+void orc_produce_body_preconditioners(orc* o) {
+  const int nb = o->nb, n3 = 3 * nb;
+  const double a = o->a, eta = o->p.viscosity;
+  const double s = std::sqrt(2.0 / PI) * a, c2 = std::sqrt(2.0 / PI);
+  for (int n = 0; n < o->M; ++n) {
+    const double* sh = &o->shapes[(size_t)n * n3];
+    Mat Mb((size_t)n3 * n3, 0.0);
+    for (int i = 0; i < nb; ++i)
+      for (int j = 0; j < nb; ++j) {
+        double d[3] = {sh[3 * i] - sh[3 * j], sh[3 * i + 1] - sh[3 * j + 1], sh[3 * i + 2] - sh[3 * j + 2]};
+        const double r = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        double Aii, Brr;
+        if (i == j || r < 1e-10 * s) {
+          Aii = 1.0 / (6.0 * PI * eta * a);
+          Brr = 0.0;
+        } else {
+          const double er = std::erf(r / (std::sqrt(2.0) * s)), e = std::exp(-r * r / (2.0 * s * s));
+          const double g1 = (1.0 - s * s / (r * r)) * er + c2 * (s / r) * e;
+          const double g2 = 2.0 * s * s / (r * r * r) * er - 2.0 * c2 * s / (r * r) * e;
+          Aii = (2.0 * er / r - g1 / r) / (8.0 * PI * eta);
+          Brr = (g1 / r - g2) / (8.0 * PI * eta) / (r * r);
+        }
+        for (int p = 0; p < 3; ++p)
+          for (int q = 0; q < 3; ++q)
+            Mb[(size_t)(3 * j + q) * n3 + 3 * i + p] = (p == q ? Aii : 0.0) + Brr * d[p] * d[q];
+      }
+    Mat Minv, N;
+    dense_inv_sympd(Mb, n3, Minv);
+    Mat K((size_t)n3 * 6, 0.0);
+    for (int m = 0; m < nb; m++) {
+      double C[3][3];
+      rcross(&sh[3 * m], C);
+      for (int dd = 0; dd < 3; ++dd) K[(size_t)dd * n3 + 3 * m + dd] = 1.0;
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) K[(size_t)(3 + j) * n3 + 3 * m + i] = C[i][j];
+    }
+    Mat KtMK(36, 0.0);
+    std::vector<double> col(n3), t(n3);
+    for (int j = 0; j < 6; ++j) {
+      for (int i = 0; i < n3; ++i) col[i] = K[(size_t)j * n3 + i];
+      gemv(Minv, n3, n3, col.data(), t.data());
+      for (int i = 0; i < 6; ++i) {
+        double sum = 0.0;
+        for (int r = 0; r < n3; ++r) sum += K[(size_t)i * n3 + r] * t[r];
+        KtMK[(size_t)j * 6 + i] = sum;
+      }
+    }
+    sym_inv_or_pinv(KtMK, 6, N);
+    std::copy(Minv.begin(), Minv.end(), o->body_Minv.begin() + (size_t)n * n3 * n3);
+    std::copy(N.begin(), N.end(), o->body_N.begin() + 36 * (size_t)n);
+  }
 }
 
 // gmres_solver.cpp:58-70
@@ -1946,9 +2078,10 @@ double orc_calculate_potential(orc* o) {
 
 // main.cpp:113-210 with Philox uniforms (see mcmc_uniform).
 int orc_mcmc_run(orc* o, uint64_t seed, int64_t n_steps, fcm_mcmc_state* st) {
-  double body_radius = 0.0;  // collection_of_rigid_bodies.cpp:110-114
-  for (int m = 0; m < o->nb; ++m) {
-    const double* r = &o->blob_ref_pos[3 * m];
+  double body_radius = 0.0;  // collection_of_rigid_bodies.cpp:110-114 (over every shape)
+  const std::vector<double>& all_refs = o->per_body ? o->shapes : o->blob_ref_pos;
+  for (size_t m = 0; m < all_refs.size(); m += 3) {
+    const double* r = &all_refs[m];
     body_radius = std::max(body_radius, std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]));
   }
   if (body_radius == 0.0) body_radius = o->a;

@@ -96,6 +96,12 @@ void orc_get_grid(orc* o, int which, double* out);  /* 0..2 fx,fy,fz 3..5 ux,uy,
 void orc_produce_reference_matrices(orc* o);
 void orc_get_reference_matrices(orc* o, double* ref_Minv, double* ref_N, double* ref_KTKinv);
 void orc_set_reference_matrices(orc* o, const double* ref_Minv, const double* ref_N);
+/* Per-body shapes (3*nb per body) with per-body ref_KTKinv and preconditioner
+ * blocks; no counterpart in the reference. */
+void orc_set_body_shapes(orc* o, const double* shapes);
+void orc_set_body_preconditioners(orc* o, const double* Minv, const double* N);
+void orc_get_body_preconditioners(orc* o, double* Minv, double* N, double* KTKinv);
+void orc_produce_body_preconditioners(orc* o);
 
 void orc_assemble_RHS(orc* o);
 void orc_get_RHS(orc* o, double* rhs);

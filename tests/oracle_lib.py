@@ -80,6 +80,10 @@ def lib():
             "orc_produce_reference_matrices": (None, [vp]),
             "orc_get_reference_matrices": (None, [vp, D, D, D]),
             "orc_set_reference_matrices": (None, [vp, D, D]),
+            "orc_set_body_shapes": (None, [vp, D]),
+            "orc_set_body_preconditioners": (None, [vp, D, D]),
+            "orc_get_body_preconditioners": (None, [vp, D, D, D]),
+            "orc_produce_body_preconditioners": (None, [vp]),
             "orc_assemble_RHS": (None, [vp]),
             "orc_get_RHS": (None, [vp, D]),
             "orc_set_RHS": (None, [vp, D]),
@@ -131,6 +135,7 @@ class Oracle:
         if not self.h:
             raise ValueError("orc_create rejected the parameters")
         self.M = params.num_bodies
+        self.nb = params.blobs_per_body
         self.Nb = params.num_blobs
         self.n = params.system_size
         self.P = params.nx * params.ny * params.pad
@@ -333,6 +338,28 @@ class Oracle:
                                          _dp(_f64(np.asarray(N).ravel(order="F"))))
 
     # gmres_solver
+    def set_body_shapes(self, shapes):
+        lib().orc_set_body_shapes(self.h, _dp(_f64(shapes, 3 * self.nb * self.M)))
+
+    def produce_body_preconditioners(self):
+        lib().orc_produce_body_preconditioners(self.h)
+
+    def set_body_preconditioners(self, Minv=None, N=None):
+        n3 = 3 * self.nb
+        m = _f64(Minv, n3 * n3 * self.M) if Minv is not None else None
+        n = _f64(N, 36 * self.M) if N is not None else None
+        lib().orc_set_body_preconditioners(self.h, _dp(m) if m is not None else None,
+                                           _dp(n) if n is not None else None)
+
+    def get_body_preconditioners(self):
+        """(Minv, N, KTKinv) as flat column-major blocks, body after body."""
+        n3 = 3 * self.nb
+        Minv = np.zeros(n3 * n3 * self.M)
+        N = np.zeros(36 * self.M)
+        K = np.zeros(36 * self.M)
+        lib().orc_get_body_preconditioners(self.h, _dp(Minv), _dp(N), _dp(K))
+        return Minv, N, K
+
     def assemble_RHS(self):
         lib().orc_assemble_RHS(self.h)
 

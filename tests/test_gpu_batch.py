@@ -101,3 +101,51 @@ def test_batch_long_x_grid_mixed_paths(gpu):
         assert np.max(np.abs(s.get_bodies()[0] - m.get_bodies()[0])) <= 1e-8
         assert np.max(np.abs(s.get_bodies()[1] - m.get_bodies()[1])) <= 1e-8
     b.close()
+
+
+def test_batch_members_against_the_oracle(gpu):
+    """A three-member FP64 batch of uneven suspensions (64^3, 96^3 and 128^3 grids,
+    50 / 150 / 300 rods) against each member's own CPU oracle, not against a solo
+    GPU step: M F through the member context within 1e-10, then three
+    deterministic EM steps of the batch (the lockstep batched spread, projection,
+    interpolation and GMRES kernels inside the step graph from the second step on)
+    against the oracle's steps, bodies within 1e-9 and GMRES iterations within one
+    (gmres_solver.cpp:148-306, fcm_fluid_solver.cpp:363-424, :552-701)."""
+    import os
+
+    from tests.conftest import rel_err
+    from tests.oracle_lib import Oracle, lib
+    lib().orc_set_threads(os.cpu_count() or 1)
+    insts = []
+    for M, grid, phi, seed in ((50, 64, 0.05, 21), (150, 96, 0.10, 22), (300, 128, 0.15, 23)):
+        insts.append(configs.rod_suspension(M=M, grid=grid, phi=phi, seed=seed, gmres_tol=1e-10, noise=0))
+    b = _batch(insts)
+    oracles = []
+    for m, (p, ref, x, q, fe) in zip(b.members, insts):
+        o = Oracle(p, ref)
+        o.set_bodies(x, q)
+        o.set_external_forces(fe)
+        Minv, N, _ = m.get_reference_matrices()
+        o.set_reference_matrices(Minv, N)  # the same preconditioner on both sides
+        oracles.append(o)
+    rng = np.random.default_rng(3)
+    for m, o, (p, *_rest) in zip(b.members, oracles, insts):
+        F = rng.standard_normal(3 * p.num_blobs)
+        for s in (m, o):
+            s.fill_all_blob_pos()
+            s.set_up_gaussians()
+        assert rel_err(m.apply_mobility(F), o.apply_mobility(F)) < 1e-10
+    for k in range(3):
+        infos = b.step([0, 0, 0], k)
+        for i, o in enumerate(oracles):
+            so, io = o.step(0, k)
+            assert so == 0 and infos[i].status == 0
+            assert abs(io.gmres_iters - infos[i].gmres_iters) <= 1, (k, i)
+            xm, qm = b.members[i].get_bodies()
+            xo, qo = o.get_bodies()
+            assert np.abs(xm - xo).max() < 1e-9, (k, i)
+            assert np.abs(qm - qo).max() < 1e-9, (k, i)
+    for o, (p, ref, x, q, fe) in zip(oracles, insts):
+        assert np.abs(o.get_bodies()[0] - x).max() > 1e-5  # the bodies moved
+        o.close()
+    b.close()

@@ -54,6 +54,10 @@ SIGNATURES = {
     "fcm_list_get_pairs": (ctypes.c_int, [VP, VP, ctypes.c_int64, I64]),
     "fcm_apply_barrier_forces": (ctypes.c_int, [VP, VP]),
     "fcm_set_up_gaussians": (ctypes.c_int, [VP, VP]),
+    "fcm_get_gaussians": (ctypes.c_int, [VP, ctypes.c_int32, VP, VP]),
+    "fcm_set_body_shapes": (ctypes.c_int, [VP, VP]),
+    "fcm_set_body_preconditioners": (ctypes.c_int, [VP, VP, VP]),
+    "fcm_get_body_preconditioners": (ctypes.c_int, [VP, VP, VP, VP]),
     "fcm_produce_random_velocity_field": (ctypes.c_int, [VP, ctypes.c_uint64, ctypes.c_uint64]),
     "fcm_inject_random_stress": (ctypes.c_int, [VP, VP, VP, VP, VP, VP, VP]),
     "fcm_calculate_random_blob_velocities": (ctypes.c_int, [VP, VP]),

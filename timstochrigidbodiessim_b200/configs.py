@@ -134,7 +134,7 @@ def _rsa(rng, M, ref, L, min_dist, max_trials=None, max_fail=None, batch=2048, m
         cq = random_unit_quaternions(rng, batch)
         cY = ((cx[:, None, :] + np.einsum("nij,mj->nmi", rotation_matrices(cq), ref)) % L)
         if tree is not None:
-            hit = tree.query_ball_point(cY.reshape(-1, 3), r=min_dist * (1.0 - 1e-12), return_length=True)
+            hit = tree.query_ball_point(cY.reshape(-1, 3), r=min_dist * (1.0 - 1e-12), return_length=True, workers=-1)
             ok = ~(hit.reshape(batch, nb) > 0).any(axis=1)
         else:
             ok = np.ones(batch, dtype=bool)
@@ -247,8 +247,38 @@ def random_walk_cluster(rng, nb=12, bond=2.2 * A, min_dist=2.0 * A, draws=32, ma
     return best
 
 
+def random_walk_clusters(rng, M, nb=12, bond=2.2 * A, min_dist=2.0 * A, draws=4, max_rounds=100000):
+    """M independent random cluster shapes, grown all at once: each starts from a
+    seed blob, and every new blob is bonded at distance `bond` to a randomly
+    chosen earlier blob of its cluster, at least min_dist from all of them (a
+    rejected draw is drawn again); of `draws` clusters grown per shape the most
+    compact (smallest largest distance from the centroid) is kept, re-centred on
+    its centroid.  Returns (M, nb, 3)."""
+    n = M * draws
+    pts = np.zeros((n, nb, 3))
+    rounds = 0
+    for k in range(1, nb):
+        todo = np.arange(n)
+        while len(todo):
+            rounds += 1
+            if rounds > max_rounds:
+                raise RuntimeError("clusters could not grow")
+            j = rng.integers(0, k, len(todo))
+            v = rng.standard_normal((len(todo), 3))
+            c = pts[todo, j] + bond * v / np.linalg.norm(v, axis=1, keepdims=True)
+            d = np.linalg.norm(pts[todo, :k] - c[:, None, :], axis=2).min(axis=1)
+            ok = d >= min_dist * (1.0 - 1e-12)
+            pts[todo[ok], k] = c[ok]
+            todo = todo[~ok]
+    pts -= pts.mean(axis=1, keepdims=True)
+    r = np.linalg.norm(pts, axis=2).max(axis=1).reshape(M, draws)
+    best = r.argmin(axis=1)
+    return pts.reshape(M, draws, nb, 3)[np.arange(M), best]
+
+
 def lattice_start(rng, M, ref, L, min_dist=2.0 * A, tries=16, rounds=12, jitter=0.0):
-    """Bodies of shape ref (nb, 3) near the sites of a cubic lattice of side
+    """Bodies of shape ref (nb, 3) -- or each of its own shape, ref (M, nb, 3) --
+    near the sites of a cubic lattice of side
     M^(1/3) in the box L (each centre within +-jitter spacings of its site),
     each placed and turned to keep its blobs at least min_dist from the blobs of
     the bodies placed before it.  Sites are filled in 27 classes
@@ -257,8 +287,12 @@ def lattice_start(rng, M, ref, L, min_dist=2.0 * A, tries=16, rounds=12, jitter=
     orientation after `rounds` batches of `tries` draws keeps the draw with the
     largest clearance.  Returns x (M, 3), q (M, 4)."""
     from scipy.spatial import cKDTree
-    ref = np.asarray(ref, dtype=np.float64).reshape(-1, 3)
-    nb = len(ref)
+    ref = np.asarray(ref, dtype=np.float64)
+    if ref.ndim == 3:  # (M, nb, 3): one shape per body
+        shapes = ref
+    else:
+        shapes = np.broadcast_to(ref.reshape(1, -1, 3), (M, ref.size // 3, 3))
+    nb = shapes.shape[1]
     side = int(round(M ** (1.0 / 3.0)))
     if side ** 3 != M:
         raise ValueError("M must be a cube for the lattice start")
@@ -282,8 +316,9 @@ def lattice_start(rng, M, ref, L, min_dist=2.0 * A, tries=16, rounds=12, jitter=
             sel = np.nonzero(todo)[0]
             qs = random_unit_quaternions(rng, len(sel) * tries)
             xs = np.repeat(x[mem[sel]], tries, axis=0) + rng.uniform(-jitter, jitter, (len(sel) * tries, 3)) * sp
-            cb = (xs[:, None, :] + np.einsum("tij,nj->tni", rotation_matrices(qs), ref)) % L   # (s*t, nb, 3)
-            dist, _ = tree.query(cb.reshape(-1, 3), k=1)
+            sh = np.repeat(shapes[mem[sel]], tries, axis=0)                                    # (s*t, nb, 3)
+            cb = (xs[:, None, :] + np.einsum("tij,tnj->tni", rotation_matrices(qs), sh)) % L   # (s*t, nb, 3)
+            dist, _ = tree.query(cb.reshape(-1, 3), k=1, workers=-1)
             dist = dist.reshape(len(sel), tries, nb).min(axis=2)
             k = dist.argmax(axis=1)
             dk = dist[np.arange(len(sel)), k]
@@ -294,21 +329,27 @@ def lattice_start(rng, M, ref, L, min_dist=2.0 * A, tries=16, rounds=12, jitter=
             todo[sel] = best_d[sel] < min_dist
         q[mem] = best_q
         x[mem] = best_x % L
-        Yc = (x[mem][:, None, :] + np.einsum("mij,nj->mni", rotation_matrices(best_q), ref)).reshape(-1, 3)
+        Yc = (x[mem][:, None, :] + np.einsum("mij,mnj->mni", rotation_matrices(best_q), shapes[mem])).reshape(-1, 3)
         placed_Y = np.concatenate([placed_Y, Yc])
     return x, q
 
 
 def cluster_suspension(M, grid, phi, nb=12, seed=1234, gmres_tol=1e-10, gmres_max_iter=100, dt=0.01, kT=1.0,
-                       noise=1, algorithm=2, precision=0, ngauss=20):
-    """M rigid bodies of one random cluster shape (random_walk_cluster; the
-    bodies of a collection share blob_ref_pos, as collection_of_rigid_bodies.hpp
-    has one) at volume fraction phi: centres on a cubic lattice (side M^(1/3)),
-    orientations drawn to clear the neighbours (lattice_start); what overlap
-    remains is left to the Metropolis equilibration.  Params, blob_ref_pos, x,
-    q and external forces."""
+                       noise=1, algorithm=2, precision=0, ngauss=20, per_body=True):
+    """M rigid random clusters of nb blobs at volume fraction phi.  With per_body
+    (the default) every body has its own shape (random_walk_clusters), and the
+    returned blob_ref_pos holds 3*nb values per body (set on a context with
+    set_body_shapes, see make_suspension); otherwise one shape
+    (random_walk_cluster, the most compact of 32 draws) is shared by all bodies, as
+    the reference's collection has one blob_ref_pos.  Centres on a cubic lattice
+    (side M^(1/3)), orientations drawn to clear the neighbours (lattice_start);
+    what overlap remains is left to the Metropolis equilibration.  Params,
+    blob_ref_pos, x, q and external forces."""
     rng = np.random.default_rng(seed)
-    ref = random_walk_cluster(rng, nb)
+    if per_body:
+        shapes = random_walk_clusters(rng, M, nb)
+    else:
+        shapes = random_walk_cluster(rng, nb)
     Nb = M * nb
     L = box_for_volume_fraction(Nb, phi)
     rc = 2.2 * A
@@ -318,10 +359,33 @@ def cluster_suspension(M, grid, phi, nb=12, seed=1234, gmres_tol=1e-10, gmres_ma
                            potential=3, steric_fs=40.0 * kT / A, steric_rc=rc, gmres_max_iter=gmres_max_iter,
                            gmres_tol=gmres_tol, fd_delta=1e-5, algorithm=algorithm, precision=precision,
                            noise=noise, skip_on_overlap=0)
-    x, q = lattice_start(rng, M, ref, L)
+    x, q = lattice_start(rng, M, shapes, L)
     fe = np.zeros(6 * M)
     fe[2::6] = -1.0
-    return p, ref.ravel(), x.ravel(), q.ravel(), fe
+    return p, shapes.ravel(), x.ravel(), q.ravel(), fe
+
+
+def has_body_shapes(p, ref):
+    """Whether blob_ref_pos `ref` holds one shape per body (3*nb*M values) rather
+    than the single shared shape (3*nb)."""
+    n = np.asarray(ref).size
+    return p.num_bodies > 1 and n == 3 * p.blobs_per_body * p.num_bodies
+
+
+def make_suspension(p, ref, stream=None, cls=None):
+    """A context (Suspension, or `cls`, e.g. the oracle) for params p and
+    blob_ref_pos ref: the shared shape, or per-body shapes set with
+    set_body_shapes (the oracle then also forms its per-body preconditioner)."""
+    if cls is None:
+        from .fcm import Suspension
+        s = Suspension(p, np.asarray(ref).ravel()[:3 * p.blobs_per_body], stream=stream)
+    else:
+        s = cls(p, np.asarray(ref).ravel()[:3 * p.blobs_per_body])
+    if has_body_shapes(p, ref):
+        s.set_body_shapes(np.asarray(ref).ravel())
+        if hasattr(s, "produce_body_preconditioners"):
+            s.produce_body_preconditioners()
+    return s
 
 
 # The benchmark workloads (sizes as stated; synthetic, seeded).
@@ -354,8 +418,7 @@ def workload(name, **overrides):
 def equilibrate(p, ref, x, q, steps, seed=1234, stream=None):
     """Metropolis equilibration on the GPU (fcm_mcmc_run, main.cpp:113-210) of
     bodies x, q; returns the new (x, q) and the final fcm_mcmc_state."""
-    from .fcm import Suspension
-    s = Suspension(p, ref, stream=stream)
+    s = make_suspension(p, ref, stream=stream)
     try:
         s.set_bodies(x, q)
         st = s.mcmc_run(seed, steps)
@@ -384,6 +447,12 @@ def ensemble_member(i, seed0=0, nb=6, gmres_tol=1e-10, dt=0.01, precision=0, **k
     p, ref, x, q, fe = rod_suspension(M=M, grid=grid, L=L, nb=nb, seed=seed0 + i, gmres_tol=gmres_tol, dt=dt,
                                       precision=precision, **kw)
     return p.as_dict(), ref, x, q, fe
+
+
+def ensemble_body_counts(n_instances=64, seed0=0):
+    """Body count of every ensemble instance (the first draw of ensemble_member),
+    without building the instances."""
+    return [int(np.random.default_rng(seed0 + i).integers(50, 501)) for i in range(n_instances)]
 
 
 def ensemble(n_instances=64, seed0=0, workers=1, **kw):

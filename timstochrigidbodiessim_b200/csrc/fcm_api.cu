@@ -8,6 +8,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <nvtx3/nvToolsExt.h>
@@ -112,6 +113,10 @@ namespace {
 const double PI = 3.14159265358979323846264338327950288;
 
 // ------------------------------------------------------------------ helpers
+// True for memory the kernels of the current device may use in place: device
+// memory of the current device, or managed memory.  Device memory of another GPU
+// is not: it goes through the copy path (cudaMemcpyDefault copies between
+// devices), so no kernel of this device dereferences another GPU's memory.
 bool is_device_ptr(const void* p) {
   if (!p) return false;
   cudaPointerAttributes a;
@@ -119,7 +124,14 @@ bool is_device_ptr(const void* p) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeManaged) return true;
+  if (a.type != cudaMemoryTypeDevice) return false;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.device == dev;
 }
 
 int copy_in(Ctx* c, void* dst, const void* src, size_t bytes) {
@@ -233,6 +245,103 @@ std::vector<double> reference_K(const std::vector<double>& ref, int nb) {
       for (int j = 0; j < 3; ++j) K[(size_t)(3 + j) * n3 + 3 * m + i] = C[i][j];
   }
   return K;
+}
+
+// K^T K of a shape (6x6, column-major).
+std::vector<double> shape_KTK(const std::vector<double>& K, int nb) {
+  const int n3 = 3 * nb;
+  std::vector<double> KTK(36, 0.0);
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) {
+      double s = 0.0;
+      for (int t = 0; t < n3; ++t) s += K[(size_t)i * n3 + t] * K[(size_t)j * n3 + t];
+      KTK[(size_t)j * 6 + i] = s;
+    }
+  return KTK;
+}
+
+// Free-space FCM mobility between two blobs whose force envelopes are Gaussians of
+// variance sigma^2 = a^2/pi per dimension (the envelope of fcm_fluid_solver.cpp:
+// 135-136).  The Stokes flow of one Gaussian force density, averaged over the
+// other Gaussian, is the Stokeslet regularised by a Gaussian of variance
+// s^2 = 2 sigma^2.  Writing u = (1/eta)(-phi I + grad grad psi) F with
+// lap phi = Gaussian and lap psi = phi gives
+//   M(r) = [A(r) I + B(r) r r^T / r^2] / (8 pi eta r),
+//   A = (1 + s^2/r^2) erf(r / (sqrt2 s)) - sqrt(2/pi) (s/r) exp(-r^2 / (2 s^2)),
+//   B = (1 - 3 s^2/r^2) erf(r / (sqrt2 s)) + 3 sqrt(2/pi) (s/r) exp(-r^2 / (2 s^2)),
+// which tends to the Oseen tensor far away and to I / (6 pi eta a) as r -> 0.
+void fcm_pair_mobility(const double* d, double a, double eta, double out[3][3]) {
+  const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+  const double s = std::sqrt(2.0) * a / std::sqrt(PI);
+  const double self = 1.0 / (6.0 * PI * eta * a);
+  if (r2 < 1e-20 * s * s) {
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) out[i][j] = i == j ? self : 0.0;
+    return;
+  }
+  const double r = std::sqrt(r2), sr = s / r, x = r / (std::sqrt(2.0) * s);
+  const double er = std::erf(x), ex = std::sqrt(2.0 / PI) * sr * std::exp(-x * x);
+  const double A = (1.0 + sr * sr) * er - ex, B = (1.0 - 3.0 * sr * sr) * er + 3.0 * ex;
+  const double f = 1.0 / (8.0 * PI * eta * r);
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) out[i][j] = f * ((i == j ? A : 0.0) + B * d[i] * d[j] / r2);
+}
+
+// Preconditioner blocks of one body shape (body frame): ref_Minv = inverse of the
+// shape's blob-blob mobility (fcm_pair_mobility between every pair of its blobs),
+// ref_N = inv(K^T ref_Minv K) and ref_KTKinv = inv(K^T K)
+// (collection_of_rigid_bodies.cpp:117-130, fcm_fluid_solver.cpp:866-877 with the
+// analytic mobility in place of the probed one).
+bool body_preconditioner(const double* shape, int nb, double a, double eta, double* Minv_out, double* N_out,
+                         double* KTKinv_out) {
+  const int n3 = 3 * nb;
+  std::vector<double> ref(shape, shape + n3), Mb((size_t)n3 * n3), Minv, N, KTKinv;
+  for (int i = 0; i < nb; ++i)
+    for (int j = 0; j < nb; ++j) {
+      const double d[3] = {ref[3 * i] - ref[3 * j], ref[3 * i + 1] - ref[3 * j + 1], ref[3 * i + 2] - ref[3 * j + 2]};
+      double m[3][3];
+      fcm_pair_mobility(d, a, eta, m);
+      for (int p = 0; p < 3; ++p)
+        for (int q = 0; q < 3; ++q) Mb[(size_t)(3 * j + q) * n3 + 3 * i + p] = m[p][q];
+    }
+  if (!dense_inv_sympd(Mb, n3, Minv)) return false;
+  const std::vector<double> K = reference_K(ref, nb);
+  std::vector<double> KtMK(36, 0.0), t(n3);
+  for (int j = 0; j < 6; ++j) {
+    for (int i = 0; i < n3; ++i) {
+      double sum = 0.0;
+      for (int k = 0; k < n3; ++k) sum += Minv[(size_t)k * n3 + i] * K[(size_t)j * n3 + k];
+      t[i] = sum;
+    }
+    for (int i = 0; i < 6; ++i) {
+      double sum = 0.0;
+      for (int r = 0; r < n3; ++r) sum += K[(size_t)i * n3 + r] * t[r];
+      KtMK[(size_t)j * 6 + i] = sum;
+    }
+  }
+  if (!sym_inv_or_pinv(KtMK, 6, N, nullptr)) return false;
+  if (!sym_inv_or_pinv(shape_KTK(K, nb), 6, KTKinv, nullptr)) return false;
+  std::copy(Minv.begin(), Minv.end(), Minv_out);
+  std::copy(N.begin(), N.end(), N_out);
+  std::copy(KTKinv.begin(), KTKinv.end(), KTKinv_out);
+  return true;
+}
+
+// f(lo, hi) over [0, n) on the host's hardware threads.
+template <class F>
+void parallel_ranges(long long n, F&& f) {
+  const int nt = (int)std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+  if (nt == 1 || n < 64) {
+    f(0LL, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const long long chunk = (n + nt - 1) / nt;
+  for (int t = 0; t < nt; ++t) {
+    const long long lo = t * chunk, hi = std::min(n, lo + chunk);
+    if (lo < hi) th.emplace_back([&f, lo, hi] { f(lo, hi); });
+  }
+  for (auto& x : th) x.join();
 }
 
 // ------------------------------------------------------------------ cuFFT exec
@@ -1324,14 +1433,7 @@ int create_ctx(const fcm_params* p, const double* ref, Ctx** out) {
   // ref_KTKinv = inv(K^T K) (collection_of_rigid_bodies.cpp:117-130)
   {
     const std::vector<double> K = reference_K(href, nb);
-    std::vector<double> KTK(36, 0.0);
-    for (int i = 0; i < 6; ++i)
-      for (int j = 0; j < 6; ++j) {
-        double s = 0.0;
-        for (int t = 0; t < n3; ++t) s += K[(size_t)i * n3 + t] * K[(size_t)j * n3 + t];
-        KTK[(size_t)j * 6 + i] = s;
-      }
-    if (!sym_inv_or_pinv(KTK, 6, c->h_KTKinv, nullptr)) {
+    if (!sym_inv_or_pinv(shape_KTK(K, nb), 6, c->h_KTKinv, nullptr)) {
       set_error("K^T K of the body shape could not be inverted");
       return fail(FCM_ERR_INVALID);
     }
@@ -2237,6 +2339,9 @@ int create_batch(int n, const fcm_params* params, const double* const* refs, Bat
     m.ref = c->d_ref;
     m.Minv = c->d_Minv;
     m.N = c->d_N;
+    m.ref_stride = c->ref_stride;
+    m.minv_stride = c->minv_stride;
+    m.n_stride = c->n_stride;
     m.sys_a = c->d_sys_a;
     m.sys_b = c->d_sys_b;
     m.rhs = c->d_rhs;
@@ -2777,6 +2882,51 @@ int fcm_set_up_gaussians(fcm_ctx* ctx, const double* Y) {
   return set_up_gaussians_dev(c, c->d_Y);
 }
 
+int fcm_get_gaussians(fcm_ctx* ctx, int32_t precision, int32_t* ind, double* w) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  if (!c->gauss_ready) {
+    set_error("fcm_get_gaussians: set_up_gaussians must come first");
+    return FCM_ERR_STATE;
+  }
+  if (precision != 0 && !(precision == 1 && c->p.precision == 1)) {
+    set_error("fcm_get_gaussians: precision must be 0, or 1 in a context of precision 1");
+    return FCM_ERR_INVALID;
+  }
+  const int n = c->Nb;
+  const int W = precision == 0 ? c->g64.blobs.W : c->g32.blobs.W;
+  const int* d_base = precision == 0 ? c->g64.blobs.base : c->g32.blobs.base;
+  std::vector<int> base(3 * (size_t)n);
+  FCM_CUDA(cudaMemcpyAsync(base.data(), d_base, sizeof(int) * base.size(), cudaMemcpyDeviceToHost, c->stream));
+  std::vector<double> wt;
+  if (w) {
+    wt.resize(3 * (size_t)n * W);
+    if (precision == 0) {
+      FCM_CUDA(cudaMemcpyAsync(wt.data(), c->g64.blobs.w, sizeof(double) * wt.size(), cudaMemcpyDeviceToHost,
+                               c->stream));
+    } else {
+      std::vector<float> wf(wt.size());
+      FCM_CUDA(cudaMemcpyAsync(wf.data(), c->g32.blobs.w, sizeof(float) * wf.size(), cudaMemcpyDeviceToHost,
+                               c->stream));
+      FCM_CUDA(cudaStreamSynchronize(c->stream));
+      for (size_t i = 0; i < wf.size(); ++i) wt[i] = wf[i];
+    }
+  }
+  FCM_CUDA(cudaStreamSynchronize(c->stream));
+  const int nd[3] = {c->g.nx, c->g.ny, c->g.nz};
+  for (int b = 0; b < n; ++b)
+    for (int d = 0; d < 3; ++d) {
+      const size_t row = (3 * (size_t)b + d) * W;
+      for (int i = 0; i < W; ++i) {
+        const int xg = base[3 * (size_t)b + d] + i;  // fcm_fluid_solver.cpp:141-151
+        const int r = xg % nd[d];
+        if (ind) ind[row + i] = r < 0 ? r + nd[d] : r;
+        if (w) w[row + i] = wt[row + i];
+      }
+    }
+  return FCM_OK;
+}
+
 int fcm_produce_random_velocity_field(fcm_ctx* ctx, uint64_t seed, uint64_t counter) {
   CTX_CHECK(ctx);
   return noise_dev(ctx->c, seed, counter);
@@ -3131,14 +3281,25 @@ int fcm_autotune(fcm_ctx* ctx, int32_t reps, double* us, int32_t* variants) {
   });
 }
 
+namespace {
+int refuse_per_body(const Ctx* c, const char* what) {
+  if (!c->per_body) return FCM_OK;
+  set_error(std::string(what) + ": the context has per-body shapes (fcm_set_body_shapes); use "
+                                "fcm_set_body_preconditioners / fcm_get_body_preconditioners");
+  return FCM_ERR_STATE;
+}
+}  // namespace
+
 int fcm_produce_reference_matrices(fcm_ctx* ctx) {
   CTX_CHECK(ctx);
+  FCM_TRY(refuse_per_body(ctx->c, "fcm_produce_reference_matrices"));
   return guard([&] { return reference_matrices_dev(ctx->c); });
 }
 
 int fcm_get_reference_matrices(fcm_ctx* ctx, double* Minv, double* N, double* KTKinv) {
   CTX_CHECK(ctx);
   Ctx* c = ctx->c;
+  FCM_TRY(refuse_per_body(c, "fcm_get_reference_matrices"));
   const int n3 = 3 * c->nb;
   if (Minv) std::memcpy(Minv, c->h_Minv.data(), sizeof(double) * n3 * n3);
   if (N) std::memcpy(N, c->h_N.data(), sizeof(double) * 36);
@@ -3149,6 +3310,7 @@ int fcm_get_reference_matrices(fcm_ctx* ctx, double* Minv, double* N, double* KT
 int fcm_set_reference_matrices(fcm_ctx* ctx, const double* Minv, const double* N) {
   CTX_CHECK(ctx);
   Ctx* c = ctx->c;
+  FCM_TRY(refuse_per_body(c, "fcm_set_reference_matrices"));
   const int n3 = 3 * c->nb;
   FCM_CUDA(cudaStreamSynchronize(c->stream));
   if (Minv) {
@@ -3161,6 +3323,136 @@ int fcm_set_reference_matrices(fcm_ctx* ctx, const double* Minv, const double* N
   }
   FCM_CUDA(cudaStreamSynchronize(c->stream));
   c->have_ref = true;
+  return FCM_OK;
+}
+
+// ------------------------------------------------------------------ per-body shapes
+namespace {
+// Drop every captured graph that holds the shape or preconditioner pointers.
+void drop_graphs(Ctx* c) {
+  for (int i = 0; i < 2; ++i)
+    if (c->iter_graph[i]) {
+      cudaGraphExecDestroy(c->iter_graph[i]);
+      c->iter_graph[i] = nullptr;
+    }
+  if (c->mcmc_graph) {
+    cudaGraphExecDestroy(c->mcmc_graph);
+    c->mcmc_graph = nullptr;
+  }
+  c->graph_stale = true;
+}
+}  // namespace
+
+int fcm_set_body_shapes(fcm_ctx* ctx, const double* shapes) {
+  CTX_CHECK(ctx);
+  return guard([&] {
+    Ctx* c = ctx->c;
+    if (!shapes) {
+      set_error("fcm_set_body_shapes: shapes is NULL");
+      return (int)FCM_ERR_INVALID;
+    }
+    if (c->in_batch) {
+      set_error("fcm_set_body_shapes: not available to batch members");
+      return (int)FCM_ERR_STATE;
+    }
+    if (c->step_pending) {
+      set_error("fcm_set_body_shapes: a step is in flight on this context");
+      return (int)FCM_ERR_STATE;
+    }
+    const int M = c->M, nb = c->nb, n3 = 3 * nb;
+    std::vector<double> hs((size_t)n3 * M);
+    FCM_CUDA(cudaStreamSynchronize(c->stream));
+    FCM_CUDA(cudaMemcpy(hs.data(), shapes, sizeof(double) * hs.size(), cudaMemcpyDefault));
+    for (double v : hs)
+      if (!std::isfinite(v)) {
+        set_error("fcm_set_body_shapes: non-finite coordinate");
+        return (int)FCM_ERR_INVALID;
+      }
+    std::vector<double> Minv((size_t)M * n3 * n3), N(36 * (size_t)M), KTKinv(36 * (size_t)M);
+    std::atomic<long long> bad{-1};
+    const double a = c->p.blob_radius, eta = c->p.viscosity;
+    parallel_ranges(M, [&](long long lo, long long hi) {
+      for (long long n = lo; n < hi; ++n)
+        if (!body_preconditioner(&hs[(size_t)n * n3], nb, a, eta, &Minv[(size_t)n * n3 * n3], &N[36 * (size_t)n],
+                                 &KTKinv[36 * (size_t)n]))
+          bad = n;
+    });
+    if (bad >= 0) {
+      set_error("fcm_set_body_shapes: the preconditioner of body " + std::to_string(bad.load()) +
+                " could not be formed (coincident blobs?)");
+      return (int)FCM_ERR_INVALID;
+    }
+    double *d_ref = nullptr, *d_Minv = nullptr, *d_N = nullptr, *d_KTKinv = nullptr;
+    auto release = [&] {
+      cudaFree(d_ref);
+      cudaFree(d_Minv);
+      cudaFree(d_N);
+      cudaFree(d_KTKinv);
+    };
+    if (dev_alloc(&d_ref, hs.size()) || dev_alloc(&d_Minv, Minv.size()) || dev_alloc(&d_N, N.size()) ||
+        dev_alloc(&d_KTKinv, KTKinv.size())) {
+      release();
+      set_error("fcm_set_body_shapes: device allocation failed");
+      return (int)FCM_ERR_NOMEM;
+    }
+    if (cudaMemcpy(d_ref, hs.data(), sizeof(double) * hs.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(d_Minv, Minv.data(), sizeof(double) * Minv.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(d_N, N.data(), sizeof(double) * N.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(d_KTKinv, KTKinv.data(), sizeof(double) * KTKinv.size(), cudaMemcpyHostToDevice) !=
+            cudaSuccess) {
+      release();
+      set_error("fcm_set_body_shapes: copy to the device failed");
+      return (int)FCM_ERR_CUDA;
+    }
+    drop_graphs(c);
+    cudaFree(c->d_ref);
+    cudaFree(c->d_Minv);
+    cudaFree(c->d_N);
+    cudaFree(c->d_KTKinv);
+    c->d_ref = d_ref;
+    c->d_Minv = d_Minv;
+    c->d_N = d_N;
+    c->d_KTKinv = d_KTKinv;
+    c->per_body = true;
+    c->ref_stride = n3;
+    c->minv_stride = (long long)n3 * n3;
+    c->n_stride = 36;
+    // the Metropolis rotation scale: the largest |r| over every shape
+    // (collection_of_rigid_bodies.cpp:110-114 over all bodies)
+    c->body_radius = 0.0;
+    for (size_t m = 0; m < hs.size(); m += 3)
+      c->body_radius = std::max(c->body_radius, std::sqrt(hs[m] * hs[m] + hs[m + 1] * hs[m + 1] + hs[m + 2] * hs[m + 2]));
+    c->have_ref = true;
+    return (int)FCM_OK;
+  });
+}
+
+int fcm_set_body_preconditioners(fcm_ctx* ctx, const double* Minv, const double* N) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  if (!c->per_body) {
+    set_error("fcm_set_body_preconditioners: call fcm_set_body_shapes first");
+    return FCM_ERR_STATE;
+  }
+  const size_t n3 = 3 * (size_t)c->nb;
+  FCM_CUDA(cudaStreamSynchronize(c->stream));
+  if (Minv) FCM_CUDA(cudaMemcpy(c->d_Minv, Minv, sizeof(double) * n3 * n3 * c->M, cudaMemcpyDefault));
+  if (N) FCM_CUDA(cudaMemcpy(c->d_N, N, sizeof(double) * 36 * c->M, cudaMemcpyDefault));
+  return FCM_OK;
+}
+
+int fcm_get_body_preconditioners(fcm_ctx* ctx, double* Minv, double* N, double* KTKinv) {
+  CTX_CHECK(ctx);
+  Ctx* c = ctx->c;
+  if (!c->per_body) {
+    set_error("fcm_get_body_preconditioners: call fcm_set_body_shapes first");
+    return FCM_ERR_STATE;
+  }
+  const size_t n3 = 3 * (size_t)c->nb;
+  FCM_CUDA(cudaStreamSynchronize(c->stream));
+  if (Minv) FCM_CUDA(cudaMemcpy(Minv, c->d_Minv, sizeof(double) * n3 * n3 * c->M, cudaMemcpyDefault));
+  if (N) FCM_CUDA(cudaMemcpy(N, c->d_N, sizeof(double) * 36 * c->M, cudaMemcpyDefault));
+  if (KTKinv) FCM_CUDA(cudaMemcpy(KTKinv, c->d_KTKinv, sizeof(double) * 36 * c->M, cudaMemcpyDefault));
   return FCM_OK;
 }
 

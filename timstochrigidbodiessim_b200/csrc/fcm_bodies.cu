@@ -54,16 +54,17 @@ __device__ __forceinline__ void cross3(const double* a, const double* b, double*
 }
 
 // collection_of_rigid_bodies.cpp:155-193: Y = x + R r_m, wrapped p - L floor(p/L).
+// Body n's shape starts at ref + n*rs (rs = 0: one shape shared by all bodies).
 __global__ void k_fill_blob_pos(const double* __restrict__ x, const double* __restrict__ q,
-                                const double* __restrict__ ref, int Nb, int nb, double Lx, double Ly, double Lz,
-                                double* __restrict__ Y) {
+                                const double* __restrict__ ref, int rs, int Nb, int nb, double Lx, double Ly,
+                                double Lz, double* __restrict__ Y) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= Nb) return;
   const int n = i / nb, m = i - n * nb;
   double R[3][3];
   quat_matrix(q + 4 * n, R);
   double r[3];
-  rot(R, ref + 3 * m, r);
+  rot(R, ref + (size_t)n * rs + 3 * m, r);
   const double L[3] = {Lx, Ly, Lz};
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -73,14 +74,14 @@ __global__ void k_fill_blob_pos(const double* __restrict__ x, const double* __re
 }
 
 // collection_of_rigid_bodies.cpp:707-731: out_m (+)= U + Omega x (R r_m).
-__device__ __forceinline__ void multiply_K_one(const double* __restrict__ q, const double* __restrict__ ref,
+__device__ __forceinline__ void multiply_K_one(const double* __restrict__ q, const double* __restrict__ ref, int rs,
                                                const double* __restrict__ in, double* __restrict__ out, int i,
                                                int nb, int subtract) {
   const int n = i / nb, m = i - n * nb;
   double R[3][3];
   quat_matrix(q + 4 * n, R);
   double r[3], c[3];
-  rot(R, ref + 3 * m, r);
+  rot(R, ref + (size_t)n * rs + 3 * m, r);
   cross3(in + 6 * n + 3, r, c);
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -89,21 +90,22 @@ __device__ __forceinline__ void multiply_K_one(const double* __restrict__ q, con
   }
 }
 
-__global__ void k_multiply_K(const double* __restrict__ q, const double* __restrict__ ref, const double* __restrict__ in,
-                             double* __restrict__ out, int Nb, int nb, int subtract) {
+__global__ void k_multiply_K(const double* __restrict__ q, const double* __restrict__ ref, int rs,
+                             const double* __restrict__ in, double* __restrict__ out, int Nb, int nb, int subtract) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= Nb) return;
-  multiply_K_one(q, ref, in, out, i, nb, subtract);
+  multiply_K_one(q, ref, rs, in, out, i, nb, subtract);
 }
 
 // collection_of_rigid_bodies.cpp:733-757: F = sum lambda_m, T = sum (R r_m) x lambda_m;
 // out = scale * K^T in + add_scale * add.
-__device__ __forceinline__ void multiply_KT_one(const double* __restrict__ q, const double* __restrict__ ref,
+__device__ __forceinline__ void multiply_KT_one(const double* __restrict__ q, const double* __restrict__ ref, int rs,
                                                 const double* __restrict__ in, double* __restrict__ out, int n,
                                                 int nb, double scale, const double* __restrict__ add,
                                                 double add_scale) {
   double R[3][3];
   quat_matrix(q + 4 * n, R);
+  ref += (size_t)n * rs;
   double acc[6] = {0, 0, 0, 0, 0, 0};
   for (int m = 0; m < nb; ++m) {
     const double* l = in + 3 * (n * nb + m);
@@ -120,12 +122,12 @@ __device__ __forceinline__ void multiply_KT_one(const double* __restrict__ q, co
   for (int d = 0; d < 6; ++d) out[6 * n + d] = scale * acc[d] + (add ? add_scale * add[6 * n + d] : 0.0);
 }
 
-__global__ void k_multiply_KT(const double* __restrict__ q, const double* __restrict__ ref,
+__global__ void k_multiply_KT(const double* __restrict__ q, const double* __restrict__ ref, int rs,
                               const double* __restrict__ in, double* __restrict__ out, int M, int nb, double scale,
                               const double* __restrict__ add, double add_scale) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= M) return;
-  multiply_KT_one(q, ref, in, out, n, nb, scale, add, add_scale);
+  multiply_KT_one(q, ref, rs, in, out, n, nb, scale, add, add_scale);
 }
 
 // gmres_solver.cpp:85-146, one warp per body, applied in the body frame:
@@ -133,9 +135,11 @@ __global__ void k_multiply_KT(const double* __restrict__ q, const double* __rest
 // matrices are B ref_Minv B^T, K_rot = B K_ref C and C^T ref_N C, so
 //   U' = ref_N (-C in_U - K_ref^T ref_Minv B^T in_l),   out_U = C^T U'
 //   out_l = B ref_Minv (K_ref U' + B^T in_l).
-// Shared memory per warp: 2*(3nb) + 12 doubles.
-__device__ __forceinline__ void pinv_block(const double* __restrict__ q, const double* __restrict__ ref,
-                                           const double* __restrict__ Minv, const double* __restrict__ Nm,
+// Shared memory per warp: 2*(3nb) + 12 doubles.  With per-body shapes body n's
+// shape, ref_Minv and ref_N start at ref + n*rs, Minv + n*ms and Nm + n*ns.
+__device__ __forceinline__ void pinv_block(const double* __restrict__ q, const double* __restrict__ ref, int rs,
+                                           const double* __restrict__ Minv, long long ms,
+                                           const double* __restrict__ Nm, int ns,
                                            const double* __restrict__ in, double* __restrict__ out, int M, int nb,
                                            int Nb, double* sm) {
   const int warps = blockDim.x >> 5;
@@ -146,6 +150,9 @@ __device__ __forceinline__ void pinv_block(const double* __restrict__ q, const d
   double* t = xl + n3;                           // Minv * lambda'
   double* u = t + n3;                            // 12: in_U' (6), U' (6)
   if (n >= M) return;
+  ref += (size_t)n * rs;
+  Minv += (size_t)n * ms;
+  Nm += (size_t)n * ns;
   double R[3][3];
   quat_matrix(q + 4 * n, R);
   const double* inl = in + (size_t)n3 * n;
@@ -200,20 +207,23 @@ __device__ __forceinline__ void pinv_block(const double* __restrict__ q, const d
   for (int m = lane; m < nb; m += 32) rot(R, t + 3 * m, ol + 3 * m);
 }
 
-__global__ void k_pinv(const double* __restrict__ q, const double* __restrict__ ref, const double* __restrict__ Minv,
-                       const double* __restrict__ Nm, const double* __restrict__ in, double* __restrict__ out, int M,
-                       int nb, int Nb) {
+__global__ void k_pinv(const double* __restrict__ q, const double* __restrict__ ref, int rs,
+                       const double* __restrict__ Minv, long long ms, const double* __restrict__ Nm, int ns,
+                       const double* __restrict__ in, double* __restrict__ out, int M, int nb, int Nb) {
   extern __shared__ double sm[];
-  pinv_block(q, ref, Minv, Nm, in, out, M, nb, Nb, sm);
+  pinv_block(q, ref, rs, Minv, ms, Nm, ns, in, out, M, nb, Nb, sm);
 }
 
 // Rigid projection of blob velocities with ref_KTKinv
-// (collection_of_rigid_bodies.cpp:580-600, :909-939).
-__global__ void k_rigid_projection(const double* __restrict__ q, const double* __restrict__ ref,
-                                   const double* __restrict__ KTKinv, const double* __restrict__ V,
+// (collection_of_rigid_bodies.cpp:580-600, :909-939); per-body shapes carry their
+// own ref_KTKinv (strides rs, ks).
+__global__ void k_rigid_projection(const double* __restrict__ q, const double* __restrict__ ref, int rs,
+                                   const double* __restrict__ KTKinv, int ks, const double* __restrict__ V,
                                    double* __restrict__ U, int M, int nb) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= M) return;
+  ref += (size_t)n * rs;
+  KTKinv += (size_t)n * ks;
   double R[3][3];
   quat_matrix(q + 4 * n, R);
   double b[6] = {0, 0, 0, 0, 0, 0};
@@ -326,7 +336,7 @@ __global__ void k_divU_terms(const double* __restrict__ U, const double* __restr
 
 int launch_fill_blob_pos(const Ctx& c, const double* x, const double* q, double* Y, cudaStream_t s) {
   if (c.Nb == 0) return FCM_OK;
-  k_fill_blob_pos<<<(c.Nb + 127) / 128, 128, 0, s>>>(x, q, c.d_ref, c.Nb, c.nb, c.g.Lx, c.g.Ly, c.g.Lz, Y);
+  k_fill_blob_pos<<<(c.Nb + 127) / 128, 128, 0, s>>>(x, q, c.d_ref, c.ref_stride, c.Nb, c.nb, c.g.Lx, c.g.Ly, c.g.Lz, Y);
   FCM_LAUNCH_CHECK();
   return FCM_OK;
 }
@@ -334,7 +344,7 @@ int launch_fill_blob_pos(const Ctx& c, const double* x, const double* q, double*
 int launch_multiply_K(const Ctx& c, const double* qm, const double* in6, double* out3, double subtract,
                       cudaStream_t s) {
   if (c.Nb == 0) return FCM_OK;
-  k_multiply_K<<<(c.Nb + 127) / 128, 128, 0, s>>>(qm, c.d_ref, in6, out3, c.Nb, c.nb, subtract != 0.0 ? 1 : 0);
+  k_multiply_K<<<(c.Nb + 127) / 128, 128, 0, s>>>(qm, c.d_ref, c.ref_stride, in6, out3, c.Nb, c.nb, subtract != 0.0 ? 1 : 0);
   FCM_LAUNCH_CHECK();
   return FCM_OK;
 }
@@ -342,7 +352,7 @@ int launch_multiply_K(const Ctx& c, const double* qm, const double* in6, double*
 int launch_multiply_KT(const Ctx& c, const double* qm, const double* in3, double* out6, double scale,
                        const double* add6, double add_scale, cudaStream_t s) {
   if (c.M == 0) return FCM_OK;
-  k_multiply_KT<<<(c.M + 127) / 128, 128, 0, s>>>(qm, c.d_ref, in3, out6, c.M, c.nb, scale, add6, add_scale);
+  k_multiply_KT<<<(c.M + 127) / 128, 128, 0, s>>>(qm, c.d_ref, c.ref_stride, in3, out6, c.M, c.nb, scale, add6, add_scale);
   FCM_LAUNCH_CHECK();
   return FCM_OK;
 }
@@ -351,14 +361,16 @@ int launch_pinv(const Ctx& c, const double* qm, const double* in, double* out, c
   if (c.M == 0) return FCM_OK;
   const int warps = 4;
   const size_t shm = sizeof(double) * warps * (size_t)(6 * c.nb + 12);
-  k_pinv<<<(c.M + warps - 1) / warps, 32 * warps, shm, s>>>(qm, c.d_ref, c.d_Minv, c.d_N, in, out, c.M, c.nb, c.Nb);
+  k_pinv<<<(c.M + warps - 1) / warps, 32 * warps, shm, s>>>(qm, c.d_ref, c.ref_stride, c.d_Minv, c.minv_stride, c.d_N,
+                                                                 c.n_stride, in, out, c.M, c.nb, c.Nb);
   FCM_LAUNCH_CHECK();
   return FCM_OK;
 }
 
 int launch_rigid_projection(const Ctx& c, const double* q, const double* V, double* U6, cudaStream_t s) {
   if (c.M == 0) return FCM_OK;
-  k_rigid_projection<<<(c.M + 127) / 128, 128, 0, s>>>(q, c.d_ref, c.d_KTKinv, V, U6, c.M, c.nb);
+  k_rigid_projection<<<(c.M + 127) / 128, 128, 0, s>>>(q, c.d_ref, c.ref_stride, c.d_KTKinv, c.n_stride, V, U6,
+                                                       c.M, c.nb);
   FCM_LAUNCH_CHECK();
   return FCM_OK;
 }
@@ -411,7 +423,8 @@ __global__ void k_b_pinv(const BMember* __restrict__ mem, int in, int out, int m
   extern __shared__ double sm[];
   const BMember& m = mem[blockIdx.y];
   if (bskip(m, mask)) return;
-  pinv_block(m.qm, m.ref, m.Minv, m.N, bvec(m, in), bvec(m, out), m.M, m.nb, m.Nb, sm);
+  pinv_block(m.qm, m.ref, m.ref_stride, m.Minv, m.minv_stride, m.N, m.n_stride, bvec(m, in), bvec(m, out), m.M,
+             m.nb, m.Nb, sm);
 }
 
 // out[lambda] -= K in[U] (blocks [0, blob_blocks)) and out[U] = -K^T in[lambda]
@@ -423,10 +436,10 @@ __global__ void k_b_K_KT(const BMember* __restrict__ mem, int in, int out, int b
   double* y = bvec(m, out);
   if ((int)blockIdx.x < blob_blocks) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < m.Nb) multiply_K_one(m.qm, m.ref, x + 3 * (size_t)m.Nb, y, i, m.nb, 1);
+    if (i < m.Nb) multiply_K_one(m.qm, m.ref, m.ref_stride, x + 3 * (size_t)m.Nb, y, i, m.nb, 1);
   } else {
     const int n = (blockIdx.x - blob_blocks) * blockDim.x + threadIdx.x;
-    if (n < m.M) multiply_KT_one(m.qm, m.ref, x, y + 3 * (size_t)m.Nb, n, m.nb, -1.0, nullptr, 0.0);
+    if (n < m.M) multiply_KT_one(m.qm, m.ref, m.ref_stride, x, y + 3 * (size_t)m.Nb, n, m.nb, -1.0, nullptr, 0.0);
   }
 }
 

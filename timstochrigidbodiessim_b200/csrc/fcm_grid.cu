@@ -1287,7 +1287,10 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_SCRATCH_BYTE
 inline size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 // Device address of g_noalloc_scratch on the current device, looked up once per
-// device (the name is only a host-side stand-in in host code).
+// device (the name is only a host-side stand-in in host code).  The address is
+// kept for the life of the process: cudaDeviceReset unloads the library's device
+// code, and the array may come back elsewhere, so the call is not to be used
+// after a cudaDeviceReset in the same process.
 int noalloc_scratch_address(void** out) {
   static std::mutex mtx;
   static void* addr[256] = {};
@@ -1311,13 +1314,22 @@ int noalloc_scratch_address(void** out) {
   return FCM_OK;
 }
 
+// Device memory of the current device (where the kernels run) or managed memory.
+// A device pointer of another GPU is refused: a kernel here would read or write
+// that GPU's memory (an illegal address, or silent peer traffic).
 bool on_device(const void* p) {
   cudaPointerAttributes a;
   if (!p || cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeManaged) return true;
+  int dev = -1;
+  if (a.type != cudaMemoryTypeDevice || cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.device == dev;
 }
 
 }  // namespace
@@ -1353,7 +1365,7 @@ extern "C" int fcm_interp_noalloc(int32_t nx, int32_t ny, int32_t nz, double dx,
     return FCM_ERR_INVALID;
   }
   if (!on_device(Y) || !on_device(grid) || !on_device(V)) {
-    set_error("fcm_interp_noalloc: Y, grid and V must be device pointers");
+    set_error("fcm_interp_noalloc: Y, grid and V must be device pointers of the current device");
     return FCM_ERR_INVALID;
   }
   void* base_ptr = nullptr;

@@ -189,8 +189,15 @@ struct Ctx {
   cudaStream_t stream = 0;
   int device = 0;
 
-  // shape
-  double* d_ref = nullptr;   // 3*nb
+  // shape: 3*nb doubles (one shape for every body, as the reference's collection
+  // has), or 3*nb per body after fcm_set_body_shapes.  With per-body shapes
+  // d_Minv, d_N and d_KTKinv hold one block per body as well; the strides below
+  // are 0 for the shared shape and one block for per-body shapes.
+  double* d_ref = nullptr;
+  bool per_body = false;
+  int ref_stride = 0;        // 0 or 3*nb
+  long long minv_stride = 0; // 0 or (3nb)^2
+  int n_stride = 0;          // 0 or 36 (ref_N and ref_KTKinv)
   // bodies (x 3M, q 4M) current / midstep / saved start of step
   double *d_x = nullptr, *d_q = nullptr, *d_xm = nullptr, *d_qm = nullptr, *d_xs = nullptr, *d_qs = nullptr;
   double *d_Y = nullptr;     // all_blob_pos Nb*3
@@ -303,6 +310,8 @@ struct BMember {
   int hn;  // columns of the member's Krylov basis (maxit_alloc + 1)
   int red_blocks, md_blocks;  // the member's own reduction grids (same sums as its single solve)
   const double *qm, *ref, *Minv, *N;
+  int ref_stride, n_stride;   // per-body shape strides (0: one shared shape)
+  long long minv_stride;
   double *sys_a, *sys_b, *rhs, *soln, *res, *dx;
   GmState* gm;
   double *Qm, *Hd, *beta, *CS, *SN, *hA, *hB, *hnorm, *y;

@@ -204,6 +204,16 @@ class Suspension:
         k, p = _in(Y, 3 * self.Nb)
         self._c(self.L.fcm_set_up_gaussians(self.h, p), "fcm_set_up_gaussians")
 
+    def get_gaussians(self, precision=0, width=None):
+        """(indices, weights) of the last set_up_gaussians on the grid of one
+        precision, each (Nb, 3, W): the reference's indx/indy/indz and
+        gaussx/y/z.  W is ngauss for FP64; pass `width` for the FP32 grid."""
+        W = self.p.ngauss if width is None else width
+        ind = np.zeros(self.Nb * 3 * W, dtype=np.int32)
+        w = np.zeros(self.Nb * 3 * W)
+        self._c(self.L.fcm_get_gaussians(self.h, precision, ind.ctypes.data, w.ctypes.data), "fcm_get_gaussians")
+        return ind.reshape(self.Nb, 3, W), w.reshape(self.Nb, 3, W)
+
     def produce_random_velocity_field(self, seed, counter):
         self._c(self.L.fcm_produce_random_velocity_field(self.h, seed, counter), "fcm_produce_random_velocity_field")
 
@@ -353,6 +363,30 @@ class Suspension:
                 "fcm_set_reference_matrices")
 
     # -------------------------------------------------- gmres_solver
+    def set_body_shapes(self, shapes):
+        """Per-body reference blob positions (M, nb, 3) or 3*nb*M; each body gets
+        its own ref_KTKinv and the analytic FCM preconditioner blocks."""
+        k, p = _in(shapes, 3 * self.nb * self.M)
+        self._c(self.L.fcm_set_body_shapes(self.h, p), "fcm_set_body_shapes")
+
+    def set_body_preconditioners(self, Minv=None, N=None):
+        n3 = 3 * self.nb
+        km, pm = _in(Minv, n3 * n3 * self.M)
+        kn, pn = _in(N, 36 * self.M)
+        self._c(self.L.fcm_set_body_preconditioners(self.h, pm, pn), "fcm_set_body_preconditioners")
+
+    def get_body_preconditioners(self):
+        """(Minv (M, 3nb, 3nb), N (M, 6, 6), KTKinv (M, 6, 6)); each block as
+        stored (column-major), returned transposed into row-major numpy order."""
+        n3 = 3 * self.nb
+        Minv = np.zeros(self.M * n3 * n3)
+        N = np.zeros(36 * self.M)
+        K = np.zeros(36 * self.M)
+        self._c(self.L.fcm_get_body_preconditioners(self.h, Minv.ctypes.data, N.ctypes.data, K.ctypes.data),
+                "fcm_get_body_preconditioners")
+        return (Minv.reshape(self.M, n3, n3).transpose(0, 2, 1), N.reshape(self.M, 6, 6).transpose(0, 2, 1),
+                K.reshape(self.M, 6, 6).transpose(0, 2, 1))
+
     def assemble_RHS(self):
         self._c(self.L.fcm_assemble_RHS(self.h), "fcm_assemble_RHS")
 
