@@ -1,16 +1,20 @@
-"""Benchmark: Brownian rigid-rod time steps (body-steps/s) of the FCM mobility
+"""Benchmark: Brownian rigid-body time steps (body-steps/s) of the FCM mobility
 solve on B200, headline = mixed-precision solver, beside the plain FP64 GPU path.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload rods2048_phi0.10_g256] [--algorithm em|gdc]
+                  [--workload clusters32768_phi0.20_g512] [--algorithm em|gdc]
 
+Default workload: the largest single-GPU configuration, 32,768 rigid 12-blob
+random clusters, each of its own shape (393,216 blobs), volume fraction 0.20,
+512^3 grid, equilibrated by 10^4 Metropolis steps on the device (untimed).
 One step = one Euler-Maruyama time step (main.cpp:222-451): Philox
 fluctuating field, random blob velocities, steric forces, right-preconditioned
 GMRES of the rigid saddle-point system to the workload's tolerance, body
 update.  N > 1 runs N independent replicas, one per GPU (the solve does not
 shard; no collective on the data path), value = all replicas' body-steps / the
-slowest rank's time.  --impl reference times the CPU FP64 oracle (the
-reference's algorithm restated, all host threads) on the same workload.
+slowest rank's time; the ensemble workload instead splits its 64 instances
+across the ranks.  --impl reference times whole steps of the CPU FP64 oracle
+(the reference's algorithm restated, all host threads) on the same workload.
 """
 import argparse
 import json
@@ -39,12 +43,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="rods2048_phi0.10_g256")
+    ap.add_argument("--workload", default="clusters32768_phi0.20_g512")
     ap.add_argument("--algorithm", default="em", choices=["em", "gdc"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default kernel variants instead of fcm_autotune's choice")
-    ap.add_argument("--ens-modes", default="fp64,fp64_graph,mixed_batch,mixed",
+    ap.add_argument("--ens-modes", default="fp64,fp64_graph,fp64_many,fp64_batch,mixed_batch,mixed",
                     help="ensemble arms to time (the JSON line needs fp64, fp64_graph and mixed)")
     ap.add_argument("--nvtx", action="store_true", help="mark the timed region with an NVTX range 'timed'")
     ap.add_argument("--mixed-tol", type=float, default=None,
@@ -54,6 +58,10 @@ def parse():
                          "kernels a profiler can list one by one")
     ap.add_argument("--kernels-only", type=int, default=0, metavar="R",
                     help="profiling mode: R FP64 spread+interp launches and R FP32 mobility products, no steps")
+    ap.add_argument("--ref-budget", type=float, default=180.0,
+                    help="--impl reference: seconds of whole oracle steps to time at most (at least one step)")
+    ap.add_argument("--no-step-errors", action="store_true",
+                    help="skip the untimed replay that measures the mixed-vs-FP64 velocity error of every timed step")
     return ap.parse_args()
 
 
@@ -143,17 +151,20 @@ VARIANT_LEGEND = ("variants [FP64 spread, FP64 solve, FP32 spread, FP32 solve]: 
 AUTOTUNE = {"on": True}
 
 
-def setup_suspension(p, ref, x, q, fe, stream):
-    """A context for the workload; unless --no-autotune, its kernel variants are
-    chosen by fcm_autotune on the start configuration (untimed; s.tuning holds the
+def setup_suspension(p, ref, x, q, fe, stream, tune=True):
+    """A context for the workload (per-body shapes with their analytic
+    preconditioner blocks, or the shared shape with its probed reference
+    matrices); unless --no-autotune, its kernel variants are chosen by
+    fcm_autotune on the start configuration (untimed; s.tuning holds the
     variants and the microseconds per call of each candidate)."""
-    from timstochrigidbodiessim_b200.fcm import Suspension
-    s = Suspension(p, ref, stream=stream)
+    from timstochrigidbodiessim_b200 import configs
+    s = configs.make_suspension(p, ref, stream=stream)
     s.set_bodies(x, q)
     s.set_external_forces(fe)
-    s.produce_reference_matrices()
+    if not configs.has_body_shapes(p, ref):
+        s.produce_reference_matrices()
     s.tuning = None
-    if AUTOTUNE["on"]:
+    if AUTOTUNE["on"] and tune:
         s.fill_all_blob_pos()
         s.set_up_gaussians()
         v, us = s.autotune(reps=3)
@@ -252,6 +263,48 @@ def rel_vel_error(p, ref, x, q, fe, stream):
             float(np.linalg.norm(L32 - L64) / np.linalg.norm(L64)))
 
 
+def step_velocity_errors(p, ref, x, q, fe, seed, start, K, stream):
+    """Relative body- and blob-velocity error of the mixed-precision step against
+    the FP64 step on each of K steps of the mixed trajectory, replayed untimed
+    from the state the timed region started from (step indices start ..
+    start + K - 1; host-driven steps reproduce the graph steps bit for bit).  At
+    every step both contexts hold the same bodies and draw the same Philox noise
+    (seed, index); each forms its own random velocities (FP32 grid in the mixed
+    context), forces and RHS, and solves (FP64 to the workload's tolerance, mixed
+    with FP64 refinement to MIXED_TOL); the mixed context then advances with its
+    own solution and the FP64 context takes its bodies.  Returns per-step lists
+    (bodies, blobs)."""
+    ctx = {}
+    for prec in (0, 1):
+        pp = p.copy(precision=prec)
+        if prec == 1:
+            pp.gmres_tol = MIXED_TOL
+        ctx[prec] = setup_suspension(pp, ref, x, q, fe, stream, tune=False)
+    Nb = p.num_blobs
+    eU, eL = [], []
+    for k in range(K):
+        sol = {}
+        for prec, s in ctx.items():
+            s.fill_all_blob_pos()
+            s.produce_random_velocity_field(seed, start + k)
+            s.set_up_gaussians()
+            s.calculate_random_blob_velocities()
+            s.calculate_forces()
+            s.assemble_RHS()
+            st, soln, it, rel = s.invert_saddle_point_system()
+            sol[prec] = soln
+        U64, U32 = sol[0][3 * Nb:], sol[1][3 * Nb:]
+        L64, L32 = sol[0][:3 * Nb], sol[1][:3 * Nb]
+        eU.append(float(np.linalg.norm(U32 - U64) / np.linalg.norm(U64)))
+        eL.append(float(np.linalg.norm(L32 - L64) / np.linalg.norm(L64)))
+        ctx[1].end_of_step_update(U32, 1.0)
+        xb, qb = ctx[1].get_bodies()
+        ctx[0].set_bodies(xb, qb)
+    for s in ctx.values():
+        s.close()
+    return eU, eL
+
+
 def cpu_baseline(p, ref, x, q, fe, gmres_iters):
     """The CPU oracle (the reference's algorithm restated, FP64) on a bounded
     sample of the same workload: one fluctuating-field solve plus one saddle-point
@@ -259,9 +312,10 @@ def cpu_baseline(p, ref, x, q, fe, gmres_iters):
     estimated as noise + (iters + 2) products, iters = the FP64 GPU path's GMRES
     iteration count on this workload."""
     from tests.oracle_lib import Oracle, lib
+    from timstochrigidbodiessim_b200 import configs
     threads = os.cpu_count() or 1
     lib().orc_set_threads(threads)
-    o = Oracle(p, ref)
+    o = configs.make_suspension(p, ref, cls=Oracle)
     o.set_bodies(x, q)
     o.set_external_forces(fe)
     o.fill_all_blob_pos()
@@ -278,8 +332,9 @@ def cpu_baseline(p, ref, x, q, fe, gmres_iters):
     t_step = (t1 - t0) + (gmres_iters + 2) * (t2 - t1)
     o.close()
     return {"value": p.num_bodies / t_step, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": "1 fluctuating field + forces (%.2fs) and 1 preconditioned saddle-point product (%.2fs) of "
-                      "the same workload, FP64, step = noise + (%.1f GMRES iters + 2) products" %
+            "sample": "bounded sample: 1 fluctuating field + forces (%.2fs) and 1 preconditioned saddle-point "
+                      "product (%.2fs) of the same workload, FP64, scaled to a step as noise + (%.1f GMRES iters "
+                      "+ 2) products; bench.py --impl reference times whole oracle steps" %
                       (t1 - t0, t2 - t1, gmres_iters)}
 
 
@@ -311,6 +366,7 @@ def run_ours(args):
         s = setup_suspension(pp, ref, x, q, fe, stream)
         for i in range(args.warmup):
             run_step(s, seed, i, mode)
+        start_state = s.get_bodies() if tag == "mixed" else None  # for the untimed error replay
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
@@ -325,7 +381,8 @@ def run_ours(args):
         t = max_over_ranks(t)
         if world > 1:
             dist.barrier()
-        results[tag] = dict(t=t, iters=float(np.mean(iters)), launches=l1 - l0, clocks=clocks, s=s, tuning=s.tuning)
+        results[tag] = dict(t=t, iters=float(np.mean(iters)), launches=l1 - l0, clocks=clocks, s=s, tuning=s.tuning,
+                            start=start_state)
     # rooflines of the spread / interpolation kernels on the FP32 grid (the mixed
     # path's) and the FP64 grid
     kr = {"fp32": kernel_roofline(results["mixed"]["s"], p, stream, 1),
@@ -344,7 +401,17 @@ def run_ours(args):
     e1.record(stream)
     e1.synchronize()
     t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    for r in results.values():  # free the grids before the replay contexts are made
+        r["s"].close()
     err_U, err_l = rel_vel_error(p, ref, x, q, fe, stream) if rank == 0 else (None, None)
+    step_err = None
+    if rank == 0 and not args.no_step_errors:
+        x0, q0 = results["mixed"]["start"]
+        eU, eL = step_velocity_errors(p, ref, x0, q0, fe, seed, args.warmup, args.steps, stream)
+        step_err = {"steps": len(eU), "bodies": {"max": max(eU), "mean": float(np.mean(eU))},
+                    "blobs": {"max": max(eL), "mean": float(np.mean(eL))},
+                    "what": "every timed step replayed untimed: the mixed step's body and blob velocities "
+                            "against the FP64 step's on the same bodies and Philox noise"}
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -399,7 +466,12 @@ def run_ours(args):
             "mixed_over_fp64_graph": value / fp64g_value,
             "gmres_iters_mixed": results["mixed"]["iters"],
             "mixed_gmres_tol": MIXED_TOL,
-            "rel_vel_error_mixed_vs_fp64": {"bodies": err_U, "blobs": err_l},
+            "tolerances": "the FP64 arms solve to a %g relative residual, the mixed arm refines to %g "
+                          "(FP32 grid GMRES inside FP64 iterative refinement)" % (p.gmres_tol, MIXED_TOL),
+            "rel_vel_error_mixed_vs_fp64": {"per_step": step_err,
+                                            "start_rhs": {"bodies": err_U, "blobs": err_l,
+                                                          "what": "one deterministic solve of the start "
+                                                                  "configuration's RHS"}},
             "roofline": dict(kernels[0], bound="hbm", peak=hbm, unit="GB/s", peak_source=peak_src),
             "roofline_kernels": kernels,
             "cpu_baseline": cpu,
@@ -409,8 +481,6 @@ def run_ours(args):
             "clocks": results["mixed"]["clocks"],
         }
         print(json.dumps(line))
-    for r in results.values():
-        r["s"].close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -418,6 +488,18 @@ def run_ours(args):
 
 # ----------------------------------------------------------------- reference
 def run_reference(args):
+    """Whole time steps of the CPU FP64 oracle (the reference's algorithm
+    restated: Philox stress through the polar method, spread, FFT solve,
+    interpolation, steric forces, right-preconditioned GMRES to the workload's
+    tolerance, body update; main.cpp:222-451) on all host threads, from the same
+    start configuration as the GPU arm before its Metropolis equilibration (that
+    equilibration would take the oracle far longer than the bench may run).
+    Whole steps are timed one after another until --steps are done or
+    --ref-budget seconds are spent (at least one); the steps actually timed are
+    in the line.  One saddle-point product is also timed on one thread and on all
+    threads, and the single-thread figure (one reference MPI rank,
+    run_rigid_bodies_sim.sh:15) is the whole-step figure scaled by that ratio,
+    labelled as derived."""
     rank, world, local = dist_env()
     if rank != 0:
         return
@@ -426,44 +508,62 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     lib().orc_set_threads(threads)
     algorithm = 1 if args.algorithm == "gdc" else 2
-    p, ref, x, q, fe = configs.workload(args.workload, algorithm=algorithm)
-    o = Oracle(p, ref)
+    seed = 1234
+    p, ref, x, q, fe = configs.workload(args.workload, seed=seed, algorithm=algorithm)
+    t0 = time.perf_counter()
+    o = configs.make_suspension(p, ref, cls=Oracle)
     o.set_bodies(x, q)
     o.set_external_forces(fe)
-    o.produce_reference_matrices()
-    # GMRES iterations of this workload (one full deterministic solve, untimed)
+    if not configs.has_body_shapes(p, ref):
+        o.produce_reference_matrices()
+    t_setup = time.perf_counter() - t0
+    budget = max(0.0, args.ref_budget)
+    # one saddle-point product on all threads sizes the run: a step is about 30
     o.fill_all_blob_pos()
     o.set_up_gaussians()
-    o.calculate_forces()
-    o.assemble_RHS()
-    st, soln, iters, rel = o.invert_saddle_point_system()
-    n = p.system_size
-    v = np.random.default_rng(0).standard_normal(n)
-
-    def sample(i):
+    v = np.random.default_rng(0).standard_normal(p.system_size)
+    t0 = time.perf_counter()
+    o.multiply_by_saddle_point_matrix(o.multiply_by_Pinv(v))
+    t_all = time.perf_counter() - t0
+    # untimed warm-up steps only where they cost a small part of the budget
+    warm = args.warmup if 30.0 * t_all * args.warmup < 0.25 * budget else 0
+    for i in range(warm):
+        o.step(seed, i)
+    t_start = time.perf_counter()
+    ts, iters = [], []
+    for k in range(args.steps):
+        if ts and time.perf_counter() - t_start + np.mean(ts) > budget:
+            break
         t0 = time.perf_counter()
-        o.produce_random_velocity_field(1234, i)
-        o.calculate_random_blob_velocities()
-        o.calculate_forces()
-        t1 = time.perf_counter()
-        o.multiply_by_saddle_point_matrix(o.multiply_by_Pinv(v))
-        t2 = time.perf_counter()
-        return (t1 - t0) + (iters + 2) * (t2 - t1)
-
-    for i in range(args.warmup):
-        sample(i)
-    ts = [sample(args.warmup + i) for i in range(args.steps)]
+        st, info = o.step(seed, warm + k)
+        ts.append(time.perf_counter() - t0)
+        iters.append(info.gmres_iters)
     t_step = float(np.mean(ts))
     value = p.num_bodies / t_step
-    desc = ("per step: 1 fluctuating field + forces and 1 preconditioned saddle-point product, FP64, "
-            "scaled to noise + (%d GMRES iterations + 2) products; iterations from one full solve" % iters)
+    # thread scaling of one saddle-point product of the same workload
+    o.fill_all_blob_pos()
+    o.set_up_gaussians()
+    lib().orc_set_threads(1)
+    t0 = time.perf_counter()
+    o.multiply_by_saddle_point_matrix(o.multiply_by_Pinv(v))
+    t_one = time.perf_counter() - t0
+    lib().orc_set_threads(threads)
+    o.close()
+    desc = ("%d whole EM step(s) of the CPU FP64 oracle timed (%d untimed warm-up), %.1f GMRES iterations per "
+            "step to tol %g, %d threads; set-up (%.1fs) untimed" % (len(ts), warm, float(np.mean(iters)),
+                                                                    p.gmres_tol, threads, t_setup))
     print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * t_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded random rods)",
-        "config": {"workload": args.workload, "bodies": p.num_bodies, "grid": [p.nx, p.ny, p.nz],
-                   "algorithm": args.algorithm, "gmres_tol": p.gmres_tol},
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": len(ts),
+        "steps_requested": args.steps, "warmup": warm, "ms_per_step": 1e3 * t_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (the GPU arm's workload and seed, before its Metropolis equilibration)",
+        "config": {"workload": args.workload, "bodies": p.num_bodies, "blobs_per_body": p.blobs_per_body,
+                   "grid": [p.nx, p.ny, p.nz], "algorithm": args.algorithm, "gmres_tol": p.gmres_tol},
+        "gmres_iters": float(np.mean(iters)),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc},
+        "single_thread": {"value": value * t_all / t_one, "unit": UNIT, "cores": 1,
+                          "derived": "whole-step figure x (one saddle-point product on all threads %.2fs / on one "
+                                     "thread %.2fs)" % (t_all, t_one)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
@@ -491,28 +591,45 @@ def run_kernels_only(args):
     print(json.dumps({"kernels_only": args.kernels_only, "workload": args.workload}))
 
 
+def ensemble_shard(n_instances, rank, world):
+    """Instances of rank `rank` out of `world`: rank, rank + world, ... (every
+    instance exactly once over the ranks; no data is exchanged)."""
+    return list(range(rank, n_instances, world))
+
+
 def run_ensemble(args):
-    """Ensemble of 64 independent suspensions (seeds 0..63).  Plain FP64 GPU path:
-    the instances one after another on one stream, host-driven steps (fcm_step).
-    Mixed-precision path (the line's value): the 64 instances as 64 contexts on 64
-    streams, one CUDA graph per instance step (fcm_step_many).  Also timed: FP64
-    device-resident graph steps one instance after another, and the mixed
-    instances as one fcm_batch (per-instance work as concurrent graph branches,
-    the solves in lockstep as batched kernels, one CUDA graph per step).  Device
-    time: events on a root stream that every instance stream joins."""
+    """Ensemble of 64 independent suspensions (seeds 0..63).  Arms, each with the
+    same instances and steps:
+      fp64        instances one after another on one stream, host-driven fcm_step;
+      fp64_graph  instances one after another, device-resident graph steps;
+      fp64_many   64 contexts on 64 streams, one graph per instance step
+                  (fcm_step_many): the concurrency the mixed arm gets;
+      fp64_batch  one FP64 fcm_batch (lockstep batched solves, one graph per step);
+      mixed_batch the same batch with FP32 grids inside FP64 refinement;
+      mixed       (the line's value) fcm_step_many over 64 mixed contexts.
+    With N ranks each takes instances rank, rank + N, ... (no collective on the
+    data path); value = all instances' body-steps / the slowest rank's device
+    time.  Device time: events on a root stream that every instance stream joins."""
     os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")  # streams -> hardware queues
     from timstochrigidbodiessim_b200 import configs
-    insts = configs.ensemble(64, workers=min(16, os.cpu_count() or 1))  # before any CUDA call
+    rank, world, local = dist_env()
+    all_insts = configs.ensemble(64, workers=min(16, os.cpu_count() or 1))  # before any CUDA call
+    mine = ensemble_shard(len(all_insts), rank, world)
+    insts = [all_insts[i] for i in mine]
     import torch
+    import torch.distributed as dist
     from timstochrigidbodiessim_b200 import capi
     from timstochrigidbodiessim_b200.fcm import Batch, step_many
-    torch.cuda.set_device(0)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
     lib = capi.load()
     root = torch.cuda.current_stream()
-    total_bodies = sum(p.num_bodies for p, *_ in insts)
-    seeds = list(range(len(insts)))
+    total_bodies = sum(p.num_bodies for p, *_ in all_insts)
+    seeds = [i for i in mine]
     res = {}
-    modes = (("fp64", 0, "host"), ("fp64_graph", 0, "graph"), ("mixed_batch", 1, "batch"), ("mixed", 1, "many"))
+    modes = (("fp64", 0, "host"), ("fp64_graph", 0, "graph"), ("fp64_many", 0, "many"), ("fp64_batch", 0, "batch"),
+             ("mixed_batch", 1, "batch"), ("mixed", 1, "many"))
     wanted = set(args.ens_modes.split(","))
     for tag, prec, mode in modes:
         if tag not in wanted:
@@ -523,7 +640,8 @@ def run_ensemble(args):
             pps = []
             for p, ref, x, q, fe in insts:
                 pp = p.copy(precision=prec)
-                pp.gmres_tol = MIXED_TOL
+                if prec == 1:
+                    pp.gmres_tol = MIXED_TOL
                 pps.append((pp, ref))
             batch = Batch(pps, stream=streams[0])
             for m, (p, ref, x, q, fe) in zip(batch.members, insts):
@@ -551,9 +669,11 @@ def run_ensemble(args):
                     else:
                         s.step(seeds[k], i)
         torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        sampler = ClockSampler(0)
+        sampler = ClockSampler(local)
         if tag == "mixed":
             sampler.start()
         l0 = lib.fcm_kernel_launch_count()
@@ -588,13 +708,14 @@ def run_ensemble(args):
         if args.nvtx:
             torch.cuda.nvtx.range_pop()
         clocks = sampler.stop() if tag == "mixed" else None
-        t = e0.elapsed_time(e1) / 1e3
+        t = max_over_ranks(e0.elapsed_time(e1) / 1e3)
         tunings = {}
         for s in ([] if batch is not None else ss):
             if s.tuning is not None:
                 key = str(s.tuning["variants"])
                 tunings[key] = tunings.get(key, 0) + 1
-        res[tag] = dict(t=t, iters=float(np.mean(iters)), launches=lib.fcm_kernel_launch_count() - l0,
+        res[tag] = dict(t=t, iters=float(np.mean(iters)) if iters else 0.0,
+                        launches=lib.fcm_kernel_launch_count() - l0,
                         clocks=clocks, rounds=[float(np.mean([r[i] for r in rounds])) for i in (0, 1)] if rounds else None,
                         tunings=tunings or None)
         if batch is not None:
@@ -603,38 +724,58 @@ def run_ensemble(args):
             for s in ss:
                 s.close()
     if not {"fp64", "fp64_graph", "mixed"} <= set(res):
-        print(json.dumps({"ensemble_partial": {k: {"ms_per_step": 1e3 * v["t"] / args.steps, "iters": v["iters"],
-                                                    "rounds": v["rounds"]} for k, v in res.items()}}))
+        if rank == 0:
+            print(json.dumps({"ensemble_partial": {k: {"ms_per_step": 1e3 * v["t"] / args.steps, "iters": v["iters"],
+                                                        "rounds": v["rounds"]} for k, v in res.items()}}))
+        if world > 1:
+            dist.destroy_process_group()
         return
-    # velocity error of the mixed solve against the FP64 solve, every instance
+    # velocity error of the mixed solve against the FP64 solve, every instance of this rank
     errs = [rel_vel_error(p, ref, x, q, fe, root) for p, ref, x, q, fe in insts]
-    value = total_bodies * args.steps / res["mixed"]["t"]
-    fp64 = total_bodies * args.steps / res["fp64"]["t"]
-    fp64g = total_bodies * args.steps / res["fp64_graph"]["t"]
-    grids = sorted({p.nx for p, *_ in insts})
+    eU = max_over_ranks(max(e[0] for e in errs) if errs else 0.0)
+    eL = max_over_ranks(max(e[1] for e in errs) if errs else 0.0)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    val = {k: total_bodies * args.steps / v["t"] for k, v in res.items()}
+    value = val["mixed"]
+    grids = sorted({p.nx for p, *_ in all_insts})
+
+    def arm(tag, mode):
+        if tag not in res:
+            return None
+        out = {"value": val[tag], "ms_per_step": 1e3 * res[tag]["t"] / args.steps,
+               "gmres_iters": res[tag]["iters"], "mode": mode}
+        if res[tag]["rounds"]:
+            out["lockstep_rounds"] = {"gmres_iters": res[tag]["rounds"][0], "sweeps": res[tag]["rounds"][1]}
+        return out
+
+    ratio = lambda a, b: val[a] / val[b] if a in val and b in val else None
     print(json.dumps({
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * res["mixed"]["t"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * res["mixed"]["t"] / args.steps, "higher_is_better": True,
+        "scaling": "strong" if world > 1 else "weak",
         "vs_baseline": None, "dtype": "f32 grid + f64 refinement", "data": "synthetic (seeded random rods, Philox noise)",
-        "config": {"workload": "ensemble64_rods50-500_g64-128", "instances": len(insts), "bodies": total_bodies,
-                   "grids": grids, "gmres_tol_fp64": insts[0][0].gmres_tol, "mixed_gmres_tol": MIXED_TOL,
+        "config": {"workload": "ensemble64_rods50-500_g64-128", "instances": len(all_insts), "bodies": total_bodies,
+                   "grids": grids, "gmres_tol_fp64": all_insts[0][0].gmres_tol, "mixed_gmres_tol": MIXED_TOL,
                    "seeds": "0..63",
-                   "parallelism": "64 contexts on 64 streams, one CUDA graph per instance step (fcm_step_many)",
+                   "parallelism": "64 contexts on 64 streams, one CUDA graph per instance step (fcm_step_many)"
+                                  + ("; instances r, r+%d, ... on rank r" % world if world > 1 else ""),
                    "kernel_variants": {"legend": VARIANT_LEGEND, "members_per_choice": {
                        k: res[k]["tunings"] for k in ("fp64", "mixed") if k in res}}},
-        "fp64": {"value": fp64, "ms_per_step": 1e3 * res["fp64"]["t"] / args.steps, "gmres_iters": res["fp64"]["iters"],
-                 "mode": "instances one after another, host-driven fcm_step"},
-        "fp64_graph": {"value": fp64g, "ms_per_step": 1e3 * res["fp64_graph"]["t"] / args.steps,
-                       "mode": "instances one after another, device-resident graph steps"},
-        "mixed_batch": None if "mixed_batch" not in res else {
-            "value": total_bodies * args.steps / res["mixed_batch"]["t"],
-            "ms_per_step": 1e3 * res["mixed_batch"]["t"] / args.steps,
-            "lockstep_rounds": {"gmres_iters": res["mixed_batch"]["rounds"][0],
-                                "sweeps": res["mixed_batch"]["rounds"][1]},
-            "mode": "one fcm_batch: lockstep batched solve, one CUDA graph per step"},
-        "mixed_over_fp64": value / fp64, "mixed_over_fp64_graph": value / fp64g,
+        "fp64": arm("fp64", "instances one after another, host-driven fcm_step"),
+        "fp64_graph": arm("fp64_graph", "instances one after another, device-resident graph steps"),
+        "fp64_many": arm("fp64_many", "64 contexts on 64 streams, fcm_step_many (the mixed arm's concurrency)"),
+        "fp64_batch": arm("fp64_batch", "one FP64 fcm_batch: lockstep batched solve, one CUDA graph per step"),
+        "mixed_batch": arm("mixed_batch", "one mixed fcm_batch: lockstep batched solve, one CUDA graph per step"),
+        "mixed_over_fp64_many": ratio("mixed", "fp64_many"),
+        "mixed_batch_over_fp64_batch": ratio("mixed_batch", "fp64_batch"),
+        "mixed_batch_over_fp64_graph": ratio("mixed_batch", "fp64_graph"),
+        "mixed_over_fp64": ratio("mixed", "fp64"), "mixed_over_fp64_graph": ratio("mixed", "fp64_graph"),
         "gmres_iters_mixed": res["mixed"]["iters"],
-        "rel_vel_error_mixed_vs_fp64_max": {"bodies": max(e[0] for e in errs), "blobs": max(e[1] for e in errs)},
+        "rel_vel_error_mixed_vs_fp64_max": {"bodies": eU, "blobs": eL},
         "gpu_launches": res["mixed"]["launches"],
         "clocks": res["mixed"]["clocks"],
     }))

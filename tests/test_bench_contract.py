@@ -30,6 +30,11 @@ def test_reference_arm_line():
     cb = d["cpu_baseline"]
     assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    # whole oracle steps are timed (no scaling of a sample), the single-thread figure is labelled as derived
+    assert "whole EM step" in cb["sample"] and d["gmres_iters"] > 0
+    assert abs(d["ms_per_step"] - 1e3 * d["config"]["bodies"] / d["value"]) < 1e-6 * d["ms_per_step"]
+    st = d["single_thread"]
+    assert st["cores"] == 1 and 0 < st["value"] <= d["value"] * 1.5 and "derived" in st
 
 
 def test_reference_arm_other_ranks_exit_quietly():
