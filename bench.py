@@ -143,10 +143,11 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------- ours
-VARIANT_LEGEND = ("variants [FP64 spread, FP64 solve, FP32 spread, FP32 solve]: spread 0 persistent pipelined, "
-                  "1 one CTA per tile; solve 0 cuFFT 3D + projection, 1 cuFFT (y, z) + fused x-transform, "
-                  "2 library (y, z) + fused x-transform.  us[5P + v]: precision P, v 0-1 spread, 2-4 solve "
-                  "variants, microseconds per call, -1 not available")
+VARIANT_LEGEND = ("variants [FP64 spread, FP64 solve, FP32 spread, FP32 solve, FP64 interp, FP32 interp]: spread "
+                  "0 persistent pipelined, 1 one CTA per tile; solve 0 cuFFT 3D + projection, 1 cuFFT (y, z) + "
+                  "fused x-transform, 2 library (y, z) + fused x-transform; interp 0 shuffle reduction, 1 / 2 "
+                  "shared-memory reduction with 64 / 32 threads per tile.  us[8P + v]: precision P, v 0-1 spread, "
+                  "2-4 solve, 5-7 interp variants, microseconds per call, -1 not available")
 
 AUTOTUNE = {"on": True}
 

@@ -295,7 +295,8 @@ int fcm_spread(fcm_ctx* ctx, int32_t precision, const double* F);
 int fcm_stokes_solve(fcm_ctx* ctx, int32_t precision);
 int fcm_interp(fcm_ctx* ctx, int32_t precision, double* V);
 
-/* Kernel variants of the grid stages (no reference counterpart).  variants[4]:
+/* Kernel variants of the grid stages (no reference counterpart).
+ * variants[FCM_NUM_VARIANTS]:
  *   [0] FP64 spread, [2] FP32 spread: 0 = the persistent software-pipelined tile
  *       kernel, 1 = one CTA per 8^3 tile.  Both sum every grid point's blobs in the
  *       same order, so the grids are the same bit for bit.
@@ -303,22 +304,29 @@ int fcm_interp(fcm_ctx* ctx, int32_t precision, double* V);
  *       projection kernel, 1 = cuFFT (y, z) transforms around the fused x-transform
  *       + projection kernel, 2 = the library's own (y, z) transforms around it
  *       (FP32 only).  The solves agree within rounding.
- * A variant the grid does not allow (1 and 2 need supported lengths, 2 also
- * nz <= 512) or out of range is refused with FCM_ERR_INVALID; the spread entries
- * have no effect where the grid is not tiled (atomic spreading), the FP32 entries
- * none in a context without an FP32 grid (they are still range-checked).  The defaults are those measured fastest on B200: [0, 1 or 0, 1, 2 up to
- * 256 points along z else 1 or 0].  Step graphs are rebuilt on the next step.
- * Refused for a context owned by a batch. */
+ *   [4] FP64 interpolation, [5] FP32 interpolation: 0 = 64 threads per 8^3 tile
+ *       with a warp shuffle reduction, 1 = 64 threads per tile with a shared-memory
+ *       reduction, 2 = one warp per tile (two y-rows per thread) with a
+ *       shared-memory reduction.  They agree within rounding.
+ * A variant the grid does not allow (solve 1 and 2 need supported lengths, 2 also
+ * nz <= 512) or out of range is refused with FCM_ERR_INVALID; the spread and
+ * interpolation entries have no effect where the grid is not tiled, the FP32
+ * entries none in a context without an FP32 grid (they are still range-checked).
+ * Step graphs are rebuilt on the next step.  Refused for a context owned by a
+ * batch. */
+#define FCM_NUM_VARIANTS 6
 int fcm_get_variants(fcm_ctx* ctx, int32_t* variants);
 int fcm_set_variants(fcm_ctx* ctx, const int32_t* variants);
 /* Times every variant the grids allow on this context (reps timed calls of each,
  * 5 when reps <= 0, after one untimed call; zero forces, zeroed grids) and keeps
- * the fastest per stage and precision.  us (may be NULL) receives 10 doubles,
- * [5 P + v] for precision P (0 FP64, 1 FP32): v = 0, 1 the spread variants, v =
- * 2, 3, 4 the solve variants 0, 1, 2, in microseconds per call, -1 where not
+ * the fastest per stage and precision.  us (may be NULL) receives
+ * FCM_NUM_TUNE_TIMES doubles, [8 P + v] for precision P (0 FP64, 1 FP32): v = 0, 1
+ * the spread variants, v = 2, 3, 4 the solve variants 0, 1, 2, v = 5, 6, 7 the
+ * interpolation variants 0, 1, 2, in microseconds per call, -1 where not
  * available; variants (may be NULL) receives the choice as fcm_get_variants does.
  * Needs set_up_gaussians first; overwrites the grid work arrays, so call it
  * between steps. */
+#define FCM_NUM_TUNE_TIMES 16
 int fcm_autotune(fcm_ctx* ctx, int32_t reps, double* us, int32_t* variants);
 /* fcm_fluid_solver.cpp:842-881: single-body mobility at the box centre,
  * ref_Minv = inv_sympd(M_body) ((3nb)^2), ref_N = inv(K^T ref_Minv K) (6x6). */

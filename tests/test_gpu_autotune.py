@@ -2,9 +2,11 @@
 counterpart).  The two spread kernels sum every grid point's blobs in the same
 order, so M F is the same bit for bit whichever runs; the Stokes-solve variants
 (cuFFT 3D + projection, cuFFT (y, z) + fused x-transform, the library's (y, z)
-kernels + fused x-transform) agree with the oracle within 1e-10 (FP64) and 1e-6
-(FP32) relative.  fcm_autotune times what the grid allows, keeps the fastest by
-its own timings, and the results after tuning still match the oracle."""
+kernels + fused x-transform) and the three interpolation kernels (shuffle or
+shared-memory reduction, one or two y-rows per thread) agree with the oracle
+within 1e-10 (FP64) and 1e-6 (FP32) relative.  fcm_autotune times what the grid
+allows, keeps the fastest by its own timings, and the results after tuning still
+match the oracle."""
 import numpy as np
 import pytest
 
@@ -40,7 +42,8 @@ def _mf(g, F, prec):
 
 def test_variants_agree(gpu):
     g, Vo, F = _setup()
-    assert g.get_variants() == [0, 1, 1, 2]  # the defaults on a 64^3 grid
+    v0 = g.get_variants()
+    assert v0[:4] == [0, 1, 1, 2]  # the spread and solve defaults on a 64^3 grid
     for prec in (0, 1):
         for sv in ((0, 1) if prec == 0 else (0, 1, 2)):
             out = []
@@ -51,18 +54,26 @@ def test_variants_agree(gpu):
                 out.append(_mf(g, F, prec))
             assert np.array_equal(out[0], out[1]), (prec, sv)
             assert rel_err(out[0], Vo) < TOL[prec], (prec, sv)
+        for iv in (0, 1, 2):
+            v = g.get_variants()
+            v[4 + prec] = iv
+            g.set_variants(v)
+            assert g.get_variants()[4 + prec] == iv
+            assert rel_err(_mf(g, F, prec), Vo) < TOL[prec], (prec, iv)
 
 
 def test_autotune_keeps_the_fastest(gpu):
     g, Vo, F = _setup()
     v, us = g.autotune(reps=3)
     assert np.all(us[[0, 1, 2, 3]] > 0) and us[4] == -1  # FP64 has no library (y, z) variant
-    assert np.all(us[5:10] > 0)
+    assert np.all(us[5:8] > 0) and np.all(us[8:16] > 0)
     for P in (0, 1):
-        spread, solve = us[5 * P:5 * P + 2], us[5 * P + 2:5 * P + 5]
+        t = us[8 * P:8 * P + 8]
+        spread, solve, interp = t[0:2], t[2:5], t[5:8]
         assert v[2 * P] == (0 if spread[0] <= spread[1] else 1)
-        best = min((t, i) for i, t in enumerate(solve) if t >= 0)[1]
+        best = min((x, i) for i, x in enumerate(solve) if x >= 0)[1]
         assert v[2 * P + 1] == best
+        assert v[4 + P] == int(np.argmin(interp))
     assert g.get_variants() == v
     for prec in (0, 1):
         assert rel_err(_mf(g, F, prec), Vo) < TOL[prec], prec
@@ -71,16 +82,20 @@ def test_autotune_keeps_the_fastest(gpu):
 def test_variants_refused_where_the_grid_does_not_allow_them(gpu):
     g, _, _ = _setup()
     with pytest.raises(FcmError):
-        g.set_variants([0, 2, 1, 2])  # no library (y, z) variant in FP64
+        g.set_variants([0, 2, 1, 2, 0, 0])  # no library (y, z) variant in FP64
     with pytest.raises(FcmError):
-        g.set_variants([2, 1, 1, 2])  # out of range
-    # 20 points along x: no fused x-transform, so only the 3D solve
+        g.set_variants([2, 1, 1, 2, 0, 0])  # out of range
+    with pytest.raises(FcmError):
+        g.set_variants([0, 1, 1, 2, 3, 0])  # no interpolation variant 3
+    # 20 points along x: no fused x-transform, so only the 3D solve; not tiled, so
+    # the spread and interpolation variants are not timed
     h, Vo, F = _setup((20, 24, 16), nbodies=12)
     assert h.get_variants()[1] == 0 and h.get_variants()[3] == 0
     with pytest.raises(FcmError):
-        h.set_variants([0, 1, 1, 0])
+        h.set_variants([0, 1, 1, 0, 0, 0])
     v, us = h.autotune(reps=2)
-    assert us[3] == -1 and us[8] == -1 and us[9] == -1
+    assert us[3] == -1 and us[11] == -1 and us[12] == -1
+    assert np.all(us[5:8] == -1) and np.all(us[13:16] == -1)
     assert v[1] == 0 and v[3] == 0
     for prec in (0, 1):
         assert rel_err(_mf(h, F, prec), Vo) < TOL[prec], prec

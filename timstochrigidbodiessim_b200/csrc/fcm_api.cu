@@ -2519,12 +2519,14 @@ static void get_variants(const Ctx* c, int32_t* v) {
   v[1] = solve_variant(c, 0);
   v[2] = c->spread_pipe[1] ? 0 : 1;
   v[3] = solve_variant(c, 1);
+  v[4] = c->interp_variant[0];
+  v[5] = c->interp_variant[1];
 }
 
 static int set_variants(Ctx* c, const int32_t* v) {
   for (int P = 0; P < 2; ++P) {
-    const int sp = v[2 * P], sv = v[2 * P + 1];
-    if (sp < 0 || sp > 1 || sv < 0 || sv > (P == 1 ? 2 : 1)) {
+    const int sp = v[2 * P], sv = v[2 * P + 1], iv = v[4 + P];
+    if (sp < 0 || sp > 1 || sv < 0 || sv > (P == 1 ? 2 : 1) || iv < 0 || iv > 2) {
       set_error("kernel variant out of range");
       return FCM_ERR_INVALID;
     }
@@ -2539,6 +2541,7 @@ static int set_variants(Ctx* c, const int32_t* v) {
     c->spread_pipe[P] = v[2 * P] == 0;
     c->xfft[P] = v[2 * P + 1] >= 1;
     if (P == 1) c->yz32 = v[3] == 2;
+    c->interp_variant[P] = v[4 + P];
   }
   c->graph_stale = true;
   return FCM_OK;
@@ -2597,6 +2600,16 @@ static int tune_precision(Ctx* c, int reps, double* t) {
     if (t[2 + v] >= 0.0 && t[2 + v] < t[2 + best]) best = v;
   c->xfft[P] = best >= 1;
   if (P == 1) c->yz32 = best == 2;
+  if (bt.tiled) {  // interpolation of the (zeroed) grid into scratch
+    for (int v = 0; v < 3; ++v) {
+      c->interp_variant[P] = v;
+      FCM_TRY(time_calls(c, reps, [&] { return interp_t<T>(c, bt, gb.r, c->d_tmp3); }, &t[5 + v]));
+    }
+    int bi = 0;
+    for (int v = 1; v < 3; ++v)
+      if (t[5 + v] < t[5 + bi]) bi = v;
+    c->interp_variant[P] = bi;
+  }
   return FCM_OK;
 }
 
@@ -3265,13 +3278,13 @@ int fcm_autotune(fcm_ctx* ctx, int32_t reps, double* us, int32_t* variants) {
   }
   return guard([&]() -> int {
     const int R = reps > 0 ? reps : 5;
-    double t[10];
+    double t[FCM_NUM_TUNE_TIMES];
     for (double& v : t) v = -1.0;
     FCM_TRY(ensure_grid<double>(c));
     FCM_TRY(tune_precision<double>(c, R, t));
     if (c->p.precision == 1) {
       FCM_TRY(ensure_grid<float>(c));
-      FCM_TRY(tune_precision<float>(c, R, t + 5));
+      FCM_TRY(tune_precision<float>(c, R, t + FCM_NUM_TUNE_TIMES / 2));
     }
     c->det_ready = false;
     c->graph_stale = true;

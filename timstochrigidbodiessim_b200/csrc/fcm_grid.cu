@@ -615,6 +615,142 @@ __global__ void __launch_bounds__(64) k_interp_tiled(const T* __restrict__ wc, c
   interp_tile<T>(wc, grid, g, offset, list, G, partial, blockIdx.x);
 }
 
+// Tiled interpolation with R y-rows per thread: 64/R threads per 8x8x8 tile (one
+// warp for R = 2).  Thread t = (yq, z) = (t/8, t%8) holds the x-columns of rows
+// yq + r*8/R, r < R, three components each, in registers.  Per blob and row the
+// thread contracts its column with the blob's x-weights (x-halves and y-halves the
+// stencil misses are skipped; both tests are uniform over the CTA), scales by
+// wy*wz and adds the rows.  The per-thread values of a staging round go to a
+// shared buffer [3*SCB][64/R + pad] and each row (blob, component) is summed by
+// one thread in lane order (the padding keeps the vector reads conflict-free).
+// In FP32 the x-contraction runs on x-point pairs with the packed two-lane FMA.
+// The partial per (blob, tile) goes to partial[blob][j][3] as in k_interp_tiled;
+// k_interp_reduce sums them.  Fewer instructions per (blob, tile) than the
+// shuffle reduction of k_interp_tiled: the three components need no padding
+// slot, and with R = 2 the weight loads and flag tests are shared by two rows.
+template <typename T, int R>
+__global__ void __launch_bounds__(64 / R) k_interp_rows(const T* __restrict__ wc, const T* __restrict__ grid,
+                                                        TileGeom g, const int* __restrict__ offset,
+                                                        const unsigned long long* __restrict__ list, long long G,
+                                                        T* __restrict__ partial) {
+  constexpr int NT = 64 / R;                    // threads per tile
+  constexpr int RS = NT + 16 / (int)sizeof(T);  // padded reduction row
+  constexpr int YS = TE / R;                    // row step between a thread's rows
+  __shared__ __align__(16) T sw[SCB][3][TE];
+  __shared__ unsigned sflag[SCB];
+  __shared__ unsigned sblob[SCB];
+  __shared__ __align__(16) T sred[3 * SCB][RS];
+  const int tile = blockIdx.x;
+  const int b0 = offset[tile], b1 = offset[tile + 1];
+  if (b0 == b1) return;  // no blob meets this tile (uniform over the CTA)
+  const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
+  const int t = threadIdx.x;
+  const int z = t & 7, yq = t >> 3;
+  T u[R][3][TE];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int oy = ty * TE + yq + r * YS;
+    const bool live = oy < g.ycut;  // rows at or above the slip channel's upper wall read as 0
+    const long long base = ((long long)(tx * TE) * g.ny + oy) * g.nz + tz * TE + z;
+#pragma unroll
+    for (int x = 0; x < TE; ++x)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) u[r][c][x] = live ? grid[c * G + base + (long long)x * g.ny * g.nz] : (T)0;
+  }
+  for (int c0 = b0; c0 < b1; c0 += SCB) {
+    const int nc = min(SCB, b1 - c0);
+    if (c0 != b0) __syncthreads();
+    for (int i = t; i < 4 * nc; i += NT) {
+      const int k = i >> 2, d = i & 3;
+      const unsigned long long e = list[c0 + k];
+      const unsigned b = (unsigned)(e >> 32), lo = (unsigned)e;
+      if (d < 3) {
+        copy8(sw[k][d], wc + ((size_t)(3 * b + d) * NCH + ((lo >> (2 * d)) & 3u)) * TE);
+      } else {
+        sflag[k] = lo;
+        sblob[k] = b;
+      }
+    }
+    __syncthreads();
+    for (int k = 0; k < nc; ++k) {
+      const unsigned fl = sflag[k];
+      T p0 = 0, p1 = 0, p2 = 0;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int h = R == 2 ? r : (yq >> 2);  // y-half of this row
+        if (!((fl >> (EYM + h)) & 1u)) continue;
+        T s0, s1, s2;
+        if constexpr (sizeof(T) == 4) {
+          float2 a0 = make_float2(0.f, 0.f), a1 = a0, a2 = a0;
+#pragma unroll
+          for (int xh = 0; xh < 2; ++xh) {
+            if (!((fl >> (EXM + xh)) & 1u)) continue;
+            const float4 w4 = *reinterpret_cast<const float4*>(&sw[k][0][4 * xh]);
+            const float2 wa = make_float2(w4.x, w4.y), wb = make_float2(w4.z, w4.w);
+            const int x0 = 4 * xh;
+            a0 = __ffma2_rn(wa, make_float2(u[r][0][x0], u[r][0][x0 + 1]), a0);
+            a1 = __ffma2_rn(wa, make_float2(u[r][1][x0], u[r][1][x0 + 1]), a1);
+            a2 = __ffma2_rn(wa, make_float2(u[r][2][x0], u[r][2][x0 + 1]), a2);
+            a0 = __ffma2_rn(wb, make_float2(u[r][0][x0 + 2], u[r][0][x0 + 3]), a0);
+            a1 = __ffma2_rn(wb, make_float2(u[r][1][x0 + 2], u[r][1][x0 + 3]), a1);
+            a2 = __ffma2_rn(wb, make_float2(u[r][2][x0 + 2], u[r][2][x0 + 3]), a2);
+          }
+          s0 = a0.x + a0.y;
+          s1 = a1.x + a1.y;
+          s2 = a2.x + a2.y;
+        } else {
+          s0 = 0;
+          s1 = 0;
+          s2 = 0;
+#pragma unroll
+          for (int xh = 0; xh < 2; ++xh) {
+            if (!((fl >> (EXM + xh)) & 1u)) continue;
+            T wx[4];
+            load_wx4<T>(sw[k][0], 4 * xh, wx);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              s0 += wx[i] * u[r][0][4 * xh + i];
+              s1 += wx[i] * u[r][1][4 * xh + i];
+              s2 += wx[i] * u[r][2][4 * xh + i];
+            }
+          }
+        }
+        const T wyz = sw[k][1][yq + r * YS] * sw[k][2][z];
+        p0 += s0 * wyz;
+        p1 += s1 * wyz;
+        p2 += s2 * wyz;
+      }
+      sred[3 * k][t] = p0;
+      sred[3 * k + 1][t] = p1;
+      sred[3 * k + 2][t] = p2;
+    }
+    __syncthreads();
+    for (int rr = t; rr < 3 * nc; rr += NT) {
+      T sum = 0;
+      if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int j = 0; j < NT; j += 4) {
+          const float4 v = *reinterpret_cast<const float4*>(&sred[rr][j]);
+          sum += v.x;
+          sum += v.y;
+          sum += v.z;
+          sum += v.w;
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < NT; j += 2) {
+          const double2 v = *reinterpret_cast<const double2*>(&sred[rr][j]);
+          sum += v.x;
+          sum += v.y;
+        }
+      }
+      const int k = rr / 3, c = rr - 3 * (rr / 3);
+      const unsigned jt = (sflag[k] >> EJ) & 63u;
+      partial[((size_t)sblob[k] * 64 + jt) * 3 + c] = sum;
+    }
+  }
+}
+
 // V = DX^3 * sum over the blob's tiles (in canonical order j) of the partials.
 template <typename T>
 __device__ __forceinline__ void interp_reduce_one(const int* __restrict__ base, const T* __restrict__ partial,
@@ -847,7 +983,13 @@ int launch_interp(const Ctx& c, const BlobTable<T>& t, const T* grid, double* dV
   if (t.tiled) {
     TileGeom g = tile_geom(c.g, t.W);
     g.ycut = ycut;
-    k_interp_tiled<T><<<t.ntiles, 64, 0, s>>>(t.wc, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial);
+    const int v = c.interp_variant[sizeof(T) == 8 ? 0 : 1];
+    if (v == 2)
+      k_interp_rows<T, 2><<<t.ntiles, 32, 0, s>>>(t.wc, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial);
+    else if (v == 1)
+      k_interp_rows<T, 1><<<t.ntiles, 64, 0, s>>>(t.wc, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial);
+    else
+      k_interp_tiled<T><<<t.ntiles, 64, 0, s>>>(t.wc, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial);
     FCM_LAUNCH_CHECK();
     k_interp_reduce<T><<<(t.n + 127) / 128, 128, 0, s>>>(t.base, t.partial, t.n, g, dx3, dV);
     FCM_LAUNCH_CHECK();

@@ -275,6 +275,10 @@ struct Ctx {
   // spread kernel per precision: the persistent software-pipelined one (FP64
   // default) or one CTA per tile (FP32 default); both sum in the same order
   bool spread_pipe[2] = {true, false};
+  // interpolation kernel per precision: 0 the shuffle-reduced tile kernel
+  // (k_interp_tiled), 1 / 2 the shared-memory reduced kernel with one / two y-rows
+  // per thread (k_interp_rows, 64 / 32 threads per tile)
+  int interp_variant[2] = {0, 0};
   void* d_ytw32 = nullptr;
   void* d_ztw32 = nullptr;
   void* d_xtw64 = nullptr;

@@ -325,24 +325,29 @@ class Suspension:
         self._c(self.L.fcm_interp(self.h, precision, po), "fcm_interp")
         return V
 
-    # kernel variants: [FP64 spread, FP64 solve, FP32 spread, FP32 solve]; spread
-    # 0 = persistent pipelined, 1 = one CTA per tile; solve 0 = cuFFT 3D,
-    # 1 = cuFFT (y, z) + fused x-transform, 2 = the library's (y, z) + fused x
+    # kernel variants: [FP64 spread, FP64 solve, FP32 spread, FP32 solve, FP64
+    # interp, FP32 interp]; spread 0 = persistent pipelined, 1 = one CTA per tile;
+    # solve 0 = cuFFT 3D, 1 = cuFFT (y, z) + fused x-transform, 2 = the library's
+    # (y, z) + fused x; interp 0 = shuffle reduction, 1 / 2 = shared-memory
+    # reduction with 64 / 32 threads per tile
+    NUM_VARIANTS = 6
+
     def get_variants(self):
-        v, pv = _out(None, 4, np.int32)
+        v, pv = _out(None, self.NUM_VARIANTS, np.int32)
         self._c(self.L.fcm_get_variants(self.h, pv), "fcm_get_variants")
         return [int(x) for x in v]
 
     def set_variants(self, variants):
-        v, pv = _in(variants, 4, np.int32)
+        v, pv = _in(variants, self.NUM_VARIANTS, np.int32)
         self._c(self.L.fcm_set_variants(self.h, pv), "fcm_set_variants")
 
     def autotune(self, reps=5):
         """Time every variant the grids allow and keep the fastest.  Returns
-        (variants, us): us[5 P + v] microseconds per call for precision P, v = 0, 1
-        spread variants, 2, 3, 4 solve variants (-1 where not available)."""
-        us, pu = _out(None, 10)
-        v, pv = _out(None, 4, np.int32)
+        (variants, us): us[8 P + v] microseconds per call for precision P, v = 0, 1
+        spread variants, 2, 3, 4 solve variants, 5, 6, 7 interpolation variants
+        (-1 where not available)."""
+        us, pu = _out(None, 16)
+        v, pv = _out(None, self.NUM_VARIANTS, np.int32)
         self._c(self.L.fcm_autotune(self.h, reps, pu, pv), "fcm_autotune")
         return [int(x) for x in v], us
 
