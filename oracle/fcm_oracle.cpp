@@ -21,6 +21,7 @@
 // Build: oracle/Makefile (g++ -O3 -fopenmp -ffp-contract=off).
 
 #include "fcm_oracle.h"
+#include "philox.h"
 
 #include <algorithm>
 #include <cmath>
@@ -37,66 +38,8 @@ namespace {
 const double PI = 3.14159265358979323846264338327950288;  // config.hpp:86
 int g_threads = 1;
 
-// ============================================================ Philox4x32-10
-// Counter-based generator of Salmon, Moraes, Dror and Shaw, "Parallel random
-// numbers: as easy as 1, 2, 3" (SC'11): 10 rounds of the 4x32 Philox S-box with
-// multipliers 0xD2511F53 / 0xCD9E8D57 and Weyl key increments 0x9E3779B9 /
-// 0xBB67AE85.
-struct Philox {
-  static inline void mulhilo(uint32_t a, uint32_t b, uint32_t& hi, uint32_t& lo) {
-    uint64_t p = (uint64_t)a * (uint64_t)b;
-    hi = (uint32_t)(p >> 32);
-    lo = (uint32_t)p;
-  }
-  static void gen(const uint32_t ctr_in[4], uint32_t k0, uint32_t k1, uint32_t out[4]) {
-    uint32_t c0 = ctr_in[0], c1 = ctr_in[1], c2 = ctr_in[2], c3 = ctr_in[3];
-    for (int r = 0; r < 10; ++r) {
-      uint32_t hi0, lo0, hi1, lo1;
-      mulhilo(0xD2511F53u, c0, hi0, lo0);
-      mulhilo(0xCD9E8D57u, c2, hi1, lo1);
-      uint32_t n0 = hi1 ^ c1 ^ k0, n1 = lo1, n2 = hi0 ^ c3 ^ k1, n3 = lo0;
-      c0 = n0; c1 = n1; c2 = n2; c3 = n3;
-      k0 += 0x9E3779B9u;
-      k1 += 0xBB67AE85u;
-    }
-    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
-  }
-};
-
-// Sequential uniform stream on (0,1) built from Philox blocks, standing in for
-// SPRNG's sprng() (parallel_random_numbers.hpp:13-17).
-struct UniformStream {
-  uint32_t key0, key1;
-  uint64_t block;
-  uint32_t buf[4];
-  int pos;
-  UniformStream(uint64_t seed, uint64_t stream) : key0((uint32_t)seed), key1((uint32_t)(seed >> 32)), block(0), pos(4) {
-    stream_lo = (uint32_t)stream;
-    stream_hi = (uint32_t)(stream >> 32);
-  }
-  uint32_t stream_lo, stream_hi;
-  double next() {
-    if (pos == 4) {
-      uint32_t c[4] = {(uint32_t)block, (uint32_t)(block >> 32), stream_lo, stream_hi};
-      Philox::gen(c, key0, key1, buf);
-      ++block;
-      pos = 0;
-    }
-    uint32_t a = buf[pos++];
-    return ((double)a + 0.5) * (1.0 / 4294967296.0);
-  }
-  // parallel_random_numbers.cpp:8-19 (Marsaglia polar method, one normal).
-  double gaussian_random() {
-    double x1, x2, w = 10.0;
-    while (w > 1.0 || w == 1) {
-      x1 = 2.0 * next() - 1.0;
-      x2 = 2.0 * next() - 1.0;
-      w = x1 * x1 + x2 * x2;
-    }
-    w = std::sqrt((-2.0 * std::log(w)) / w);
-    return w * x1;
-  }
-};
+using orcrng::Philox;
+using orcrng::UniformStream;
 
 // ============================================================ 1-D complex FFT
 // Stockham autosort, radices 4, 2, 3, 5 and generic odd primes, applied to `vb`
@@ -640,6 +583,9 @@ struct orc {
   // ((3nb)^2) and ref_N (36)
   bool per_body = false;
   std::vector<double> shapes, body_KTKinv, body_Minv, body_N;
+  // noise from one sequential stream (orc_set_sequential_noise)
+  bool seq_noise = false;
+  UniformStream seq_rng{0, 0};
   std::vector<Body> bodies, midstep_bodies, temp_bodies;
   std::vector<double> blob_forces, ext_forces, U0;
   double body_radius = 0;
@@ -1538,13 +1484,18 @@ void orc_inject_random_stress(orc* o, const double* sxx, const double* syy, cons
 // x-plane i draws from its own stream (seed; counter*2^20 + i), as each
 // reference MPI rank draws its x-slab from its own SPRNG stream, so the planes
 // fill in parallel.
+// In sequential mode (orc_set_sequential_noise) every plane draws, in plane
+// order, from one stream that continues across calls -- the single SPRNG stream
+// of one reference rank -- and (seed, counter) are not used.
 void orc_produce_random_velocity_field(orc* o, uint64_t seed, uint64_t counter) {
   const double var1 = std::sqrt(2.0 * o->kT * o->eta / (o->DX * o->DX * o->DX * o->DT));
   const double var2 = std::sqrt(2.0) * var1;
   const int Ny = o->Ny, pad = o->pad;
-#pragma omp parallel for num_threads(g_threads) schedule(static)
+  const bool seq = o->seq_noise;
+#pragma omp parallel for num_threads(seq ? 1 : g_threads) schedule(static)
   for (int i = 0; i < o->Nx; i++) {
-    UniformStream rng(seed, (counter << 20) + (uint64_t)i);
+    UniformStream plane_rng(seed, (counter << 20) + (uint64_t)i);
+    UniformStream& rng = seq ? o->seq_rng : plane_rng;
     const size_t x_index = (size_t)i * Ny * pad;
     const int half_y = Ny / 2;
     for (int k = 0; k < pad; k++)
@@ -1585,6 +1536,11 @@ void orc_produce_random_velocity_field(orc* o, uint64_t seed, uint64_t counter) 
       }
   }
   random_field_from_stress(o);
+}
+
+void orc_set_sequential_noise(orc* o, int on, uint64_t seed, uint64_t stream) {
+  o->seq_noise = on != 0;
+  o->seq_rng = UniformStream(seed, stream);
 }
 
 void orc_calculate_random_blob_velocities(orc* o, double* V) {

@@ -102,6 +102,11 @@ void orc_set_body_shapes(orc* o, const double* shapes);
 void orc_set_body_preconditioners(orc* o, const double* Minv, const double* N);
 void orc_get_body_preconditioners(orc* o, double* Minv, double* N, double* KTKinv);
 void orc_produce_body_preconditioners(orc* o);
+/* Noise from one stream continued across calls (on = 1): the stress of every
+ * plane drawn in plane order from UniformStream(seed, stream), as one reference
+ * rank draws from its SPRNG stream; produce_random_velocity_field's own seed and
+ * counter are then not used.  on = 0 returns to per-plane streams. */
+void orc_set_sequential_noise(orc* o, int on, uint64_t seed, uint64_t stream);
 
 void orc_assemble_RHS(orc* o);
 void orc_get_RHS(orc* o, double* rhs);

@@ -84,6 +84,7 @@ def lib():
             "orc_set_body_preconditioners": (None, [vp, D, D]),
             "orc_get_body_preconditioners": (None, [vp, D, D, D]),
             "orc_produce_body_preconditioners": (None, [vp]),
+            "orc_set_sequential_noise": (None, [vp, ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64]),
             "orc_assemble_RHS": (None, [vp]),
             "orc_get_RHS": (None, [vp, D]),
             "orc_set_RHS": (None, [vp, D]),
@@ -255,6 +256,11 @@ class Oracle:
 
     def produce_random_velocity_field(self, seed, counter):
         lib().orc_produce_random_velocity_field(self.h, seed, counter)
+
+    def set_sequential_noise(self, on, seed=0, stream=0):
+        """Noise from one stream continued across calls (the SPRNG stream of one
+        reference rank); on=False returns to per-plane streams."""
+        lib().orc_set_sequential_noise(self.h, int(bool(on)), seed, stream)
 
     def calculate_random_blob_velocities(self):
         V = np.zeros(3 * self.Nb)
