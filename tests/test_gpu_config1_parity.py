@@ -140,7 +140,7 @@ def test_config1_em_step_injected_noise(cfg1, cfg1_step):
     (xg, qg), (xo, qo) = G["bodies"], O["bodies"]
     assert np.abs(xg - xo).max() < 1e-9
     assert np.abs(qg - qo).max() < 1e-9
-    assert np.abs(xg - cfg1[3]).max() > 1e-6  # the bodies moved
+    assert np.abs(xg - cfg1[2]).max() > 1e-6  # the bodies moved
 
 
 def test_config1_mixed_precision_solve_vs_oracle(cfg1, cfg1_step):
