@@ -58,6 +58,8 @@ def parse():
                          "kernels a profiler can list one by one")
     ap.add_argument("--kernels-only", type=int, default=0, metavar="R",
                     help="profiling mode: R FP64 spread+interp launches and R FP32 mobility products, no steps")
+    ap.add_argument("--variants", default=None,
+                    help="--kernels-only: six comma-separated kernel variants (fcm_set_variants) to run")
     ap.add_argument("--ref-budget", type=float, default=180.0,
                     help="--impl reference: seconds of whole oracle steps to time at most (at least one step)")
     ap.add_argument("--no-step-errors", action="store_true",
@@ -144,10 +146,11 @@ class ClockSampler:
 
 # ----------------------------------------------------------------- ours
 VARIANT_LEGEND = ("variants [FP64 spread, FP64 solve, FP32 spread, FP32 solve, FP64 interp, FP32 interp]: spread "
-                  "0 persistent pipelined, 1 one CTA per tile; solve 0 cuFFT 3D + projection, 1 cuFFT (y, z) + "
-                  "fused x-transform, 2 library (y, z) + fused x-transform; interp 0 shuffle reduction, 1 / 2 "
-                  "shared-memory reduction with 64 / 32 threads per tile.  us[8P + v]: precision P, v 0-1 spread, "
-                  "2-4 solve, 5-7 interp variants, microseconds per call, -1 not available")
+                  "0 persistent pipelined, 1 / 2 / 3 one CTA per tile staging 16 / 8 / 32 blobs per round; solve "
+                  "0 cuFFT 3D + projection, 1 cuFFT (y, z) + fused x-transform, 2 library (y, z) + fused "
+                  "x-transform; interp 0 shuffle reduction, 1 / 2 shared-memory reduction with 64 / 32 threads "
+                  "per tile.  us[10P + v]: precision P, v 0-3 spread, 4-6 solve, 7-9 interp variants, "
+                  "microseconds per call, -1 not available")
 
 AUTOTUNE = {"on": True}
 
@@ -572,12 +575,13 @@ def run_reference(args):
 def run_kernels_only(args):
     import torch
     from timstochrigidbodiessim_b200 import configs
-    from timstochrigidbodiessim_b200.fcm import Suspension
     torch.cuda.set_device(0)
     stream = torch.cuda.Stream()
     p, ref, x, q, fe = configs.workload(args.workload)
     for prec in (0, 1):
-        s = Suspension(p.copy(precision=prec), ref, stream=stream)
+        s = configs.make_suspension(p.copy(precision=prec), ref, stream=stream)
+        if args.variants:
+            s.set_variants([int(v) for v in args.variants.split(",")])
         s.set_bodies(x, q)
         s.fill_all_blob_pos()
         s.set_up_gaussians()

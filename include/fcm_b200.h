@@ -298,8 +298,9 @@ int fcm_interp(fcm_ctx* ctx, int32_t precision, double* V);
 /* Kernel variants of the grid stages (no reference counterpart).
  * variants[FCM_NUM_VARIANTS]:
  *   [0] FP64 spread, [2] FP32 spread: 0 = the persistent software-pipelined tile
- *       kernel, 1 = one CTA per 8^3 tile.  Both sum every grid point's blobs in the
- *       same order, so the grids are the same bit for bit.
+ *       kernel, 1 / 2 / 3 = one CTA per 8^3 tile staging 16 / 8 / 32 blobs per
+ *       round.  All sum every grid point's blobs in the same order, so the grids
+ *       are the same bit for bit.
  *   [1] FP64 Stokes solve, [3] FP32 Stokes solve: 0 = cuFFT 3D transforms and the
  *       projection kernel, 1 = cuFFT (y, z) transforms around the fused x-transform
  *       + projection kernel, 2 = the library's own (y, z) transforms around it
@@ -320,13 +321,13 @@ int fcm_set_variants(fcm_ctx* ctx, const int32_t* variants);
 /* Times every variant the grids allow on this context (reps timed calls of each,
  * 5 when reps <= 0, after one untimed call; zero forces, zeroed grids) and keeps
  * the fastest per stage and precision.  us (may be NULL) receives
- * FCM_NUM_TUNE_TIMES doubles, [8 P + v] for precision P (0 FP64, 1 FP32): v = 0, 1
- * the spread variants, v = 2, 3, 4 the solve variants 0, 1, 2, v = 5, 6, 7 the
+ * FCM_NUM_TUNE_TIMES doubles, [10 P + v] for precision P (0 FP64, 1 FP32): v = 0..3
+ * the spread variants, v = 4, 5, 6 the solve variants 0, 1, 2, v = 7, 8, 9 the
  * interpolation variants 0, 1, 2, in microseconds per call, -1 where not
  * available; variants (may be NULL) receives the choice as fcm_get_variants does.
  * Needs set_up_gaussians first; overwrites the grid work arrays, so call it
  * between steps. */
-#define FCM_NUM_TUNE_TIMES 16
+#define FCM_NUM_TUNE_TIMES 20
 int fcm_autotune(fcm_ctx* ctx, int32_t reps, double* us, int32_t* variants);
 /* fcm_fluid_solver.cpp:842-881: single-body mobility at the box centre,
  * ref_Minv = inv_sympd(M_body) ((3nb)^2), ref_N = inv(K^T ref_Minv K) (6x6). */

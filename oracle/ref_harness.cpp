@@ -65,12 +65,20 @@ void rh_config(double* o) {
 // blob_ref_pos (3 x nb) as 3*nb values, blob after blob.
 void rh_blob_ref_pos(double* out) { copy_out(C->blob_ref_pos, out); }
 
+// Set the bodies and populate the cell list from their blobs, as seed_the_bodies
+// does (collection_of_rigid_bodies.cpp:428-429).  The reference populates the
+// list only there, at the midstep and at the end of a step (:609, :778), so an
+// Euler-Maruyama run started from a state file reaches calculate_forces with a
+// never-populated list (all-zero head and next arrays) and its traversal loops
+// forever; the harness populates it here.
 void rh_set_bodies(const double* x, const double* q) {
   for (int n = 0; n < NUM_BODIES; ++n) {
     C->bodies[n].x = {x[3 * n], x[3 * n + 1], x[3 * n + 2]};
     C->bodies[n].q = quaternion(q[4 * n], q[4 * n + 1], q[4 * n + 2], q[4 * n + 3]);
   }
   C->midstep_bodies = C->bodies;
+  C->fill_all_blob_pos();
+  C->list.populate(C->all_blob_pos);
 }
 
 void rh_get_bodies(double* x, double* q) {

@@ -99,15 +99,15 @@ class Reference:
         self.L.rh_produce_reference_matrices()
 
     def get_reference_matrices(self):
-        """(ref_Minv, ref_N, ref_KTKinv) as flat column-major arrays."""
+        """(ref_Minv, ref_N, ref_KTKinv) as matrices, as the oracle returns them."""
         n3 = 3 * self.nb
         Minv, N, K = np.zeros(n3 * n3), np.zeros(36), np.zeros(36)
         self.L.rh_get_reference_matrices(_dp(Minv), _dp(N), _dp(K))
-        return Minv, N, K
+        return Minv.reshape(n3, n3, order="F"), N.reshape(6, 6, order="F"), K.reshape(6, 6, order="F")
 
     def set_reference_matrices(self, Minv, N):
-        Minv = np.ascontiguousarray(Minv, dtype=np.float64)
-        N = np.ascontiguousarray(N, dtype=np.float64)
+        Minv = np.ascontiguousarray(np.asarray(Minv).ravel(order="F"), dtype=np.float64)
+        N = np.ascontiguousarray(np.asarray(N).ravel(order="F"), dtype=np.float64)
         self.L.rh_set_reference_matrices(_dp(Minv), _dp(N))
 
     def sprng_reset(self, seed, stream=0):

@@ -1,5 +1,6 @@
 """Kernel variants of the grid stages and their autotuner (no reference
-counterpart).  The two spread kernels sum every grid point's blobs in the same
+counterpart).  The four spread kernels (persistent pipelined; one CTA per tile
+staging 16, 8 or 32 blobs per round) sum every grid point's blobs in the same
 order, so M F is the same bit for bit whichever runs; the Stokes-solve variants
 (cuFFT 3D + projection, cuFFT (y, z) + fused x-transform, the library's (y, z)
 kernels + fused x-transform) and the three interpolation kernels (shuffle or
@@ -47,12 +48,13 @@ def test_variants_agree(gpu):
     for prec in (0, 1):
         for sv in ((0, 1) if prec == 0 else (0, 1, 2)):
             out = []
-            for sp in (0, 1):
+            for sp in (0, 1, 2, 3):
                 v = g.get_variants()
                 v[2 * prec], v[2 * prec + 1] = sp, sv
                 g.set_variants(v)
                 out.append(_mf(g, F, prec))
-            assert np.array_equal(out[0], out[1]), (prec, sv)
+            for o_ in out[1:]:
+                assert np.array_equal(out[0], o_), (prec, sv)
             assert rel_err(out[0], Vo) < TOL[prec], (prec, sv)
         for iv in (0, 1, 2):
             v = g.get_variants()
@@ -65,12 +67,12 @@ def test_variants_agree(gpu):
 def test_autotune_keeps_the_fastest(gpu):
     g, Vo, F = _setup()
     v, us = g.autotune(reps=3)
-    assert np.all(us[[0, 1, 2, 3]] > 0) and us[4] == -1  # FP64 has no library (y, z) variant
-    assert np.all(us[5:8] > 0) and np.all(us[8:16] > 0)
+    assert np.all(us[0:6] > 0) and us[6] == -1  # FP64 has no library (y, z) variant
+    assert np.all(us[7:10] > 0) and np.all(us[10:20] > 0)
     for P in (0, 1):
-        t = us[8 * P:8 * P + 8]
-        spread, solve, interp = t[0:2], t[2:5], t[5:8]
-        assert v[2 * P] == (0 if spread[0] <= spread[1] else 1)
+        t = us[10 * P:10 * P + 10]
+        spread, solve, interp = t[0:4], t[4:7], t[7:10]
+        assert v[2 * P] == int(np.argmin(spread))
         best = min((x, i) for i, x in enumerate(solve) if x >= 0)[1]
         assert v[2 * P + 1] == best
         assert v[4 + P] == int(np.argmin(interp))
@@ -84,7 +86,7 @@ def test_variants_refused_where_the_grid_does_not_allow_them(gpu):
     with pytest.raises(FcmError):
         g.set_variants([0, 2, 1, 2, 0, 0])  # no library (y, z) variant in FP64
     with pytest.raises(FcmError):
-        g.set_variants([2, 1, 1, 2, 0, 0])  # out of range
+        g.set_variants([4, 1, 1, 2, 0, 0])  # out of range
     with pytest.raises(FcmError):
         g.set_variants([0, 1, 1, 2, 3, 0])  # no interpolation variant 3
     # 20 points along x: no fused x-transform, so only the 3D solve; not tiled, so
@@ -94,8 +96,8 @@ def test_variants_refused_where_the_grid_does_not_allow_them(gpu):
     with pytest.raises(FcmError):
         h.set_variants([0, 1, 1, 0, 0, 0])
     v, us = h.autotune(reps=2)
-    assert us[3] == -1 and us[11] == -1 and us[12] == -1
-    assert np.all(us[5:8] == -1) and np.all(us[13:16] == -1)
+    assert us[5] == -1 and us[15] == -1 and us[16] == -1
+    assert np.all(us[0:4] == -1) and np.all(us[7:10] == -1) and np.all(us[17:20] == -1)
     assert v[1] == 0 and v[3] == 0
     for prec in (0, 1):
         assert rel_err(_mf(h, F, prec), Vo) < TOL[prec], prec

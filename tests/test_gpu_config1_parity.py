@@ -200,9 +200,9 @@ def test_dense_tiles_at_cluster_density(gpu):
     o.set_up_force_distribution(F)
     o.produce_deterministic_velocity_field()
     Vo = o.calculate_deterministic_blob_velocities()
-    for variant in (0, 1, 2):
+    for variant in (0, 1, 2, 3):
         v = g.get_variants()
-        g.set_variants([min(variant, 1), v[1], min(variant, 1), v[3], variant, variant])
+        g.set_variants([variant, v[1], variant, v[3], min(variant, 2), min(variant, 2)])
         g.set_up_force_distribution(F)
         g.produce_deterministic_velocity_field()
         assert rel_err(g.calculate_deterministic_blob_velocities(), Vo) < TOL, variant

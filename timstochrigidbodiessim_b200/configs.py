@@ -399,6 +399,10 @@ WORKLOADS = {
     # 32,768 rigid 12-blob random clusters (393,216 blobs), volume fraction
     # 0.20, 512^3 grid; started on a lattice, equilibrated by Metropolis steps
     "clusters32768_phi0.20_g512": dict(kind="clusters", M=32768, grid=512, phi=0.20, mcmc_steps=10000),
+    # the same grid spacing (0.394a), volume fraction and cluster size in one
+    # eighth of the volume: 4096 clusters (49,152 blobs) on a 256^3 grid, the
+    # profiling stand-in for the 512^3 suspension
+    "clusters4096_phi0.20_g256": dict(kind="clusters", M=4096, grid=256, phi=0.20, mcmc_steps=2000),
 }
 
 

@@ -2515,9 +2515,9 @@ static int solve_variant(const Ctx* c, int P) {
 }
 
 static void get_variants(const Ctx* c, int32_t* v) {
-  v[0] = c->spread_pipe[0] ? 0 : 1;
+  v[0] = c->spread_variant[0];
   v[1] = solve_variant(c, 0);
-  v[2] = c->spread_pipe[1] ? 0 : 1;
+  v[2] = c->spread_variant[1];
   v[3] = solve_variant(c, 1);
   v[4] = c->interp_variant[0];
   v[5] = c->interp_variant[1];
@@ -2526,7 +2526,7 @@ static void get_variants(const Ctx* c, int32_t* v) {
 static int set_variants(Ctx* c, const int32_t* v) {
   for (int P = 0; P < 2; ++P) {
     const int sp = v[2 * P], sv = v[2 * P + 1], iv = v[4 + P];
-    if (sp < 0 || sp > 1 || sv < 0 || sv > (P == 1 ? 2 : 1) || iv < 0 || iv > 2) {
+    if (sp < 0 || sp > 3 || sv < 0 || sv > (P == 1 ? 2 : 1) || iv < 0 || iv > 2) {
       set_error("kernel variant out of range");
       return FCM_ERR_INVALID;
     }
@@ -2538,7 +2538,7 @@ static int set_variants(Ctx* c, const int32_t* v) {
   }
   for (int P = 0; P < 2; ++P) {
     if (P == 1 && c->p.precision != 1) continue;
-    c->spread_pipe[P] = v[2 * P] == 0;
+    c->spread_variant[P] = v[2 * P];
     c->xfft[P] = v[2 * P + 1] >= 1;
     if (P == 1) c->yz32 = v[3] == 2;
     c->interp_variant[P] = v[4 + P];
@@ -2582,32 +2582,35 @@ static int tune_precision(Ctx* c, int reps, double* t) {
   const BlobTable<T>& bt = gb.blobs;
   FCM_CUDA(cudaMemsetAsync(c->d_tmp3, 0, sizeof(double) * 3 * (size_t)(c->Nb > 0 ? c->Nb : 1), c->stream));
   if (bt.tiled) {
-    for (int v = 0; v < 2; ++v) {
-      c->spread_pipe[P] = v == 0;
+    for (int v = 0; v < 4; ++v) {
+      c->spread_variant[P] = v;
       FCM_TRY(time_calls(c, reps, [&] { return spread_t<T>(c, bt, c->d_tmp3); }, &t[v]));
     }
-    c->spread_pipe[P] = t[0] <= t[1];
+    int bs = 0;
+    for (int v = 1; v < 4; ++v)
+      if (t[v] < t[bs]) bs = v;
+    c->spread_variant[P] = bs;
   }
   FCM_CUDA(cudaMemsetAsync(gb.r, 0, sizeof(T) * 3 * (size_t)c->g.G, c->stream));
   for (int v = 0; v < 3; ++v) {
     if ((v >= 1 && !c->xfft_cap[P]) || (v == 2 && (P == 0 || !c->yz32_cap))) continue;
     c->xfft[P] = v >= 1;
     if (P == 1) c->yz32 = v == 2;
-    FCM_TRY(time_calls(c, reps, [&] { return stokes_t<T>(c); }, &t[2 + v]));
+    FCM_TRY(time_calls(c, reps, [&] { return stokes_t<T>(c); }, &t[4 + v]));
   }
   int best = 0;
   for (int v = 1; v < 3; ++v)
-    if (t[2 + v] >= 0.0 && t[2 + v] < t[2 + best]) best = v;
+    if (t[4 + v] >= 0.0 && t[4 + v] < t[4 + best]) best = v;
   c->xfft[P] = best >= 1;
   if (P == 1) c->yz32 = best == 2;
   if (bt.tiled) {  // interpolation of the (zeroed) grid into scratch
     for (int v = 0; v < 3; ++v) {
       c->interp_variant[P] = v;
-      FCM_TRY(time_calls(c, reps, [&] { return interp_t<T>(c, bt, gb.r, c->d_tmp3); }, &t[5 + v]));
+      FCM_TRY(time_calls(c, reps, [&] { return interp_t<T>(c, bt, gb.r, c->d_tmp3); }, &t[7 + v]));
     }
     int bi = 0;
     for (int v = 1; v < 3; ++v)
-      if (t[5 + v] < t[5 + bi]) bi = v;
+      if (t[7 + v] < t[7 + bi]) bi = v;
     c->interp_variant[P] = bi;
   }
   return FCM_OK;
@@ -3501,7 +3504,14 @@ int fcm_multiply_by_saddle_point_matrix(fcm_ctx* ctx, const double* in, double* 
     return FCM_ERR_STATE;
   }
   FCM_TRY(copy_in(c, c->d_sys_b, in, sizeof(double) * c->nsys));
-  FCM_TRY(saddle_matvec(c, 0, c->d_sys_b, c->d_sys_a));
+  // as the reference's product (gmres_solver.cpp:72-83) leaves M lambda in fcm.V
+  // (calculate_deterministic_blob_velocities), the context's V takes it here too
+  const double* lam = c->d_sys_b;
+  FCM_TRY(mobility_dev(c, 0, lam, c->d_sys_a));
+  FCM_CUDA(cudaMemcpyAsync(c->d_V, c->d_sys_a, sizeof(double) * 3 * (size_t)c->Nb, cudaMemcpyDeviceToDevice,
+                           c->stream));
+  FCM_TRY(launch_multiply_K(*c, c->d_qm, lam + 3 * (size_t)c->Nb, c->d_sys_a, 1.0, c->stream));
+  FCM_TRY(launch_multiply_KT(*c, c->d_qm, lam, c->d_sys_a + 3 * (size_t)c->Nb, -1.0, nullptr, 0.0, c->stream));
   return copy_out(c, out, c->d_sys_a, sizeof(double) * c->nsys);
 }
 

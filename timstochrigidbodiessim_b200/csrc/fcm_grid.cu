@@ -184,6 +184,27 @@ __device__ __forceinline__ void stage_blobs(const unsigned long long* __restrict
   }
 }
 
+// The same staging for NB blobs per round (any NB): the (blob, lane) pairs are
+// dealt to the 64 threads in turn.
+template <typename T, int NB>
+__device__ __forceinline__ void stage_blobs_n(const unsigned long long* __restrict__ list, int c0, int nc,
+                                              const T* __restrict__ wc, const double* __restrict__ F,
+                                              T (*sw)[3][TE], T (*sF)[4], unsigned* sflag) {
+  for (int i = threadIdx.x; i < 4 * nc; i += 64) {
+    const int k = i >> 2, d = i & 3;
+    const unsigned long long e = list[c0 + k];
+    const unsigned b = (unsigned)(e >> 32), lo = (unsigned)e;
+    if (d < 3) {
+      copy8(sw[k][d], wc + ((size_t)(3 * b + d) * NCH + ((lo >> (2 * d)) & 3u)) * TE);
+    } else {
+      sflag[k] = lo;
+      sF[k][0] = (T)F[3 * (size_t)b];
+      sF[k][1] = (T)F[3 * (size_t)b + 1];
+      sF[k][2] = (T)F[3 * (size_t)b + 2];
+    }
+  }
+}
+
 template <typename T>
 struct V4 {};
 template <>
@@ -223,14 +244,16 @@ __device__ __forceinline__ bool skip_x_half(unsigned fl, int h) {
 // accumulated in registers.  Warp h covers y-half h and skips blobs whose
 // stencil misses it; in FP64 an x-half the stencil misses is skipped by the
 // whole CTA (both branches are uniform).
-template <typename T>
+// NB blobs are staged per round (SCB by default); every point sums its blobs in
+// ascending blob order whatever NB is, so the grids are the same bit for bit.
+template <typename T, int NB = SCB>
 __device__ __forceinline__ void spread_tile(const T* __restrict__ wc, const double* __restrict__ F,
                                             const TileGeom& g, const int* __restrict__ offset,
                                             const unsigned long long* __restrict__ list, long long G,
                                             T* __restrict__ grid, int tile) {
-  __shared__ __align__(16) T sw[SCB][3][TE];
-  __shared__ __align__(16) T sF[SCB][4];
-  __shared__ unsigned sflag[SCB];
+  __shared__ __align__(16) T sw[NB][3][TE];
+  __shared__ __align__(16) T sF[NB][4];
+  __shared__ unsigned sflag[NB];
   const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
   const int t = threadIdx.x;
   const int z = t & 7, y = t >> 3, yh = t >> 5;
@@ -244,10 +267,10 @@ __device__ __forceinline__ void spread_tile(const T* __restrict__ wc, const doub
     for (int x = 0; x < TE / 2; ++x)
 #pragma unroll
       for (int c = 0; c < 3; ++c) acc2[x][c] = make_float2(0.f, 0.f);
-    for (int c0 = b0; c0 < b1; c0 += SCB) {
-      const int nc = min(SCB, b1 - c0);
+    for (int c0 = b0; c0 < b1; c0 += NB) {
+      const int nc = min(NB, b1 - c0);
       if (c0 != b0) __syncthreads();
-      stage_blobs<T>(list, c0, nc, wc, F, sw, sF, sflag);
+      stage_blobs_n<T, NB>(list, c0, nc, wc, F, sw, sF, sflag);
       __syncthreads();
       for (int k = 0; k < nc; ++k) {
         const unsigned fl = sflag[k];
@@ -281,10 +304,10 @@ __device__ __forceinline__ void spread_tile(const T* __restrict__ wc, const doub
   for (int x = 0; x < TE; ++x)
 #pragma unroll
     for (int c = 0; c < 3; ++c) acc[x][c] = 0;
-  for (int c0 = b0; c0 < b1; c0 += SCB) {
-    const int nc = min(SCB, b1 - c0);
+  for (int c0 = b0; c0 < b1; c0 += NB) {
+    const int nc = min(NB, b1 - c0);
     if (c0 != b0) __syncthreads();
-    stage_blobs<T>(list, c0, nc, wc, F, sw, sF, sflag);
+    stage_blobs_n<T, NB>(list, c0, nc, wc, F, sw, sF, sflag);
     __syncthreads();
     for (int k = 0; k < nc; ++k) {
       const unsigned fl = sflag[k];
@@ -315,12 +338,12 @@ __device__ __forceinline__ void spread_tile(const T* __restrict__ wc, const doub
   }
 }
 
-template <typename T>
+template <typename T, int NB = SCB>
 __global__ void __launch_bounds__(64) k_spread_tiled(const T* __restrict__ wc, const double* __restrict__ F,
                                                      TileGeom g, const int* __restrict__ offset,
                                                      const unsigned long long* __restrict__ list, long long G,
                                                      T* __restrict__ grid) {
-  spread_tile<T>(wc, F, g, offset, list, G, grid, blockIdx.x);
+  spread_tile<T, NB>(wc, F, g, offset, list, G, grid, blockIdx.x);
 }
 
 // ------------------------------------------------------------------ persistent pipelined tiles
@@ -956,14 +979,19 @@ template <typename T>
 int launch_spread(const Ctx& c, const BlobTable<T>& t, const double* dF, T* grid, cudaStream_t s) {
   if (t.tiled) {
     // by default FP64 takes the persistent pipelined kernel (its staging latency is
-    // the limit), FP32 one CTA per tile; fcm_autotune may choose the other
-    if (c.spread_pipe[sizeof(T) == 8 ? 0 : 1]) {
+    // the limit), FP32 one CTA per tile staging 16 blobs per round; fcm_autotune may
+    // choose another (one CTA per tile with 8 or 32 blobs per round)
+    const int v = c.spread_variant[sizeof(T) == 8 ? 0 : 1];
+    const TileGeom tg = tile_geom(c.g, t.W);
+    if (v == 0) {
       const int ctas = std::min(t.ntiles, persistent_ctas(k_spread_pipe<T>, 64, c.device));
-      k_spread_pipe<T><<<ctas, 64, 0, s>>>(t.wc, dF, tile_geom(c.g, t.W), t.tile_offset, t.tile_list, c.g.G, grid,
-                                          t.ntiles);
+      k_spread_pipe<T><<<ctas, 64, 0, s>>>(t.wc, dF, tg, t.tile_offset, t.tile_list, c.g.G, grid, t.ntiles);
+    } else if (v == 2) {
+      k_spread_tiled<T, 8><<<t.ntiles, 64, 0, s>>>(t.wc, dF, tg, t.tile_offset, t.tile_list, c.g.G, grid);
+    } else if (v == 3) {
+      k_spread_tiled<T, 32><<<t.ntiles, 64, 0, s>>>(t.wc, dF, tg, t.tile_offset, t.tile_list, c.g.G, grid);
     } else {
-      k_spread_tiled<T><<<t.ntiles, 64, 0, s>>>(t.wc, dF, tile_geom(c.g, t.W), t.tile_offset, t.tile_list, c.g.G,
-                                                 grid);
+      k_spread_tiled<T, 16><<<t.ntiles, 64, 0, s>>>(t.wc, dF, tg, t.tile_offset, t.tile_list, c.g.G, grid);
     }
     FCM_LAUNCH_CHECK();
     return FCM_OK;

@@ -272,9 +272,10 @@ struct Ctx {
   // precision (its (y, z) plans exist), the library's (y, z) kernels up to 512 points
   bool xfft_cap[2] = {false, false};
   bool yz32_cap = false;
-  // spread kernel per precision: the persistent software-pipelined one (FP64
-  // default) or one CTA per tile (FP32 default); both sum in the same order
-  bool spread_pipe[2] = {true, false};
+  // spread kernel per precision: 0 the persistent software-pipelined one (FP64
+  // default), 1 / 2 / 3 one CTA per tile staging 16 (FP32 default) / 8 / 32 blobs
+  // per round; all sum every point's blobs in the same order
+  int spread_variant[2] = {0, 1};
   // interpolation kernel per precision: 0 the shuffle-reduced tile kernel
   // (k_interp_tiled), 1 / 2 the shared-memory reduced kernel with one / two y-rows
   // per thread (k_interp_rows, 64 / 32 threads per tile)

@@ -326,7 +326,8 @@ class Suspension:
         return V
 
     # kernel variants: [FP64 spread, FP64 solve, FP32 spread, FP32 solve, FP64
-    # interp, FP32 interp]; spread 0 = persistent pipelined, 1 = one CTA per tile;
+    # interp, FP32 interp]; spread 0 = persistent pipelined, 1 / 2 / 3 = one CTA
+    # per tile staging 16 / 8 / 32 blobs per round;
     # solve 0 = cuFFT 3D, 1 = cuFFT (y, z) + fused x-transform, 2 = the library's
     # (y, z) + fused x; interp 0 = shuffle reduction, 1 / 2 = shared-memory
     # reduction with 64 / 32 threads per tile
@@ -343,10 +344,10 @@ class Suspension:
 
     def autotune(self, reps=5):
         """Time every variant the grids allow and keep the fastest.  Returns
-        (variants, us): us[8 P + v] microseconds per call for precision P, v = 0, 1
-        spread variants, 2, 3, 4 solve variants, 5, 6, 7 interpolation variants
+        (variants, us): us[10 P + v] microseconds per call for precision P, v = 0-3
+        spread variants, 4, 5, 6 solve variants, 7, 8, 9 interpolation variants
         (-1 where not available)."""
-        us, pu = _out(None, 16)
+        us, pu = _out(None, 20)
         v, pv = _out(None, self.NUM_VARIANTS, np.int32)
         self._c(self.L.fcm_autotune(self.h, reps, pu, pv), "fcm_autotune")
         return [int(x) for x in v], us
