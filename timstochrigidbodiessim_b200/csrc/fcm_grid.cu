@@ -801,6 +801,39 @@ __global__ void k_interp_reduce(const int* __restrict__ base, const T* __restric
   interp_reduce_one<T>(base, partial, g, dx3, V, b);
 }
 
+// The same sums with eight lanes per blob: lane k adds the partials j = k, k + 8,
+// ... (consecutive lanes read consecutive partials, so the loads coalesce), then
+// the eight lanes combine in a fixed butterfly.  Deterministic; 16 blobs per
+// 128-thread CTA.
+template <typename T>
+__global__ void __launch_bounds__(128) k_interp_reduce8(const int* __restrict__ base, const T* __restrict__ partial,
+                                                        int n, TileGeom g, double dx3, double* __restrict__ V) {
+  const int b = blockIdx.x * 16 + (threadIdx.x >> 3), k = threadIdx.x & 7;
+  double s0 = 0, s1 = 0, s2 = 0;
+  if (b < n) {
+    int f[3], cnt[3];
+    blob_tiles(base, b, g, f, cnt);
+    const int nj = cnt[0] * cnt[1] * cnt[2];
+    const T* p = partial + (size_t)b * 64 * 3;
+    for (int j = k; j < nj; j += 8) {
+      s0 += (double)p[3 * j];
+      s1 += (double)p[3 * j + 1];
+      s2 += (double)p[3 * j + 2];
+    }
+  }
+#pragma unroll
+  for (int off = 4; off >= 1; off >>= 1) {  // groups of eight lanes, aligned in the warp
+    s0 += __shfl_xor_sync(0xffffffffu, s0, off);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, off);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, off);
+  }
+  if (b < n && k == 0) {
+    V[3 * b] = s0 * dx3;
+    V[3 * b + 1] = s1 * dx3;
+    V[3 * b + 2] = s2 * dx3;
+  }
+}
+
 // Spreading of grids that cannot be tiled: one CTA per blob, each thread owns
 // stencil columns (j,k) and walks x, atomics into the zeroed grid.
 template <typename T>
@@ -1019,7 +1052,7 @@ int launch_interp(const Ctx& c, const BlobTable<T>& t, const T* grid, double* dV
     else
       k_interp_tiled<T><<<t.ntiles, 64, 0, s>>>(t.wc, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial);
     FCM_LAUNCH_CHECK();
-    k_interp_reduce<T><<<(t.n + 127) / 128, 128, 0, s>>>(t.base, t.partial, t.n, g, dx3, dV);
+    k_interp_reduce8<T><<<(t.n + 15) / 16, 128, 0, s>>>(t.base, t.partial, t.n, g, dx3, dV);
     FCM_LAUNCH_CHECK();
     return FCM_OK;
   }
