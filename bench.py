@@ -58,6 +58,8 @@ def parse():
                          "kernels a profiler can list one by one")
     ap.add_argument("--kernels-only", type=int, default=0, metavar="R",
                     help="profiling mode: R FP64 spread+interp launches and R FP32 mobility products, no steps")
+    ap.add_argument("--kernels-precision", type=int, default=None, choices=[0, 1],
+                    help="--kernels-only: run only this precision's grid (0 FP64, 1 FP32)")
     ap.add_argument("--variants", default=None,
                     help="--kernels-only: six comma-separated kernel variants (fcm_set_variants) to run")
     ap.add_argument("--ref-budget", type=float, default=180.0,
@@ -578,7 +580,7 @@ def run_kernels_only(args):
     torch.cuda.set_device(0)
     stream = torch.cuda.Stream()
     p, ref, x, q, fe = configs.workload(args.workload)
-    for prec in (0, 1):
+    for prec in ((0, 1) if args.kernels_precision is None else (args.kernels_precision,)):
         s = configs.make_suspension(p.copy(precision=prec), ref, stream=stream)
         if args.variants:
             s.set_variants([int(v) for v in args.variants.split(",")])

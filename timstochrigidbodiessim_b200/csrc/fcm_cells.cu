@@ -42,16 +42,26 @@ __global__ void k_cell_ids(const double* __restrict__ Y, int Nb, CellGeom g, int
 }
 
 // Single-CTA exclusive scan of n ints (n up to a few million).
+// Exclusive prefix sum of in[0..n) into out[0..n], out[n] = total, by one CTA:
+// each pass covers blockDim.x * 8 entries, every thread summing eight
+// consecutive ones, the thread totals scanned by warp shuffles and a second
+// warp level.
 __global__ void k_exclusive_scan(const int* __restrict__ in, int* __restrict__ out, int n) {
+  constexpr int IPT = 8;
   __shared__ int warp_sums[32];
   __shared__ int carry;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int base = 0; base < n; base += blockDim.x) {
-    const int i = base + threadIdx.x;
-    const int v = (i < n) ? in[i] : 0;
-    int x = v;
+  for (int base = 0; base < n; base += blockDim.x * IPT) {
+    const int i0 = base + threadIdx.x * IPT;
+    int v[IPT], tot = 0;
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+      v[k] = (i0 + k < n) ? in[i0 + k] : 0;
+      tot += v[k];
+    }
+    int x = tot;
     for (int off = 1; off < 32; off <<= 1) {
       const int y = __shfl_up_sync(0xffffffffu, x, off);
       if (lane >= off) x += y;
@@ -59,18 +69,22 @@ __global__ void k_exclusive_scan(const int* __restrict__ in, int* __restrict__ o
     if (lane == 31) warp_sums[wid] = x;
     __syncthreads();
     if (wid == 0) {
-      int s = (lane < (int)(blockDim.x >> 5)) ? warp_sums[lane] : 0;
+      int s2 = (lane < (int)(blockDim.x >> 5)) ? warp_sums[lane] : 0;
       for (int off = 1; off < 32; off <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, s, off);
-        if (lane >= off) s += y;
+        const int y = __shfl_up_sync(0xffffffffu, s2, off);
+        if (lane >= off) s2 += y;
       }
-      warp_sums[lane] = s;
+      warp_sums[lane] = s2;
     }
     __syncthreads();
-    const int wprefix = (wid > 0) ? warp_sums[wid - 1] : 0;
-    if (i < n) out[i] = carry + wprefix + x - v;
+    int run = carry + ((wid > 0) ? warp_sums[wid - 1] : 0) + x - tot;
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+      if (i0 + k < n) out[i0 + k] = run;
+      run += v[k];
+    }
     __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) carry += wprefix + x;
+    if (threadIdx.x == blockDim.x - 1) carry = run;
     __syncthreads();
   }
   if (threadIdx.x == 0) out[n] = carry;

@@ -143,6 +143,55 @@ __global__ void k_tile_sort(const int* __restrict__ offset, int ntiles, unsigned
   }
 }
 
+// The same order, one warp per tile: the tile's entries (all distinct) are
+// loaded into a shared buffer padded to a power of two with all-ones keys and
+// bitonic-sorted by the warp; tiles with more than TSORT entries are sorted by
+// lane 0 in place as k_tile_sort does.  128 threads = four tiles per CTA.
+constexpr int TSORT = 256;
+__global__ void __launch_bounds__(128) k_tile_sort_warp(const int* __restrict__ offset, int ntiles,
+                                                        unsigned long long* __restrict__ list) {
+  __shared__ unsigned long long buf[4][TSORT];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int t = blockIdx.x * 4 + w;
+  if (t >= ntiles) return;  // uniform over the warp
+  const int b = offset[t], e = offset[t + 1], n = e - b;
+  if (n < 2) return;
+  if (n > TSORT) {
+    if (lane == 0)
+      for (int i = b + 1; i < e; ++i) {
+        const unsigned long long v = list[i];
+        int j = i - 1;
+        while (j >= b && list[j] > v) {
+          list[j + 1] = list[j];
+          --j;
+        }
+        list[j + 1] = v;
+      }
+    return;
+  }
+  int P = 2;
+  while (P < n) P <<= 1;
+  unsigned long long* a = buf[w];
+  for (int i = lane; i < P; i += 32) a[i] = i < n ? list[b + i] : ~0ull;
+  __syncwarp();
+  for (int k = 2; k <= P; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = lane; i < P; i += 32) {
+        const int l = i ^ j;
+        if (l > i) {
+          const unsigned long long x = a[i], y = a[l];
+          const bool up = (i & k) == 0;
+          if ((x > y) == up) {
+            a[i] = y;
+            a[l] = x;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  for (int i = lane; i < n; i += 32) list[b + i] = a[i];
+}
+
 // Eight consecutive T from global (aligned to 8*sizeof(T)) to shared memory.
 __device__ __forceinline__ void copy8(double* dst, const double* __restrict__ src) {
   const double2* s = reinterpret_cast<const double2*>(src);
@@ -1002,7 +1051,7 @@ int launch_set_up_gaussians(const Ctx& c, BlobTable<T>& t, const double* dY, cud
     FCM_TRY(launch_exclusive_scan(t.tile_count, t.tile_offset, t.ntiles, s));
     k_tile_fill<<<(t.n + 127) / 128, 128, 0, s>>>(t.base, t.n, g, t.tile_offset, t.tile_cursor, t.tile_list);
     FCM_LAUNCH_CHECK();
-    k_tile_sort<<<(t.ntiles + 127) / 128, 128, 0, s>>>(t.tile_offset, t.ntiles, t.tile_list);
+    k_tile_sort_warp<<<(t.ntiles + 3) / 4, 128, 0, s>>>(t.tile_offset, t.ntiles, t.tile_list);
     FCM_LAUNCH_CHECK();
   }
   return FCM_OK;
