@@ -479,6 +479,26 @@ int fcm_step_many(fcm_ctx* const* ctxs, int32_t n, const uint64_t* seeds, uint64
 int fcm_interp_noalloc(int32_t nx, int32_t ny, int32_t nz, double dx, double blob_radius, int32_t ngauss,
                        int32_t nblobs, const double* Y, const double* grid, double* V, void* stream);
 
+/* ================================================================ bounds-checked build
+ * No counterpart in the reference (which has no device code).  The library is
+ * also built with every device index checked (libfcm_b200_debug.so, same entry
+ * points): grid point indices against the grid, blob ids read from the tile and
+ * cell lists against the blob count, tile and cell ids, tile-list and cell-list
+ * slots against their ranges and capacities, per-(blob, tile) partials, spectrum
+ * indices of the fused x-transform and projection, and Krylov columns against the
+ * columns allocated.  A kernel that meets an index outside its range counts it,
+ * keeps the first one's site, index and limit, skips the access and runs on: no
+ * trap, no assert.  This call waits for the current device, then writes
+ * *checked = 1 in the checked build (0 in the release build, whose counts are
+ * always zero), the number of violations on the current device since the last
+ * reset, and the first one's site (1 grid point, 2 blob id, 3 tile id, 4 list
+ * slot, 5 partial, 6 cell id, 7 spectrum index, 8 Krylov column; 0 none), index
+ * and limit; reset != 0 then clears the counts.  Any output pointer may be NULL.
+ * Returns FCM_OK or FCM_ERR_CUDA. */
+#define FCM_BOUNDS_SITES 8
+int fcm_debug_bounds(int32_t* checked, int64_t* count, int32_t* site, int64_t* index, int64_t* limit,
+                     int32_t reset);
+
 #ifdef __cplusplus
 }
 #endif

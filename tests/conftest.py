@@ -42,6 +42,22 @@ def gpu():
     return capi.load()
 
 
+@pytest.fixture(autouse=True)
+def _bounds_checked_run():
+    """With FCM_B200_BOUNDS_CHECK=1 the bounds-checked library is loaded
+    (timstochrigidbodiessim_b200.capi); then every test that touched the GPU must
+    end with no device index outside its range (fcm_debug_bounds)."""
+    if os.environ.get("FCM_B200_BOUNDS_CHECK") != "1" or not _cuda_available():
+        yield
+        return
+    from timstochrigidbodiessim_b200 import capi
+    capi.debug_bounds(reset=True)
+    yield
+    checked, count, site, index, limit = capi.debug_bounds(reset=True)
+    assert checked, "FCM_B200_BOUNDS_CHECK=1 but the release library is loaded"
+    assert count == 0, "%d device indices out of range; first: %s %d of %d" % (count, site, index, limit)
+
+
 def rel_err(a, b):
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)

@@ -1,7 +1,8 @@
 """Build recipe of the B200 FCM library: every CUDA source in csrc/ is compiled
 for sm_100a and linked, with cuFFT, into timstochrigidbodiessim_b200/libfcm_b200.so
-(in-tree, so it ships with the repository snapshot).  Run
-``python -m timstochrigidbodiessim_b200.build``.
+(in-tree, so it ships with the repository snapshot), and a second time with
+-DFCM_BOUNDS_CHECK (every device index checked, violations counted and skipped)
+into libfcm_b200_debug.so.  Run ``python -m timstochrigidbodiessim_b200.build``.
 """
 import concurrent.futures as cf
 import glob
@@ -15,6 +16,8 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(PKG, "libfcm_b200.so")
+DEBUG_LIB = os.path.join(PKG, "libfcm_b200_debug.so")
+DEBUG_BUILD = os.path.join(BUILD, "bounds_check")
 HOST_LIB = os.path.join(PKG, "libfcm_b200_host.so")
 DRIVER = os.path.join(PKG, "rigid_bodies_sim")
 HOST_DIR = os.path.join(CSRC, "host")
@@ -32,8 +35,8 @@ def _sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
 
 
-def _compile(src, extra):
-    obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+def _compile(src, extra, out_dir=BUILD):
+    obj = os.path.join(out_dir, os.path.basename(src) + ".o")
     if (os.path.exists(obj) and os.path.getmtime(obj) > os.path.getmtime(src)
             and all(os.path.getmtime(obj) > os.path.getmtime(h)
                     for h in glob.glob(os.path.join(CSRC, "*.cuh")) + [os.path.join(ROOT, "include", "fcm_b200.h")])):
@@ -45,25 +48,31 @@ def _compile(src, extra):
     return obj, r.stderr
 
 
-def build(verbose=False, ptxas_info=False):
-    os.makedirs(BUILD, exist_ok=True)
-    extra = ["-Xptxas", "-v"] if ptxas_info else []
+def _build_lib(lib, out_dir, extra, verbose):
+    os.makedirs(out_dir, exist_ok=True)
     srcs = _sources()
     with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
-        results = list(ex.map(lambda s: _compile(s, extra), srcs))
+        results = list(ex.map(lambda s: _compile(s, extra, out_dir), srcs))
     objs = [o for o, _ in results]
     if verbose:
         for _, log in results:
             if log:
                 sys.stderr.write(log)
     newest = max(os.path.getmtime(o) for o in objs)
-    if not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
-        cmd = [NVCC] + GENCODE + ["-shared", "-o", LIB] + objs + [
+    if not os.path.exists(lib) or os.path.getmtime(lib) < newest:
+        cmd = [NVCC] + GENCODE + ["-shared", "-o", lib] + objs + [
             "-L" + os.path.join(CUDA_HOME, "lib64"), "-lcufft", "-lcudart",
             "-Xlinker", "-rpath," + os.path.join(CUDA_HOME, "lib64")]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (" ".join(cmd), r.stderr))
+
+
+def build(verbose=False, ptxas_info=False, bounds_check=True):
+    extra = ["-Xptxas", "-v"] if ptxas_info else []
+    _build_lib(LIB, BUILD, extra, verbose)
+    if bounds_check:
+        _build_lib(DEBUG_LIB, DEBUG_BUILD, extra + ["-DFCM_BOUNDS_CHECK"], verbose)
     _build_host()
     return LIB
 
@@ -90,7 +99,7 @@ def _build_host():
 
 def clean():
     shutil.rmtree(BUILD, ignore_errors=True)
-    for f in (LIB, HOST_LIB, DRIVER):
+    for f in (LIB, DEBUG_LIB, HOST_LIB, DRIVER):
         if os.path.exists(f):
             os.remove(f)
 
@@ -98,4 +107,4 @@ def clean():
 if __name__ == "__main__":
     if "--clean" in sys.argv:
         clean()
-    print(build(verbose=True, ptxas_info="--ptxas" in sys.argv))
+    print(build(verbose=True, ptxas_info="--ptxas" in sys.argv, bounds_check="--no-bounds-check" not in sys.argv))

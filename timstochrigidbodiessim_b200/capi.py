@@ -2,14 +2,19 @@
 
 The library is loaded from the package directory; if it is missing the import
 fails loudly (build it with ``python -m timstochrigidbodiessim_b200.build``).
-There is no CPU fallback.
+There is no CPU fallback.  With FCM_B200_BOUNDS_CHECK=1 in the environment the
+bounds-checked build of the same library (libfcm_b200_debug.so) is loaded
+instead; fcm_debug_bounds reports what its index checks found.
 """
 import ctypes
 import os
 
 from .params import FcmMcmcState, FcmParams, FcmStepInfo
 
-LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libfcm_b200.so")
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+DEBUG_LIB_PATH = os.path.join(PKG_DIR, "libfcm_b200_debug.so")
+LIB_PATH = DEBUG_LIB_PATH if os.environ.get("FCM_B200_BOUNDS_CHECK") == "1" else os.path.join(PKG_DIR,
+                                                                                               "libfcm_b200.so")
 
 D = ctypes.POINTER(ctypes.c_double)
 I32 = ctypes.POINTER(ctypes.c_int32)
@@ -22,6 +27,7 @@ SIGNATURES = {
     "fcm_last_error": (ctypes.c_char_p, []),
     "fcm_version": (ctypes.c_char_p, []),
     "fcm_kernel_launch_count": (ctypes.c_int64, []),
+    "fcm_debug_bounds": (ctypes.c_int, [I32, I64, I32, I64, I64, ctypes.c_int32]),
     "fcm_fft_create": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(VP)]),
     "fcm_fft_destroy": (ctypes.c_int, [VP]),
     "fcm_fft_local_sizes": (ctypes.c_int, [VP, I32, I32, I32, I32, I64, I32]),
@@ -131,6 +137,22 @@ def load(path=LIB_PATH):
         f.argtypes = args
     _lib = L
     return L
+
+
+BOUNDS_SITES = {0: "none", 1: "grid point", 2: "blob id", 3: "tile id", 4: "list slot", 5: "partial",
+                6: "cell id", 7: "spectrum index", 8: "Krylov column"}
+
+
+def debug_bounds(reset=False):
+    """fcm_debug_bounds: (checked, violations, first site name, index, limit) on
+    the current device; checked is False for the release build."""
+    L = load()
+    chk, site = ctypes.c_int32(0), ctypes.c_int32(0)
+    cnt, idx, lim = ctypes.c_int64(0), ctypes.c_int64(0), ctypes.c_int64(0)
+    check(L.fcm_debug_bounds(ctypes.byref(chk), ctypes.byref(cnt), ctypes.byref(site), ctypes.byref(idx),
+                             ctypes.byref(lim), 1 if reset else 0), "fcm_debug_bounds")
+    return bool(chk.value), int(cnt.value), BOUNDS_SITES.get(site.value, str(site.value)), int(idx.value), \
+        int(lim.value)
 
 
 def check(status, where, ok=(0,)):

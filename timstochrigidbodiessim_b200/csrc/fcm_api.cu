@@ -369,14 +369,17 @@ GridBufs<double>& grid_of<double>(Ctx* c) { return c->g64; }
 template <>
 GridBufs<float>& grid_of<float>(Ctx* c) { return c->g32; }
 
-// Stencil width of the FP32 tables: the reference's W, narrowed where it reaches
-// beyond 6.5 sigma on each side (weights below 7e-10 of the peak, under the
-// FP32 path's accuracy; the FP64 residual of the refinement keeps the full W).
+// Stencil width of the FP32 tables: the reference's W, narrowed to the smallest
+// even width whose excluded points all lie at least 5.5 sigma from the blob
+// (a W-point stencil starting at int(Y/DX) - W/2 + 1 excludes only points W/2
+// or more grid spacings away).  The Gaussian mass beyond 5.5 sigma is 3.8e-8 of
+// the total per dimension, below FP32 rounding; the FP64 residual of the
+// refinement keeps the full W.
 int fp32_stencil(const Ctx* c) {
   const double PI = 3.14159265358979323846264338327950288;
   const double sigma = c->p.blob_radius / std::sqrt(PI);
-  const int half = (int)std::ceil(6.5 * sigma / c->g.dx);
-  return std::min(c->p.ngauss, 2 * half + 2);
+  const int half = (int)std::ceil(5.5 * sigma / c->g.dx);
+  return std::min(c->p.ngauss, std::max(2, 2 * half));
 }
 
 // The fused x-transform path of the Stokes solve (stokes_t) when nx has a kernel
@@ -2380,8 +2383,8 @@ int create_batch(int n, const fcm_params* params, const double* const* refs, Bat
       m.spec[1] = c->g32.c;
       m.partial[1] = c->g32.blobs.partial;
     }
-    m.tg[0] = tile_geom(c->g, c->g64.blobs.W);
-    m.tg[1] = tile_geom(c->g, B->precision == 1 ? c->g32.blobs.W : c->g64.blobs.W);
+    m.tg[0] = tile_geom(c->g, c->g64.blobs);
+    m.tg[1] = B->precision == 1 ? tile_geom(c->g, c->g32.blobs) : tile_geom(c->g, c->g64.blobs);
     m.kp = make_kparams(*c);
     m.dx3 = c->g.dx * c->g.dx * c->g.dx;
     m.xfft[0] = c->xfft[0] ? 1 : 0;
@@ -2648,6 +2651,34 @@ void fcm_default_params(fcm_params* p) {
 const char* fcm_last_error(void) { return g_err.c_str(); }
 const char* fcm_version(void) { return "fcm_b200 0.1 (sm_100a)"; }
 int64_t fcm_kernel_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int fcm_debug_bounds(int32_t* checked, int64_t* count, int32_t* site, int64_t* index, int64_t* limit,
+                     int32_t reset) {
+  return guard([&] {
+#ifdef FCM_BOUNDS_CHECK
+    const int on = 1;
+    FCM_CUDA(cudaDeviceSynchronize());
+#else
+    const int on = 0;
+#endif
+    int (*readers[])(BoundsRecord*, int) = {bounds_read_grid, bounds_read_cells, bounds_read_kspace,
+                                            bounds_read_blas};
+    unsigned long long total = 0;
+    BoundsRecord first{};
+    for (auto rd : readers) {
+      BoundsRecord r{};
+      FCM_TRY(rd(&r, reset));
+      if (r.count && !total) first = r;
+      total += r.count;
+    }
+    if (checked) *checked = on;
+    if (count) *count = (int64_t)total;
+    if (site) *site = total ? first.site : 0;
+    if (index) *index = total ? first.index : 0;
+    if (limit) *limit = total ? first.limit : 0;
+    return (int)FCM_OK;
+  });
+}
 
 int fcm_create(const fcm_params* p, const double* blob_ref_pos, fcm_ctx** out) {
   return guard([&] {

@@ -258,9 +258,10 @@ __global__ void k_gs_update(const GmState* __restrict__ st, const double* __rest
 
 // Q[k+1] = w / |w| (|w| = 0: a happy breakdown, the column is left as w)
 __global__ void k_gm_normalize(const GmState* __restrict__ st, const double* __restrict__ w,
-                               const double* __restrict__ hnorm, long long n, double* __restrict__ Q) {
+                               const double* __restrict__ hnorm, long long n, double* __restrict__ Q, int hn) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= n || st->done) return;
+  if (!FCM_INB(st->k + 1, hn, BS_KRYLOV)) return;
   const double s = *hnorm;
   Q[(size_t)(st->k + 1) * n + t] = (s != 0.0) ? w[t] / s : w[t];
 }
@@ -272,6 +273,11 @@ __device__ __forceinline__ void givens_step(GmState* st, double* __restrict__ H,
                                             const double* __restrict__ hnorm) {
   if (st->done) return;
   const int iter = st->k + 1;
+  if (!FCM_INB(iter, hn, BS_KRYLOV)) {  // no column left for Q[k+1]: end the solve
+    st->done = 1;
+    st->status = FCM_ERR_NOT_CONVERGED;
+    return;
+  }
   double* col = H + (size_t)(iter - 1) * hn;
   for (int i = 0; i < iter; ++i) col[i] = hA[i] + hB[i];
   col[iter] = *hnorm;
@@ -388,7 +394,7 @@ int gm_orthogonalize(const Ctx& c, double* w, cudaStream_t s) {
     FCM_LAUNCH_CHECK();
   }
   FCM_TRY(blas_norm_sq_partial(c, w, n, c.d_hnorm, s));
-  k_gm_normalize<<<nblk(n, 256), 256, 0, s>>>(c.gm, w, c.d_hnorm, n, c.d_Qm);
+  k_gm_normalize<<<nblk(n, 256), 256, 0, s>>>(c.gm, w, c.d_hnorm, n, c.d_Qm, c.maxit_alloc + 1);
   FCM_LAUNCH_CHECK();
   k_gm_givens<<<1, 32, 0, s>>>(c.gm, c.d_Hd, c.maxit_alloc + 1, c.d_beta, c.d_CS, c.d_SN, c.d_hA, c.d_hB,
                                c.d_hnorm);
@@ -548,6 +554,7 @@ __global__ void k_b_normalize(const BMember* __restrict__ mem) {
   const BMember& m = mem[blockIdx.y];
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= m.nsys || m.gm->done) return;
+  if (!FCM_INB(m.gm->k + 1, m.hn, BS_KRYLOV)) return;
   const double s = *m.hnorm;
   m.Qm[(size_t)(m.gm->k + 1) * m.nsys + t] = (s != 0.0) ? m.sys_b[t] / s : m.sys_b[t];
 }
@@ -626,5 +633,7 @@ int b_gm_finish(const BatchGeom& b, cudaStream_t s) {
   FCM_LAUNCH_CHECK();
   return FCM_OK;
 }
+
+FCM_BOUNDS_READER(bounds_read_blas)
 
 }  // namespace fcm

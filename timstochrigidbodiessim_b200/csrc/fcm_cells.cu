@@ -38,7 +38,7 @@ __global__ void k_cell_ids(const double* __restrict__ Y, int Nb, CellGeom g, int
   const int cz = cell_coord(Y[3 * i + 2], g.Lz, g.N);
   const int id = cx + cy * g.N + cz * g.N * g.N;
   cell[i] = id;
-  atomicAdd(count + id, 1);
+  if (FCM_INB(id, (long long)g.N * g.N * g.N, BS_CELL)) atomicAdd(count + id, 1);
 }
 
 // Single-CTA exclusive scan of n ints (n up to a few million).
@@ -90,12 +90,14 @@ __global__ void k_exclusive_scan(const int* __restrict__ in, int* __restrict__ o
   if (threadIdx.x == 0) out[n] = carry;
 }
 
-__global__ void k_cell_scatter(const int* __restrict__ cell, int Nb, const int* __restrict__ start,
+__global__ void k_cell_scatter(const int* __restrict__ cell, int Nb, int ncell, const int* __restrict__ start,
                                int* __restrict__ cursor, int* __restrict__ sorted) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= Nb) return;
   const int c = cell[i];
-  sorted[start[c] + atomicAdd(cursor + c, 1)] = i;
+  if (!FCM_INB(c, ncell, BS_CELL)) return;
+  const int slot = start[c] + atomicAdd(cursor + c, 1);
+  if (FCM_INB(slot, start[c + 1], BS_LIST) && FCM_INB(slot, Nb, BS_LIST)) sorted[slot] = i;
 }
 
 // Ascending blob order within each cell, so every traversal is deterministic.
@@ -103,6 +105,7 @@ __global__ void k_cell_sort(const int* __restrict__ start, int ncell, int* __res
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncell) return;
   const int b = start[c], e = start[c + 1];
+  if (!FCM_INB(b, (long long)e + 1, BS_LIST) || !FCM_INB(e, (long long)start[ncell] + 1, BS_LIST)) return;
   for (int i = b + 1; i < e; ++i) {
     const int v = sorted[i];
     int j = i - 1;
@@ -217,6 +220,7 @@ template <class Fn>
 __device__ __forceinline__ void visit_partners(const PairArgs& a, int i, Fn fn) {
   const int N = a.g.N;
   const int id = a.cell[i];
+  if (!FCM_INB(id, (long long)N * N * N, BS_CELL)) return;
   const int cx = id % N, cy = (id / N) % N, cz = id / (N * N);
   const int body = i / a.nb;
   const double x1 = a.Y[3 * i], y1 = a.Y[3 * i + 1], z1 = a.Y[3 * i + 2];
@@ -229,7 +233,9 @@ __device__ __forceinline__ void visit_partners(const PairArgs& a, int i, Fn fn) 
         const int c = xx + yy * N + zz * N * N;
         const int e = a.start[c + 1];
         for (int s = a.start[c]; s < e; ++s) {
+          if (!FCM_INB(s, a.Nb, BS_LIST)) break;
           const int j = a.sorted[s];
+          if (!FCM_INB(j, a.Nb, BS_BLOB)) continue;
           if (j == i || j / a.nb == body) continue;
           const double xd = min_image(__dsub_rn(x1, a.Y[3 * j]), a.g.Lx);
           const double yd = min_image(__dsub_rn(y1, a.Y[3 * j + 1]), a.g.Ly);
@@ -371,7 +377,7 @@ int cells_build(Ctx& c, cudaStream_t s) {
   FCM_LAUNCH_CHECK();
   k_exclusive_scan<<<1, 1024, 0, s>>>(c.d_cell_count, c.d_cell_start, nc);
   FCM_LAUNCH_CHECK();
-  k_cell_scatter<<<(c.Nb + 255) / 256, 256, 0, s>>>(c.d_cell, c.Nb, c.d_cell_start, c.d_cell_cursor,
+  k_cell_scatter<<<(c.Nb + 255) / 256, 256, 0, s>>>(c.d_cell, c.Nb, nc, c.d_cell_start, c.d_cell_cursor,
                                                     c.d_cell_sorted);
   FCM_LAUNCH_CHECK();
   k_cell_sort<<<(nc + 255) / 256, 256, 0, s>>>(c.d_cell_start, nc, c.d_cell_sorted);
@@ -424,5 +430,7 @@ int cells_count_pairs(const Ctx& c, long long* d_count, int* pairs, long long ca
   FCM_LAUNCH_CHECK();
   return FCM_OK;
 }
+
+FCM_BOUNDS_READER(bounds_read_cells)
 
 }  // namespace fcm

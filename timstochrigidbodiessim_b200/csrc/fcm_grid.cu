@@ -102,7 +102,7 @@ __global__ void k_tile_count(const int* __restrict__ base, int n, TileGeom g, in
       for (int oz = 0; oz < cnt[2]; ++oz) {
         const int tile = (wrap_index(f[0] + ox, g.ntx) * g.nty + wrap_index(f[1] + oy, g.nty)) * g.ntz +
                          wrap_index(f[2] + oz, g.ntz);
-        atomicAdd(count + tile, 1);
+        if (FCM_INB(tile, (long long)g.ntx * g.nty * g.ntz, BS_TILE)) atomicAdd(count + tile, 1);
       }
 }
 
@@ -118,20 +118,25 @@ __global__ void k_tile_fill(const int* __restrict__ base, int n, TileGeom g, con
       for (int oz = 0; oz < cnt[2]; ++oz) {
         const int tile = (wrap_index(f[0] + ox, g.ntx) * g.nty + wrap_index(f[1] + oy, g.nty)) * g.ntz +
                          wrap_index(f[2] + oz, g.ntz);
+        if (!FCM_INB(tile, (long long)g.ntx * g.nty * g.ntz, BS_TILE)) continue;
         const unsigned j = (unsigned)((ox * cnt[1] + oy) * cnt[2] + oz);
         const unsigned lo = (unsigned)ox | ((unsigned)oy << 2) | ((unsigned)oz << 4) | (j << EJ) |
                             (half_mask(lx, g.W, (f[0] + ox) * TE) << EXM) |
                             (half_mask(ly, g.W, (f[1] + oy) * TE) << EYM) |
                             (half_mask(lz, g.W, (f[2] + oz) * TE) << EZM);
-        list[offset[tile] + atomicAdd(cursor + tile, 1)] = ((unsigned long long)b << 32) | lo;
+        const int slot = offset[tile] + atomicAdd(cursor + tile, 1);
+        if (FCM_INB(slot, offset[tile + 1], BS_LIST) && FCM_INB(slot, g.list_cap, BS_LIST))
+          list[slot] = ((unsigned long long)b << 32) | lo;
       }
 }
 
 // Ascending blob order within each tile (a blob meets a tile at most once).
-__global__ void k_tile_sort(const int* __restrict__ offset, int ntiles, unsigned long long* __restrict__ list) {
+__global__ void k_tile_sort(const int* __restrict__ offset, int ntiles, unsigned long long* __restrict__ list,
+                            long long cap) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ntiles) return;
   const int b = offset[t], e = offset[t + 1];
+  if (!FCM_INB(b, (long long)e + 1, BS_LIST) || !FCM_INB(e, cap + 1, BS_LIST)) return;
   for (int i = b + 1; i < e; ++i) {
     const unsigned long long v = list[i];
     int j = i - 1;
@@ -149,12 +154,13 @@ __global__ void k_tile_sort(const int* __restrict__ offset, int ntiles, unsigned
 // lane 0 in place as k_tile_sort does.  128 threads = four tiles per CTA.
 constexpr int TSORT = 256;
 __global__ void __launch_bounds__(128) k_tile_sort_warp(const int* __restrict__ offset, int ntiles,
-                                                        unsigned long long* __restrict__ list) {
+                                                        unsigned long long* __restrict__ list, long long cap) {
   __shared__ unsigned long long buf[4][TSORT];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int t = blockIdx.x * 4 + w;
   if (t >= ntiles) return;  // uniform over the warp
   const int b = offset[t], e = offset[t + 1], n = e - b;
+  if (!FCM_INB(b, (long long)e + 1, BS_LIST) || !FCM_INB(e, cap + 1, BS_LIST)) return;  // uniform over the warp
   if (n < 2) return;
   if (n > TSORT) {
     if (lane == 0)
@@ -210,16 +216,36 @@ __device__ __forceinline__ void copy8(float* dst, const float* __restrict__ src)
   d[1] = b;
 }
 
+// The tile-list entry at slot.  In the bounds-checked build a slot beyond the
+// list's capacity or a blob id beyond the tables reads as entry 0, whose empty
+// half masks make the spreading and interpolation skip it.
+__device__ __forceinline__ unsigned long long list_entry(const unsigned long long* __restrict__ list, long long slot,
+                                                         const TileGeom& g) {
+  if (!FCM_INB(slot, g.list_cap, BS_LIST)) return 0ull;
+  const unsigned long long e = list[slot];
+  if (!FCM_INB(e >> 32, g.nblobs, BS_BLOB)) return 0ull;
+  return e;
+}
+
+// A tile's entry range [b0, b1) of the list; in the bounds-checked build a range
+// outside 0 <= b0 <= b1 <= capacity reads as empty.
+__device__ __forceinline__ void tile_range(const int* __restrict__ offset, int tile, const TileGeom& g, int& b0,
+                                           int& b1) {
+  b0 = offset[tile];
+  b1 = offset[tile + 1];
+  if (!FCM_INB(b0, (long long)b1 + 1, BS_LIST) || !FCM_INB(b1, g.list_cap + 1, BS_LIST)) b1 = b0;
+}
+
 // Stage blobs list[c0 .. c0+nc) (nc <= SCB) of a tile: lane (k, d) = (t/4, t%4)
 // copies chunk d of blob k for d < 3; lane d = 3 copies the entry's low word and,
 // when F is given, the blob's force.
 template <typename T>
 __device__ __forceinline__ void stage_blobs(const unsigned long long* __restrict__ list, int c0, int nc,
                                             const T* __restrict__ wc, const double* __restrict__ F,
-                                            T (*sw)[3][TE], T (*sF)[4], unsigned* sflag) {
+                                            T (*sw)[3][TE], T (*sF)[4], unsigned* sflag, const TileGeom& g) {
   const int k = threadIdx.x >> 2, d = threadIdx.x & 3;
   if (k >= nc) return;
-  const unsigned long long e = list[c0 + k];
+  const unsigned long long e = list_entry(list, c0 + k, g);
   const unsigned b = (unsigned)(e >> 32), lo = (unsigned)e;
   if (d < 3) {
     copy8(sw[k][d], wc + ((size_t)(3 * b + d) * NCH + ((lo >> (2 * d)) & 3u)) * TE);
@@ -238,10 +264,10 @@ __device__ __forceinline__ void stage_blobs(const unsigned long long* __restrict
 template <typename T, int NB>
 __device__ __forceinline__ void stage_blobs_n(const unsigned long long* __restrict__ list, int c0, int nc,
                                               const T* __restrict__ wc, const double* __restrict__ F,
-                                              T (*sw)[3][TE], T (*sF)[4], unsigned* sflag) {
+                                              T (*sw)[3][TE], T (*sF)[4], unsigned* sflag, const TileGeom& g) {
   for (int i = threadIdx.x; i < 4 * nc; i += 64) {
     const int k = i >> 2, d = i & 3;
-    const unsigned long long e = list[c0 + k];
+    const unsigned long long e = list_entry(list, c0 + k, g);
     const unsigned b = (unsigned)(e >> 32), lo = (unsigned)e;
     if (d < 3) {
       copy8(sw[k][d], wc + ((size_t)(3 * b + d) * NCH + ((lo >> (2 * d)) & 3u)) * TE);
@@ -306,7 +332,9 @@ __device__ __forceinline__ void spread_tile(const T* __restrict__ wc, const doub
   const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
   const int t = threadIdx.x;
   const int z = t & 7, y = t >> 3, yh = t >> 5;
-  const int b0 = offset[tile], b1 = offset[tile + 1];
+  if (!FCM_INB(tile, (long long)g.ntx * g.nty * g.ntz, BS_TILE)) return;  // uniform over the CTA
+  int b0, b1;
+  tile_range(offset, tile, g, b0, b1);
   if constexpr (sizeof(T) == 4) {
     // FP32: the x-points in pairs, one packed two-lane FMA (fma.rn.f32x2) per pair
     // and component; each lane rounds as the scalar FMA does, so the sums are the
@@ -319,7 +347,7 @@ __device__ __forceinline__ void spread_tile(const T* __restrict__ wc, const doub
     for (int c0 = b0; c0 < b1; c0 += NB) {
       const int nc = min(NB, b1 - c0);
       if (c0 != b0) __syncthreads();
-      stage_blobs_n<T, NB>(list, c0, nc, wc, F, sw, sF, sflag);
+      stage_blobs_n<T, NB>(list, c0, nc, wc, F, sw, sF, sflag, g);
       __syncthreads();
       for (int k = 0; k < nc; ++k) {
         const unsigned fl = sflag[k];
@@ -343,6 +371,7 @@ __device__ __forceinline__ void spread_tile(const T* __restrict__ wc, const doub
 #pragma unroll
     for (int x = 0; x < TE; ++x) {
       const long long idx = ((long long)(ox + x) * g.ny + oy) * g.nz + oz;
+      if (!FCM_INB(idx, G, BS_GRID)) continue;
 #pragma unroll
       for (int c = 0; c < 3; ++c) grid[c * G + idx] = (x & 1) ? acc2[x >> 1][c].y : acc2[x >> 1][c].x;
     }
@@ -356,7 +385,7 @@ __device__ __forceinline__ void spread_tile(const T* __restrict__ wc, const doub
   for (int c0 = b0; c0 < b1; c0 += NB) {
     const int nc = min(NB, b1 - c0);
     if (c0 != b0) __syncthreads();
-    stage_blobs_n<T, NB>(list, c0, nc, wc, F, sw, sF, sflag);
+    stage_blobs_n<T, NB>(list, c0, nc, wc, F, sw, sF, sflag, g);
     __syncthreads();
     for (int k = 0; k < nc; ++k) {
       const unsigned fl = sflag[k];
@@ -381,6 +410,7 @@ __device__ __forceinline__ void spread_tile(const T* __restrict__ wc, const doub
 #pragma unroll
   for (int x = 0; x < TE; ++x) {
     const long long idx = ((long long)(ox + x) * g.ny + oy) * g.nz + oz;
+    if (!FCM_INB(idx, G, BS_GRID)) continue;
     grid[idx] = acc[x][0];
     grid[G + idx] = acc[x][1];
     grid[2 * G + idx] = acc[x][2];
@@ -486,7 +516,7 @@ __global__ void __launch_bounds__(64) k_spread_pipe(const T* __restrict__ wc, co
   TileItem nx2 = v2 ? gen.item() : TileItem{0, 0, 0, 0};
   // prologue: the first round straight into buffer 0
   if (k < cur.nc) {
-    const unsigned long long e = list[cur.c0 + k];
+    const unsigned long long e = list_entry(list, cur.c0 + k, g);
     const unsigned b = (unsigned)(e >> 32), lo = (unsigned)e;
     if (d < 3) {
       chunk_async<T>(sw[0][k][d], wc + ((size_t)(3 * b + d) * NCH + ((lo >> (2 * d)) & 3u)) * TE);
@@ -498,7 +528,7 @@ __global__ void __launch_bounds__(64) k_spread_pipe(const T* __restrict__ wc, co
     }
   }
   cp_async_commit();
-  unsigned long long e1 = (v1 && k < nx1.nc) ? list[nx1.c0 + k] : 0ull;
+  unsigned long long e1 = (v1 && k < nx1.nc) ? list_entry(list, nx1.c0 + k, g) : 0ull;
   cp_async_wait_all();
   __syncthreads();
   T acc[TE][3];
@@ -524,7 +554,7 @@ __global__ void __launch_bounds__(64) k_spread_pipe(const T* __restrict__ wc, co
     }
     cp_async_commit();
     // the entries of the round after
-    const unsigned long long e2 = (v2 && k < nx2.nc) ? list[nx2.c0 + k] : 0ull;
+    const unsigned long long e2 = (v2 && k < nx2.nc) ? list_entry(list, nx2.c0 + k, g) : 0ull;
     // accumulate this round
     for (int kk = 0; kk < cur.nc; ++kk) {
       const unsigned fl = sflag[buf][kk];
@@ -556,9 +586,11 @@ __global__ void __launch_bounds__(64) k_spread_pipe(const T* __restrict__ wc, co
 #pragma unroll
       for (int x = 0; x < TE; ++x) {
         const long long idx = ((long long)(ox + x) * g.ny + oy) * g.nz + oz;
-        grid[idx] = acc[x][0];
-        grid[G + idx] = acc[x][1];
-        grid[2 * G + idx] = acc[x][2];
+        if (FCM_INB(idx, G, BS_GRID)) {
+          grid[idx] = acc[x][0];
+          grid[G + idx] = acc[x][1];
+          grid[2 * G + idx] = acc[x][2];
+        }
 #pragma unroll
         for (int c = 0; c < 3; ++c) acc[x][c] = 0;
       }
@@ -610,7 +642,9 @@ __device__ __forceinline__ void interp_tile(const T* __restrict__ wc, const T* _
   __shared__ unsigned sflag[SCB];
   __shared__ unsigned sblob[SCB];
   __shared__ T sred[SCB / 4][2][16];
-  const int b0 = offset[tile], b1 = offset[tile + 1];
+  if (!FCM_INB(tile, (long long)g.ntx * g.nty * g.ntz, BS_TILE)) return;  // uniform over the CTA
+  int b0, b1;
+  tile_range(offset, tile, g, b0, b1);
   if (b0 == b1) return;  // no blob meets this tile (uniform over the CTA)
   const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
   const int t = threadIdx.x;
@@ -622,6 +656,10 @@ __device__ __forceinline__ void interp_tile(const T* __restrict__ wc, const T* _
 #pragma unroll
     for (int x = 0; x < TE; ++x) {
       const long long idx = ((long long)(ox + x) * g.ny + oy) * g.nz + oz;
+      if (!FCM_INB(idx, G, BS_GRID)) {
+        u[x][0] = u[x][1] = u[x][2] = (T)0;
+        continue;
+      }
       u[x][0] = live ? grid[idx] : (T)0;
       u[x][1] = live ? grid[G + idx] : (T)0;
       u[x][2] = live ? grid[2 * G + idx] : (T)0;
@@ -630,8 +668,8 @@ __device__ __forceinline__ void interp_tile(const T* __restrict__ wc, const T* _
   for (int c0 = b0; c0 < b1; c0 += SCB) {
     const int nc = min(SCB, b1 - c0);
     if (c0 != b0) __syncthreads();
-    stage_blobs<T>(list, c0, nc, wc, nullptr, sw, nullptr, sflag);
-    if ((t & 3) == 3 && (t >> 2) < nc) sblob[t >> 2] = (unsigned)(list[c0 + (t >> 2)] >> 32);
+    stage_blobs<T>(list, c0, nc, wc, nullptr, sw, nullptr, sflag, g);
+    if ((t & 3) == 3 && (t >> 2) < nc) sblob[t >> 2] = (unsigned)(list_entry(list, c0 + (t >> 2), g) >> 32);
     __syncthreads();
     for (int k0 = 0; k0 < nc; k0 += 4) {
       T v[16];
@@ -673,7 +711,8 @@ __device__ __forceinline__ void interp_tile(const T* __restrict__ wc, const T* _
       const int grp = t >> 4, i = t & 15, c = i & 3, k = 4 * grp + (i >> 2);
       if (c < 3 && k < nc) {
         const unsigned jt = (sflag[k] >> EJ) & 63u;
-        partial[((size_t)sblob[k] * 64 + jt) * 3 + c] = sred[grp][0][i] + sred[grp][1][i];
+        if (FCM_INB((long long)sblob[k] * 64 + jt, (long long)g.nblobs * 64, BS_PARTIAL))
+          partial[((size_t)sblob[k] * 64 + jt) * 3 + c] = sred[grp][0][i] + sred[grp][1][i];
       }
     }
   }
@@ -713,7 +752,8 @@ __global__ void __launch_bounds__(64 / R) k_interp_rows(const T* __restrict__ wc
   __shared__ unsigned sblob[SCB];
   __shared__ __align__(16) T sred[3 * SCB][RS];
   const int tile = blockIdx.x;
-  const int b0 = offset[tile], b1 = offset[tile + 1];
+  int b0, b1;
+  tile_range(offset, tile, g, b0, b1);
   if (b0 == b1) return;  // no blob meets this tile (uniform over the CTA)
   const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
   const int t = threadIdx.x;
@@ -725,16 +765,19 @@ __global__ void __launch_bounds__(64 / R) k_interp_rows(const T* __restrict__ wc
     const bool live = oy < g.ycut;  // rows at or above the slip channel's upper wall read as 0
     const long long base = ((long long)(tx * TE) * g.ny + oy) * g.nz + tz * TE + z;
 #pragma unroll
-    for (int x = 0; x < TE; ++x)
+    for (int x = 0; x < TE; ++x) {
+      const bool in = FCM_INB(base + (long long)x * g.ny * g.nz, G, BS_GRID);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) u[r][c][x] = live ? grid[c * G + base + (long long)x * g.ny * g.nz] : (T)0;
+      for (int c = 0; c < 3; ++c)
+        u[r][c][x] = (live && in) ? grid[c * G + base + (long long)x * g.ny * g.nz] : (T)0;
+    }
   }
   for (int c0 = b0; c0 < b1; c0 += SCB) {
     const int nc = min(SCB, b1 - c0);
     if (c0 != b0) __syncthreads();
     for (int i = t; i < 4 * nc; i += NT) {
       const int k = i >> 2, d = i & 3;
-      const unsigned long long e = list[c0 + k];
+      const unsigned long long e = list_entry(list, c0 + k, g);
       const unsigned b = (unsigned)(e >> 32), lo = (unsigned)e;
       if (d < 3) {
         copy8(sw[k][d], wc + ((size_t)(3 * b + d) * NCH + ((lo >> (2 * d)) & 3u)) * TE);
@@ -818,7 +861,8 @@ __global__ void __launch_bounds__(64 / R) k_interp_rows(const T* __restrict__ wc
       }
       const int k = rr / 3, c = rr - 3 * (rr / 3);
       const unsigned jt = (sflag[k] >> EJ) & 63u;
-      partial[((size_t)sblob[k] * 64 + jt) * 3 + c] = sum;
+      if (FCM_INB((long long)sblob[k] * 64 + jt, (long long)g.nblobs * 64, BS_PARTIAL))
+        partial[((size_t)sblob[k] * 64 + jt) * 3 + c] = sum;
     }
   }
 }
@@ -829,7 +873,8 @@ __device__ __forceinline__ void interp_reduce_one(const int* __restrict__ base, 
                                                   const TileGeom& g, double dx3, double* __restrict__ V, int b) {
   int f[3], cnt[3];
   blob_tiles(base, b, g, f, cnt);
-  const int nj = cnt[0] * cnt[1] * cnt[2];
+  int nj = cnt[0] * cnt[1] * cnt[2];
+  if (!FCM_INB(nj - 1, 64, BS_PARTIAL)) nj = 0;
   double s0 = 0, s1 = 0, s2 = 0;
   const T* p = partial + (size_t)b * 64 * 3;
   for (int j = 0; j < nj; ++j) {
@@ -862,7 +907,8 @@ __global__ void __launch_bounds__(128) k_interp_reduce8(const int* __restrict__ 
   if (b < n) {
     int f[3], cnt[3];
     blob_tiles(base, b, g, f, cnt);
-    const int nj = cnt[0] * cnt[1] * cnt[2];
+    int nj = cnt[0] * cnt[1] * cnt[2];
+    if (!FCM_INB(nj - 1, 64, BS_PARTIAL)) nj = 0;
     const T* p = partial + (size_t)b * 64 * 3;
     for (int j = k; j < nj; j += 8) {
       s0 += (double)p[3 * j];
@@ -902,6 +948,7 @@ __global__ void k_spread_atomic(const int* __restrict__ base, const T* __restric
       const int xx = wrap_index(bx + i, nx);
       const T wt = gx[i] * wyz;
       const long long idx = ((long long)xx * ny + yy) * nz + zz;
+      if (!FCM_INB(idx, G, BS_GRID)) continue;
       atomicAdd(grid + idx, f0 * wt);
       atomicAdd(grid + G + idx, f1 * wt);
       atomicAdd(grid + 2 * G + idx, f2 * wt);
@@ -929,6 +976,7 @@ __global__ void __launch_bounds__(NT) k_interp_block(const int* __restrict__ bas
       const int xx = wrap_index(bx + i, nx);
       const T wt = gx[i] * wyz;
       const long long idx = ((long long)xx * ny + yy) * nz + zz;
+      if (!FCM_INB(idx, G, BS_GRID)) continue;
       s0 += grid[idx] * wt;
       s1 += grid[G + idx] * wt;
       s2 += grid[2 * G + idx] * wt;
@@ -962,8 +1010,8 @@ __global__ void __launch_bounds__(NT) k_interp_block(const int* __restrict__ bas
 
 }  // namespace
 
-TileGeom tile_geom(const GridDims& g, int W) {
-  return TileGeom{g.nx / TE, g.ny / TE, g.nz / TE, g.nx, g.ny, g.nz, W, g.ny};
+TileGeom tile_geom(const GridDims& g, int W, int nblobs, long long list_cap) {
+  return TileGeom{g.nx / TE, g.ny / TE, g.nz / TE, g.nx, g.ny, g.nz, W, g.ny, nblobs, list_cap};
 }
 
 // CTAs of a persistent kernel: as many as fit on the device at once
@@ -1043,7 +1091,7 @@ int launch_set_up_gaussians(const Ctx& c, BlobTable<T>& t, const double* dY, cud
                                                           t.tiled ? t.wc : nullptr, t.ypos);
   FCM_LAUNCH_CHECK();
   if (t.tiled) {
-    const TileGeom g = tile_geom(c.g, t.W);
+    const TileGeom g = tile_geom(c.g, t);
     FCM_CUDA(cudaMemsetAsync(t.tile_count, 0, sizeof(int) * (size_t)t.ntiles, s));
     FCM_CUDA(cudaMemsetAsync(t.tile_cursor, 0, sizeof(int) * (size_t)t.ntiles, s));
     k_tile_count<<<(t.n + 127) / 128, 128, 0, s>>>(t.base, t.n, g, t.tile_count);
@@ -1051,7 +1099,7 @@ int launch_set_up_gaussians(const Ctx& c, BlobTable<T>& t, const double* dY, cud
     FCM_TRY(launch_exclusive_scan(t.tile_count, t.tile_offset, t.ntiles, s));
     k_tile_fill<<<(t.n + 127) / 128, 128, 0, s>>>(t.base, t.n, g, t.tile_offset, t.tile_cursor, t.tile_list);
     FCM_LAUNCH_CHECK();
-    k_tile_sort_warp<<<(t.ntiles + 3) / 4, 128, 0, s>>>(t.tile_offset, t.ntiles, t.tile_list);
+    k_tile_sort_warp<<<(t.ntiles + 3) / 4, 128, 0, s>>>(t.tile_offset, t.ntiles, t.tile_list, t.tile_cap);
     FCM_LAUNCH_CHECK();
   }
   return FCM_OK;
@@ -1064,7 +1112,7 @@ int launch_spread(const Ctx& c, const BlobTable<T>& t, const double* dF, T* grid
     // the limit), FP32 one CTA per tile staging 16 blobs per round; fcm_autotune may
     // choose another (one CTA per tile with 8 or 32 blobs per round)
     const int v = c.spread_variant[sizeof(T) == 8 ? 0 : 1];
-    const TileGeom tg = tile_geom(c.g, t.W);
+    const TileGeom tg = tile_geom(c.g, t);
     if (v == 0) {
       const int ctas = std::min(t.ntiles, persistent_ctas(k_spread_pipe<T>, 64, c.device));
       k_spread_pipe<T><<<ctas, 64, 0, s>>>(t.wc, dF, tg, t.tile_offset, t.tile_list, c.g.G, grid, t.ntiles);
@@ -1091,7 +1139,7 @@ int launch_interp(const Ctx& c, const BlobTable<T>& t, const T* grid, double* dV
   const double dx3 = c.g.dx * c.g.dx * c.g.dx;
   const int ycut = c.p.slip_channel ? c.g.ny / 2 : c.g.ny;  // fcm_fluid_solver.cpp:387-389
   if (t.tiled) {
-    TileGeom g = tile_geom(c.g, t.W);
+    TileGeom g = tile_geom(c.g, t);
     g.ycut = ycut;
     const int v = c.interp_variant[sizeof(T) == 8 ? 0 : 1];
     if (v == 2)
@@ -1215,10 +1263,10 @@ template <typename T>
 __device__ __forceinline__ void stage_dipoles(const unsigned long long* __restrict__ list, int c0, int nc,
                                               const T* __restrict__ wd, const T* __restrict__ hd,
                                               const double* __restrict__ D9, T (*sg)[3][TE], T (*sh)[3][TE],
-                                              T (*sD)[9], unsigned* sflag, unsigned* sblob) {
+                                              T (*sD)[9], unsigned* sflag, unsigned* sblob, const TileGeom& g) {
   const int k = threadIdx.x >> 2, d = threadIdx.x & 3;
   if (k >= nc) return;
-  const unsigned long long e = list[c0 + k];
+  const unsigned long long e = list_entry(list, c0 + k, g);
   const unsigned b = (unsigned)(e >> 32), lo = (unsigned)e;
   if (d < 3) {
     const size_t off = ((size_t)(3 * b + d) * NCH + ((lo >> (2 * d)) & 3u)) * TE;
@@ -1245,7 +1293,8 @@ __global__ void __launch_bounds__(64) k_spread_dipole_tiled(const T* __restrict_
   __shared__ T sD[SCB][9];
   __shared__ unsigned sflag[SCB], sblob[SCB];
   const int tile = blockIdx.x;
-  const int b0 = offset[tile], b1 = offset[tile + 1];
+  int b0, b1;
+  tile_range(offset, tile, g, b0, b1);
   if (b0 == b1) return;
   const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
   const int t = threadIdx.x;
@@ -1258,7 +1307,7 @@ __global__ void __launch_bounds__(64) k_spread_dipole_tiled(const T* __restrict_
   for (int c0 = b0; c0 < b1; c0 += SCB) {
     const int nc = min(SCB, b1 - c0);
     if (c0 != b0) __syncthreads();
-    stage_dipoles<T>(list, c0, nc, wd, hd, D9, sg, sh, sD, sflag, sblob);
+    stage_dipoles<T>(list, c0, nc, wd, hd, D9, sg, sh, sD, sflag, sblob, g);
     __syncthreads();
     for (int k = 0; k < nc; ++k) {
       const unsigned fl = sflag[k];
@@ -1288,6 +1337,7 @@ __global__ void __launch_bounds__(64) k_spread_dipole_tiled(const T* __restrict_
 #pragma unroll
   for (int x = 0; x < TE; ++x) {
     const long long idx = ((long long)(ox + x) * g.ny + oy) * g.nz + oz;
+    if (!FCM_INB(idx, G, BS_GRID)) continue;
     grid[idx] += acc[x][0];
     grid[G + idx] += acc[x][1];
     grid[2 * G + idx] += acc[x][2];
@@ -1306,7 +1356,8 @@ __global__ void __launch_bounds__(64) k_interp_dipole_tiled(const T* __restrict_
   __shared__ unsigned sflag[SCB], sblob[SCB];
   __shared__ T sred[SCB][2][16];
   const int tile = blockIdx.x;
-  const int b0 = offset[tile], b1 = offset[tile + 1];
+  int b0, b1;
+  tile_range(offset, tile, g, b0, b1);
   if (b0 == b1) return;
   const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
   const int t = threadIdx.x;
@@ -1318,6 +1369,10 @@ __global__ void __launch_bounds__(64) k_interp_dipole_tiled(const T* __restrict_
 #pragma unroll
     for (int x = 0; x < TE; ++x) {
       const long long idx = ((long long)(ox + x) * g.ny + oy) * g.nz + oz;
+      if (!FCM_INB(idx, G, BS_GRID)) {
+        u[x][0] = u[x][1] = u[x][2] = (T)0;
+        continue;
+      }
       u[x][0] = live ? grid[idx] : (T)0;
       u[x][1] = live ? grid[G + idx] : (T)0;
       u[x][2] = live ? grid[2 * G + idx] : (T)0;
@@ -1326,7 +1381,7 @@ __global__ void __launch_bounds__(64) k_interp_dipole_tiled(const T* __restrict_
   for (int c0 = b0; c0 < b1; c0 += SCB) {
     const int nc = min(SCB, b1 - c0);
     if (c0 != b0) __syncthreads();
-    stage_dipoles<T>(list, c0, nc, wd, hd, nullptr, sg, sh, nullptr, sflag, sblob);
+    stage_dipoles<T>(list, c0, nc, wd, hd, nullptr, sg, sh, nullptr, sflag, sblob, g);
     __syncthreads();
     for (int k = 0; k < nc; ++k) {
       const unsigned fl = sflag[k];
@@ -1365,7 +1420,8 @@ __global__ void __launch_bounds__(64) k_interp_dipole_tiled(const T* __restrict_
     for (int e = t; e < nc * 9; e += 64) {
       const int k = e / 9, vv = e - 9 * k;
       const unsigned jt = (sflag[k] >> EJ) & 63u;
-      partial9[((size_t)sblob[k] * 64 + jt) * 9 + vv] = sred[k][0][vv] + sred[k][1][vv];
+      if (FCM_INB((long long)sblob[k] * 64 + jt, (long long)g.nblobs * 64, BS_PARTIAL))
+        partial9[((size_t)sblob[k] * 64 + jt) * 9 + vv] = sred[k][0][vv] + sred[k][1][vv];
     }
   }
 }
@@ -1377,7 +1433,8 @@ __global__ void k_interp_dipole_reduce(const int* __restrict__ base, const T* __
   if (b >= n) return;
   int f[3], cnt[3];
   blob_tiles(base, b, g, f, cnt);
-  const int nj = cnt[0] * cnt[1] * cnt[2];
+  int nj = cnt[0] * cnt[1] * cnt[2];
+  if (!FCM_INB(nj - 1, 64, BS_PARTIAL)) nj = 0;
   double M[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   const T* p = partial9 + (size_t)b * 64 * 9;
   for (int j = 0; j < nj; ++j)
@@ -1429,7 +1486,7 @@ template <typename T>
 int launch_spread_dipoles(const Ctx& c, BlobTable<T>& t, const double* dD, T* grid, cudaStream_t s) {
   FCM_TRY(ensure_dipole_tables<T>(c, t, s));
   if (t.n == 0) return FCM_OK;
-  k_spread_dipole_tiled<T><<<t.ntiles, 64, 0, s>>>(t.wd, t.hd, dD, tile_geom(c.g, t.W), t.tile_offset, t.tile_list,
+  k_spread_dipole_tiled<T><<<t.ntiles, 64, 0, s>>>(t.wd, t.hd, dD, tile_geom(c.g, t), t.tile_offset, t.tile_list,
                                                    c.g.G, grid);
   FCM_LAUNCH_CHECK();
   return FCM_OK;
@@ -1439,7 +1496,7 @@ template <typename T>
 int launch_interp_dipoles(const Ctx& c, BlobTable<T>& t, const T* grid, double* dOm, double* dE, cudaStream_t s) {
   FCM_TRY(ensure_dipole_tables<T>(c, t, s));
   if (t.n == 0) return FCM_OK;
-  const TileGeom g = tile_geom(c.g, t.W);
+  const TileGeom g = tile_geom(c.g, t);
   k_interp_dipole_tiled<T><<<t.ntiles, 64, 0, s>>>(t.wd, t.hd, grid, g, t.tile_offset, t.tile_list, c.g.G,
                                                    t.partial9);
   FCM_LAUNCH_CHECK();
@@ -1514,6 +1571,8 @@ template int b_spread<double>(const BatchGeom&, int, int, cudaStream_t);
 template int b_spread<float>(const BatchGeom&, int, int, cudaStream_t);
 template int b_interp<double>(const BatchGeom&, int, int, cudaStream_t);
 template int b_interp<float>(const BatchGeom&, int, int, cudaStream_t);
+
+FCM_BOUNDS_READER(bounds_read_grid)
 
 }  // namespace fcm
 
@@ -1650,7 +1709,7 @@ extern "C" int fcm_interp_noalloc(int32_t nx, int32_t ny, int32_t nz, double dx,
   const double PI = 3.14159265358979323846264338327950288;
   const double anorm = 1.0 / (sqrt(2.0) * blob_radius);
   const double anorm2 = 2.0 * blob_radius * blob_radius / PI;
-  const TileGeom g{nx / TE, ny / TE, nz / TE, nx, ny, nz, W, ny};
+  const TileGeom g{nx / TE, ny / TE, nz / TE, nx, ny, nz, W, ny, n, (long long)cap};
   const long long G = (long long)nx * ny * nz;
   // the array keeps the previous call's contents: counters start at zero
   FCM_CUDA(cudaMemsetAsync(s_count, 0, sizeof(int) * (size_t)ntiles, s));
@@ -1663,7 +1722,7 @@ extern "C" int fcm_interp_noalloc(int32_t nx, int32_t ny, int32_t nz, double dx,
   FCM_TRY(launch_exclusive_scan(s_count, s_offset, (int)ntiles, s));
   k_tile_fill<<<(n + 127) / 128, 128, 0, s>>>(s_base, n, g, s_offset, s_cursor, s_list);
   FCM_LAUNCH_CHECK();
-  k_tile_sort<<<(unsigned)((ntiles + 127) / 128), 128, 0, s>>>(s_offset, (int)ntiles, s_list);
+  k_tile_sort<<<(unsigned)((ntiles + 127) / 128), 128, 0, s>>>(s_offset, (int)ntiles, s_list, (long long)cap);
   FCM_LAUNCH_CHECK();
   k_interp_tiled<double><<<(unsigned)ntiles, 64, 0, s>>>(s_wc, grid, g, s_offset, s_list, G, s_partial);
   FCM_LAUNCH_CHECK();

@@ -65,6 +65,66 @@ long long launch_count();
     }                                                                           \
   } while (0)
 
+// ------------------------------------------------------------------ bounds-checked build
+// Compiled with -DFCM_BOUNDS_CHECK (libfcm_b200_debug.so), FCM_INB(i, n, site) is
+// true when 0 <= i < n.  Otherwise the violation is counted in this translation
+// unit's device record (the first violation's site, index and limit are kept) and
+// the caller skips the access.  Nothing traps: the kernel runs to its end and the
+// host reads the records through fcm_debug_bounds.  In the release build FCM_INB
+// is the constant true and every check compiles away.
+enum BoundsSite : int {
+  BS_GRID = 1,      // grid point index against the grid's 3 G values
+  BS_BLOB = 2,      // blob id (from a tile list or a cell list) against the blob count
+  BS_TILE = 3,      // tile index against the tile count
+  BS_LIST = 4,      // tile-list or cell-list slot against its range or capacity
+  BS_PARTIAL = 5,   // per-(blob, tile) partial against its table
+  BS_CELL = 6,      // cell id against the cell count
+  BS_SPECTRUM = 7,  // spectrum index against the spectrum's 3 Gc values
+  BS_KRYLOV = 8,    // Krylov column (GMRES iteration) against the columns allocated
+};
+struct BoundsRecord {
+  unsigned long long count;
+  long long index, limit;
+  int site, pad;
+};
+#ifdef FCM_BOUNDS_CHECK
+static __device__ BoundsRecord g_fcm_bounds;
+static __device__ __noinline__ void fcm_bounds_record(long long i, long long n, int site) {
+  if (atomicAdd(&g_fcm_bounds.count, 1ull) == 0ull) {
+    g_fcm_bounds.index = i;
+    g_fcm_bounds.limit = n;
+    g_fcm_bounds.site = site;
+  }
+}
+static __device__ __forceinline__ bool fcm_inb(long long i, long long n, int site) {
+  if (i >= 0 && i < n) return true;
+  fcm_bounds_record(i, n, site);
+  return false;
+}
+#define FCM_INB(i, n, site) ::fcm::fcm_inb((long long)(i), (long long)(n), (site))
+#define FCM_BOUNDS_READER(fn)                                                                   \
+  int fn(BoundsRecord* out, int reset) {                                                        \
+    FCM_CUDA(cudaMemcpyFromSymbol(out, g_fcm_bounds, sizeof(BoundsRecord)));                    \
+    if (reset) {                                                                                \
+      const BoundsRecord z{};                                                                   \
+      FCM_CUDA(cudaMemcpyToSymbol(g_fcm_bounds, &z, sizeof(BoundsRecord)));                     \
+    }                                                                                           \
+    return FCM_OK;                                                                              \
+  }
+#else
+#define FCM_INB(i, n, site) true
+#define FCM_BOUNDS_READER(fn)          \
+  int fn(BoundsRecord* out, int) {     \
+    *out = BoundsRecord{};             \
+    return FCM_OK;                     \
+  }
+#endif
+// The record of each translation unit with checked kernels.
+int bounds_read_grid(BoundsRecord* out, int reset);
+int bounds_read_cells(BoundsRecord* out, int reset);
+int bounds_read_kspace(BoundsRecord* out, int reset);
+int bounds_read_blas(BoundsRecord* out, int reset);
+
 template <typename T>
 struct cplx_t;
 template <>
@@ -132,7 +192,9 @@ constexpr int TILE_X = 8, TILE_Y = 8, TILE_Z = 8;
 // Tile grid of the tiled spread / interpolation (fcm_grid.cu).
 struct TileGeom {
   int ntx, nty, ntz, nx, ny, nz, W;
-  int ycut;  // interpolation reads rows y < ycut only (ny, or ny/2 in a slip channel)
+  int ycut;            // interpolation reads rows y < ycut only (ny, or ny/2 in a slip channel)
+  int nblobs;          // blobs of the tables
+  long long list_cap;  // capacity of the tile list (entries)
 };
 
 // k-space geometry of the projection (fcm_kspace.cu).
@@ -411,7 +473,13 @@ struct BatchGeom {
 };
 
 KParams make_kparams(const Ctx& c);
-TileGeom tile_geom(const GridDims& g, int W);
+// Tile geometry of a grid for tables of nblobs blobs with a tile list of
+// list_cap entries.
+TileGeom tile_geom(const GridDims& g, int W, int nblobs, long long list_cap);
+template <typename T>
+inline TileGeom tile_geom(const GridDims& g, const BlobTable<T>& t) {
+  return tile_geom(g, t.W, t.n, t.tile_cap);
+}
 
 // batched kernels (fcm_blas.cu, fcm_bodies.cu, fcm_grid.cu, fcm_kspace.cu)
 int b_gm_init(const BatchGeom& b, int vec, double tol, int use_rs_tol, int mask, cudaStream_t s);

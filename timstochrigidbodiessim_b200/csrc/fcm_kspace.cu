@@ -74,6 +74,7 @@ __device__ __forceinline__ bool is_plane(int kz, const KParams& k) {
 
 template <typename C, typename T>
 __device__ __forceinline__ void store3(C* spec, long long Gc, long long t, const V2<T> u[3]) {
+  if (!FCM_INB(t, Gc, BS_SPECTRUM)) return;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     C v;
@@ -85,6 +86,10 @@ __device__ __forceinline__ void store3(C* spec, long long Gc, long long t, const
 
 template <typename C, typename T>
 __device__ __forceinline__ void load3(const C* spec, long long Gc, long long t, V2<T> f[3]) {
+  if (!FCM_INB(t, Gc, BS_SPECTRUM)) {
+    for (int c = 0; c < 3; ++c) f[c] = V2<T>{(T)0, (T)0};
+    return;
+  }
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     const C v = spec[c * Gc + t];
@@ -490,7 +495,8 @@ __device__ __forceinline__ void xfft_planes_cta(C* __restrict__ spec, const KPar
   for (int i = threadIdx.x; i < N * NC; i += blockDim.x) {
     const int col = i % NC, x = i / NC, c = col % 3, r = (col / 3) & 1, y = y0 + col / 6;
     const int yr = r ? (k.ny - y) % k.ny : y;
-    const bool live = y <= h && !(r && yr == y);
+    const bool live = y <= h && !(r && yr == y) &&
+                      FCM_INB(c * k.Gc + x * xs + (long long)yr * k.nzh + kz, 3 * k.Gc, BS_SPECTRUM);
     s[x * NC + col] = live ? ldt<T>(spec[c * k.Gc + x * xs + (long long)yr * k.nzh + kz]) : V2<T>{(T)0, (T)0};
   }
   __syncthreads();
@@ -553,7 +559,8 @@ __device__ __forceinline__ void xfft_planes_cta(C* __restrict__ spec, const KPar
     C o;
     o.x = v.x;
     o.y = v.y;
-    spec[c * k.Gc + x * xs + (long long)yr * k.nzh + kz] = o;
+    if (FCM_INB(c * k.Gc + x * xs + (long long)yr * k.nzh + kz, 3 * k.Gc, BS_SPECTRUM))
+      spec[c * k.Gc + x * xs + (long long)yr * k.nzh + kz] = o;
   }
 }
 
@@ -585,7 +592,9 @@ __device__ __forceinline__ void xfft_interior_cta(C* __restrict__ spec, const KP
     V2<T> a[N1];
 #pragma unroll
     for (int j = 0; j < N1; ++j)
-      a[j] = mine ? ldt<T>(src[(long long)(j * N2 + n2) * xs]) : V2<T>{(T)0, (T)0};
+      a[j] = (mine && FCM_INB(c * k.Gc + row + kzl + (long long)(j * N2 + n2) * xs, 3 * k.Gc, BS_SPECTRUM))
+                 ? ldt<T>(src[(long long)(j * N2 + n2) * xs])
+                 : V2<T>{(T)0, (T)0};
     dft<T, N1, false>(a);
 #pragma unroll
     for (int j = 1; j < N1; ++j) a[j] = cmul(a[j], ldt<T>(__ldg(&twN[n2 * j])));
@@ -648,7 +657,8 @@ __device__ __forceinline__ void xfft_interior_cta(C* __restrict__ spec, const KP
       C o;
       o.x = a[j].x;
       o.y = a[j].y;
-      dst[(long long)(j * N2 + n2) * xs] = o;
+      if (FCM_INB(c * k.Gc + row + kzl + (long long)(j * N2 + n2) * xs, 3 * k.Gc, BS_SPECTRUM))
+        dst[(long long)(j * N2 + n2) * xs] = o;
     }
   }
 }
@@ -1489,5 +1499,7 @@ template int launch_project<float>(const Ctx&, cufftComplex*, cudaStream_t);
 template int launch_noise_kspace<double>(const Ctx&, cufftDoubleComplex*, uint64_t, uint64_t, const uint64_t*,
                                          cudaStream_t);
 template int launch_noise_kspace<float>(const Ctx&, cufftComplex*, uint64_t, uint64_t, const uint64_t*, cudaStream_t);
+
+FCM_BOUNDS_READER(bounds_read_kspace)
 
 }  // namespace fcm
