@@ -101,3 +101,19 @@ def test_variants_refused_where_the_grid_does_not_allow_them(gpu):
     assert v[1] == 0 and v[3] == 0
     for prec in (0, 1):
         assert rel_err(_mf(h, F, prec), Vo) < TOL[prec], prec
+
+
+@pytest.mark.parametrize("nx", [384, 512])
+def test_long_x_transforms(gpu, nx):
+    """The fused x-transform of the long FP32 lengths (384 = 16 x 24, 512 = 32 x 16)
+    against the 3D transforms and the oracle, on thin boxes (nx x 32 x 32)."""
+    g, Vo, F = _setup((nx, 32, 32), nbodies=24)
+    out = []
+    for sv in (0, 1, 2):
+        v = g.get_variants()
+        v[3] = sv
+        g.set_variants(v)
+        out.append(_mf(g, F, 1))
+        assert rel_err(out[-1], Vo) < TOL[1], sv
+    assert rel_err(out[1], out[0]) < TOL[1]
+    assert rel_err(out[2], out[0]) < TOL[1]

@@ -625,6 +625,70 @@ __device__ __forceinline__ T warp_reduce_scatter16(T v[16], int lane) {
   return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
 }
 
+// The x-column of one (y, z) point of a tile, three components, in registers,
+// and its contraction with a blob's x-weights: s_c = sum_x wx[x] u_c[x] (x-halves
+// the stencil misses skipped where skip_x_half says so).  FP64 sums the points in
+// order; FP32 holds the column as x-point pairs and sums even and odd points in
+// the two lanes of the packed FMA (fma.rn.f32x2), then adds the lanes.
+template <typename T>
+struct XColumn {
+  T u[3][TE];
+  __device__ __forceinline__ void set(int x, T a, T b, T c) {
+    u[0][x] = a;
+    u[1][x] = b;
+    u[2][x] = c;
+  }
+  __device__ __forceinline__ void contract(const T* wrow, unsigned fl, T& s0, T& s1, T& s2) const {
+    s0 = 0;
+    s1 = 0;
+    s2 = 0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (skip_x_half<T>(fl, h)) continue;
+      T wx[4];
+      load_wx4<T>(wrow, 4 * h, wx);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        s0 += wx[i] * u[0][4 * h + i];
+        s1 += wx[i] * u[1][4 * h + i];
+        s2 += wx[i] * u[2][4 * h + i];
+      }
+    }
+  }
+};
+template <>
+struct XColumn<float> {
+  float2 u[3][TE / 2];
+  __device__ __forceinline__ void set(int x, float a, float b, float c) {
+    if (x & 1) {
+      u[0][x >> 1].y = a;
+      u[1][x >> 1].y = b;
+      u[2][x >> 1].y = c;
+    } else {
+      u[0][x >> 1].x = a;
+      u[1][x >> 1].x = b;
+      u[2][x >> 1].x = c;
+    }
+  }
+  __device__ __forceinline__ void contract(const float* wrow, unsigned, float& s0, float& s1, float& s2) const {
+    float2 a0 = make_float2(0.f, 0.f), a1 = a0, a2 = a0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const float4 w4 = *reinterpret_cast<const float4*>(wrow + 4 * h);
+      const float2 wa = make_float2(w4.x, w4.y), wb = make_float2(w4.z, w4.w);
+      a0 = __ffma2_rn(wa, u[0][2 * h], a0);
+      a1 = __ffma2_rn(wa, u[1][2 * h], a1);
+      a2 = __ffma2_rn(wa, u[2][2 * h], a2);
+      a0 = __ffma2_rn(wb, u[0][2 * h + 1], a0);
+      a1 = __ffma2_rn(wb, u[1][2 * h + 1], a1);
+      a2 = __ffma2_rn(wb, u[2][2 * h + 1], a2);
+    }
+    s0 = a0.x + a0.y;
+    s1 = a1.x + a1.y;
+    s2 = a2.x + a2.y;
+  }
+};
+
 // Tiled interpolation: one CTA (64 threads) per 8x8x8 tile.  Thread (y, z) =
 // (t/8, t%8) loads the eight points of its x-column (three components) into
 // registers once.  Blobs are taken four at a time: each thread forms
@@ -649,20 +713,15 @@ __device__ __forceinline__ void interp_tile(const T* __restrict__ wc, const T* _
   const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
   const int t = threadIdx.x;
   const int z = t & 7, y = t >> 3, yh = t >> 5, lane = t & 31;
-  T u[TE][3];
+  XColumn<T> col;
   {
     const int ox = tx * TE, oy = ty * TE + y, oz = tz * TE + z;
     const bool live = oy < g.ycut;  // rows at or above the slip channel's upper wall read as 0
 #pragma unroll
     for (int x = 0; x < TE; ++x) {
       const long long idx = ((long long)(ox + x) * g.ny + oy) * g.nz + oz;
-      if (!FCM_INB(idx, G, BS_GRID)) {
-        u[x][0] = u[x][1] = u[x][2] = (T)0;
-        continue;
-      }
-      u[x][0] = live ? grid[idx] : (T)0;
-      u[x][1] = live ? grid[G + idx] : (T)0;
-      u[x][2] = live ? grid[2 * G + idx] : (T)0;
+      const bool in = live && FCM_INB(idx, G, BS_GRID);
+      col.set(x, in ? grid[idx] : (T)0, in ? grid[G + idx] : (T)0, in ? grid[2 * G + idx] : (T)0);
     }
   }
   for (int c0 = b0; c0 < b1; c0 += SCB) {
@@ -679,19 +738,8 @@ __device__ __forceinline__ void interp_tile(const T* __restrict__ wc, const T* _
         T p0 = 0, p1 = 0, p2 = 0;
         const unsigned fl = k < nc ? sflag[k] : 0u;
         if ((fl >> (EYM + yh)) & 1u) {
-          T s0 = 0, s1 = 0, s2 = 0;
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            if (skip_x_half<T>(fl, h)) continue;
-            T wx[4];
-            load_wx4<T>(sw[k][0], 4 * h, wx);
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-              s0 += wx[i] * u[4 * h + i][0];
-              s1 += wx[i] * u[4 * h + i][1];
-              s2 += wx[i] * u[4 * h + i][2];
-            }
-          }
+          T s0, s1, s2;
+          col.contract(sw[k][0], fl, s0, s1, s2);
           const T wyz = sw[k][1][y] * sw[k][2][z];
           p0 = s0 * wyz;
           p1 = s1 * wyz;

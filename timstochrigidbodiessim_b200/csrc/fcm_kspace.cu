@@ -1186,6 +1186,11 @@ int xfft_run(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s, bool 
   return FCM_OK;
 }
 
+// First factor of the 512-point x-transform (32 by default; 16 is the other split).
+#ifndef FCM_XFFT512_N1
+#define FCM_XFFT512_N1 32
+#endif
+
 template <typename T>
 int xfft_dispatch(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s, bool prepare,
                   const BatchGeom* b = nullptr, const int* gidx = nullptr, int nm = 0, int mask = 0) {
@@ -1205,7 +1210,10 @@ int xfft_dispatch(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s, 
       if constexpr (sizeof(T) == 4) return xfft_run<T, 16, 24>(c, spec, s, prepare, b, gidx, nm, mask);
       break;
     case 512:
-      if constexpr (sizeof(T) == 4) return xfft_run<T, 16, 32>(c, spec, s, prepare, b, gidx, nm, mask);
+      // 32 x 16: the middle step has N1 * TK = 256 items, one per thread (16 x 32
+      // left half the CTA idle there while it ran six 32-point DFTs per item)
+      if constexpr (sizeof(T) == 4)
+        return xfft_run<T, FCM_XFFT512_N1, 512 / FCM_XFFT512_N1>(c, spec, s, prepare, b, gidx, nm, mask);
       break;
     default: break;
   }
