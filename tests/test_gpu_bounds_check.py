@@ -3,7 +3,7 @@
 libfcm_b200_debug.so is the same library compiled with -DFCM_BOUNDS_CHECK:
 every grid point index, blob id from a tile or cell list, tile and cell id,
 list slot, per-(blob, tile) partial, spectrum index of the fused x-transform and
-Krylov column is checked against its range before the access; a kernel that
+Krylov column is checked (every kernel variant, through the autotuner's tests) against its range before the access; a kernel that
 meets one outside counts it and skips the access (no trap).  This test runs the
 parity suites in a child process with FCM_B200_BOUNDS_CHECK=1, where
 tests/conftest.py requires every test to end with no violation
@@ -24,7 +24,8 @@ pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 SUITES = ["tests/test_gpu_parity.py", "tests/test_gpu_config1_parity.py", "tests/test_gpu_tiles.py",
           "tests/test_gpu_shapes.py", "tests/test_gpu_batch.py", "tests/test_gpu_vs_reference.py",
-          "tests/test_gpu_slip.py", "tests/test_gpu_dipoles.py", "tests/test_gpu_graph_step.py"]
+          "tests/test_gpu_slip.py", "tests/test_gpu_dipoles.py", "tests/test_gpu_graph_step.py",
+          "tests/test_gpu_autotune.py"]
 
 
 def test_release_build_reports_unchecked(gpu):

@@ -915,6 +915,181 @@ __global__ void __launch_bounds__(64 / R) k_interp_rows(const T* __restrict__ wc
   }
 }
 
+// Tiled interpolation in contraction order: one CTA (96 threads) per 8x8x8 tile.
+// The tile's grid values go to shared memory as su[c][x][z][y] (y fastest, each
+// (c, x) block padded to 68 so that eight threads' 16-byte reads of different
+// blocks meet different banks).  Blobs are taken 16 per round, in four groups of
+// four; thread t = (group, c, x) = (t / 24, (t % 24) / 8, t % 8) forms, for the
+// four blobs of its group and the eight y of its (c, x) row,
+//   T1[b][y] = sum_z wz[b][z] u[c][x][y][z]          (a 4 x 8 x 8 register GEMM),
+// then s[b] = wx[b][x] * sum_y wy[b][y] T1[b][y], and the eight x of a (blob, c)
+// are added in x order from shared memory into partial[blob][j][c].  Every point of
+// the tile enters (the chunk weights are zero outside a stencil), so no half masks
+// are tested; per (blob, tile) pair this issues about a third of the instructions
+// of the shuffle-reduction kernel, which matters where many blobs meet each tile.
+// In FP32 the z-contraction and the y-sum run on the packed two-lane FMA over
+// y-pairs.
+constexpr int IG_B = 16;          // blobs per round
+constexpr int IG_T = 96;          // threads: 4 groups x 3 components x 8 x
+constexpr int IG_P = TE * TE + 4; // padded (c, x) block of su
+
+template <typename T>
+__global__ void __launch_bounds__(IG_T) k_interp_gemm(const T* __restrict__ wc, const T* __restrict__ grid,
+                                                      TileGeom g, const int* __restrict__ offset,
+                                                      const unsigned long long* __restrict__ list, long long G,
+                                                      T* __restrict__ partial) {
+  __shared__ __align__(16) T su[3 * TE * IG_P];
+  __shared__ __align__(16) T swz[IG_B / 4][TE][4];  // [group][z][blob of the group]
+  __shared__ __align__(16) T swx[IG_B / 4][TE][4];  // [group][x][blob of the group]
+  __shared__ __align__(16) T swy[IG_B][TE];         // [blob][y]
+  __shared__ __align__(16) T sred[IG_B][3][TE];     // [blob][c][x]
+  __shared__ unsigned sflag[IG_B], sblob[IG_B];
+  const int tile = blockIdx.x;
+  if (!FCM_INB(tile, (long long)g.ntx * g.nty * g.ntz, BS_TILE)) return;  // uniform over the CTA
+  int b0, b1;
+  tile_range(offset, tile, g, b0, b1);
+  if (b0 == b1) return;  // no blob meets this tile (uniform over the CTA)
+  const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
+  const int t = threadIdx.x;
+  // the tile's values, row (c, x, y) of eight z at a time, transposed into su
+  for (int r = t; r < 3 * TE * TE; r += IG_T) {
+    const int y = r & 7, cx = r >> 3, c = cx >> 3, x = cx & 7;
+    const int oy = ty * TE + y;
+    const long long idx = ((long long)(tx * TE + x) * g.ny + oy) * g.nz + tz * TE;
+    const bool live = oy < g.ycut && FCM_INB(idx + TE - 1, G, BS_GRID);
+    T v[TE];
+    if constexpr (sizeof(T) == 4) {
+      const float4* src = reinterpret_cast<const float4*>(grid + c * G + idx);
+      const float4 a = live ? __ldg(src) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4 b = live ? __ldg(src + 1) : make_float4(0.f, 0.f, 0.f, 0.f);
+      v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+    } else {
+      const double2* src = reinterpret_cast<const double2*>(grid + c * G + idx);
+#pragma unroll
+      for (int i = 0; i < TE / 2; ++i) {
+        const double2 a = live ? __ldg(src + i) : make_double2(0.0, 0.0);
+        v[2 * i] = a.x;
+        v[2 * i + 1] = a.y;
+      }
+    }
+#pragma unroll
+    for (int z = 0; z < TE; ++z) su[cx * IG_P + z * TE + y] = v[z];
+  }
+  const int grp = t / 24, p = t % 24, c = p >> 3, x = p & 7;
+  for (int c0 = b0; c0 < b1; c0 += IG_B) {
+    const int nc = min(IG_B, b1 - c0);
+    __syncthreads();  // su written; the previous round's weights and sums consumed
+    for (int i = t; i < 4 * IG_B; i += IG_T) {
+      const int k = i >> 2, d = i & 3, kg = k >> 2, kj = k & 3;
+      if (k < nc) {
+        const unsigned long long e = list_entry(list, c0 + k, g);
+        const unsigned b = (unsigned)(e >> 32), lo = (unsigned)e;
+        if (d < 3) {
+          const T* src = wc + ((size_t)(3 * b + d) * NCH + ((lo >> (2 * d)) & 3u)) * TE;
+#pragma unroll
+          for (int q = 0; q < TE; ++q) {
+            const T w = __ldg(src + q);
+            if (d == 0) swx[kg][q][kj] = w;
+            else if (d == 1) swy[k][q] = w;
+            else swz[kg][q][kj] = w;
+          }
+        } else {
+          sflag[k] = lo;
+          sblob[k] = b;
+        }
+      } else if (d < 3) {  // an empty slot of a group: zero weights
+#pragma unroll
+        for (int q = 0; q < TE; ++q) {
+          if (d == 0) swx[kg][q][kj] = 0;
+          else if (d == 1) swy[k][q] = 0;
+          else swz[kg][q][kj] = 0;
+        }
+      }
+    }
+    __syncthreads();
+    if (4 * grp < nc) {
+      const T* col = su + p * IG_P;
+      if constexpr (sizeof(T) == 4) {
+        float2 acc[4][TE / 2];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+          for (int i = 0; i < TE / 2; ++i) acc[j][i] = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int z = 0; z < TE; ++z) {
+          const float4 ua = *reinterpret_cast<const float4*>(col + z * TE);
+          const float4 ub = *reinterpret_cast<const float4*>(col + z * TE + 4);
+          const float4 w4 = *reinterpret_cast<const float4*>(&swz[grp][z][0]);
+          const float2 u2[4] = {make_float2(ua.x, ua.y), make_float2(ua.z, ua.w), make_float2(ub.x, ub.y),
+                                make_float2(ub.z, ub.w)};
+          const float wj[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const float2 w2 = make_float2(wj[j], wj[j]);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) acc[j][i] = __ffma2_rn(w2, u2[i], acc[j][i]);
+          }
+        }
+        const float4 wx4 = *reinterpret_cast<const float4*>(&swx[grp][x][0]);
+        const float wxj[4] = {wx4.x, wx4.y, wx4.z, wx4.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int k = 4 * grp + j;
+          const float4 ya = *reinterpret_cast<const float4*>(&swy[k][0]);
+          const float4 yb = *reinterpret_cast<const float4*>(&swy[k][4]);
+          float2 s2 = make_float2(0.f, 0.f);
+          s2 = __ffma2_rn(make_float2(ya.x, ya.y), acc[j][0], s2);
+          s2 = __ffma2_rn(make_float2(ya.z, ya.w), acc[j][1], s2);
+          s2 = __ffma2_rn(make_float2(yb.x, yb.y), acc[j][2], s2);
+          s2 = __ffma2_rn(make_float2(yb.z, yb.w), acc[j][3], s2);
+          sred[k][c][x] = (s2.x + s2.y) * wxj[j];
+        }
+      } else {
+        T acc[4][TE];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+          for (int y = 0; y < TE; ++y) acc[j][y] = 0;
+#pragma unroll
+        for (int z = 0; z < TE; ++z) {
+          T u[TE];
+#pragma unroll
+          for (int y = 0; y < TE; y += 2) {
+            const double2 a = *reinterpret_cast<const double2*>(col + z * TE + y);
+            u[y] = a.x;
+            u[y + 1] = a.y;
+          }
+          const double2 wa = *reinterpret_cast<const double2*>(&swz[grp][z][0]);
+          const double2 wb = *reinterpret_cast<const double2*>(&swz[grp][z][2]);
+          const T wj[4] = {wa.x, wa.y, wb.x, wb.y};
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int y = 0; y < TE; ++y) acc[j][y] += wj[j] * u[y];
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int k = 4 * grp + j;
+          T sy = 0;
+#pragma unroll
+          for (int y = 0; y < TE; ++y) sy += swy[k][y] * acc[j][y];
+          sred[k][c][x] = sy * swx[grp][x][j];
+        }
+      }
+    }
+    __syncthreads();
+    for (int i = t; i < 3 * nc; i += IG_T) {
+      const int k = i / 3, cc = i - 3 * k;
+      T sum = 0;
+#pragma unroll
+      for (int xx = 0; xx < TE; ++xx) sum += sred[k][cc][xx];
+      const unsigned jt = (sflag[k] >> EJ) & 63u;
+      if (FCM_INB((long long)sblob[k] * 64 + jt, (long long)g.nblobs * 64, BS_PARTIAL))
+        partial[((size_t)sblob[k] * 64 + jt) * 3 + cc] = sum;
+    }
+  }
+}
+
 // V = DX^3 * sum over the blob's tiles (in canonical order j) of the partials.
 template <typename T>
 __device__ __forceinline__ void interp_reduce_one(const int* __restrict__ base, const T* __restrict__ partial,
@@ -1193,7 +1368,7 @@ int launch_interp(const Ctx& c, const BlobTable<T>& t, const T* grid, double* dV
     if (v == 2)
       k_interp_rows<T, 2><<<t.ntiles, 32, 0, s>>>(t.wc, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial);
     else if (v == 1)
-      k_interp_rows<T, 1><<<t.ntiles, 64, 0, s>>>(t.wc, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial);
+      k_interp_gemm<T><<<t.ntiles, IG_T, 0, s>>>(t.wc, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial);
     else
       k_interp_tiled<T><<<t.ntiles, 64, 0, s>>>(t.wc, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial);
     FCM_LAUNCH_CHECK();

@@ -329,8 +329,8 @@ class Suspension:
     # interp, FP32 interp]; spread 0 = persistent pipelined, 1 / 2 / 3 = one CTA
     # per tile staging 16 / 8 / 32 blobs per round;
     # solve 0 = cuFFT 3D, 1 = cuFFT (y, z) + fused x-transform, 2 = the library's
-    # (y, z) + fused x; interp 0 = shuffle reduction, 1 / 2 = shared-memory
-    # reduction with 64 / 32 threads per tile
+    # (y, z) + fused x; interp 0 = shuffle reduction, 1 = contraction order (z
+    # as a register GEMM, then y, x), 2 = shared-memory reduction, 32 threads
     NUM_VARIANTS = 6
 
     def get_variants(self):
