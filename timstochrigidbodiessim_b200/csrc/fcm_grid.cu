@@ -925,25 +925,56 @@ __global__ void __launch_bounds__(64 / R) k_interp_rows(const T* __restrict__ wc
 // then s[b] = wx[b][x] * sum_y wy[b][y] T1[b][y], and the eight x of a (blob, c)
 // are added in x order from shared memory into partial[blob][j][c].  Every point of
 // the tile enters (the chunk weights are zero outside a stencil), so no half masks
-// are tested; per (blob, tile) pair this issues about a third of the instructions
-// of the shuffle-reduction kernel, which matters where many blobs meet each tile.
-// In FP32 the z-contraction and the y-sum run on the packed two-lane FMA over
-// y-pairs.
+// are tested.  The weights of the next round are loaded while the current round
+// is contracted (two staging buffers), and the tile's values are loaded while the
+// first round's list entries and weights are.  In FP32 the z-contraction and the
+// y-sum run on the packed two-lane FMA over y-pairs.
 constexpr int IG_B = 16;          // blobs per round
 constexpr int IG_T = 96;          // threads: 4 groups x 3 components x 8 x
 constexpr int IG_P = TE * TE + 4; // padded (c, x) block of su
+
+// Staging of one round: threads i < 64 take (d, k) = (i / 16, i % 16): the x-, y-
+// or z-weight chunk (d < 3) or the list entry (d = 3) of the round's blob k.
+template <typename T>
+struct IgStage {
+  T w[TE];
+  unsigned long long e;
+  __device__ __forceinline__ void load(const unsigned long long* __restrict__ list, const T* __restrict__ wc,
+                                       int c0, int nc, const TileGeom& g) {
+    const int i = threadIdx.x, k = i & 15, d = i >> 4;
+    e = 0ull;
+    if (i >= 64 || k >= nc) return;
+    e = list_entry(list, c0 + k, g);
+    if (d == 3) return;
+    const unsigned b = (unsigned)(e >> 32), lo = (unsigned)e;
+    const T* src = wc + ((size_t)(3 * b + d) * NCH + ((lo >> (2 * d)) & 3u)) * TE;
+    if constexpr (sizeof(T) == 4) {
+      const float4 a = __ldg(reinterpret_cast<const float4*>(src));
+      const float4 c = __ldg(reinterpret_cast<const float4*>(src) + 1);
+      w[0] = a.x, w[1] = a.y, w[2] = a.z, w[3] = a.w, w[4] = c.x, w[5] = c.y, w[6] = c.z, w[7] = c.w;
+    } else {
+#pragma unroll
+      for (int q = 0; q < TE / 2; ++q) {
+        const double2 a = __ldg(reinterpret_cast<const double2*>(src) + q);
+        w[2 * q] = a.x;
+        w[2 * q + 1] = a.y;
+      }
+    }
+  }
+};
 
 template <typename T>
 __global__ void __launch_bounds__(IG_T) k_interp_gemm(const T* __restrict__ wc, const T* __restrict__ grid,
                                                       TileGeom g, const int* __restrict__ offset,
                                                       const unsigned long long* __restrict__ list, long long G,
                                                       T* __restrict__ partial) {
+  constexpr int ZD = sizeof(T) == 4 ? 2 : 1;        // z-weights held twice in FP32 (packed-FMA operands)
   __shared__ __align__(16) T su[3 * TE * IG_P];
-  __shared__ __align__(16) T swz[IG_B / 4][TE][4];  // [group][z][blob of the group]
-  __shared__ __align__(16) T swx[IG_B / 4][TE][4];  // [group][x][blob of the group]
-  __shared__ __align__(16) T swy[IG_B][TE];         // [blob][y]
-  __shared__ __align__(16) T sred[IG_B][3][TE];     // [blob][c][x]
-  __shared__ unsigned sflag[IG_B], sblob[IG_B];
+  __shared__ __align__(16) T swz[2][IG_B / 4][TE][4 * ZD];  // [buffer][group][z][blob of the group]
+  __shared__ __align__(16) T swx[2][IG_B / 4][TE][4];       // [buffer][group][x][blob of the group]
+  __shared__ __align__(16) T swy[2][IG_B][TE];              // [buffer][blob][y]
+  __shared__ __align__(16) T sred[IG_B][3][TE];             // [blob][c][x]
+  __shared__ unsigned sflag[2][IG_B], sblob[2][IG_B];
   const int tile = blockIdx.x;
   if (!FCM_INB(tile, (long long)g.ntx * g.nty * g.ntz, BS_TILE)) return;  // uniform over the CTA
   int b0, b1;
@@ -951,62 +982,73 @@ __global__ void __launch_bounds__(IG_T) k_interp_gemm(const T* __restrict__ wc, 
   if (b0 == b1) return;  // no blob meets this tile (uniform over the CTA)
   const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
   const int t = threadIdx.x;
-  // the tile's values, row (c, x, y) of eight z at a time, transposed into su
-  for (int r = t; r < 3 * TE * TE; r += IG_T) {
-    const int y = r & 7, cx = r >> 3, c = cx >> 3, x = cx & 7;
+  // the staged weights of one round into buffer `buf` (zeros for empty slots)
+  auto stage_store = [&](const IgStage<T>& st, int nc, int buf) {
+    if (t >= 64) return;
+    const int k = t & 15, d = t >> 4, kg = k >> 2, kj = k & 3;
+    const bool live = k < nc;
+    if (d == 3) {
+      if (live) {
+        sflag[buf][k] = (unsigned)st.e;
+        sblob[buf][k] = (unsigned)(st.e >> 32);
+      }
+      return;
+    }
+#pragma unroll
+    for (int q = 0; q < TE; ++q) {
+      const T w = live ? st.w[q] : (T)0;
+      if (d == 0) {
+        swx[buf][kg][q][kj] = w;
+      } else if (d == 1) {
+        swy[buf][k][q] = w;
+      } else {
+#pragma unroll
+        for (int r = 0; r < ZD; ++r) swz[buf][kg][q][ZD * kj + r] = w;
+      }
+    }
+  };
+  // prologue: the tile's two rows per thread (row r = (c, x, y), eight z) and the
+  // first round's weights are loaded together, then stored
+  T rv[2][TE];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int r = t + h * IG_T, y = r & 7, cx = r >> 3, c = cx >> 3, x = cx & 7;
     const int oy = ty * TE + y;
     const long long idx = ((long long)(tx * TE + x) * g.ny + oy) * g.nz + tz * TE;
     const bool live = oy < g.ycut && FCM_INB(idx + TE - 1, G, BS_GRID);
-    T v[TE];
     if constexpr (sizeof(T) == 4) {
       const float4* src = reinterpret_cast<const float4*>(grid + c * G + idx);
       const float4 a = live ? __ldg(src) : make_float4(0.f, 0.f, 0.f, 0.f);
       const float4 b = live ? __ldg(src + 1) : make_float4(0.f, 0.f, 0.f, 0.f);
-      v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+      rv[h][0] = a.x, rv[h][1] = a.y, rv[h][2] = a.z, rv[h][3] = a.w;
+      rv[h][4] = b.x, rv[h][5] = b.y, rv[h][6] = b.z, rv[h][7] = b.w;
     } else {
       const double2* src = reinterpret_cast<const double2*>(grid + c * G + idx);
 #pragma unroll
-      for (int i = 0; i < TE / 2; ++i) {
-        const double2 a = live ? __ldg(src + i) : make_double2(0.0, 0.0);
-        v[2 * i] = a.x;
-        v[2 * i + 1] = a.y;
+      for (int q = 0; q < TE / 2; ++q) {
+        const double2 a = live ? __ldg(src + q) : make_double2(0.0, 0.0);
+        rv[h][2 * q] = a.x;
+        rv[h][2 * q + 1] = a.y;
       }
     }
-#pragma unroll
-    for (int z = 0; z < TE; ++z) su[cx * IG_P + z * TE + y] = v[z];
   }
+  IgStage<T> st;
+  st.load(list, wc, b0, min(IG_B, b1 - b0), g);
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int r = t + h * IG_T, y = r & 7, cx = r >> 3;
+#pragma unroll
+    for (int z = 0; z < TE; ++z) su[cx * IG_P + z * TE + y] = rv[h][z];
+  }
+  stage_store(st, min(IG_B, b1 - b0), 0);
+  __syncthreads();
   const int grp = t / 24, p = t % 24, c = p >> 3, x = p & 7;
-  for (int c0 = b0; c0 < b1; c0 += IG_B) {
+  int buf = 0;
+  for (int c0 = b0; c0 < b1; c0 += IG_B, buf ^= 1) {
     const int nc = min(IG_B, b1 - c0);
-    __syncthreads();  // su written; the previous round's weights and sums consumed
-    for (int i = t; i < 4 * IG_B; i += IG_T) {
-      const int k = i >> 2, d = i & 3, kg = k >> 2, kj = k & 3;
-      if (k < nc) {
-        const unsigned long long e = list_entry(list, c0 + k, g);
-        const unsigned b = (unsigned)(e >> 32), lo = (unsigned)e;
-        if (d < 3) {
-          const T* src = wc + ((size_t)(3 * b + d) * NCH + ((lo >> (2 * d)) & 3u)) * TE;
-#pragma unroll
-          for (int q = 0; q < TE; ++q) {
-            const T w = __ldg(src + q);
-            if (d == 0) swx[kg][q][kj] = w;
-            else if (d == 1) swy[k][q] = w;
-            else swz[kg][q][kj] = w;
-          }
-        } else {
-          sflag[k] = lo;
-          sblob[k] = b;
-        }
-      } else if (d < 3) {  // an empty slot of a group: zero weights
-#pragma unroll
-        for (int q = 0; q < TE; ++q) {
-          if (d == 0) swx[kg][q][kj] = 0;
-          else if (d == 1) swy[k][q] = 0;
-          else swz[kg][q][kj] = 0;
-        }
-      }
-    }
-    __syncthreads();
+    const bool more = c0 + IG_B < b1;
+    const int ncn = more ? min(IG_B, b1 - c0 - IG_B) : 0;
+    if (more) st.load(list, wc, c0 + IG_B, ncn, g);  // the next round's weights, in flight meanwhile
     if (4 * grp < nc) {
       const T* col = su + p * IG_P;
       if constexpr (sizeof(T) == 4) {
@@ -1019,24 +1061,24 @@ __global__ void __launch_bounds__(IG_T) k_interp_gemm(const T* __restrict__ wc, 
         for (int z = 0; z < TE; ++z) {
           const float4 ua = *reinterpret_cast<const float4*>(col + z * TE);
           const float4 ub = *reinterpret_cast<const float4*>(col + z * TE + 4);
-          const float4 w4 = *reinterpret_cast<const float4*>(&swz[grp][z][0]);
+          const float4 wa = *reinterpret_cast<const float4*>(&swz[buf][grp][z][0]);
+          const float4 wb = *reinterpret_cast<const float4*>(&swz[buf][grp][z][4]);
           const float2 u2[4] = {make_float2(ua.x, ua.y), make_float2(ua.z, ua.w), make_float2(ub.x, ub.y),
                                 make_float2(ub.z, ub.w)};
-          const float wj[4] = {w4.x, w4.y, w4.z, w4.w};
+          const float2 w2[4] = {make_float2(wa.x, wa.y), make_float2(wa.z, wa.w), make_float2(wb.x, wb.y),
+                                make_float2(wb.z, wb.w)};
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const float2 w2 = make_float2(wj[j], wj[j]);
+          for (int j = 0; j < 4; ++j)
 #pragma unroll
-            for (int i = 0; i < 4; ++i) acc[j][i] = __ffma2_rn(w2, u2[i], acc[j][i]);
-          }
+            for (int i = 0; i < 4; ++i) acc[j][i] = __ffma2_rn(w2[j], u2[i], acc[j][i]);
         }
-        const float4 wx4 = *reinterpret_cast<const float4*>(&swx[grp][x][0]);
+        const float4 wx4 = *reinterpret_cast<const float4*>(&swx[buf][grp][x][0]);
         const float wxj[4] = {wx4.x, wx4.y, wx4.z, wx4.w};
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           const int k = 4 * grp + j;
-          const float4 ya = *reinterpret_cast<const float4*>(&swy[k][0]);
-          const float4 yb = *reinterpret_cast<const float4*>(&swy[k][4]);
+          const float4 ya = *reinterpret_cast<const float4*>(&swy[buf][k][0]);
+          const float4 yb = *reinterpret_cast<const float4*>(&swy[buf][k][4]);
           float2 s2 = make_float2(0.f, 0.f);
           s2 = __ffma2_rn(make_float2(ya.x, ya.y), acc[j][0], s2);
           s2 = __ffma2_rn(make_float2(ya.z, ya.w), acc[j][1], s2);
@@ -1059,8 +1101,8 @@ __global__ void __launch_bounds__(IG_T) k_interp_gemm(const T* __restrict__ wc, 
             u[y] = a.x;
             u[y + 1] = a.y;
           }
-          const double2 wa = *reinterpret_cast<const double2*>(&swz[grp][z][0]);
-          const double2 wb = *reinterpret_cast<const double2*>(&swz[grp][z][2]);
+          const double2 wa = *reinterpret_cast<const double2*>(&swz[buf][grp][z][0]);
+          const double2 wb = *reinterpret_cast<const double2*>(&swz[buf][grp][z][2]);
           const T wj[4] = {wa.x, wa.y, wb.x, wb.y};
 #pragma unroll
           for (int j = 0; j < 4; ++j)
@@ -1072,21 +1114,23 @@ __global__ void __launch_bounds__(IG_T) k_interp_gemm(const T* __restrict__ wc, 
           const int k = 4 * grp + j;
           T sy = 0;
 #pragma unroll
-          for (int y = 0; y < TE; ++y) sy += swy[k][y] * acc[j][y];
-          sred[k][c][x] = sy * swx[grp][x][j];
+          for (int y = 0; y < TE; ++y) sy += swy[buf][k][y] * acc[j][y];
+          sred[k][c][x] = sy * swx[buf][grp][x][j];
         }
       }
     }
+    if (more) stage_store(st, ncn, buf ^ 1);
     __syncthreads();
     for (int i = t; i < 3 * nc; i += IG_T) {
       const int k = i / 3, cc = i - 3 * k;
       T sum = 0;
 #pragma unroll
       for (int xx = 0; xx < TE; ++xx) sum += sred[k][cc][xx];
-      const unsigned jt = (sflag[k] >> EJ) & 63u;
-      if (FCM_INB((long long)sblob[k] * 64 + jt, (long long)g.nblobs * 64, BS_PARTIAL))
-        partial[((size_t)sblob[k] * 64 + jt) * 3 + cc] = sum;
+      const unsigned jt = (sflag[buf][k] >> EJ) & 63u;
+      if (FCM_INB((long long)sblob[buf][k] * 64 + jt, (long long)g.nblobs * 64, BS_PARTIAL))
+        partial[((size_t)sblob[buf][k] * 64 + jt) * 3 + cc] = sum;
     }
+    __syncthreads();
   }
 }
 

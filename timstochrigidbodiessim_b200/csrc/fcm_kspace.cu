@@ -564,9 +564,28 @@ __device__ __forceinline__ void xfft_planes_cta(C* __restrict__ spec, const KPar
   }
 }
 
-// Interior CTA (every kz of the chunk except the Hermitian planes): the step over
-// n1 reads its pencils straight from the spectrum into registers and writes the
-// transformed, twiddled values to shared memory [N][3 TK]; after one barrier each
+// One spectrum element (8 bytes FP32, 16 bytes FP64) from global to shared memory
+// by an asynchronous copy (cp.async; the element addresses are aligned to their
+// size, the rows of nz/2 + 1 elements are not 16-byte aligned in FP32).
+template <typename C>
+__device__ __forceinline__ void elem_async(C* dst, const C* src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  if constexpr (sizeof(C) == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+// Whether the interior CTAs bring their pencils into shared memory by
+// asynchronous copies before the first step (all of the CTA's loads in flight at
+// once) rather than loading each pencil into registers in the first step.
+#ifndef FCM_XFFT_ASYNC
+#define FCM_XFFT_ASYNC 1
+#endif
+
+// Interior CTA (every kz of the chunk except the Hermitian planes): the CTA's
+// pencils [N][3 TK] are copied asynchronously into shared memory, then the step
+// over n1 transforms them in place (twiddled); after one barrier each
 // thread takes one (k1, kz) and runs, without barriers, the forward step over n2
 // of the three components, the projection of those N2 modes and the inverse step
 // over n2 with its twiddles; after a second barrier the inverse step over n1 goes
@@ -583,18 +602,38 @@ __device__ __forceinline__ void xfft_interior_cta(C* __restrict__ spec, const KP
   const int kzn = k.nz / 2;
   const long long xs = (long long)k.ny * k.nzh;  // x stride of the spectrum
   const long long row = (long long)y * k.nzh + k0;
+#if FCM_XFFT_ASYNC
+  // the CTA's pencils: element (x, column) to s[x][column]; columns the CTA does
+  // not transform (kz = 0, kz >= nz/2) are not copied and not used
+  for (int i = threadIdx.x; i < N1 * N2 * NC; i += blockDim.x) {
+    const int col = i % NC, x = i / NC, kzl = col % TK, c = col / TK;
+    const int kz = k0 + kzl;
+    const long long e = c * k.Gc + row + kzl + (long long)x * xs;
+    if (kz != 0 && kz < kzn && FCM_INB(e, 3 * k.Gc, BS_SPECTRUM))
+      elem_async<C>(reinterpret_cast<C*>(s + (size_t)x * NC + col), spec + e);
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  __syncthreads();
+#endif
   // forward step over n1: item (column, n2), column = c*TK + kz_local
   for (int i = threadIdx.x; i < N2 * NC; i += blockDim.x) {
     const int col = i % NC, n2 = i / NC, kzl = col % TK, c = col / TK;
     const int kz = k0 + kzl;
     const bool mine = kz != 0 && kz < kzn;
-    const C* src = spec + c * k.Gc + row + kzl;
     V2<T> a[N1];
+#if FCM_XFFT_ASYNC
+    if (!mine) continue;
+#pragma unroll
+    for (int j = 0; j < N1; ++j) a[j] = s[(j * N2 + n2) * NC + col];
+#else
+    const C* src = spec + c * k.Gc + row + kzl;
 #pragma unroll
     for (int j = 0; j < N1; ++j)
       a[j] = (mine && FCM_INB(c * k.Gc + row + kzl + (long long)(j * N2 + n2) * xs, 3 * k.Gc, BS_SPECTRUM))
                  ? ldt<T>(src[(long long)(j * N2 + n2) * xs])
                  : V2<T>{(T)0, (T)0};
+#endif
     dft<T, N1, false>(a);
 #pragma unroll
     for (int j = 1; j < N1; ++j) a[j] = cmul(a[j], ldt<T>(__ldg(&twN[n2 * j])));
@@ -847,6 +886,12 @@ __global__ void __launch_bounds__(256) k_zfft_c2r(const C* __restrict__ in, T* _
 }
 
 // C2C along y, in place: blockIdx.y = x-plane (3 nx per grid), TK kz per CTA.
+// Both directions split NY = Y1 Y2 the same way (input n = j Y2 + n2, output
+// k = k1 + Y1 k2): Y1-point DFTs over j, the twiddles W_NY^(n2 k1) (conjugated for
+// the inverse), Y2-point DFTs over n2.  The CTA's [NY][TK] block is first copied
+// into shared memory by asynchronous copies (all of its loads in flight at once);
+// the first step transforms it in place, the second writes the result to the
+// spectrum.
 template <typename T, typename C, int Y1, int Y2, int TK, bool INV>
 __global__ void __launch_bounds__(256) k_yfft(C* __restrict__ spec, int nzh, const C* __restrict__ twY) {
   constexpr int NY = Y1 * Y2;
@@ -854,65 +899,51 @@ __global__ void __launch_bounds__(256) k_yfft(C* __restrict__ spec, int nzh, con
   V2<T>* s = reinterpret_cast<V2<T>*>(yfft_smem);  // [NY][TK]
   const int k0 = (int)blockIdx.x * TK;
   C* base = spec + (long long)blockIdx.y * NY * nzh + k0;
-  if (!INV) {
-    for (int i = threadIdx.x; i < Y2 * TK; i += blockDim.x) {
-      const int kzl = i % TK, n2 = i / TK;
-      const bool live = k0 + kzl < nzh;
-      V2<T> a[Y1];
+#if FCM_XFFT_ASYNC
+  for (int i = threadIdx.x; i < NY * TK; i += blockDim.x) {
+    const int kzl = i % TK, y = i / TK;
+    if (k0 + kzl < nzh) elem_async<C>(reinterpret_cast<C*>(s + i), base + (long long)y * nzh + kzl);
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  __syncthreads();
+#endif
+  for (int i = threadIdx.x; i < Y2 * TK; i += blockDim.x) {
+    const int kzl = i % TK, n2 = i / TK;
+    const bool live = k0 + kzl < nzh;
+    V2<T> a[Y1];
+#if FCM_XFFT_ASYNC
+    if (!live) continue;
 #pragma unroll
-      for (int j = 0; j < Y1; ++j)
-        a[j] = live ? ldt<T>(base[(long long)(j * Y2 + n2) * nzh + kzl]) : V2<T>{(T)0, (T)0};
-      dft<T, Y1, false>(a);
+    for (int j = 0; j < Y1; ++j) a[j] = s[(j * Y2 + n2) * TK + kzl];
+#else
 #pragma unroll
-      for (int j = 1; j < Y1; ++j) a[j] = cmul(a[j], ldt<T>(__ldg(&twY[n2 * j])));
+    for (int j = 0; j < Y1; ++j)
+      a[j] = live ? ldt<T>(base[(long long)(j * Y2 + n2) * nzh + kzl]) : V2<T>{(T)0, (T)0};
+#endif
+    dft<T, Y1, INV>(a);
 #pragma unroll
-      for (int j = 0; j < Y1; ++j) s[(j * Y2 + n2) * TK + kzl] = a[j];
+    for (int j = 1; j < Y1; ++j) {
+      const V2<T> w = ldt<T>(__ldg(&twY[n2 * j]));
+      a[j] = INV ? cmulc(a[j], w) : cmul(a[j], w);
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < Y1 * TK; i += blockDim.x) {
-      const int kzl = i % TK, k1 = i / TK;
-      if (k0 + kzl >= nzh) continue;
-      V2<T> b[Y2];
 #pragma unroll
-      for (int j = 0; j < Y2; ++j) b[j] = s[(k1 * Y2 + j) * TK + kzl];
-      dft<T, Y2, false>(b);
+    for (int j = 0; j < Y1; ++j) s[(j * Y2 + n2) * TK + kzl] = a[j];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < Y1 * TK; i += blockDim.x) {
+    const int kzl = i % TK, k1 = i / TK;
+    if (k0 + kzl >= nzh) continue;
+    V2<T> b[Y2];
 #pragma unroll
-      for (int j = 0; j < Y2; ++j) {
-        C o;
-        o.x = b[j].x;
-        o.y = b[j].y;
-        base[(long long)(k1 + Y1 * j) * nzh + kzl] = o;
-      }
-    }
-  } else {
-    for (int i = threadIdx.x; i < Y1 * TK; i += blockDim.x) {
-      const int kzl = i % TK, k1 = i / TK;
-      const bool live = k0 + kzl < nzh;
-      V2<T> b[Y2];
+    for (int j = 0; j < Y2; ++j) b[j] = s[(k1 * Y2 + j) * TK + kzl];
+    dft<T, Y2, INV>(b);
 #pragma unroll
-      for (int j = 0; j < Y2; ++j)
-        b[j] = live ? ldt<T>(base[(long long)(k1 + Y1 * j) * nzh + kzl]) : V2<T>{(T)0, (T)0};
-      dft<T, Y2, true>(b);
-#pragma unroll
-      for (int j = 1; j < Y2; ++j) b[j] = cmulc(b[j], ldt<T>(__ldg(&twY[j * k1])));
-#pragma unroll
-      for (int j = 0; j < Y2; ++j) s[(k1 * Y2 + j) * TK + kzl] = b[j];
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < Y2 * TK; i += blockDim.x) {
-      const int kzl = i % TK, n2 = i / TK;
-      if (k0 + kzl >= nzh) continue;
-      V2<T> a[Y1];
-#pragma unroll
-      for (int j = 0; j < Y1; ++j) a[j] = s[(j * Y2 + n2) * TK + kzl];
-      dft<T, Y1, true>(a);
-#pragma unroll
-      for (int j = 0; j < Y1; ++j) {
-        C o;
-        o.x = a[j].x;
-        o.y = a[j].y;
-        base[(long long)(j * Y2 + n2) * nzh + kzl] = o;
-      }
+    for (int j = 0; j < Y2; ++j) {
+      C o;
+      o.x = b[j].x;
+      o.y = b[j].y;
+      base[(long long)(k1 + Y1 * j) * nzh + kzl] = o;
     }
   }
 }
@@ -1290,6 +1321,25 @@ int zfft(const Ctx& c, const T* r, typename cplx_t<T>::type* spec, T* r_out, lon
   });
 }
 
+// Dynamic shared memory above the default 48 KB for `kernel`, set once per device.
+template <typename K>
+int smem_attr_once(K kernel, size_t smem) {
+  if (smem <= 48 * 1024) return FCM_OK;
+  static std::mutex mu;
+  static std::vector<bool> done;
+  int dev = 0;
+  FCM_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if ((int)done.size() <= dev) done.resize(dev + 1, false);
+  if (!done[dev]) {
+    FCM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    done[dev] = true;
+  }
+  return FCM_OK;
+}
+
+// y pass: 16 kz per CTA (rows of 128 bytes in FP32; the second step has Y1 * 16 =
+// 256 items, one per thread, for Y1 = 16); 64 KB of shared memory at 512 points.
 template <typename T>
 int yfft(const Ctx& c, typename cplx_t<T>::type* spec, int nplanes, bool inverse, cudaStream_t s) {
   using C = typename cplx_t<T>::type;
@@ -1297,13 +1347,16 @@ int yfft(const Ctx& c, typename cplx_t<T>::type* spec, int nplanes, bool inverse
   const int nzh = c.g.nzh;
   return with_factors(c.g.ny, [&](auto a, auto b) -> int {
     constexpr int Y1 = decltype(a)::value, Y2 = decltype(b)::value;
-    constexpr int TK = Y1 * Y2 <= 256 ? 16 : 8;
+    constexpr int TK = 16;
     const size_t smem = (size_t)Y1 * Y2 * TK * sizeof(C);
     const dim3 grid((unsigned)((nzh + TK - 1) / TK), (unsigned)nplanes);
-    if (inverse)
+    if (inverse) {
+      FCM_TRY(smem_attr_once(k_yfft<T, C, Y1, Y2, TK, true>, smem));
       k_yfft<T, C, Y1, Y2, TK, true><<<grid, 256, smem, s>>>(spec, nzh, tw);
-    else
+    } else {
+      FCM_TRY(smem_attr_once(k_yfft<T, C, Y1, Y2, TK, false>, smem));
       k_yfft<T, C, Y1, Y2, TK, false><<<grid, 256, smem, s>>>(spec, nzh, tw);
+    }
     FCM_LAUNCH_CHECK();
     return (int)FCM_OK;
   });
