@@ -304,7 +304,8 @@ int fcm_interp(fcm_ctx* ctx, int32_t precision, double* V);
  *   [1] FP64 Stokes solve, [3] FP32 Stokes solve: 0 = cuFFT 3D transforms and the
  *       projection kernel, 1 = cuFFT (y, z) transforms around the fused x-transform
  *       + projection kernel, 2 = the library's own (y, z) transforms around it
- *       (FP32 only).  The solves agree within rounding.
+ *       (FP32 only).  FP64 defaults to 0 beyond 256 points along x.  The solves
+ *       agree within rounding.
  *   [4] FP64 interpolation, [5] FP32 interpolation: 0 = 64 threads per 8^3 tile
  *       with a warp shuffle reduction, 1 = 96 threads per tile in contraction
  *       order (the tile in shared memory, z contracted as a 4-blob x 8-y register

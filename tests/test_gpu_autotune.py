@@ -104,17 +104,22 @@ def test_variants_refused_where_the_grid_does_not_allow_them(gpu):
         assert rel_err(_mf(h, F, prec), Vo) < TOL[prec], prec
 
 
-@pytest.mark.parametrize("nx", [384, 512])
-def test_long_x_transforms(gpu, nx):
-    """The fused x-transform of the long FP32 lengths (384 = 16 x 24, 512 = 32 x 16)
-    against the 3D transforms and the oracle, on thin boxes (nx x 32 x 32)."""
-    g, Vo, F = _setup((nx, 32, 32), nbodies=24)
-    out = []
-    for sv in (0, 1, 2):
-        v = g.get_variants()
-        v[3] = sv
-        g.set_variants(v)
-        out.append(_mf(g, F, 1))
-        assert rel_err(out[-1], Vo) < TOL[1], sv
-    assert rel_err(out[1], out[0]) < TOL[1]
-    assert rel_err(out[2], out[0]) < TOL[1]
+@pytest.mark.parametrize("n", [(384, 32, 32), (512, 32, 32), (32, 512, 32), (32, 32, 512), (32, 384, 384)])
+def test_long_transforms(gpu, n):
+    """The long lengths (384 = 16 x 24, 512 = 32 x 16) of the fused x-transform and
+    of the library's y and z passes (64 KB of shared memory per y CTA at 512), in
+    both precisions against the 3D transforms and the oracle, on thin boxes.  FP64
+    keeps the 3D transforms by default beyond 256 points along x; the fused path is
+    a tunable variant."""
+    g, Vo, F = _setup(n, nbodies=24)
+    assert g.get_variants()[1] == (0 if n[0] > 256 else 1)
+    for prec in (0, 1):
+        out = []
+        for sv in ((0, 1) if prec == 0 else (0, 1, 2)):
+            v = g.get_variants()
+            v[2 * prec + 1] = sv
+            g.set_variants(v)
+            out.append(_mf(g, F, prec))
+            assert rel_err(out[-1], Vo) < TOL[prec], (prec, sv)
+        for o_ in out[1:]:
+            assert rel_err(o_, out[0]) < TOL[prec], prec

@@ -390,8 +390,8 @@ int setup_xfft(Ctx* c) {
   int n1 = 0, n2 = 0;
   const bool ok = xfft_factor(c->g.nx, &n1, &n2) && c->g.nz % 2 == 0;
   c->xfft[1] = ok;
-  c->xfft[0] = ok && c->g.nx <= 256;
-  c->xfft_cap[0] = c->xfft[0];
+  c->xfft[0] = ok && c->g.nx <= 256;  // FP64 beyond 256 points: the 3D transforms unless tuned
+  c->xfft_cap[0] = ok;
   c->xfft_cap[1] = c->xfft[1];
   if (!ok) return FCM_OK;
   FCM_TRY(xfft_tables_init());

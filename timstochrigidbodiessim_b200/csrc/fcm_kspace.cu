@@ -707,7 +707,7 @@ __device__ __forceinline__ void xfft_interior_cta(C* __restrict__ spec, const KP
 // whose register-resident pencils take about 150 registers.
 template <typename T, int N1, int N2, int TK, bool PLANES>
 constexpr int xfft_block() {
-  return (sizeof(T) == 8 && !PLANES && N1 * N2 <= 256) ? 128 : 256;
+  return (sizeof(T) == 8 && !PLANES) ? 128 : 256;
 }
 
 // CTAs per SM the register allocation must allow: three for the FP32 transforms up
@@ -1158,11 +1158,11 @@ namespace {
 
 // kz per interior CTA: shared memory N * 3 TK elements near 100 KB (two CTAs per
 // SM), TK * N1 threads busy in the middle step.  At 256 points in FP32, 12 kz per
-// CTA (three CTAs per SM) took 171 us against 129 us with 16.  FP64 grids beyond 256
-// points use the 3D transforms instead.
+// CTA (three CTAs per SM) took 171 us against 129 us with 16.  FP64 beyond 256
+// points: 4 kz (98 KB at 512); the autotuner weighs it against the 3D transforms.
 template <typename T>
 constexpr int xfft_tk(int n) {
-  return sizeof(T) == 4 ? (n <= 256 ? 16 : 8) : 8;
+  return sizeof(T) == 4 ? (n <= 256 ? 16 : 8) : (n <= 256 ? 8 : 4);
 }
 
 // Row pairs per plane CTA: one (ny/2 + 1 CTAs per plane; four pairs per CTA left
@@ -1237,15 +1237,12 @@ int xfft_dispatch(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s, 
     case 128: return xfft_run<T, 8, 16>(c, spec, s, prepare, b, gidx, nm, mask);
     case 192: return xfft_run<T, 12, 16>(c, spec, s, prepare, b, gidx, nm, mask);
     case 256: return xfft_run<T, 16, 16>(c, spec, s, prepare, b, gidx, nm, mask);
-    case 384:
-      if constexpr (sizeof(T) == 4) return xfft_run<T, 16, 24>(c, spec, s, prepare, b, gidx, nm, mask);
-      break;
+    case 384: return xfft_run<T, 16, 24>(c, spec, s, prepare, b, gidx, nm, mask);
     case 512:
-      // 32 x 16: the middle step has N1 * TK = 256 items, one per thread (16 x 32
-      // left half the CTA idle there while it ran six 32-point DFTs per item)
-      if constexpr (sizeof(T) == 4)
-        return xfft_run<T, FCM_XFFT512_N1, 512 / FCM_XFFT512_N1>(c, spec, s, prepare, b, gidx, nm, mask);
-      break;
+      // 32 x 16: the middle step has N1 * TK = 256 items in FP32 (128 in FP64), one
+      // per thread (16 x 32 left half the CTA idle there while it ran six 32-point
+      // DFTs per item)
+      return xfft_run<T, FCM_XFFT512_N1, 512 / FCM_XFFT512_N1>(c, spec, s, prepare, b, gidx, nm, mask);
     default: break;
   }
   set_error("fused x-transform: unsupported length " + std::to_string(c.g.nx));
@@ -1321,19 +1318,21 @@ int zfft(const Ctx& c, const T* r, typename cplx_t<T>::type* spec, T* r_out, lon
   });
 }
 
-// Dynamic shared memory above the default 48 KB for `kernel`, set once per device.
+// Dynamic shared memory above the default 48 KB for `kernel`, set once per kernel
+// and device (kernels of one signature share the template instance, so the cache
+// is keyed by the kernel's address).
 template <typename K>
 int smem_attr_once(K kernel, size_t smem) {
   if (smem <= 48 * 1024) return FCM_OK;
   static std::mutex mu;
-  static std::vector<bool> done;
+  static std::vector<std::pair<int, const void*>> done;
   int dev = 0;
   FCM_CUDA(cudaGetDevice(&dev));
+  const std::pair<int, const void*> key(dev, reinterpret_cast<const void*>(kernel));
   std::lock_guard<std::mutex> lock(mu);
-  if ((int)done.size() <= dev) done.resize(dev + 1, false);
-  if (!done[dev]) {
+  if (std::find(done.begin(), done.end(), key) == done.end()) {
     FCM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    done[dev] = true;
+    done.push_back(key);
   }
   return FCM_OK;
 }
