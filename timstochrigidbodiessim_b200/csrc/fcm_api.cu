@@ -411,13 +411,12 @@ int setup_xfft(Ctx* c) {
   c->d_xtw32 = d32;
   FCM_CUDA(cudaMemcpy(d64, wd.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
   FCM_CUDA(cudaMemcpy(d32, wf.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
-  // FP32 (y, z) transforms by the library's kernels for nz up to 256, where they beat
-  // cuFFT's 2D plans (64^3, 96^3: the 64-suspension ensemble ran 11% faster; 256^3:
-  // 328 against 364 us per solve); at 512^3 they took 3324 against 3201 us (z passes
-  // 732 + 736 against 919 + 958 us, y passes 783 + 1074 against 662 + 662 us), so
-  // longer lines stay with cuFFT
+  // FP32 (y, z) transforms by the library's kernels, where they beat cuFFT's 2D
+  // plans: 64^3, 96^3 (the 64-suspension ensemble ran 11% faster), 256^3 (328
+  // against 364 us per solve) and, with 16 kz per y CTA, 512^3 (the whole FP32 solve
+  // 4091 against 4477 us)
   c->yz32_cap = xfft_factor(c->g.ny, &n1, &n2) && xfft_factor(c->g.nz, &n1, &n2) && 3 * c->g.nx <= 65535;
-  c->yz32 = c->yz32_cap && c->g.nz <= 256;
+  c->yz32 = c->yz32_cap;
   if (c->yz32_cap) {
     for (int d = 0; d < 2; ++d) {
       const int m = d == 0 ? c->g.ny : c->g.nz;

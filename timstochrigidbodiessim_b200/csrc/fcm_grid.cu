@@ -927,8 +927,11 @@ __global__ void __launch_bounds__(64 / R) k_interp_rows(const T* __restrict__ wc
 // the tile enters (the chunk weights are zero outside a stencil), so no half masks
 // are tested.  The weights of the next round are loaded while the current round
 // is contracted (two staging buffers), and the tile's values are loaded while the
-// first round's list entries and weights are.  In FP32 the z-contraction and the
-// y-sum run on the packed two-lane FMA over y-pairs.
+// first round's list entries and weights are.  In FP32 each thread holds its
+// (c, x) block of the tile (64 values) in registers for the whole tile, so the
+// contraction reads only the weights (broadcast) from shared memory, and the
+// z-contraction and the y-sum run on the packed two-lane FMA over y-pairs; FP64
+// reads the block from shared memory.
 constexpr int IG_B = 16;          // blobs per round
 constexpr int IG_T = 96;          // threads: 4 groups x 3 components x 8 x
 constexpr int IG_P = TE * TE + 4; // padded (c, x) block of su
@@ -1043,6 +1046,21 @@ __global__ void __launch_bounds__(IG_T) k_interp_gemm(const T* __restrict__ wc, 
   stage_store(st, min(IG_B, b1 - b0), 0);
   __syncthreads();
   const int grp = t / 24, p = t % 24, c = p >> 3, x = p & 7;
+  // FP32: the thread's (c, x) block of the tile, u[z][y] as y-pairs, in registers
+  // for the whole tile (the contraction then reads only weights from shared memory)
+  float2 ur[TE][TE / 2];
+  if constexpr (sizeof(T) == 4) {
+    const T* col = su + p * IG_P;
+#pragma unroll
+    for (int z = 0; z < TE; ++z) {
+      const float4 ua = *reinterpret_cast<const float4*>(col + z * TE);
+      const float4 ub = *reinterpret_cast<const float4*>(col + z * TE + 4);
+      ur[z][0] = make_float2(ua.x, ua.y);
+      ur[z][1] = make_float2(ua.z, ua.w);
+      ur[z][2] = make_float2(ub.x, ub.y);
+      ur[z][3] = make_float2(ub.z, ub.w);
+    }
+  }
   int buf = 0;
   for (int c0 = b0; c0 < b1; c0 += IG_B, buf ^= 1) {
     const int nc = min(IG_B, b1 - c0);
@@ -1050,7 +1068,6 @@ __global__ void __launch_bounds__(IG_T) k_interp_gemm(const T* __restrict__ wc, 
     const int ncn = more ? min(IG_B, b1 - c0 - IG_B) : 0;
     if (more) st.load(list, wc, c0 + IG_B, ncn, g);  // the next round's weights, in flight meanwhile
     if (4 * grp < nc) {
-      const T* col = su + p * IG_P;
       if constexpr (sizeof(T) == 4) {
         float2 acc[4][TE / 2];
 #pragma unroll
@@ -1059,18 +1076,14 @@ __global__ void __launch_bounds__(IG_T) k_interp_gemm(const T* __restrict__ wc, 
           for (int i = 0; i < TE / 2; ++i) acc[j][i] = make_float2(0.f, 0.f);
 #pragma unroll
         for (int z = 0; z < TE; ++z) {
-          const float4 ua = *reinterpret_cast<const float4*>(col + z * TE);
-          const float4 ub = *reinterpret_cast<const float4*>(col + z * TE + 4);
           const float4 wa = *reinterpret_cast<const float4*>(&swz[buf][grp][z][0]);
           const float4 wb = *reinterpret_cast<const float4*>(&swz[buf][grp][z][4]);
-          const float2 u2[4] = {make_float2(ua.x, ua.y), make_float2(ua.z, ua.w), make_float2(ub.x, ub.y),
-                                make_float2(ub.z, ub.w)};
           const float2 w2[4] = {make_float2(wa.x, wa.y), make_float2(wa.z, wa.w), make_float2(wb.x, wb.y),
                                 make_float2(wb.z, wb.w)};
 #pragma unroll
           for (int j = 0; j < 4; ++j)
 #pragma unroll
-            for (int i = 0; i < 4; ++i) acc[j][i] = __ffma2_rn(w2[j], u2[i], acc[j][i]);
+            for (int i = 0; i < 4; ++i) acc[j][i] = __ffma2_rn(w2[j], ur[z][i], acc[j][i]);
         }
         const float4 wx4 = *reinterpret_cast<const float4*>(&swx[buf][grp][x][0]);
         const float wxj[4] = {wx4.x, wx4.y, wx4.z, wx4.w};
@@ -1087,6 +1100,7 @@ __global__ void __launch_bounds__(IG_T) k_interp_gemm(const T* __restrict__ wc, 
           sred[k][c][x] = (s2.x + s2.y) * wxj[j];
         }
       } else {
+        const T* col = su + p * IG_P;
         T acc[4][TE];
 #pragma unroll
         for (int j = 0; j < 4; ++j)

@@ -576,16 +576,11 @@ __device__ __forceinline__ void elem_async(C* dst, const C* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
 }
 
-// Whether the interior CTAs bring their pencils into shared memory by
-// asynchronous copies before the first step (all of the CTA's loads in flight at
-// once) rather than loading each pencil into registers in the first step.
-#ifndef FCM_XFFT_ASYNC
-#define FCM_XFFT_ASYNC 1
-#endif
-
-// Interior CTA (every kz of the chunk except the Hermitian planes): the CTA's
-// pencils [N][3 TK] are copied asynchronously into shared memory, then the step
-// over n1 transforms them in place (twiddled); after one barrier each
+// Interior CTA (every kz of the chunk except the Hermitian planes): the step over
+// n1 transforms the CTA's pencils [N][3 TK] into shared memory (twiddled): for
+// N >= 384 they are first copied there by asynchronous copies, all of the CTA's
+// loads in flight at once (measured 1% faster at 512 points, slower at 256), for
+// shorter pencils each is read straight into registers; after one barrier each
 // thread takes one (k1, kz) and runs, without barriers, the forward step over n2
 // of the three components, the projection of those N2 modes and the inverse step
 // over n2 with its twiddles; after a second barrier the inverse step over n1 goes
@@ -602,38 +597,39 @@ __device__ __forceinline__ void xfft_interior_cta(C* __restrict__ spec, const KP
   const int kzn = k.nz / 2;
   const long long xs = (long long)k.ny * k.nzh;  // x stride of the spectrum
   const long long row = (long long)y * k.nzh + k0;
-#if FCM_XFFT_ASYNC
-  // the CTA's pencils: element (x, column) to s[x][column]; columns the CTA does
-  // not transform (kz = 0, kz >= nz/2) are not copied and not used
-  for (int i = threadIdx.x; i < N1 * N2 * NC; i += blockDim.x) {
-    const int col = i % NC, x = i / NC, kzl = col % TK, c = col / TK;
-    const int kz = k0 + kzl;
-    const long long e = c * k.Gc + row + kzl + (long long)x * xs;
-    if (kz != 0 && kz < kzn && FCM_INB(e, 3 * k.Gc, BS_SPECTRUM))
-      elem_async<C>(reinterpret_cast<C*>(s + (size_t)x * NC + col), spec + e);
+  constexpr bool ASYNC = N1 * N2 >= 384;
+  if constexpr (ASYNC) {
+    // the CTA's pencils: element (x, column) to s[x][column]; columns the CTA does
+    // not transform (kz = 0, kz >= nz/2) are not copied and not used
+    for (int i = threadIdx.x; i < N1 * N2 * NC; i += blockDim.x) {
+      const int col = i % NC, x = i / NC, kzl = col % TK, c = col / TK;
+      const int kz = k0 + kzl;
+      const long long e = c * k.Gc + row + kzl + (long long)x * xs;
+      if (kz != 0 && kz < kzn && FCM_INB(e, 3 * k.Gc, BS_SPECTRUM))
+        elem_async<C>(reinterpret_cast<C*>(s + (size_t)x * NC + col), spec + e);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
   }
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-  __syncthreads();
-#endif
   // forward step over n1: item (column, n2), column = c*TK + kz_local
   for (int i = threadIdx.x; i < N2 * NC; i += blockDim.x) {
     const int col = i % NC, n2 = i / NC, kzl = col % TK, c = col / TK;
     const int kz = k0 + kzl;
     const bool mine = kz != 0 && kz < kzn;
     V2<T> a[N1];
-#if FCM_XFFT_ASYNC
-    if (!mine) continue;
+    if constexpr (ASYNC) {
+      if (!mine) continue;
 #pragma unroll
-    for (int j = 0; j < N1; ++j) a[j] = s[(j * N2 + n2) * NC + col];
-#else
-    const C* src = spec + c * k.Gc + row + kzl;
+      for (int j = 0; j < N1; ++j) a[j] = s[(j * N2 + n2) * NC + col];
+    } else {
+      const C* src = spec + c * k.Gc + row + kzl;
 #pragma unroll
-    for (int j = 0; j < N1; ++j)
-      a[j] = (mine && FCM_INB(c * k.Gc + row + kzl + (long long)(j * N2 + n2) * xs, 3 * k.Gc, BS_SPECTRUM))
-                 ? ldt<T>(src[(long long)(j * N2 + n2) * xs])
-                 : V2<T>{(T)0, (T)0};
-#endif
+      for (int j = 0; j < N1; ++j)
+        a[j] = (mine && FCM_INB(c * k.Gc + row + kzl + (long long)(j * N2 + n2) * xs, 3 * k.Gc, BS_SPECTRUM))
+                   ? ldt<T>(src[(long long)(j * N2 + n2) * xs])
+                   : V2<T>{(T)0, (T)0};
+    }
     dft<T, N1, false>(a);
 #pragma unroll
     for (int j = 1; j < N1; ++j) a[j] = cmul(a[j], ldt<T>(__ldg(&twN[n2 * j])));
@@ -888,10 +884,9 @@ __global__ void __launch_bounds__(256) k_zfft_c2r(const C* __restrict__ in, T* _
 // C2C along y, in place: blockIdx.y = x-plane (3 nx per grid), TK kz per CTA.
 // Both directions split NY = Y1 Y2 the same way (input n = j Y2 + n2, output
 // k = k1 + Y1 k2): Y1-point DFTs over j, the twiddles W_NY^(n2 k1) (conjugated for
-// the inverse), Y2-point DFTs over n2.  The CTA's [NY][TK] block is first copied
-// into shared memory by asynchronous copies (all of its loads in flight at once);
-// the first step transforms it in place, the second writes the result to the
-// spectrum.
+// the inverse), Y2-point DFTs over n2.  The first step reads its pencils straight
+// into registers and writes them to shared memory (an asynchronous-copy prologue
+// measured slower here), the second writes the result to the spectrum.
 template <typename T, typename C, int Y1, int Y2, int TK, bool INV>
 __global__ void __launch_bounds__(256) k_yfft(C* __restrict__ spec, int nzh, const C* __restrict__ twY) {
   constexpr int NY = Y1 * Y2;
@@ -899,28 +894,13 @@ __global__ void __launch_bounds__(256) k_yfft(C* __restrict__ spec, int nzh, con
   V2<T>* s = reinterpret_cast<V2<T>*>(yfft_smem);  // [NY][TK]
   const int k0 = (int)blockIdx.x * TK;
   C* base = spec + (long long)blockIdx.y * NY * nzh + k0;
-#if FCM_XFFT_ASYNC
-  for (int i = threadIdx.x; i < NY * TK; i += blockDim.x) {
-    const int kzl = i % TK, y = i / TK;
-    if (k0 + kzl < nzh) elem_async<C>(reinterpret_cast<C*>(s + i), base + (long long)y * nzh + kzl);
-  }
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-  __syncthreads();
-#endif
   for (int i = threadIdx.x; i < Y2 * TK; i += blockDim.x) {
     const int kzl = i % TK, n2 = i / TK;
     const bool live = k0 + kzl < nzh;
     V2<T> a[Y1];
-#if FCM_XFFT_ASYNC
-    if (!live) continue;
-#pragma unroll
-    for (int j = 0; j < Y1; ++j) a[j] = s[(j * Y2 + n2) * TK + kzl];
-#else
 #pragma unroll
     for (int j = 0; j < Y1; ++j)
       a[j] = live ? ldt<T>(base[(long long)(j * Y2 + n2) * nzh + kzl]) : V2<T>{(T)0, (T)0};
-#endif
     dft<T, Y1, INV>(a);
 #pragma unroll
     for (int j = 1; j < Y1; ++j) {
