@@ -148,11 +148,12 @@ class ClockSampler:
 
 # ----------------------------------------------------------------- ours
 VARIANT_LEGEND = ("variants [FP64 spread, FP64 solve, FP32 spread, FP32 solve, FP64 interp, FP32 interp]: spread "
-                  "0 persistent pipelined, 1 / 2 / 3 one CTA per tile staging 16 / 8 / 32 blobs per round; solve "
-                  "0 cuFFT 3D + projection, 1 cuFFT (y, z) + fused x-transform, 2 library (y, z) + fused "
-                  "x-transform; interp 0 shuffle reduction, 1 contraction order (z as a register GEMM, "
-                  "then y, x), 2 shared-memory reduction with 32 threads per tile.  us[10P + v]: precision P, v 0-3 spread, 4-6 solve, 7-9 interp variants, "
-                  "microseconds per call, -1 not available")
+                  "0 persistent pipelined, 1 / 2 / 3 one CTA per tile staging 16 / 8 / 32 blobs per round, 4 "
+                  "contraction order (FP32); solve 0 cuFFT 3D + projection, 1 cuFFT (y, z) + fused x-transform, "
+                  "2 library (y, z) + fused x-transform; interp 0 shuffle reduction, 1 contraction order (z as "
+                  "a register GEMM, then y, x), 2 shared-memory reduction with 32 threads per tile.  us[12P + v]: "
+                  "precision P, v 0-4 spread, 5-7 solve, 8-10 interp variants, microseconds per call, -1 not "
+                  "available")
 
 AUTOTUNE = {"on": True}
 

@@ -1,7 +1,8 @@
 """Kernel variants of the grid stages and their autotuner (no reference
 counterpart).  The four spread kernels (persistent pipelined; one CTA per tile
 staging 16, 8 or 32 blobs per round) sum every grid point's blobs in the same
-order, so M F is the same bit for bit whichever runs; the Stokes-solve variants
+order, so M F is the same bit for bit whichever runs; the FP32 contraction-order
+spread (variant 4) agrees with them within rounding; the Stokes-solve variants
 (cuFFT 3D + projection, cuFFT (y, z) + fused x-transform, the library's (y, z)
 kernels + fused x-transform) and the three interpolation kernels (shuffle
 reduction; contraction order with z as a register GEMM; shared-memory reduction
@@ -57,6 +58,12 @@ def test_variants_agree(gpu):
             for o_ in out[1:]:
                 assert np.array_equal(out[0], o_), (prec, sv)
             assert rel_err(out[0], Vo) < TOL[prec], (prec, sv)
+            if prec == 1:  # the contraction-order spread: same grid within rounding
+                v = g.get_variants()
+                v[2], v[3] = 4, sv
+                g.set_variants(v)
+                o4 = _mf(g, F, 1)
+                assert rel_err(o4, out[0]) < TOL[1] and rel_err(o4, Vo) < TOL[1], sv
         for iv in (0, 1, 2):
             v = g.get_variants()
             v[4 + prec] = iv
@@ -68,11 +75,13 @@ def test_variants_agree(gpu):
 def test_autotune_keeps_the_fastest(gpu):
     g, Vo, F = _setup()
     v, us = g.autotune(reps=3)
-    assert np.all(us[0:6] > 0) and us[6] == -1  # FP64 has no library (y, z) variant
-    assert np.all(us[7:10] > 0) and np.all(us[10:20] > 0)
+    assert np.all(us[0:4] > 0) and us[4] == -1  # no contraction-order spread in FP64
+    assert np.all(us[5:7] > 0) and us[7] == -1  # FP64 has no library (y, z) variant
+    assert np.all(us[8:11] > 0) and us[11] == -1
+    assert np.all(us[12:23] > 0) and us[23] == -1
     for P in (0, 1):
-        t = us[10 * P:10 * P + 10]
-        spread, solve, interp = t[0:4], t[4:7], t[7:10]
+        t = us[12 * P:12 * P + 12]
+        spread, solve, interp = t[0:(5 if P else 4)], t[5:8], t[8:11]
         assert v[2 * P] == int(np.argmin(spread))
         best = min((x, i) for i, x in enumerate(solve) if x >= 0)[1]
         assert v[2 * P + 1] == best
@@ -87,7 +96,9 @@ def test_variants_refused_where_the_grid_does_not_allow_them(gpu):
     with pytest.raises(FcmError):
         g.set_variants([0, 2, 1, 2, 0, 0])  # no library (y, z) variant in FP64
     with pytest.raises(FcmError):
-        g.set_variants([4, 1, 1, 2, 0, 0])  # out of range
+        g.set_variants([4, 1, 1, 2, 0, 0])  # out of range (contraction-order spread is FP32 only)
+    with pytest.raises(FcmError):
+        g.set_variants([0, 1, 5, 2, 0, 0])  # out of range
     with pytest.raises(FcmError):
         g.set_variants([0, 1, 1, 2, 3, 0])  # no interpolation variant 3
     # 20 points along x: no fused x-transform, so only the 3D solve; not tiled, so
@@ -97,8 +108,8 @@ def test_variants_refused_where_the_grid_does_not_allow_them(gpu):
     with pytest.raises(FcmError):
         h.set_variants([0, 1, 1, 0, 0, 0])
     v, us = h.autotune(reps=2)
-    assert us[5] == -1 and us[15] == -1 and us[16] == -1
-    assert np.all(us[0:4] == -1) and np.all(us[7:10] == -1) and np.all(us[17:20] == -1)
+    assert us[6] == -1 and us[18] == -1 and us[19] == -1
+    assert np.all(us[0:5] == -1) and np.all(us[8:11] == -1) and np.all(us[12:17] == -1) and np.all(us[20:23] == -1)
     assert v[1] == 0 and v[3] == 0
     for prec in (0, 1):
         assert rel_err(_mf(h, F, prec), Vo) < TOL[prec], prec

@@ -2528,7 +2528,7 @@ static void get_variants(const Ctx* c, int32_t* v) {
 static int set_variants(Ctx* c, const int32_t* v) {
   for (int P = 0; P < 2; ++P) {
     const int sp = v[2 * P], sv = v[2 * P + 1], iv = v[4 + P];
-    if (sp < 0 || sp > 3 || sv < 0 || sv > (P == 1 ? 2 : 1) || iv < 0 || iv > 2) {
+    if (sp < 0 || sp > (P == 1 ? 4 : 3) || sv < 0 || sv > (P == 1 ? 2 : 1) || iv < 0 || iv > 2) {
       set_error("kernel variant out of range");
       return FCM_ERR_INVALID;
     }
@@ -2575,21 +2575,23 @@ static int time_calls(Ctx* c, int reps, F&& body, double* out) {
   return FCM_OK;
 }
 
-// The spread and solve variants of one precision timed on c's own grid and blob
-// table; the fastest kept.  t[0..1] spread, t[2..4] solve (-1: not available).
+// The spread, solve and interpolation variants of one precision timed on c's own
+// grid and blob table; the fastest kept.  t[0..4] spread (4: FP32 only), t[5..7]
+// solve, t[8..10] interpolation (-1: not available).
 template <typename T>
 static int tune_precision(Ctx* c, int reps, double* t) {
   constexpr int P = sizeof(T) == 8 ? 0 : 1;
   GridBufs<T>& gb = grid_of<T>(c);
   const BlobTable<T>& bt = gb.blobs;
   FCM_CUDA(cudaMemsetAsync(c->d_tmp3, 0, sizeof(double) * 3 * (size_t)(c->Nb > 0 ? c->Nb : 1), c->stream));
+  constexpr int NSP = P == 1 ? 5 : 4;  // spread variants of this precision
   if (bt.tiled) {
-    for (int v = 0; v < 4; ++v) {
+    for (int v = 0; v < NSP; ++v) {
       c->spread_variant[P] = v;
       FCM_TRY(time_calls(c, reps, [&] { return spread_t<T>(c, bt, c->d_tmp3); }, &t[v]));
     }
     int bs = 0;
-    for (int v = 1; v < 4; ++v)
+    for (int v = 1; v < NSP; ++v)
       if (t[v] < t[bs]) bs = v;
     c->spread_variant[P] = bs;
   }
@@ -2598,21 +2600,21 @@ static int tune_precision(Ctx* c, int reps, double* t) {
     if ((v >= 1 && !c->xfft_cap[P]) || (v == 2 && (P == 0 || !c->yz32_cap))) continue;
     c->xfft[P] = v >= 1;
     if (P == 1) c->yz32 = v == 2;
-    FCM_TRY(time_calls(c, reps, [&] { return stokes_t<T>(c); }, &t[4 + v]));
+    FCM_TRY(time_calls(c, reps, [&] { return stokes_t<T>(c); }, &t[5 + v]));
   }
   int best = 0;
   for (int v = 1; v < 3; ++v)
-    if (t[4 + v] >= 0.0 && t[4 + v] < t[4 + best]) best = v;
+    if (t[5 + v] >= 0.0 && t[5 + v] < t[5 + best]) best = v;
   c->xfft[P] = best >= 1;
   if (P == 1) c->yz32 = best == 2;
   if (bt.tiled) {  // interpolation of the (zeroed) grid into scratch
     for (int v = 0; v < 3; ++v) {
       c->interp_variant[P] = v;
-      FCM_TRY(time_calls(c, reps, [&] { return interp_t<T>(c, bt, gb.r, c->d_tmp3); }, &t[7 + v]));
+      FCM_TRY(time_calls(c, reps, [&] { return interp_t<T>(c, bt, gb.r, c->d_tmp3); }, &t[8 + v]));
     }
     int bi = 0;
     for (int v = 1; v < 3; ++v)
-      if (t[7 + v] < t[7 + bi]) bi = v;
+      if (t[8 + v] < t[8 + bi]) bi = v;
     c->interp_variant[P] = bi;
   }
   return FCM_OK;

@@ -327,11 +327,12 @@ class Suspension:
 
     # kernel variants: [FP64 spread, FP64 solve, FP32 spread, FP32 solve, FP64
     # interp, FP32 interp]; spread 0 = persistent pipelined, 1 / 2 / 3 = one CTA
-    # per tile staging 16 / 8 / 32 blobs per round;
+    # per tile staging 16 / 8 / 32 blobs per round, 4 = contraction order (FP32);
     # solve 0 = cuFFT 3D, 1 = cuFFT (y, z) + fused x-transform, 2 = the library's
     # (y, z) + fused x; interp 0 = shuffle reduction, 1 = contraction order (z
     # as a register GEMM, then y, x), 2 = shared-memory reduction, 32 threads
     NUM_VARIANTS = 6
+    NUM_TUNE_TIMES = 24
 
     def get_variants(self):
         v, pv = _out(None, self.NUM_VARIANTS, np.int32)
@@ -344,10 +345,10 @@ class Suspension:
 
     def autotune(self, reps=5):
         """Time every variant the grids allow and keep the fastest.  Returns
-        (variants, us): us[10 P + v] microseconds per call for precision P, v = 0-3
-        spread variants, 4, 5, 6 solve variants, 7, 8, 9 interpolation variants
-        (-1 where not available)."""
-        us, pu = _out(None, 20)
+        (variants, us): us[12 P + v] microseconds per call for precision P, v = 0-4
+        spread variants, 5, 6, 7 solve variants, 8, 9, 10 interpolation variants
+        (-1 where not available; v = 11 unused)."""
+        us, pu = _out(None, self.NUM_TUNE_TIMES)
         v, pv = _out(None, self.NUM_VARIANTS, np.int32)
         self._c(self.L.fcm_autotune(self.h, reps, pu, pv), "fcm_autotune")
         return [int(x) for x in v], us
