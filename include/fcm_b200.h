@@ -310,10 +310,10 @@ int fcm_interp(fcm_ctx* ctx, int32_t precision, double* V);
  *       (FP32 only).  FP64 defaults to 0 beyond 256 points along x.  The solves
  *       agree within rounding.
  *   [4] FP64 interpolation, [5] FP32 interpolation: 0 = 64 threads per 8^3 tile
- *       with a warp shuffle reduction, 1 = 96 threads per tile in contraction
- *       order (the tile in shared memory, z contracted as a 4-blob x 8-y register
- *       GEMM, then y and x), 2 = one warp per tile (two y-rows per thread) with a
- *       shared-memory reduction.  They agree within rounding.
+ *       with a warp shuffle reduction, 1 = one warp per tile (two y-rows per
+ *       lane, added in the lane) with the shuffle reduction, 2 = one warp per tile
+ *       (two y-rows per thread) with a shared-memory reduction.  They agree within
+ *       rounding.
  * A variant the grid does not allow (solve 1 and 2 need supported lengths, 2 also
  * nz <= 512) or out of range is refused with FCM_ERR_INVALID; the spread and
  * interpolation entries have no effect where the grid is not tiled, the FP32

@@ -4,9 +4,9 @@ staging 16, 8 or 32 blobs per round) sum every grid point's blobs in the same
 order, so M F is the same bit for bit whichever runs; the FP32 contraction-order
 spread (variant 4) agrees with them within rounding; the Stokes-solve variants
 (cuFFT 3D + projection, cuFFT (y, z) + fused x-transform, the library's (y, z)
-kernels + fused x-transform) and the three interpolation kernels (shuffle
-reduction; contraction order with z as a register GEMM; shared-memory reduction
-with two y-rows per thread) agree with the oracle
+kernels + fused x-transform) and the three interpolation kernels (64 threads per
+tile with the shuffle reduction; one warp per tile, two y-rows per lane, with the
+shuffle or a shared-memory reduction) agree with the oracle
 within 1e-10 (FP64) and 1e-6 (FP32) relative.  fcm_autotune times what the grid
 allows, keeps the fastest by its own timings, and the results after tuning still
 match the oracle."""

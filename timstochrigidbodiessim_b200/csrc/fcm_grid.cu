@@ -1057,236 +1057,88 @@ __global__ void __launch_bounds__(64 / R) k_interp_rows(const T* __restrict__ wc
   }
 }
 
-// Tiled interpolation in contraction order: one CTA (96 threads) per 8x8x8 tile.
-// The tile's grid values go to shared memory as su[c][x][z][y] (y fastest, each
-// (c, x) block padded to 68 so that eight threads' 16-byte reads of different
-// blocks meet different banks).  Blobs are taken 16 per round, in four groups of
-// four; thread t = (group, c, x) = (t / 24, (t % 24) / 8, t % 8) forms, for the
-// four blobs of its group and the eight y of its (c, x) row,
-//   T1[b][y] = sum_z wz[b][z] u[c][x][y][z]          (a 4 x 8 x 8 register GEMM),
-// then s[b] = wx[b][x] * sum_y wy[b][y] T1[b][y], and the eight x of a (blob, c)
-// are added in x order from shared memory into partial[blob][j][c].  Every point of
-// the tile enters (the chunk weights are zero outside a stencil), so no half masks
-// are tested.  The weights of the next round are loaded while the current round
-// is contracted (two staging buffers), and the tile's values are loaded while the
-// first round's list entries and weights are.  In FP32 each thread holds its
-// (c, x) block of the tile (64 values) in registers for the whole tile, so the
-// contraction reads only the weights (broadcast) from shared memory, and the
-// z-contraction and the y-sum run on the packed two-lane FMA over y-pairs; FP64
-// reads the block from shared memory.
-constexpr int IG_B = 16;          // blobs per round
-constexpr int IG_T = 96;          // threads: 4 groups x 3 components x 8 x
-constexpr int IG_P = TE * TE + 4; // padded (c, x) block of su
-
-// Staging of one round: threads i < 64 take (d, k) = (i / 16, i % 16): the x-, y-
-// or z-weight chunk (d < 3) or the list entry (d = 3) of the round's blob k.
+// Tiled interpolation by one warp per 8x8x8 tile: lane (yq, z) = (lane / 8,
+// lane % 8) holds the x-columns of rows y = yq and yq + 4 (one in each y-half),
+// three components, in registers.  Per blob it contracts each row the stencil
+// meets with the blob's x-weights (FP32: the packed FMA over x-pairs), scales by
+// wy wz and adds the two rows, so each lane carries three values per blob; the
+// warp reduces four blobs at a time with the 16-value shuffle reduce-scatter and
+// lanes 2i write value i straight to partial[blob][j][c].  Against the 64-thread
+// kernel this halves the reductions per (blob, tile) pair and needs no CTA
+// barrier or shared-memory sum: only the staged weights pass through shared memory.
 template <typename T>
-struct IgStage {
-  T w[TE];
-  unsigned long long e;
-  __device__ __forceinline__ void load(const unsigned long long* __restrict__ list, const T* __restrict__ wc,
-                                       int c0, int nc, const TileGeom& g) {
-    const int i = threadIdx.x, k = i & 15, d = i >> 4;
-    e = 0ull;
-    if (i >= 64 || k >= nc) return;
-    e = list_entry(list, c0 + k, g);
-    if (d == 3) return;
-    const unsigned b = (unsigned)(e >> 32), lo = (unsigned)e;
-    const T* src = wc + ((size_t)(3 * b + d) * NCH + ((lo >> (2 * d)) & 3u)) * TE;
-    if constexpr (sizeof(T) == 4) {
-      const float4 a = __ldg(reinterpret_cast<const float4*>(src));
-      const float4 c = __ldg(reinterpret_cast<const float4*>(src) + 1);
-      w[0] = a.x, w[1] = a.y, w[2] = a.z, w[3] = a.w, w[4] = c.x, w[5] = c.y, w[6] = c.z, w[7] = c.w;
-    } else {
-#pragma unroll
-      for (int q = 0; q < TE / 2; ++q) {
-        const double2 a = __ldg(reinterpret_cast<const double2*>(src) + q);
-        w[2 * q] = a.x;
-        w[2 * q + 1] = a.y;
-      }
-    }
-  }
-};
-
-template <typename T>
-__global__ void __launch_bounds__(IG_T) k_interp_gemm(const T* __restrict__ wc, const T* __restrict__ grid,
-                                                      TileGeom g, const int* __restrict__ offset,
-                                                      const unsigned long long* __restrict__ list, long long G,
-                                                      T* __restrict__ partial) {
-  constexpr int ZD = sizeof(T) == 4 ? 2 : 1;        // z-weights held twice in FP32 (packed-FMA operands)
-  __shared__ __align__(16) T su[3 * TE * IG_P];
-  __shared__ __align__(16) T swz[2][IG_B / 4][TE][4 * ZD];  // [buffer][group][z][blob of the group]
-  __shared__ __align__(16) T swx[2][IG_B / 4][TE][4];       // [buffer][group][x][blob of the group]
-  __shared__ __align__(16) T swy[2][IG_B][TE];              // [buffer][blob][y]
-  __shared__ __align__(16) T sred[IG_B][3][TE];             // [blob][c][x]
-  __shared__ unsigned sflag[2][IG_B], sblob[2][IG_B];
+__global__ void __launch_bounds__(32) k_interp_warp(const T* __restrict__ wc, const T* __restrict__ grid,
+                                                    TileGeom g, const int* __restrict__ offset,
+                                                    const unsigned long long* __restrict__ list, long long G,
+                                                    T* __restrict__ partial) {
+  __shared__ __align__(16) T sw[SCB][3][TE];
+  __shared__ unsigned sflag[SCB], sblob[SCB];
   const int tile = blockIdx.x;
-  if (!FCM_INB(tile, (long long)g.ntx * g.nty * g.ntz, BS_TILE)) return;  // uniform over the CTA
+  if (!FCM_INB(tile, (long long)g.ntx * g.nty * g.ntz, BS_TILE)) return;  // uniform over the warp
   int b0, b1;
   tile_range(offset, tile, g, b0, b1);
-  if (b0 == b1) return;  // no blob meets this tile (uniform over the CTA)
+  if (b0 == b1) return;  // no blob meets this tile
   const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
-  const int t = threadIdx.x;
-  // the staged weights of one round into buffer `buf` (zeros for empty slots)
-  auto stage_store = [&](const IgStage<T>& st, int nc, int buf) {
-    if (t >= 64) return;
-    const int k = t & 15, d = t >> 4, kg = k >> 2, kj = k & 3;
-    const bool live = k < nc;
-    if (d == 3) {
-      if (live) {
-        sflag[buf][k] = (unsigned)st.e;
-        sblob[buf][k] = (unsigned)(st.e >> 32);
-      }
-      return;
-    }
+  const int lane = threadIdx.x, z = lane & 7, yq = lane >> 3;
+  XColumn<T> col[2];
 #pragma unroll
-    for (int q = 0; q < TE; ++q) {
-      const T w = live ? st.w[q] : (T)0;
-      if (d == 0) {
-        swx[buf][kg][q][kj] = w;
-      } else if (d == 1) {
-        swy[buf][k][q] = w;
+  for (int r = 0; r < 2; ++r) {
+    const int ox = tx * TE, oy = ty * TE + yq + 4 * r, oz = tz * TE + z;
+    const bool live = oy < g.ycut;  // rows at or above the slip channel's upper wall read as 0
+#pragma unroll
+    for (int x = 0; x < TE; ++x) {
+      const long long idx = ((long long)(ox + x) * g.ny + oy) * g.nz + oz;
+      const bool in = live && FCM_INB(idx, G, BS_GRID);
+      col[r].set(x, in ? grid[idx] : (T)0, in ? grid[G + idx] : (T)0, in ? grid[2 * G + idx] : (T)0);
+    }
+  }
+  for (int c0 = b0; c0 < b1; c0 += SCB) {
+    const int nc = min(SCB, b1 - c0);
+    if (c0 != b0) __syncwarp();
+    for (int i = lane; i < 4 * nc; i += 32) {  // staging: lane d of blob k
+      const int k = i >> 2, d = i & 3;
+      const unsigned long long e = list_entry(list, c0 + k, g);
+      const unsigned b = (unsigned)(e >> 32), lo = (unsigned)e;
+      if (d < 3) {
+        copy8(sw[k][d], wc + ((size_t)(3 * b + d) * NCH + ((lo >> (2 * d)) & 3u)) * TE);
       } else {
-#pragma unroll
-        for (int r = 0; r < ZD; ++r) swz[buf][kg][q][ZD * kj + r] = w;
+        sflag[k] = lo;
+        sblob[k] = b;
       }
     }
-  };
-  // prologue: the tile's two rows per thread (row r = (c, x, y), eight z) and the
-  // first round's weights are loaded together, then stored
-  T rv[2][TE];
+    __syncwarp();
+    for (int k0 = 0; k0 < nc; k0 += 4) {
+      T v[16];
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int r = t + h * IG_T, y = r & 7, cx = r >> 3, c = cx >> 3, x = cx & 7;
-    const int oy = ty * TE + y;
-    const long long idx = ((long long)(tx * TE + x) * g.ny + oy) * g.nz + tz * TE;
-    const bool live = oy < g.ycut && FCM_INB(idx + TE - 1, G, BS_GRID);
-    if constexpr (sizeof(T) == 4) {
-      const float4* src = reinterpret_cast<const float4*>(grid + c * G + idx);
-      const float4 a = live ? __ldg(src) : make_float4(0.f, 0.f, 0.f, 0.f);
-      const float4 b = live ? __ldg(src + 1) : make_float4(0.f, 0.f, 0.f, 0.f);
-      rv[h][0] = a.x, rv[h][1] = a.y, rv[h][2] = a.z, rv[h][3] = a.w;
-      rv[h][4] = b.x, rv[h][5] = b.y, rv[h][6] = b.z, rv[h][7] = b.w;
-    } else {
-      const double2* src = reinterpret_cast<const double2*>(grid + c * G + idx);
+      for (int j = 0; j < 4; ++j) {
+        const int k = k0 + j;
+        const unsigned fl = k < nc ? sflag[k] : 0u;
+        T p0 = 0, p1 = 0, p2 = 0;
 #pragma unroll
-      for (int q = 0; q < TE / 2; ++q) {
-        const double2 a = live ? __ldg(src + q) : make_double2(0.0, 0.0);
-        rv[h][2 * q] = a.x;
-        rv[h][2 * q + 1] = a.y;
+        for (int r = 0; r < 2; ++r) {
+          if (!((fl >> (EYM + r)) & 1u)) continue;  // uniform over the warp
+          T s0, s1, s2;
+          col[r].contract(sw[k][0], fl, s0, s1, s2);
+          const T wyz = sw[k][1][yq + 4 * r] * sw[k][2][z];
+          p0 += s0 * wyz;
+          p1 += s1 * wyz;
+          p2 += s2 * wyz;
+        }
+        v[4 * j] = p0;
+        v[4 * j + 1] = p1;
+        v[4 * j + 2] = p2;
+        v[4 * j + 3] = 0;
       }
-    }
-  }
-  IgStage<T> st;
-  st.load(list, wc, b0, min(IG_B, b1 - b0), g);
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int r = t + h * IG_T, y = r & 7, cx = r >> 3;
-#pragma unroll
-    for (int z = 0; z < TE; ++z) su[cx * IG_P + z * TE + y] = rv[h][z];
-  }
-  stage_store(st, min(IG_B, b1 - b0), 0);
-  __syncthreads();
-  const int grp = t / 24, p = t % 24, c = p >> 3, x = p & 7;
-  // FP32: the thread's (c, x) block of the tile, u[z][y] as y-pairs, in registers
-  // for the whole tile (the contraction then reads only weights from shared memory)
-  float2 ur[TE][TE / 2];
-  if constexpr (sizeof(T) == 4) {
-    const T* col = su + p * IG_P;
-#pragma unroll
-    for (int z = 0; z < TE; ++z) {
-      const float4 ua = *reinterpret_cast<const float4*>(col + z * TE);
-      const float4 ub = *reinterpret_cast<const float4*>(col + z * TE + 4);
-      ur[z][0] = make_float2(ua.x, ua.y);
-      ur[z][1] = make_float2(ua.z, ua.w);
-      ur[z][2] = make_float2(ub.x, ub.y);
-      ur[z][3] = make_float2(ub.z, ub.w);
-    }
-  }
-  int buf = 0;
-  for (int c0 = b0; c0 < b1; c0 += IG_B, buf ^= 1) {
-    const int nc = min(IG_B, b1 - c0);
-    const bool more = c0 + IG_B < b1;
-    const int ncn = more ? min(IG_B, b1 - c0 - IG_B) : 0;
-    if (more) st.load(list, wc, c0 + IG_B, ncn, g);  // the next round's weights, in flight meanwhile
-    if (4 * grp < nc) {
-      if constexpr (sizeof(T) == 4) {
-        float2 acc[4][TE / 2];
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-          for (int i = 0; i < TE / 2; ++i) acc[j][i] = make_float2(0.f, 0.f);
-#pragma unroll
-        for (int z = 0; z < TE; ++z) {
-          const float4 wa = *reinterpret_cast<const float4*>(&swz[buf][grp][z][0]);
-          const float4 wb = *reinterpret_cast<const float4*>(&swz[buf][grp][z][4]);
-          const float2 w2[4] = {make_float2(wa.x, wa.y), make_float2(wa.z, wa.w), make_float2(wb.x, wb.y),
-                                make_float2(wb.z, wb.w)};
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int i = 0; i < 4; ++i) acc[j][i] = __ffma2_rn(w2[j], ur[z][i], acc[j][i]);
-        }
-        const float4 wx4 = *reinterpret_cast<const float4*>(&swx[buf][grp][x][0]);
-        const float wxj[4] = {wx4.x, wx4.y, wx4.z, wx4.w};
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int k = 4 * grp + j;
-          const float4 ya = *reinterpret_cast<const float4*>(&swy[buf][k][0]);
-          const float4 yb = *reinterpret_cast<const float4*>(&swy[buf][k][4]);
-          float2 s2 = make_float2(0.f, 0.f);
-          s2 = __ffma2_rn(make_float2(ya.x, ya.y), acc[j][0], s2);
-          s2 = __ffma2_rn(make_float2(ya.z, ya.w), acc[j][1], s2);
-          s2 = __ffma2_rn(make_float2(yb.x, yb.y), acc[j][2], s2);
-          s2 = __ffma2_rn(make_float2(yb.z, yb.w), acc[j][3], s2);
-          sred[k][c][x] = (s2.x + s2.y) * wxj[j];
-        }
-      } else {
-        const T* col = su + p * IG_P;
-        T acc[4][TE];
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-          for (int y = 0; y < TE; ++y) acc[j][y] = 0;
-#pragma unroll
-        for (int z = 0; z < TE; ++z) {
-          T u[TE];
-#pragma unroll
-          for (int y = 0; y < TE; y += 2) {
-            const double2 a = *reinterpret_cast<const double2*>(col + z * TE + y);
-            u[y] = a.x;
-            u[y + 1] = a.y;
-          }
-          const double2 wa = *reinterpret_cast<const double2*>(&swz[buf][grp][z][0]);
-          const double2 wb = *reinterpret_cast<const double2*>(&swz[buf][grp][z][2]);
-          const T wj[4] = {wa.x, wa.y, wb.x, wb.y};
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int y = 0; y < TE; ++y) acc[j][y] += wj[j] * u[y];
-        }
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int k = 4 * grp + j;
-          T sy = 0;
-#pragma unroll
-          for (int y = 0; y < TE; ++y) sy += swy[buf][k][y] * acc[j][y];
-          sred[k][c][x] = sy * swx[buf][grp][x][j];
+      const T sum = warp_reduce_scatter16<T>(v, lane);
+      if (!(lane & 1)) {  // lanes 2i and 2i + 1 hold value i = 4 j + c
+        const int i = lane >> 1, j = i >> 2, cc = i & 3, k = k0 + j;
+        if (cc < 3 && k < nc) {
+          const unsigned jt = (sflag[k] >> EJ) & 63u;
+          if (FCM_INB((long long)sblob[k] * 64 + jt, (long long)g.nblobs * 64, BS_PARTIAL))
+            partial[((size_t)sblob[k] * 64 + jt) * 3 + cc] = sum;
         }
       }
     }
-    if (more) stage_store(st, ncn, buf ^ 1);
-    __syncthreads();
-    for (int i = t; i < 3 * nc; i += IG_T) {
-      const int k = i / 3, cc = i - 3 * k;
-      T sum = 0;
-#pragma unroll
-      for (int xx = 0; xx < TE; ++xx) sum += sred[k][cc][xx];
-      const unsigned jt = (sflag[buf][k] >> EJ) & 63u;
-      if (FCM_INB((long long)sblob[buf][k] * 64 + jt, (long long)g.nblobs * 64, BS_PARTIAL))
-        partial[((size_t)sblob[buf][k] * 64 + jt) * 3 + cc] = sum;
-    }
-    __syncthreads();
   }
 }
 
@@ -1575,7 +1427,7 @@ int launch_interp(const Ctx& c, const BlobTable<T>& t, const T* grid, double* dV
     if (v == 2)
       k_interp_rows<T, 2><<<t.ntiles, 32, 0, s>>>(t.wc, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial);
     else if (v == 1)
-      k_interp_gemm<T><<<t.ntiles, IG_T, 0, s>>>(t.wc, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial);
+      k_interp_warp<T><<<t.ntiles, 32, 0, s>>>(t.wc, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial);
     else
       k_interp_tiled<T><<<t.ntiles, 64, 0, s>>>(t.wc, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial);
     FCM_LAUNCH_CHECK();

@@ -701,9 +701,18 @@ __device__ __forceinline__ void xfft_interior_cta(C* __restrict__ spec, const KP
 // Threads per CTA: 256 (an FP32 CTA sized to one pencil DFT per thread and step,
 // 384 threads at 256 points, measured slower); 128 for the FP64 interior CTAs,
 // whose register-resident pencils take about 150 registers.
+// FP32 interior CTAs of the 512-point transform: kz per CTA and threads (8 and 256:
+// two CTAs per SM; 4 and 128 give four smaller CTAs per SM).
+#ifndef FCM_XFFT512_TK
+#define FCM_XFFT512_TK 8
+#endif
+#ifndef FCM_XFFT512_THREADS
+#define FCM_XFFT512_THREADS 256
+#endif
+
 template <typename T, int N1, int N2, int TK, bool PLANES>
 constexpr int xfft_block() {
-  return (sizeof(T) == 8 && !PLANES) ? 128 : 256;
+  return (sizeof(T) == 8 && !PLANES) ? 128 : (!PLANES && N1 * N2 == 512) ? FCM_XFFT512_THREADS : 256;
 }
 
 // CTAs per SM the register allocation must allow: three for the FP32 transforms up
@@ -711,7 +720,7 @@ constexpr int xfft_block() {
 // registers.
 template <typename T, int N, int BLOCK, bool PLANES>
 constexpr int xfft_min_blocks() {
-  return sizeof(T) == 4 ? (N <= 256 ? 3 : 2) : (N <= 256 ? 2 : 1);
+  return sizeof(T) == 4 ? (N <= 256 ? 3 : (BLOCK == 128 ? 4 : 2)) : (N <= 256 ? 2 : 1);
 }
 
 template <typename T, typename C, int N1, int N2, int TK, bool PLANES>
@@ -1142,7 +1151,7 @@ namespace {
 // points: 4 kz (98 KB at 512); the autotuner weighs it against the 3D transforms.
 template <typename T>
 constexpr int xfft_tk(int n) {
-  return sizeof(T) == 4 ? (n <= 256 ? 16 : 8) : (n <= 256 ? 8 : 4);
+  return sizeof(T) == 4 ? (n <= 256 ? 16 : n == 512 ? FCM_XFFT512_TK : 8) : (n <= 256 ? 8 : 4);
 }
 
 // Row pairs per plane CTA: one (ny/2 + 1 CTAs per plane; four pairs per CTA left

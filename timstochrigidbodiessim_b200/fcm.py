@@ -329,8 +329,9 @@ class Suspension:
     # interp, FP32 interp]; spread 0 = persistent pipelined, 1 / 2 / 3 = one CTA
     # per tile staging 16 / 8 / 32 blobs per round, 4 = contraction order (FP32);
     # solve 0 = cuFFT 3D, 1 = cuFFT (y, z) + fused x-transform, 2 = the library's
-    # (y, z) + fused x; interp 0 = shuffle reduction, 1 = contraction order (z
-    # as a register GEMM, then y, x), 2 = shared-memory reduction, 32 threads
+    # (y, z) + fused x; interp 0 = shuffle reduction, 64 threads per tile, 1 =
+    # one warp per tile (two y-rows per lane) with the shuffle reduction, 2 = one
+    # warp per tile with a shared-memory reduction
     NUM_VARIANTS = 6
     NUM_TUNE_TIMES = 24
 
