@@ -149,7 +149,7 @@ class ClockSampler:
 # ----------------------------------------------------------------- ours
 VARIANT_LEGEND = ("variants [FP64 spread, FP64 solve, FP32 spread, FP32 solve, FP64 interp, FP32 interp]: spread "
                   "0 persistent pipelined, 1 / 2 / 3 one CTA per tile staging 16 / 8 / 32 blobs per round, 4 "
-                  "contraction order (FP32); solve 0 cuFFT 3D + projection, 1 cuFFT (y, z) + fused x-transform, "
+                  "one warp per tile (two y-rows per lane); solve 0 cuFFT 3D + projection, 1 cuFFT (y, z) + fused x-transform, "
                   "2 library (y, z) + fused x-transform; interp 0 shuffle reduction with 64 threads per tile, 1 "
                   "one warp per tile (two y-rows per lane) with the shuffle reduction, 2 one warp per tile with "
                   "a shared-memory reduction.  us[12P + v]: "

@@ -299,11 +299,9 @@ int fcm_interp(fcm_ctx* ctx, int32_t precision, double* V);
  * variants[FCM_NUM_VARIANTS]:
  *   [0] FP64 spread, [2] FP32 spread: 0 = the persistent software-pipelined tile
  *       kernel, 1 / 2 / 3 = one CTA per 8^3 tile staging 16 / 8 / 32 blobs per
- *       round; these sum every grid point's blobs in the same order, so the grids
- *       are the same bit for bit.  4 (FP32 only) = 96 threads per tile in
- *       contraction order (each thread's 8 x 8 points of one (component, x) in
- *       registers, a quarter of the blobs each, the quarters added at the end):
- *       the same grid within rounding.
+ *       round, 4 = one warp per tile staging 16 blobs per round, two y-rows per
+ *       lane.  All sum every grid point's blobs in the same order with the same
+ *       products, so the grids are the same bit for bit.
  *   [1] FP64 Stokes solve, [3] FP32 Stokes solve: 0 = cuFFT 3D transforms and the
  *       projection kernel, 1 = cuFFT (y, z) transforms around the fused x-transform
  *       + projection kernel, 2 = the library's own (y, z) transforms around it
@@ -329,7 +327,7 @@ int fcm_set_variants(fcm_ctx* ctx, const int32_t* variants);
  * FCM_NUM_TUNE_TIMES doubles, [12 P + v] for precision P (0 FP64, 1 FP32): v = 0..4
  * the spread variants, v = 5, 6, 7 the solve variants 0, 1, 2, v = 8, 9, 10 the
  * interpolation variants 0, 1, 2, in microseconds per call, -1 where not
- * available (v = 11 is always -1); variants (may be NULL) receives the choice as fcm_get_variants does.
+ * available (v = 11 always); variants (may be NULL) receives the choice as fcm_get_variants does.
  * Needs set_up_gaussians first; overwrites the grid work arrays, so call it
  * between steps. */
 #define FCM_NUM_TUNE_TIMES 24

@@ -1,8 +1,8 @@
 """Kernel variants of the grid stages and their autotuner (no reference
 counterpart).  The four spread kernels (persistent pipelined; one CTA per tile
 staging 16, 8 or 32 blobs per round) sum every grid point's blobs in the same
-order, so M F is the same bit for bit whichever runs; the FP32 contraction-order
-spread (variant 4) agrees with them within rounding; the Stokes-solve variants
+order with the same products, and so does the one-warp-per-tile spread (variant
+4), so M F is the same bit for bit whichever runs; the Stokes-solve variants
 (cuFFT 3D + projection, cuFFT (y, z) + fused x-transform, the library's (y, z)
 kernels + fused x-transform) and the three interpolation kernels (64 threads per
 tile with the shuffle reduction; one warp per tile, two y-rows per lane, with the
@@ -50,7 +50,7 @@ def test_variants_agree(gpu):
     for prec in (0, 1):
         for sv in ((0, 1) if prec == 0 else (0, 1, 2)):
             out = []
-            for sp in (0, 1, 2, 3):
+            for sp in (0, 1, 2, 3, 4):
                 v = g.get_variants()
                 v[2 * prec], v[2 * prec + 1] = sp, sv
                 g.set_variants(v)
@@ -58,12 +58,6 @@ def test_variants_agree(gpu):
             for o_ in out[1:]:
                 assert np.array_equal(out[0], o_), (prec, sv)
             assert rel_err(out[0], Vo) < TOL[prec], (prec, sv)
-            if prec == 1:  # the contraction-order spread: same grid within rounding
-                v = g.get_variants()
-                v[2], v[3] = 4, sv
-                g.set_variants(v)
-                o4 = _mf(g, F, 1)
-                assert rel_err(o4, out[0]) < TOL[1] and rel_err(o4, Vo) < TOL[1], sv
         for iv in (0, 1, 2):
             v = g.get_variants()
             v[4 + prec] = iv
@@ -75,13 +69,12 @@ def test_variants_agree(gpu):
 def test_autotune_keeps_the_fastest(gpu):
     g, Vo, F = _setup()
     v, us = g.autotune(reps=3)
-    assert np.all(us[0:4] > 0) and us[4] == -1  # no contraction-order spread in FP64
-    assert np.all(us[5:7] > 0) and us[7] == -1  # FP64 has no library (y, z) variant
+    assert np.all(us[0:7] > 0) and us[7] == -1  # FP64 has no library (y, z) variant
     assert np.all(us[8:11] > 0) and us[11] == -1
     assert np.all(us[12:23] > 0) and us[23] == -1
     for P in (0, 1):
         t = us[12 * P:12 * P + 12]
-        spread, solve, interp = t[0:(5 if P else 4)], t[5:8], t[8:11]
+        spread, solve, interp = t[0:5], t[5:8], t[8:11]
         assert v[2 * P] == int(np.argmin(spread))
         best = min((x, i) for i, x in enumerate(solve) if x >= 0)[1]
         assert v[2 * P + 1] == best
@@ -96,7 +89,7 @@ def test_variants_refused_where_the_grid_does_not_allow_them(gpu):
     with pytest.raises(FcmError):
         g.set_variants([0, 2, 1, 2, 0, 0])  # no library (y, z) variant in FP64
     with pytest.raises(FcmError):
-        g.set_variants([4, 1, 1, 2, 0, 0])  # out of range (contraction-order spread is FP32 only)
+        g.set_variants([5, 1, 1, 2, 0, 0])  # out of range
     with pytest.raises(FcmError):
         g.set_variants([0, 1, 5, 2, 0, 0])  # out of range
     with pytest.raises(FcmError):
@@ -109,7 +102,7 @@ def test_variants_refused_where_the_grid_does_not_allow_them(gpu):
         h.set_variants([0, 1, 1, 0, 0, 0])
     v, us = h.autotune(reps=2)
     assert us[6] == -1 and us[18] == -1 and us[19] == -1
-    assert np.all(us[0:5] == -1) and np.all(us[8:11] == -1) and np.all(us[12:17] == -1) and np.all(us[20:23] == -1)
+    assert np.all(us[0:5] == -1) and np.all(us[8:12] == -1) and np.all(us[12:17] == -1) and np.all(us[20:24] == -1)
     assert v[1] == 0 and v[3] == 0
     for prec in (0, 1):
         assert rel_err(_mf(h, F, prec), Vo) < TOL[prec], prec

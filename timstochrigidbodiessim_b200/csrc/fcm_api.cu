@@ -2528,7 +2528,7 @@ static void get_variants(const Ctx* c, int32_t* v) {
 static int set_variants(Ctx* c, const int32_t* v) {
   for (int P = 0; P < 2; ++P) {
     const int sp = v[2 * P], sv = v[2 * P + 1], iv = v[4 + P];
-    if (sp < 0 || sp > (P == 1 ? 4 : 3) || sv < 0 || sv > (P == 1 ? 2 : 1) || iv < 0 || iv > 2) {
+    if (sp < 0 || sp > 4 || sv < 0 || sv > (P == 1 ? 2 : 1) || iv < 0 || iv > 2) {
       set_error("kernel variant out of range");
       return FCM_ERR_INVALID;
     }
@@ -2576,22 +2576,21 @@ static int time_calls(Ctx* c, int reps, F&& body, double* out) {
 }
 
 // The spread, solve and interpolation variants of one precision timed on c's own
-// grid and blob table; the fastest kept.  t[0..4] spread (4: FP32 only), t[5..7]
-// solve, t[8..10] interpolation (-1: not available).
+// grid and blob table; the fastest kept.  t[0..4] spread, t[5..7] solve, t[8..10]
+// interpolation (-1: not available).
 template <typename T>
 static int tune_precision(Ctx* c, int reps, double* t) {
   constexpr int P = sizeof(T) == 8 ? 0 : 1;
   GridBufs<T>& gb = grid_of<T>(c);
   const BlobTable<T>& bt = gb.blobs;
   FCM_CUDA(cudaMemsetAsync(c->d_tmp3, 0, sizeof(double) * 3 * (size_t)(c->Nb > 0 ? c->Nb : 1), c->stream));
-  constexpr int NSP = P == 1 ? 5 : 4;  // spread variants of this precision
   if (bt.tiled) {
-    for (int v = 0; v < NSP; ++v) {
+    for (int v = 0; v < 5; ++v) {
       c->spread_variant[P] = v;
       FCM_TRY(time_calls(c, reps, [&] { return spread_t<T>(c, bt, c->d_tmp3); }, &t[v]));
     }
     int bs = 0;
-    for (int v = 1; v < NSP; ++v)
+    for (int v = 1; v < 5; ++v)
       if (t[v] < t[bs]) bs = v;
     c->spread_variant[P] = bs;
   }

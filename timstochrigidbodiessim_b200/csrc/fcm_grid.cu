@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <mutex>
 #include <string>
+#include <type_traits>
 
 #include "fcm_internal.cuh"
 
@@ -425,145 +426,107 @@ __global__ void __launch_bounds__(64) k_spread_tiled(const T* __restrict__ wc, c
   spread_tile<T, NB>(wc, F, g, offset, list, G, grid, blockIdx.x);
 }
 
-// ------------------------------------------------------------------ spreading in contraction order
-// FP32 only: one CTA (96 threads) per 8x8x8 tile.  Thread t = (quarter q, c, x) =
-// (t / 24, (t % 24) / 8, t % 8) holds the 8 x 8 (y, z) points of its (c, x) row
-// block in registers and, for the blobs q, q + 4, ... of each staged round of 16,
-// adds g_y * wz[z] with g_y = F_c wx[x] wy[y] (the packed two-lane FMA over
-// z-pairs: 32 per blob and thread, against two shared loads of broadcast weights).
-// The staged weights are F_c wx[x] (24 per blob), wy twice over (the packed
-// operand) and wz; the next round's are loaded while the current round is added.
-// At the end the four quarters' blocks are added in quarter order through shared
-// memory and every point of the tile is written once (zero where no blob meets
-// it).  The sums run in another order than k_spread_tiled's (blob quarters,
-// F wx wy wz products), so the grid agrees with theirs within rounding, not bit
-// for bit.
-constexpr int SG_B = 16;           // blobs per round
-constexpr int SG_T = 96;           // threads: 4 blob quarters x 3 components x 8 x
-constexpr int SG_P = TE * TE + 4;  // padded (c, x) block of the quarter sums
-
-struct SgStage {
-  float w[TE];
-  double f[3];
-  unsigned long long e;
-  // thread i < 48: (d, k) = (i / 16, i % 16), chunk d of the round's blob k (d = 0
-  // also fetches the blob's force)
-  __device__ __forceinline__ void load(const unsigned long long* __restrict__ list, const float* __restrict__ wc,
-                                       const double* __restrict__ F, int c0, int nc, const TileGeom& g) {
-    const int i = threadIdx.x, k = i & 15, d = i >> 4;
-    e = 0ull;
-    if (i >= 48 || k >= nc) return;
-    e = list_entry(list, c0 + k, g);
-    const unsigned b = (unsigned)(e >> 32), lo = (unsigned)e;
-    const float* src = wc + ((size_t)(3 * b + d) * NCH + ((lo >> (2 * d)) & 3u)) * TE;
-    const float4 a = __ldg(reinterpret_cast<const float4*>(src));
-    const float4 c = __ldg(reinterpret_cast<const float4*>(src) + 1);
-    w[0] = a.x, w[1] = a.y, w[2] = a.z, w[3] = a.w, w[4] = c.x, w[5] = c.y, w[6] = c.z, w[7] = c.w;
-    if (d == 0) {
-      f[0] = F[3 * (size_t)b];
-      f[1] = F[3 * (size_t)b + 1];
-      f[2] = F[3 * (size_t)b + 2];
-    }
-  }
-};
-
-__global__ void __launch_bounds__(SG_T) k_spread_gemm(const float* __restrict__ wc, const double* __restrict__ F,
-                                                      TileGeom g, const int* __restrict__ offset,
-                                                      const unsigned long long* __restrict__ list, long long G,
-                                                      float* __restrict__ grid) {
-  __shared__ __align__(16) float sfx[2][SG_B][3 * TE];  // [buffer][blob][c * 8 + x]: F_c wx[x]
-  __shared__ __align__(16) float swy[2][SG_B][2 * TE];  // [buffer][blob][2 y + r]: wy[y] twice
-  __shared__ __align__(16) float swz[2][SG_B][TE];      // [buffer][blob][z]
-  __shared__ __align__(16) float sacc[4][3 * TE * SG_P];
+// Tiled spreading by one warp per 8x8x8 tile: lane (yq, z) = (lane / 8, lane % 8)
+// owns the x-columns of rows y = yq and yq + 4 (eight points each, three
+// components, in registers) and adds each staged blob to the rows its stencil
+// meets (FP32: the packed FMA over x-pairs).  The flag, x-weights and force of a
+// blob are read once for both rows.  Every point sums its blobs in ascending order
+// with the products of k_spread_tiled (f_c = F_c wy wz, then f_c wx), so the grid
+// is the same bit for bit.
+template <typename T>
+__global__ void __launch_bounds__(32) k_spread_warp(const T* __restrict__ wc, const double* __restrict__ F,
+                                                    TileGeom g, const int* __restrict__ offset,
+                                                    const unsigned long long* __restrict__ list, long long G,
+                                                    T* __restrict__ grid) {
+  __shared__ __align__(16) T sw[SCB][3][TE];
+  __shared__ __align__(16) T sF[SCB][4];
+  __shared__ unsigned sflag[SCB];
   const int tile = blockIdx.x;
-  if (!FCM_INB(tile, (long long)g.ntx * g.nty * g.ntz, BS_TILE)) return;  // uniform over the CTA
+  if (!FCM_INB(tile, (long long)g.ntx * g.nty * g.ntz, BS_TILE)) return;  // uniform over the warp
   int b0, b1;
   tile_range(offset, tile, g, b0, b1);
   const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
-  const int t = threadIdx.x;
-  const int q = t / 24, p = t % 24, c = p >> 3, x = p & 7;
-  auto stage_store = [&](const SgStage& st, int nc, int buf) {
-    if (t >= 48) return;
-    const int k = t & 15, d = t >> 4;
-    if (k >= nc) return;
-    if (d == 0) {
+  const int lane = threadIdx.x, z = lane & 7, yq = lane >> 3;
+  constexpr int XA = sizeof(T) == 4 ? TE / 2 : TE;  // x accumulators per row (pairs in FP32)
+  using A = typename std::conditional<sizeof(T) == 4, float2, T>::type;
+  A acc[2][XA][3];
 #pragma unroll
-      for (int cc = 0; cc < 3; ++cc)
+  for (int r = 0; r < 2; ++r)
 #pragma unroll
-        for (int xx = 0; xx < TE; ++xx) sfx[buf][k][cc * TE + xx] = (float)st.f[cc] * st.w[xx];
-    } else if (d == 1) {
+    for (int x = 0; x < XA; ++x)
 #pragma unroll
-      for (int y = 0; y < TE; ++y) {
-        swy[buf][k][2 * y] = st.w[y];
-        swy[buf][k][2 * y + 1] = st.w[y];
+      for (int c = 0; c < 3; ++c) {
+        if constexpr (sizeof(T) == 4) acc[r][x][c] = make_float2(0.f, 0.f);
+        else acc[r][x][c] = 0;
       }
-    } else {
-#pragma unroll
-      for (int z = 0; z < TE; ++z) swz[buf][k][z] = st.w[z];
+  for (int c0 = b0; c0 < b1; c0 += SCB) {
+    const int nc = min(SCB, b1 - c0);
+    if (c0 != b0) __syncwarp();
+    for (int i = lane; i < 4 * nc; i += 32) {  // staging: lane d of blob k
+      const int k = i >> 2, d = i & 3;
+      const unsigned long long e = list_entry(list, c0 + k, g);
+      const unsigned b = (unsigned)(e >> 32), lo = (unsigned)e;
+      if (d < 3) {
+        copy8(sw[k][d], wc + ((size_t)(3 * b + d) * NCH + ((lo >> (2 * d)) & 3u)) * TE);
+      } else {
+        sflag[k] = lo;
+        sF[k][0] = (T)F[3 * (size_t)b];
+        sF[k][1] = (T)F[3 * (size_t)b + 1];
+        sF[k][2] = (T)F[3 * (size_t)b + 2];
+      }
     }
-  };
-  float2 acc[TE][TE / 2];  // [y][z pair]
+    __syncwarp();
+    for (int k = 0; k < nc; ++k) {
+      const unsigned fl = sflag[k];
 #pragma unroll
-  for (int y = 0; y < TE; ++y)
+      for (int r = 0; r < 2; ++r) {
+        if (!((fl >> (EYM + r)) & 1u)) continue;  // uniform over the warp
+        const T wyz = sw[k][1][yq + 4 * r] * sw[k][2][z];
+        const T f0 = sF[k][0] * wyz, f1 = sF[k][1] * wyz, f2 = sF[k][2] * wyz;
+        if constexpr (sizeof(T) == 4) {
+          const float2 fc[3] = {make_float2(f0, f0), make_float2(f1, f1), make_float2(f2, f2)};
 #pragma unroll
-    for (int i = 0; i < TE / 2; ++i) acc[y][i] = make_float2(0.f, 0.f);
-  if (b0 < b1) {
-    SgStage st;
-    st.load(list, wc, F, b0, min(SG_B, b1 - b0), g);
-    stage_store(st, min(SG_B, b1 - b0), 0);
-    __syncthreads();
-    int buf = 0;
-    for (int c0 = b0; c0 < b1; c0 += SG_B, buf ^= 1) {
-      const int nc = min(SG_B, b1 - c0);
-      const bool more = c0 + SG_B < b1;
-      const int ncn = more ? min(SG_B, b1 - c0 - SG_B) : 0;
-      if (more) st.load(list, wc, F, c0 + SG_B, ncn, g);  // the next round's weights, in flight meanwhile
-      for (int k = q; k < nc; k += 4) {
-        const float fx = sfx[buf][k][p];
-        const float2 fx2 = make_float2(fx, fx);
-        const float4 za = *reinterpret_cast<const float4*>(&swz[buf][k][0]);
-        const float4 zb = *reinterpret_cast<const float4*>(&swz[buf][k][4]);
-        const float2 wz2[4] = {make_float2(za.x, za.y), make_float2(za.z, za.w), make_float2(zb.x, zb.y),
-                               make_float2(zb.z, zb.w)};
+          for (int h = 0; h < 2; ++h) {
+            const float4 v = *reinterpret_cast<const float4*>(&sw[k][0][4 * h]);
+            const float2 wa = make_float2(v.x, v.y), wb = make_float2(v.z, v.w);
 #pragma unroll
-        for (int y = 0; y < TE; y += 2) {
-          const float4 wy4 = *reinterpret_cast<const float4*>(&swy[buf][k][2 * y]);
-          const float2 g0 = __ffma2_rn(fx2, make_float2(wy4.x, wy4.y), make_float2(0.f, 0.f));
-          const float2 g1 = __ffma2_rn(fx2, make_float2(wy4.z, wy4.w), make_float2(0.f, 0.f));
+            for (int c = 0; c < 3; ++c) {
+              acc[r][2 * h][c] = __ffma2_rn(fc[c], wa, acc[r][2 * h][c]);
+              acc[r][2 * h + 1][c] = __ffma2_rn(fc[c], wb, acc[r][2 * h + 1][c]);
+            }
+          }
+        } else {
 #pragma unroll
-          for (int i = 0; i < TE / 2; ++i) {
-            acc[y][i] = __ffma2_rn(g0, wz2[i], acc[y][i]);
-            acc[y + 1][i] = __ffma2_rn(g1, wz2[i], acc[y + 1][i]);
+          for (int h = 0; h < 2; ++h) {
+            if (skip_x_half<T>(fl, h)) continue;
+            T wx[4];
+            load_wx4<T>(sw[k][0], 4 * h, wx);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              acc[r][4 * h + i][0] += f0 * wx[i];
+              acc[r][4 * h + i][1] += f1 * wx[i];
+              acc[r][4 * h + i][2] += f2 * wx[i];
+            }
           }
         }
       }
-      if (more) stage_store(st, ncn, buf ^ 1);
-      __syncthreads();
     }
   }
-  // the quarters' blocks, added in quarter order; four z per thread and store
-  float* mine = sacc[q] + p * SG_P;
 #pragma unroll
-  for (int y = 0; y < TE; ++y) {
-    *reinterpret_cast<float4*>(mine + y * TE) = make_float4(acc[y][0].x, acc[y][0].y, acc[y][1].x, acc[y][1].y);
-    *reinterpret_cast<float4*>(mine + y * TE + 4) =
-        make_float4(acc[y][2].x, acc[y][2].y, acc[y][3].x, acc[y][3].y);
-  }
-  __syncthreads();
-  for (int Q = t; Q < 3 * TE * TE * 2; Q += SG_T) {  // (c, x, y, z half)
-    const int zh = Q & 1, y = (Q >> 1) & 7, pp = Q >> 4, cc = pp >> 3, xx = pp & 7;
-    const int off = pp * SG_P + y * TE + 4 * zh;
-    float4 v = *reinterpret_cast<const float4*>(sacc[0] + off);
+  for (int r = 0; r < 2; ++r) {
+    const int ox = tx * TE, oy = ty * TE + yq + 4 * r, oz = tz * TE + z;
 #pragma unroll
-    for (int r = 1; r < 4; ++r) {
-      const float4 a = *reinterpret_cast<const float4*>(sacc[r] + off);
-      v.x += a.x;
-      v.y += a.y;
-      v.z += a.z;
-      v.w += a.w;
+    for (int x = 0; x < TE; ++x) {
+      const long long idx = ((long long)(ox + x) * g.ny + oy) * g.nz + oz;
+      if (!FCM_INB(idx, G, BS_GRID)) continue;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        if constexpr (sizeof(T) == 4)
+          grid[c * G + idx] = (x & 1) ? acc[r][x >> 1][c].y : acc[r][x >> 1][c].x;
+        else
+          grid[c * G + idx] = acc[r][x][c];
+      }
     }
-    const long long idx = ((long long)(tx * TE + xx) * g.ny + ty * TE + y) * g.nz + tz * TE + 4 * zh;
-    if (FCM_INB(idx + 3, G, BS_GRID)) *reinterpret_cast<float4*>(grid + cc * G + idx) = v;
   }
 }
 
@@ -1396,12 +1359,7 @@ int launch_spread(const Ctx& c, const BlobTable<T>& t, const double* dF, T* grid
     } else if (v == 3) {
       k_spread_tiled<T, 32><<<t.ntiles, 64, 0, s>>>(t.wc, dF, tg, t.tile_offset, t.tile_list, c.g.G, grid);
     } else if (v == 4) {
-      if constexpr (sizeof(T) == 4) {
-        k_spread_gemm<<<t.ntiles, SG_T, 0, s>>>(t.wc, dF, tg, t.tile_offset, t.tile_list, c.g.G, grid);
-      } else {
-        set_error("spread variant 4 is FP32 only");
-        return FCM_ERR_INVALID;
-      }
+      k_spread_warp<T><<<t.ntiles, 32, 0, s>>>(t.wc, dF, tg, t.tile_offset, t.tile_list, c.g.G, grid);
     } else {
       k_spread_tiled<T, 16><<<t.ntiles, 64, 0, s>>>(t.wc, dF, tg, t.tile_offset, t.tile_list, c.g.G, grid);
     }
