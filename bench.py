@@ -401,10 +401,12 @@ def run_ours(args):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     K2 = max(2, args.steps // 2)
+    e2e_iters = []
     e0.record(stream)
     for i in range(K2):
         sm.set_bodies(xs, qs)
-        run_step(sm, seed, 10000 + i, args.step_mode)
+        st_, info_ = run_step(sm, seed, 10000 + i, args.step_mode)
+        e2e_iters.append(info_.gmres_iters)
         xs, qs = sm.get_bodies()
     e1.record(stream)
     e1.synchronize()
@@ -488,7 +490,7 @@ def run_ours(args):
             "roofline_kernels": kernels,
             "cpu_baseline": cpu,
             "e2e": {"value": replica_throughput(M, K2, world, t_e2e), "unit": UNIT, "h2d_bytes_per_step": 7 * 8 * M,
-                    "d2h_bytes_per_step": 7 * 8 * M},
+                    "d2h_bytes_per_step": 7 * 8 * M, "steps": K2, "gmres_iters": float(np.mean(e2e_iters))},
             "gpu_launches": results["mixed"]["launches"],
             "clocks": results["mixed"]["clocks"],
         }

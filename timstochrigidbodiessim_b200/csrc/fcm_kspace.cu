@@ -1288,25 +1288,6 @@ int with_factors(int n, F&& f) {
   return FCM_ERR_INVALID;
 }
 
-template <typename T>
-int zfft(const Ctx& c, const T* r, typename cplx_t<T>::type* spec, T* r_out, long long nlines, bool inverse,
-         cudaStream_t s) {
-  using C = typename cplx_t<T>::type;
-  const C* tw = (const C*)c.d_ztw32;
-  return with_factors(c.g.nz, [&](auto a, auto b) -> int {
-    constexpr int Z1 = decltype(a)::value, Z2 = decltype(b)::value;
-    constexpr int Q = 256 / Z2;
-    const size_t smem = (size_t)Q * Z1 * (Z2 + 1) * sizeof(C);
-    const unsigned grid = (unsigned)((nlines + 2 * Q - 1) / (2 * Q));
-    if (inverse)
-      k_zfft_c2r<T, C, Z1, Z2><<<grid, 256, smem, s>>>(spec, r_out, nlines, tw);
-    else
-      k_zfft_r2c<T, C, Z1, Z2><<<grid, 256, smem, s>>>(r, spec, nlines, tw);
-    FCM_LAUNCH_CHECK();
-    return (int)FCM_OK;
-  });
-}
-
 // Dynamic shared memory above the default 48 KB for `kernel`, set once per kernel
 // and device (kernels of one signature share the template instance, so the cache
 // is keyed by the kernel's address).
@@ -1324,6 +1305,46 @@ int smem_attr_once(K kernel, size_t smem) {
     done.push_back(key);
   }
   return FCM_OK;
+}
+
+// z passes of Z1 x Z2 points, Q = 256 / Z2 complex pencils (two real lines each)
+// per CTA.
+template <typename T, int Z1, int Z2>
+int zfft_run(const T* r, typename cplx_t<T>::type* spec, T* r_out, long long nlines, bool inverse,
+             const typename cplx_t<T>::type* tw, cudaStream_t s) {
+  using C = typename cplx_t<T>::type;
+  constexpr int Q = 256 / Z2;
+  const size_t smem = (size_t)Q * Z1 * (Z2 + 1) * sizeof(C);
+  const unsigned grid = (unsigned)((nlines + 2 * Q - 1) / (2 * Q));
+  if (inverse) {
+    FCM_TRY(smem_attr_once(k_zfft_c2r<T, C, Z1, Z2>, smem));
+    k_zfft_c2r<T, C, Z1, Z2><<<grid, 256, smem, s>>>(spec, r_out, nlines, tw);
+  } else {
+    FCM_TRY(smem_attr_once(k_zfft_r2c<T, C, Z1, Z2>, smem));
+    k_zfft_r2c<T, C, Z1, Z2><<<grid, 256, smem, s>>>(r, spec, nlines, tw);
+  }
+  FCM_LAUNCH_CHECK();
+  return (int)FCM_OK;
+}
+
+// At 512 points the split is 32 x 16 (the middle step then has Q Z1 = 512 items, two
+// per thread; 16 x 32 left half the CTA idle there), elsewhere the table's.
+#ifndef FCM_ZFFT512_Z1
+#define FCM_ZFFT512_Z1 16
+#endif
+
+template <typename T>
+int zfft(const Ctx& c, const T* r, typename cplx_t<T>::type* spec, T* r_out, long long nlines, bool inverse,
+         cudaStream_t s) {
+  using C = typename cplx_t<T>::type;
+  const C* tw = (const C*)c.d_ztw32;
+  return with_factors(c.g.nz, [&](auto a, auto b) -> int {
+    constexpr int Z1 = decltype(a)::value, Z2 = decltype(b)::value;
+    if constexpr (Z1 * Z2 == 512)
+      return zfft_run<T, FCM_ZFFT512_Z1, 512 / FCM_ZFFT512_Z1>(r, spec, r_out, nlines, inverse, tw, s);
+    else
+      return zfft_run<T, Z1, Z2>(r, spec, r_out, nlines, inverse, tw, s);
+  });
 }
 
 // y pass: 16 kz per CTA (rows of 128 bytes in FP32; the second step has Y1 * 16 =
