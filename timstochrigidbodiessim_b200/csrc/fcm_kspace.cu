@@ -890,6 +890,12 @@ __global__ void __launch_bounds__(256) k_zfft_c2r(const C* __restrict__ in, T* _
   }
 }
 
+// Whether the y pass's first step loads two items per thread before transforming
+// either (where the items divide evenly among the threads).
+#ifndef FCM_YFFT_BATCH
+#define FCM_YFFT_BATCH 1
+#endif
+
 // C2C along y, in place: blockIdx.y = x-plane (3 nx per grid), TK kz per CTA.
 // Both directions split NY = Y1 Y2 the same way (input n = j Y2 + n2, output
 // k = k1 + Y1 k2): Y1-point DFTs over j, the twiddles W_NY^(n2 k1) (conjugated for
@@ -903,21 +909,32 @@ __global__ void __launch_bounds__(256) k_yfft(C* __restrict__ spec, int nzh, con
   V2<T>* s = reinterpret_cast<V2<T>*>(yfft_smem);  // [NY][TK]
   const int k0 = (int)blockIdx.x * TK;
   C* base = spec + (long long)blockIdx.y * NY * nzh + k0;
-  for (int i = threadIdx.x; i < Y2 * TK; i += blockDim.x) {
-    const int kzl = i % TK, n2 = i / TK;
-    const bool live = k0 + kzl < nzh;
-    V2<T> a[Y1];
+  // first step: IPT items per thread when they divide evenly (every item's loads
+  // issued before any transform), else one item at a time
+  constexpr int IPT = (FCM_YFFT_BATCH && (Y2 * TK) % 256 == 0 && Y2 * TK / 256 <= 2) ? Y2 * TK / 256 : 1;
+  for (int i0 = threadIdx.x; i0 < Y2 * TK; i0 += IPT * blockDim.x) {
+    V2<T> a[IPT][Y1];
 #pragma unroll
-    for (int j = 0; j < Y1; ++j)
-      a[j] = live ? ldt<T>(base[(long long)(j * Y2 + n2) * nzh + kzl]) : V2<T>{(T)0, (T)0};
-    dft<T, Y1, INV>(a);
+    for (int u = 0; u < IPT; ++u) {
+      const int i = i0 + u * blockDim.x, kzl = i % TK, n2 = i / TK;
+      const bool live = i < Y2 * TK && k0 + kzl < nzh;
 #pragma unroll
-    for (int j = 1; j < Y1; ++j) {
-      const V2<T> w = ldt<T>(__ldg(&twY[n2 * j]));
-      a[j] = INV ? cmulc(a[j], w) : cmul(a[j], w);
+      for (int j = 0; j < Y1; ++j)
+        a[u][j] = live ? ldt<T>(base[(long long)(j * Y2 + n2) * nzh + kzl]) : V2<T>{(T)0, (T)0};
     }
 #pragma unroll
-    for (int j = 0; j < Y1; ++j) s[(j * Y2 + n2) * TK + kzl] = a[j];
+    for (int u = 0; u < IPT; ++u) {
+      const int i = i0 + u * blockDim.x, kzl = i % TK, n2 = i / TK;
+      if (i >= Y2 * TK) break;
+      dft<T, Y1, INV>(a[u]);
+#pragma unroll
+      for (int j = 1; j < Y1; ++j) {
+        const V2<T> w = ldt<T>(__ldg(&twY[n2 * j]));
+        a[u][j] = INV ? cmulc(a[u][j], w) : cmul(a[u][j], w);
+      }
+#pragma unroll
+      for (int j = 0; j < Y1; ++j) s[(j * Y2 + n2) * TK + kzl] = a[u][j];
+    }
   }
   __syncthreads();
   for (int i = threadIdx.x; i < Y1 * TK; i += blockDim.x) {
