@@ -108,13 +108,15 @@ def test_variants_refused_where_the_grid_does_not_allow_them(gpu):
         assert rel_err(_mf(h, F, prec), Vo) < TOL[prec], prec
 
 
-@pytest.mark.parametrize("n", [(384, 32, 32), (512, 32, 32), (32, 512, 32), (32, 32, 512), (32, 384, 384)])
+@pytest.mark.parametrize("n", [(384, 32, 32), (512, 32, 32), (32, 512, 32), (32, 32, 512), (32, 384, 384),
+                               (512, 64, 64), (256, 256, 64)])
 def test_long_transforms(gpu, n):
     """The long lengths (384 = 16 x 24, 512 = 32 x 16) of the fused x-transform and
     of the library's y and z passes (64 KB of shared memory per y CTA at 512), in
-    both precisions against the 3D transforms and the oracle, on thin boxes.  FP64
-    keeps the 3D transforms by default beyond 256 points along x; the fused path is
-    a tunable variant."""
+    both precisions against the 3D transforms and the oracle, on thin boxes; the
+    last two boxes give the persistent FP32 x-transform CTAs (one per SM) more than
+    one block each.  FP64 keeps the 3D transforms by default beyond 256 points along
+    x; the fused path is a tunable variant."""
     g, Vo, F = _setup(n, nbodies=24)
     assert g.get_variants()[1] == (0 if n[0] > 256 else 1)
     for prec in (0, 1):
