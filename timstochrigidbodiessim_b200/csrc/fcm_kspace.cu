@@ -719,33 +719,6 @@ __device__ __forceinline__ void xfft_interior_cta(C* __restrict__ spec, const KP
   }
 }
 
-// Persistent interior CTAs, one per SM, with two shared-memory buffers: while the
-// CTA transforms block b, the asynchronous copies of its next block (b + grid)
-// fill the other buffer, so the loads overlap the FFT arithmetic and the barriers
-// of the three steps.  Blocks are (y, kz block) pairs, kz blocks fastest.
-template <typename T, typename C, int N1, int N2, int TK>
-__global__ void __launch_bounds__(256, 1) k_xfft_persist(C* __restrict__ spec, KParams k,
-                                                          const C* __restrict__ twN, int nkzb) {
-  constexpr int NB = N1 * N2 * 3 * TK;  // elements per buffer
-  extern __shared__ __align__(16) unsigned char xfft_smem[];
-  V2<T>* sb = reinterpret_cast<V2<T>*>(xfft_smem);
-  const int nblocks = nkzb * k.ny;
-  int blk = blockIdx.x;
-  if (blk >= nblocks) return;  // uniform over the CTA
-  xfft_block_copy<T, C, N1, N2, TK>(spec, k, blk / nkzb, (blk % nkzb) * TK, sb);
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-  for (int buf = 0; blk < nblocks; blk += gridDim.x, buf ^= 1) {
-    const int nxt = blk + gridDim.x;
-    if (nxt < nblocks) xfft_block_copy<T, C, N1, N2, TK>(spec, k, nxt / nkzb, (nxt % nkzb) * TK, sb + (buf ^ 1) * NB);
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // this block's copies done
-    __syncthreads();
-    xfft_interior_block<T, C, N1, N2, TK, true>(spec, k, twN, blk / nkzb, (blk % nkzb) * TK, sb + buf * NB);
-    __syncthreads();  // the buffer is refilled two blocks on
-  }
-  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-}
-
 // Threads per CTA: 256 (an FP32 CTA sized to one pencil DFT per thread and step,
 // 384 threads at 256 points, measured slower); 128 for the FP64 interior CTAs,
 // whose register-resident pencils take about 150 registers.
@@ -1227,27 +1200,6 @@ constexpr int xfft_pairs(int n) {
   return 1;
 }
 
-// Interior x-transforms of 256 points and more as persistent CTAs with two buffers
-// (FP32; smaller grids, whose blocks barely outnumber the SMs, keep one block per CTA).
-#ifndef FCM_XFFT_PERSIST
-#define FCM_XFFT_PERSIST 1
-#endif
-
-// Streaming multiprocessors of a device, looked up once per device.
-int sm_count(int device) {
-  static std::mutex mu;
-  static int cache[64] = {0};
-  const int d = (device >= 0 && device < 64) ? device : 0;
-  std::lock_guard<std::mutex> lock(mu);
-  if (!cache[d]) {
-    int n = 0;
-    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, d) != cudaSuccess || n < 1) n = 1;
-    cudaGetLastError();
-    cache[d] = n;
-  }
-  return cache[d];
-}
-
 template <typename K>
 int xfft_smem_attr(K kernel, size_t smem) {
   FCM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1266,13 +1218,11 @@ int xfft_run(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s, bool 
   constexpr int PP = xfft_pairs<T>(N);
   const size_t smem_i = (size_t)N * 3 * TK * sizeof(C);
   const size_t smem_p = (size_t)N * (6 * PP + 1) * sizeof(C);
-  constexpr bool PERSIST = FCM_XFFT_PERSIST && sizeof(T) == 4 && N >= 256;
   if (prepare) {
     FCM_TRY(xfft_smem_attr(k_xfft_project<T, C, N1, N2, TK, false>, smem_i));
     FCM_TRY(xfft_smem_attr(k_xfft_project<T, C, N1, N2, PP, true>, smem_p));
     FCM_TRY(xfft_smem_attr(k_b_xfft_project<T, C, P, N1, N2, TK, false>, smem_i));
     FCM_TRY(xfft_smem_attr(k_b_xfft_project<T, C, P, N1, N2, PP, true>, smem_p));
-    if constexpr (PERSIST) FCM_TRY(xfft_smem_attr(k_xfft_persist<T, C, N1, N2, TK>, 2 * smem_i));
     return FCM_OK;
   }
   const C* tw = (const C*)(sizeof(T) == 4 ? c.d_xtw32 : c.d_xtw64);
@@ -1287,13 +1237,7 @@ int xfft_run(const Ctx& c, typename cplx_t<T>::type* spec, cudaStream_t s, bool 
     k_b_xfft_project<T, C, P, N1, N2, PP, true><<<gp, BP, smem_p, s>>>(b->mem, gidx, mask, tw);
   } else {
     const KParams k = make_kparams(c);
-    if constexpr (PERSIST && BI == 256) {
-      const int nkzb = (kzn + TK - 1) / TK;
-      const int ctas = std::min(nkzb * c.g.ny, sm_count(c.device));
-      k_xfft_persist<T, C, N1, N2, TK><<<ctas, 256, 2 * smem_i, s>>>(spec, k, tw, nkzb);
-    } else {
-      k_xfft_project<T, C, N1, N2, TK, false><<<gi, BI, smem_i, s>>>(spec, k, tw);
-    }
+    k_xfft_project<T, C, N1, N2, TK, false><<<gi, BI, smem_i, s>>>(spec, k, tw);
     FCM_LAUNCH_CHECK();
     k_xfft_project<T, C, N1, N2, PP, true><<<gp, BP, smem_p, s>>>(spec, k, tw);
   }
