@@ -312,6 +312,8 @@ int fcm_interp(fcm_ctx* ctx, int32_t precision, double* V);
  *       lane, added in the lane) with the shuffle reduction, 2 = one warp per tile
  *       (two y-rows per thread) with a shared-memory reduction.  They agree within
  *       rounding.
+ * Defaults: spread 0 (FP64) and 4 (FP32), solve 1 (FP64 up to 256 points along
+ * x, else 0) and 2 (FP32, where the grid allows, else 1 or 0), interpolation 1.
  * A variant the grid does not allow (solve 1 and 2 need supported lengths, 2 also
  * nz <= 512) or out of range is refused with FCM_ERR_INVALID; the spread and
  * interpolation entries have no effect where the grid is not tiled, the FP32

@@ -46,7 +46,7 @@ def _mf(g, F, prec):
 def test_variants_agree(gpu):
     g, Vo, F = _setup()
     v0 = g.get_variants()
-    assert v0[:4] == [0, 1, 1, 2]  # the spread and solve defaults on a 64^3 grid
+    assert v0 == [0, 1, 4, 2, 1, 1]  # the defaults on a 64^3 grid
     for prec in (0, 1):
         for sv in ((0, 1) if prec == 0 else (0, 1, 2)):
             out = []

@@ -376,45 +376,45 @@ __device__ __forceinline__ void spread_tile(const T* __restrict__ wc, const doub
 #pragma unroll
       for (int c = 0; c < 3; ++c) grid[c * G + idx] = (x & 1) ? acc2[x >> 1][c].y : acc2[x >> 1][c].x;
     }
-    return;
-  }
-  T acc[TE][3];
+  } else {
+    T acc[TE][3];
 #pragma unroll
-  for (int x = 0; x < TE; ++x)
+    for (int x = 0; x < TE; ++x)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) acc[x][c] = 0;
-  for (int c0 = b0; c0 < b1; c0 += NB) {
-    const int nc = min(NB, b1 - c0);
-    if (c0 != b0) __syncthreads();
-    stage_blobs_n<T, NB>(list, c0, nc, wc, F, sw, sF, sflag, g);
-    __syncthreads();
-    for (int k = 0; k < nc; ++k) {
-      const unsigned fl = sflag[k];
-      if (!((fl >> (EYM + yh)) & 1u)) continue;
-      const T wyz = sw[k][1][y] * sw[k][2][z];
-      const T f0 = sF[k][0] * wyz, f1 = sF[k][1] * wyz, f2 = sF[k][2] * wyz;
+      for (int c = 0; c < 3; ++c) acc[x][c] = 0;
+    for (int c0 = b0; c0 < b1; c0 += NB) {
+      const int nc = min(NB, b1 - c0);
+      if (c0 != b0) __syncthreads();
+      stage_blobs_n<T, NB>(list, c0, nc, wc, F, sw, sF, sflag, g);
+      __syncthreads();
+      for (int k = 0; k < nc; ++k) {
+        const unsigned fl = sflag[k];
+        if (!((fl >> (EYM + yh)) & 1u)) continue;
+        const T wyz = sw[k][1][y] * sw[k][2][z];
+        const T f0 = sF[k][0] * wyz, f1 = sF[k][1] * wyz, f2 = sF[k][2] * wyz;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        if (skip_x_half<T>(fl, h)) continue;
-        T wx[4];
-        load_wx4<T>(sw[k][0], 4 * h, wx);
+        for (int h = 0; h < 2; ++h) {
+          if (skip_x_half<T>(fl, h)) continue;
+          T wx[4];
+          load_wx4<T>(sw[k][0], 4 * h, wx);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          acc[4 * h + i][0] += f0 * wx[i];
-          acc[4 * h + i][1] += f1 * wx[i];
-          acc[4 * h + i][2] += f2 * wx[i];
+          for (int i = 0; i < 4; ++i) {
+            acc[4 * h + i][0] += f0 * wx[i];
+            acc[4 * h + i][1] += f1 * wx[i];
+            acc[4 * h + i][2] += f2 * wx[i];
+          }
         }
       }
     }
-  }
-  const int ox = tx * TE, oy = ty * TE + y, oz = tz * TE + z;
+    const int ox = tx * TE, oy = ty * TE + y, oz = tz * TE + z;
 #pragma unroll
-  for (int x = 0; x < TE; ++x) {
-    const long long idx = ((long long)(ox + x) * g.ny + oy) * g.nz + oz;
-    if (!FCM_INB(idx, G, BS_GRID)) continue;
-    grid[idx] = acc[x][0];
-    grid[G + idx] = acc[x][1];
-    grid[2 * G + idx] = acc[x][2];
+    for (int x = 0; x < TE; ++x) {
+      const long long idx = ((long long)(ox + x) * g.ny + oy) * g.nz + oz;
+      if (!FCM_INB(idx, G, BS_GRID)) continue;
+      grid[idx] = acc[x][0];
+      grid[G + idx] = acc[x][1];
+      grid[2 * G + idx] = acc[x][2];
+    }
   }
 }
 
@@ -426,6 +426,16 @@ __global__ void __launch_bounds__(64) k_spread_tiled(const T* __restrict__ wc, c
   spread_tile<T, NB>(wc, F, g, offset, list, G, grid, blockIdx.x);
 }
 
+// Resident one-warp CTAs per SM the register allocation of the FP32 warp kernels
+// must allow (without spills: interpolation 80 registers, spread 72; FP64 keeps 12
+// and 16, the allocation it takes unbounded).
+#ifndef FCM_INTERP_WARP_MINB
+#define FCM_INTERP_WARP_MINB 24
+#endif
+#ifndef FCM_SPREAD_WARP_MINB
+#define FCM_SPREAD_WARP_MINB 28
+#endif
+
 // Tiled spreading by one warp per 8x8x8 tile: lane (yq, z) = (lane / 8, lane % 8)
 // owns the x-columns of rows y = yq and yq + 4 (eight points each, three
 // components, in registers) and adds each staged blob to the rows its stencil
@@ -434,7 +444,7 @@ __global__ void __launch_bounds__(64) k_spread_tiled(const T* __restrict__ wc, c
 // with the products of k_spread_tiled (f_c = F_c wy wz, then f_c wx), so the grid
 // is the same bit for bit.
 template <typename T>
-__global__ void __launch_bounds__(32) k_spread_warp(const T* __restrict__ wc, const double* __restrict__ F,
+__global__ void __launch_bounds__(32, sizeof(T) == 4 ? FCM_SPREAD_WARP_MINB : 16) k_spread_warp(const T* __restrict__ wc, const double* __restrict__ F,
                                                     TileGeom g, const int* __restrict__ offset,
                                                     const unsigned long long* __restrict__ list, long long G,
                                                     T* __restrict__ grid) {
@@ -1030,7 +1040,7 @@ __global__ void __launch_bounds__(64 / R) k_interp_rows(const T* __restrict__ wc
 // kernel this halves the reductions per (blob, tile) pair and needs no CTA
 // barrier or shared-memory sum: only the staged weights pass through shared memory.
 template <typename T>
-__global__ void __launch_bounds__(32) k_interp_warp(const T* __restrict__ wc, const T* __restrict__ grid,
+__global__ void __launch_bounds__(32, sizeof(T) == 4 ? FCM_INTERP_WARP_MINB : 12) k_interp_warp(const T* __restrict__ wc, const T* __restrict__ grid,
                                                     TileGeom g, const int* __restrict__ offset,
                                                     const unsigned long long* __restrict__ list, long long G,
                                                     T* __restrict__ partial) {

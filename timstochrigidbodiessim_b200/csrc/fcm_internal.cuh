@@ -335,13 +335,14 @@ struct Ctx {
   bool xfft_cap[2] = {false, false};
   bool yz32_cap = false;
   // spread kernel per precision: 0 the persistent software-pipelined one (FP64
-  // default), 1 / 2 / 3 one CTA per tile staging 16 (FP32 default) / 8 / 32 blobs
-  // per round; all sum every point's blobs in the same order
-  int spread_variant[2] = {0, 1};
-  // interpolation kernel per precision: 0 the shuffle-reduced tile kernel
-  // (k_interp_tiled), 1 / 2 the shared-memory reduced kernel with one / two y-rows
-  // per thread (k_interp_rows, 64 / 32 threads per tile)
-  int interp_variant[2] = {0, 0};
+  // default), 1 / 2 / 3 one CTA per tile staging 16 / 8 / 32 blobs per round, 4
+  // one warp per tile (FP32 default); all sum every point's blobs in the same order
+  int spread_variant[2] = {0, 4};
+  // interpolation kernel per precision: 0 the 64-thread shuffle-reduced tile
+  // kernel (k_interp_tiled), 1 one warp per tile with two y-rows per lane and the
+  // shuffle reduction (k_interp_warp, the default), 2 the shared-memory reduced
+  // kernel with two y-rows per thread (k_interp_rows, 32 threads per tile)
+  int interp_variant[2] = {1, 1};
   void* d_ytw32 = nullptr;
   void* d_ztw32 = nullptr;
   void* d_xtw64 = nullptr;
