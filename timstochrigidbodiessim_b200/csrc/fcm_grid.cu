@@ -426,16 +426,6 @@ __global__ void __launch_bounds__(64) k_spread_tiled(const T* __restrict__ wc, c
   spread_tile<T, NB>(wc, F, g, offset, list, G, grid, blockIdx.x);
 }
 
-// Resident one-warp CTAs per SM the register allocation of the FP32 warp kernels
-// must allow (without spills: interpolation 80 registers, spread 72; FP64 keeps 12
-// and 16, the allocation it takes unbounded).
-#ifndef FCM_INTERP_WARP_MINB
-#define FCM_INTERP_WARP_MINB 24
-#endif
-#ifndef FCM_SPREAD_WARP_MINB
-#define FCM_SPREAD_WARP_MINB 28
-#endif
-
 // Tiled spreading by one warp per 8x8x8 tile: lane (yq, z) = (lane / 8, lane % 8)
 // owns the x-columns of rows y = yq and yq + 4 (eight points each, three
 // components, in registers) and adds each staged blob to the rows its stencil
@@ -444,7 +434,7 @@ __global__ void __launch_bounds__(64) k_spread_tiled(const T* __restrict__ wc, c
 // with the products of k_spread_tiled (f_c = F_c wy wz, then f_c wx), so the grid
 // is the same bit for bit.
 template <typename T>
-__global__ void __launch_bounds__(32, sizeof(T) == 4 ? FCM_SPREAD_WARP_MINB : 16) k_spread_warp(const T* __restrict__ wc, const double* __restrict__ F,
+__global__ void __launch_bounds__(32) k_spread_warp(const T* __restrict__ wc, const double* __restrict__ F,
                                                     TileGeom g, const int* __restrict__ offset,
                                                     const unsigned long long* __restrict__ list, long long G,
                                                     T* __restrict__ grid) {
@@ -1040,7 +1030,7 @@ __global__ void __launch_bounds__(64 / R) k_interp_rows(const T* __restrict__ wc
 // kernel this halves the reductions per (blob, tile) pair and needs no CTA
 // barrier or shared-memory sum: only the staged weights pass through shared memory.
 template <typename T>
-__global__ void __launch_bounds__(32, sizeof(T) == 4 ? FCM_INTERP_WARP_MINB : 12) k_interp_warp(const T* __restrict__ wc, const T* __restrict__ grid,
+__global__ void __launch_bounds__(32) k_interp_warp(const T* __restrict__ wc, const T* __restrict__ grid,
                                                     TileGeom g, const int* __restrict__ offset,
                                                     const unsigned long long* __restrict__ list, long long G,
                                                     T* __restrict__ partial) {
