@@ -313,6 +313,17 @@ def step_velocity_errors(p, ref, x, q, fe, seed, start, K, stream):
     return eU, eL
 
 
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), or None."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def cpu_baseline(p, ref, x, q, fe, gmres_iters):
     """The CPU oracle (the reference's algorithm restated, FP64) on a bounded
     sample of the same workload: one fluctuating-field solve plus one saddle-point
@@ -339,7 +350,7 @@ def cpu_baseline(p, ref, x, q, fe, gmres_iters):
     t2 = time.perf_counter()
     t_step = (t1 - t0) + (gmres_iters + 2) * (t2 - t1)
     o.close()
-    return {"value": p.num_bodies / t_step, "unit": UNIT, "cores": threads, "kind": "port",
+    return {"value": p.num_bodies / t_step, "unit": UNIT, "cores": threads, "kind": "port", "cpu": cpu_model(),
             "sample": "bounded sample: 1 fluctuating field + forces (%.2fs) and 1 preconditioned saddle-point "
                       "product (%.2fs) of the same workload, FP64, scaled to a step as noise + (%.1f GMRES iters "
                       "+ 2) products; bench.py --impl reference times whole oracle steps" %
@@ -450,7 +461,8 @@ def run_ours(args):
                 ach = bytes_ / t_k / 1e9
                 kernels.append({"kernel": "fcm %s (%s)" % (name, tag), "bytes_per_launch": bytes_,
                                 "ms_per_launch": 1e3 * t_k, "achieved": ach, "frac": ach / hbm,
-                                "traffic": traffic.get("%s_%s" % (name, tag))})
+                                "traffic": traffic.get("%s_%s" % (name, tag)),
+                                "stencil_touches_per_s": p.num_blobs * p.ngauss ** 3 / t_k})
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             cpu = cpu_baseline(p, ref, x, q, fe, results["fp64"]["iters"])
@@ -582,7 +594,8 @@ def run_reference(args):
         "config": {"workload": args.workload, "bodies": p.num_bodies, "blobs_per_body": p.blobs_per_body,
                    "grid": [p.nx, p.ny, p.nz], "algorithm": args.algorithm, "gmres_tol": p.gmres_tol},
         "gmres_iters": float(np.mean(iters)),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc,
+                         "cpu": cpu_model()},
         "single_thread": {"value": value * t_all / t_one, "unit": UNIT, "cores": 1,
                           "derived": "whole-step figure x (one saddle-point product on all threads %.2fs / on one "
                                      "thread %.2fs)" % (t_all, t_one)},
