@@ -791,6 +791,46 @@ __device__ __forceinline__ int zpos(int k) {  // position of mode k after the tw
   return (k % Z1) * Z2 + k / Z1;
 }
 
+// Whether the z passes' middle step shares each row between two lanes where it
+// would otherwise leave half the CTA idle (Z2 = 2 Z1).
+#ifndef FCM_ZFFT_PAIR
+#define FCM_ZFFT_PAIR 1
+#endif
+
+// The Z2-point DFT of one shared-memory row (positions row[zpad(j)], j < Z2) by a
+// pair of lanes (lane and lane ^ 1): lane half h transforms the samples 2m + h
+// (Z2/2 points), the odd lane scales its result by W_Z2^k (conjugated for the
+// inverse), the pair swaps halves with shuffles and lane h writes outputs
+// k + h Z2/2 = E[k] +- W^k O[k].  Both lanes read their samples before either
+// writes (the shuffles order them).  With tw, output j > 0 is then scaled by the
+// outer twiddle tw[j k1] (conjugated for the inverse) before the store.
+template <typename T, int Z2, bool INV, typename C>
+__device__ __forceinline__ void pair_dft_row(V2<T>* row, int half, const C* __restrict__ tw, int k1) {
+  constexpr int H = Z2 / 2;
+  V2<T> a[H];
+#pragma unroll
+  for (int m = 0; m < H; ++m) a[m] = row[zpad<Z2>(2 * m + half)];
+  dft<T, H, INV>(a);
+  if (half) {
+#pragma unroll
+    for (int k = 1; k < H; ++k) {
+      const V2<T> w = w96<T>(k * (96 / Z2));
+      a[k] = INV ? cmulc(a[k], w) : cmul(a[k], w);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < H; ++k) {
+    const V2<T> o{__shfl_xor_sync(0xffffffffu, a[k].x, 1), __shfl_xor_sync(0xffffffffu, a[k].y, 1)};
+    V2<T> x = half ? csub(o, a[k]) : cadd(a[k], o);
+    const int j = k + half * H;
+    if (tw && j > 0) {
+      const V2<T> w = ldt<T>(__ldg(&tw[j * k1]));
+      x = INV ? cmulc(x, w) : cmul(x, w);
+    }
+    row[zpad<Z2>(j)] = x;
+  }
+}
+
 template <typename T, typename C, int Z1, int Z2>
 __global__ void __launch_bounds__(256) k_zfft_r2c(const T* __restrict__ in, C* __restrict__ out, long long nlines,
                                                   const C* __restrict__ twZ) {
@@ -817,14 +857,20 @@ __global__ void __launch_bounds__(256) k_zfft_r2c(const T* __restrict__ in, C* _
     for (int j = 0; j < Z1; ++j) s[p * PS + zpad<Z2>(j * Z2 + n2)] = a[j];
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < Q * Z1; i += blockDim.x) {
-    const int p = i / Z1, k1 = i % Z1;
-    V2<T> b[Z2];
+  if constexpr (FCM_ZFFT_PAIR && 2 * Q * Z1 == 256 && Z2 % 2 == 0 && 96 % Z2 == 0) {
+    // half the threads would have an item: each row is shared by a lane pair
+    const int i = threadIdx.x >> 1, p = i / Z1, k1 = i % Z1;
+    pair_dft_row<T, Z2, false, C>(s + p * PS + zpad<Z2>(k1 * Z2), threadIdx.x & 1, nullptr, 0);
+  } else {
+    for (int i = threadIdx.x; i < Q * Z1; i += blockDim.x) {
+      const int p = i / Z1, k1 = i % Z1;
+      V2<T> b[Z2];
 #pragma unroll
-    for (int j = 0; j < Z2; ++j) b[j] = s[p * PS + zpad<Z2>(k1 * Z2 + j)];
-    dft<T, Z2, false>(b);
+      for (int j = 0; j < Z2; ++j) b[j] = s[p * PS + zpad<Z2>(k1 * Z2 + j)];
+      dft<T, Z2, false>(b);
 #pragma unroll
-    for (int j = 0; j < Z2; ++j) s[p * PS + zpad<Z2>(k1 * Z2 + j)] = b[j];
+      for (int j = 0; j < Z2; ++j) s[p * PS + zpad<Z2>(k1 * Z2 + j)] = b[j];
+    }
   }
   __syncthreads();
   constexpr int NZH = N / 2 + 1;  // the spectrum's row length (nzh); a constant divisor below
@@ -883,16 +929,22 @@ __global__ void __launch_bounds__(256) k_zfft_c2r(const C* __restrict__ in, T* _
     if (k > 0 && 2 * k < N) s[p * PS + zpad<Z2>(zpos<Z1, Z2>(N - k))] = V2<T>{a.x + bb.y, bb.x - a.y};
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < Q * Z1; i += blockDim.x) {
-    const int p = i / Z1, k1 = i % Z1;
-    V2<T> b[Z2];
+  if constexpr (FCM_ZFFT_PAIR && 2 * Q * Z1 == 256 && Z2 % 2 == 0 && 96 % Z2 == 0) {
+    // half the threads would have an item: each row is shared by a lane pair
+    const int i = threadIdx.x >> 1, p = i / Z1, k1 = i % Z1;
+    pair_dft_row<T, Z2, true, C>(s + p * PS + zpad<Z2>(k1 * Z2), threadIdx.x & 1, twZ, k1);
+  } else {
+    for (int i = threadIdx.x; i < Q * Z1; i += blockDim.x) {
+      const int p = i / Z1, k1 = i % Z1;
+      V2<T> b[Z2];
 #pragma unroll
-    for (int j = 0; j < Z2; ++j) b[j] = s[p * PS + zpad<Z2>(k1 * Z2 + j)];
-    dft<T, Z2, true>(b);
+      for (int j = 0; j < Z2; ++j) b[j] = s[p * PS + zpad<Z2>(k1 * Z2 + j)];
+      dft<T, Z2, true>(b);
 #pragma unroll
-    for (int j = 1; j < Z2; ++j) b[j] = cmulc(b[j], ldt<T>(__ldg(&twZ[j * k1])));
+      for (int j = 1; j < Z2; ++j) b[j] = cmulc(b[j], ldt<T>(__ldg(&twZ[j * k1])));
 #pragma unroll
-    for (int j = 0; j < Z2; ++j) s[p * PS + zpad<Z2>(k1 * Z2 + j)] = b[j];
+      for (int j = 0; j < Z2; ++j) s[p * PS + zpad<Z2>(k1 * Z2 + j)] = b[j];
+    }
   }
   __syncthreads();
   for (int i = threadIdx.x; i < Q * Z2; i += blockDim.x) {
