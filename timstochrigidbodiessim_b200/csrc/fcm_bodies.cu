@@ -137,6 +137,13 @@ __global__ void k_multiply_KT(const double* __restrict__ q, const double* __rest
 //   out_l = B ref_Minv (K_ref U' + B^T in_l).
 // Shared memory per warp: 2*(3nb) + 12 doubles.  With per-body shapes body n's
 // shape, ref_Minv and ref_N start at ref + n*rs, Minv + n*ms and Nm + n*ns.
+// Columns of the per-body matrix-vector products unrolled together (their loads in
+// flight at once; the products are latency-bound with one warp per body).
+#ifndef FCM_PINV_UNROLL
+#define FCM_PINV_UNROLL 6
+#endif
+constexpr int kPinvUnroll = FCM_PINV_UNROLL;
+
 __device__ __forceinline__ void pinv_block(const double* __restrict__ q, const double* __restrict__ ref, int rs,
                                            const double* __restrict__ Minv, long long ms,
                                            const double* __restrict__ Nm, int ns,
@@ -165,6 +172,7 @@ __device__ __forceinline__ void pinv_block(const double* __restrict__ q, const d
   __syncwarp();
   for (int row = lane; row < n3; row += 32) {
     double s = 0.0;
+#pragma unroll kPinvUnroll
     for (int j = 0; j < n3; ++j) s += Minv[(size_t)j * n3 + row] * xl[j];
     t[row] = s;
   }
@@ -199,6 +207,7 @@ __device__ __forceinline__ void pinv_block(const double* __restrict__ q, const d
   __syncwarp();
   for (int row = lane; row < n3; row += 32) {
     double s = 0.0;
+#pragma unroll kPinvUnroll
     for (int j = 0; j < n3; ++j) s += Minv[(size_t)j * n3 + row] * xl[j];
     t[row] = s;
   }
