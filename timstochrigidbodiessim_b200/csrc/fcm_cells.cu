@@ -90,6 +90,89 @@ __global__ void k_exclusive_scan(const int* __restrict__ in, int* __restrict__ o
   if (threadIdx.x == 0) out[n] = carry;
 }
 
+// The same scan over many CTAs, for long inputs: chunks of SCAN_CH = 8192 entries.
+// k_scan_chunk_sums writes each chunk's total to out[chunk * SCAN_CH] (the chunk's
+// first output slot), k_scan_chunk_offsets turns those totals into exclusive chunk
+// offsets in place (one CTA) and writes out[n], k_scan_chunks scans every chunk
+// from its offset.  Integer sums: the result is that of k_exclusive_scan.
+constexpr int SCAN_T = 1024, SCAN_IPT = 8, SCAN_CH = SCAN_T * SCAN_IPT;
+
+// Block-wide exclusive scan of the thread totals `tot`; returns the thread's
+// exclusive prefix within the block and writes the block total to *total.
+__device__ __forceinline__ int block_exclusive(int tot, int* warp_sums, int* total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = tot;
+  for (int off = 1; off < 32; off <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, off);
+    if (lane >= off) x += y;
+  }
+  if (lane == 31) warp_sums[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int s2 = (lane < (int)(blockDim.x >> 5)) ? warp_sums[lane] : 0;
+    for (int off = 1; off < 32; off <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, s2, off);
+      if (lane >= off) s2 += y;
+    }
+    warp_sums[lane] = s2;
+  }
+  __syncthreads();
+  *total = warp_sums[(blockDim.x >> 5) - 1];
+  return ((wid > 0) ? warp_sums[wid - 1] : 0) + x - tot;
+}
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_chunk_sums(const int* __restrict__ in, int* __restrict__ out,
+                                                           int n) {
+  __shared__ int warp_sums[32];
+  const long long i0 = (long long)blockIdx.x * SCAN_CH + (long long)threadIdx.x * SCAN_IPT;
+  int tot = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_IPT; ++k) tot += (i0 + k < n) ? in[i0 + k] : 0;
+  int total = 0;
+  block_exclusive(tot, warp_sums, &total);
+  if (threadIdx.x == 0) out[(long long)blockIdx.x * SCAN_CH] = total;
+}
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_chunk_offsets(int* __restrict__ out, int n, int nchunks) {
+  __shared__ int warp_sums[32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < nchunks; base += SCAN_T) {
+    const int c = base + threadIdx.x;
+    const int v = c < nchunks ? out[(long long)c * SCAN_CH] : 0;
+    int total = 0;
+    const int ex = block_exclusive(v, warp_sums, &total);
+    if (c < nchunks) out[(long long)c * SCAN_CH] = carry + ex;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[n] = carry;
+}
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_chunks(const int* __restrict__ in, int* __restrict__ out, int n) {
+  __shared__ int warp_sums[32];
+  __shared__ int offset;
+  const long long c0 = (long long)blockIdx.x * SCAN_CH;
+  if (threadIdx.x == 0) offset = out[c0];
+  __syncthreads();
+  const long long i0 = c0 + (long long)threadIdx.x * SCAN_IPT;
+  int v[SCAN_IPT], tot = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_IPT; ++k) {
+    v[k] = (i0 + k < n) ? in[i0 + k] : 0;
+    tot += v[k];
+  }
+  int total = 0;
+  int run = offset + block_exclusive(tot, warp_sums, &total);
+#pragma unroll
+  for (int k = 0; k < SCAN_IPT; ++k) {
+    if (i0 + k < n) out[i0 + k] = run;
+    run += v[k];
+  }
+}
+
 __global__ void k_cell_scatter(const int* __restrict__ cell, int Nb, int ncell, const int* __restrict__ start,
                                int* __restrict__ cursor, int* __restrict__ sorted) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -358,7 +441,17 @@ PairArgs pair_args(const Ctx& c) {
 }  // namespace
 
 int launch_exclusive_scan(const int* in, int* out, int n, cudaStream_t s) {
-  k_exclusive_scan<<<1, 1024, 0, s>>>(in, out, n);
+  if (n <= 2 * SCAN_CH) {  // one or two chunks: one CTA
+    k_exclusive_scan<<<1, SCAN_T, 0, s>>>(in, out, n);
+    FCM_LAUNCH_CHECK();
+    return FCM_OK;
+  }
+  const int nchunks = (n + SCAN_CH - 1) / SCAN_CH;
+  k_scan_chunk_sums<<<nchunks, SCAN_T, 0, s>>>(in, out, n);
+  FCM_LAUNCH_CHECK();
+  k_scan_chunk_offsets<<<1, SCAN_T, 0, s>>>(out, n, nchunks);
+  FCM_LAUNCH_CHECK();
+  k_scan_chunks<<<nchunks, SCAN_T, 0, s>>>(in, out, n);
   FCM_LAUNCH_CHECK();
   return FCM_OK;
 }
