@@ -77,6 +77,46 @@ __global__ void k_set_up_gaussians(const double* __restrict__ Y, int n, int W, d
   }
 }
 
+// The same tables with one warp per (blob, dimension): lane i takes grid point
+// c0 + i of the blob's NCH * TE = 32-point chunk window (c0 = floor(base/8)*8),
+// evaluates its weight with the arithmetic above when it lies in the stencil
+// (s = c0 + i - base in [0, W)) and writes wc[i] and w[s]; every store is
+// coalesced and each weight is computed once (the window holds the stencil since
+// W <= 25 on tiled grids).  Without wc the lanes write w[i], i = lane, lane + 32, ...
+template <typename T>
+__global__ void __launch_bounds__(128) k_set_up_gaussians_warp(const double* __restrict__ Y, int n, int W, double dx,
+                                                               double anorm, double anorm2, int* __restrict__ base,
+                                                               T* __restrict__ w, T* __restrict__ wc,
+                                                               double* __restrict__ ypos) {
+  const long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (t >= 3LL * n) return;  // uniform over the warp
+  const double y = Y[t];
+  const int xc = (int)__ddiv_rn(y, dx);
+  const int b = xc - W / 2 + 1;
+  if (lane == 0) {
+    base[t] = b;
+    if (ypos) ypos[t] = y;
+  }
+  if (!wc) {
+    for (int i = lane; i < W; i += 32) {
+      const double xx = __dsub_rn(__dmul_rn((double)(b + i), dx), y);
+      w[t * W + i] = (T)(anorm * exp(__ddiv_rn(-__dmul_rn(xx, xx), anorm2)));
+    }
+    return;
+  }
+  const int c0 = floordiv(b, TE) * TE;  // first grid point of the window
+  const int g = c0 + lane, sidx = g - b;
+  T val = (T)0;
+  if (sidx >= 0 && sidx < W) {
+    const double xx = __dsub_rn(__dmul_rn((double)g, dx), y);
+    const double e = exp(__ddiv_rn(-__dmul_rn(xx, xx), anorm2));
+    val = (T)(anorm * e);
+    w[t * W + sidx] = val;
+  }
+  wc[t * NCH * TE + lane] = val;
+}
+
 // (blob, tile) overlaps of a blob: per dimension the tiles first..first+cnt-1.
 __device__ __forceinline__ void blob_tiles(const int* base, int b, const TileGeom& g, int f[3], int cnt[3]) {
 #pragma unroll
@@ -1325,7 +1365,8 @@ int launch_set_up_gaussians(const Ctx& c, BlobTable<T>& t, const double* dY, cud
   const double anorm = 1.0 / (sqrt(2.0) * a);
   const double anorm2 = 2.0 * a * a / PI;
   const int nt = 3 * t.n;
-  k_set_up_gaussians<T><<<(nt + 127) / 128, 128, 0, s>>>(dY, t.n, t.W, c.g.dx, anorm, anorm2, t.base, t.w,
+  k_set_up_gaussians_warp<T><<<(unsigned)((32LL * nt + 127) / 128), 128, 0, s>>>(dY, t.n, t.W, c.g.dx, anorm, anorm2,
+                                                                               t.base, t.w,
                                                           t.tiled ? t.wc : nullptr, t.ypos);
   FCM_LAUNCH_CHECK();
   if (t.tiled) {
