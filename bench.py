@@ -149,12 +149,13 @@ class ClockSampler:
 # ----------------------------------------------------------------- ours
 VARIANT_LEGEND = ("variants [FP64 spread, FP64 solve, FP32 spread, FP32 solve, FP64 interp, FP32 interp]: spread "
                   "0 persistent pipelined, 1 / 2 / 3 one CTA per tile staging 16 / 8 / 32 blobs per round, 4 "
-                  "one warp per tile (two y-rows per lane); solve 0 cuFFT 3D + projection, 1 cuFFT (y, z) + fused x-transform, "
+                  "one warp per tile (two y-rows per lane), 5 one warp per tile on the tensor cores (3xTF32, FP32 "
+                  "only); solve 0 cuFFT 3D + projection, 1 cuFFT (y, z) + fused x-transform, "
                   "2 library (y, z) + fused x-transform; interp 0 shuffle reduction with 64 threads per tile, 1 "
                   "one warp per tile (two y-rows per lane) with the shuffle reduction, 2 one warp per tile with "
-                  "a shared-memory reduction.  us[12P + v]: "
-                  "precision P, v 0-4 spread, 5-7 solve, 8-10 interp variants, microseconds per call, -1 not "
-                  "available")
+                  "a shared-memory reduction, 3 one warp per tile on the tensor cores (3xTF32, FP32 only).  "
+                  "us[16P + v]: precision P, v 0-5 spread, 6-8 solve, 9-12 interp variants, microseconds per "
+                  "call, -1 not available")
 
 AUTOTUNE = {"on": True}
 

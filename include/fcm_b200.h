@@ -301,7 +301,9 @@ int fcm_interp(fcm_ctx* ctx, int32_t precision, double* V);
  *       kernel, 1 / 2 / 3 = one CTA per 8^3 tile staging 16 / 8 / 32 blobs per
  *       round, 4 = one warp per tile staging 16 blobs per round, two y-rows per
  *       lane.  All sum every grid point's blobs in the same order with the same
- *       products, so the grids are the same bit for bit.
+ *       products, so the grids are the same bit for bit.  FP32 only: 5 = one warp
+ *       per tile on the tensor cores (mma.sync with TF32 operands split in two,
+ *       3xTF32, FP32 accumulators), equal to the others to FP32 rounding.
  *   [1] FP64 Stokes solve, [3] FP32 Stokes solve: 0 = cuFFT 3D transforms and the
  *       projection kernel, 1 = cuFFT (y, z) transforms around the fused x-transform
  *       + projection kernel, 2 = the library's own (y, z) transforms around it
@@ -310,8 +312,8 @@ int fcm_interp(fcm_ctx* ctx, int32_t precision, double* V);
  *   [4] FP64 interpolation, [5] FP32 interpolation: 0 = 64 threads per 8^3 tile
  *       with a warp shuffle reduction, 1 = one warp per tile (two y-rows per
  *       lane, added in the lane) with the shuffle reduction, 2 = one warp per tile
- *       (two y-rows per thread) with a shared-memory reduction.  They agree within
- *       rounding.
+ *       (two y-rows per thread) with a shared-memory reduction; FP32 only: 3 = one
+ *       warp per tile on the tensor cores (3xTF32).  They agree within rounding.
  * Defaults: spread 0 (FP64) and 4 (FP32), solve 1 (FP64 up to 256 points along
  * x, else 0) and 2 (FP32, where the grid allows, else 1 or 0), interpolation 1.
  * A variant the grid does not allow (solve 1 and 2 need supported lengths, 2 also
@@ -326,13 +328,14 @@ int fcm_set_variants(fcm_ctx* ctx, const int32_t* variants);
 /* Times every variant the grids allow on this context (reps timed calls of each,
  * 5 when reps <= 0, after one untimed call; zero forces, zeroed grids) and keeps
  * the fastest per stage and precision.  us (may be NULL) receives
- * FCM_NUM_TUNE_TIMES doubles, [12 P + v] for precision P (0 FP64, 1 FP32): v = 0..4
- * the spread variants, v = 5, 6, 7 the solve variants 0, 1, 2, v = 8, 9, 10 the
- * interpolation variants 0, 1, 2, in microseconds per call, -1 where not
- * available (v = 11 always); variants (may be NULL) receives the choice as fcm_get_variants does.
+ * FCM_NUM_TUNE_TIMES doubles, [16 P + v] for precision P (0 FP64, 1 FP32): v = 0..5
+ * the spread variants, v = 6, 7, 8 the solve variants 0, 1, 2, v = 9..12 the
+ * interpolation variants 0..3, in microseconds per call, -1 where not available
+ * (FP64 v = 5 and 12, v = 13..15 always); variants (may be NULL) receives the
+ * choice as fcm_get_variants does.
  * Needs set_up_gaussians first; overwrites the grid work arrays, so call it
  * between steps. */
-#define FCM_NUM_TUNE_TIMES 24
+#define FCM_NUM_TUNE_TIMES 32
 int fcm_autotune(fcm_ctx* ctx, int32_t reps, double* us, int32_t* variants);
 /* fcm_fluid_solver.cpp:842-881: single-body mobility at the box centre,
  * ref_Minv = inv_sympd(M_body) ((3nb)^2), ref_N = inv(K^T ref_Minv K) (6x6). */

@@ -58,7 +58,12 @@ def test_variants_agree(gpu):
             for o_ in out[1:]:
                 assert np.array_equal(out[0], o_), (prec, sv)
             assert rel_err(out[0], Vo) < TOL[prec], (prec, sv)
-        for iv in (0, 1, 2):
+        if prec == 1:  # the tensor-core spread agrees with the FMA kernels to FP32 rounding
+            v = g.get_variants()
+            v[2], v[3] = 5, 0
+            g.set_variants(v)
+            assert rel_err(_mf(g, F, prec), Vo) < TOL[prec]
+        for iv in ((0, 1, 2) if prec == 0 else (0, 1, 2, 3)):
             v = g.get_variants()
             v[4 + prec] = iv
             g.set_variants(v)
@@ -69,12 +74,13 @@ def test_variants_agree(gpu):
 def test_autotune_keeps_the_fastest(gpu):
     g, Vo, F = _setup()
     v, us = g.autotune(reps=3)
-    assert np.all(us[0:7] > 0) and us[7] == -1  # FP64 has no library (y, z) variant
-    assert np.all(us[8:11] > 0) and us[11] == -1
-    assert np.all(us[12:23] > 0) and us[23] == -1
+    # FP64 has no library (y, z) variant and no tensor-core spread or interpolation
+    assert np.all(us[0:5] > 0) and us[5] == -1 and np.all(us[6:8] > 0) and us[8] == -1
+    assert np.all(us[9:12] > 0) and np.all(us[12:16] == -1)
+    assert np.all(us[16:29] > 0) and np.all(us[29:32] == -1)
     for P in (0, 1):
-        t = us[12 * P:12 * P + 12]
-        spread, solve, interp = t[0:5], t[5:8], t[8:11]
+        t = us[16 * P:16 * P + 16]
+        spread, solve, interp = t[0:5 + P], t[6:9], t[9:12 + P]
         assert v[2 * P] == int(np.argmin(spread))
         best = min((x, i) for i, x in enumerate(solve) if x >= 0)[1]
         assert v[2 * P + 1] == best
@@ -89,11 +95,13 @@ def test_variants_refused_where_the_grid_does_not_allow_them(gpu):
     with pytest.raises(FcmError):
         g.set_variants([0, 2, 1, 2, 0, 0])  # no library (y, z) variant in FP64
     with pytest.raises(FcmError):
-        g.set_variants([5, 1, 1, 2, 0, 0])  # out of range
+        g.set_variants([5, 1, 1, 2, 0, 0])  # no tensor-core spread in FP64
     with pytest.raises(FcmError):
-        g.set_variants([0, 1, 5, 2, 0, 0])  # out of range
+        g.set_variants([0, 1, 6, 2, 0, 0])  # out of range
     with pytest.raises(FcmError):
-        g.set_variants([0, 1, 1, 2, 3, 0])  # no interpolation variant 3
+        g.set_variants([0, 1, 1, 2, 3, 0])  # no tensor-core interpolation in FP64
+    with pytest.raises(FcmError):
+        g.set_variants([0, 1, 1, 2, 0, 4])  # out of range
     # 20 points along x: no fused x-transform, so only the 3D solve; not tiled, so
     # the spread and interpolation variants are not timed
     h, Vo, F = _setup((20, 24, 16), nbodies=12)
@@ -101,8 +109,8 @@ def test_variants_refused_where_the_grid_does_not_allow_them(gpu):
     with pytest.raises(FcmError):
         h.set_variants([0, 1, 1, 0, 0, 0])
     v, us = h.autotune(reps=2)
-    assert us[6] == -1 and us[18] == -1 and us[19] == -1
-    assert np.all(us[0:5] == -1) and np.all(us[8:12] == -1) and np.all(us[12:17] == -1) and np.all(us[20:24] == -1)
+    assert us[6] > 0 and us[7] == -1 and us[8] == -1 and us[22] > 0 and us[23] == -1 and us[24] == -1
+    assert np.all(us[0:6] == -1) and np.all(us[9:16] == -1) and np.all(us[16:22] == -1) and np.all(us[25:32] == -1)
     assert v[1] == 0 and v[3] == 0
     for prec in (0, 1):
         assert rel_err(_mf(h, F, prec), Vo) < TOL[prec], prec

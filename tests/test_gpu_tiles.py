@@ -102,3 +102,28 @@ def test_stage_precision_checks(gpu):
         g.spread(np.zeros(3 * n), 1)  # FP32 grid on an FP64 context
     with pytest.raises(FcmError):
         g.stokes_solve(2)
+
+
+def test_dense_tensor_core_fp32_stages(gpu, dense):
+    """The tensor-core spread (FP32 variant 5) and interpolation (variant 3), each
+    alone beside the FMA kernels and both together, on the dense ragged tile lists:
+    within 1e-6 of the FMA kernels' velocities (both FP32; 3xTF32 keeps every
+    product to FP32 rounding) and within 1e-5 of the FP64 oracle, on two calls."""
+    n, Y, F, _, V = dense
+    g = Suspension(_params(n, precision=1), [0, 0, 0])
+    g.set_up_gaussians(Y)
+
+    def mf(sp, ip):
+        v = g.get_variants()
+        v[2], v[5] = sp, ip
+        g.set_variants(v)
+        g.spread(F, 1)
+        g.stokes_solve(1)
+        return g.interp(1)
+
+    V_fma = mf(4, 1)
+    assert rel_err(V_fma, V) < 1e-5
+    for sp, ip in ((5, 1), (4, 3), (5, 3), (5, 3)):
+        Vt = mf(sp, ip)
+        assert rel_err(Vt, V_fma) < 1e-6, (sp, ip)
+        assert rel_err(Vt, V) < 1e-5, (sp, ip)

@@ -2528,7 +2528,8 @@ static void get_variants(const Ctx* c, int32_t* v) {
 static int set_variants(Ctx* c, const int32_t* v) {
   for (int P = 0; P < 2; ++P) {
     const int sp = v[2 * P], sv = v[2 * P + 1], iv = v[4 + P];
-    if (sp < 0 || sp > 4 || sv < 0 || sv > (P == 1 ? 2 : 1) || iv < 0 || iv > 2) {
+    // the tensor-core spread (5) and interpolation (3) exist for FP32 grids only
+    if (sp < 0 || sp > (P == 1 ? 5 : 4) || sv < 0 || sv > (P == 1 ? 2 : 1) || iv < 0 || iv > (P == 1 ? 3 : 2)) {
       set_error("kernel variant out of range");
       return FCM_ERR_INVALID;
     }
@@ -2576,21 +2577,23 @@ static int time_calls(Ctx* c, int reps, F&& body, double* out) {
 }
 
 // The spread, solve and interpolation variants of one precision timed on c's own
-// grid and blob table; the fastest kept.  t[0..4] spread, t[5..7] solve, t[8..10]
-// interpolation (-1: not available).
+// grid and blob table; the fastest kept.  t[0..5] spread, t[6..8] solve, t[9..12]
+// interpolation (-1: not available; the tensor-core spread 5 and interpolation 3
+// are FP32 only).
 template <typename T>
 static int tune_precision(Ctx* c, int reps, double* t) {
   constexpr int P = sizeof(T) == 8 ? 0 : 1;
   GridBufs<T>& gb = grid_of<T>(c);
   const BlobTable<T>& bt = gb.blobs;
   FCM_CUDA(cudaMemsetAsync(c->d_tmp3, 0, sizeof(double) * 3 * (size_t)(c->Nb > 0 ? c->Nb : 1), c->stream));
+  constexpr int NSP = P == 1 ? 6 : 5, NIP = P == 1 ? 4 : 3;
   if (bt.tiled) {
-    for (int v = 0; v < 5; ++v) {
+    for (int v = 0; v < NSP; ++v) {
       c->spread_variant[P] = v;
       FCM_TRY(time_calls(c, reps, [&] { return spread_t<T>(c, bt, c->d_tmp3); }, &t[v]));
     }
     int bs = 0;
-    for (int v = 1; v < 5; ++v)
+    for (int v = 1; v < NSP; ++v)
       if (t[v] < t[bs]) bs = v;
     c->spread_variant[P] = bs;
   }
@@ -2599,21 +2602,21 @@ static int tune_precision(Ctx* c, int reps, double* t) {
     if ((v >= 1 && !c->xfft_cap[P]) || (v == 2 && (P == 0 || !c->yz32_cap))) continue;
     c->xfft[P] = v >= 1;
     if (P == 1) c->yz32 = v == 2;
-    FCM_TRY(time_calls(c, reps, [&] { return stokes_t<T>(c); }, &t[5 + v]));
+    FCM_TRY(time_calls(c, reps, [&] { return stokes_t<T>(c); }, &t[6 + v]));
   }
   int best = 0;
   for (int v = 1; v < 3; ++v)
-    if (t[5 + v] >= 0.0 && t[5 + v] < t[5 + best]) best = v;
+    if (t[6 + v] >= 0.0 && t[6 + v] < t[6 + best]) best = v;
   c->xfft[P] = best >= 1;
   if (P == 1) c->yz32 = best == 2;
   if (bt.tiled) {  // interpolation of the (zeroed) grid into scratch
-    for (int v = 0; v < 3; ++v) {
+    for (int v = 0; v < NIP; ++v) {
       c->interp_variant[P] = v;
-      FCM_TRY(time_calls(c, reps, [&] { return interp_t<T>(c, bt, gb.r, c->d_tmp3); }, &t[8 + v]));
+      FCM_TRY(time_calls(c, reps, [&] { return interp_t<T>(c, bt, gb.r, c->d_tmp3); }, &t[9 + v]));
     }
     int bi = 0;
-    for (int v = 1; v < 3; ++v)
-      if (t[8 + v] < t[8 + bi]) bi = v;
+    for (int v = 1; v < NIP; ++v)
+      if (t[9 + v] < t[9 + bi]) bi = v;
     c->interp_variant[P] = bi;
   }
   return FCM_OK;

@@ -1145,6 +1145,293 @@ __global__ void __launch_bounds__(32) k_interp_warp(const T* __restrict__ wc, co
   }
 }
 
+// ------------------------------------------------------------------ tensor-core tiles (FP32 grids)
+// FP32 spreading and interpolation of one 8x8x8 tile by one warp on the tensor
+// cores (mma.sync m16n8k8 with TF32 operands and FP32 accumulators).  Seen as a
+// 64 x 24 matrix C[(y, z), (c, x)], a tile's grid is a sum over its blobs k of
+// (wy_k[y] wz_k[z]) (F_kc wx_k[x]): the product of a 64 x K and a K x 24 matrix,
+// K the tile's blobs, eight per k-step (blobs padded with zero weights).  Every
+// operand is split into its TF32 rounding and the FP32 remainder, and three
+// products are summed (hi*lo, lo*hi, then hi*hi; lo*lo dropped), which keeps
+// each term to about 2^-22 relative, the rounding level of FP32 itself.  The
+// grid agrees with the FMA kernels' to FP32 rounding, not bit for bit.
+// Interpolation is the transpose: P[k, (c, x)] = sum over (y, z) of
+// (wy_k[y] wz_k[z]) grid_c[x][y][z] (16 blobs x 64 (y, z) times 64 x 24, the
+// tile's grid held as operand fragments in registers), then
+// partial_kc = sum over x of P[k, (c, x)] wx_k[x].
+//
+// Fragments of m16n8k8 (g = lane / 4, t = lane % 4): A (16 x 8, row-major)
+// a0 (g, t), a1 (g + 8, t), a2 (g, t + 4), a3 (g + 8, t + 4); B (8 x 8,
+// column-major) b0 (t, g), b1 (t + 4, g); C (16 x 8) c0 (g, 2t), c1 (g, 2t + 1),
+// c2 (g + 8, 2t), c3 (g + 8, 2t + 1).
+
+// a = hi + lo with hi the TF32 rounding of a (low 13 mantissa bits zero) and lo
+// the exact FP32 remainder (read as TF32 by the tensor core).
+__device__ __forceinline__ void tf32_split(float a, unsigned& hi, unsigned& lo) {
+  unsigned h;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(a));
+  hi = h;
+  lo = __float_as_uint(a - __uint_as_float(h));
+}
+
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
+  asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// d += a * b in 3xTF32.
+__device__ __forceinline__ void mma_3xtf32(float (&d)[4], const unsigned (&ah)[4], const unsigned (&al)[4],
+                                           unsigned bh0, unsigned bh1, unsigned bl0, unsigned bl1) {
+  mma_tf32(d, al, bh0, bh1);
+  mma_tf32(d, ah, bl0, bl1);
+  mma_tf32(d, ah, bh0, bh1);
+}
+
+// Software pipeline of a warp's staging.  A round is RB blobs of the tile's list
+// (RB / 8 items of four parts per lane: part 0-2 the blob's x, y, z weight chunk,
+// part 3 its force or nothing); while a round is computed from one shared buffer,
+// the next round's chunks are in flight to registers and the entries of the
+// round after that are being loaded, so a warp waits on memory once per tile,
+// not once per round.  Slots past the tile's list read as entry 0, whose empty
+// half masks mark padding: zero weights and forces.
+template <int RB, bool WITH_F>
+struct MmaStage {
+  static constexpr int NI = RB / 8;  // items per lane
+  unsigned long long e[NI];          // entries of the round after the one in flight
+  float4 v0[NI], v1[NI];             // chunks in flight
+  double f0[NI], f1[NI], f2[NI];     // forces in flight (part 3, WITH_F)
+  unsigned long long ef[NI];         // entries of the round in flight
+
+  __device__ __forceinline__ void load_entries(const unsigned long long* __restrict__ list, int b0, int b1, int r,
+                                               const TileGeom& g) {
+#pragma unroll
+    for (int i = 0; i < NI; ++i) {
+      const int slot = b0 + RB * r + 8 * i + (threadIdx.x >> 2);
+      e[i] = slot < b1 ? list_entry(list, slot, g) : 0ull;
+    }
+  }
+  __device__ __forceinline__ void issue(const float* __restrict__ wc, const double* __restrict__ F) {
+    const int d = threadIdx.x & 3;
+#pragma unroll
+    for (int i = 0; i < NI; ++i) {
+      ef[i] = e[i];
+      const unsigned b = (unsigned)(e[i] >> 32), lo = (unsigned)e[i];
+      const bool ok = ((lo >> EXM) & 63u) != 0u;
+      v0[i] = v1[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      f0[i] = f1[i] = f2[i] = 0.0;
+      if (ok && d < 3) {
+        const float4* src =
+            reinterpret_cast<const float4*>(wc + ((size_t)(3 * b + d) * NCH + ((lo >> (2 * d)) & 3u)) * TE);
+        v0[i] = __ldg(src);
+        v1[i] = __ldg(src + 1);
+      } else if (WITH_F && ok) {
+        f0[i] = F[3 * (size_t)b];
+        f1[i] = F[3 * (size_t)b + 1];
+        f2[i] = F[3 * (size_t)b + 2];
+      }
+    }
+  }
+  __device__ __forceinline__ void put(float (*sw)[3][TE], float (*sF)[4], unsigned* sflag, unsigned* sblob) const {
+    const int d = threadIdx.x & 3;
+#pragma unroll
+    for (int i = 0; i < NI; ++i) {
+      const int k = 8 * i + (threadIdx.x >> 2);
+      if (d < 3) {
+        *reinterpret_cast<float4*>(&sw[k][d][0]) = v0[i];
+        *reinterpret_cast<float4*>(&sw[k][d][4]) = v1[i];
+      } else {
+        if (WITH_F) *reinterpret_cast<float4*>(sF[k]) = make_float4((float)f0[i], (float)f1[i], (float)f2[i], 0.f);
+        if (sflag) sflag[k] = (unsigned)ef[i];
+        if (sblob) sblob[k] = (unsigned)(ef[i] >> 32);
+      }
+    }
+  }
+};
+
+__global__ void __launch_bounds__(32) k_spread_mma(const float* __restrict__ wc, const double* __restrict__ F,
+                                                   TileGeom g, const int* __restrict__ offset,
+                                                   const unsigned long long* __restrict__ list, long long G,
+                                                   float* __restrict__ grid) {
+  __shared__ __align__(16) float sw[2][8][3][TE];
+  __shared__ __align__(16) float sF[2][8][4];
+  const int tile = blockIdx.x;
+  if (!FCM_INB(tile, (long long)g.ntx * g.nty * g.ntz, BS_TILE)) return;  // uniform over the warp
+  int b0, b1;
+  tile_range(offset, tile, g, b0, b1);
+  const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
+  const int lane = threadIdx.x, gq = lane >> 2, tq = lane & 3;
+  float acc[4][3][4];  // [(y, z) row block m][component][fragment]
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) acc[m][c][r] = 0.f;
+  const int R = (b1 - b0 + 7) >> 3;  // rounds of eight blobs (one k-step)
+  MmaStage<8, true> st;
+  if (R > 0) {
+    st.load_entries(list, b0, b1, 0, g);
+    st.issue(wc, F);
+    st.put(sw[0], sF[0], nullptr, nullptr);
+    st.load_entries(list, b0, b1, 1, g);
+    st.issue(wc, F);
+    st.load_entries(list, b0, b1, 2, g);
+  }
+  for (int r = 0; r < R; ++r) {
+    __syncwarp();
+    const int cur = r & 1;
+    if (r + 1 < R) {
+      st.put(sw[cur ^ 1], sF[cur ^ 1], nullptr, nullptr);
+      st.issue(wc, F);
+      st.load_entries(list, b0, b1, r + 3, g);
+    }
+    const int ka = tq, kb = tq + 4;
+    // B = (F_kc wx_k[x]) for blobs ka, kb and x = gq
+    const float xa = sw[cur][ka][0][gq], xb = sw[cur][kb][0][gq];
+    const float4 fa = *reinterpret_cast<const float4*>(sF[cur][ka]);
+    const float4 fb = *reinterpret_cast<const float4*>(sF[cur][kb]);
+    unsigned bh[3][2], bl[3][2];
+    tf32_split(fa.x * xa, bh[0][0], bl[0][0]);
+    tf32_split(fb.x * xb, bh[0][1], bl[0][1]);
+    tf32_split(fa.y * xa, bh[1][0], bl[1][0]);
+    tf32_split(fb.y * xb, bh[1][1], bl[1][1]);
+    tf32_split(fa.z * xa, bh[2][0], bl[2][0]);
+    tf32_split(fb.z * xb, bh[2][1], bl[2][1]);
+    // A = (wy_k[y] wz_k[z]) for rows (y, z) = (2m, gq), (2m + 1, gq)
+    const float za = sw[cur][ka][2][gq], zb = sw[cur][kb][2][gq];
+    float ya[TE], yb[TE];
+    *reinterpret_cast<float4*>(ya) = *reinterpret_cast<const float4*>(&sw[cur][ka][1][0]);
+    *reinterpret_cast<float4*>(ya + 4) = *reinterpret_cast<const float4*>(&sw[cur][ka][1][4]);
+    *reinterpret_cast<float4*>(yb) = *reinterpret_cast<const float4*>(&sw[cur][kb][1][0]);
+    *reinterpret_cast<float4*>(yb + 4) = *reinterpret_cast<const float4*>(&sw[cur][kb][1][4]);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      unsigned ah[4], al[4];
+      tf32_split(ya[2 * m] * za, ah[0], al[0]);
+      tf32_split(ya[2 * m + 1] * za, ah[1], al[1]);
+      tf32_split(yb[2 * m] * zb, ah[2], al[2]);
+      tf32_split(yb[2 * m + 1] * zb, ah[3], al[3]);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) mma_3xtf32(acc[m][c], ah, al, bh[c][0], bh[c][1], bl[c][0], bl[c][1]);
+    }
+  }
+  const int ox = tx * TE, oy = ty * TE, oz = tz * TE + gq;
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int x = 2 * tq + (r & 1), y = 2 * m + (r >> 1);
+      const long long idx = ((long long)(ox + x) * g.ny + oy + y) * g.nz + oz;
+      if (!FCM_INB(idx, G, BS_GRID)) continue;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) grid[c * G + idx] = acc[m][c][r];
+    }
+}
+
+__global__ void __launch_bounds__(32) k_interp_mma(const float* __restrict__ wc, const float* __restrict__ grid,
+                                                   TileGeom g, const int* __restrict__ offset,
+                                                   const unsigned long long* __restrict__ list, long long G,
+                                                   float* __restrict__ partial) {
+  __shared__ __align__(16) float sw[2][16][3][TE];
+  __shared__ unsigned sflag[2][16], sblob[2][16];
+  const int tile = blockIdx.x;
+  if (!FCM_INB(tile, (long long)g.ntx * g.nty * g.ntz, BS_TILE)) return;  // uniform over the warp
+  int b0, b1;
+  tile_range(offset, tile, g, b0, b1);
+  if (b0 == b1) return;  // no blob meets this tile
+  const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
+  const int lane = threadIdx.x, gq = lane >> 2, tq = lane & 3;
+  const int R = (b1 - b0 + 15) >> 4;  // rounds of sixteen blobs (one m-tile)
+  MmaStage<16, false> st;
+  st.load_entries(list, b0, b1, 0, g);
+  st.issue(wc, nullptr);
+  // the tile's grid as B fragments: k-step j holds rows (y, z) = (j, tq), (j, tq + 4)
+  // and column x = gq of each component (loaded while round 0 is in flight)
+  unsigned gh[TE][3][2], gl[TE][3][2];
+  {
+    const int ox = tx * TE + gq, oz = tz * TE + tq;
+#pragma unroll
+    for (int j = 0; j < TE; ++j) {
+      const int oy = ty * TE + j;
+      const bool live = oy < g.ycut;  // rows at or above the slip channel's upper wall read as 0
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const long long idx = ((long long)ox * g.ny + oy) * g.nz + oz + 4 * h;
+        const bool in = live && FCM_INB(idx, G, BS_GRID);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) tf32_split(in ? grid[c * G + idx] : 0.f, gh[j][c][h], gl[j][c][h]);
+      }
+    }
+  }
+  st.put(sw[0], nullptr, sflag[0], sblob[0]);
+  if (R > 1) {
+    st.load_entries(list, b0, b1, 1, g);
+    st.issue(wc, nullptr);
+    st.load_entries(list, b0, b1, 2, g);
+  }
+  for (int r = 0; r < R; ++r) {
+    __syncwarp();
+    const int cur = r & 1;
+    if (r + 1 < R) {
+      st.put(sw[cur ^ 1], nullptr, sflag[cur ^ 1], sblob[cur ^ 1]);
+      st.issue(wc, nullptr);
+      st.load_entries(list, b0, b1, r + 3, g);
+    }
+    // rows of A: blobs gq and gq + 8; columns (y, z) = (j, tq), (j, tq + 4)
+    float ya[TE], yb[TE];
+    *reinterpret_cast<float4*>(ya) = *reinterpret_cast<const float4*>(&sw[cur][gq][1][0]);
+    *reinterpret_cast<float4*>(ya + 4) = *reinterpret_cast<const float4*>(&sw[cur][gq][1][4]);
+    *reinterpret_cast<float4*>(yb) = *reinterpret_cast<const float4*>(&sw[cur][gq + 8][1][0]);
+    *reinterpret_cast<float4*>(yb + 4) = *reinterpret_cast<const float4*>(&sw[cur][gq + 8][1][4]);
+    const float za0 = sw[cur][gq][2][tq], za1 = sw[cur][gq][2][tq + 4];
+    const float zb0 = sw[cur][gq + 8][2][tq], zb1 = sw[cur][gq + 8][2][tq + 4];
+    float acc[3][4];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[c][q] = 0.f;
+#pragma unroll
+    for (int j = 0; j < TE; ++j) {
+      unsigned ah[4], al[4];
+      tf32_split(ya[j] * za0, ah[0], al[0]);
+      tf32_split(yb[j] * zb0, ah[1], al[1]);
+      tf32_split(ya[j] * za1, ah[2], al[2]);
+      tf32_split(yb[j] * zb1, ah[3], al[3]);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) mma_3xtf32(acc[c], ah, al, gh[j][c][0], gh[j][c][1], gl[j][c][0], gl[j][c][1]);
+    }
+    // contract x: lane (gq, tq) holds x = 2tq, 2tq + 1 of blobs gq (c0, c1) and gq + 8 (c2, c3)
+    const float2 wa = *reinterpret_cast<const float2*>(&sw[cur][gq][0][2 * tq]);
+    const float2 wb = *reinterpret_cast<const float2*>(&sw[cur][gq + 8][0][2 * tq]);
+    float pa[3], pb[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      pa[c] = acc[c][0] * wa.x + acc[c][1] * wa.y;
+      pb[c] = acc[c][2] * wb.x + acc[c][3] * wb.y;
+      pa[c] += __shfl_xor_sync(0xffffffffu, pa[c], 1);
+      pb[c] += __shfl_xor_sync(0xffffffffu, pb[c], 1);
+      pa[c] += __shfl_xor_sync(0xffffffffu, pa[c], 2);
+      pb[c] += __shfl_xor_sync(0xffffffffu, pb[c], 2);
+    }
+    if (tq < 2) {  // lane tq = 0 writes blob gq, lane tq = 1 blob gq + 8
+      const int k = gq + 8 * tq;
+      const unsigned fl = sflag[cur][k];
+      if (16 * r + k < b1 - b0 && ((fl >> EXM) & 63u) != 0u) {
+        const unsigned jt = (fl >> EJ) & 63u;
+        if (FCM_INB((long long)sblob[cur][k] * 64 + jt, (long long)g.nblobs * 64, BS_PARTIAL)) {
+          float* out = partial + ((size_t)sblob[cur][k] * 64 + jt) * 3;
+          out[0] = tq ? pb[0] : pa[0];
+          out[1] = tq ? pb[1] : pa[1];
+          out[2] = tq ? pb[2] : pa[2];
+        }
+      }
+    }
+  }
+}
+
+
 // V = DX^3 * sum over the blob's tiles (in canonical order j) of the partials.
 template <typename T>
 __device__ __forceinline__ void interp_reduce_one(const int* __restrict__ base, const T* __restrict__ partial,
@@ -1401,6 +1688,9 @@ int launch_spread(const Ctx& c, const BlobTable<T>& t, const double* dF, T* grid
       k_spread_tiled<T, 32><<<t.ntiles, 64, 0, s>>>(t.wc, dF, tg, t.tile_offset, t.tile_list, c.g.G, grid);
     } else if (v == 4) {
       k_spread_warp<T><<<t.ntiles, 32, 0, s>>>(t.wc, dF, tg, t.tile_offset, t.tile_list, c.g.G, grid);
+    } else if (v == 5 && sizeof(T) == 4) {
+      if constexpr (sizeof(T) == 4)
+        k_spread_mma<<<t.ntiles, 32, 0, s>>>(t.wc, dF, tg, t.tile_offset, t.tile_list, c.g.G, grid);
     } else {
       k_spread_tiled<T, 16><<<t.ntiles, 64, 0, s>>>(t.wc, dF, tg, t.tile_offset, t.tile_list, c.g.G, grid);
     }
@@ -1423,6 +1713,15 @@ int launch_interp(const Ctx& c, const BlobTable<T>& t, const T* grid, double* dV
     TileGeom g = tile_geom(c.g, t);
     g.ycut = ycut;
     const int v = c.interp_variant[sizeof(T) == 8 ? 0 : 1];
+    if constexpr (sizeof(T) == 4) {
+      if (v == 3) {
+        k_interp_mma<<<t.ntiles, 32, 0, s>>>(t.wc, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial);
+        FCM_LAUNCH_CHECK();
+        k_interp_reduce8<T><<<(t.n + 15) / 16, 128, 0, s>>>(t.base, t.partial, t.n, g, dx3, dV);
+        FCM_LAUNCH_CHECK();
+        return FCM_OK;
+      }
+    }
     if (v == 2)
       k_interp_rows<T, 2><<<t.ntiles, 32, 0, s>>>(t.wc, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial);
     else if (v == 1)

@@ -328,13 +328,14 @@ class Suspension:
     # kernel variants: [FP64 spread, FP64 solve, FP32 spread, FP32 solve, FP64
     # interp, FP32 interp]; spread 0 = persistent pipelined, 1 / 2 / 3 = one CTA
     # per tile staging 16 / 8 / 32 blobs per round, 4 = one warp per tile (two
-    # y-rows per lane);
+    # y-rows per lane), 5 = one warp per tile on the tensor cores (FP32 only);
     # solve 0 = cuFFT 3D, 1 = cuFFT (y, z) + fused x-transform, 2 = the library's
     # (y, z) + fused x; interp 0 = shuffle reduction, 64 threads per tile, 1 =
     # one warp per tile (two y-rows per lane) with the shuffle reduction, 2 = one
-    # warp per tile with a shared-memory reduction
+    # warp per tile with a shared-memory reduction, 3 = one warp per tile on the
+    # tensor cores (FP32 only)
     NUM_VARIANTS = 6
-    NUM_TUNE_TIMES = 24
+    NUM_TUNE_TIMES = 32
 
     def get_variants(self):
         v, pv = _out(None, self.NUM_VARIANTS, np.int32)
@@ -347,9 +348,9 @@ class Suspension:
 
     def autotune(self, reps=5):
         """Time every variant the grids allow and keep the fastest.  Returns
-        (variants, us): us[12 P + v] microseconds per call for precision P, v = 0-4
-        spread variants, 5, 6, 7 solve variants, 8, 9, 10 interpolation variants
-        (-1 where not available; v = 11 unused)."""
+        (variants, us): us[16 P + v] microseconds per call for precision P, v = 0-5
+        spread variants, 6, 7, 8 solve variants, 9-12 interpolation variants
+        (-1 where not available; v = 13-15 unused)."""
         us, pu = _out(None, self.NUM_TUNE_TIMES)
         v, pv = _out(None, self.NUM_VARIANTS, np.int32)
         self._c(self.L.fcm_autotune(self.h, reps, pu, pv), "fcm_autotune")
