@@ -18,6 +18,7 @@
 // atomics touch the grid.  Grids that cannot be tiled (a dimension not a multiple
 // of 8, W + 8 > n, or W > 25) use the per-blob atomic scatter.
 #include <algorithm>
+#include <map>
 #include <mutex>
 #include <string>
 #include <type_traits>
@@ -1189,13 +1190,12 @@ __device__ __forceinline__ void mma_3xtf32(float (&d)[4], const unsigned (&ah)[4
   mma_tf32(d, ah, bh0, bh1);
 }
 
-// Software pipeline of a warp's staging.  A round is RB blobs of the tile's list
-// (RB / 8 items of four parts per lane: part 0-2 the blob's x, y, z weight chunk,
-// part 3 its force or nothing); while a round is computed from one shared buffer,
-// the next round's chunks are in flight to registers and the entries of the
-// round after that are being loaded, so a warp waits on memory once per tile,
-// not once per round.  Slots past the tile's list read as entry 0, whose empty
-// half masks mark padding: zero weights and forces.
+// Staging of a warp's rounds of RB blobs (RB / 8 items of four parts per lane:
+// part 0-2 the blob's x, y, z weight chunk, part 3 its force or nothing).  The
+// kernels below keep three rounds in a pipeline: one computed from a shared
+// buffer, the next one's chunks in flight to registers, the entries of the one
+// after that being loaded.  Slots past a round's blobs read as entry 0, whose
+// empty half masks mark padding: zero weights and forces, nothing written.
 template <int RB, bool WITH_F>
 struct MmaStage {
   static constexpr int NI = RB / 8;  // items per lane
@@ -1204,12 +1204,12 @@ struct MmaStage {
   double f0[NI], f1[NI], f2[NI];     // forces in flight (part 3, WITH_F)
   unsigned long long ef[NI];         // entries of the round in flight
 
-  __device__ __forceinline__ void load_entries(const unsigned long long* __restrict__ list, int b0, int b1, int r,
+  __device__ __forceinline__ void load_entries(const unsigned long long* __restrict__ list, const TileItem& it,
                                                const TileGeom& g) {
 #pragma unroll
     for (int i = 0; i < NI; ++i) {
-      const int slot = b0 + RB * r + 8 * i + (threadIdx.x >> 2);
-      e[i] = slot < b1 ? list_entry(list, slot, g) : 0ull;
+      const int k = 8 * i + (threadIdx.x >> 2);
+      e[i] = k < it.nc ? list_entry(list, it.c0 + k, g) : 0ull;
     }
   }
   __device__ __forceinline__ void issue(const float* __restrict__ wc, const double* __restrict__ F) {
@@ -1250,6 +1250,10 @@ struct MmaStage {
   }
 };
 
+// One warp per tile in rounds of eight blobs (one k-step), the staging pipelined
+// within the tile.  (A persistent form with the pipeline running on across
+// tiles, like k_interp_mma's, measured 2% slower: its 168 registers leave fewer
+// warps per SM.)
 __global__ void __launch_bounds__(32) k_spread_mma(const float* __restrict__ wc, const double* __restrict__ F,
                                                    TileGeom g, const int* __restrict__ offset,
                                                    const unsigned long long* __restrict__ list, long long G,
@@ -1270,14 +1274,18 @@ __global__ void __launch_bounds__(32) k_spread_mma(const float* __restrict__ wc,
 #pragma unroll
       for (int r = 0; r < 4; ++r) acc[m][c][r] = 0.f;
   const int R = (b1 - b0 + 7) >> 3;  // rounds of eight blobs (one k-step)
+  auto round = [&](int r) {
+    const int c0 = b0 + 8 * r;
+    return TileItem{tile, c0, max(0, min(8, b1 - c0)), 0};
+  };
   MmaStage<8, true> st;
   if (R > 0) {
-    st.load_entries(list, b0, b1, 0, g);
+    st.load_entries(list, round(0), g);
     st.issue(wc, F);
     st.put(sw[0], sF[0], nullptr, nullptr);
-    st.load_entries(list, b0, b1, 1, g);
+    st.load_entries(list, round(1), g);
     st.issue(wc, F);
-    st.load_entries(list, b0, b1, 2, g);
+    st.load_entries(list, round(2), g);
   }
   for (int r = 0; r < R; ++r) {
     __syncwarp();
@@ -1285,7 +1293,7 @@ __global__ void __launch_bounds__(32) k_spread_mma(const float* __restrict__ wc,
     if (r + 1 < R) {
       st.put(sw[cur ^ 1], sF[cur ^ 1], nullptr, nullptr);
       st.issue(wc, F);
-      st.load_entries(list, b0, b1, r + 3, g);
+      st.load_entries(list, round(r + 3), g);
     }
     const int ka = tq, kb = tq + 4;
     // B = (F_kc wx_k[x]) for blobs ka, kb and x = gq
@@ -1330,105 +1338,159 @@ __global__ void __launch_bounds__(32) k_spread_mma(const float* __restrict__ wc,
     }
 }
 
+// Grid tile of the interpolation in shared memory: [component][x][y][z] with each
+// x-plane padded to 68 floats, so the fragment reads (eight x-planes, four z)
+// fall in 32 different banks.
+constexpr int SGX = TE * TE + 4;
+
+// Asynchronous copy of a tile's three 8^3 blocks (3 x 8 x 8 rows of 32 bytes, two
+// 16-byte copies each, twelve per lane) into sg; rows at or above ycut are left
+// to the reader, which reads them as 0.
+__device__ __forceinline__ void grid_tile_async(const float* __restrict__ grid, const TileGeom& g, long long G,
+                                                int tile, float* sg) {
+  const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
+#pragma unroll
+  for (int q = 0; q < 12; ++q) {
+    const int i = threadIdx.x + 32 * q, row = i >> 1, half = i & 1;
+    const int c = row >> 6, x = (row >> 3) & 7, y = row & 7;
+    const long long idx = ((long long)(tx * TE + x) * g.ny + ty * TE + y) * g.nz + tz * TE + 4 * half;
+    float* dst = sg + c * TE * SGX + x * SGX + y * TE + 4 * half;
+    if (FCM_INB(idx + 3, G, BS_GRID))
+      cp_async16(dst, grid + c * G + idx);
+    else
+      *reinterpret_cast<float4*>(dst) = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  cp_async_commit();
+}
+
+// Persistent like k_spread_mma, in rounds of 16 blobs (one m-tile); the grid of
+// the warp's next tile is copied to the other shared buffer while the current
+// tile's rounds run, and turned into operand fragments when that tile starts.
 __global__ void __launch_bounds__(32) k_interp_mma(const float* __restrict__ wc, const float* __restrict__ grid,
                                                    TileGeom g, const int* __restrict__ offset,
                                                    const unsigned long long* __restrict__ list, long long G,
-                                                   float* __restrict__ partial) {
-  __shared__ __align__(16) float sw[2][16][3][TE];
-  __shared__ unsigned sflag[2][16], sblob[2][16];
-  const int tile = blockIdx.x;
-  if (!FCM_INB(tile, (long long)g.ntx * g.nty * g.ntz, BS_TILE)) return;  // uniform over the warp
-  int b0, b1;
-  tile_range(offset, tile, g, b0, b1);
-  if (b0 == b1) return;  // no blob meets this tile
-  const int tz = tile % g.ntz, ty = (tile / g.ntz) % g.nty, tx = tile / (g.ntz * g.nty);
+                                                   float* __restrict__ partial, int ntiles) {
+  __shared__ __align__(16) float sw[2][SCB][3][TE];
+  __shared__ unsigned sflag[2][SCB], sblob[2][SCB];
+  __shared__ __align__(16) float sg[2][3 * TE * SGX];
+  ItemGen gen{offset, ntiles, (int)gridDim.x, 0, 0, 0, 0, 0, 0, 0};
+  if (!gen.first()) return;  // uniform over the warp
+  TileItem cur = gen.item();
+  grid_tile_async(grid, g, G, cur.tile, sg[0]);
+  bool v1 = gen.next();
+  TileItem nx1 = v1 ? gen.item() : TileItem{0, 0, 0, 0};
+  bool v2 = v1 && gen.next();
+  TileItem nx2 = v2 ? gen.item() : TileItem{0, 0, 0, 0};
   const int lane = threadIdx.x, gq = lane >> 2, tq = lane & 3;
-  const int R = (b1 - b0 + 15) >> 4;  // rounds of sixteen blobs (one m-tile)
-  MmaStage<16, false> st;
-  st.load_entries(list, b0, b1, 0, g);
+  MmaStage<SCB, false> st;
+  st.load_entries(list, cur, g);
   st.issue(wc, nullptr);
-  // the tile's grid as B fragments: k-step j holds rows (y, z) = (j, tq), (j, tq + 4)
-  // and column x = gq of each component (loaded while round 0 is in flight)
-  unsigned gh[TE][3][2], gl[TE][3][2];
-  {
-    const int ox = tx * TE + gq, oz = tz * TE + tq;
-#pragma unroll
-    for (int j = 0; j < TE; ++j) {
-      const int oy = ty * TE + j;
-      const bool live = oy < g.ycut;  // rows at or above the slip channel's upper wall read as 0
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const long long idx = ((long long)ox * g.ny + oy) * g.nz + oz + 4 * h;
-        const bool in = live && FCM_INB(idx, G, BS_GRID);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) tf32_split(in ? grid[c * G + idx] : 0.f, gh[j][c][h], gl[j][c][h]);
-      }
-    }
-  }
   st.put(sw[0], nullptr, sflag[0], sblob[0]);
-  if (R > 1) {
-    st.load_entries(list, b0, b1, 1, g);
+  if (v1) {
+    st.load_entries(list, nx1, g);
     st.issue(wc, nullptr);
-    st.load_entries(list, b0, b1, 2, g);
   }
-  for (int r = 0; r < R; ++r) {
+  if (v2) st.load_entries(list, nx2, g);
+  unsigned gh[TE][3][2], gl[TE][3][2];
+  bool first = true;  // cur is the first round of its tile
+  int gbuf = 0, buf = 0;
+  while (true) {
+    if (first) {
+      // this tile's grid (copied while the previous tile ran) into fragments: k-step j
+      // holds rows (y, z) = (j, tq), (j, tq + 4) and column x = gq of each component
+      cp_async_wait_all();
+      __syncwarp();
+      const int ty = (cur.tile / g.ntz) % g.nty;
+      const float* sgt = sg[gbuf];
+#pragma unroll
+      for (int j = 0; j < TE; ++j) {
+        const bool live = ty * TE + j < g.ycut;  // rows at or above the slip channel's upper wall read as 0
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            tf32_split(live ? sgt[c * TE * SGX + gq * SGX + j * TE + tq + 4 * h] : 0.f, gh[j][c][h], gl[j][c][h]);
+      }
+      gbuf ^= 1;
+      const int nt = cur.tile + (int)gridDim.x;
+      if (nt < ntiles) grid_tile_async(grid, g, G, nt, sg[gbuf]);
+    }
     __syncwarp();
-    const int cur = r & 1;
-    if (r + 1 < R) {
-      st.put(sw[cur ^ 1], nullptr, sflag[cur ^ 1], sblob[cur ^ 1]);
-      st.issue(wc, nullptr);
-      st.load_entries(list, b0, b1, r + 3, g);
-    }
-    // rows of A: blobs gq and gq + 8; columns (y, z) = (j, tq), (j, tq + 4)
-    float ya[TE], yb[TE];
-    *reinterpret_cast<float4*>(ya) = *reinterpret_cast<const float4*>(&sw[cur][gq][1][0]);
-    *reinterpret_cast<float4*>(ya + 4) = *reinterpret_cast<const float4*>(&sw[cur][gq][1][4]);
-    *reinterpret_cast<float4*>(yb) = *reinterpret_cast<const float4*>(&sw[cur][gq + 8][1][0]);
-    *reinterpret_cast<float4*>(yb + 4) = *reinterpret_cast<const float4*>(&sw[cur][gq + 8][1][4]);
-    const float za0 = sw[cur][gq][2][tq], za1 = sw[cur][gq][2][tq + 4];
-    const float zb0 = sw[cur][gq + 8][2][tq], zb1 = sw[cur][gq + 8][2][tq + 4];
-    float acc[3][4];
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) acc[c][q] = 0.f;
-#pragma unroll
-    for (int j = 0; j < TE; ++j) {
-      unsigned ah[4], al[4];
-      tf32_split(ya[j] * za0, ah[0], al[0]);
-      tf32_split(yb[j] * zb0, ah[1], al[1]);
-      tf32_split(ya[j] * za1, ah[2], al[2]);
-      tf32_split(yb[j] * zb1, ah[3], al[3]);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) mma_3xtf32(acc[c], ah, al, gh[j][c][0], gh[j][c][1], gl[j][c][0], gl[j][c][1]);
-    }
-    // contract x: lane (gq, tq) holds x = 2tq, 2tq + 1 of blobs gq (c0, c1) and gq + 8 (c2, c3)
-    const float2 wa = *reinterpret_cast<const float2*>(&sw[cur][gq][0][2 * tq]);
-    const float2 wb = *reinterpret_cast<const float2*>(&sw[cur][gq + 8][0][2 * tq]);
-    float pa[3], pb[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      pa[c] = acc[c][0] * wa.x + acc[c][1] * wa.y;
-      pb[c] = acc[c][2] * wb.x + acc[c][3] * wb.y;
-      pa[c] += __shfl_xor_sync(0xffffffffu, pa[c], 1);
-      pb[c] += __shfl_xor_sync(0xffffffffu, pb[c], 1);
-      pa[c] += __shfl_xor_sync(0xffffffffu, pa[c], 2);
-      pb[c] += __shfl_xor_sync(0xffffffffu, pb[c], 2);
-    }
-    if (tq < 2) {  // lane tq = 0 writes blob gq, lane tq = 1 blob gq + 8
-      const int k = gq + 8 * tq;
-      const unsigned fl = sflag[cur][k];
-      if (16 * r + k < b1 - b0 && ((fl >> EXM) & 63u) != 0u) {
-        const unsigned jt = (fl >> EJ) & 63u;
-        if (FCM_INB((long long)sblob[cur][k] * 64 + jt, (long long)g.nblobs * 64, BS_PARTIAL)) {
-          float* out = partial + ((size_t)sblob[cur][k] * 64 + jt) * 3;
-          out[0] = tq ? pb[0] : pa[0];
-          out[1] = tq ? pb[1] : pa[1];
-          out[2] = tq ? pb[2] : pa[2];
+    bool v3 = false;
+    TileItem nx3{0, 0, 0, 0};
+    if (v1) {
+      st.put(sw[buf ^ 1], nullptr, sflag[buf ^ 1], sblob[buf ^ 1]);
+      if (v2) {
+        st.issue(wc, nullptr);
+        v3 = gen.next();
+        if (v3) {
+          nx3 = gen.item();
+          st.load_entries(list, nx3, g);
         }
       }
     }
+    if (cur.nc > 0) {  // uniform over the warp
+      // rows of A: blobs gq and gq + 8; columns (y, z) = (j, tq), (j, tq + 4)
+      float ya[TE], yb[TE];
+      *reinterpret_cast<float4*>(ya) = *reinterpret_cast<const float4*>(&sw[buf][gq][1][0]);
+      *reinterpret_cast<float4*>(ya + 4) = *reinterpret_cast<const float4*>(&sw[buf][gq][1][4]);
+      *reinterpret_cast<float4*>(yb) = *reinterpret_cast<const float4*>(&sw[buf][gq + 8][1][0]);
+      *reinterpret_cast<float4*>(yb + 4) = *reinterpret_cast<const float4*>(&sw[buf][gq + 8][1][4]);
+      const float za0 = sw[buf][gq][2][tq], za1 = sw[buf][gq][2][tq + 4];
+      const float zb0 = sw[buf][gq + 8][2][tq], zb1 = sw[buf][gq + 8][2][tq + 4];
+      float acc[3][4];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[c][q] = 0.f;
+#pragma unroll
+      for (int j = 0; j < TE; ++j) {
+        unsigned ah[4], al[4];
+        tf32_split(ya[j] * za0, ah[0], al[0]);
+        tf32_split(yb[j] * zb0, ah[1], al[1]);
+        tf32_split(ya[j] * za1, ah[2], al[2]);
+        tf32_split(yb[j] * zb1, ah[3], al[3]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          mma_3xtf32(acc[c], ah, al, gh[j][c][0], gh[j][c][1], gl[j][c][0], gl[j][c][1]);
+      }
+      // contract x: lane (gq, tq) holds x = 2tq, 2tq + 1 of blobs gq (c0, c1) and gq + 8 (c2, c3)
+      const float2 wa = *reinterpret_cast<const float2*>(&sw[buf][gq][0][2 * tq]);
+      const float2 wb = *reinterpret_cast<const float2*>(&sw[buf][gq + 8][0][2 * tq]);
+      float pa[3], pb[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        pa[c] = acc[c][0] * wa.x + acc[c][1] * wa.y;
+        pb[c] = acc[c][2] * wb.x + acc[c][3] * wb.y;
+        pa[c] += __shfl_xor_sync(0xffffffffu, pa[c], 1);
+        pb[c] += __shfl_xor_sync(0xffffffffu, pb[c], 1);
+        pa[c] += __shfl_xor_sync(0xffffffffu, pa[c], 2);
+        pb[c] += __shfl_xor_sync(0xffffffffu, pb[c], 2);
+      }
+      if (tq < 2) {  // lane tq = 0 writes blob gq, lane tq = 1 blob gq + 8
+        const int k = gq + 8 * tq;
+        const unsigned fl = sflag[buf][k];
+        if (k < cur.nc && ((fl >> EXM) & 63u) != 0u) {
+          const unsigned jt = (fl >> EJ) & 63u;
+          if (FCM_INB((long long)sblob[buf][k] * 64 + jt, (long long)g.nblobs * 64, BS_PARTIAL)) {
+            float* out = partial + ((size_t)sblob[buf][k] * 64 + jt) * 3;
+            out[0] = tq ? pb[0] : pa[0];
+            out[1] = tq ? pb[1] : pa[1];
+            out[2] = tq ? pb[2] : pa[2];
+          }
+        }
+      }
+    }
+    first = cur.last != 0;
+    if (!v1) break;
+    cur = nx1;
+    nx1 = nx2;
+    v1 = v2;
+    nx2 = nx3;
+    v2 = v3;
+    buf ^= 1;
   }
+  cp_async_wait_all();  // no copy outlives the kernel
 }
 
 
@@ -1580,22 +1642,24 @@ TileGeom tile_geom(const GridDims& g, int W, int nblobs, long long list_cap) {
 }
 
 // CTAs of a persistent kernel: as many as fit on the device at once
-// (resident CTAs per SM x SMs), looked up once per kernel and device.
+// (resident CTAs per SM x SMs), looked up once per kernel and device (keyed by
+// the kernel's address: kernels of one signature share this instantiation).
 template <typename K>
 int persistent_ctas(K kernel, int threads, int device) {
   static std::mutex mtx;
-  static int cache[64] = {0};
+  static std::map<std::pair<const void*, int>, int> cache;
   std::lock_guard<std::mutex> lock(mtx);
   const int dev = (device >= 0 && device < 64) ? device : 0;
-  if (!cache[dev]) {
+  int& n = cache[{reinterpret_cast<const void*>(kernel), dev}];
+  if (!n) {
     int per_sm = 0, sms = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm < 1)
       per_sm = 1;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 1;
     cudaGetLastError();
-    cache[dev] = per_sm * sms;
+    n = per_sm * sms;
   }
-  return cache[dev];
+  return n;
 }
 
 template <typename T>
@@ -1714,8 +1778,10 @@ int launch_interp(const Ctx& c, const BlobTable<T>& t, const T* grid, double* dV
     g.ycut = ycut;
     const int v = c.interp_variant[sizeof(T) == 8 ? 0 : 1];
     if constexpr (sizeof(T) == 4) {
-      if (v == 3) {
-        k_interp_mma<<<t.ntiles, 32, 0, s>>>(t.wc, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial);
+      // the tensor-core kernel copies 16-byte rows of the grid asynchronously
+      if (v == 3 && (reinterpret_cast<uintptr_t>(grid) & 15u) == 0) {
+        k_interp_mma<<<std::min(t.ntiles, persistent_ctas(k_interp_mma, 32, c.device)), 32, 0, s>>>(
+            t.wc, grid, g, t.tile_offset, t.tile_list, c.g.G, t.partial, t.ntiles);
         FCM_LAUNCH_CHECK();
         k_interp_reduce8<T><<<(t.n + 15) / 16, 128, 0, s>>>(t.base, t.partial, t.n, g, dx3, dV);
         FCM_LAUNCH_CHECK();
