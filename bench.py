@@ -272,7 +272,7 @@ def rel_vel_error(p, ref, x, q, fe, stream):
             float(np.linalg.norm(L32 - L64) / np.linalg.norm(L64)))
 
 
-def step_velocity_errors(p, ref, x, q, fe, seed, start, K, stream):
+def step_velocity_errors(p, ref, x, q, fe, seed, start, K, stream, variants=None):
     """Relative body- and blob-velocity error of the mixed-precision step against
     the FP64 step on each of K steps of the mixed trajectory, replayed untimed
     from the state the timed region started from (step indices start ..
@@ -281,14 +281,17 @@ def step_velocity_errors(p, ref, x, q, fe, seed, start, K, stream):
     (seed, index); each forms its own random velocities (FP32 grid in the mixed
     context), forces and RHS, and solves (FP64 to the workload's tolerance, mixed
     with FP64 refinement to MIXED_TOL); the mixed context then advances with its
-    own solution and the FP64 context takes its bodies.  Returns per-step lists
-    (bodies, blobs)."""
+    own solution and the FP64 context takes its bodies.  variants ({precision:
+    kernel variants}) gives each context the kernels its timed arm ran with.
+    Returns per-step lists (bodies, blobs)."""
     ctx = {}
     for prec in (0, 1):
         pp = p.copy(precision=prec)
         if prec == 1:
             pp.gmres_tol = MIXED_TOL
         ctx[prec] = setup_suspension(pp, ref, x, q, fe, stream, tune=False)
+        if variants and variants.get(prec):
+            ctx[prec].set_variants(variants[prec])
     Nb = p.num_blobs
     eU, eL = [], []
     for k in range(K):
@@ -435,11 +438,14 @@ def run_ours(args):
     step_err = None
     if rank == 0 and not args.no_step_errors:
         x0, q0 = results["mixed"]["start"]
-        eU, eL = step_velocity_errors(p, ref, x0, q0, fe, seed, args.warmup, args.steps, stream)
+        tuned = {prec: (results[tag]["tuning"] or {}).get("variants") for prec, tag in ((0, "fp64"), (1, "mixed"))}
+        eU, eL = step_velocity_errors(p, ref, x0, q0, fe, seed, args.warmup, args.steps, stream, tuned)
         step_err = {"steps": len(eU), "bodies": {"max": max(eU), "mean": float(np.mean(eU))},
                     "blobs": {"max": max(eL), "mean": float(np.mean(eL))},
-                    "what": "every timed step replayed untimed: the mixed step's body and blob velocities "
-                            "against the FP64 step's on the same bodies and Philox noise"}
+                    "variants": tuned,
+                    "what": "every timed step replayed untimed with the timed arms' kernel variants: the mixed "
+                            "step's body and blob velocities against the FP64 step's on the same bodies and "
+                            "Philox noise"}
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
