@@ -1166,11 +1166,12 @@ __global__ void __launch_bounds__(32) k_interp_warp(const T* __restrict__ wc, co
 // column-major) b0 (t, g), b1 (t + 4, g); C (16 x 8) c0 (g, 2t), c1 (g, 2t + 1),
 // c2 (g + 8, 2t), c3 (g + 8, 2t + 1).
 
-// a = hi + lo with hi the TF32 rounding of a (low 13 mantissa bits zero) and lo
-// the exact FP32 remainder (read as TF32 by the tensor core).
+// a = hi + lo with hi the TF32 rounding of a (low 13 mantissa bits zero; to
+// nearest, ties away from zero: half of bit 13 added to the magnitude bits, then
+// truncated, a carry into the exponent rounding up a binade) and lo the exact
+// FP32 remainder (Sterbenz), read as TF32 by the tensor core.  Finite a only.
 __device__ __forceinline__ void tf32_split(float a, unsigned& hi, unsigned& lo) {
-  unsigned h;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(a));
+  const unsigned h = (__float_as_uint(a) + 0x1000u) & 0xffffe000u;
   hi = h;
   lo = __float_as_uint(a - __uint_as_float(h));
 }
