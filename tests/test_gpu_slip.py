@@ -175,3 +175,28 @@ def test_slip_shear_flow_and_refusals(gpu):
         g.set_up_dipole_distribution(T=np.zeros(3 * p.num_blobs))
     with pytest.raises(FcmError):
         Batch([(p, ref)])
+
+
+def test_slip_fp32_tile_variants_match_oracle(gpu):
+    """The FP32 tile kernels in the channel, where the force grid is mirrored and
+    the interpolation reads nothing at or above the upper wall (ny/2): each FP32
+    spread and interpolation variant, the tensor-core ones included, within 1e-5
+    of the oracle's FP64 channel mobility."""
+    p, ref, x, q, fe = _channel()
+    p32 = p.copy(precision=1)
+    g = Suspension(p32, ref)
+    o = Oracle(p, ref)
+    for s in (g, o):
+        s.set_bodies(x, q)
+        s.fill_all_blob_pos()
+        s.set_up_gaussians()
+    F = np.random.default_rng(5).standard_normal(3 * p.num_blobs)
+    Vo = o.apply_mobility(F)
+    for sp in (0, 4, 5):
+        for ip in (1, 3):
+            v = g.get_variants()
+            v[2], v[5] = sp, ip
+            g.set_variants(v)
+            g.spread(F, 1)
+            g.stokes_solve(1)
+            assert rel_err(g.interp(1), Vo) < 1e-5, (sp, ip)
