@@ -114,3 +114,13 @@ def test_ensemble_members_are_valid():
         assert not len(pr) or np.all(body[pr[:, 0]] == body[pr[:, 1]])
     assert configs.nearest_fft_size(117) == 128 and configs.nearest_fft_size(40) == 64
     assert configs.nearest_fft_size(100) == 96
+
+
+def test_array_sizes_match_header():
+    """The Python mirror's array sizes of the variant calls equal the header's
+    (fcm_get/set_variants, fcm_autotune: 16 timings per precision)."""
+    from timstochrigidbodiessim_b200.fcm import Suspension
+    txt = open(HEADER).read()
+    defs = dict(re.findall(r"#define\s+(FCM_[A-Z_]+)\s+(\d+)", txt))
+    assert int(defs["FCM_NUM_VARIANTS"]) == Suspension.NUM_VARIANTS == 6
+    assert int(defs["FCM_NUM_TUNE_TIMES"]) == Suspension.NUM_TUNE_TIMES == 32
